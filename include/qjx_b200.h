@@ -1,0 +1,139 @@
+/*
+ * qjx_b200.h -- C ABI of the B200 quantum-jump trajectory engine (os_d_b200).
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary; every call returns
+ * a qjx_status and qjx_last_error() gives the message.  Complex arrays are interleaved
+ * (re, im) doubles, matrices row-major d x d, exactly like MKL_Complex16 arrays in the
+ * reference (source/cpp/QJX/QJX/data.h:36-58).  The caller owns every host buffer; the
+ * engine owns its device memory and copies in/out.  A handle is bound to one CUDA
+ * stream and is not re-entrant; distinct handles may run concurrently.
+ *
+ * Which reference interface each entry point replaces:
+ *   qjx_create           init_split_structure_dimer + copies per thread
+ *                        (source/cpp/QJX/QJX/core.cpp:6-22, 9880-9926; qj_proc.cpp:122-167)
+ *   qjx_set_states       StdNewDelBehaviour::init_data -> init_basic_data / init_start_state
+ *                        (source/cpp/QJX/QJX/newdel_exp.cpp:98-117, 332-375, 656-679)
+ *   qjx_set_uniforms     the per-trajectory VSL streams (newdel_exp.cpp:244-296): the caller
+ *                        may inject any pre-generated uniform sequence instead of Philox
+ *   qjx_init_thresholds  eta_0 draw of trans_process_single (experiment.cpp:3249-3265)
+ *   qjx_run_periods      the OpenMP loop over trajectories calling PropagateBehavior::one_period
+ *                        -> DimerCoreBehaviour::ex_period -> one_period_branch
+ *                        (experiment.cpp:411-430, 477-501; propagator.cpp:27-30; core.cpp:84-95;
+ *                        qj_proc.cpp:271-343), batched over all trajectories, with the
+ *                        per-dump calc_chars_std fused in (core.cpp:697-725)
+ *   qjx_reset_times      resresh_times (experiment.cpp:2214-2219)
+ *   qjx_observe          calc_chars_std_start / calc_chars_std (core.cpp:665-725)
+ *   qjx_get_observables  ed->norm_evo / mean_evo / ... arrays (core.cpp:795-816)
+ *   qjx_get_jumps        ed->jump_times / diss_types / jump_norms / jump_etas (qj_proc.cpp:296-307,
+ *                        experiment.cpp:1371-1374)
+ *   qjx_build_dimer      DimerNewDelBehaviour::init_sizes/init_hamiltonians/init_dissipators/
+ *                        init_hamiltonians_qj + init_split_branches (newdel.cpp:3-37, 450-498,
+ *                        1454-1498, 2285-2388; qj_proc.cpp:4-120)
+ *   qjx_fb_*             f-basis Lindblad RK4 (source/cpp/CQdiss_os_dimer/CQdiss/calcODE.cpp:75-118,
+ *                        249-389)
+ */
+#ifndef QJX_B200_H
+#define QJX_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    QJX_OK = 0,
+    QJX_ERR_INVALID_ARG = 1,
+    QJX_ERR_OOM = 2,
+    QJX_ERR_NORM_GT_ONE = 3,        /* replaces the throw in is_norm_crossed (experiment.cpp:1247-1251) */
+    QJX_ERR_RNG_EXHAUSTED = 4,      /* injected uniform sequence of a trajectory ran out */
+    QJX_ERR_ZERO_JUMP_WEIGHTS = 5,  /* every jump channel had zero weight (reference loops forever) */
+    QJX_ERR_TIMEOUT = 6,            /* a bounded device wait gave up */
+    QJX_ERR_CUDA = 7,
+    QJX_ERR_UNSUPPORTED = 8,
+    QJX_ERR_STATE = 9
+} qjx_status;
+
+typedef struct qjx_engine qjx_engine;
+
+typedef struct {
+    int d;             /* sys_size (N + 1 for the dimer) */
+    int n_traj;        /* num_trajectories */
+    int deep;          /* ex_deep: split levels per branch */
+    int num_branches;  /* num_ham_qj */
+    int num_diss;      /* number of jump operators */
+    int num_robs;      /* number of random observables */
+    double T;          /* period */
+    int record;        /* params "jump": 0 none, 1 times + types, 2 also norms + etas */
+    int rng_kind;      /* 0: Philox4x32-10 (seed, trajectory, draw index); 1: injected uniforms */
+    uint64_t seed;
+    int rec_cap;       /* jump records buffered on the device per trajectory (0 -> 1024) */
+    int keep_adr;      /* 0: keep the latest |psi_k|^2/|psi|^2 only; 1: keep it for every dump */
+    int max_dumps;     /* capacity of the observable arrays (dump_num_total) */
+    int device;        /* CUDA device ordinal */
+} qjx_config;
+
+typedef struct {
+    int64_t micro_steps;     /* lock-step micro-steps launched */
+    int64_t matvecs;         /* complex d x d matvecs executed (trajectory-steps) */
+    int64_t jumps;           /* jumps recorded */
+    double kernel_ms;        /* device time of the micro-step kernels (CUDA events) */
+    double last_call_ms;     /* device time of the last run/observe call */
+} qjx_stats;
+
+/* U: [num_branches][deep][d][d] split propagators exp(K_b dt_l), dt_l = T 2^-(l+2).
+ * L: [num_diss][d][d] jump operators; g: [num_diss] rates (head->g, core.cpp:9905).
+ * HE: [d][d] energy operator H + E0 * H_drv (experiment.cpp:1440).  R: [num_robs][d][d]. */
+qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, const double *g,
+                      const double *HE, const double *R, qjx_engine **out);
+void qjx_destroy(qjx_engine *h);
+const char *qjx_last_error(const qjx_engine *h);
+const char *qjx_status_string(qjx_status s);
+
+/* psi: [n_traj][d] complex initial states; resets times, counters and records. */
+qjx_status qjx_set_states(qjx_engine *h, const double *psi);
+/* Injected uniforms (rng_kind 1): u concatenated, offsets [n_traj + 1]. */
+qjx_status qjx_set_uniforms(qjx_engine *h, const double *u, const int64_t *offsets);
+qjx_status qjx_init_thresholds(qjx_engine *h);
+/* Advance every trajectory by n_periods periods.  is_obs gates jump recording like ed->is_obs.
+ * dump_at[i] (ascending, 1..n_periods) are period counts, relative to this call, after which
+ * observables are taken into dump slot dump_base + i. */
+qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, const int *dump_at, int n_dumps,
+                           int dump_base);
+qjx_status qjx_reset_times(qjx_engine *h);
+/* Observables of the current states into dump slot `dump`; is_start writes mean_start. */
+qjx_status qjx_observe(qjx_engine *h, int dump, int is_start);
+/* Per-dump arrays laid out [dump][trajectory]; robs [dump][trajectory][num_robs] complex;
+ * adr [dump][trajectory][d] (keep_adr 1) or [trajectory][d] latest (keep_adr 0).  NULL skips. */
+qjx_status qjx_get_observables(qjx_engine *h, int dump0, int n_dumps, double *norm, double *mean,
+                               double *dispersion, double *m2, double *energy, double *robs, double *adr);
+qjx_status qjx_get_mean_start(qjx_engine *h, double *mean_start);
+/* Current states [n_traj][d] complex, times, etas, jump counts (any pointer may be NULL). */
+qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, int *jumps_counts);
+/* Jump records of one trajectory accumulated since qjx_set_states. */
+qjx_status qjx_jump_count(qjx_engine *h, int tr, int64_t *count);
+qjx_status qjx_get_jumps(qjx_engine *h, int tr, double *times, int *types, double *norms, double *etas);
+qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats);
+
+/* Dimer model on the host (FP64): H, Hd, L [d][d]; Utree [2][deep][d][d] (any may be NULL). */
+qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
+                           double *H, double *Hd, double *L, double *Utree);
+/* exp(A) of a complex n x n matrix, Higham (2005) scaling and squaring. */
+qjx_status qjx_expm(int n, const double *A, double *out);
+
+/* ---- f-basis Lindblad RK4 (density-matrix oracle of the ensemble) ---- */
+typedef struct qjx_fb qjx_fb;
+/* CSR (0-based) Gs and Qs_drv of size n x n, Ks [n]; x0 [n] initial f-vector.
+ * drv_type 0: E(t) = -A sign(sin(w t + phase)), 1: -A sin(w t + phase) (calcODE.cpp:91-117). */
+qjx_status qjx_fb_create(int n, const int *gs_rowptr, const int *gs_col, const double *gs_val,
+                         const int *qs_rowptr, const int *qs_col, const double *qs_val, const double *Ks,
+                         const double *x0, double drv_ampl, double drv_freq, double drv_phase, int drv_type,
+                         double T, int num_steps, int device, qjx_fb **out);
+/* Integrate n_periods periods of num_steps RK4 steps starting at period index period0. */
+qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods);
+qjx_status qjx_fb_get(qjx_fb *h, double *x, double *last_period_ms);
+void qjx_fb_destroy(qjx_fb *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,194 @@
+"""ctypes bindings of the CPU oracle (TEST INFRASTRUCTURE).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this
+module; the product (os_d_b200) never does.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build_oracle
+
+_lib = None
+
+c_double_p = C.POINTER(C.c_double)
+c_int_p = C.POINTER(C.c_int)
+c_i64_p = C.POINTER(C.c_int64)
+
+
+class OrcProblem(C.Structure):
+    _fields_ = [("d", C.c_int), ("n_traj", C.c_int), ("deep", C.c_int), ("num_branches", C.c_int),
+                ("num_diss", C.c_int), ("num_robs", C.c_int), ("record", C.c_int), ("rng_kind", C.c_int),
+                ("T", C.c_double), ("seed", C.c_uint64),
+                ("U", c_double_p), ("L", c_double_p), ("g", c_double_p), ("HE", c_double_p), ("R", c_double_p),
+                ("inj_u", c_double_p), ("inj_off", c_i64_p)]
+
+
+class OrcState(C.Structure):
+    _fields_ = [("phi", c_double_p), ("eta", c_double_p), ("t", c_double_p), ("rng_pos", c_i64_p),
+                ("jumps_counts", c_int_p), ("matvecs", c_i64_p), ("rec_cap", C.c_int), ("n_rec", c_int_p),
+                ("jump_times", c_double_p), ("jump_norms", c_double_p), ("jump_etas", c_double_p),
+                ("diss_types", c_int_p), ("error", c_int_p)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = build_oracle.build()
+        _lib = C.CDLL(path)
+        L = _lib
+        L.orc_dimer_operators.argtypes = [C.c_int] + [C.c_double] * 5 + [c_double_p] * 5
+        L.orc_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
+        L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
+        L.orc_philox_uniform.restype = C.c_double
+        L.orc_init.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int, C.c_int]
+        L.orc_run_periods.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_int]
+        L.orc_observables.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int] + [c_double_p] * 8
+        L.orc_dump_periods.argtypes = [C.c_int, C.c_int, C.c_int, c_int_p]
+        L.orc_matvec.argtypes = [C.c_int, c_double_p, c_double_p, c_double_p]
+        L.orc_norm_square.argtypes = [C.c_int, c_double_p]
+        L.orc_norm_square.restype = C.c_double
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(c_double_p) if a is not None else None
+
+
+def _cplx(shape):
+    return np.zeros(shape, dtype=np.complex128)
+
+
+def dimer_operators(N, J, U, E, A, g):
+    d = N + 1
+    H, Hd, L, K0, K1 = (_cplx((d, d)) for _ in range(5))
+    rc = lib().orc_dimer_operators(N, J, U, E, A, g, _dp(H), _dp(Hd), _dp(L), _dp(K0), _dp(K1))
+    assert rc == 0
+    return H, Hd, L, K0, K1
+
+
+def expm(A):
+    A = np.ascontiguousarray(A, dtype=np.complex128)
+    out = np.empty_like(A)
+    assert lib().orc_expm(A.shape[0], _dp(A), _dp(out)) == 0
+    return out
+
+
+def split_tree(K, T, deep):
+    K = np.ascontiguousarray(K, dtype=np.complex128)
+    d = K.shape[0]
+    out = np.empty((deep, d, d), dtype=np.complex128)
+    assert lib().orc_split_tree(d, _dp(K), T, deep, _dp(out)) == 0
+    return out
+
+
+def philox4x32_10(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().orc_philox4x32_10(c, k, o)
+    return list(o)
+
+
+def philox_uniform(seed, tr, idx):
+    return lib().orc_philox_uniform(seed, tr, idx)
+
+
+def matvec(M, x):
+    M = np.ascontiguousarray(M, dtype=np.complex128)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.empty_like(x)
+    lib().orc_matvec(M.shape[0], _dp(M), _dp(x), _dp(out))
+    return out
+
+
+def norm_square(x):
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    return lib().orc_norm_square(x.shape[0], _dp(x))
+
+
+def dump_periods(dump_type, dump_num, num_obs_periods):
+    out = np.zeros(dump_num + 2, dtype=np.int32)
+    n = lib().orc_dump_periods(dump_type, dump_num, num_obs_periods, out.ctypes.data_as(c_int_p))
+    assert n > 0
+    return out[:n].copy()
+
+
+class Ensemble:
+    """One QJ ensemble run by the oracle, mirroring the Std task flow."""
+
+    def __init__(self, U, L, g, HE, R, T, n_traj, seed=0, record=2, rng_kind=0, inj_u=None, inj_off=None,
+                 rec_cap=4096):
+        self.U = np.ascontiguousarray(U, dtype=np.complex128)  # [nb, deep, d, d]
+        nb, deep, d, _ = self.U.shape
+        self.L = np.ascontiguousarray(L, dtype=np.complex128).reshape(-1, d, d)
+        self.g = np.ascontiguousarray(g, dtype=np.float64)
+        self.HE = np.ascontiguousarray(HE, dtype=np.complex128)
+        self.R = np.ascontiguousarray(R if R is not None and len(R) else np.zeros((0, d, d)), dtype=np.complex128)
+        self.d, self.n, self.deep, self.nb = d, n_traj, deep, nb
+        self.inj_u = None if inj_u is None else np.ascontiguousarray(inj_u, dtype=np.float64)
+        self.inj_off = None if inj_off is None else np.ascontiguousarray(inj_off, dtype=np.int64)
+        p = OrcProblem()
+        p.d, p.n_traj, p.deep, p.num_branches = d, n_traj, deep, nb
+        p.num_diss, p.num_robs, p.record, p.rng_kind = self.L.shape[0], self.R.shape[0], record, rng_kind
+        p.T, p.seed = T, seed
+        p.U, p.L, p.g, p.HE = _dp(self.U), _dp(self.L), _dp(self.g), _dp(self.HE)
+        p.R = _dp(self.R) if self.R.size else None
+        p.inj_u = _dp(self.inj_u)
+        p.inj_off = self.inj_off.ctypes.data_as(c_i64_p) if self.inj_off is not None else None
+        self.p = p
+        n = n_traj
+        self.phi = _cplx((n, d))
+        self.eta = np.zeros(n)
+        self.t = np.zeros(n)
+        self.rng_pos = np.zeros(n, np.int64)
+        self.jumps_counts = np.zeros(n, np.int32)
+        self.matvecs = np.zeros(n, np.int64)
+        self.rec_cap = rec_cap
+        self.n_rec = np.zeros(n, np.int32)
+        self.jump_times = np.zeros((n, rec_cap))
+        self.jump_norms = np.zeros((n, rec_cap))
+        self.jump_etas = np.zeros((n, rec_cap))
+        self.diss_types = np.zeros((n, rec_cap), np.int32)
+        self.error = np.zeros(n, np.int32)
+        s = OrcState()
+        s.phi, s.eta, s.t = _dp(self.phi), _dp(self.eta), _dp(self.t)
+        s.rng_pos = self.rng_pos.ctypes.data_as(c_i64_p)
+        s.jumps_counts = self.jumps_counts.ctypes.data_as(c_int_p)
+        s.matvecs = self.matvecs.ctypes.data_as(c_i64_p)
+        s.rec_cap = rec_cap
+        s.n_rec = self.n_rec.ctypes.data_as(c_int_p)
+        s.jump_times, s.jump_norms, s.jump_etas = _dp(self.jump_times), _dp(self.jump_norms), _dp(self.jump_etas)
+        s.diss_types = self.diss_types.ctypes.data_as(c_int_p)
+        s.error = self.error.ctypes.data_as(c_int_p)
+        self.s = s
+        self.mean_start = np.zeros(n)
+
+    def init(self, start_type=0, start_state=0):
+        lib().orc_init(C.byref(self.p), C.byref(self.s), start_type, start_state)
+
+    def run_periods(self, n_periods, is_obs=1, tr0=0, tr1=None, n_threads=0):
+        tr1 = self.n if tr1 is None else tr1
+        return lib().orc_run_periods(C.byref(self.p), C.byref(self.s), tr0, tr1, n_periods, is_obs, n_threads)
+
+    def observables(self, is_start=False, want_adr=False):
+        n, d = self.n, self.d
+        out = {k: np.zeros(n) for k in ("norm", "mean", "dispersion", "m2", "energy")}
+        robs = np.zeros((n, max(self.R.shape[0], 1)), np.complex128)
+        adr = np.zeros((n, d)) if want_adr else None
+        lib().orc_observables(C.byref(self.p), C.byref(self.s), int(is_start), _dp(self.mean_start),
+                              _dp(out["norm"]), _dp(out["mean"]), _dp(out["dispersion"]), _dp(out["m2"]),
+                              _dp(out["energy"]), _dp(robs), _dp(adr))
+        out["random_obs"] = robs[:, : self.R.shape[0]]
+        if want_adr:
+            out["adr"] = adr
+        return out
+
+    def jumps(self, tr):
+        k = int(self.n_rec[tr])
+        return (self.jump_times[tr, :k].copy(), self.diss_types[tr, :k].copy(),
+                self.jump_norms[tr, :k].copy(), self.jump_etas[tr, :k].copy())

@@ -1,0 +1,725 @@
+/*
+ * qjx_oracle.c -- CPU restatement of the QJX QJ path (TEST INFRASTRUCTURE, see header).
+ * Build: gcc -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -shared -fPIC (oracle/build_oracle.py).
+ * -ffp-contract=off is part of the arithmetic contract: only the explicit fma() calls fuse.
+ */
+#include "qjx_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ operators */
+
+int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
+                        double *H, double *Hd, double *L, double *K0, double *K1)
+{
+    if (N < 1) return 1;
+    const int d = N + 1;
+    const size_t dd = (size_t)d * d;
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(Hd, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 2 * dd * sizeof(double));
+
+    /* newdel.cpp:458-460: U is divided by (sys_size - 1) */
+    const double Us = U / (double)(d - 1);
+    for (int st = 0; st < d; st++) {
+        size_t idx = (size_t)st * d + st;
+        /* newdel.cpp:484-485 */
+        H[2 * idx] = 2.0 * Us * (double)(st * (st - 1) + (d - (st + 1)) * (d - (st + 1) - 1));
+        Hd[2 * idx] = (double)((d - (st + 1)) - st);
+    }
+    for (int st = 0; st < d - 1; st++) {
+        size_t dl = (size_t)(st + 1) * d + st, ur = (size_t)st * d + (st + 1);
+        /* newdel.cpp:493-494 */
+        H[2 * dl] -= J * sqrt((double)((d - (st + 1)) * (st + 1)));
+        H[2 * ur] -= J * sqrt((double)((st + 1) * (d - (st + 1))));
+    }
+    /* dissipator (newdel.cpp:1484-1497) */
+    for (int st = 0; st < d; st++) {
+        size_t idx = (size_t)st * d + st;
+        L[2 * idx] = (double)(st - (d - (st + 1)));
+    }
+    for (int st = 0; st < d - 1; st++) {
+        size_t dl = (size_t)(st + 1) * d + st, ur = (size_t)st * d + (st + 1);
+        L[2 * dl] -= sqrt((double)((d - (st + 1)) * (st + 1)));
+        L[2 * ur] += sqrt((double)((st + 1) * (d - (st + 1))));
+    }
+
+    /* newdel.cpp:2293-2294: gamma = g / (sys_size - 1) */
+    const double gamma = g / (double)(d - 1);
+    /* diss_part = gamma * L^H L (zgemm ConjTrans/NoTrans, newdel.cpp:2327-2342) */
+    double *dp = (double *)malloc(2 * dd * sizeof(double));
+    if (!dp) return 2;
+    for (int i = 0; i < d; i++) {
+        for (int j = 0; j < d; j++) {
+            double sr = 0.0, si = 0.0;
+            for (int k = 0; k < d; k++) {
+                const double ar = L[2 * ((size_t)k * d + i)], ai = L[2 * ((size_t)k * d + i) + 1];
+                const double br = L[2 * ((size_t)k * d + j)], bi = L[2 * ((size_t)k * d + j) + 1];
+                sr = sr + (ar * br + ai * bi);
+                si = si + (ar * bi - ai * br);
+            }
+            dp[2 * ((size_t)i * d + j)] = gamma * sr;
+            dp[2 * ((size_t)i * d + j) + 1] = gamma * si;
+        }
+    }
+    const double E0 = E + A, E1 = E - A; /* newdel.cpp:2369-2370 */
+    for (size_t idx = 0; idx < dd; idx++) {
+        /* hamitlonian_part = H - (i/2) diss_part  (newdel.cpp:2344-2352) */
+        double hr = H[2 * idx] + 0.5 * dp[2 * idx + 1];
+        double hi = 0.0 - 0.5 * dp[2 * idx];
+        /* K_b = -i (hp + E_b Hd)  (newdel.cpp:2378-2382) */
+        K0[2 * idx] = 0.0 + (hi + E0 * 0.0);
+        K0[2 * idx + 1] = 0.0 - (hr + E0 * Hd[2 * idx]);
+        K1[2 * idx] = 0.0 + (hi + E1 * 0.0);
+        K1[2 * idx + 1] = 0.0 - (hr + E1 * Hd[2 * idx]);
+    }
+    free(dp);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ expm */
+
+static void cmatmul(int n, const double *A, const double *B, double *C)
+{
+    /* C = A * B, complex row-major; i-k-j loop order */
+    memset(C, 0, 2 * (size_t)n * n * sizeof(double));
+    for (int i = 0; i < n; i++) {
+        double *c = C + 2 * (size_t)i * n;
+        for (int k = 0; k < n; k++) {
+            const double ar = A[2 * ((size_t)i * n + k)], ai = A[2 * ((size_t)i * n + k) + 1];
+            if (ar == 0.0 && ai == 0.0) continue;
+            const double *b = B + 2 * (size_t)k * n;
+            for (int j = 0; j < n; j++) {
+                const double br = b[2 * j], bi = b[2 * j + 1];
+                c[2 * j] += ar * br - ai * bi;
+                c[2 * j + 1] += ar * bi + ai * br;
+            }
+        }
+    }
+}
+
+/* out = sum_i c[i] * M_i + c0 * I   (M_i complex n x n, c real) */
+static void lincomb(int n, int cnt, const double *c, const double *const *M, double c0, double *out)
+{
+    const size_t nn = (size_t)n * n;
+    for (size_t e = 0; e < 2 * nn; e++) {
+        double s = 0.0;
+        for (int i = 0; i < cnt; i++) s += c[i] * M[i][e];
+        out[e] = s;
+    }
+    for (int i = 0; i < n; i++) out[2 * ((size_t)i * n + i)] += c0;
+}
+
+/* Solve P X = Q (complex n x n) by Gaussian elimination with partial pivoting; Q is
+ * overwritten with X, P is destroyed. */
+static int csolve(int n, double *P, double *Q)
+{
+    for (int c = 0; c < n; c++) {
+        int piv = c;
+        double best = -1.0;
+        for (int r = c; r < n; r++) {
+            double v = hypot(P[2 * ((size_t)r * n + c)], P[2 * ((size_t)r * n + c) + 1]);
+            if (v > best) { best = v; piv = r; }
+        }
+        if (best == 0.0) return 1;
+        if (piv != c) {
+            for (int j = 0; j < n; j++) {
+                for (int q = 0; q < 2; q++) {
+                    double t = P[2 * ((size_t)c * n + j) + q];
+                    P[2 * ((size_t)c * n + j) + q] = P[2 * ((size_t)piv * n + j) + q];
+                    P[2 * ((size_t)piv * n + j) + q] = t;
+                    t = Q[2 * ((size_t)c * n + j) + q];
+                    Q[2 * ((size_t)c * n + j) + q] = Q[2 * ((size_t)piv * n + j) + q];
+                    Q[2 * ((size_t)piv * n + j) + q] = t;
+                }
+            }
+        }
+        const double pr = P[2 * ((size_t)c * n + c)], pi = P[2 * ((size_t)c * n + c) + 1];
+        const double den = pr * pr + pi * pi;
+        const double ir = pr / den, ii = -pi / den; /* 1 / pivot */
+        for (int r = c + 1; r < n; r++) {
+            const double ar = P[2 * ((size_t)r * n + c)], ai = P[2 * ((size_t)r * n + c) + 1];
+            if (ar == 0.0 && ai == 0.0) continue;
+            const double fr = ar * ir - ai * ii, fi = ar * ii + ai * ir;
+            for (int j = c; j < n; j++) {
+                const double br = P[2 * ((size_t)c * n + j)], bi = P[2 * ((size_t)c * n + j) + 1];
+                P[2 * ((size_t)r * n + j)] -= fr * br - fi * bi;
+                P[2 * ((size_t)r * n + j) + 1] -= fr * bi + fi * br;
+            }
+            for (int j = 0; j < n; j++) {
+                const double br = Q[2 * ((size_t)c * n + j)], bi = Q[2 * ((size_t)c * n + j) + 1];
+                Q[2 * ((size_t)r * n + j)] -= fr * br - fi * bi;
+                Q[2 * ((size_t)r * n + j) + 1] -= fr * bi + fi * br;
+            }
+        }
+    }
+    for (int c = n - 1; c >= 0; c--) {
+        const double pr = P[2 * ((size_t)c * n + c)], pi = P[2 * ((size_t)c * n + c) + 1];
+        const double den = pr * pr + pi * pi;
+        const double ir = pr / den, ii = -pi / den;
+        for (int j = 0; j < n; j++) {
+            double sr = Q[2 * ((size_t)c * n + j)], si = Q[2 * ((size_t)c * n + j) + 1];
+            for (int k = c + 1; k < n; k++) {
+                const double ar = P[2 * ((size_t)c * n + k)], ai = P[2 * ((size_t)c * n + k) + 1];
+                const double xr = Q[2 * ((size_t)k * n + j)], xi = Q[2 * ((size_t)k * n + j) + 1];
+                sr -= ar * xr - ai * xi;
+                si -= ar * xi + ai * xr;
+            }
+            Q[2 * ((size_t)c * n + j)] = sr * ir - si * ii;
+            Q[2 * ((size_t)c * n + j) + 1] = sr * ii + si * ir;
+        }
+    }
+    return 0;
+}
+
+/* Pade coefficients b_0..b_m (Higham 2005, "The scaling and squaring method for the
+ * matrix exponential revisited", SIAM J. Matrix Anal. Appl. 26(4)). */
+static const double PADE3[] = {120.0, 60.0, 12.0, 1.0};
+static const double PADE5[] = {30240.0, 15120.0, 3360.0, 420.0, 30.0, 1.0};
+static const double PADE7[] = {17297280.0, 8648640.0, 1995840.0, 277200.0, 25200.0, 1512.0, 56.0, 1.0};
+static const double PADE9[] = {17643225600.0, 8821612800.0, 2075673600.0, 302702400.0, 30270240.0,
+                               2162160.0, 110880.0, 3960.0, 90.0, 1.0};
+static const double PADE13[] = {64764752532480000.0, 32382376266240000.0, 7771770303897600.0,
+                                1187353796428800.0, 129060195264000.0, 10559470521600.0,
+                                670442572800.0, 33522128640.0, 1323241920.0, 40840800.0,
+                                960960.0, 16380.0, 182.0, 1.0};
+/* theta_m thresholds on ||A||_1 (Higham 2005, Table 2.3) */
+static const double THETA[] = {1.495585217958292e-2, 2.539398330063230e-1, 9.504178996162932e-1,
+                               2.097847961257068e0, 5.371920351148152e0};
+
+int orc_expm(int n, const double *Ain, double *out)
+{
+    const size_t nn = (size_t)n * n, bytes = 2 * nn * sizeof(double);
+    double *A = (double *)malloc(bytes), *A2 = (double *)malloc(bytes), *A4 = (double *)malloc(bytes);
+    double *A6 = (double *)malloc(bytes), *W = (double *)malloc(bytes), *Uo = (double *)malloc(bytes);
+    double *V = (double *)malloc(bytes), *T = (double *)malloc(bytes);
+    if (!A || !A2 || !A4 || !A6 || !W || !Uo || !V || !T) return 2;
+    memcpy(A, Ain, bytes);
+
+    double l1 = 0.0;
+    for (int j = 0; j < n; j++) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++) s += hypot(A[2 * ((size_t)i * n + j)], A[2 * ((size_t)i * n + j) + 1]);
+        if (s > l1) l1 = s;
+    }
+    int m, s = 0;
+    if (l1 <= THETA[0]) m = 3;
+    else if (l1 <= THETA[1]) m = 5;
+    else if (l1 <= THETA[2]) m = 7;
+    else if (l1 <= THETA[3]) m = 9;
+    else {
+        m = 13;
+        s = (int)ceil(log2(l1 / THETA[4]));
+        if (s < 0) s = 0;
+        const double sc = ldexp(1.0, -s);
+        for (size_t e = 0; e < 2 * nn; e++) A[e] *= sc;
+    }
+
+    cmatmul(n, A, A, A2);
+    if (m == 3) {
+        const double *M1[] = {A2};
+        double c1[] = {PADE3[3]};
+        lincomb(n, 1, c1, M1, PADE3[1], W);
+        cmatmul(n, A, W, Uo);
+        double c2[] = {PADE3[2]};
+        lincomb(n, 1, c2, M1, PADE3[0], V);
+    } else if (m == 5) {
+        cmatmul(n, A2, A2, A4);
+        const double *M1[] = {A4, A2};
+        double cu[] = {PADE5[5], PADE5[3]}, cv[] = {PADE5[4], PADE5[2]};
+        lincomb(n, 2, cu, M1, PADE5[1], W);
+        cmatmul(n, A, W, Uo);
+        lincomb(n, 2, cv, M1, PADE5[0], V);
+    } else if (m == 7) {
+        cmatmul(n, A2, A2, A4);
+        cmatmul(n, A4, A2, A6);
+        const double *M1[] = {A6, A4, A2};
+        double cu[] = {PADE7[7], PADE7[5], PADE7[3]}, cv[] = {PADE7[6], PADE7[4], PADE7[2]};
+        lincomb(n, 3, cu, M1, PADE7[1], W);
+        cmatmul(n, A, W, Uo);
+        lincomb(n, 3, cv, M1, PADE7[0], V);
+    } else if (m == 9) {
+        cmatmul(n, A2, A2, A4);
+        cmatmul(n, A4, A2, A6);
+        cmatmul(n, A6, A2, T); /* A8 */
+        const double *M1[] = {T, A6, A4, A2};
+        double cu[] = {PADE9[9], PADE9[7], PADE9[5], PADE9[3]};
+        double cv[] = {PADE9[8], PADE9[6], PADE9[4], PADE9[2]};
+        lincomb(n, 4, cu, M1, PADE9[1], W);
+        cmatmul(n, A, W, Uo);
+        lincomb(n, 4, cv, M1, PADE9[0], V);
+    } else {
+        cmatmul(n, A2, A2, A4);
+        cmatmul(n, A4, A2, A6);
+        const double *M3[] = {A6, A4, A2};
+        /* U = A [A6 (b13 A6 + b11 A4 + b9 A2) + b7 A6 + b5 A4 + b3 A2 + b1 I] */
+        double c_hi_u[] = {PADE13[13], PADE13[11], PADE13[9]};
+        lincomb(n, 3, c_hi_u, M3, 0.0, T);
+        cmatmul(n, A6, T, W);
+        double c_lo_u[] = {PADE13[7], PADE13[5], PADE13[3]};
+        lincomb(n, 3, c_lo_u, M3, PADE13[1], T);
+        for (size_t e = 0; e < 2 * nn; e++) T[e] += W[e];
+        cmatmul(n, A, T, Uo);
+        /* V = A6 (b12 A6 + b10 A4 + b8 A2) + b6 A6 + b4 A4 + b2 A2 + b0 I */
+        double c_hi_v[] = {PADE13[12], PADE13[10], PADE13[8]};
+        lincomb(n, 3, c_hi_v, M3, 0.0, T);
+        cmatmul(n, A6, T, W);
+        double c_lo_v[] = {PADE13[6], PADE13[4], PADE13[2]};
+        lincomb(n, 3, c_lo_v, M3, PADE13[0], V);
+        for (size_t e = 0; e < 2 * nn; e++) V[e] += W[e];
+    }
+    /* (V - U) X = (V + U) */
+    for (size_t e = 0; e < 2 * nn; e++) {
+        const double u = Uo[e], v = V[e];
+        T[e] = v - u;
+        out[e] = v + u;
+    }
+    int rc = csolve(n, T, out);
+    for (int k = 0; k < s && rc == 0; k++) {
+        cmatmul(n, out, out, W);
+        memcpy(out, W, bytes);
+    }
+    free(A); free(A2); free(A4); free(A6); free(W); free(Uo); free(V); free(T);
+    return rc;
+}
+
+int orc_split_tree(int d, const double *K, double T, int deep, double *U_out)
+{
+    if (deep < 1) return 1;
+    const size_t dd = (size_t)d * d;
+    double *dts = (double *)malloc(sizeof(double) * deep);
+    double dt = T * 0.5; /* qj_proc.cpp:15-16 */
+    for (int l = 0; l < deep; l++) { dt *= 0.5; dts[l] = dt; }
+    int rc = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : rc)
+    for (int l = 0; l < deep; l++) {
+        double *scaled = (double *)malloc(2 * dd * sizeof(double));
+        for (size_t e = 0; e < dd; e++) {
+            scaled[2 * e] = K[2 * e] * dts[l];
+            scaled[2 * e + 1] = K[2 * e + 1] * dts[l];
+        }
+        rc |= orc_expm(d, scaled, U_out + 2 * dd * (size_t)l);
+        free(scaled);
+    }
+    free(dts);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ Philox */
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+double orc_philox_uniform(uint64_t seed, uint64_t tr, uint64_t idx)
+{
+    const uint64_t blk = idx >> 1;
+    const uint32_t ctr[4] = {(uint32_t)blk, (uint32_t)(blk >> 32), (uint32_t)tr, (uint32_t)(tr >> 32)};
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    orc_philox4x32_10(ctr, key, o);
+    const uint32_t a = (idx & 1) ? o[2] : o[0];
+    const uint32_t b = (idx & 1) ? o[3] : o[1];
+    const uint64_t m = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
+    return (double)(m + 1) * 0x1p-53;
+}
+
+/* ------------------------------------------------------------------ canonical kernels */
+
+void orc_matvec(int d, const double *M, const double *x, double *out)
+{
+    for (int i = 0; i < d; i++) {
+        const double *row = M + 2 * (size_t)i * d;
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < d; k++) {
+            const double mr = row[2 * k], mi = row[2 * k + 1];
+            const double xr = x[2 * k], xi = x[2 * k + 1];
+            re = fma(mr, xr, re);
+            re = fma(-mi, xi, re);
+            im = fma(mr, xi, im);
+            im = fma(mi, xr, im);
+        }
+        out[2 * i] = re;
+        out[2 * i + 1] = im;
+    }
+}
+
+/* Same arithmetic as orc_matvec on a transposed planar copy (MTr/MTi are [k][ld],
+ * ld = d rounded up to ORC_RB); rows are processed ORC_RB at a time so the compiler
+ * vectorises across rows.  Each output keeps its own k-ascending fma chain, so the
+ * result is bit-identical to orc_matvec (fnmadd(a,b,c) == fma(-a,b,c) exactly). */
+#define ORC_RB 8
+#if defined(__AVX2__) && defined(__FMA__)
+#include <immintrin.h>
+static void matvec_t(int d, int ld, const double *MTr, const double *MTi, const double *x, double *out)
+{
+    for (int i0 = 0; i0 < d; i0 += ORC_RB) {
+        __m256d re0 = _mm256_setzero_pd(), re1 = _mm256_setzero_pd();
+        __m256d im0 = _mm256_setzero_pd(), im1 = _mm256_setzero_pd();
+        for (int k = 0; k < d; k++) {
+            const __m256d xr = _mm256_set1_pd(x[2 * k]), xi = _mm256_set1_pd(x[2 * k + 1]);
+            const double *cr = MTr + (size_t)k * ld + i0, *ci = MTi + (size_t)k * ld + i0;
+            const __m256d r0 = _mm256_loadu_pd(cr), r1 = _mm256_loadu_pd(cr + 4);
+            const __m256d q0 = _mm256_loadu_pd(ci), q1 = _mm256_loadu_pd(ci + 4);
+            re0 = _mm256_fmadd_pd(r0, xr, re0);  re1 = _mm256_fmadd_pd(r1, xr, re1);
+            re0 = _mm256_fnmadd_pd(q0, xi, re0); re1 = _mm256_fnmadd_pd(q1, xi, re1);
+            im0 = _mm256_fmadd_pd(r0, xi, im0);  im1 = _mm256_fmadd_pd(r1, xi, im1);
+            im0 = _mm256_fmadd_pd(q0, xr, im0);  im1 = _mm256_fmadd_pd(q1, xr, im1);
+        }
+        double re[ORC_RB], im[ORC_RB];
+        _mm256_storeu_pd(re, re0); _mm256_storeu_pd(re + 4, re1);
+        _mm256_storeu_pd(im, im0); _mm256_storeu_pd(im + 4, im1);
+        for (int r = 0; r < ORC_RB && i0 + r < d; r++) {
+            out[2 * (i0 + r)] = re[r];
+            out[2 * (i0 + r) + 1] = im[r];
+        }
+    }
+}
+#else
+static void matvec_t(int d, int ld, const double *MTr, const double *MTi, const double *x, double *out)
+{
+    for (int i0 = 0; i0 < d; i0 += ORC_RB) {
+        double re[ORC_RB] = {0}, im[ORC_RB] = {0};
+        for (int k = 0; k < d; k++) {
+            const double xr = x[2 * k], xi = x[2 * k + 1];
+            const double *cr = MTr + (size_t)k * ld + i0, *ci = MTi + (size_t)k * ld + i0;
+            for (int r = 0; r < ORC_RB; r++) {
+                re[r] = fma(cr[r], xr, re[r]);
+                re[r] = fma(-ci[r], xi, re[r]);
+                im[r] = fma(cr[r], xi, im[r]);
+                im[r] = fma(ci[r], xr, im[r]);
+            }
+        }
+        for (int r = 0; r < ORC_RB && i0 + r < d; r++) {
+            out[2 * (i0 + r)] = re[r];
+            out[2 * (i0 + r) + 1] = im[r];
+        }
+    }
+}
+#endif
+
+typedef struct { int ld; double *r, *i; } tmat;
+
+static int tmat_make(int d, int count, const double *M, tmat *out)
+{
+    const int ld = (d + ORC_RB - 1) / ORC_RB * ORC_RB;
+    const size_t per = (size_t)d * ld;
+    out->ld = ld;
+    out->r = (double *)calloc(per * (count > 0 ? count : 1), sizeof(double));
+    out->i = (double *)calloc(per * (count > 0 ? count : 1), sizeof(double));
+    if (!out->r || !out->i) return 1;
+    for (int c = 0; c < count; c++)
+        for (int i = 0; i < d; i++)
+            for (int k = 0; k < d; k++) {
+                const size_t src = (size_t)c * d * d + (size_t)i * d + k;
+                out->r[per * c + (size_t)k * ld + i] = M[2 * src];
+                out->i[per * c + (size_t)k * ld + i] = M[2 * src + 1];
+            }
+    return 0;
+}
+
+static void tmat_free(tmat *t) { free(t->r); free(t->i); }
+
+double orc_norm_square(int d, const double *x)
+{
+    double n = 0.0;
+    for (int i = 0; i < d; i++) {
+        const double a = x[2 * i] * x[2 * i];
+        const double b = x[2 * i + 1] * x[2 * i + 1];
+        n = n + (a + b);
+    }
+    return n;
+}
+
+/* ------------------------------------------------------------------ QJ engine */
+
+typedef struct {
+    const orc_problem *p;
+    orc_state *s;
+    int tr;
+    int is_obs;
+    double *phi, *aux, *res, *gn;
+    const tmat *tU, *tL;
+    double dt[64];
+    int err;
+} traj_ctx;
+
+static double draw(traj_ctx *c)
+{
+    const orc_problem *p = c->p;
+    int64_t *pos = &c->s->rng_pos[c->tr];
+    if (p->rng_kind == 0) return orc_philox_uniform(p->seed, (uint64_t)c->tr, (uint64_t)(*pos)++);
+    const int64_t lo = p->inj_off[c->tr], hi = p->inj_off[c->tr + 1];
+    if (lo + *pos >= hi) { c->err = 3; return 0.5; }
+    return p->inj_u[lo + (*pos)++];
+}
+
+/* recovery (experiment.cpp:1273-1382) on aux */
+static void recovery(traj_ctx *c)
+{
+    const orc_problem *p = c->p;
+    const int d = p->d, k = p->num_diss;
+    double *phi = c->aux;
+    double norm = sqrt(orc_norm_square(d, phi));
+    for (int st = 0; st < d; st++) {
+        phi[2 * st] /= norm;
+        phi[2 * st + 1] /= norm;
+    }
+    double tmp = 0.0, ran = draw(c);
+    for (int i = 0; i < k; i++) {
+        matvec_t(d, c->tL->ld, c->tL->r + (size_t)d * c->tL->ld * i, c->tL->i + (size_t)d * c->tL->ld * i, phi, c->res);
+        c->s->matvecs[c->tr]++;
+        c->gn[i] = orc_norm_square(d, c->res);
+        c->gn[i] *= p->g[i];
+        tmp += c->gn[i];
+    }
+    ran *= tmp;
+    /* Same walk as experiment.cpp:1326-1334, with the index held below k - 1 before the
+     * test (the reference's loop reads gnorms[1] when k == 1 and ran > gnorms[0], which
+     * its own uniforms in [0,1) cannot produce; injected uniforms above 1 could). */
+    int index = 0;
+    while (index < k - 1 && ran - c->gn[index] > 0.0) {
+        ran -= c->gn[index];
+        index++;
+    }
+    if (tmp == 0.0) { c->err = 2; return; } /* reference would loop forever / read out of range */
+    for (int it = 0; c->gn[index] == 0; it++) {
+        if (it > 2 * k) { c->err = 2; return; }
+        if (index == 0) index++;
+        else index--;
+        if (index >= k) { c->err = 2; return; }
+    }
+    matvec_t(d, c->tL->ld, c->tL->r + (size_t)d * c->tL->ld * index, c->tL->i + (size_t)d * c->tL->ld * index, phi, c->res);
+    c->s->matvecs[c->tr]++;
+    for (int st = 0; st < d; st++) {
+        phi[2 * st] = c->res[2 * st] / sqrt(c->gn[index] / p->g[index]);
+        phi[2 * st + 1] = c->res[2 * st + 1] / sqrt(c->gn[index] / p->g[index]);
+    }
+    if (p->record > 0 && c->is_obs == 1) {
+        orc_state *s = c->s;
+        int r = s->n_rec[c->tr] - 1; /* the record pushed just before this recovery */
+        if (r >= 0 && r < s->rec_cap) s->diss_types[(size_t)c->tr * s->rec_cap + r] = index;
+    }
+}
+
+/* one_period_branch (qj_proc.cpp:271-343), recursion over split levels */
+static void one_period_branch(traj_ctx *c, int b, int level)
+{
+    const orc_problem *p = c->p;
+    orc_state *s = c->s;
+    const int d = p->d;
+    const size_t dd = (size_t)d * d;
+    const size_t moff = (size_t)d * c->tU->ld * ((size_t)b * p->deep + level);
+    const double *Ur = c->tU->r + moff, *Ui = c->tU->i + moff;
+    (void)dd;
+    double *t = &s->t[c->tr];
+    double *eta = &s->eta[c->tr];
+    const double dt = c->dt[level];
+
+    if (level == p->deep - 1) {
+        for (int counter = 0; counter != 2; counter++) {
+            matvec_t(d, c->tU->ld, Ur, Ui, c->phi, c->aux);
+            s->matvecs[c->tr]++;
+            const double nrm = orc_norm_square(d, c->aux);
+            if (nrm > 1.0) { c->err = 1; return; }
+            if (!(nrm > *eta)) {
+                if (p->record > 0 && c->is_obs == 1) {
+                    const int r = s->n_rec[c->tr];
+                    if (r >= s->rec_cap) { c->err = 4; return; }
+                    const size_t o = (size_t)c->tr * s->rec_cap + r;
+                    s->jump_times[o] = *t + dt;
+                    s->jump_norms[o] = orc_norm_square(d, c->aux);
+                    s->jump_etas[o] = *eta;
+                    s->diss_types[o] = -1;
+                    s->n_rec[c->tr] = r + 1;
+                    s->jumps_counts[c->tr]++;
+                }
+                recovery(c);
+                if (c->err) return;
+                *eta = draw(c);
+                while (*eta == 0.0) *eta = draw(c);
+                if (c->err) return;
+            }
+            memcpy(c->phi, c->aux, 2 * (size_t)d * sizeof(double));
+            *t += dt;
+        }
+    } else {
+        for (int counter = 0; counter != 2; counter++) {
+            matvec_t(d, c->tU->ld, Ur, Ui, c->phi, c->aux);
+            s->matvecs[c->tr]++;
+            const double nrm = orc_norm_square(d, c->aux);
+            if (nrm > 1.0) { c->err = 1; return; }
+            if (!(nrm > *eta)) {
+                one_period_branch(c, b, level + 1);
+                if (c->err) return;
+                *t -= dt;
+            } else {
+                memcpy(c->phi, c->aux, 2 * (size_t)d * sizeof(double));
+            }
+            *t += dt;
+        }
+    }
+}
+
+int orc_init(const orc_problem *p, orc_state *s, int start_type, int start_state)
+{
+    const int d = p->d;
+    for (int tr = 0; tr < p->n_traj; tr++) {
+        double *phi = s->phi + 2 * (size_t)tr * d;
+        memset(phi, 0, 2 * (size_t)d * sizeof(double));
+        if (start_type == 0) phi[2 * start_state] = 1.0;
+        else for (int i = 0; i < d; i++) phi[2 * i] = sqrt(1.0 / (double)d);
+        s->t[tr] = 0.0;
+        s->rng_pos[tr] = 0;
+        s->jumps_counts[tr] = 0;
+        s->matvecs[tr] = 0;
+        s->n_rec[tr] = 0;
+        s->error[tr] = 0;
+        traj_ctx c = {0};
+        c.p = p; c.s = s; c.tr = tr;
+        s->eta[tr] = 0.0;
+        while (s->eta[tr] == 0.0 && c.err == 0) s->eta[tr] = draw(&c);
+        s->error[tr] = c.err;
+    }
+    return 0;
+}
+
+int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_periods, int is_obs, int n_threads)
+{
+    if (p->deep < 1 || p->deep > 60) return 1;
+    int bad = 0;
+    tmat tU, tL;
+    if (tmat_make(p->d, p->num_branches * p->deep, p->U, &tU) || tmat_make(p->d, p->num_diss, p->L, &tL)) return 2;
+#ifdef _OPENMP
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads) reduction(+ : bad)
+#endif
+    for (int tr = tr0; tr < tr1; tr++) {
+        if (s->error[tr]) { bad++; continue; }
+        const int d = p->d;
+        traj_ctx c = {0};
+        c.p = p; c.s = s; c.tr = tr; c.is_obs = is_obs;
+        c.tU = &tU; c.tL = &tL;
+        c.phi = s->phi + 2 * (size_t)tr * d;
+        c.aux = (double *)calloc(2 * (size_t)d, sizeof(double));
+        c.res = (double *)calloc(2 * (size_t)d, sizeof(double));
+        c.gn = (double *)calloc((size_t)p->num_diss + 1, sizeof(double));
+        double dt = p->T * 0.5;
+        for (int l = 0; l < p->deep; l++) { dt *= 0.5; c.dt[l] = dt; }
+        for (int per = 0; per < n_periods && !c.err; per++)
+            for (int b = 0; b < p->num_branches && !c.err; b++) one_period_branch(&c, b, 0);
+        s->error[tr] = c.err;
+        if (c.err) bad++;
+        free(c.aux); free(c.res); free(c.gn);
+    }
+    (void)n_threads;
+    tmat_free(&tU);
+    tmat_free(&tL);
+    return bad;
+}
+
+int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
+                    double *mean_start, double *norm_o, double *mean_o, double *disp_o,
+                    double *m2_o, double *energy_o, double *robs, double *adr_o)
+{
+    const int d = p->d;
+    tmat tH, tR;
+    if (tmat_make(d, 1, p->HE, &tH) || tmat_make(d, p->num_robs, p->R, &tR)) return 2;
+    const size_t per = (size_t)d * tH.ld;
+#pragma omp parallel for schedule(static)
+    for (int tr = 0; tr < p->n_traj; tr++) {
+        const double *phi = s->phi + 2 * (size_t)tr * d;
+        double *adr = (double *)malloc(sizeof(double) * d);
+        double *xh = (double *)malloc(2 * sizeof(double) * d);
+        double *sm = (double *)malloc(2 * sizeof(double) * d);
+        const double norm = orc_norm_square(d, phi);
+        for (int st = 0; st < d; st++) {
+            /* mult_scalar_double(mult_scalar_complex(phi, phi, 1), 1/norm).real */
+            const double a = phi[2 * st] * phi[2 * st], b = phi[2 * st + 1] * phi[2 * st + 1];
+            adr[st] = (0.0 + (a + b)) * (1.0 / norm);
+        }
+        double mean = 0.0;
+        for (int st = 0; st < d; st++) mean = mean + (double)st * adr[st];
+        const double ms = is_start ? mean : mean_start[tr];
+        const double disp = (mean - ms) * (mean - ms);
+        double m2 = 0.0;
+        for (int st = 0; st < d; st++) m2 = m2 + ((double)st - mean) * ((double)st - mean) * adr[st];
+        /* normalised state and energy <psi|H + E0 Hd|psi> (experiment.cpp:1423-1469) */
+        const double sq = sqrt(norm);
+        for (int st = 0; st < d; st++) {
+            xh[2 * st] = phi[2 * st] / sq;
+            xh[2 * st + 1] = phi[2 * st + 1] / sq;
+        }
+        matvec_t(d, tH.ld, tH.r, tH.i, xh, sm);
+        double energy = 0.0;
+        for (int st = 0; st < d; st++) {
+            const double a = xh[2 * st] * sm[2 * st], b = xh[2 * st + 1] * sm[2 * st + 1];
+            energy = energy + (a + b);
+        }
+        /* random observables <psi|R|psi> (experiment.cpp:2023-2078) */
+        for (int o = 0; o < p->num_robs; o++) {
+            matvec_t(d, tR.ld, tR.r + per * o, tR.i + per * o, xh, sm);
+            double rr = 0.0, ri = 0.0;
+            for (int st = 0; st < d; st++) {
+                const double cr = xh[2 * st], ci = -xh[2 * st + 1];
+                const double tr_ = cr * sm[2 * st] - ci * sm[2 * st + 1];
+                const double ti_ = ci * sm[2 * st] + cr * sm[2 * st + 1];
+                rr = rr + tr_;
+                ri = ri + ti_;
+            }
+            robs[2 * ((size_t)tr * p->num_robs + o)] = rr;
+            robs[2 * ((size_t)tr * p->num_robs + o) + 1] = ri;
+        }
+        if (is_start) mean_start[tr] = mean;
+        norm_o[tr] = norm;
+        mean_o[tr] = mean;
+        disp_o[tr] = disp;
+        m2_o[tr] = m2;
+        energy_o[tr] = energy;
+        if (adr_o) memcpy(adr_o + (size_t)tr * d, adr, sizeof(double) * d);
+        free(adr); free(xh); free(sm);
+    }
+    tmat_free(&tH);
+    tmat_free(&tR);
+    return 0;
+}
+
+int orc_dump_periods(int dump_type, int dump_num, int num_obs_periods, int *periods)
+{
+    if (dump_type == 0) {
+        periods[0] = 0;
+        const int shift = num_obs_periods / dump_num;
+        for (int i = 0; i < dump_num; i++) periods[i + 1] = (i + 1) * shift;
+        return dump_num + 1;
+    } else if (dump_type == 1) {
+        periods[0] = 0;
+        const double begin_decade = log10(1.0);
+        const double end_decade = log10((double)num_obs_periods);
+        const double num_decades = end_decade - begin_decade;
+        const double num_decades_dump = (double)dump_num / num_decades;
+        for (int i = 0; i < dump_num + 1; i++) {
+            const int cur = (int)(pow(10.0, begin_decade) * pow(10.0, (1.0 / num_decades_dump) * (double)i));
+            periods[i + 1] = cur > periods[i] ? cur : periods[i] + 1;
+        }
+        return dump_num + 2;
+    }
+    return -1;
+}

@@ -1,0 +1,127 @@
+/*
+ * qjx_oracle.h -- CPU restatement of the QJX quantum-jump path (TEST INFRASTRUCTURE).
+ *
+ * This library is the checker for the CUDA engine in os_d_b200.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.  The product
+ * never links or calls it.
+ *
+ * It restates, in plain C, the reference's algorithm for sys_id 0 (Bose dimer),
+ * task_id 1 (Std), prop_id 0 (QJ):
+ *   operators          source/cpp/QJX/QJX/newdel.cpp:3-37, 450-498, 1454-1498, 2285-2388
+ *   split tree / expm  source/cpp/QJX/QJX/qj_proc.cpp:4-120, core.cpp:9880-9926
+ *   period bisection   source/cpp/QJX/QJX/qj_proc.cpp:264-343, core.cpp:84-95
+ *   norm test / jump   source/cpp/QJX/QJX/experiment.cpp:1239-1382
+ *   observables        source/cpp/QJX/QJX/core.cpp:665-725, experiment.cpp:1395-1469, 2023-2078
+ *   Std task flow      source/cpp/QJX/QJX/experiment.cpp:411-542, 3249-3271
+ *   dump schedule      source/cpp/QJX/QJX/newdel_exp.cpp:408-455
+ *
+ * Parity status: the reference needs Intel MKL and Eigen, neither of which exists in
+ * this image, and it ships no golden data, so this restatement is "parity unpinned"
+ * against the reference binary.  It is pinned instead to independent known-answer
+ * tests (closed-form operators, scipy expm, Philox KAT vectors, dense Lindblad).
+ *
+ * Arithmetic contract (shared bit-for-bit with the CUDA engine):
+ *   complex matvec out_i = sum_k M_ik x_k, k ascending from 0, per k:
+ *       re = fma(Mr, xr, re); re = fma(-Mi, xi, re); im = fma(Mr, xi, im); im = fma(Mi, xr, im)
+ *   norm_square  n = n + (re*re + im*im), i ascending, no contraction
+ *   every other expression is evaluated literally (compiled with -ffp-contract=off).
+ *
+ * Complex arrays are interleaved (re, im) doubles, matrices row-major d x d, like
+ * MKL_Complex16 in the reference.
+ */
+#ifndef QJX_ORACLE_H
+#define QJX_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Dimer operators (newdel.cpp).  Outputs are complex d x d, d = N + 1:
+ *   H   : hamiltonian            (newdel.cpp:450-498)
+ *   Hd  : hamiltonian_drv        (newdel.cpp:485)
+ *   L   : dissipators[0]         (newdel.cpp:1454-1498)
+ *   K0,K1: hamiltonians_qj[0/1] = -i (H - i/2 gamma L^H L + E_b Hd), gamma = g/N,
+ *          E_0 = E + A, E_1 = E - A  (newdel.cpp:2285-2388) */
+int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
+                        double *H, double *Hd, double *L, double *K0, double *K1);
+
+/* Matrix exponential exp(A), complex n x n, Higham (2005) scaling and squaring with
+ * Pade [m/m], m in {3,5,7,9,13}.  Replaces Eigen MatrixXcd::exp() (qj_proc.cpp:55,98). */
+int orc_expm(int n, const double *A, double *out);
+
+/* Split tree of one branch: U_l = exp(K * dt_l), dt_l = T * 2^-(l+2), l = 0..deep-1,
+ * dt computed by repeated halving like init_split_branches (qj_proc.cpp:15-24). */
+int orc_split_tree(int d, const double *K, double T, int deep, double *U_out);
+
+/* Philox4x32-10 (Salmon et al., SC'11).  ctr[4], key[2] -> out[4]. */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* Uniform in (0,1]: draw number `idx` of trajectory `tr` under `seed`. */
+double orc_philox_uniform(uint64_t seed, uint64_t tr, uint64_t idx);
+
+/* One ensemble problem for the QJ engine. */
+typedef struct {
+    int d;              /* sys_size = N + 1 */
+    int n_traj;
+    int deep;           /* ex_deep */
+    int num_branches;   /* num_ham_qj (2 for the dimer) */
+    int num_diss;       /* 1 for the dimer */
+    int num_robs;       /* random observables */
+    int record;         /* params "jump": 0 none, 1 times+types, 2 also norms+etas */
+    int rng_kind;       /* 0 = Philox(seed, tr, idx); 1 = injected per-trajectory uniforms */
+    double T;           /* period */
+    uint64_t seed;
+    const double *U;    /* [num_branches][deep][d][d] complex */
+    const double *L;    /* [num_diss][d][d] complex */
+    const double *g;    /* [num_diss] rates (1.0 for the dimer) */
+    const double *HE;   /* [d][d] complex: H + E0 * Hd (energy observable) */
+    const double *R;    /* [num_robs][d][d] complex random observables */
+    const double *inj_u;      /* rng_kind 1: concatenated uniforms */
+    const int64_t *inj_off;   /* rng_kind 1: [n_traj + 1] offsets into inj_u */
+} orc_problem;
+
+/* Mutable per-run state and outputs. */
+typedef struct {
+    double *phi;        /* [n_traj][d] complex, current states (in/out) */
+    double *eta;        /* [n_traj] */
+    double *t;          /* [n_traj] times_all */
+    int64_t *rng_pos;   /* [n_traj] next draw index */
+    int *jumps_counts;  /* [n_traj] */
+    int64_t *matvecs;   /* [n_traj] complex matvecs executed (work counter) */
+    /* jump records, capacity cap per trajectory; n_rec[tr] = records written */
+    int rec_cap;
+    int *n_rec;
+    double *jump_times; /* [n_traj][rec_cap] */
+    double *jump_norms;
+    double *jump_etas;
+    int *diss_types;
+    int *error;         /* [n_traj] 0 ok; 1 norm>1; 2 all jump weights zero; 3 rng exhausted; 4 record overflow */
+} orc_state;
+
+/* Initial state: start_type 0 -> |start_state>, else uniform sqrt(1/d) (newdel_exp.cpp:656-679);
+ * draw eta_0 (experiment.cpp:3260-3265).  Sets t = 0, counts = 0. */
+int orc_init(const orc_problem *p, orc_state *s, int start_type, int start_state);
+
+/* Advance trajectories [tr0, tr1) by n_periods periods; is_obs gates jump recording
+ * exactly like ed->is_obs (qj_proc.cpp:296).  OpenMP over trajectories. */
+int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_periods, int is_obs, int n_threads);
+
+/* Observables of every trajectory (calc_chars_std[_start], core.cpp:665-725).
+ * mean_start is written when is_start != 0 and read otherwise.  adr may be NULL. */
+int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
+                    double *mean_start, double *norm, double *mean, double *dispersion,
+                    double *m2, double *energy, double *robs /* [n_traj][num_robs] complex */,
+                    double *adr /* [n_traj][d] */);
+
+/* Dump schedule (newdel_exp.cpp:408-455).  Returns dump_num_total, fills periods
+ * (caller provides dump_num + 2 ints). */
+int orc_dump_periods(int dump_type, int dump_num, int num_obs_periods, int *periods);
+
+/* Canonical kernels, exported for unit tests. */
+void orc_matvec(int d, const double *M, const double *x, double *out);
+double orc_norm_square(int d, const double *x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

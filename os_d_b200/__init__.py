@@ -1,0 +1,7 @@
+"""os_d_b200: B200-native quantum-jump trajectory engine (drop-in for os_d's QJX QJ path).
+
+The compute path is the native library libqjx_b200.so (sm_100a kernels behind a C ABI,
+include/qjx_b200.h).  Importing this package never falls back to CPU code.
+"""
+from ._native import QjxError, build_dimer, expm, lib  # noqa: F401
+from .engine import Engine, FBasis  # noqa: F401

@@ -1,0 +1,119 @@
+"""ctypes binding of libqjx_b200.so (the C ABI in include/qjx_b200.h).
+
+The library is the product: there is no Python or CPU fallback.  If the shared object
+is missing or lacks a symbol, loading fails with an error.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqjx_b200.so")
+
+c_double_p = C.POINTER(C.c_double)
+c_int_p = C.POINTER(C.c_int)
+c_i64_p = C.POINTER(C.c_int64)
+
+# every entry point declared in include/qjx_b200.h
+EXPORTS = [
+    "qjx_create", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
+    "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
+    "qjx_get_mean_start", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
+    "qjx_build_dimer", "qjx_expm", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
+]
+
+
+class QjxConfig(C.Structure):
+    _fields_ = [("d", C.c_int), ("n_traj", C.c_int), ("deep", C.c_int), ("num_branches", C.c_int),
+                ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
+                ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
+                ("max_dumps", C.c_int), ("device", C.c_int)]
+
+
+class QjxStats(C.Structure):
+    _fields_ = [("micro_steps", C.c_int64), ("matvecs", C.c_int64), ("jumps", C.c_int64),
+                ("kernel_ms", C.c_double), ("last_call_ms", C.c_double)]
+
+
+_lib = None
+
+
+class QjxError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QjxError(f"native library missing: {LIB_PATH} (run os_d_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        for name in EXPORTS:
+            if not hasattr(L, name):
+                raise QjxError(f"native library lacks {name}")
+        vp = C.c_void_p
+        L.qjx_create.argtypes = [C.POINTER(QjxConfig)] + [c_double_p] * 5 + [C.POINTER(vp)]
+        L.qjx_destroy.argtypes = [vp]
+        L.qjx_destroy.restype = None
+        L.qjx_last_error.argtypes = [vp]
+        L.qjx_last_error.restype = C.c_char_p
+        L.qjx_status_string.argtypes = [C.c_int]
+        L.qjx_status_string.restype = C.c_char_p
+        L.qjx_set_states.argtypes = [vp, c_double_p]
+        L.qjx_set_uniforms.argtypes = [vp, c_double_p, c_i64_p]
+        L.qjx_init_thresholds.argtypes = [vp]
+        L.qjx_run_periods.argtypes = [vp, C.c_int, C.c_int, c_int_p, C.c_int, C.c_int]
+        L.qjx_reset_times.argtypes = [vp]
+        L.qjx_observe.argtypes = [vp, C.c_int, C.c_int]
+        L.qjx_get_observables.argtypes = [vp, C.c_int, C.c_int] + [c_double_p] * 7
+        L.qjx_get_mean_start.argtypes = [vp, c_double_p]
+        L.qjx_get_states.argtypes = [vp, c_double_p, c_double_p, c_double_p, c_int_p]
+        L.qjx_jump_count.argtypes = [vp, C.c_int, c_i64_p]
+        L.qjx_get_jumps.argtypes = [vp, C.c_int, c_double_p, c_int_p, c_double_p, c_double_p]
+        L.qjx_get_stats.argtypes = [vp, C.POINTER(QjxStats)]
+        L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 4
+        L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_fb_create.argtypes = ([C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_int_p, c_double_p,
+                                     c_double_p, c_double_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                                     C.c_double, C.c_int, C.c_int, C.POINTER(vp)])
+        L.qjx_fb_run.argtypes = [vp, C.c_int, C.c_int]
+        L.qjx_fb_get.argtypes = [vp, c_double_p, c_double_p]
+        L.qjx_fb_destroy.argtypes = [vp]
+        L.qjx_fb_destroy.restype = None
+        _lib = L
+    return _lib
+
+
+def dp(a):
+    return None if a is None else a.ctypes.data_as(c_double_p)
+
+
+def ip(a):
+    return None if a is None else a.ctypes.data_as(c_int_p)
+
+
+def check(status, handle=None, what=""):
+    if status != 0:
+        msg = lib().qjx_status_string(status).decode()
+        if handle:
+            msg += ": " + lib().qjx_last_error(handle).decode()
+        raise QjxError(f"{what} failed ({status}): {msg}")
+
+
+def build_dimer(N, J, U, E, A, g, omega, deep):
+    """Dimer operators and split propagators built by the library (host FP64)."""
+    d = N + 1
+    H = np.zeros((d, d), np.complex128)
+    Hd = np.zeros_like(H)
+    Lm = np.zeros_like(H)
+    Ut = np.zeros((2, deep, d, d), np.complex128)
+    check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(Lm), dp(Ut)), what="qjx_build_dimer")
+    return H, Hd, Lm, Ut
+
+
+def expm(A):
+    A = np.ascontiguousarray(A, np.complex128)
+    out = np.empty_like(A)
+    check(lib().qjx_expm(A.shape[0], dp(A), dp(out)), what="qjx_expm")
+    return out

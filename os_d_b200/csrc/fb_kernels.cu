@@ -1,0 +1,217 @@
+// fb_kernels.cu -- f-basis Lindblad RK4 on the GPU (density-matrix oracle of the QJ ensemble).
+//
+// The reference integrates dx/dt = Gs x + E(t) Qs_drv x - Ks with classic RK4
+// (source/cpp/CQdiss_os_dimer/CQdiss/calcODE.cpp:75-118 calcVectValue_real, :249-389
+// calcODE_trans/std), two mkl_dcsrgemv per stage.  Here one kernel per RK stage computes
+// both CSR row products, the stage vector k = (Gs x + drv Qs x - Ks) h and the next stage
+// argument (or the RK4 update) in one pass; the steps of a period are captured once as a
+// CUDA graph and replayed.
+//
+// Canonical row sum (shared bit-for-bit with the CPU oracle): lane l of a warp accumulates
+// the row's nonzeros l, l+32, l+64, ... in CSR order with fma, then the 32 partial sums are
+// combined by an xor butterfly (offsets 16, 8, 4, 2, 1).  All other arithmetic is literal
+// (-fmad=false).  The drive uses sin() of the stage time (CUDA libdevice), so drv_type 1
+// matches the CPU within rounding, not bit-for-bit.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/qjx_b200.h"
+
+namespace fb {
+
+struct FbParams {
+    int n;
+    const int *gr, *gc;
+    const double *gv;
+    const int *qr, *qc;
+    const double *qv;
+    const double *Ks;
+    double drv_ampl;  // -A (calcODE.cpp:91)
+    double drv_freq, drv_phase;
+    int drv_type;
+    double *x, *val, *k1, *k2, *k3;
+};
+
+__device__ __forceinline__ double warp_row_sum(const int *rp, const int *ci, const double *v, const double *x, int row,
+                                               int lane)
+{
+    double s = 0.0;
+    const int b = rp[row], e = rp[row + 1];
+    for (int j = b + lane; j < e; j += 32) s = __fma_rn(v[j], x[ci[j]], s);
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, off));
+    return s;
+}
+
+// stage 1..4 of one RK4 step at time t (calcODE.cpp:278-302)
+__global__ void rk_stage(const FbParams P, int stage, double t, double h)
+{
+    const int warps = blockDim.x >> 5;
+    const int row = blockIdx.x * warps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= P.n) return;
+    const double *arg = (stage == 1) ? P.x : P.val;
+    const double tt = (stage == 1) ? t : ((stage == 4) ? __dadd_rn(t, h) : __dadd_rn(t, __ddiv_rn(h, 2.0)));
+    const double t1 = warp_row_sum(P.gr, P.gc, P.gv, arg, row, lane);
+    const double t2 = warp_row_sum(P.qr, P.qc, P.qv, arg, row, lane);
+    if (lane != 0) return;
+    double drv;
+    const double sn = sin(__dadd_rn(__dmul_rn(P.drv_freq, tt), P.drv_phase));
+    if (P.drv_type == 1) drv = __dmul_rn(P.drv_ampl, sn);
+    else drv = __dmul_rn(P.drv_ampl, (sn < 0.0) ? -1.0 : 1.0);
+    const double k = __dmul_rn(__dsub_rn(__dadd_rn(t1, __dmul_rn(drv, t2)), P.Ks[row]), h);
+    const double x = P.x[row];
+    if (stage == 1) {
+        P.k1[row] = k;
+        P.val[row] = __dadd_rn(x, __ddiv_rn(k, 2.0));
+    } else if (stage == 2) {
+        P.k2[row] = k;
+        P.val[row] = __dadd_rn(x, __ddiv_rn(k, 2.0));
+    } else if (stage == 3) {
+        P.k3[row] = k;
+        P.val[row] = __dadd_rn(x, k);
+    }
+    // stage 4 is finished by rk_update once every row has read val
+    if (stage == 4) P.k3[row] = __dadd_rn(__dadd_rn(__dadd_rn(P.k1[row], __dmul_rn(2.0, P.k2[row])),
+                                                     __dmul_rn(2.0, P.k3[row])), k);
+}
+
+// x += (k1 + 2 k2 + 2 k3 + k4) / 6  (calcODE.cpp:299-302); the sum was left in k3.
+__global__ void rk_update(const FbParams P)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.n) P.x[i] = __dadd_rn(P.x[i], __ddiv_rn(P.k3[i], 6.0));
+}
+
+}  // namespace fb
+
+struct qjx_fb {
+    fb::FbParams P{};
+    int device = 0;
+    double T = 0.0;
+    int num_steps = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<void *> allocs;
+    double last_ms = 0.0;
+};
+
+static void *fb_alloc(qjx_fb *h, size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+    h->allocs.push_back(p);
+    return p;
+}
+
+extern "C" qjx_status qjx_fb_create(int n, const int *gs_rowptr, const int *gs_col, const double *gs_val,
+                                    const int *qs_rowptr, const int *qs_col, const double *qs_val, const double *Ks,
+                                    const double *x0, double drv_ampl, double drv_freq, double drv_phase, int drv_type,
+                                    double T, int num_steps, int device, qjx_fb **out)
+{
+    if (n < 1 || !gs_rowptr || !gs_col || !gs_val || !qs_rowptr || !qs_col || !qs_val || !Ks || !x0 || !out ||
+        num_steps < 1 || !(T > 0.0) || (drv_type != 0 && drv_type != 1))
+        return QJX_ERR_INVALID_ARG;
+    *out = nullptr;
+    qjx_fb *h = new (std::nothrow) qjx_fb();
+    if (!h) return QJX_ERR_OOM;
+    h->device = device;
+    h->T = T;
+    h->num_steps = num_steps;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete h;
+        return QJX_ERR_CUDA;
+    }
+    cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    cudaEventCreate(&h->e0);
+    cudaEventCreate(&h->e1);
+    const int gnz = gs_rowptr[n], qnz = qs_rowptr[n];
+    fb::FbParams &P = h->P;
+    P.n = n;
+    int *gr = (int *)fb_alloc(h, sizeof(int) * (n + 1)), *gc = (int *)fb_alloc(h, sizeof(int) * gnz);
+    int *qr = (int *)fb_alloc(h, sizeof(int) * (n + 1)), *qc = (int *)fb_alloc(h, sizeof(int) * qnz);
+    double *gv = (double *)fb_alloc(h, sizeof(double) * gnz), *qv = (double *)fb_alloc(h, sizeof(double) * qnz);
+    double *ks = (double *)fb_alloc(h, sizeof(double) * n);
+    P.x = (double *)fb_alloc(h, sizeof(double) * n);
+    P.val = (double *)fb_alloc(h, sizeof(double) * n);
+    P.k1 = (double *)fb_alloc(h, sizeof(double) * n);
+    P.k2 = (double *)fb_alloc(h, sizeof(double) * n);
+    P.k3 = (double *)fb_alloc(h, sizeof(double) * n);
+    if (!gr || !gc || !qr || !qc || !gv || !qv || !ks || !P.x || !P.val || !P.k1 || !P.k2 || !P.k3) {
+        qjx_fb_destroy(h);
+        return QJX_ERR_OOM;
+    }
+    cudaMemcpy(gr, gs_rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice);
+    cudaMemcpy(gc, gs_col, sizeof(int) * gnz, cudaMemcpyHostToDevice);
+    cudaMemcpy(gv, gs_val, sizeof(double) * gnz, cudaMemcpyHostToDevice);
+    cudaMemcpy(qr, qs_rowptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice);
+    cudaMemcpy(qc, qs_col, sizeof(int) * qnz, cudaMemcpyHostToDevice);
+    cudaMemcpy(qv, qs_val, sizeof(double) * qnz, cudaMemcpyHostToDevice);
+    cudaMemcpy(ks, Ks, sizeof(double) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(P.x, x0, sizeof(double) * n, cudaMemcpyHostToDevice);
+    P.gr = gr;
+    P.gc = gc;
+    P.gv = gv;
+    P.qr = qr;
+    P.qc = qc;
+    P.qv = qv;
+    P.Ks = ks;
+    P.drv_ampl = -drv_ampl;
+    P.drv_freq = drv_freq;
+    P.drv_phase = drv_phase;
+    P.drv_type = drv_type;
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        qjx_fb_destroy(h);
+        return QJX_ERR_CUDA;
+    }
+    *out = h;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods)
+{
+    if (!h || period0 < 0 || n_periods < 0) return QJX_ERR_INVALID_ARG;
+    if (cudaSetDevice(h->device) != cudaSuccess) return QJX_ERR_CUDA;
+    const fb::FbParams &P = h->P;
+    const double step = h->T / double(h->num_steps);  // data.cpp:10
+    const int warps = 8, rblocks = (P.n + warps - 1) / warps, ublocks = (P.n + 255) / 256;
+    cudaEventRecord(h->e0, h->stream);
+    for (int p = period0; p < period0 + n_periods; p++) {
+        for (int s = 0; s < h->num_steps; s++) {
+            const double t = double(p) * h->T + double(s) * step;  // calcODE.cpp:280
+            for (int stage = 1; stage <= 4; stage++) fb::rk_stage<<<rblocks, warps * 32, 0, h->stream>>>(P, stage, t, step);
+            fb::rk_update<<<ublocks, 256, 0, h->stream>>>(P);
+        }
+    }
+    cudaEventRecord(h->e1, h->stream);
+    if (cudaEventSynchronize(h->e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return QJX_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->e0, h->e1);
+    h->last_ms = ms;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_fb_get(qjx_fb *h, double *x, double *last_period_ms)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (cudaSetDevice(h->device) != cudaSuccess) return QJX_ERR_CUDA;
+    if (x && cudaMemcpy(x, h->P.x, sizeof(double) * h->P.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return QJX_ERR_CUDA;
+    if (last_period_ms) *last_period_ms = h->last_ms;
+    return QJX_OK;
+}
+
+extern "C" void qjx_fb_destroy(qjx_fb *h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->e0) cudaEventDestroy(h->e0);
+    if (h->e1) cudaEventDestroy(h->e1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}

@@ -1,0 +1,191 @@
+// qjx_device.cuh -- device-side building blocks of the QJ trajectory engine (sm_100a).
+//
+// Arithmetic contract (bit-identical to the CPU oracle):
+//   * complex matvec: per output, k ascending from 0, per k
+//       re = fma(Mr, xr, re); re = fma(-Mi, xi, re); im = fma(Mr, xi, im); im = fma(Mi, xr, im)
+//   * norm_square: n = n + (re*re + im*im), rows ascending, no contraction
+//   * everything else literal; this translation unit is compiled with -fmad=false and the
+//     intended fused operations are written as __fma_rn.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qjx {
+
+// ---- launch geometry of the micro-step kernel ----
+constexpr int kThreads = 256;          // 8 warps
+constexpr int kTY = 32;                // row threads: rows ty + 32 i, i < MT
+constexpr int kTX = 8;                 // column threads: columns tx + 8 j, j < kNT
+constexpr int kNT = 4;                 // columns per thread
+constexpr int kNC = kTX * kNT;         // 32 trajectory columns per tile
+constexpr int kKB = 8;                 // k rows per propagator slab
+constexpr int kStages = 3;             // slab pipeline depth
+constexpr int kMaxGroups = 256;        // distinct matrices in one engine
+constexpr int kMaxMT = 8;              // d <= 256
+
+// ---- trajectory phases ----
+enum Phase : int {
+    PH_STEP = 0,    // split step U[b][lvl] psi
+    PH_REC_W = 1,   // jump-channel weight ||L_sub psi_hat||^2 g_sub
+    PH_REC_A = 2,   // apply chosen channel L_sub psi_hat / sqrt(w/g)
+    PH_OBS_E = 3,   // energy <psi_hat| H + E0 Hd |psi_hat>
+    PH_OBS_R = 4,   // random observable sub
+    PH_DONE = 5,
+    PH_ERROR = 6
+};
+
+enum ErrCode : int { ERR_NONE = 0, ERR_NORM = 1, ERR_ZERO_W = 2, ERR_RNG = 3, ERR_TIMEOUT = 6 };
+
+// Per-trajectory state (one 96-byte record per trajectory).
+struct __align__(16) TrajState {
+    double t;          // times_all
+    double eta;        // etas_all
+    double ran;        // channel-choice uniform drawn at the jump (recovery's first draw)
+    double tmpw;       // running sum of channel weights
+    long long rng_pos; // next draw index
+    unsigned long long mask;  // bit l = step counter of split level l (0 or 1)
+    int lvl, b, phase, cur;   // level, branch, phase, slot holding psi
+    int sub, pc, di, jumps;   // channel / observable index, periods done, next dump, jumps_counts
+    int nrec, err, paused, pad;
+};
+static_assert(sizeof(TrajState) == 96, "TrajState layout");
+
+struct Params {
+    int d, MD, n, deep, nb, nd, nr, G;
+    int gL0, gHE, gR0;
+    const double2 *mats;     // [G][d][MD]  transposed matrices: mats[g][k][row]
+    double2 *psi;            // [2][n][MD]
+    TrajState *st;           // [n]
+    double *gn;              // [n][nd] channel weights
+    const double *g;         // [nd]
+    const double *dt;        // [deep]
+    int *cnt;                // [3][G]
+    int *lists;              // [2][G][n]
+    // rng
+    int rng_kind;
+    unsigned long long seed;
+    const double *inj_u;
+    const long long *inj_off;
+    // run
+    int record;
+    int target;
+    const int *dump_at;
+    int n_dumps;
+    int dump_base;
+    // observables
+    int keep_adr;
+    double *o_norm, *o_mean, *o_disp, *o_m2, *o_energy;  // [max_dumps][n]
+    double2 *o_robs;                                        // [max_dumps][n][nr]
+    double *o_adr;                                          // keep_adr ? [max_dumps][n][d] : [n][d]
+    double *mean_start;                                     // [n]
+    // jump records, record-major [rec_cap][n]
+    int rec_cap;
+    double *r_time, *r_norm, *r_eta;
+    int *r_type;
+    // control: [0] error count, [1] first error trajectory, [2] paused count, [3] first error code,
+    //          [4] timeouts
+    int *ctrl;
+    long long *work;         // [0] trajectory-matvecs executed
+};
+
+// ---------------------------------------------------------------- Philox4x32-10
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+        const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Uniform in (0,1]: draw `idx` of trajectory `tr` (identical to the host definition).
+__device__ __forceinline__ double philox_uniform(unsigned long long seed, unsigned long long tr,
+                                                 unsigned long long idx)
+{
+    const unsigned long long blk = idx >> 1;
+    uint32_t c[4] = {(uint32_t)blk, (uint32_t)(blk >> 32), (uint32_t)tr, (uint32_t)(tr >> 32)};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint32_t a = (idx & 1) ? c[2] : c[0];
+    const uint32_t b = (idx & 1) ? c[3] : c[1];
+    const unsigned long long m = ((unsigned long long)(a >> 5) << 26) | (unsigned long long)(b >> 6);
+    return __dmul_rn((double)(m + 1), 0x1p-53);
+}
+
+// Next uniform of a trajectory; sets *err on an exhausted injected sequence.
+__device__ __forceinline__ double draw(const Params &P, int tr, TrajState &s, int *err)
+{
+    if (P.rng_kind == 0) return philox_uniform(P.seed, (unsigned long long)tr, (unsigned long long)(s.rng_pos++));
+    const long long lo = P.inj_off[tr], hi = P.inj_off[tr + 1];
+    if (lo + s.rng_pos >= hi) { *err = ERR_RNG; return 0.5; }
+    return P.inj_u[lo + (s.rng_pos++)];
+}
+
+// ---------------------------------------------------------------- canonical reductions
+__device__ __forceinline__ double seq_norm(const double2 *x, int d)
+{
+    double n = 0.0;
+    for (int i = 0; i < d; i++) {
+        const double2 v = x[i];
+        n = __dadd_rn(n, __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y)));
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------- TMA bulk copies + mbarriers
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after `limit` polls and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit)
+{
+    for (long long i = 0; i < limit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// 1-D TMA bulk copy global -> shared, completion counted in bytes on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+}  // namespace qjx

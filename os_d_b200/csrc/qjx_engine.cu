@@ -1,0 +1,563 @@
+// qjx_engine.cu -- host side of the QJ trajectory engine: device memory, the micro-step
+// loop (CUDA graphs of 6 micro-steps, bounded host polling), jump-record draining, and the
+// C ABI declared in include/qjx_b200.h.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/qjx_b200.h"
+#include "qjx_device.cuh"
+
+namespace qjx {
+cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st);
+size_t step_smem_bytes(int MD);
+cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st);
+cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st);
+cudaError_t launch_init_state(const Params &P, cudaStream_t st);
+cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
+cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
+cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
+}  // namespace qjx
+
+using namespace qjx;
+
+struct qjx_engine {
+    qjx_config cfg{};
+    Params P{};
+    int MD = 0;
+    int grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    // device allocations
+    std::vector<void *> allocs;
+    double *d_inj_u = nullptr;
+    long long *d_inj_off = nullptr;
+    int *d_dump_at = nullptr;
+    int dump_cap = 0;
+    // host mirrors
+    int *h_cnt = nullptr;   // pinned [G]
+    int *h_ctrl = nullptr;  // pinned [8]
+    std::vector<std::vector<double>> jt, jn, je;
+    std::vector<std::vector<int>> jtype;
+    qjx_stats stats{};
+    bool states_set = false;
+};
+
+static void *dalloc(qjx_engine *h, size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, bytes ? bytes : 16);
+    h->allocs.push_back(p);
+    return p;
+}
+
+static qjx_status fail(qjx_engine *h, qjx_status s, const std::string &msg)
+{
+    if (h) h->err = msg;
+    return s;
+}
+
+static qjx_status cuda_fail(qjx_engine *h, cudaError_t e, const char *where)
+{
+    return fail(h, QJX_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+extern "C" const char *qjx_status_string(qjx_status s)
+{
+    switch (s) {
+    case QJX_OK: return "ok";
+    case QJX_ERR_INVALID_ARG: return "invalid argument";
+    case QJX_ERR_OOM: return "out of device memory";
+    case QJX_ERR_NORM_GT_ONE: return "norm more than 1";
+    case QJX_ERR_RNG_EXHAUSTED: return "injected uniform sequence exhausted";
+    case QJX_ERR_ZERO_JUMP_WEIGHTS: return "all jump channels have zero weight";
+    case QJX_ERR_TIMEOUT: return "bounded device wait gave up";
+    case QJX_ERR_CUDA: return "CUDA error";
+    case QJX_ERR_UNSUPPORTED: return "unsupported configuration";
+    case QJX_ERR_STATE: return "call out of order";
+    }
+    return "unknown";
+}
+
+extern "C" const char *qjx_last_error(const qjx_engine *h) { return h ? h->err.c_str() : "null handle"; }
+
+// Transposes row-major complex d x d matrices into the device layout mats[g][k][row]
+// (row padded to MD with zeros), so one K-slab is one contiguous TMA bulk copy.
+static void pack_transposed(const double *M, int d, int MD, double *out)
+{
+    for (int i = 0; i < d; i++)
+        for (int k = 0; k < d; k++) {
+            out[2 * ((size_t)k * MD + i)] = M[2 * ((size_t)i * d + k)];
+            out[2 * ((size_t)k * MD + i) + 1] = M[2 * ((size_t)i * d + k) + 1];
+        }
+}
+
+extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, const double *g,
+                                 const double *HE, const double *R, qjx_engine **out)
+{
+    if (!cfg || !out || !U || !L || !g || !HE) return QJX_ERR_INVALID_ARG;
+    *out = nullptr;
+    const qjx_config &c = *cfg;
+    if (c.d < 2 || c.n_traj < 1 || c.deep < 1 || c.deep > 62 || c.num_branches < 1 || c.num_diss < 1 ||
+        c.num_robs < 0 || !(c.T > 0.0) || (c.num_robs > 0 && !R))
+        return QJX_ERR_INVALID_ARG;
+    const int G = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;
+    if (c.d > 32 * kMaxMT || G > kMaxGroups) return QJX_ERR_UNSUPPORTED;
+
+    qjx_engine *h = new (std::nothrow) qjx_engine();
+    if (!h) return QJX_ERR_OOM;
+    h->cfg = c;
+    if (h->cfg.rec_cap <= 0) h->cfg.rec_cap = 1024;
+    if (h->cfg.max_dumps <= 0) h->cfg.max_dumps = 1;
+    auto bail = [&](qjx_status s) {
+        qjx_destroy(h);
+        return s;
+    };
+    if (cudaSetDevice(c.device) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    h->grid = sms > 0 ? sms : 148;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+
+    const int d = c.d, n = c.n_traj;
+    const int MD = 32 * ((d + 31) / 32);
+    h->MD = MD;
+    Params &P = h->P;
+    P.d = d;
+    P.MD = MD;
+    P.n = n;
+    P.deep = c.deep;
+    P.nb = c.num_branches;
+    P.nd = c.num_diss;
+    P.nr = c.num_robs;
+    P.G = G;
+    P.gL0 = c.num_branches * c.deep;
+    P.gHE = P.gL0 + c.num_diss;
+    P.gR0 = P.gHE + 1;
+    P.rng_kind = c.rng_kind;
+    P.seed = c.seed;
+    P.keep_adr = c.keep_adr;
+    P.rec_cap = h->cfg.rec_cap;
+
+    // matrices in the transposed padded layout
+    const size_t per = (size_t)d * MD * 2;
+    std::vector<double> host((size_t)G * per, 0.0);
+    const size_t dd2 = (size_t)d * d * 2;
+    for (int b = 0; b < c.num_branches; b++)
+        for (int l = 0; l < c.deep; l++)
+            pack_transposed(U + dd2 * ((size_t)b * c.deep + l), d, MD, host.data() + per * (b * c.deep + l));
+    for (int i = 0; i < c.num_diss; i++) pack_transposed(L + dd2 * i, d, MD, host.data() + per * (P.gL0 + i));
+    pack_transposed(HE, d, MD, host.data() + per * P.gHE);
+    for (int i = 0; i < c.num_robs; i++) pack_transposed(R + dd2 * i, d, MD, host.data() + per * (P.gR0 + i));
+    double2 *mats = (double2 *)dalloc(h, host.size() * sizeof(double));
+    if (!mats) return bail(QJX_ERR_OOM);
+    cudaMemcpy(mats, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
+    P.mats = mats;
+
+    // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24)
+    std::vector<double> dts(c.deep);
+    double dt = c.T * 0.5;
+    for (int l = 0; l < c.deep; l++) {
+        dt *= 0.5;
+        dts[l] = dt;
+    }
+    double *d_dt = (double *)dalloc(h, sizeof(double) * c.deep);
+    double *d_g = (double *)dalloc(h, sizeof(double) * c.num_diss);
+    if (!d_dt || !d_g) return bail(QJX_ERR_OOM);
+    cudaMemcpy(d_dt, dts.data(), sizeof(double) * c.deep, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_g, g, sizeof(double) * c.num_diss, cudaMemcpyHostToDevice);
+    P.dt = d_dt;
+    P.g = d_g;
+
+    P.psi = (double2 *)dalloc(h, (size_t)2 * n * MD * sizeof(double2));
+    P.st = (TrajState *)dalloc(h, (size_t)n * sizeof(TrajState));
+    P.gn = (double *)dalloc(h, (size_t)n * c.num_diss * sizeof(double));
+    P.cnt = (int *)dalloc(h, (size_t)3 * G * sizeof(int));
+    P.lists = (int *)dalloc(h, (size_t)2 * G * n * sizeof(int));
+    const size_t nd_ = (size_t)h->cfg.max_dumps * n;
+    P.o_norm = (double *)dalloc(h, nd_ * sizeof(double));
+    P.o_mean = (double *)dalloc(h, nd_ * sizeof(double));
+    P.o_disp = (double *)dalloc(h, nd_ * sizeof(double));
+    P.o_m2 = (double *)dalloc(h, nd_ * sizeof(double));
+    P.o_energy = (double *)dalloc(h, nd_ * sizeof(double));
+    P.o_robs = (double2 *)dalloc(h, nd_ * std::max(1, c.num_robs) * sizeof(double2));
+    P.o_adr = (double *)dalloc(h, (c.keep_adr ? nd_ : (size_t)n) * d * sizeof(double));
+    P.mean_start = (double *)dalloc(h, (size_t)n * sizeof(double));
+    const size_t rc = (size_t)P.rec_cap * n;
+    P.r_time = (double *)dalloc(h, rc * sizeof(double));
+    P.r_norm = (double *)dalloc(h, rc * sizeof(double));
+    P.r_eta = (double *)dalloc(h, rc * sizeof(double));
+    P.r_type = (int *)dalloc(h, rc * sizeof(int));
+    P.ctrl = (int *)dalloc(h, 16 * sizeof(int));
+    P.work = (long long *)dalloc(h, 2 * sizeof(long long));
+    if (!P.psi || !P.st || !P.gn || !P.cnt || !P.lists || !P.o_norm || !P.o_mean || !P.o_disp || !P.o_m2 ||
+        !P.o_energy || !P.o_robs || !P.o_adr || !P.mean_start || !P.r_time || !P.r_norm || !P.r_eta || !P.r_type ||
+        !P.ctrl || !P.work)
+        return bail(QJX_ERR_OOM);
+    if (cudaMallocHost(&h->h_cnt, sizeof(int) * G) != cudaSuccess ||
+        cudaMallocHost(&h->h_ctrl, sizeof(int) * 16) != cudaSuccess)
+        return bail(QJX_ERR_OOM);
+    h->jt.assign(n, {});
+    h->jn.assign(n, {});
+    h->je.assign(n, {});
+    h->jtype.assign(n, {});
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(QJX_ERR_CUDA);
+    if (launch_init_state(P, h->stream) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    *out = h;
+    return QJX_OK;
+}
+
+extern "C" void qjx_destroy(qjx_engine *h)
+{
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->d_inj_u) cudaFree(h->d_inj_u);
+    if (h->d_inj_off) cudaFree(h->d_inj_off);
+    if (h->d_dump_at) cudaFree(h->d_dump_at);
+    if (h->h_cnt) cudaFreeHost(h->h_cnt);
+    if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+extern "C" qjx_status qjx_set_states(qjx_engine *h, const double *psi)
+{
+    if (!h || !psi) return QJX_ERR_INVALID_ARG;
+    const Params &P = h->P;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaMemsetAsync(P.psi, 0, (size_t)2 * P.n * P.MD * sizeof(double2), h->stream));
+    CK(cudaMemcpy2DAsync(P.psi, (size_t)P.MD * sizeof(double2), psi, (size_t)P.d * sizeof(double2),
+                         (size_t)P.d * sizeof(double2), P.n, cudaMemcpyHostToDevice, h->stream));
+    CK(launch_init_state(P, h->stream));
+    CK(cudaMemsetAsync(P.ctrl, 0, 16 * sizeof(int), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < P.n; i++) {
+        h->jt[i].clear();
+        h->jn[i].clear();
+        h->je[i].clear();
+        h->jtype[i].clear();
+    }
+    h->states_set = true;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_set_uniforms(qjx_engine *h, const double *u, const int64_t *offsets)
+{
+    if (!h || !u || !offsets) return QJX_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    const int n = h->P.n;
+    const int64_t total = offsets[n];
+    if (offsets[0] != 0 || total < 0) return fail(h, QJX_ERR_INVALID_ARG, "offsets must start at 0");
+    for (int i = 0; i < n; i++)
+        if (offsets[i + 1] < offsets[i]) return fail(h, QJX_ERR_INVALID_ARG, "offsets must be non-decreasing");
+    if (h->d_inj_u) cudaFree(h->d_inj_u);
+    if (h->d_inj_off) cudaFree(h->d_inj_off);
+    h->d_inj_u = nullptr;
+    h->d_inj_off = nullptr;
+    CK(cudaMalloc(&h->d_inj_u, std::max<int64_t>(total, 1) * sizeof(double)));
+    CK(cudaMalloc(&h->d_inj_off, (size_t)(n + 1) * sizeof(long long)));
+    CK(cudaMemcpy(h->d_inj_u, u, total * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_inj_off, offsets, (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+    h->P.inj_u = h->d_inj_u;
+    h->P.inj_off = h->d_inj_off;
+    return QJX_OK;
+}
+
+static qjx_status check_ctrl(qjx_engine *h)
+{
+    const int *c = h->h_ctrl;
+    if (c[0] == 0) return QJX_OK;
+    char buf[160];
+    snprintf(buf, sizeof buf, "device error code %d on trajectory %d (%d errors)", c[3], c[1], c[0]);
+    h->err = buf;
+    switch (c[3]) {
+    case ERR_NORM: return QJX_ERR_NORM_GT_ONE;
+    case ERR_ZERO_W: return QJX_ERR_ZERO_JUMP_WEIGHTS;
+    case ERR_RNG: return QJX_ERR_RNG_EXHAUSTED;
+    case ERR_TIMEOUT: return QJX_ERR_TIMEOUT;
+    default: return QJX_ERR_CUDA;
+    }
+}
+
+extern "C" qjx_status qjx_init_thresholds(qjx_engine *h)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    if (h->P.rng_kind == 1 && !h->P.inj_u) return fail(h, QJX_ERR_STATE, "qjx_set_uniforms first");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(launch_thresholds(h->P, h->stream));
+    CK(cudaMemcpyAsync(h->h_ctrl, h->P.ctrl, 16 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return check_ctrl(h);
+}
+
+extern "C" qjx_status qjx_reset_times(qjx_engine *h)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(launch_reset_times(h->P, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return QJX_OK;
+}
+
+// Copies the device jump records into the per-trajectory host vectors and empties the
+// device buffers.
+static qjx_status drain_records(qjx_engine *h)
+{
+    const Params &P = h->P;
+    if (!P.record) return QJX_OK;
+    const int n = P.n;
+    std::vector<TrajState> st(n);
+    CK(cudaMemcpyAsync(st.data(), P.st, n * sizeof(TrajState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int maxrec = 0;
+    for (int i = 0; i < n; i++) maxrec = std::max(maxrec, st[i].nrec);
+    if (maxrec == 0) return QJX_OK;
+    const size_t cntv = (size_t)maxrec * n;
+    std::vector<double> t(cntv), nr(cntv), e(cntv);
+    std::vector<int> ty(cntv);
+    CK(cudaMemcpyAsync(t.data(), P.r_time, cntv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(nr.data(), P.r_norm, cntv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(e.data(), P.r_eta, cntv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(ty.data(), P.r_type, cntv * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < n; i++)
+        for (int r = 0; r < st[i].nrec; r++) {
+            const size_t o = (size_t)r * n + i;
+            h->jt[i].push_back(t[o]);
+            h->jn[i].push_back(nr[o]);
+            h->je[i].push_back(e[o]);
+            h->jtype[i].push_back(ty[o]);
+        }
+    CK(launch_clear_records(P, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->stats.jumps += (int64_t)0;
+    return QJX_OK;
+}
+
+// Runs lock-step micro-steps until every trajectory is done for this call.  Step 0 of the
+// call reads buckets written into cnt[0] / lists[0] by the schedule or observe kernel.
+static qjx_status run_until_idle(qjx_engine *h)
+{
+    Params &P = h->P;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < 6; s++) {
+        cudaError_t e = launch_step(P, s, h->grid, h->stream);
+        if (e != cudaSuccess) {
+            cudaStreamEndCapture(h->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            return cuda_fail(h, e, "launch_step");
+        }
+    }
+    CK(cudaStreamEndCapture(h->stream, &graph));
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return cuda_fail(h, ie, "cudaGraphInstantiate");
+
+    qjx_status rs = QJX_OK;
+    int batch = 1;
+    int64_t steps = 0;
+    long long work0 = 0;
+    cudaMemcpy(&work0, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
+    cudaEventRecord(h->ev0, h->stream);
+    while (true) {
+        for (int b = 0; b < batch; b++) {
+            cudaError_t e = cudaGraphLaunch(exec, h->stream);
+            if (e != cudaSuccess) {
+                rs = cuda_fail(h, e, "cudaGraphLaunch");
+                break;
+            }
+        }
+        if (rs != QJX_OK) break;
+        steps += 6 * batch;
+        cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
+        cudaMemcpyAsync(h->h_ctrl, P.ctrl, sizeof(int) * 16, cudaMemcpyDeviceToHost, h->stream);
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) {
+            rs = cuda_fail(h, e, "micro-step batch");
+            break;
+        }
+        rs = check_ctrl(h);
+        if (rs != QJX_OK) break;
+        long long active = 0;
+        for (int g = 0; g < P.G; g++) active += h->h_cnt[g];
+        if (active == 0) {
+            if (h->h_ctrl[2] > 0) {  // paused on full record buffers: drain and resume
+                rs = drain_records(h);
+                if (rs != QJX_OK) break;
+                cudaMemsetAsync(P.ctrl + 2, 0, sizeof(int), h->stream);
+                cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream);
+                cudaError_t le = launch_schedule(P, 1, h->stream);
+                if (le != cudaSuccess) {
+                    rs = cuda_fail(h, le, "launch_schedule");
+                    break;
+                }
+                continue;
+            }
+            break;
+        }
+        batch = std::min(batch * 2, 16);
+    }
+    cudaEventRecord(h->ev1, h->stream);
+    cudaEventSynchronize(h->ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.kernel_ms += ms;
+    h->stats.last_call_ms = ms;
+    h->stats.micro_steps += steps;
+    long long work1 = 0;
+    cudaMemcpy(&work1, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
+    h->stats.matvecs += work1 - work0;
+    cudaGraphExecDestroy(exec);
+    return rs;
+}
+
+extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, const int *dump_at, int n_dumps,
+                                      int dump_base)
+{
+    if (!h || n_periods < 0 || n_dumps < 0 || (n_dumps > 0 && !dump_at)) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    if (dump_base < 0 || dump_base + n_dumps > h->cfg.max_dumps)
+        return fail(h, QJX_ERR_INVALID_ARG, "dump slots exceed max_dumps");
+    for (int i = 0; i < n_dumps; i++)
+        if (dump_at[i] < 1 || dump_at[i] > n_periods || (i > 0 && dump_at[i] <= dump_at[i - 1]))
+            return fail(h, QJX_ERR_INVALID_ARG, "dump_at must be ascending within 1..n_periods");
+    if (n_periods == 0) return QJX_OK;
+    CK(cudaSetDevice(h->cfg.device));
+    Params &P = h->P;
+    if (n_dumps > h->dump_cap) {
+        if (h->d_dump_at) cudaFree(h->d_dump_at);
+        h->d_dump_at = nullptr;
+        CK(cudaMalloc(&h->d_dump_at, sizeof(int) * n_dumps));
+        h->dump_cap = n_dumps;
+    }
+    if (n_dumps) CK(cudaMemcpy(h->d_dump_at, dump_at, sizeof(int) * n_dumps, cudaMemcpyHostToDevice));
+    P.dump_at = h->d_dump_at;
+    P.n_dumps = n_dumps;
+    P.dump_base = dump_base;
+    P.target = n_periods;
+    P.record = (is_obs == 1 && h->cfg.record > 0) ? 1 : 0;
+    CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
+    CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
+    CK(launch_schedule(P, 0, h->stream));
+    qjx_status s = run_until_idle(h);
+    if (s != QJX_OK) return s;
+    return drain_records(h);
+}
+
+extern "C" qjx_status qjx_observe(qjx_engine *h, int dump, int is_start)
+{
+    if (!h || dump < 0 || dump >= h->cfg.max_dumps) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    CK(cudaSetDevice(h->cfg.device));
+    Params &P = h->P;
+    P.target = 0;
+    P.n_dumps = 1;
+    P.dump_base = dump;
+    P.record = 0;
+    CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
+    CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
+    CK(launch_observe(P, dump, is_start, h->stream));
+    return run_until_idle(h);
+}
+
+extern "C" qjx_status qjx_get_observables(qjx_engine *h, int dump0, int n_dumps, double *norm, double *mean,
+                                          double *dispersion, double *m2, double *energy, double *robs,
+                                          double *adr)
+{
+    if (!h || dump0 < 0 || n_dumps < 0 || dump0 + n_dumps > h->cfg.max_dumps) return QJX_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    const Params &P = h->P;
+    const size_t o = (size_t)dump0 * P.n, cnt = (size_t)n_dumps * P.n;
+    if (norm) CK(cudaMemcpy(norm, P.o_norm + o, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (mean) CK(cudaMemcpy(mean, P.o_mean + o, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (dispersion) CK(cudaMemcpy(dispersion, P.o_disp + o, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (m2) CK(cudaMemcpy(m2, P.o_m2 + o, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (energy) CK(cudaMemcpy(energy, P.o_energy + o, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (robs && P.nr > 0)
+        CK(cudaMemcpy(robs, P.o_robs + o * P.nr, cnt * P.nr * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (adr) {
+        if (P.keep_adr)
+            CK(cudaMemcpy(adr, P.o_adr + o * P.d, cnt * P.d * sizeof(double), cudaMemcpyDeviceToHost));
+        else
+            CK(cudaMemcpy(adr, P.o_adr, (size_t)P.n * P.d * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_get_mean_start(qjx_engine *h, double *mean_start)
+{
+    if (!h || !mean_start) return QJX_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaMemcpy(mean_start, h->P.mean_start, h->P.n * sizeof(double), cudaMemcpyDeviceToHost));
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, int *jumps_counts)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    const Params &P = h->P;
+    std::vector<TrajState> st(P.n);
+    CK(cudaMemcpy(st.data(), P.st, P.n * sizeof(TrajState), cudaMemcpyDeviceToHost));
+    if (psi) {
+        std::vector<double2> all((size_t)2 * P.n * P.MD);
+        CK(cudaMemcpy(all.data(), P.psi, all.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < P.n; i++)
+            memcpy(psi + (size_t)2 * i * P.d, all.data() + ((size_t)st[i].cur * P.n + i) * P.MD,
+                   (size_t)P.d * sizeof(double2));
+    }
+    for (int i = 0; i < P.n; i++) {
+        if (t) t[i] = st[i].t;
+        if (eta) eta[i] = st[i].eta;
+        if (jumps_counts) jumps_counts[i] = st[i].jumps;
+    }
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_jump_count(qjx_engine *h, int tr, int64_t *count)
+{
+    if (!h || !count || tr < 0 || tr >= h->P.n) return QJX_ERR_INVALID_ARG;
+    *count = (int64_t)h->jt[tr].size();
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_get_jumps(qjx_engine *h, int tr, double *times, int *types, double *norms, double *etas)
+{
+    if (!h || tr < 0 || tr >= h->P.n) return QJX_ERR_INVALID_ARG;
+    const size_t k = h->jt[tr].size();
+    if (times) memcpy(times, h->jt[tr].data(), k * sizeof(double));
+    if (types) memcpy(types, h->jtype[tr].data(), k * sizeof(int));
+    if (norms) memcpy(norms, h->jn[tr].data(), k * sizeof(double));
+    if (etas) memcpy(etas, h->je[tr].data(), k * sizeof(double));
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats)
+{
+    if (!h || !stats) return QJX_ERR_INVALID_ARG;
+    int64_t jumps = 0;
+    for (auto &v : h->jt) jumps += (int64_t)v.size();
+    h->stats.jumps = jumps;
+    *stats = h->stats;
+    return QJX_OK;
+}

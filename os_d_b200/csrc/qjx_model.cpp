@@ -1,0 +1,268 @@
+// qjx_model.cpp -- host construction of the dimer model and its split propagators (FP64).
+//
+// DimerNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp):
+//   init_sizes            :3-37     d = N + 1, T = 2 pi / omega, one jump operator, two branches
+//   init_hamiltonians     :450-498  H (interaction 2 (U/N) [k(k-1) + (N-k)(N-k-1)], hopping -J sqrt),
+//                                    H_drv = diag(N - 2k)
+//   init_dissipators      :1454-1498 L = diag(2k - N) + sqrt((k+1)(N-k)) (|k><k+1| - |k+1><k|)
+//   init_hamiltonians_qj  :2285-2388 K_b = -i (H - i/2 gamma L^H L + E_b H_drv), gamma = g/N,
+//                                    E_0 = E + A (first half period), E_1 = E - A
+// init_split_branches (source/cpp/QJX/QJX/qj_proc.cpp:4-120): U_{b,l} = exp(K_b dt_l),
+// dt_l = T 2^-(l+2).  The reference uses Eigen's MatrixXcd::exp(); this file implements the
+// same published method (Higham 2005 scaling and squaring with diagonal Pade approximants).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/qjx_b200.h"
+
+namespace {
+
+using cvec = std::vector<double>;  // interleaved complex, row-major
+
+void matmul(int n, const double *A, const double *B, double *C)
+{
+    std::memset(C, 0, sizeof(double) * 2 * (size_t)n * n);
+    for (int i = 0; i < n; i++) {
+        double *c = C + 2 * (size_t)i * n;
+        for (int k = 0; k < n; k++) {
+            const double ar = A[2 * ((size_t)i * n + k)], ai = A[2 * ((size_t)i * n + k) + 1];
+            if (ar == 0.0 && ai == 0.0) continue;
+            const double *b = B + 2 * (size_t)k * n;
+            for (int j = 0; j < n; j++) {
+                c[2 * j] += ar * b[2 * j] - ai * b[2 * j + 1];
+                c[2 * j + 1] += ar * b[2 * j + 1] + ai * b[2 * j];
+            }
+        }
+    }
+}
+
+// out = sum_i c_i M_i + c0 I
+void combine(int n, const std::vector<const double *> &M, const std::vector<double> &c, double c0, double *out)
+{
+    const size_t e2 = 2 * (size_t)n * n;
+    for (size_t e = 0; e < e2; e++) {
+        double s = 0.0;
+        for (size_t i = 0; i < M.size(); i++) s += c[i] * M[i][e];
+        out[e] = s;
+    }
+    for (int i = 0; i < n; i++) out[2 * ((size_t)i * n + i)] += c0;
+}
+
+// Solves P X = Q by LU with partial pivoting (P destroyed, X returned in Q).
+bool solve(int n, double *P, double *Q)
+{
+    auto at = [n](double *M, int r, int c) { return M + 2 * ((size_t)r * n + c); };
+    for (int c = 0; c < n; c++) {
+        int piv = c;
+        double best = -1.0;
+        for (int r = c; r < n; r++) {
+            const double v = std::hypot(at(P, r, c)[0], at(P, r, c)[1]);
+            if (v > best) {
+                best = v;
+                piv = r;
+            }
+        }
+        if (best == 0.0) return false;
+        if (piv != c)
+            for (int j = 0; j < n; j++)
+                for (int q = 0; q < 2; q++) {
+                    std::swap(at(P, c, j)[q], at(P, piv, j)[q]);
+                    std::swap(at(Q, c, j)[q], at(Q, piv, j)[q]);
+                }
+        const double pr = at(P, c, c)[0], pi = at(P, c, c)[1], den = pr * pr + pi * pi;
+        const double ir = pr / den, ii = -pi / den;
+        for (int r = c + 1; r < n; r++) {
+            const double ar = at(P, r, c)[0], ai = at(P, r, c)[1];
+            if (ar == 0.0 && ai == 0.0) continue;
+            const double fr = ar * ir - ai * ii, fi = ar * ii + ai * ir;
+            for (int j = c; j < n; j++) {
+                const double br = at(P, c, j)[0], bi = at(P, c, j)[1];
+                at(P, r, j)[0] -= fr * br - fi * bi;
+                at(P, r, j)[1] -= fr * bi + fi * br;
+            }
+            for (int j = 0; j < n; j++) {
+                const double br = at(Q, c, j)[0], bi = at(Q, c, j)[1];
+                at(Q, r, j)[0] -= fr * br - fi * bi;
+                at(Q, r, j)[1] -= fr * bi + fi * br;
+            }
+        }
+    }
+    for (int c = n - 1; c >= 0; c--) {
+        const double pr = at(P, c, c)[0], pi = at(P, c, c)[1], den = pr * pr + pi * pi;
+        const double ir = pr / den, ii = -pi / den;
+        for (int j = 0; j < n; j++) {
+            double sr = at(Q, c, j)[0], si = at(Q, c, j)[1];
+            for (int k = c + 1; k < n; k++) {
+                const double ar = at(P, c, k)[0], ai = at(P, c, k)[1];
+                const double xr = at(Q, k, j)[0], xi = at(Q, k, j)[1];
+                sr -= ar * xr - ai * xi;
+                si -= ar * xi + ai * xr;
+            }
+            at(Q, c, j)[0] = sr * ir - si * ii;
+            at(Q, c, j)[1] = sr * ii + si * ir;
+        }
+    }
+    return true;
+}
+
+// Diagonal Pade coefficients b_0..b_m and thresholds theta_m on ||A||_1 from Higham (2005).
+const double kB3[] = {120.0, 60.0, 12.0, 1.0};
+const double kB5[] = {30240.0, 15120.0, 3360.0, 420.0, 30.0, 1.0};
+const double kB7[] = {17297280.0, 8648640.0, 1995840.0, 277200.0, 25200.0, 1512.0, 56.0, 1.0};
+const double kB9[] = {17643225600.0, 8821612800.0, 2075673600.0, 302702400.0, 30270240.0,
+                      2162160.0,     110880.0,     3960.0,       90.0,        1.0};
+const double kB13[] = {64764752532480000.0, 32382376266240000.0, 7771770303897600.0, 1187353796428800.0,
+                       129060195264000.0,   10559470521600.0,    670442572800.0,     33522128640.0,
+                       1323241920.0,        40840800.0,          960960.0,           16380.0,
+                       182.0,               1.0};
+const double kTheta[] = {1.495585217958292e-2, 2.539398330063230e-1, 9.504178996162932e-1, 2.097847961257068e0,
+                         5.371920351148152e0};
+
+bool expm(int n, const double *Ain, double *out)
+{
+    const size_t e2 = 2 * (size_t)n * n;
+    cvec A(Ain, Ain + e2), A2(e2), A4(e2), A6(e2), A8(e2), W(e2), T(e2), Uo(e2), V(e2);
+    double l1 = 0.0;
+    for (int j = 0; j < n; j++) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++) s += std::hypot(A[2 * ((size_t)i * n + j)], A[2 * ((size_t)i * n + j) + 1]);
+        l1 = std::max(l1, s);
+    }
+    int m = 13, sq = 0;
+    if (l1 <= kTheta[0]) m = 3;
+    else if (l1 <= kTheta[1]) m = 5;
+    else if (l1 <= kTheta[2]) m = 7;
+    else if (l1 <= kTheta[3]) m = 9;
+    else {
+        sq = std::max(0, (int)std::ceil(std::log2(l1 / kTheta[4])));
+        const double sc = std::ldexp(1.0, -sq);
+        for (double &x : A) x *= sc;
+    }
+    matmul(n, A.data(), A.data(), A2.data());
+    if (m == 3) {
+        combine(n, {A2.data()}, {kB3[3]}, kB3[1], W.data());
+        matmul(n, A.data(), W.data(), Uo.data());
+        combine(n, {A2.data()}, {kB3[2]}, kB3[0], V.data());
+    } else if (m == 5) {
+        matmul(n, A2.data(), A2.data(), A4.data());
+        combine(n, {A4.data(), A2.data()}, {kB5[5], kB5[3]}, kB5[1], W.data());
+        matmul(n, A.data(), W.data(), Uo.data());
+        combine(n, {A4.data(), A2.data()}, {kB5[4], kB5[2]}, kB5[0], V.data());
+    } else if (m == 7) {
+        matmul(n, A2.data(), A2.data(), A4.data());
+        matmul(n, A4.data(), A2.data(), A6.data());
+        combine(n, {A6.data(), A4.data(), A2.data()}, {kB7[7], kB7[5], kB7[3]}, kB7[1], W.data());
+        matmul(n, A.data(), W.data(), Uo.data());
+        combine(n, {A6.data(), A4.data(), A2.data()}, {kB7[6], kB7[4], kB7[2]}, kB7[0], V.data());
+    } else if (m == 9) {
+        matmul(n, A2.data(), A2.data(), A4.data());
+        matmul(n, A4.data(), A2.data(), A6.data());
+        matmul(n, A6.data(), A2.data(), A8.data());
+        combine(n, {A8.data(), A6.data(), A4.data(), A2.data()}, {kB9[9], kB9[7], kB9[5], kB9[3]}, kB9[1],
+                W.data());
+        matmul(n, A.data(), W.data(), Uo.data());
+        combine(n, {A8.data(), A6.data(), A4.data(), A2.data()}, {kB9[8], kB9[6], kB9[4], kB9[2]}, kB9[0],
+                V.data());
+    } else {
+        matmul(n, A2.data(), A2.data(), A4.data());
+        matmul(n, A4.data(), A2.data(), A6.data());
+        const std::vector<const double *> M3 = {A6.data(), A4.data(), A2.data()};
+        combine(n, M3, {kB13[13], kB13[11], kB13[9]}, 0.0, T.data());
+        matmul(n, A6.data(), T.data(), W.data());
+        combine(n, M3, {kB13[7], kB13[5], kB13[3]}, kB13[1], T.data());
+        for (size_t e = 0; e < e2; e++) T[e] += W[e];
+        matmul(n, A.data(), T.data(), Uo.data());
+        combine(n, M3, {kB13[12], kB13[10], kB13[8]}, 0.0, T.data());
+        matmul(n, A6.data(), T.data(), W.data());
+        combine(n, M3, {kB13[6], kB13[4], kB13[2]}, kB13[0], V.data());
+        for (size_t e = 0; e < e2; e++) V[e] += W[e];
+    }
+    for (size_t e = 0; e < e2; e++) {
+        T[e] = V[e] - Uo[e];
+        out[e] = V[e] + Uo[e];
+    }
+    if (!solve(n, T.data(), out)) return false;
+    for (int k = 0; k < sq; k++) {
+        matmul(n, out, out, W.data());
+        std::memcpy(out, W.data(), sizeof(double) * e2);
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" qjx_status qjx_expm(int n, const double *A, double *out)
+{
+    if (n < 1 || !A || !out) return QJX_ERR_INVALID_ARG;
+    return expm(n, A, out) ? QJX_OK : QJX_ERR_INVALID_ARG;
+}
+
+extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega,
+                                      int deep, double *H, double *Hd, double *L, double *Utree)
+{
+    if (N < 1 || deep < 1 || !(omega > 0.0)) return QJX_ERR_INVALID_ARG;
+    const int d = N + 1;
+    const size_t dd = (size_t)d * d, e2 = 2 * dd;
+    cvec h(e2, 0.0), hd(e2, 0.0), l(e2, 0.0);
+    const double Us = U / double(d - 1);
+    for (int k = 0; k < d; k++) {
+        const size_t ii = 2 * ((size_t)k * d + k);
+        h[ii] = 2.0 * Us * double(k * (k - 1) + (d - (k + 1)) * (d - (k + 1) - 1));
+        hd[ii] = double((d - (k + 1)) - k);
+        l[ii] = double(k - (d - (k + 1)));
+    }
+    for (int k = 0; k < d - 1; k++) {
+        const size_t dl = 2 * ((size_t)(k + 1) * d + k), ur = 2 * ((size_t)k * d + (k + 1));
+        const double s = std::sqrt(double((d - (k + 1)) * (k + 1)));
+        h[dl] -= J * s;
+        h[ur] -= J * s;
+        l[dl] -= s;
+        l[ur] += s;
+    }
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (Hd) std::memcpy(Hd, hd.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), e2 * sizeof(double));
+    if (!Utree) return QJX_OK;
+
+    // gamma L^H L (real L), H_eff = H - i/2 gamma L^H L, K_b = -i (H_eff + E_b H_drv)
+    const double gamma = g / double(d - 1);
+    cvec K[2] = {cvec(e2), cvec(e2)};
+    const double Eb[2] = {E + A, E - A};
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            double sr = 0.0, si = 0.0;
+            for (int k = 0; k < d; k++) {
+                const double ar = l[2 * ((size_t)k * d + i)], ai = l[2 * ((size_t)k * d + i) + 1];
+                const double br = l[2 * ((size_t)k * d + j)], bi = l[2 * ((size_t)k * d + j) + 1];
+                sr = sr + (ar * br + ai * bi);
+                si = si + (ar * bi - ai * br);
+            }
+            const size_t idx = (size_t)i * d + j;
+            const double hr = h[2 * idx] + 0.5 * (gamma * si);
+            const double hi = 0.0 - 0.5 * (gamma * sr);
+            for (int b = 0; b < 2; b++) {
+                K[b][2 * idx] = 0.0 + (hi + Eb[b] * 0.0);
+                K[b][2 * idx + 1] = 0.0 - (hr + Eb[b] * hd[2 * idx]);
+            }
+        }
+    const double T = 2.0 * 3.1415926535897932384626433832795 / omega;
+    std::vector<double> dts(deep);
+    double dt = T * 0.5;
+    for (int lv = 0; lv < deep; lv++) {
+        dt *= 0.5;
+        dts[lv] = dt;
+    }
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) collapse(2) reduction(&& : ok)
+    for (int b = 0; b < 2; b++)
+        for (int lv = 0; lv < deep; lv++) {
+            cvec scaled(e2);
+            for (size_t e = 0; e < dd; e++) {
+                scaled[2 * e] = K[b][2 * e] * dts[lv];
+                scaled[2 * e + 1] = K[b][2 * e + 1] * dts[lv];
+            }
+            ok = expm(d, scaled.data(), Utree + e2 * ((size_t)b * deep + lv)) && ok;
+        }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

@@ -1,0 +1,165 @@
+"""Python handles over the C ABI (include/qjx_b200.h): QJ ensemble engine and f-basis RK4.
+
+These mirror the reference's in-process strategy API for the Std task with the QJ
+propagator (source/cpp/QJX/QJX/experiment.cpp:411-542: trans_process then obser_process),
+batched over every trajectory of the ensemble.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class Engine:
+    """One ensemble of trajectories resident on a GPU."""
+
+    def __init__(self, U, L, g, HE, R=None, T=2 * np.pi, n_traj=1, seed=0, record=0, rng_kind=0, rec_cap=1024,
+                 keep_adr=0, max_dumps=1, device=0):
+        U = np.ascontiguousarray(U, np.complex128)
+        nb, deep, d, _ = U.shape
+        L = np.ascontiguousarray(L, np.complex128).reshape(-1, d, d)
+        g = np.ascontiguousarray(np.atleast_1d(g), np.float64)
+        HE = np.ascontiguousarray(HE, np.complex128)
+        R = np.zeros((0, d, d), np.complex128) if R is None else np.ascontiguousarray(R, np.complex128).reshape(-1, d, d)
+        cfg = N.QjxConfig()
+        cfg.d, cfg.n_traj, cfg.deep, cfg.num_branches = d, n_traj, deep, nb
+        cfg.num_diss, cfg.num_robs, cfg.T, cfg.record = L.shape[0], R.shape[0], T, record
+        cfg.rng_kind, cfg.seed, cfg.rec_cap, cfg.keep_adr = rng_kind, seed, rec_cap, keep_adr
+        cfg.max_dumps, cfg.device = max_dumps, device
+        self.cfg = cfg
+        self.d, self.n, self.nr = d, n_traj, R.shape[0]
+        self.keep_adr = keep_adr
+        h = C.c_void_p()
+        N.check(N.lib().qjx_create(C.byref(cfg), N.dp(U), N.dp(L), N.dp(g), N.dp(HE), N.dp(R) if R.size else None,
+                                   C.byref(h)), what="qjx_create")
+        self.h = h
+
+    def _chk(self, st, what):
+        N.check(st, self.h, what)
+
+    def close(self):
+        if self.h:
+            N.lib().qjx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_states(self, psi):
+        psi = np.ascontiguousarray(psi, np.complex128)
+        assert psi.shape == (self.n, self.d)
+        self._chk(N.lib().qjx_set_states(self.h, N.dp(psi)), "qjx_set_states")
+
+    def set_uniforms(self, u, offsets):
+        u = np.ascontiguousarray(u, np.float64)
+        off = np.ascontiguousarray(offsets, np.int64)
+        self._chk(N.lib().qjx_set_uniforms(self.h, N.dp(u), off.ctypes.data_as(N.c_i64_p)), "qjx_set_uniforms")
+
+    def init_thresholds(self):
+        self._chk(N.lib().qjx_init_thresholds(self.h), "qjx_init_thresholds")
+
+    def run_periods(self, n_periods, is_obs=1, dump_at=(), dump_base=0):
+        da = np.ascontiguousarray(dump_at, np.int32)
+        self._chk(N.lib().qjx_run_periods(self.h, n_periods, is_obs, N.ip(da) if da.size else None, int(da.size),
+                                          dump_base), "qjx_run_periods")
+
+    def reset_times(self):
+        self._chk(N.lib().qjx_reset_times(self.h), "qjx_reset_times")
+
+    def observe(self, dump, is_start=False):
+        self._chk(N.lib().qjx_observe(self.h, dump, int(is_start)), "qjx_observe")
+
+    def observables(self, dump0=0, n_dumps=1, want_adr=False):
+        n = self.n
+        out = {k: np.zeros((n_dumps, n)) for k in ("norm", "mean", "dispersion", "m2", "energy")}
+        robs = np.zeros((n_dumps, n, max(self.nr, 1)), np.complex128)
+        adr = None
+        if want_adr:
+            adr = np.zeros((n_dumps, n, self.d)) if self.keep_adr else np.zeros((n, self.d))
+        self._chk(N.lib().qjx_get_observables(self.h, dump0, n_dumps, N.dp(out["norm"]), N.dp(out["mean"]),
+                                              N.dp(out["dispersion"]), N.dp(out["m2"]), N.dp(out["energy"]),
+                                              N.dp(robs), N.dp(adr)), "qjx_get_observables")
+        out["random_obs"] = robs[:, :, : self.nr]
+        if want_adr:
+            out["adr"] = adr
+        return out
+
+    def mean_start(self):
+        ms = np.zeros(self.n)
+        self._chk(N.lib().qjx_get_mean_start(self.h, N.dp(ms)), "qjx_get_mean_start")
+        return ms
+
+    def states(self):
+        psi = np.zeros((self.n, self.d), np.complex128)
+        t = np.zeros(self.n)
+        eta = np.zeros(self.n)
+        jc = np.zeros(self.n, np.int32)
+        self._chk(N.lib().qjx_get_states(self.h, N.dp(psi), N.dp(t), N.dp(eta), N.ip(jc)), "qjx_get_states")
+        return psi, t, eta, jc
+
+    def jumps(self, tr):
+        k = C.c_int64()
+        self._chk(N.lib().qjx_jump_count(self.h, tr, C.byref(k)), "qjx_jump_count")
+        k = k.value
+        times, norms, etas = np.zeros(k), np.zeros(k), np.zeros(k)
+        types = np.zeros(k, np.int32)
+        self._chk(N.lib().qjx_get_jumps(self.h, tr, N.dp(times), N.ip(types), N.dp(norms), N.dp(etas)),
+                  "qjx_get_jumps")
+        return times, types, norms, etas
+
+    def stats(self):
+        s = N.QjxStats()
+        self._chk(N.lib().qjx_get_stats(self.h, C.byref(s)), "qjx_get_stats")
+        return {k: getattr(s, k) for k, _ in N.QjxStats._fields_}
+
+
+class FBasis:
+    """f-basis RK4 of dx/dt = Gs x + E(t) Qs_drv x - Ks on a GPU."""
+
+    def __init__(self, Gs, Qs, Ks, x0, drv_ampl, drv_freq=1.0, drv_phase=0.0, drv_type=0, T=2 * np.pi,
+                 num_steps=1000, device=0):
+        n = Gs.shape[0]
+        self.n = n
+        self._keep = []
+
+        def csr(M):
+            M = M.tocsr()
+            M.sort_indices()
+            a = (np.ascontiguousarray(M.indptr, np.int32), np.ascontiguousarray(M.indices, np.int32),
+                 np.ascontiguousarray(M.data, np.float64))
+            self._keep.append(a)
+            return a
+
+        gr, gc, gv = csr(Gs)
+        qr, qc, qv = csr(Qs)
+        Ks = np.ascontiguousarray(Ks, np.float64)
+        x0 = np.ascontiguousarray(x0, np.float64)
+        h = C.c_void_p()
+        N.check(N.lib().qjx_fb_create(n, N.ip(gr), N.ip(gc), N.dp(gv), N.ip(qr), N.ip(qc), N.dp(qv), N.dp(Ks),
+                                      N.dp(x0), drv_ampl, drv_freq, drv_phase, drv_type, T, num_steps, device,
+                                      C.byref(h)), what="qjx_fb_create")
+        self.h = h
+
+    def run(self, period0, n_periods):
+        N.check(N.lib().qjx_fb_run(self.h, period0, n_periods), what="qjx_fb_run")
+
+    def get(self):
+        x = np.zeros(self.n)
+        ms = C.c_double()
+        N.check(N.lib().qjx_fb_get(self.h, N.dp(x), C.byref(ms)), what="qjx_fb_get")
+        return x, ms.value
+
+    def close(self):
+        if self.h:
+            N.lib().qjx_fb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
