@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark of the QJ trajectory engine on one node.
+
+Workload: the driven dissipative Bose dimer at N = 200 (Hilbert dim 201), 10^4 trajectories
+per GPU, ex_deep 16, QJ propagator, complex FP64 end to end (the plain drop-in form), Philox
+thresholds seed 7, start state |N,0>.  One step = one dump interval of 10 periods for every
+trajectory with the observables taken at its end (1000 periods with 100 dumps is the full
+job).  Metric: trajectory-periods per second over all GPUs.
+
+  python bench.py --gpus N --steps K --warmup W            # this engine
+  python bench.py --impl reference --steps K --warmup W    # CPU restatement of the reference
+
+Multi-GPU: one process per GPU (torchrun); trajectories are sharded (rank r owns global
+trajectories r*n .. r*n+n-1, so the ensemble is the one a single GPU would run), the
+ensemble sums of the observables are all-reduced over NCCL once per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BOSONS = 200
+PRM = dict(J=1.0, U=0.5, E=1.0, A=1.5, g=0.1, omega=1.0)
+DEEP = 16
+SEED = 7
+METRIC = "traj*periods/s"
+WORKLOAD = ("dimer N=200 (dim 201), ex_deep 16, QJ propagator, complex FP64 plain form, "
+            "10^4 trajectories per GPU x 10 periods per step")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-traj", type=int, default=10000)
+    ap.add_argument("--periods-per-step", type=int, default=10)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def model():
+    import os_d_b200 as q
+
+    H, Hd, L, Ut = q.build_dimer(N_BOSONS, PRM["J"], PRM["U"], PRM["E"], PRM["A"], PRM["g"], PRM["omega"], DEEP)
+    d = N_BOSONS + 1
+    HE = H + PRM["E"] * Hd
+    rng = np.random.default_rng(1)  # one random observable X X^H / (tr/d)
+    X = 0.5 * (rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d)))
+    R = X @ X.conj().T
+    R = (R / (np.trace(R).real / d))[None]
+    T = 2.0 * 3.1415926535897932384626433832795 / PRM["omega"]
+    return dict(H=H, Hd=Hd, L=L, U=Ut, HE=HE, R=R, T=T, d=d)
+
+
+def start_states(n, d):
+    psi = np.zeros((n, d), np.complex128)
+    psi[:, 0] = 1.0
+    return psi
+
+
+# ---------------------------------------------------------------- CPU restatement (baseline)
+def cpu_rate(M, n_traj, periods, threads, tr_base=0):
+    """Trajectory-periods/s of the CPU oracle (OpenMP over trajectories like the reference)."""
+    from oracle import oracle_py as O
+
+    ens = O.Ensemble(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n_traj, seed=SEED, record=0)
+    ens.init(0, 0)
+    t0 = time.perf_counter()
+    bad = ens.run_periods(periods, is_obs=1, n_threads=threads)
+    dt = time.perf_counter() - t0
+    if bad:
+        raise RuntimeError("oracle reported trajectory errors")
+    return n_traj * periods / dt, dt, float(ens.matvecs.sum()) / (n_traj * periods)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    M = model()
+    threads = os.cpu_count() or 1
+    sample = 2 * threads
+    for _ in range(args.warmup):
+        cpu_rate(M, sample, 1, threads)
+    rates = []
+    tot = 0.0
+    for _ in range(args.steps):
+        r, dt, mv = cpu_rate(M, sample, 1, threads)
+        rates.append(r)
+        tot += dt
+    value = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("10^4 trajectories per GPU x 10 periods per step",
+                                                f"{sample} trajectories x 1 period per step (bounded CPU sample)"),
+                   "n_traj": sample, "dim": M["d"], "ex_deep": DEEP, "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{sample} trajectories x 1 period at dim 201 per step, OpenMP over trajectories"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference (source/cpp/QJX) needs Intel MKL and Eigen, absent here; this arm times the "
+                 "C restatement of its algorithm (oracle/qjx_oracle.c) on the host cores"),
+        "matvecs_per_traj_period": mv,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.gpu = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in self.f.read().strip().splitlines():
+            c = [x.strip() for x in row.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax.append(float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- this engine
+def run_ours(args):
+    import torch
+
+    import os_d_b200 as q
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def allreduce(x, op="sum"):
+        t = torch.tensor(x, dtype=torch.float64, device="cuda")
+        if pg:
+            pg.all_reduce(t, op=pg.ReduceOp.MAX if op == "max" else pg.ReduceOp.SUM)
+        return t.cpu().numpy()
+
+    M = model()
+    n, d, P = args.n_traj, M["d"], args.periods_per_step
+    steps_total = args.warmup + args.steps
+    eng = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, record=0, rec_cap=16,
+                   keep_adr=0, max_dumps=steps_total + 1, device=local, tr_base=rank * n)
+    psi0 = start_states(n, d)
+    eng.set_states(psi0)
+    eng.init_thresholds()
+    eng.reset_times()
+    eng.observe(0, is_start=True)
+    if args.profile:
+        eng.run_periods(1, is_obs=1)
+        eng.close()
+        return
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def one_step(slot):
+        eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=slot)
+        ob = eng.observables(slot, 1)
+        # ensemble <n1 - n2> = N - 2 mean, reduced over ranks (the one exchange of the path)
+        return allreduce([float(np.sum(N_BOSONS - 2.0 * ob["mean"][0])), float(n)])
+
+    for w in range(args.warmup):
+        one_step(1 + w)
+    st0 = eng.stats()
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    t0 = time.perf_counter()
+    dev_ms = 0.0
+    ens_sum = None
+    for k in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps
+        torch.cuda.synchronize()
+        ens_sum = one_step(1 + args.warmup + k)
+        dev_ms += eng.stats()["last_call_ms"]
+    barrier()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    st1 = eng.stats()
+    dev_ms_max = float(allreduce([dev_ms], "max")[0])
+    value = world * n * P * args.steps / (dev_ms_max * 1e-3)
+    ms_per_step = dev_ms_max / args.steps
+
+    # roofline of the dominant kernel (step_kernel, grouped FP64 complex GEMM + fused epilogue)
+    matvecs = st1["matvecs"] - st0["matvecs"]
+    launches_step = st1["micro_steps"] - st0["micro_steps"]
+    kern_ms = st1["step_kernel_ms"] - st0["step_kernel_ms"]
+    flops = 8.0 * d * d * matvecs
+    achieved = flops / (kern_ms * 1e-3) / 1e12
+    peak = q.measure_fp64_peak(local)
+    roofline = {"bound": "tensor", "pipe": "FP64 FMA (FP64 has no tcgen05 kind; DMMA and FFMA share the FP64 peak)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "measured live: FP64 FFMA-chain microbenchmark (qjx_measure_fp64_peak)",
+                "traffic": None, "kernel": "qjx::step_kernel<7>",
+                "algorithmic_flops_per_launch": flops / max(launches_step, 1),
+                "avg_launch_ms": kern_ms / max(launches_step, 1),
+                "matvecs_per_traj_period": matvecs / (n * P * args.steps)}
+    traffic_file = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            tf = json.load(f)
+        roofline["traffic"] = tf.get("bytes_per_launch")
+        roofline["traffic_source"] = tf.get("source")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_traj_per_gpu": n, "dim": d, "ex_deep": DEEP,
+                   "periods_per_step": P, "seed": SEED, "start": "|N,0>", "parallelism": f"dp{world} (trajectories)",
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "wall_s": wall, "roofline": roofline, "clocks": clk,
+        "gpu_launches": int(st1["launches"] - st0["launches"]),
+        "ensemble_n1_minus_n2": float(ens_sum[0] / ens_sum[1]) if ens_sum is not None else None,
+    }
+
+    # e2e through the public C ABI with host buffers, copies inside the timed region
+    if not args.no_e2e:
+        host_psi = torch.empty((n, d), dtype=torch.complex128, pin_memory=True).numpy()
+        host_psi[:] = psi0
+        barrier()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            eng.set_states(host_psi)
+            eng.init_thresholds()
+            eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=1 + args.warmup + k)
+            ob = eng.observables(1 + args.warmup + k, 1)
+            eng.states()
+            allreduce([float(np.sum(N_BOSONS - 2.0 * ob["mean"][0])), float(n)])
+        barrier()
+        e2e_s = float(allreduce([time.perf_counter() - t0], "max")[0])
+        line["e2e"] = {"value": world * n * P * args.steps / e2e_s, "unit": METRIC,
+                       "h2d_bytes_per_step": int(n * d * 16), "d2h_bytes_per_step": int(n * d * 16 + 5 * n * 8 + n * 16),
+                       "path": "qjx_set_states + qjx_init_thresholds + qjx_run_periods + qjx_get_observables + "
+                               "qjx_get_states per step"}
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = 2 * threads
+        rate, dt, mv = cpu_rate(M, sample, 1, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
+                                "sample": f"{sample} trajectories x 1 period at dim 201 ({dt:.1f} s), "
+                                          f"OpenMP over trajectories, oracle/qjx_oracle.c"}
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -70,14 +70,18 @@ typedef struct {
     int keep_adr;      /* 0: keep the latest |psi_k|^2/|psi|^2 only; 1: keep it for every dump */
     int max_dumps;     /* capacity of the observable arrays (dump_num_total) */
     int device;        /* CUDA device ordinal */
+    int64_t tr_base;   /* global index of trajectory 0 (Philox stream id = tr_base + local index), so
+                          an ensemble sharded over GPUs draws exactly the numbers of one big run */
 } qjx_config;
 
 typedef struct {
     int64_t micro_steps;     /* lock-step micro-steps launched */
     int64_t matvecs;         /* complex d x d matvecs executed (trajectory-steps) */
     int64_t jumps;           /* jumps recorded */
-    double kernel_ms;        /* device time of the micro-step kernels (CUDA events) */
+    double kernel_ms;        /* device time of run/observe calls, first to last launch (CUDA events) */
     double last_call_ms;     /* device time of the last run/observe call */
+    double step_kernel_ms;   /* device time of the micro-step kernel batches alone (CUDA events) */
+    int64_t launches;        /* kernels launched by the engine */
 } qjx_stats;
 
 /* U: [num_branches][deep][d][d] split propagators exp(K_b dt_l), dt_l = T 2^-(l+2).
@@ -113,6 +117,9 @@ qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, in
 qjx_status qjx_jump_count(qjx_engine *h, int tr, int64_t *count);
 qjx_status qjx_get_jumps(qjx_engine *h, int tr, double *times, int *types, double *norms, double *etas);
 qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats);
+/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA): an FFMA-chain
+ * microbenchmark, used as the roofline peak of the FP64 contraction. */
+qjx_status qjx_measure_fp64_peak(int device, double *tflops);
 
 /* Dimer model on the host (FP64): H, Hd, L [d][d]; Utree [2][deep][d][d] (any may be NULL). */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,

@@ -20,7 +20,7 @@ EXPORTS = [
     "qjx_create", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
-    "qjx_build_dimer", "qjx_expm", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
+    "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
 
@@ -28,12 +28,13 @@ class QjxConfig(C.Structure):
     _fields_ = [("d", C.c_int), ("n_traj", C.c_int), ("deep", C.c_int), ("num_branches", C.c_int),
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
-                ("max_dumps", C.c_int), ("device", C.c_int)]
+                ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64)]
 
 
 class QjxStats(C.Structure):
     _fields_ = [("micro_steps", C.c_int64), ("matvecs", C.c_int64), ("jumps", C.c_int64),
-                ("kernel_ms", C.c_double), ("last_call_ms", C.c_double)]
+                ("kernel_ms", C.c_double), ("last_call_ms", C.c_double), ("step_kernel_ms", C.c_double),
+                ("launches", C.c_int64)]
 
 
 _lib = None
@@ -72,6 +73,7 @@ def lib():
         L.qjx_jump_count.argtypes = [vp, C.c_int, c_i64_p]
         L.qjx_get_jumps.argtypes = [vp, C.c_int, c_double_p, c_int_p, c_double_p, c_double_p]
         L.qjx_get_stats.argtypes = [vp, C.POINTER(QjxStats)]
+        L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p]
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 4
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_fb_create.argtypes = ([C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_int_p, c_double_p,
@@ -110,6 +112,12 @@ def build_dimer(N, J, U, E, A, g, omega, deep):
     Ut = np.zeros((2, deep, d, d), np.complex128)
     check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(Lm), dp(Ut)), what="qjx_build_dimer")
     return H, Hd, Lm, Ut
+
+
+def measure_fp64_peak(device=0):
+    out = C.c_double()
+    check(lib().qjx_measure_fp64_peak(device, C.byref(out)), what="qjx_measure_fp64_peak")
+    return out.value
 
 
 def expm(A):

@@ -64,6 +64,7 @@ struct Params {
     // rng
     int rng_kind;
     unsigned long long seed;
+    long long tr_base;
     const double *inj_u;
     const long long *inj_off;
     // run
@@ -118,7 +119,8 @@ __device__ __forceinline__ double philox_uniform(unsigned long long seed, unsign
 // Next uniform of a trajectory; sets *err on an exhausted injected sequence.
 __device__ __forceinline__ double draw(const Params &P, int tr, TrajState &s, int *err)
 {
-    if (P.rng_kind == 0) return philox_uniform(P.seed, (unsigned long long)tr, (unsigned long long)(s.rng_pos++));
+    if (P.rng_kind == 0)
+        return philox_uniform(P.seed, (unsigned long long)(P.tr_base + tr), (unsigned long long)(s.rng_pos++));
     const long long lo = P.inj_off[tr], hi = P.inj_off[tr + 1];
     if (lo + s.rng_pos >= hi) { *err = ERR_RNG; return 0.5; }
     return P.inj_u[lo + (s.rng_pos++)];

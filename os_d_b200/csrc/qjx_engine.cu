@@ -20,6 +20,7 @@ cudaError_t launch_init_state(const Params &P, cudaStream_t st);
 cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
 cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
 cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
+cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st);
 }  // namespace qjx
 
 using namespace qjx;
@@ -30,7 +31,7 @@ struct qjx_engine {
     int MD = 0;
     int grid = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, eb0 = nullptr, eb1 = nullptr;
     std::string err;
     // device allocations
     std::vector<void *> allocs;
@@ -131,6 +132,8 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(QJX_ERR_CUDA);
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
+    cudaEventCreate(&h->eb0);
+    cudaEventCreate(&h->eb1);
 
     const int d = c.d, n = c.n_traj;
     const int MD = 32 * ((d + 31) / 32);
@@ -149,6 +152,7 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     P.gR0 = P.gHE + 1;
     P.rng_kind = c.rng_kind;
     P.seed = c.seed;
+    P.tr_base = c.tr_base;
     P.keep_adr = c.keep_adr;
     P.rec_cap = h->cfg.rec_cap;
 
@@ -233,6 +237,8 @@ extern "C" void qjx_destroy(qjx_engine *h)
     if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->eb0) cudaEventDestroy(h->eb0);
+    if (h->eb1) cudaEventDestroy(h->eb1);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -380,6 +386,7 @@ static qjx_status run_until_idle(qjx_engine *h)
     cudaMemcpy(&work0, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
     cudaEventRecord(h->ev0, h->stream);
     while (true) {
+        cudaEventRecord(h->eb0, h->stream);
         for (int b = 0; b < batch; b++) {
             cudaError_t e = cudaGraphLaunch(exec, h->stream);
             if (e != cudaSuccess) {
@@ -389,6 +396,7 @@ static qjx_status run_until_idle(qjx_engine *h)
         }
         if (rs != QJX_OK) break;
         steps += 6 * batch;
+        cudaEventRecord(h->eb1, h->stream);
         cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
         cudaMemcpyAsync(h->h_ctrl, P.ctrl, sizeof(int) * 16, cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -396,6 +404,9 @@ static qjx_status run_until_idle(qjx_engine *h)
             rs = cuda_fail(h, e, "micro-step batch");
             break;
         }
+        float bms = 0.f;
+        cudaEventElapsedTime(&bms, h->eb0, h->eb1);
+        h->stats.step_kernel_ms += bms;
         rs = check_ctrl(h);
         if (rs != QJX_OK) break;
         long long active = 0;
@@ -407,6 +418,7 @@ static qjx_status run_until_idle(qjx_engine *h)
                 cudaMemsetAsync(P.ctrl + 2, 0, sizeof(int), h->stream);
                 cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream);
                 cudaError_t le = launch_schedule(P, 1, h->stream);
+                h->stats.launches += 2;
                 if (le != cudaSuccess) {
                     rs = cuda_fail(h, le, "launch_schedule");
                     break;
@@ -424,6 +436,7 @@ static qjx_status run_until_idle(qjx_engine *h)
     h->stats.kernel_ms += ms;
     h->stats.last_call_ms = ms;
     h->stats.micro_steps += steps;
+    h->stats.launches += steps;
     long long work1 = 0;
     cudaMemcpy(&work1, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
     h->stats.matvecs += work1 - work0;
@@ -459,6 +472,7 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
     CK(launch_schedule(P, 0, h->stream));
+    h->stats.launches += 1;
     qjx_status s = run_until_idle(h);
     if (s != QJX_OK) return s;
     return drain_records(h);
@@ -477,6 +491,7 @@ extern "C" qjx_status qjx_observe(qjx_engine *h, int dump, int is_start)
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
     CK(launch_observe(P, dump, is_start, h->stream));
+    h->stats.launches += 1;
     return run_until_idle(h);
 }
 
@@ -559,5 +574,37 @@ extern "C" qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats)
     for (auto &v : h->jt) jumps += (int64_t)v.size();
     h->stats.jumps = jumps;
     *stats = h->stats;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_measure_fp64_peak(int device, double *tflops)
+{
+    if (!tflops) return QJX_ERR_INVALID_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return QJX_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *out = nullptr;
+    if (cudaMalloc(&out, 16) != cudaSuccess) return QJX_ERR_OOM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 4, iters = 1 << 16;
+    launch_fp64_peak(out, blocks, iters, 0);  // warm-up
+    double best = 0.0;
+    for (int r = 0; r < 5; r++) {
+        cudaEventRecord(a, 0);
+        launch_fp64_peak(out, blocks, iters, 0);
+        cudaEventRecord(b, 0);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        const double fl = 2.0 * 8.0 * (double)iters * blocks * 256.0;
+        best = std::max(best, fl / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (cudaGetLastError() != cudaSuccess) return QJX_ERR_CUDA;
+    *tflops = best;
     return QJX_OK;
 }

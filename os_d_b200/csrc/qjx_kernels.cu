@@ -696,6 +696,28 @@ cudaError_t launch_reset_times(const Params &P, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// FP64 FMA throughput microbenchmark: 8 independent fma chains per thread.
+__global__ void fp64_peak_kernel(double *out, int iters, double a, double b)
+{
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) x[i] = threadIdx.x * 1e-9 + i;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = __fma_rn(x[i], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += x[i];
+    if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
+cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st)
+{
+    fp64_peak_kernel<<<blocks, 256, 0, st>>>(out, iters, 0.9999999, 1e-7);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_clear_records(const Params &P, cudaStream_t st)
 {
     clear_records_kernel<<<(P.n + 255) / 256, 256, 0, st>>>(P);
