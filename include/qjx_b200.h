@@ -117,9 +117,16 @@ qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, in
 qjx_status qjx_jump_count(qjx_engine *h, int tr, int64_t *count);
 qjx_status qjx_get_jumps(qjx_engine *h, int tr, double *times, int *types, double *norms, double *etas);
 qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats);
-/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA): an FFMA-chain
- * microbenchmark, used as the roofline peak of the FP64 contraction. */
-qjx_status qjx_measure_fp64_peak(int device, double *tflops);
+/* Per-CTA trace of the micro-step kernel (profiling aid, off by default): enabling clears
+ * and starts accumulating, per persistent CTA, clock64 cycles {total, setup, (reserved),
+ * MMA loop, epilogue} and counts {sub-tiles, 8-column blocks, columns}.  qjx_get_trace
+ * copies [n_ctas][n_fields] int64 (out may be NULL to query the shape). */
+qjx_status qjx_set_trace(qjx_engine *h, int enable);
+qjx_status qjx_get_trace(qjx_engine *h, int64_t *out, int *n_ctas, int *n_fields);
+/* Measured FP64 throughput of the device in TFLOP/s (2 flops per FMA): an FFMA-chain
+ * microbenchmark and an m8n8k4 FP64 tensor-core (DMMA) chain microbenchmark; the larger is
+ * the roofline peak of the FP64 contraction.  Either pointer may be NULL. */
+qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_tflops);
 
 /* Dimer model on the host (FP64): H, Hd, L [d][d]; Utree [2][deep][d][d] (any may be NULL). */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,

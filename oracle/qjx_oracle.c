@@ -438,15 +438,29 @@ static int tmat_make(int d, int count, const double *M, tmat *out)
 
 static void tmat_free(tmat *t) { free(t->r); free(t->i); }
 
+/* Canonical 32-way reduction: lane l holds the literal running sum of the terms with index
+ * l, l+32, l+64, ... (ascending); the 32 partial sums are then combined by an xor
+ * butterfly, offsets 16, 8, 4, 2, 1 (q[l] = p[l] + p[l ^ off]).  Addition is commutative,
+ * so every lane of a GPU warp ends with the value returned here. */
+static double lanes_finish(double p[32])
+{
+    for (int off = 16; off >= 1; off >>= 1) {
+        double q[32];
+        for (int l = 0; l < 32; l++) q[l] = p[l] + p[l ^ off];
+        memcpy(p, q, sizeof(q));
+    }
+    return p[0];
+}
+
 double orc_norm_square(int d, const double *x)
 {
-    double n = 0.0;
+    double p[32] = {0};
     for (int i = 0; i < d; i++) {
         const double a = x[2 * i] * x[2 * i];
         const double b = x[2 * i + 1] * x[2 * i + 1];
-        n = n + (a + b);
+        p[i & 31] = p[i & 31] + (a + b);
     }
-    return n;
+    return lanes_finish(p);
 }
 
 /* ------------------------------------------------------------------ QJ engine */
@@ -656,12 +670,14 @@ int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
             const double a = phi[2 * st] * phi[2 * st], b = phi[2 * st + 1] * phi[2 * st + 1];
             adr[st] = (0.0 + (a + b)) * (1.0 / norm);
         }
-        double mean = 0.0;
-        for (int st = 0; st < d; st++) mean = mean + (double)st * adr[st];
+        double ps[32] = {0};
+        for (int st = 0; st < d; st++) ps[st & 31] = ps[st & 31] + (double)st * adr[st];
+        const double mean = lanes_finish(ps);
         const double ms = is_start ? mean : mean_start[tr];
         const double disp = (mean - ms) * (mean - ms);
-        double m2 = 0.0;
-        for (int st = 0; st < d; st++) m2 = m2 + ((double)st - mean) * ((double)st - mean) * adr[st];
+        memset(ps, 0, sizeof(ps));
+        for (int st = 0; st < d; st++) ps[st & 31] = ps[st & 31] + ((double)st - mean) * ((double)st - mean) * adr[st];
+        const double m2 = lanes_finish(ps);
         /* normalised state and energy <psi|H + E0 Hd|psi> (experiment.cpp:1423-1469) */
         const double sq = sqrt(norm);
         for (int st = 0; st < d; st++) {
@@ -669,22 +685,24 @@ int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
             xh[2 * st + 1] = phi[2 * st + 1] / sq;
         }
         matvec_t(d, tH.ld, tH.r, tH.i, xh, sm);
-        double energy = 0.0;
+        memset(ps, 0, sizeof(ps));
         for (int st = 0; st < d; st++) {
             const double a = xh[2 * st] * sm[2 * st], b = xh[2 * st + 1] * sm[2 * st + 1];
-            energy = energy + (a + b);
+            ps[st & 31] = ps[st & 31] + (a + b);
         }
+        const double energy = lanes_finish(ps);
         /* random observables <psi|R|psi> (experiment.cpp:2023-2078) */
         for (int o = 0; o < p->num_robs; o++) {
             matvec_t(d, tR.ld, tR.r + per * o, tR.i + per * o, xh, sm);
-            double rr = 0.0, ri = 0.0;
+            double pr[32] = {0}, pi[32] = {0};
             for (int st = 0; st < d; st++) {
                 const double cr = xh[2 * st], ci = -xh[2 * st + 1];
                 const double tr_ = cr * sm[2 * st] - ci * sm[2 * st + 1];
                 const double ti_ = ci * sm[2 * st] + cr * sm[2 * st + 1];
-                rr = rr + tr_;
-                ri = ri + ti_;
+                pr[st & 31] = pr[st & 31] + tr_;
+                pi[st & 31] = pi[st & 31] + ti_;
             }
+            const double rr = lanes_finish(pr), ri = lanes_finish(pi);
             robs[2 * ((size_t)tr * p->num_robs + o)] = rr;
             robs[2 * ((size_t)tr * p->num_robs + o) + 1] = ri;
         }

@@ -23,7 +23,9 @@
  * Arithmetic contract (shared bit-for-bit with the CUDA engine):
  *   complex matvec out_i = sum_k M_ik x_k, k ascending from 0, per k:
  *       re = fma(Mr, xr, re); re = fma(-Mi, xi, re); im = fma(Mr, xi, im); im = fma(Mi, xr, im)
- *   norm_square  n = n + (re*re + im*im), i ascending, no contraction
+ *   reductions over the d components (norm_square, mean, m2, energy, random observables):
+ *       32 lane sums, lane l = literal running sum over i = l, l+32, ... ascending, then an
+ *       xor butterfly over offsets 16, 8, 4, 2, 1 (a GPU warp's shfl_xor reduction)
  *   every other expression is evaluated literally (compiled with -ffp-contract=off).
  *
  * Complex arrays are interleaved (re, im) doubles, matrices row-major d x d, like

@@ -20,7 +20,7 @@ EXPORTS = [
     "qjx_create", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
-    "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
+    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
 
@@ -73,7 +73,9 @@ def lib():
         L.qjx_jump_count.argtypes = [vp, C.c_int, c_i64_p]
         L.qjx_get_jumps.argtypes = [vp, C.c_int, c_double_p, c_int_p, c_double_p, c_double_p]
         L.qjx_get_stats.argtypes = [vp, C.POINTER(QjxStats)]
-        L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p]
+        L.qjx_set_trace.argtypes = [vp, C.c_int]
+        L.qjx_get_trace.argtypes = [vp, c_i64_p, c_int_p, c_int_p]
+        L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 4
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_fb_create.argtypes = ([C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_int_p, c_double_p,
@@ -115,9 +117,10 @@ def build_dimer(N, J, U, E, A, g, omega, deep):
 
 
 def measure_fp64_peak(device=0):
-    out = C.c_double()
-    check(lib().qjx_measure_fp64_peak(device, C.byref(out)), what="qjx_measure_fp64_peak")
-    return out.value
+    """(FFMA TFLOP/s, FP64 tensor-core DMMA TFLOP/s) measured on the device."""
+    f, m = C.c_double(), C.c_double()
+    check(lib().qjx_measure_fp64_peak(device, C.byref(f), C.byref(m)), what="qjx_measure_fp64_peak")
+    return f.value, m.value
 
 
 def expm(A):

@@ -13,15 +13,16 @@
 namespace qjx {
 
 // ---- launch geometry of the micro-step kernel ----
-constexpr int kThreads = 256;          // 8 warps
-constexpr int kTY = 32;                // row threads: rows ty + 32 i, i < MT
-constexpr int kTX = 8;                 // column threads: columns tx + 8 j, j < kNT
-constexpr int kNT = 4;                 // columns per thread
-constexpr int kNC = kTX * kNT;         // 32 trajectory columns per tile
-constexpr int kKB = 8;                 // k rows per propagator slab
-constexpr int kStages = 3;             // slab pipeline depth
+constexpr int kThreads = 512;          // 16 warps (micro-step kernel)
+constexpr int kNC = 32;                // trajectory columns per sub-tile (max)
+constexpr int kKB = 16;                // k rows per propagator slab (8 k pairs)
+constexpr int kStages = 2;             // slab pipeline depth
 constexpr int kMaxGroups = 256;        // distinct matrices in one engine
-constexpr int kMaxMT = 8;              // d <= 256
+constexpr int kMaxMD = 256;            // d <= 256
+// Thread layouts of a sub-tile (rows ty + TY i, columns tx + TX j, TY * TX = 256):
+//   TY = 32: MD = 32 * MT padded rows, TX = 8 column threads, up to 4 columns each
+//   TY = 16: MD = 16 * MT padded rows, TX = 16 column threads, up to 2 columns each
+// The host picks the layout with fewer padded rows.
 
 // ---- trajectory phases ----
 enum Phase : int {
@@ -87,7 +88,13 @@ struct Params {
     //          [4] timeouts
     int *ctrl;
     long long *work;         // [0] trajectory-matvecs executed
+    // optional per-CTA trace, accumulated over micro-steps: [grid][kTraceFields] clock64 cycles
+    // and counts (null: tracing off)
+    long long *trace;
 };
+// trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
+// sub-tiles, 8-column blocks, columns
+constexpr int kTraceFields = 8;
 
 // ---------------------------------------------------------------- Philox4x32-10
 __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
@@ -127,14 +134,25 @@ __device__ __forceinline__ double draw(const Params &P, int tr, TrajState &s, in
 }
 
 // ---------------------------------------------------------------- canonical reductions
-__device__ __forceinline__ double seq_norm(const double2 *x, int d)
+// Lane l holds the literal running sum of the terms with index l, l+32, ... (ascending);
+// the 32 partial sums are combined by an xor butterfly over offsets 16, 8, 4, 2, 1.  IEEE
+// addition is commutative, so every lane ends with the same value, and the CPU oracle
+// reproduces it exactly.
+__device__ __forceinline__ double warp_allsum(double s)
 {
-    double n = 0.0;
-    for (int i = 0; i < d; i++) {
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, off));
+    return s;
+}
+
+__device__ __forceinline__ double warp_norm(const double2 *x, int d, int lane)
+{
+    double s = 0.0;
+    for (int i = lane; i < d; i += 32) {
         const double2 v = x[i];
-        n = __dadd_rn(n, __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y)));
+        s = __dadd_rn(s, __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y)));
     }
-    return n;
+    return warp_allsum(s);
 }
 
 // ---------------------------------------------------------------- TMA bulk copies + mbarriers
@@ -146,6 +164,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p)
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)

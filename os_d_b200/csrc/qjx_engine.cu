@@ -3,6 +3,7 @@
 // C ABI declared in include/qjx_b200.h.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -13,6 +14,8 @@
 
 namespace qjx {
 cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st);
+int pick_layout(int d, int *rows_per_block);
+cudaError_t launch_dmma_peak(double *out, int blocks, int iters, cudaStream_t st);
 size_t step_smem_bytes(int MD);
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st);
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st);
@@ -94,7 +97,8 @@ extern "C" const char *qjx_status_string(qjx_status s)
 extern "C" const char *qjx_last_error(const qjx_engine *h) { return h ? h->err.c_str() : "null handle"; }
 
 // Transposes row-major complex d x d matrices into the device layout mats[g][k][row]
-// (row padded to MD with zeros), so one K-slab is one contiguous TMA bulk copy.
+// (rows padded to MD and k to an even count with zeros), so one K-slab is one contiguous
+// TMA bulk copy and the last k pair of the FP64 MMA multiplies exact zeros.
 static void pack_transposed(const double *M, int d, int MD, double *out)
 {
     for (int i = 0; i < d; i++)
@@ -114,7 +118,7 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
         c.num_robs < 0 || !(c.T > 0.0) || (c.num_robs > 0 && !R))
         return QJX_ERR_INVALID_ARG;
     const int G = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;
-    if (c.d > 32 * kMaxMT || G > kMaxGroups) return QJX_ERR_UNSUPPORTED;
+    if (c.d > kMaxMD || G > kMaxGroups) return QJX_ERR_UNSUPPORTED;
 
     qjx_engine *h = new (std::nothrow) qjx_engine();
     if (!h) return QJX_ERR_OOM;
@@ -136,7 +140,9 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     cudaEventCreate(&h->eb1);
 
     const int d = c.d, n = c.n_traj;
-    const int MD = 32 * ((d + 31) / 32);
+    int rows_per_block = 0;
+    const int MD = pick_layout(d, &rows_per_block);
+    const int kp = (d + 1) & ~1;  // k rows padded to whole pairs for the m8n8k4 MMA
     h->MD = MD;
     Params &P = h->P;
     P.d = d;
@@ -156,8 +162,8 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     P.keep_adr = c.keep_adr;
     P.rec_cap = h->cfg.rec_cap;
 
-    // matrices in the transposed padded layout
-    const size_t per = (size_t)d * MD * 2;
+    // matrices in the transposed padded layout mats[g][k][row], k < kp, row < MD (zero padded)
+    const size_t per = (size_t)kp * MD * 2;
     std::vector<double> host((size_t)G * per, 0.0);
     const size_t dd2 = (size_t)d * d * 2;
     for (int b = 0; b < c.num_branches; b++)
@@ -381,6 +387,9 @@ static qjx_status run_until_idle(qjx_engine *h)
 
     qjx_status rs = QJX_OK;
     int batch = 1;
+    // QJX_TRACE_BUCKETS=<file>: append the bucket sizes seen at every host poll (profiling aid)
+    FILE *bucket_log = nullptr;
+    if (const char *fn = getenv("QJX_TRACE_BUCKETS")) bucket_log = fopen(fn, "a");
     int64_t steps = 0;
     long long work0 = 0;
     cudaMemcpy(&work0, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
@@ -411,6 +420,10 @@ static qjx_status run_until_idle(qjx_engine *h)
         if (rs != QJX_OK) break;
         long long active = 0;
         for (int g = 0; g < P.G; g++) active += h->h_cnt[g];
+        if (bucket_log) {
+            for (int g = 0; g < P.G; g++) fprintf(bucket_log, g ? " %d" : "%d", h->h_cnt[g]);
+            fprintf(bucket_log, "\n");
+        }
         if (active == 0) {
             if (h->h_ctrl[2] > 0) {  // paused on full record buffers: drain and resume
                 rs = drain_records(h);
@@ -429,6 +442,7 @@ static qjx_status run_until_idle(qjx_engine *h)
         }
         batch = std::min(batch * 2, 16);
     }
+    if (bucket_log) fclose(bucket_log);
     cudaEventRecord(h->ev1, h->stream);
     cudaEventSynchronize(h->ev1);
     float ms = 0.f;
@@ -577,9 +591,35 @@ extern "C" qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats)
     return QJX_OK;
 }
 
-extern "C" qjx_status qjx_measure_fp64_peak(int device, double *tflops)
+extern "C" qjx_status qjx_set_trace(qjx_engine *h, int enable)
 {
-    if (!tflops) return QJX_ERR_INVALID_ARG;
+    if (!h) return QJX_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->cfg.device));
+    if (enable && !h->P.trace) {
+        h->P.trace = (long long *)dalloc(h, (size_t)h->grid * kTraceFields * sizeof(long long));
+        if (!h->P.trace) return QJX_ERR_OOM;
+    } else if (enable) {
+        CK(cudaMemset(h->P.trace, 0, (size_t)h->grid * kTraceFields * sizeof(long long)));
+    } else {
+        h->P.trace = nullptr;  // buffer stays owned by the engine until qjx_destroy
+    }
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_get_trace(qjx_engine *h, int64_t *out, int *n_ctas, int *n_fields)
+{
+    if (!h || !n_ctas || !n_fields) return QJX_ERR_INVALID_ARG;
+    *n_ctas = h->grid;
+    *n_fields = kTraceFields;
+    if (!h->P.trace || !out) return h->P.trace ? QJX_OK : QJX_ERR_STATE;
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaMemcpy(out, h->P.trace, (size_t)h->grid * kTraceFields * sizeof(long long), cudaMemcpyDeviceToHost));
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_tflops)
+{
+    if (!ffma_tflops && !dmma_tflops) return QJX_ERR_INVALID_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return QJX_ERR_CUDA;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -589,22 +629,29 @@ extern "C" qjx_status qjx_measure_fp64_peak(int device, double *tflops)
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     const int blocks = sms * 4, iters = 1 << 16;
-    launch_fp64_peak(out, blocks, iters, 0);  // warm-up
-    double best = 0.0;
-    for (int r = 0; r < 5; r++) {
+    double best = 0.0, best_mma = 0.0;
+    for (int r = 0; r < 6; r++) {  // first round of each is a warm-up
         cudaEventRecord(a, 0);
         launch_fp64_peak(out, blocks, iters, 0);
         cudaEventRecord(b, 0);
         cudaEventSynchronize(b);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, a, b);
-        const double fl = 2.0 * 8.0 * (double)iters * blocks * 256.0;
-        best = std::max(best, fl / (ms * 1e-3) / 1e12);
+        const double fl = 2.0 * 8.0 * (double)iters * blocks * 256.0;  // 8 fma chains per thread
+        if (r) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+        cudaEventRecord(a, 0);
+        launch_dmma_peak(out, blocks, iters / 4, 0);
+        cudaEventRecord(b, 0);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        const double fm = 512.0 * 8.0 * (double)(iters / 4) * blocks * 8.0;  // 8 mma chains per warp
+        if (r) best_mma = std::max(best_mma, fm / (ms * 1e-3) / 1e12);
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaFree(out);
     if (cudaGetLastError() != cudaSuccess) return QJX_ERR_CUDA;
-    *tflops = best;
+    if (ffma_tflops) *ffma_tflops = best;
+    if (dmma_tflops) *dmma_tflops = best_mma;
     return QJX_OK;
 }

@@ -97,7 +97,7 @@ __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const doub
                          int lane, int dump, int is_start)
 {
     const int d = P.d;
-    const double nrm = seq_norm(col, d);
+    const double nrm = warp_norm(col, d, lane);
     const double sq = __dsqrt_rn(nrm);
     const double inv = __ddiv_rn(1.0, nrm);
     double2 *hat = slot_ptr(P, s.cur ^ 1, tr);
@@ -110,16 +110,17 @@ __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const doub
         wscr[k] = a;
         if (adr_out) adr_out[k] = a;
     }
-    __syncwarp();
     double mean = 0.0;
-    for (int k = 0; k < d; k++) mean = __dadd_rn(mean, __dmul_rn((double)k, wscr[k]));
+    for (int k = lane; k < d; k += 32) mean = __dadd_rn(mean, __dmul_rn((double)k, wscr[k]));
+    mean = warp_allsum(mean);
     const double ms = is_start ? mean : P.mean_start[tr];
     const double disp = __dmul_rn(__dsub_rn(mean, ms), __dsub_rn(mean, ms));
     double m2 = 0.0;
-    for (int k = 0; k < d; k++) {
+    for (int k = lane; k < d; k += 32) {
         const double dk = __dsub_rn((double)k, mean);
         m2 = __dadd_rn(m2, __dmul_rn(__dmul_rn(dk, dk), wscr[k]));
     }
+    m2 = warp_allsum(m2);
     if (lane == 0) {
         const size_t o = (size_t)dump * P.n + tr;
         if (is_start) P.mean_start[tr] = mean;
@@ -200,7 +201,7 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
 
     switch (s.phase) {
     case PH_STEP: {
-        const double nrm = seq_norm(col, d);
+        const double nrm = warp_norm(col, d, lane);
         if (nrm > 1.0) {  // is_norm_crossed throws (experiment.cpp:1247-1251)
             err = ERR_NORM;
             break;
@@ -249,7 +250,7 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
     } break;
 
     case PH_REC_W: {  // gnorms[i] = norm_square(L_i psi_hat) * g[i]  (experiment.cpp:1301-1322)
-        double w = seq_norm(col, d);
+        double w = warp_norm(col, d, lane);
         w = __dmul_rn(w, P.g[s.sub]);
         if (lane == 0) P.gn[(size_t)tr * P.nd + s.sub] = w;
         s.tmpw = __dadd_rn(s.tmpw, w);
@@ -295,13 +296,12 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
 
     case PH_OBS_E: {  // energy <psi_hat| H + E0 Hd |psi_hat>  (experiment.cpp:1423-1469)
         const double2 *hat = slot_ptr(P, s.cur ^ 1, tr);
-        for (int k = lane; k < d; k += 32) wscr_c[k] = hat[k];
-        __syncwarp();
         double e = 0.0;
-        for (int k = 0; k < d; k++) {
-            const double2 h = wscr_c[k], m = col[k];
+        for (int k = lane; k < d; k += 32) {
+            const double2 h = hat[k], m = col[k];
             e = __dadd_rn(e, __dadd_rn(__dmul_rn(h.x, m.x), __dmul_rn(h.y, m.y)));
         }
+        e = warp_allsum(e);
         if (lane == 0) P.o_energy[(size_t)(P.dump_base + s.di) * P.n + tr] = e;
         __syncwarp();
         if (P.nr > 0) {
@@ -315,15 +315,15 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
 
     case PH_OBS_R: {  // <psi_hat| R |psi_hat>  (experiment.cpp:2037-2068)
         const double2 *hat = slot_ptr(P, s.cur ^ 1, tr);
-        for (int k = lane; k < d; k += 32) wscr_c[k] = hat[k];
-        __syncwarp();
         double rr = 0.0, ri = 0.0;
-        for (int k = 0; k < d; k++) {
-            const double2 h = wscr_c[k], m = col[k];
+        for (int k = lane; k < d; k += 32) {
+            const double2 h = hat[k], m = col[k];
             const double cr = h.x, ci = -h.y;
             rr = __dadd_rn(rr, __dsub_rn(__dmul_rn(cr, m.x), __dmul_rn(ci, m.y)));
             ri = __dadd_rn(ri, __dadd_rn(__dmul_rn(ci, m.x), __dmul_rn(cr, m.y)));
         }
+        rr = warp_allsum(rr);
+        ri = warp_allsum(ri);
         if (lane == 0) P.o_robs[((size_t)(P.dump_base + s.di) * P.n + tr) * P.nr + s.sub] = make_double2(rr, ri);
         __syncwarp();
         if (s.sub + 1 < P.nr) {
@@ -353,24 +353,162 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
     __syncwarp();
 }
 
-// One lock-step micro-step: grouped FP64 GEMM over the buckets of step `s` (persistent
-// CTAs stride over tiles) with the fused epilogue.  MD = 32 * MT padded rows.
-template <int MT>
+// Accumulates M_g * B for one sub-tile of NTE x TX columns (all rows), streaming the
+// propagator in K-slabs through the TMA pipeline, then stages the result in Bt.
+// Per output the k-ascending fma chain of the oracle is kept; within one k the four fmas
+// are issued in two passes (re += Mr xr, im += Mr xi for every output, then re -= Mi xi,
+// im += Mi xr), which leaves each chain's order unchanged.
+__device__ __forceinline__ double neg(double x)
+{
+    return __longlong_as_double(__double_as_longlong(x) ^ (long long)0x8000000000000000ull);
+}
+
+// FP64 tensor-core MMA D = A(8x4) B(4x8) + D.  On sm_100a its accumulation equals the
+// sequential chain fma(a3,b3, fma(a2,b2, fma(a1,b1, fma(a0,b0,c)))) bit for bit (checked on
+// the device against that chain, the reverse chain and a single rounding), which is the
+// oracle's per-output k-ascending order.
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+// Complex sub-tile product on the FP64 tensor core.  Rows are in 8-row blocks (RB of them,
+// MD = 8 RB), columns in 8-column blocks (CB active of 4).  For one pair of complex k the
+// real parts use A = [Mr_k, -Mi_k, Mr_k+1, -Mi_k+1] against B = [xr_k; xi_k; xr_k+1; xi_k+1]
+// and the imaginary parts A = [Mr_k, Mi_k, ...] against B = [xi_k; xr_k; ...]; that is the
+// k-ascending chain re += Mr xr; re -= Mi xi; im += Mr xi; im += Mi xr of the contract.
+// WPC warps share one column block; warp `sub` of them owns row blocks sub, sub + WPC, ...
+template <int NRB, int WPC>
+__device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, double2 *Us, uint64_t *bar,
+                                          int *released, uint32_t &phase, int d, int kp, int RB, int MD,
+                                          int warp, int lane, int tid)
+{
+    const int S16 = MD + 1;
+    const int g = lane >> 2, t = lane & 3;
+    // warp w runs on scheduler w % 4; rotating the row-block index by column block gives
+    // each scheduler the same number of row blocks
+    const int cb = warp / WPC, sub = (warp % WPC + cb * (WPC / 4)) % WPC;
+    const int th = t >> 1, todd = t & 1;
+    const int nslab = (kp + kKB - 1) / kKB;
+    bool ok = true;
+    double re[NRB][2], im[NRB][2];
+#pragma unroll
+    for (int i = 0; i < NRB; i++) re[i][0] = re[i][1] = im[i][0] = im[i][1] = 0.0;
+
+    if (!mbar_wait_bounded(&bar[kStages], (phase >> kStages) & 1u, kWaitLimit)) ok = false;
+    phase ^= 1u << kStages;
+    const double2 *bcol = Bt + (8 * cb + g) * S16;
+    for (int sl = 0; sl < nslab; sl++) {
+        const int q = sl % kStages;
+        if (!mbar_wait_bounded(&bar[q], (phase >> q) & 1u, kWaitLimit)) ok = false;
+        phase ^= 1u << q;
+        const int k0 = sl * kKB;
+        const int kc = min(kKB, kp - k0);  // even
+        const double *Uq = reinterpret_cast<const double *>(Us + q * kKB * MD);
+#pragma unroll 2
+        for (int kk = 0; kk < kc; kk += 2) {
+            const double2 xb = bcol[k0 + kk + th];
+            const double bre = todd ? xb.y : xb.x;
+            const double bim = todd ? xb.x : xb.y;
+            const double *urow = Uq + 2 * (size_t)(kk + th) * MD + todd;
+#pragma unroll
+            for (int i = 0; i < NRB; i++) {
+                const int rb = sub + WPC * i;
+                if (rb < RB) {
+                    const double v = urow[2 * (8 * rb + g)];
+                    dmma(re[i][0], re[i][1], todd ? neg(v) : v, bre);
+                    dmma(im[i][0], im[i][1], v, bim);
+                }
+            }
+        }
+        // release the stage: the last of the 16 warps to finish it issues the refill, so no
+        // warp waits for another's release (no CTA-wide barrier per slab)
+        __syncwarp();
+        if (lane == 0 && sl + kStages < nslab) {
+            __threadfence_block();
+            if (atomicAdd(&released[q], 1) == kThreads / 32 - 1) {
+                released[q] = 0;
+                const int sn = sl + kStages;
+                const int kn = min(kKB, kp - sn * kKB);
+                fence_proxy_async();
+                mbar_expect_tx(&bar[q], (uint32_t)(kn * MD * 16));
+                bulk_g2s(Us + q * kKB * MD, mat + (size_t)sn * kKB * MD, (uint32_t)(kn * MD * 16), &bar[q]);
+            }
+        }
+    }
+    __syncthreads();
+    // stage: thread (g, t) of row block rb holds rows 8 rb + g, columns 8 cb + 2t, 8 cb + 2t + 1
+#pragma unroll
+    for (int i = 0; i < NRB; i++) {
+        const int rb = sub + WPC * i;
+        const int row = 8 * rb + g;
+        if (rb < RB && row < d) {
+            Bt[(8 * cb + 2 * t) * S16 + row] = make_double2(re[i][0], im[i][0]);
+            Bt[(8 * cb + 2 * t + 1) * S16 + row] = make_double2(re[i][1], im[i][1]);
+        }
+    }
+    return ok;
+}
+
+// Estimated cost of a bucket of m columns cut into sub-tiles the way the kernel cuts them
+// (32-column chunks; a rest of 17..24 columns as 16 + rest), in units of ~5k cycles: 2 per
+// sub-tile (gather, epilogue), 6 per active 8-column block (MMA loop), and 3 more per
+// sub-tile of the jump-operator and observable buckets, whose epilogues renormalise, draw
+// and reduce.
+__device__ __forceinline__ int subtile_cost(int m, bool heavy_epilogue)
+{
+    int c = 0;
+    while (m > 0) {
+        const int s = (m > 24) ? min(m, kNC) : (m > 16 ? 16 : m);
+        const int cb = (s + 7) / 8;
+        c += 2 + 6 * ((cb == 3) ? 4 : cb) + (heavy_epilogue ? 3 : 0);
+        m -= s;
+    }
+    return c;
+}
+
+// Column position of cost offset k (monotone in k).
+__device__ __forceinline__ int cost_to_column(const int *cstart, const int *kc, const int *cnt, int G, long long k)
+{
+    if (k >= kc[G]) return cstart[G];
+    int lo = 0, hi = G;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (kc[mid] <= k) lo = mid;
+        else hi = mid;
+    }
+    const int cost = kc[lo + 1] - kc[lo];
+    if (cost <= 0) return cstart[lo];
+    const long long off = (k - kc[lo]) * (long long)cnt[lo] / cost;
+    const int col = (int)min((long long)cnt[lo], ((off + 4) / 8) * 8);
+    return cstart[lo] + col;
+}
+
+// One lock-step micro-step: grouped complex GEMM over the buckets of step `s` on the FP64
+// tensor core, with the fused epilogue.  The concatenated bucket lists (C columns) are split
+// into equal column ranges, one per persistent CTA; each range is processed as sub-tiles of
+// at most 32 columns of one matrix, and a sub-tile costs in proportion to its active 8-column
+// blocks (1, 2 or 4): the warps are spread over the row blocks of the active column blocks.
+template <int NRB>
 __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s)
 {
-    constexpr int MD = 32 * MT;
-    constexpr int S16 = MD + 1;  // odd column stride: conflict-free column reads
     extern __shared__ __align__(128) unsigned char smem[];
+    const int MD = P.MD;          // 8 * RB padded rows
+    const int RB = MD / 8;
+    const int S16 = MD + 1;       // odd column stride: conflict-free column reads
+    const int kp = (P.d + 1) & ~1;  // k rows padded to pairs (the matrices carry a zero row)
     double2 *Bt = reinterpret_cast<double2 *>(smem);
     double2 *Us = Bt + kNC * S16;
     __shared__ __align__(8) uint64_t bar[kStages + 1];
-    __shared__ int s_tstart[kMaxGroups + 1];
+    __shared__ int released[kStages];
+    __shared__ int s_cstart[kMaxGroups + 1];
+    __shared__ int s_kc[kMaxGroups + 1];
     __shared__ int s_tr[kNC];
     __shared__ long long s_src[kNC];
-    __shared__ int s_abort;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ty = warp * 4 + (lane & 3), tx = lane >> 2;
     const int G = P.G, n = P.n, d = P.d;
     const int *cnt_cur = P.cnt + (s % 3) * G;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
@@ -380,34 +518,47 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
     if (blockIdx.x == 0)
         for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
     if (tid == 0) {
-        int acc = 0;
+        int acc = 0, kacc = 0;
         for (int g = 0; g < G; g++) {
-            s_tstart[g] = acc;
-            acc += (cnt_cur[g] + kNC - 1) / kNC;
+            s_cstart[g] = acc;
+            s_kc[g] = kacc;
+            acc += cnt_cur[g];
+            kacc += subtile_cost(cnt_cur[g], g >= P.gL0);
         }
-        s_tstart[G] = acc;
+        s_cstart[G] = acc;
+        s_kc[G] = kacc;
         for (int q = 0; q <= kStages; q++) mbar_init(&bar[q], 1);
-        s_abort = 0;
+        for (int q = 0; q < kStages; q++) released[q] = 0;
     }
     __syncthreads();
-    const int total = s_tstart[G];
-    const int nslab = (d + kKB - 1) / kKB;
+    // equal shares of the estimated cost, mapped back to column positions (8-column aligned
+    // inside each bucket): buckets that split into many narrow sub-tiles get shorter ranges
+    const long long K = s_kc[G];
+    const int c_lo = cost_to_column(s_cstart, s_kc, cnt_cur, G, K * blockIdx.x / gridDim.x);
+    const int c_hi = cost_to_column(s_cstart, s_kc, cnt_cur, G, K * (blockIdx.x + 1) / gridDim.x);
+    const int nslab = (kp + kKB - 1) / kKB;
     uint32_t phase = 0;
     long long work = 0;
+    long long tr_setup = 0, tr_loop = 0, tr_epi = 0, tr_sub = 0, tr_cb = 0;
+    const long long t_begin = clock64();
 
-    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+    for (int pos = c_lo; pos < c_hi;) {
+        const long long t0 = clock64();
         int lo = 0, hi = G;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (s_tstart[mid] <= tile) lo = mid;
+            if (s_cstart[mid] <= pos) lo = mid;
             else hi = mid;
         }
         const int g = lo;
-        const int col0 = (tile - s_tstart[g]) * kNC;
-        const int ncol = min(kNC, cnt_cur[g] - col0);
+        const int idx = pos - s_cstart[g];
+        // piece of this group left in the range, cut so that no sub-tile has 3 column blocks
+        const int m = min(c_hi - pos, cnt_cur[g] - idx);
+        const int ncol = (m > 24) ? min(m, kNC) : (m > 16 ? 16 : m);
+        const int ncb = (ncol + 7) / 8;
         if (tid < kNC) {
             if (tid < ncol) {
-                const int tr = list_cur[(size_t)g * n + col0 + tid];
+                const int tr = list_cur[(size_t)g * n + idx + tid];
                 const int ph = P.st[tr].phase, cur = P.st[tr].cur;
                 const int slot = (ph >= PH_OBS_E) ? (cur ^ 1) : cur;
                 s_tr[tid] = tr;
@@ -417,107 +568,59 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             }
         }
         __syncthreads();
-        const double2 *mat = P.mats + (size_t)g * d * MD;
+        const double2 *mat = P.mats + (size_t)g * kp * MD;
         if (tid == 0) {
             fence_proxy_async();
-            mbar_expect_tx(&bar[kStages], (uint32_t)(ncol * d * 16));
-            for (int c = 0; c < ncol; c++) bulk_g2s(Bt + c * S16, P.psi + s_src[c], (uint32_t)(d * 16), &bar[kStages]);
+            mbar_expect_tx(&bar[kStages], (uint32_t)(ncol * kp * 16));
+            for (int c = 0; c < ncol; c++) bulk_g2s(Bt + c * S16, P.psi + s_src[c], (uint32_t)(kp * 16), &bar[kStages]);
             for (int q = 0; q < kStages && q < nslab; q++) {
-                const int kc = min(kKB, d - q * kKB);
+                const int kc = min(kKB, kp - q * kKB);
                 mbar_expect_tx(&bar[q], (uint32_t)(kc * MD * 16));
                 bulk_g2s(Us + q * kKB * MD, mat + (size_t)q * kKB * MD, (uint32_t)(kc * MD * 16), &bar[q]);
             }
         }
-
-        double2 acc[MT][kNT];
-#pragma unroll
-        for (int i = 0; i < MT; i++)
-#pragma unroll
-            for (int j = 0; j < kNT; j++) acc[i][j] = make_double2(0.0, 0.0);
-
-        if (!mbar_wait_bounded(&bar[kStages], (phase >> kStages) & 1u, kWaitLimit)) s_abort = 1;
-        phase ^= 1u << kStages;
-
-        for (int sl = 0; sl < nslab; sl++) {
-            const int q = sl % kStages;
-            if (!mbar_wait_bounded(&bar[q], (phase >> q) & 1u, kWaitLimit)) s_abort = 1;
-            phase ^= 1u << q;
-            const int k0 = sl * kKB;
-            const int kc = min(kKB, d - k0);
-            const double2 *Uq = Us + q * kKB * MD;
-            if (kc == kKB) {
-#pragma unroll
-                for (int kk = 0; kk < kKB; kk++) {
-                    double2 a[MT], b[kNT];
-#pragma unroll
-                    for (int i = 0; i < MT; i++) a[i] = Uq[kk * MD + ty + 32 * i];
-#pragma unroll
-                    for (int j = 0; j < kNT; j++) b[j] = Bt[(tx + kTX * j) * S16 + k0 + kk];
-#pragma unroll
-                    for (int i = 0; i < MT; i++)
-#pragma unroll
-                        for (int j = 0; j < kNT; j++) {
-                            acc[i][j].x = __fma_rn(a[i].x, b[j].x, acc[i][j].x);
-                            acc[i][j].x = __fma_rn(-a[i].y, b[j].y, acc[i][j].x);
-                            acc[i][j].y = __fma_rn(a[i].x, b[j].y, acc[i][j].y);
-                            acc[i][j].y = __fma_rn(a[i].y, b[j].x, acc[i][j].y);
-                        }
-                }
-            } else {
-                for (int kk = 0; kk < kc; kk++) {
-                    double2 a[MT], b[kNT];
-#pragma unroll
-                    for (int i = 0; i < MT; i++) a[i] = Uq[kk * MD + ty + 32 * i];
-#pragma unroll
-                    for (int j = 0; j < kNT; j++) b[j] = Bt[(tx + kTX * j) * S16 + k0 + kk];
-#pragma unroll
-                    for (int i = 0; i < MT; i++)
-#pragma unroll
-                        for (int j = 0; j < kNT; j++) {
-                            acc[i][j].x = __fma_rn(a[i].x, b[j].x, acc[i][j].x);
-                            acc[i][j].x = __fma_rn(-a[i].y, b[j].y, acc[i][j].x);
-                            acc[i][j].y = __fma_rn(a[i].x, b[j].y, acc[i][j].y);
-                            acc[i][j].y = __fma_rn(a[i].y, b[j].x, acc[i][j].y);
-                        }
-                }
-            }
-            __syncthreads();
-            if (s_abort) break;
-            if (tid == 0 && sl + kStages < nslab) {
-                const int sn = sl + kStages;
-                const int kn = min(kKB, d - sn * kKB);
-                fence_proxy_async();
-                mbar_expect_tx(&bar[q], (uint32_t)(kn * MD * 16));
-                bulk_g2s(Us + q * kKB * MD, mat + (size_t)sn * kKB * MD, (uint32_t)(kn * MD * 16), &bar[q]);
-            }
-        }
-        __syncthreads();
-        if (s_abort) {
+        const long long t1 = clock64();
+        bool ok;
+        if (ncb == 1)
+            ok = tile_dmma<(NRB + 3) / 4, 16>(mat, Bt, Us, bar, released, phase, d, kp, RB, MD, warp, lane, tid);
+        else if (ncb == 2)
+            ok = tile_dmma<(NRB + 1) / 2, 8>(mat, Bt, Us, bar, released, phase, d, kp, RB, MD, warp, lane, tid);
+        else
+            ok = tile_dmma<NRB, 4>(mat, Bt, Us, bar, released, phase, d, kp, RB, MD, warp, lane, tid);
+        if (!__syncthreads_and(ok ? 1 : 0)) {  // a bounded wait gave up: report and stop
             if (tid == 0) {
                 atomicAdd(&P.ctrl[4], 1);
                 report_error(P, -1, ERR_TIMEOUT);
             }
             return;
         }
-
-        // stage M_g * psi for the column-wise epilogue
-#pragma unroll
-        for (int i = 0; i < MT; i++) {
-            const int row = ty + 32 * i;
-            if (row < d) {
-#pragma unroll
-                for (int j = 0; j < kNT; j++) Bt[(tx + kTX * j) * S16 + row] = acc[i][j];
-            }
-        }
-        __syncthreads();
+        const long long t2 = clock64();
         double2 *wscr = Us + warp * MD;
         for (int c = warp; c < ncol; c += kThreads / 32)
             column_epilogue(P, Bt + c * S16, wscr, s_tr[c], cnt_next, list_next, lane);
         work += ncol;
+        pos += ncol;
         fence_proxy_async();
         __syncthreads();
+        const long long t3 = clock64();
+        tr_setup += t1 - t0;
+        tr_loop += t2 - t1;
+        tr_epi += t3 - t2;
+        tr_sub += 1;
+        tr_cb += (ncb == 3) ? 4 : ncb;
     }
     if (tid == 0 && work) atomicAdd((unsigned long long *)P.work, (unsigned long long)work);
+    if (P.trace && tid == 0) {
+        long long *t = P.trace + (size_t)blockIdx.x * kTraceFields;
+        t[0] += clock64() - t_begin;
+        t[1] += tr_setup;
+        t[2] += 0;
+        t[3] += tr_loop;
+        t[4] += tr_epi;
+        t[5] += tr_sub;
+        t[6] += tr_cb;
+        t[7] += work;
+    }
 }
 
 // Bucket trajectories for step 0 of a call.  mode 0: start of a run of P.target periods;
@@ -626,32 +729,39 @@ __global__ void clear_records_kernel(const Params P)
 }
 
 // ---------------------------------------------------------------- host-side launchers
-template <int MT>
-static cudaError_t launch_step_mt(const Params &P, int s, int grid, cudaStream_t st)
+template <int NRB>
+static cudaError_t launch_step_t(const Params &P, int s, int grid, cudaStream_t st)
 {
-    constexpr int MD = 32 * MT;
-    const size_t smem = (size_t)(kNC * (MD + 1) + kStages * kKB * MD) * sizeof(double2);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(step_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = (size_t)(kNC * (P.MD + 1) + kStages * kKB * P.MD) * sizeof(double2);
+    static int attr_bytes = 0;
+    if (attr_bytes < (int)smem) {
+        cudaError_t e = cudaFuncSetAttribute(step_kernel<NRB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_bytes = (int)smem;
     }
-    step_kernel<MT><<<grid, kThreads, smem, st>>>(P, s);
+    step_kernel<NRB><<<grid, kThreads, smem, st>>>(P, s);
     return cudaGetLastError();
+}
+
+// Padded rows for dimension d: whole 8-row blocks (the m8n8k4 row block).
+int pick_layout(int d, int *rows_per_block)
+{
+    *rows_per_block = 8;
+    return 8 * ((d + 7) / 8);
 }
 
 cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st)
 {
-    switch (P.MD / 32) {
-    case 1: return launch_step_mt<1>(P, s, grid, st);
-    case 2: return launch_step_mt<2>(P, s, grid, st);
-    case 3: return launch_step_mt<3>(P, s, grid, st);
-    case 4: return launch_step_mt<4>(P, s, grid, st);
-    case 5: return launch_step_mt<5>(P, s, grid, st);
-    case 6: return launch_step_mt<6>(P, s, grid, st);
-    case 7: return launch_step_mt<7>(P, s, grid, st);
-    case 8: return launch_step_mt<8>(P, s, grid, st);
+    const int RB = P.MD / 8;
+    switch ((RB + 3) / 4) {  // row blocks per warp with 4 warps per column block
+    case 1: return launch_step_t<1>(P, s, grid, st);
+    case 2: return launch_step_t<2>(P, s, grid, st);
+    case 3: return launch_step_t<3>(P, s, grid, st);
+    case 4: return launch_step_t<4>(P, s, grid, st);
+    case 5: return launch_step_t<5>(P, s, grid, st);
+    case 6: return launch_step_t<6>(P, s, grid, st);
+    case 7: return launch_step_t<7>(P, s, grid, st);
+    case 8: return launch_step_t<8>(P, s, grid, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -670,7 +780,7 @@ cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(observe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(8 * 2 * 32 * kMaxMT * sizeof(double2)));
+                                             (int)(8 * 2 * kMaxMD * sizeof(double2)));
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
@@ -710,6 +820,28 @@ __global__ void fp64_peak_kernel(double *out, int iters, double a, double b)
 #pragma unroll
     for (int i = 0; i < 8; i++) s += x[i];
     if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
+// FP64 tensor-core throughput microbenchmark: 8 independent m8n8k4 accumulator chains per warp.
+__global__ void dmma_peak_kernel(double *out, int iters, double a, double b)
+{
+    double c[8][2];
+#pragma unroll
+    for (int i = 0; i < 8; i++) c[i][0] = c[i][1] = threadIdx.x * 1e-9 + i;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) dmma(c[i][0], c[i][1], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += c[i][0] + c[i][1];
+    if (s == 12345.678) out[0] = s;
+}
+
+cudaError_t launch_dmma_peak(double *out, int blocks, int iters, cudaStream_t st)
+{
+    dmma_peak_kernel<<<blocks, 256, 0, st>>>(out, iters, 1e-3, 1e-3);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st)

@@ -111,6 +111,19 @@ class Engine:
                   "qjx_get_jumps")
         return times, types, norms, etas
 
+    def set_trace(self, enable=True):
+        self._chk(N.lib().qjx_set_trace(self.h, int(enable)), "qjx_set_trace")
+
+    def trace(self):
+        """Per-CTA accumulated trace: columns total, setup, reserved, loop, epilogue cycles,
+        sub-tiles, 8-column blocks, columns."""
+        nc, nf = C.c_int(), C.c_int()
+        self._chk(N.lib().qjx_get_trace(self.h, None, C.byref(nc), C.byref(nf)), "qjx_get_trace")
+        out = np.zeros((nc.value, nf.value), np.int64)
+        self._chk(N.lib().qjx_get_trace(self.h, out.ctypes.data_as(N.c_i64_p), C.byref(nc), C.byref(nf)),
+                  "qjx_get_trace")
+        return out
+
     def stats(self):
         s = N.QjxStats()
         self._chk(N.lib().qjx_get_stats(self.h, C.byref(s)), "qjx_get_stats")
