@@ -128,11 +128,19 @@ qjx_status qjx_get_trace(qjx_engine *h, int64_t *out, int *n_ctas, int *n_fields
  * the roofline peak of the FP64 contraction.  Either pointer may be NULL. */
 qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_tflops);
 
-/* Dimer model on the host (FP64): H, Hd, L [d][d]; Utree [2][deep][d][d] (any may be NULL). */
+/* Dimer model on the host (FP64): H, Hd, L [d][d]; K [2][d][d] = hamiltonians_qj
+ * -i (H - i/2 (g/N) L^H L + (E +- A) Hd); Utree [2][deep][d][d] = exp(K_b T 2^-(l+2)),
+ * T = 2 pi / omega.  Any output may be NULL. */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
-                           double *H, double *Hd, double *L, double *Utree);
+                           double *H, double *Hd, double *L, double *K, double *Utree);
 /* exp(A) of a complex n x n matrix, Higham (2005) scaling and squaring. */
 qjx_status qjx_expm(int n, const double *A, double *out);
+/* Random observables of init_random_obs (source/cpp/QJX/QJX/newdel.cpp:3652-3750): for
+ * o < num, Gaussians from an MCG31m1 leapfrog stream (seed 3873247, index seed + o, stride
+ * mns) with Box-Muller, X = (G_re + i G_im) / 2, R = X X^H divided by its trace (type 1) or
+ * trace / d (type 2).  out: [num][d][d] complex.  The generator restates MKL's published
+ * MCG31m1 / Box-Muller definitions; MKL itself is not available to confirm the stream. */
+qjx_status qjx_random_observables(int d, int num, int seed, int mns, int type, double *out);
 
 /* ---- f-basis Lindblad RK4 (density-matrix oracle of the ensemble) ---- */
 typedef struct qjx_fb qjx_fb;

@@ -20,7 +20,8 @@ EXPORTS = [
     "qjx_create", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
-    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
+    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
+    "qjx_random_observables", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
 
@@ -76,8 +77,9 @@ def lib():
         L.qjx_set_trace.argtypes = [vp, C.c_int]
         L.qjx_get_trace.argtypes = [vp, c_i64_p, c_int_p, c_int_p]
         L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
-        L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 4
+        L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_random_observables.argtypes = [C.c_int] * 5 + [c_double_p]
         L.qjx_fb_create.argtypes = ([C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_int_p, c_double_p,
                                      c_double_p, c_double_p, C.c_double, C.c_double, C.c_double, C.c_int,
                                      C.c_double, C.c_int, C.c_int, C.POINTER(vp)])
@@ -112,8 +114,17 @@ def build_dimer(N, J, U, E, A, g, omega, deep):
     Hd = np.zeros_like(H)
     Lm = np.zeros_like(H)
     Ut = np.zeros((2, deep, d, d), np.complex128)
-    check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(Lm), dp(Ut)), what="qjx_build_dimer")
+    check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(Lm), None, dp(Ut)),
+          what="qjx_build_dimer")
     return H, Hd, Lm, Ut
+
+
+def dimer_generators(N, J, U, E, A, g):
+    """The two non-Hermitian generators K_b = -i H_eff,b of the split propagators."""
+    d = N + 1
+    K = np.zeros((2, d, d), np.complex128)
+    check(lib().qjx_build_dimer(N, J, U, E, A, g, 1.0, 1, None, None, None, dp(K), None), what="qjx_build_dimer")
+    return K
 
 
 def measure_fp64_peak(device=0):
@@ -121,6 +132,12 @@ def measure_fp64_peak(device=0):
     f, m = C.c_double(), C.c_double()
     check(lib().qjx_measure_fp64_peak(device, C.byref(f), C.byref(m)), what="qjx_measure_fp64_peak")
     return f.value, m.value
+
+
+def random_observables(d, num, seed, mns, rtype):
+    out = np.zeros((num, d, d), np.complex128)
+    check(lib().qjx_random_observables(d, num, seed, mns, rtype, dp(out)), what="qjx_random_observables")
+    return out
 
 
 def expm(A):

@@ -1,0 +1,317 @@
+// qjx_main.cpp -- qjx_b200: process-level drop-in for the reference's qjx executable on the
+// Std task with the QJ propagator (sys_id 0, task_id 1, prop_id 0).
+//
+// Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
+// processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
+// transient periods, take dump 0 (calc_chars_std_start), run the observation periods with
+// observables at every dump, and write the reference's files (core.cpp:918-1084,
+// dump.cpp:3-61, core.cpp:12567-12613) under `path` with the same names and formats.
+// The trajectories run on the GPU through the C ABI of libqjx_b200.so.
+//
+//   qjx_b200 [--config FILE] [--params FILE] [--device N] [--check]
+// --check parses both files, prints the parameter echo and the file-name suffix, and exits
+// without touching a GPU.
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/qjx_b200.h"
+#include "qjx_config.h"
+
+using namespace qjxio;
+
+namespace {
+
+[[noreturn]] void die(const std::string &msg)
+{
+    std::cout << "Error: " << msg << std::endl;
+    std::exit(EXIT_FAILURE);
+}
+
+void check(qjx_status s, qjx_engine *h, const char *what)
+{
+    if (s == QJX_OK) return;
+    std::string m = std::string(what) + " failed: " + qjx_status_string(s);
+    if (h) m += std::string(" (") + qjx_last_error(h) + ")";
+    die(m);
+}
+
+struct Dumps {
+    std::vector<double> norm, mean, disp, m2, energy;  // [dump][tr]
+    std::vector<std::complex<double>> robs;           // [dump][tr][nr]
+};
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    std::string fn_config = "config.txt", fn_params = "params.txt";
+    int device = 0;
+    bool check_only = false;
+    if (const char *e = std::getenv("QJX_DEVICE")) device = std::atoi(e);
+    for (int i = 1; i < argc; i++) {
+        std::string a = argv[i];
+        if (a == "--config" && i + 1 < argc) fn_config = argv[++i];
+        else if (a == "--params" && i + 1 < argc) fn_params = argv[++i];
+        else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
+        else if (a == "--check") check_only = true;
+        else die("unknown argument " + a);
+    }
+
+    RunParam rp;
+    ConfigParam cp;
+    if (!read_config(rp, cp, fn_config)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
+    if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
+    std::cout << params_echo(rp, cp);
+
+    if (rp.sys_id != 0) die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer, sys_id 0)");
+    if (rp.task_id != 1) die("Wrong task_id: " + std::to_string(rp.task_id) + " (this engine runs the Std task, task_id 1)");
+    if (rp.prop_id != 0) die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ propagator, prop_id 0)");
+
+    try {
+        cp.fn_suffix = dimer_suffix(rp, cp, 4);
+    } catch (const std::exception &e) {
+        die(e.what());
+    }
+    if (check_only) {
+        std::cout << "fn_suffix = " << cp.fn_suffix << std::endl;
+        return 0;
+    }
+
+    try {
+        const int N = int(param(cp, "N"));
+        const int d = N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
+        const double J = param(cp, "dimer_prm_J"), U = param(cp, "dimer_prm_U"), E = param(cp, "dimer_prm_E");
+        const double A = param(cp, "dimer_drv_ampl"), omega = param(cp, "dimer_drv_freq");
+        const double g = param(cp, "diss_gamma");
+        const int start_type = int(param(cp, "start_type")), start_state = int(param(cp, "start_state"));
+        const int jump = int(param(cp, "jump"));
+        const int dump_obs = int(param(cp, "dump_obs")), dump_evo_sep = int(param(cp, "dump_evo_sep"));
+        const int dump_evo_avg = int(param(cp, "dump_evo_avg")), dump_adr_sep = int(param(cp, "dump_adr_sep"));
+        const int dump_adr_avg_on = int(param(cp, "dump_adr_avg"));
+        const int dump_phi_on = int(param(cp, "dump_phi")), dump_phi_evo_on = int(param(cp, "dump_phi_evo"));
+        const int jumps_counts_lim = int(param(cp, "jumps_counts"));
+        const int num_robs = int(param(cp, "num_random_obs"));
+        const int robs_seed = int(param_or(cp, "random_obs_seed", 0));
+        if (n < 1 || N < 1) die("num_trajectories and N must be positive");
+        if (start_type == 0 && (start_state < 0 || start_state >= d)) die("start_state out of range");
+        const std::string &sfx = cp.fn_suffix;
+        const std::string path = rp.path;
+        const size_t dd = (size_t)d * d;
+
+        // model (newdel.cpp init_*), debug dumps (debugger.cpp:142-168, qj_proc.cpp:115-119)
+        std::vector<double> H(2 * dd), Hd(2 * dd), L(2 * dd), K(4 * dd), Ut(4 * dd * deep);
+        check(qjx_build_dimer(N, J, U, E, A, g, omega, deep, H.data(), Hd.data(), L.data(), K.data(), Ut.data()),
+              nullptr, "qjx_build_dimer");
+        std::cout << "init_sizes" << std::endl << "init_hamiltonians" << std::endl << "init_dissipators" << std::endl
+                  << "init_hamiltonians_qj" << std::endl;
+        if (rp.is_debug) {
+            save_complex_data(path + "hamiltonian" + sfx, H.data(), dd, 16, false);
+            save_complex_data(path + "dissipator_0" + sfx, L.data(), dd, 16, false);
+            for (int b = 0; b < 2; b++) {
+                save_complex_data(path + "hamiltonians_qj_" + std::to_string(b) + sfx, K.data() + 2 * dd * b, dd, 16, false);
+                save_complex_data(path + "exp_mtx_" + std::to_string(b) + sfx, Ut.data() + 2 * dd * ((size_t)b * deep + deep - 1),
+                                  dd, 16, false);
+            }
+        }
+        std::vector<double> HE(2 * dd);
+        for (size_t e = 0; e < 2 * dd; e++) HE[e] = H[e] + E * Hd[e];
+        const std::vector<double> R =
+            random_observables(d, num_robs, robs_seed, int(param_or(cp, "random_obs_mns", 1000000)),
+                               int(param_or(cp, "random_obs_type", 0)));
+
+        // dump schedule (init_dump_periods)
+        const std::vector<int> dp = dump_periods(int(param(cp, "dump_type")), int(param(cp, "dump_num")), cp.num_obs_periods);
+        if (dp.empty()) die("Wrong dump_type");
+        const int ndt = (int)dp.size();
+        bool increasing = true;
+        for (int i = 1; i < ndt; i++) increasing = increasing && dp[i] > dp[i - 1];
+
+        qjx_config cfg{};
+        cfg.d = d;
+        cfg.n_traj = n;
+        cfg.deep = deep;
+        cfg.num_branches = 2;
+        cfg.num_diss = 1;
+        cfg.num_robs = num_robs;
+        cfg.T = 2.0 * 3.1415926535897932384626433832795 / omega;
+        cfg.record = jump;
+        cfg.rng_kind = int(param_or(cp, "rng_kind", 0));
+        cfg.seed = (uint64_t)(uint32_t)cp.seed;
+        cfg.rec_cap = 1024;
+        cfg.keep_adr = ((dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1) ? 1 : 0;
+        cfg.max_dumps = ndt;
+        cfg.device = device;
+        const double gr[1] = {1.0};  // head->g (core.cpp:9905)
+        qjx_engine *h = nullptr;
+        check(qjx_create(&cfg, Ut.data(), L.data(), gr, HE.data(), num_robs ? R.data() : nullptr, &h), nullptr,
+              "qjx_create");
+
+        // init_data: start states (newdel_exp.cpp:656-679)
+        std::vector<double> psi(2 * (size_t)n * d, 0.0);
+        for (int tr = 0; tr < n; tr++)
+            for (int i = 0; i < d; i++)
+                if (start_type == 0) psi[2 * ((size_t)tr * d + i)] = (i == start_state) ? 1.0 : 0.0;
+                else psi[2 * ((size_t)tr * d + i)] = std::sqrt(1.0 / double(d));
+        check(qjx_set_states(h, psi.data()), h, "qjx_set_states");
+        std::cout << "init_data" << std::endl;
+
+        // trans_process (experiment.cpp:411-446)
+        check(qjx_init_thresholds(h), h, "qjx_init_thresholds");
+        check(qjx_run_periods(h, cp.num_tp_periods, 0, nullptr, 0, 0), h, "qjx_run_periods");
+        check(qjx_reset_times(h), h, "qjx_reset_times");
+        check(qjx_observe(h, 0, 1), h, "qjx_observe");
+
+        auto get_adr = [&](int dump) {
+            std::vector<double> adr((size_t)n * d);
+            if (cfg.keep_adr) check(qjx_get_observables(h, dump, 1, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                        adr.data()), h, "qjx_get_observables");
+            else check(qjx_get_observables(h, 0, 1, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, adr.data()),
+                       h, "qjx_get_observables");
+            return adr;
+        };
+        auto write_adr_single = [&](int dump, bool append) {  // dump_adr_single (dump.cpp:3-24)
+            if (!(dump_evo_sep == 1 && dump_adr_sep == 1)) return;
+            const std::vector<double> adr = get_adr(dump);
+            for (int tr = 0; tr < n; tr++)
+                save_double_data(path + "adr_" + std::to_string(tr) + sfx, adr.data() + (size_t)tr * d, d, 16, append);
+        };
+        auto write_adr_avg = [&](int dump, bool append) {  // dump_adr_avg (dump.cpp:26-61)
+            if (dump_adr_avg_on != 1) return;
+            const std::vector<double> adr = get_adr(dump);
+            std::vector<double> avg(d, 0.0);
+            for (int tr = 0; tr < n; tr++)
+                for (int st = 0; st < d; st++) avg[st] += adr[(size_t)tr * d + st] / double(n);
+            save_double_data(path + "adr_avg" + sfx, avg.data(), d, 16, append);
+        };
+        auto write_phi = [&](const std::string &prefix, bool append) {  // dump_phi / dump_phi_evo
+            check(qjx_get_states(h, psi.data(), nullptr, nullptr, nullptr), h, "qjx_get_states");
+            for (int tr = 0; tr < n; tr++)
+                save_complex_data(path + prefix + std::to_string(tr) + sfx, psi.data() + 2 * (size_t)tr * d, d, 16, append);
+        };
+        write_adr_single(0, false);
+        if (dump_evo_avg == 1) write_adr_avg(0, false);
+
+        // obser_process (experiment.cpp:448-542)
+        if (dump_phi_evo_on == 1) write_phi("phi_evo_", false);
+        int last_dump = 0;
+        const bool per_interval = jumps_counts_lim > 0 || !increasing || dump_phi_evo_on == 1 ||
+                                  (dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1 || rp.is_pp == 1;
+        if (!per_interval) {
+            // one call: every trajectory runs all observation periods, observables at each dump
+            std::vector<int> at(dp.begin() + 1, dp.end());
+            if (ndt > 1) check(qjx_run_periods(h, dp[ndt - 1], 1, at.data(), ndt - 1, 1), h, "qjx_run_periods");
+            last_dump = ndt - 1;
+        } else {
+            std::vector<int> jc(n);
+            bool finished = false;
+            for (int dump_id = 1; dump_id < ndt && !finished; dump_id++) {
+                if (rp.is_pp == 1) std::cout << "dump_id: " << dump_id << std::endl;
+                const int span = dp[dump_id] - dp[dump_id - 1];
+                if (jumps_counts_lim > 0) {
+                    for (int p = 0; p < span; p++) {
+                        check(qjx_run_periods(h, 1, 1, nullptr, 0, 0), h, "qjx_run_periods");
+                        check(qjx_get_states(h, nullptr, nullptr, nullptr, jc.data()), h, "qjx_get_states");
+                        bool all = true;
+                        for (int tr = 0; tr < n; tr++) all = all && jc[tr] >= jumps_counts_lim;
+                        if (all) {
+                            finished = true;
+                            break;
+                        }
+                    }
+                    check(qjx_observe(h, dump_id, 0), h, "qjx_observe");
+                } else if (span > 0) {
+                    const int at = span;
+                    check(qjx_run_periods(h, span, 1, &at, 1, dump_id), h, "qjx_run_periods");
+                } else {
+                    check(qjx_observe(h, dump_id, 0), h, "qjx_observe");
+                }
+                last_dump = dump_id;
+                write_adr_single(dump_id, true);
+                if (dump_phi_evo_on == 1) write_phi("phi_evo_", true);
+                if (dump_evo_avg == 1) write_adr_avg(dump_id, true);
+            }
+        }
+        const int nrec = last_dump + 1;
+
+        // collect observables of the recorded dumps
+        Dumps D;
+        const size_t nd_ = (size_t)nrec * n;
+        D.norm.assign(nd_, 0.0);
+        D.mean.assign(nd_, 0.0);
+        D.disp.assign(nd_, 0.0);
+        D.m2.assign(nd_, 0.0);
+        D.energy.assign(nd_, 0.0);
+        D.robs.assign(nd_ * (num_robs ? num_robs : 1), 0.0);
+        check(qjx_get_observables(h, 0, nrec, D.norm.data(), D.mean.data(), D.disp.data(), D.m2.data(), D.energy.data(),
+                                  num_robs ? reinterpret_cast<double *>(D.robs.data()) : nullptr, nullptr),
+              h, "qjx_get_observables");
+        std::vector<double> mean_start(n);
+        check(qjx_get_mean_start(h, mean_start.data()), h, "qjx_get_mean_start");
+
+        // dump_std (core.cpp:918-957): values of the last dump
+        if (dump_obs == 1) {
+            const size_t o = (size_t)last_dump * n;
+            save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
+            save_double_data(path + "mean_start" + sfx, mean_start.data(), n, 16, false);
+            save_double_data(path + "mean" + sfx, D.mean.data() + o, n, 16, false);
+            save_double_data(path + "dispersion" + sfx, D.disp.data() + o, n, 16, false);
+            save_double_data(path + "m2" + sfx, D.m2.data() + o, n, 16, false);
+            save_double_data(path + "energy" + sfx, D.energy.data() + o, n, 16, false);
+        }
+        if (dump_phi_on == 1) write_phi("phi_", false);
+        if (dump_phi_evo_on == 1) write_phi("phi_evo_", true);
+
+        // dump_std_evo (core.cpp:1008-1084): rows = dumps, columns = trajectories
+        if (dump_evo_sep == 1 && dump_obs == 1) {
+            save_int_data(path + "periods" + sfx, dp.data(), ndt, false);
+            std::vector<double> inv((size_t)ndt * n, 0.0);  // [tr][dump] like ed->*_evo
+            auto evo = [&](const std::vector<double> &v, const char *name) {
+                for (int dmp = 0; dmp < nrec; dmp++)
+                    for (int tr = 0; tr < n; tr++) inv[(size_t)tr * ndt + dmp] = v[(size_t)dmp * n + tr];
+                save_2d_inv_double_data(path + name + sfx, inv.data(), ndt, n, 16, false);
+            };
+            evo(D.norm, "norm_evo");
+            evo(D.mean, "mean_evo");
+            evo(D.disp, "dispersion_evo");
+            evo(D.m2, "m2_evo");
+            evo(D.energy, "energy_evo");
+            for (int o = 0; o < num_robs; o++) {
+                std::vector<std::vector<std::complex<double>>> v(n, std::vector<std::complex<double>>(nrec));
+                for (int tr = 0; tr < n; tr++)
+                    for (int dmp = 0; dmp < nrec; dmp++) v[tr][dmp] = D.robs[((size_t)dmp * n + tr) * num_robs + o];
+                save_2d_complex_vector(path + "random_obs_evo_" + std::to_string(robs_seed + o) + sfx, v, 16);
+            }
+            if (jump > 0) {
+                for (int tr = 0; tr < n; tr++) {
+                    int64_t k = 0;
+                    check(qjx_jump_count(h, tr, &k), h, "qjx_jump_count");
+                    std::vector<double> t(k), nr(k), et(k);
+                    std::vector<int> ty(k);
+                    check(qjx_get_jumps(h, tr, t.data(), ty.data(), nr.data(), et.data()), h, "qjx_get_jumps");
+                    save_double_vector(path + "jump_times_" + std::to_string(tr) + sfx, t, 16, false);
+                    save_int_vector(path + "diss_types_" + std::to_string(tr) + sfx, ty, false);
+                    if (jump > 1) {
+                        save_double_vector(path + "jump_norms_" + std::to_string(tr) + sfx, nr, 16, false);
+                        save_double_vector(path + "jump_etas_" + std::to_string(tr) + sfx, et, 16, false);
+                    }
+                }
+            }
+        }
+        if (dump_evo_avg == 0) write_adr_avg(last_dump, false);
+
+        qjx_stats st{};
+        qjx_get_stats(h, &st);
+        std::cout << "micro-steps: " << st.micro_steps << ", matvecs: " << st.matvecs
+                  << ", device time (ms): " << st.kernel_ms << std::endl;
+        qjx_destroy(h);
+    } catch (const std::exception &e) {
+        die(e.what());
+    }
+    return 0;
+}

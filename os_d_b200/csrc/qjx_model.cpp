@@ -199,7 +199,7 @@ extern "C" qjx_status qjx_expm(int n, const double *A, double *out)
 }
 
 extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega,
-                                      int deep, double *H, double *Hd, double *L, double *Utree)
+                                      int deep, double *H, double *Hd, double *L, double *Kout, double *Utree)
 {
     if (N < 1 || deep < 1 || !(omega > 0.0)) return QJX_ERR_INVALID_ARG;
     const int d = N + 1;
@@ -223,7 +223,7 @@ extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, doubl
     if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
     if (Hd) std::memcpy(Hd, hd.data(), e2 * sizeof(double));
     if (L) std::memcpy(L, l.data(), e2 * sizeof(double));
-    if (!Utree) return QJX_OK;
+    if (!Utree && !Kout) return QJX_OK;
 
     // gamma L^H L (real L), H_eff = H - i/2 gamma L^H L, K_b = -i (H_eff + E_b H_drv)
     const double gamma = g / double(d - 1);
@@ -246,6 +246,11 @@ extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, doubl
                 K[b][2 * idx + 1] = 0.0 - (hr + Eb[b] * hd[2 * idx]);
             }
         }
+    if (Kout) {
+        std::memcpy(Kout, K[0].data(), e2 * sizeof(double));
+        std::memcpy(Kout + e2, K[1].data(), e2 * sizeof(double));
+    }
+    if (!Utree) return QJX_OK;
     const double T = 2.0 * 3.1415926535897932384626433832795 / omega;
     std::vector<double> dts(deep);
     double dt = T * 0.5;

@@ -1,0 +1,196 @@
+"""Expected output files of the drop-in executable, computed with the CPU oracle.
+
+Replays the reference's Std task with the QJ propagator (source/cpp/QJX/QJX/experiment.cpp:
+411-542, core.cpp:918-1084, dump.cpp:3-61, core.cpp:12567-12613) on the oracle and renders
+every file with the reference's formats (source/cpp/QJX/QJX/utils.cpp, utils.h).
+"""
+import os
+
+import numpy as np
+
+from oracle import oracle_py as O
+
+TWO_PI = 2.0 * 3.1415926535897932384626433832795
+
+
+def write_files(d, files):
+    for name, text in files.items():
+        with open(os.path.join(d, name), "w") as f:
+            f.write(text)
+
+
+def config_text(cfg):
+    return "".join(f"{k} {v}\n" for k, v in cfg.items())
+
+
+def params_text(prm):
+    return "".join(f"{k} {v}\n" for k, v in prm.items())
+
+
+def fmt_double(x):
+    return "%.16e" % x
+
+
+def f_double_data(v):
+    return "".join(fmt_double(x) + "\n" for x in v)
+
+
+def f_int_data(v):
+    return "".join("%d\n" % x for x in v)
+
+
+def f_complex_data(v):
+    return "".join(fmt_double(z.real) + " " + fmt_double(z.imag) + "\n" for z in v)
+
+
+def f_2d_inv(rows_by_cols):  # array [rows][cols]
+    return "".join("".join(fmt_double(x) + " " for x in row) + "\n" for row in rows_by_cols)
+
+
+def f_2d_complex(rows_by_cols):
+    return "".join("\t".join("(%s,%s)" % (fmt_double(z.real), fmt_double(z.imag)) for z in row) + "\n"
+                   for row in rows_by_cols)
+
+
+def suffix(cfg, prm):
+    """DimerOutputBehavior::suffix_param with precision 4 (outputter.cpp:3-44, 353-388)."""
+    f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    return ("_setup(%d_%d_%d)" % (cfg.get("sys_id", 0), cfg.get("task_id", 0), cfg.get("prop_id", 0))
+            + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+            + "_N(%d)" % int(prm["N"])
+            + "_diss(%d_%s_%s)" % (int(prm["diss_type"]), f4(prm["diss_gamma"]), f4(prm["diss_phase"]))
+            + "_drv(%d_%s_%s_%s)" % (int(prm["dimer_drv_type"]), f4(prm["dimer_drv_ampl"]),
+                                     f4(prm["dimer_drv_freq"]), f4(prm["dimer_drv_phase"]))
+            + "_prm(%s_%s_%s)" % (f4(prm["dimer_prm_E"]), f4(prm["dimer_prm_U"]), f4(prm["dimer_prm_J"]))
+            + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"])) + ".txt")
+
+
+def expected_outputs(cfg, prm, R=None):
+    """All files the drop-in writes, as {relative file name: text}."""
+    N = int(prm["N"])
+    d = N + 1
+    n = cfg["num_trajectories"]
+    deep = cfg.get("ex_deep", 16)
+    seed = cfg.get("seed", 0)
+    path = cfg.get("path", "")
+    sfx = suffix(cfg, prm)
+    H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
+                                         prm["dimer_drv_ampl"], prm["diss_gamma"])
+    T = TWO_PI / prm["dimer_drv_freq"]
+    U = np.stack([O.split_tree(K0, T, deep), O.split_tree(K1, T, deep)])
+    HE = H + prm["dimer_prm_E"] * Hd
+    nr = int(prm["num_random_obs"])
+    ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
+    ens.init(int(prm["start_type"]), int(prm["start_state"]))
+    files = {}
+    if cfg.get("is_debug", 0):
+        files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
+        files[path + "dissipator_0" + sfx] = f_complex_data(L.reshape(-1))
+        files[path + "hamiltonians_qj_0" + sfx] = f_complex_data(K0.reshape(-1))
+        files[path + "hamiltonians_qj_1" + sfx] = f_complex_data(K1.reshape(-1))
+        files[path + "exp_mtx_0" + sfx] = f_complex_data(U[0, -1].reshape(-1))
+        files[path + "exp_mtx_1" + sfx] = f_complex_data(U[1, -1].reshape(-1))
+    dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
+    ndt = len(dp)
+    assert ens.run_periods(cfg.get("num_tp_periods", 0), is_obs=0) == 0
+    ens.t[:] = 0.0
+    obs = [ens.observables(is_start=True, want_adr=True)]
+    evo_sep, adr_sep = int(prm["dump_evo_sep"]), int(prm["dump_adr_sep"])
+    evo_avg, adr_avg_on = int(prm["dump_evo_avg"]), int(prm["dump_adr_avg"])
+    phi_evo_on, phi_on = int(prm["dump_phi_evo"]), int(prm["dump_phi"])
+    lim = int(prm["jumps_counts"])
+
+    def adr_avg(adr):
+        avg = np.zeros(d)
+        for tr in range(n):
+            avg += adr[tr] / float(n)
+        return avg
+
+    acc = {}
+
+    def emit(name, text, append):
+        key = path + name
+        acc[key] = (acc.get(key, "") if append else "") + text
+
+    if evo_sep == 1 and adr_sep == 1:
+        for tr in range(n):
+            emit("adr_%d" % tr + sfx, f_double_data(obs[0]["adr"][tr]), False)
+    if evo_avg == 1 and adr_avg_on == 1:
+        emit("adr_avg" + sfx, f_double_data(adr_avg(obs[0]["adr"])), False)
+    if phi_evo_on == 1:
+        for tr in range(n):
+            emit("phi_evo_%d" % tr + sfx, f_complex_data(ens.phi[tr]), False)
+    finished = False
+    for dump_id in range(1, ndt):
+        span = dp[dump_id] - dp[dump_id - 1]
+        if lim > 0:
+            for _ in range(span):
+                assert ens.run_periods(1, is_obs=1) == 0
+                if np.all(ens.jumps_counts >= lim):
+                    finished = True
+                    break
+        elif span > 0:
+            assert ens.run_periods(span, is_obs=1) == 0
+        obs.append(ens.observables(want_adr=True))
+        if evo_sep == 1 and adr_sep == 1:
+            for tr in range(n):
+                emit("adr_%d" % tr + sfx, f_double_data(obs[-1]["adr"][tr]), True)
+        if phi_evo_on == 1:
+            for tr in range(n):
+                emit("phi_evo_%d" % tr + sfx, f_complex_data(ens.phi[tr]), True)
+        if evo_avg == 1 and adr_avg_on == 1:
+            emit("adr_avg" + sfx, f_double_data(adr_avg(obs[-1]["adr"])), True)
+        if finished:
+            break
+    last = obs[-1]
+    if int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
+        emit("mean" + sfx, f_double_data(last["mean"]), False)
+        emit("dispersion" + sfx, f_double_data(last["dispersion"]), False)
+        emit("m2" + sfx, f_double_data(last["m2"]), False)
+        emit("energy" + sfx, f_double_data(last["energy"]), False)
+    if phi_on == 1:
+        for tr in range(n):
+            emit("phi_%d" % tr + sfx, f_complex_data(ens.phi[tr]), False)
+    if phi_evo_on == 1:
+        for tr in range(n):
+            emit("phi_evo_%d" % tr + sfx, f_complex_data(ens.phi[tr]), True)
+    if evo_sep == 1 and int(prm["dump_obs"]) == 1:
+        emit("periods" + sfx, f_int_data(dp), False)
+        for key, name in (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"),
+                          ("m2", "m2_evo"), ("energy", "energy_evo")):
+            grid = np.zeros((ndt, n))
+            for i, o in enumerate(obs):
+                grid[i] = o[key]
+            emit(name + sfx, f_2d_inv(grid), False)
+        for o_id in range(nr):
+            rows = [o["random_obs"][:, o_id] for o in obs]
+            emit("random_obs_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
+        if int(prm["jump"]) > 0:
+            for tr in range(n):
+                t, ty, nm, et = ens.jumps(tr)
+                emit("jump_times_%d" % tr + sfx, f_double_data(t), False)
+                emit("diss_types_%d" % tr + sfx, f_int_data(ty), False)
+                if int(prm["jump"]) > 1:
+                    emit("jump_norms_%d" % tr + sfx, f_double_data(nm), False)
+                    emit("jump_etas_%d" % tr + sfx, f_double_data(et), False)
+    if evo_avg == 0 and adr_avg_on == 1:
+        emit("adr_avg" + sfx, f_double_data(adr_avg(last["adr"])), False)
+    files.update(acc)
+    return files
+
+
+BASE_PARAMS = {
+    "num_random_obs": 1, "random_obs_seed": 100, "random_obs_mns": 1000000, "random_obs_type": 2,
+    "dump_obs": 1, "dump_phi": 0, "dump_phi_evo": 0, "dump_adr_sep": 0, "dump_adr_avg": 0, "dump_evo_sep": 1,
+    "dump_evo_avg": 0, "dump_type": 0, "dump_num": 3, "N": 16, "diss_type": 0, "diss_gamma": 0.1,
+    "diss_phase": 0.0, "dimer_drv_type": 0, "dimer_drv_ampl": 1.5, "dimer_drv_freq": 1.0, "dimer_drv_phase": 0.0,
+    "dimer_prm_E": 1.0, "dimer_prm_U": 0.5, "dimer_prm_J": 1.0, "start_type": 0, "start_state": 0,
+    "jump": 2, "jumps_counts": 0,
+}
+
+BASE_CONFIG = {
+    "sys_id": 0, "task_id": 1, "prop_id": 0, "is_debug": 0, "is_pp": 0, "seed": 3, "mns": 1000000,
+    "num_threads": 4, "num_trajectories": 12, "num_tp_periods": 2, "num_obs_periods": 6, "ex_deep": 16, "rk_ns": 100,
+}

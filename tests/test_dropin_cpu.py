@@ -1,0 +1,64 @@
+"""Parameter files, file-name suffix and error exits of the drop-in executable (no GPU)."""
+import os
+import subprocess
+
+import pytest
+
+import os_d_b200 as q
+from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, config_text, params_text, suffix
+
+EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
+
+
+def check(tmp_path, cfg, prm, extra_cfg=""):
+    (tmp_path / "config.txt").write_text(config_text(cfg) + extra_cfg)
+    (tmp_path / "params.txt").write_text(params_text(prm))
+    return subprocess.run([EXE, "--check"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+
+
+@pytest.mark.parametrize("over", [
+    {},
+    {"N": 500, "diss_gamma": 0.1, "dimer_drv_ampl": 1.55, "dimer_prm_U": 0.37, "dimer_prm_E": 1.0},
+    {"N": 7, "diss_type": 1, "diss_phase": 0.25, "dimer_drv_type": 1, "dimer_drv_freq": 2.5, "dimer_prm_J": -1.25,
+     "start_type": 1, "start_state": 3},
+])
+def test_suffix_matches_reference_rule(tmp_path, over):
+    prm = dict(BASE_PARAMS, **over)
+    r = check(tmp_path, BASE_CONFIG, prm)
+    assert r.returncode == 0, r.stdout
+    line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
+    assert line[len("fn_suffix = "):] == suffix(BASE_CONFIG, prm)
+
+
+def test_config_parsing_rules(tmp_path):
+    # lines with a number of tokens other than two are ignored; last value wins; CR tolerated
+    extra = "seed 11 12\nnum_trajectories 5\r\nmns\nseed 9\n"
+    r = check(tmp_path, BASE_CONFIG, BASE_PARAMS, extra)
+    assert r.returncode == 0
+    assert "seed = 9" in r.stdout and "num_trajectories = 5" in r.stdout and "mns = 1000000" in r.stdout
+    assert "_rnd(9_1000000)" in r.stdout
+
+
+def test_params_echo_format(tmp_path):
+    r = check(tmp_path, BASE_CONFIG, BASE_PARAMS)
+    assert r.stdout.startswith("############# parameters #############\nsys_id = 0\ntask_id = 1\nprop_id = 0\n")
+    assert "diss_gamma: 0.1\n" in r.stdout and "N: 16\n" in r.stdout
+
+
+@pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 7), ("prop_id", 1)])
+def test_unsupported_ids_exit_with_error(tmp_path, key, val):
+    r = check(tmp_path, dict(BASE_CONFIG, **{key: val}), BASE_PARAMS)
+    assert r.returncode != 0 and "Error: Wrong " + key in r.stdout
+
+
+def test_missing_param_is_an_error(tmp_path):
+    prm = dict(BASE_PARAMS)
+    del prm["diss_gamma"]
+    r = check(tmp_path, BASE_CONFIG, prm)
+    assert r.returncode != 0 and "missing key in params file: diss_gamma" in r.stdout
+
+
+def test_missing_files_use_defaults(tmp_path):
+    r = subprocess.run([EXE, "--check"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert "Unable to open file" in r.stdout and "Init with default params" in r.stdout
+    assert r.returncode != 0  # default task_id 0 is not the Std task

@@ -1,0 +1,61 @@
+"""The drop-in executable (os_d_b200/qjx_b200) on a GPU, compared file by file with the
+reference's Std-task outputs computed by the CPU oracle on the same inputs."""
+import copy
+import os
+import subprocess
+
+import pytest
+
+import os_d_b200 as q
+from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, config_text, expected_outputs, params_text
+
+pytestmark = pytest.mark.gpu
+EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
+
+
+def run_case(tmp_path, cfg, prm):
+    (tmp_path / "config.txt").write_text(config_text(cfg))
+    (tmp_path / "params.txt").write_text(params_text(prm))
+    if cfg.get("path"):
+        (tmp_path / cfg["path"]).mkdir(parents=True, exist_ok=True)
+    r = subprocess.run([EXE], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    d = int(prm["N"]) + 1
+    R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
+                             int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
+    exp = expected_outputs(cfg, prm, R)
+    written = set()
+    for root, _, names in os.walk(tmp_path):
+        for nm in names:
+            rel = os.path.relpath(os.path.join(root, nm), tmp_path)
+            if rel not in ("config.txt", "params.txt"):
+                written.add(rel)
+    assert written == set(exp), (sorted(written ^ set(exp)))[:10]
+    for name, text in exp.items():
+        got = (tmp_path / name).read_text()
+        assert got == text, name
+    return exp
+
+
+def test_std_task_files_match(tmp_path):
+    exp = run_case(tmp_path, BASE_CONFIG, BASE_PARAMS)
+    assert any(k.startswith("jump_times_") for k in exp)
+
+
+def test_per_dump_files_log_dumps_and_debug(tmp_path):
+    cfg = dict(BASE_CONFIG, is_debug=1, is_pp=1, num_obs_periods=20, path="out/")
+    prm = dict(BASE_PARAMS, dump_type=1, dump_num=4, dump_phi=1, dump_phi_evo=1, dump_adr_sep=1, dump_adr_avg=1,
+               dump_evo_avg=1, num_random_obs=2, start_type=1)
+    run_case(tmp_path, cfg, prm)
+
+
+def test_early_stop_on_jump_counts(tmp_path):
+    cfg = dict(BASE_CONFIG, num_obs_periods=40, num_trajectories=6)
+    prm = dict(BASE_PARAMS, dump_num=4, jump=1, jumps_counts=5, dump_adr_avg=1, num_random_obs=0)
+    run_case(tmp_path, cfg, prm)
+
+
+def test_dims_101_sample(tmp_path):
+    cfg = dict(BASE_CONFIG, num_trajectories=16, num_tp_periods=1, num_obs_periods=2, seed=42)
+    prm = dict(BASE_PARAMS, N=100, dump_num=2, jump=2)
+    run_case(tmp_path, cfg, prm)
