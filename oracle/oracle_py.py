@@ -192,3 +192,81 @@ class Ensemble:
         k = int(self.n_rec[tr])
         return (self.jump_times[tr, :k].copy(), self.diss_types[tr, :k].copy(),
                 self.jump_norms[tr, :k].copy(), self.jump_etas[tr, :k].copy())
+
+
+# ---------------------------------------------------------------- f-basis
+def _fb_sigs(L):
+    if getattr(L, "_fb_ready", False):
+        return
+    ip = C.POINTER(C.c_int)
+    L.orc_fb_operators.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double] + [c_double_p] * 3
+    L.orc_fb_dense.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 3
+    L.orc_fb_rk4.argtypes = ([C.c_int, ip, ip, c_double_p, ip, ip, c_double_p, c_double_p, C.c_double, C.c_double,
+                              C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, c_double_p])
+    L.orc_fb_rho.argtypes = [C.c_int, c_double_p, c_double_p]
+    L.orc_fb_rho.restype = None
+    L.orc_fb_x_from_rho.argtypes = [C.c_int, c_double_p, c_double_p]
+    L.orc_fb_x_from_rho.restype = None
+    L._fb_ready = True
+
+
+def fb_operators(N, J, U, E):
+    L = lib()
+    _fb_sigs(L)
+    d = N + 1
+    Hb, Hd, Lm = _cplx((d, d)), _cplx((d, d)), _cplx((d, d))
+    L.orc_fb_operators(N, J, U, E, _dp(Hb), _dp(Hd), _dp(Lm))
+    return Hb, Hd, Lm
+
+
+def fb_dense(N, J, U, E, g):
+    """Dense Gs, Qs_drv (n x n) and Ks (n), n = (N+1)^2 - 1."""
+    L = lib()
+    _fb_sigs(L)
+    n = (N + 1) ** 2 - 1
+    Gs, Qs, Ks = np.zeros((n, n)), np.zeros((n, n)), np.zeros(n)
+    assert L.orc_fb_dense(N, J, U, E, g, _dp(Gs), _dp(Qs), _dp(Ks)) == 0
+    return Gs, Qs, Ks
+
+
+def fb_csr(M, rel_tol=1e-14):
+    """CSR (indptr, indices, data) of a dense f-basis matrix; entries below rel_tol * max|M| are
+    structural zeros of the Liouvillian left by rounding in the projection."""
+    import scipy.sparse as sp
+
+    A = np.where(np.abs(M) > rel_tol * np.abs(M).max(), M, 0.0)
+    S = sp.csr_matrix(A)
+    S.sort_indices()
+    return S
+
+
+def fb_rk4(Gs, Qs, Ks, x, A, freq=1.0, phase=0.0, drv_type=0, T=2 * np.pi, num_steps=1000, period0=0, n_periods=1):
+    L = lib()
+    _fb_sigs(L)
+    ip = C.POINTER(C.c_int)
+    g = (np.ascontiguousarray(Gs.indptr, np.int32), np.ascontiguousarray(Gs.indices, np.int32),
+         np.ascontiguousarray(Gs.data, np.float64))
+    q = (np.ascontiguousarray(Qs.indptr, np.int32), np.ascontiguousarray(Qs.indices, np.int32),
+         np.ascontiguousarray(Qs.data, np.float64))
+    x = np.ascontiguousarray(x, np.float64).copy()
+    Ks = np.ascontiguousarray(Ks, np.float64)
+    assert L.orc_fb_rk4(len(x), g[0].ctypes.data_as(ip), g[1].ctypes.data_as(ip), _dp(g[2]), q[0].ctypes.data_as(ip),
+                        q[1].ctypes.data_as(ip), _dp(q[2]), _dp(Ks), A, freq, phase, drv_type, T, num_steps,
+                        period0, n_periods, _dp(x)) == 0
+    return x
+
+
+def fb_rho(N, x):
+    L = lib()
+    _fb_sigs(L)
+    rho = _cplx((N + 1, N + 1))
+    L.orc_fb_rho(N, _dp(np.ascontiguousarray(x, np.float64)), _dp(rho))
+    return rho
+
+
+def fb_x_from_rho(N, rho):
+    L = lib()
+    _fb_sigs(L)
+    x = np.zeros((N + 1) ** 2 - 1)
+    L.orc_fb_x_from_rho(N, _dp(np.ascontiguousarray(rho, np.complex128)), _dp(x))
+    return x

@@ -1,0 +1,138 @@
+"""The SU(N) f-basis Lindblad solver: oracle checks on CPU, GPU RK4 parity, and the QJ
+ensemble against the f-basis density matrix (the density-matrix oracle of the ensemble)."""
+import numpy as np
+import pytest
+
+from oracle import oracle_py as O
+from tests.helpers import T2PI
+
+
+def dense_rk4(Hb, Hdrv, L, gamma, A, rho, T, num_steps, periods, drv_type=0, freq=1.0, phase=0.0):
+    """RK4 of the density matrix with the stage structure of calcODE_trans (calcODE.cpp:278-302)
+    and the drive of calcVectValue_real (E(t) = -A sign(sin) or -A sin)."""
+    LdL = L.conj().T @ L
+    h = T / num_steps
+
+    def f(t, r):
+        s = np.sin(freq * t + phase)
+        e = -A * s if drv_type == 1 else -A * (-1.0 if s < 0.0 else 1.0)
+        Ht = Hb + e * Hdrv
+        return (-1j * (Ht @ r - r @ Ht) + gamma * (L @ r @ L.conj().T - 0.5 * (LdL @ r + r @ LdL))) * h
+
+    for p in range(periods):
+        for s in range(num_steps):
+            t = p * T + s * h
+            k1 = f(t, rho)
+            k2 = f(t + h / 2, rho + k1 / 2)
+            k3 = f(t + h / 2, rho + k2 / 2)
+            k4 = f(t + h, rho + k3)
+            rho = rho + (k1 + 2 * k2 + 2 * k3 + k4) / 6
+    return rho
+
+
+@pytest.mark.parametrize("N,drv_type,start", [(3, 0, "pure"), (5, 1, "mixed"), (6, 0, "pure")])
+def test_fbasis_rk4_equals_dense_density_matrix_rk4(N, drv_type, start):
+    J, U, E, A, g = 1.0, 0.5, 1.0, 1.5, 0.4
+    Gs, Qs, Ks = O.fb_dense(N, J, U, E, g)
+    Hb, Hd, L = O.fb_operators(N, J, U, E)
+    d = N + 1
+    rho0 = np.zeros((d, d), complex)
+    if start == "pure":
+        rho0[0, 0] = 1
+    else:
+        rho0 = np.eye(d) / d
+    x0 = O.fb_x_from_rho(N, rho0)
+    assert np.allclose(O.fb_rho(N, x0), rho0, atol=1e-15)
+    x = O.fb_rk4(O.fb_csr(Gs), O.fb_csr(Qs), Ks, x0, A, drv_type=drv_type, T=T2PI, num_steps=200, n_periods=2)
+    rho = dense_rk4(Hb, Hd, L, g / N, A, rho0, T2PI, 200, 2, drv_type=drv_type)
+    assert np.abs(O.fb_rho(N, x) - rho).max() < 1e-12
+    r = O.fb_rho(N, x)
+    assert abs(np.trace(r).real - 1) < 1e-13 and np.allclose(r, r.conj().T, atol=1e-15)
+
+
+def test_fbasis_operators_match_qjx_operators():
+    N, J, U, E = 9, 1.0, 0.5, 1.3
+    Hb, Hdrv, Lf = O.fb_operators(N, J, U, E)
+    H, Hd, L, K0, K1 = O.dimer_operators(N, J, U, E, 0.0, 0.1)
+    # f-basis Hamiltonian = QJX H + E Hd up to a multiple of the identity; H_drv = -Hd; same L
+    diff = Hb - (H + E * Hd)
+    assert np.allclose(diff - diff[0, 0] * np.eye(N + 1), 0, atol=1e-12)
+    assert np.allclose(Hdrv, -Hd) and np.allclose(Lf, L)
+
+
+def test_liouvillian_structure():
+    Gs, Qs, Ks = O.fb_dense(12, 1.0, 0.5, 1.0, 0.1)
+    S = O.fb_csr(Gs)
+    assert S.nnz < 0.1 * Gs.size  # sparse
+    # the drive commutator only couples the coherences of each pair (i, j): 2 x 2 blocks
+    assert np.abs(np.diag(Qs)).max() == 0.0
+    assert np.count_nonzero(Qs) == 12 * 13
+
+
+def test_qj_ensemble_within_statistical_error_of_fbasis_rho():
+    N, n, periods = 4, 3000, 3
+    J, U, E, A, g = 1.0, 0.5, 1.0, 1.5, 2.0
+    Gs, Qs, Ks = O.fb_dense(N, J, U, E, g)
+    rho0 = np.zeros((N + 1, N + 1), complex)
+    rho0[0, 0] = 1
+    x = O.fb_x_from_rho(N, rho0)
+    H, Hd, L, K0, K1 = O.dimer_operators(N, J, U, E, A, g)
+    Ut = np.stack([O.split_tree(K0, T2PI, 16), O.split_tree(K1, T2PI, 16)])
+    ens = O.Ensemble(Ut, L, [1.0], H + E * Hd, None, T2PI, n, seed=9, record=0)
+    ens.init(0, 0)
+    Gc, Qc = O.fb_csr(Gs), O.fb_csr(Qs)
+    for p in range(periods):
+        x = O.fb_rk4(Gc, Qc, Ks, x, A, T=T2PI, num_steps=2000, period0=p, n_periods=1)
+        assert ens.run_periods(1) == 0
+        pops_f = np.real(np.diag(O.fb_rho(N, x)))
+        adr = ens.observables(want_adr=True)["adr"]
+        err = adr.std(axis=0) / np.sqrt(n)
+        assert np.all(np.abs(adr.mean(axis=0) - pops_f) < 4.5 * err + 2e-3), (adr.mean(axis=0), pops_f)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,drv_type", [(5, 0), (20, 0), (20, 1)])
+def test_gpu_rk4_matches_oracle(N, drv_type):
+    import os_d_b200 as q
+
+    Gs, Qs, Ks = O.fb_dense(N, 1.0, 0.5, 1.0, 0.1)
+    Gc, Qc = O.fb_csr(Gs), O.fb_csr(Qs)
+    rho0 = np.zeros((N + 1, N + 1), complex)
+    rho0[0, 0] = 1
+    x0 = O.fb_x_from_rho(N, rho0)
+    steps, periods = 300, 2
+    x_o = O.fb_rk4(Gc, Qc, Ks, x0, 1.5, drv_type=drv_type, T=T2PI, num_steps=steps, n_periods=periods)
+    fb = q.FBasis(Gc, Qc, Ks, x0, 1.5, drv_type=drv_type, T=T2PI, num_steps=steps)
+    fb.run(0, periods)
+    x_g, _ = fb.get()
+    if drv_type == 0:
+        assert np.array_equal(x_g, x_o)  # sign of sin only: bit-exact
+    else:
+        assert np.abs(x_g - x_o).max() < 1e-12  # CUDA sin vs libm sin
+    fb.close()
+
+
+@pytest.mark.gpu
+def test_gpu_qj_ensemble_within_statistical_error_of_gpu_fbasis():
+    import os_d_b200 as q
+
+    N, n, periods = 12, 6000, 2
+    J, U, E, A, g = 1.0, 0.5, 1.0, 1.5, 1.0
+    Gs, Qs, Ks = O.fb_dense(N, J, U, E, g)
+    rho0 = np.zeros((N + 1, N + 1), complex)
+    rho0[0, 0] = 1
+    fb = q.FBasis(O.fb_csr(Gs), O.fb_csr(Qs), Ks, O.fb_x_from_rho(N, rho0), A, T=T2PI, num_steps=2000)
+    H, Hd, L, Ut = q.build_dimer(N, J, U, E, A, g, 1.0, 16)
+    eng = q.Engine(Ut, L, [1.0], H + E * Hd, None, T2PI, n, seed=21, max_dumps=periods + 1, keep_adr=1)
+    psi0 = np.zeros((n, N + 1), complex)
+    psi0[:, 0] = 1
+    eng.set_states(psi0)
+    eng.init_thresholds()
+    eng.run_periods(periods, dump_at=list(range(1, periods + 1)), dump_base=1)
+    adr = eng.observables(1, periods, want_adr=True)["adr"]
+    for p in range(periods):
+        fb.run(p, 1)
+        x, _ = fb.get()
+        pops_f = np.real(np.diag(O.fb_rho(N, x)))
+        err = adr[p].std(axis=0) / np.sqrt(n)
+        assert np.all(np.abs(adr[p].mean(axis=0) - pops_f) < 4.5 * err + 2e-3)
