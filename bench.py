@@ -307,7 +307,7 @@ def run_ours(args):
                                "qjx_get_states per step"}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample = 2 * threads
+        sample = 8 * threads  # ~10-30 s of CPU work
         rate, dt, mv = cpu_rate(M, sample, 1, threads)
         line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
                                 "sample": f"{sample} trajectories x 1 period at dim 201 ({dt:.1f} s), "

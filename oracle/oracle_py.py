@@ -22,7 +22,7 @@ class OrcProblem(C.Structure):
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("record", C.c_int), ("rng_kind", C.c_int),
                 ("T", C.c_double), ("seed", C.c_uint64),
                 ("U", c_double_p), ("L", c_double_p), ("g", c_double_p), ("HE", c_double_p), ("R", c_double_p),
-                ("inj_u", c_double_p), ("inj_off", c_i64_p)]
+                ("inj_u", c_double_p), ("inj_off", c_i64_p), ("tr_base", C.c_uint64)]
 
 
 class OrcState(C.Structure):
@@ -122,7 +122,7 @@ class Ensemble:
     """One QJ ensemble run by the oracle, mirroring the Std task flow."""
 
     def __init__(self, U, L, g, HE, R, T, n_traj, seed=0, record=2, rng_kind=0, inj_u=None, inj_off=None,
-                 rec_cap=4096):
+                 rec_cap=4096, tr_base=0):
         self.U = np.ascontiguousarray(U, dtype=np.complex128)  # [nb, deep, d, d]
         nb, deep, d, _ = self.U.shape
         self.L = np.ascontiguousarray(L, dtype=np.complex128).reshape(-1, d, d)
@@ -135,7 +135,7 @@ class Ensemble:
         p = OrcProblem()
         p.d, p.n_traj, p.deep, p.num_branches = d, n_traj, deep, nb
         p.num_diss, p.num_robs, p.record, p.rng_kind = self.L.shape[0], self.R.shape[0], record, rng_kind
-        p.T, p.seed = T, seed
+        p.T, p.seed, p.tr_base = T, seed, tr_base
         p.U, p.L, p.g, p.HE = _dp(self.U), _dp(self.L), _dp(self.g), _dp(self.HE)
         p.R = _dp(self.R) if self.R.size else None
         p.inj_u = _dp(self.inj_u)

@@ -480,7 +480,7 @@ static double draw(traj_ctx *c)
 {
     const orc_problem *p = c->p;
     int64_t *pos = &c->s->rng_pos[c->tr];
-    if (p->rng_kind == 0) return orc_philox_uniform(p->seed, (uint64_t)c->tr, (uint64_t)(*pos)++);
+    if (p->rng_kind == 0) return orc_philox_uniform(p->seed, p->tr_base + (uint64_t)c->tr, (uint64_t)(*pos)++);
     const int64_t lo = p->inj_off[c->tr], hi = p->inj_off[c->tr + 1];
     if (lo + *pos >= hi) { c->err = 3; return 0.5; }
     return p->inj_u[lo + (*pos)++];

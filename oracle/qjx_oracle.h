@@ -80,6 +80,7 @@ typedef struct {
     const double *R;    /* [num_robs][d][d] complex random observables */
     const double *inj_u;      /* rng_kind 1: concatenated uniforms */
     const int64_t *inj_off;   /* rng_kind 1: [n_traj + 1] offsets into inj_u */
+    uint64_t tr_base;         /* Philox stream of local trajectory tr is tr_base + tr (sharding) */
 } orc_problem;
 
 /* Mutable per-run state and outputs. */
