@@ -155,6 +155,28 @@ qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods);
 qjx_status qjx_fb_get(qjx_fb *h, double *x, double *last_period_ms);
 void qjx_fb_destroy(qjx_fb *h);
 
+/* Allocation-free f-basis RK4 (no counterpart in the reference, which always runs on the host).
+ * For callers that must not allocate GPU memory themselves or through this library: a host
+ * program that owns every device buffer through its own pool, or a solver called from a loop
+ * that must not pay cudaMalloc/cudaFree's device-wide synchronisation or fail under memory
+ * pressure in the middle of a run.  Same arithmetic as qjx_fb_create + qjx_fb_run (the same
+ * kernels); every pointer is DEVICE memory owned by the caller: the CSR arrays of Gs and
+ * Qs_drv (0-based), Ks [n], and x [n], advanced in place by n_periods periods of num_steps RK4
+ * steps starting at period index period0.  The RK4 stage vectors live in a static device array
+ * sized for n <= QJX_FB_NOALLOC_MAX_N (2 MiB, held by every GPU that loads the library until the
+ * process exits); larger n is rejected with QJX_ERR_UNSUPPORTED.  Work is queued on `stream`
+ * (a cudaStream_t, NULL for the default stream) and the call returns without waiting.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All calls on a device
+ * share the one array and it keeps the last call's contents (every element a call reads it
+ * writes first, so nothing needs clearing); calls that overlap on the GPU race, so serialise
+ * them on one stream per device. */
+#define QJX_FB_NOALLOC_MAX_N 65536
+qjx_status qjx_fb_rk4_noalloc(int n, const int *gs_rowptr, const int *gs_col, const double *gs_val,
+                              const int *qs_rowptr, const int *qs_col, const double *qs_val, const double *Ks,
+                              double *x, double drv_ampl, double drv_freq, double drv_phase, int drv_type, double T,
+                              int num_steps, int period0, int n_periods, int device, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

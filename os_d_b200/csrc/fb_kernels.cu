@@ -14,6 +14,7 @@
 // matches the CPU within rounding, not bit-for-bit.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -202,6 +203,70 @@ extern "C" qjx_status qjx_fb_get(qjx_fb *h, double *x, double *last_period_ms)
         return QJX_ERR_CUDA;
     if (last_period_ms) *last_period_ms = h->last_ms;
     return QJX_OK;
+}
+
+// ---------------------------------------------------------------- allocation-free variant
+// Stage vectors val, k1, k2, k3 of the allocation-free entry point, one static array shared by
+// all its calls on a device.  In host code this name is only a stand-in for the symbol; its
+// device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) double g_fb_noalloc_scratch[4 * QJX_FB_NOALLOC_MAX_N];
+
+static double *fb_noalloc_scratch_ptr(int device)
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static double *ptr[kMaxDevices] = {nullptr};
+    if (device < 0 || device >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[device]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_fb_noalloc_scratch) != cudaSuccess) return nullptr;
+        ptr[device] = static_cast<double *>(p);
+    }
+    return ptr[device];
+}
+
+extern "C" qjx_status qjx_fb_rk4_noalloc(int n, const int *gs_rowptr, const int *gs_col, const double *gs_val,
+                                         const int *qs_rowptr, const int *qs_col, const double *qs_val,
+                                         const double *Ks, double *x, double drv_ampl, double drv_freq,
+                                         double drv_phase, int drv_type, double T, int num_steps, int period0,
+                                         int n_periods, int device, void *stream)
+{
+    if (n < 1 || !gs_rowptr || !gs_col || !gs_val || !qs_rowptr || !qs_col || !qs_val || !Ks || !x ||
+        num_steps < 1 || !(T > 0.0) || (drv_type != 0 && drv_type != 1) || period0 < 0 || n_periods < 0)
+        return QJX_ERR_INVALID_ARG;
+    if (n > QJX_FB_NOALLOC_MAX_N) return QJX_ERR_UNSUPPORTED;
+    if (cudaSetDevice(device) != cudaSuccess) return QJX_ERR_CUDA;
+    double *scratch = fb_noalloc_scratch_ptr(device);
+    if (!scratch) return QJX_ERR_CUDA;
+    fb::FbParams P{};
+    P.n = n;
+    P.gr = gs_rowptr;
+    P.gc = gs_col;
+    P.gv = gs_val;
+    P.qr = qs_rowptr;
+    P.qc = qs_col;
+    P.qv = qs_val;
+    P.Ks = Ks;
+    P.drv_ampl = -drv_ampl;
+    P.drv_freq = drv_freq;
+    P.drv_phase = drv_phase;
+    P.drv_type = drv_type;
+    P.x = x;
+    P.val = scratch;
+    P.k1 = scratch + QJX_FB_NOALLOC_MAX_N;
+    P.k2 = scratch + 2 * QJX_FB_NOALLOC_MAX_N;
+    P.k3 = scratch + 3 * QJX_FB_NOALLOC_MAX_N;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const double step = T / double(num_steps);
+    const int warps = 8, rblocks = (n + warps - 1) / warps, ublocks = (n + 255) / 256;
+    for (int p = period0; p < period0 + n_periods; p++)
+        for (int s = 0; s < num_steps; s++) {
+            const double t = double(p) * T + double(s) * step;
+            for (int stage = 1; stage <= 4; stage++) fb::rk_stage<<<rblocks, warps * 32, 0, st>>>(P, stage, t, step);
+            fb::rk_update<<<ublocks, 256, 0, st>>>(P);
+        }
+    return cudaGetLastError() == cudaSuccess ? QJX_OK : QJX_ERR_CUDA;
 }
 
 extern "C" void qjx_fb_destroy(qjx_fb *h)
