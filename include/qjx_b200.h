@@ -150,8 +150,12 @@ qjx_status qjx_fb_create(int n, const int *gs_rowptr, const int *gs_col, const d
                          const int *qs_rowptr, const int *qs_col, const double *qs_val, const double *Ks,
                          const double *x0, double drv_ampl, double drv_freq, double drv_phase, int drv_type,
                          double T, int num_steps, int device, qjx_fb **out);
-/* Integrate n_periods periods of num_steps RK4 steps starting at period index period0. */
+/* Integrate n_periods periods of num_steps RK4 steps starting at period index period0.
+ * When the system fits, one thread-block cluster (<= 16 CTAs) holds it in distributed shared
+ * memory and runs a period per launch; otherwise one launch per RK stage. */
 qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods);
+/* Cluster size of the cluster-resident path (0: per-stage kernels). */
+qjx_status qjx_fb_info(qjx_fb *h, int *cluster_size);
 qjx_status qjx_fb_get(qjx_fb *h, double *x, double *last_period_ms);
 void qjx_fb_destroy(qjx_fb *h);
 

@@ -21,7 +21,7 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_fb_rk4_noalloc", "qjx_fb_create", "qjx_fb_run", "qjx_fb_get", "qjx_fb_destroy",
+    "qjx_random_observables", "qjx_fb_rk4_noalloc", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
 
@@ -85,6 +85,7 @@ def lib():
                                      C.c_double, C.c_int, C.c_int, C.POINTER(vp)])
         L.qjx_fb_run.argtypes = [vp, C.c_int, C.c_int]
         L.qjx_fb_get.argtypes = [vp, c_double_p, c_double_p]
+        L.qjx_fb_info.argtypes = [vp, c_int_p]
         L.qjx_fb_rk4_noalloc.argtypes = ([C.c_int] + [vp] * 8 + [C.c_double] * 3 + [C.c_int, C.c_double]
                                          + [C.c_int] * 4 + [vp])
         L.qjx_fb_destroy.argtypes = [vp]

@@ -12,7 +12,10 @@
 // combined by an xor butterfly (offsets 16, 8, 4, 2, 1).  All other arithmetic is literal
 // (-fmad=false).  The drive uses sin() of the stage time (CUDA libdevice), so drv_type 1
 // matches the CPU within rounding, not bit-for-bit.
+#include <cooperative_groups.h>
+
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -87,10 +90,144 @@ __global__ void rk_update(const FbParams P)
     if (i < P.n) P.x[i] = __dadd_rn(P.x[i], __ddiv_rn(P.k3[i], 6.0));
 }
 
+// ---------------------------------------------------------------- cluster-resident RK4
+// One thread-block cluster integrates the whole system: CTA r owns rows [row_lo[r], row_lo[r+1])
+// and keeps their CSR slices of Gs and Qs_drv in shared memory (the cluster's distributed shared
+// memory holds the whole Liouvillian), plus full copies of x and of the two stage arguments.
+// Each stage computes the owned rows and stores the next stage argument into every CTA of the
+// cluster (DSMEM); a hardware cluster barrier separates the stages, four per RK4 step, and no
+// kernel launch happens inside a period.  Rows are computed thread-per-row with the canonical
+// 32-lane order (lane partial sums over nonzeros l, l+32, ..., then the butterfly tree), so the
+// results equal the warp-per-row kernel bit for bit.
+struct FbClusterParams {
+    int n;
+    const int *row_lo;  // [cluster size + 1]
+    const int *gr, *gc;
+    const double *gv;
+    const int *qr, *qc;
+    const double *qv;
+    const double *Ks;
+    double *x;
+    double drv_ampl, drv_freq, drv_phase;
+    int drv_type;
+    double T, h;
+    int num_steps, period0, n_periods;
+    int max_rows, max_gnz, max_qnz;
+};
+
+__device__ __forceinline__ double row_sum_lanes(const int *rp, const int *col, const double *val, const double *arg,
+                                                int r)
+{
+    double p[32];
+#pragma unroll
+    for (int l = 0; l < 32; l++) p[l] = 0.0;
+    const int b = rp[r], e = rp[r + 1];
+    for (int base = b; base < e; base += 32) {
+#pragma unroll
+        for (int l = 0; l < 32; l++) {
+            const int j = base + l;
+            if (j < e) p[l] = __fma_rn(val[j], arg[col[j]], p[l]);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+        for (int l = 0; l < off; l++) p[l] = __dadd_rn(p[l], p[l + off]);
+    return p[0];
+}
+
+constexpr int kMaxCluster = 16;
+
+__global__ void __launch_bounds__(512, 1) rk4_cluster(const FbClusterParams P)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
+    extern __shared__ __align__(16) unsigned char fsm[];
+    const int n = P.n, tid = threadIdx.x, nt = blockDim.x;
+    double *xf = reinterpret_cast<double *>(fsm);
+    double *va = xf + n;
+    double *vb = va + n;
+    double *k1 = vb + n;
+    double *k2 = k1 + P.max_rows;
+    double *k3 = k2 + P.max_rows;
+    double *ks = k3 + P.max_rows;
+    double *gval = ks + P.max_rows;
+    double *qval = gval + P.max_gnz;
+    int *grp = reinterpret_cast<int *>(qval + P.max_qnz);
+    int *qrp = grp + P.max_rows + 1;
+    int *gcol = qrp + P.max_rows + 1;
+    int *qcol = gcol + P.max_gnz;
+    const int r0 = P.row_lo[rank], nr = P.row_lo[rank + 1] - r0;
+    const int gb = P.gr[r0], qb = P.qr[r0];
+    for (int i = tid; i < n; i += nt) xf[i] = P.x[i];
+    for (int i = tid; i <= nr; i += nt) {
+        grp[i] = P.gr[r0 + i] - gb;
+        qrp[i] = P.qr[r0 + i] - qb;
+    }
+    for (int j = tid; j < P.gr[r0 + nr] - gb; j += nt) {
+        gval[j] = P.gv[gb + j];
+        gcol[j] = P.gc[gb + j];
+    }
+    for (int j = tid; j < P.qr[r0 + nr] - qb; j += nt) {
+        qval[j] = P.qv[qb + j];
+        qcol[j] = P.qc[qb + j];
+    }
+    for (int i = tid; i < nr; i += nt) ks[i] = P.Ks[r0 + i];
+    cl.sync();
+    const double h = P.h;
+    for (int p = P.period0; p < P.period0 + P.n_periods; p++) {
+        for (int s = 0; s < P.num_steps; s++) {
+            const double t = __dadd_rn(__dmul_rn((double)p, P.T), __dmul_rn((double)s, h));
+#pragma unroll 1
+            for (int stage = 1; stage <= 4; stage++) {
+                const double *arg = (stage == 1) ? xf : ((stage == 3) ? vb : va);
+                const double tt =
+                    (stage == 1) ? t : ((stage == 4) ? __dadd_rn(t, h) : __dadd_rn(t, __ddiv_rn(h, 2.0)));
+                const double sn = sin(__dadd_rn(__dmul_rn(P.drv_freq, tt), P.drv_phase));
+                const double drv = (P.drv_type == 1) ? __dmul_rn(P.drv_ampl, sn)
+                                                     : __dmul_rn(P.drv_ampl, (sn < 0.0) ? -1.0 : 1.0);
+                for (int i = tid; i < nr; i += nt) {
+                    const double t1 = row_sum_lanes(grp, gcol, gval, arg, i);
+                    const double t2 = row_sum_lanes(qrp, qcol, qval, arg, i);
+                    const double k = __dmul_rn(__dsub_rn(__dadd_rn(t1, __dmul_rn(drv, t2)), ks[i]), h);
+                    const int row = r0 + i;
+                    const double x = xf[row];
+                    if (stage == 1) {
+                        k1[i] = k;
+                        const double v = __dadd_rn(x, __ddiv_rn(k, 2.0));
+                        for (int r = 0; r < cs; r++) *cl.map_shared_rank(va + row, r) = v;
+                    } else if (stage == 2) {
+                        k2[i] = k;
+                        const double v = __dadd_rn(x, __ddiv_rn(k, 2.0));
+                        for (int r = 0; r < cs; r++) *cl.map_shared_rank(vb + row, r) = v;
+                    } else if (stage == 3) {
+                        k3[i] = k;
+                        const double v = __dadd_rn(x, k);
+                        for (int r = 0; r < cs; r++) *cl.map_shared_rank(va + row, r) = v;
+                    } else {
+                        const double sum =
+                            __dadd_rn(__dadd_rn(__dadd_rn(k1[i], __dmul_rn(2.0, k2[i])), __dmul_rn(2.0, k3[i])), k);
+                        const double xn = __dadd_rn(x, __ddiv_rn(sum, 6.0));
+                        for (int r = 0; r < cs; r++) *cl.map_shared_rank(xf + row, r) = xn;
+                    }
+                }
+                cl.sync();
+            }
+        }
+    }
+    for (int i = tid; i < nr; i += nt) P.x[r0 + i] = xf[r0 + i];
+}
+
 }  // namespace fb
 
 struct qjx_fb {
     fb::FbParams P{};
+    // cluster-resident path (used when the system fits the shared memory of <= 16 CTAs)
+    bool cluster = false;
+    int cs = 0;
+    size_t csmem = 0;
+    fb::FbClusterParams CP{};
     int device = 0;
     double T = 0.0;
     int num_steps = 0;
@@ -168,6 +305,86 @@ extern "C" qjx_status qjx_fb_create(int n, const int *gs_rowptr, const int *gs_c
         qjx_fb_destroy(h);
         return QJX_ERR_CUDA;
     }
+    // cluster-resident path: smallest cluster (power of two <= 16) whose CTAs hold their rows'
+    // CSR slices plus three full vectors in shared memory; QJX_FB_PATH=stages forces the
+    // per-stage kernels.
+    const char *path = std::getenv("QJX_FB_PATH");
+    const bool stages_only = path && std::string(path) == "stages";
+    int smem_optin = 0;
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    for (int cs = 1; cs <= fb::kMaxCluster && !stages_only && !h->cluster; cs *= 2) {
+        // balanced contiguous row split by nonzeros + a fixed cost per row
+        std::vector<int> lo(cs + 1, n);
+        lo[0] = 0;
+        const long long total = (long long)gnz + qnz + 8LL * n;
+        int r = 0;
+        long long acc = 0;
+        for (int c = 1; c < cs; c++) {
+            const long long target = total * c / cs;
+            while (r < n && acc + (gs_rowptr[r + 1] - gs_rowptr[r]) + (qs_rowptr[r + 1] - qs_rowptr[r]) + 8 <= target) {
+                acc += (gs_rowptr[r + 1] - gs_rowptr[r]) + (qs_rowptr[r + 1] - qs_rowptr[r]) + 8;
+                r++;
+            }
+            lo[c] = r;
+        }
+        int mr = 0, mg = 0, mq = 0;
+        for (int c = 0; c < cs; c++) {
+            mr = std::max(mr, lo[c + 1] - lo[c]);
+            mg = std::max(mg, gs_rowptr[lo[c + 1]] - gs_rowptr[lo[c]]);
+            mq = std::max(mq, qs_rowptr[lo[c + 1]] - qs_rowptr[lo[c]]);
+        }
+        const size_t bytes = sizeof(double) * (3 * (size_t)n + 4 * (size_t)mr + mg + mq) +
+                             sizeof(int) * (2 * (size_t)(mr + 1) + mg + mq);
+        if (bytes + 1024 > (size_t)smem_optin) continue;
+        if (cudaFuncSetAttribute(fb::rk4_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+            continue;
+        if (cs > 8 && cudaFuncSetAttribute(fb::rk4_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+            continue;
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(cs);
+        lc.blockDim = dim3(512);
+        lc.dynamicSmemBytes = bytes;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, fb::rk4_cluster, &lc) != cudaSuccess || nclusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        int *d_lo = (int *)fb_alloc(h, sizeof(int) * (cs + 1));
+        if (!d_lo) break;
+        cudaMemcpy(d_lo, lo.data(), sizeof(int) * (cs + 1), cudaMemcpyHostToDevice);
+        fb::FbClusterParams &C = h->CP;
+        C.n = n;
+        C.row_lo = d_lo;
+        C.gr = P.gr;
+        C.gc = P.gc;
+        C.gv = P.gv;
+        C.qr = P.qr;
+        C.qc = P.qc;
+        C.qv = P.qv;
+        C.Ks = P.Ks;
+        C.x = P.x;
+        C.drv_ampl = P.drv_ampl;
+        C.drv_freq = P.drv_freq;
+        C.drv_phase = P.drv_phase;
+        C.drv_type = P.drv_type;
+        C.T = T;
+        C.h = T / double(num_steps);
+        C.num_steps = num_steps;
+        C.max_rows = mr;
+        C.max_gnz = mg;
+        C.max_qnz = mq;
+        h->cluster = true;
+        h->cs = cs;
+        h->csmem = bytes;
+    }
+    cudaGetLastError();
     *out = h;
     return QJX_OK;
 }
@@ -180,11 +397,33 @@ extern "C" qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods)
     const double step = h->T / double(h->num_steps);  // data.cpp:10
     const int warps = 8, rblocks = (P.n + warps - 1) / warps, ublocks = (P.n + 255) / 256;
     cudaEventRecord(h->e0, h->stream);
-    for (int p = period0; p < period0 + n_periods; p++) {
-        for (int s = 0; s < h->num_steps; s++) {
-            const double t = double(p) * h->T + double(s) * step;  // calcODE.cpp:280
-            for (int stage = 1; stage <= 4; stage++) fb::rk_stage<<<rblocks, warps * 32, 0, h->stream>>>(P, stage, t, step);
-            fb::rk_update<<<ublocks, 256, 0, h->stream>>>(P);
+    if (h->cluster) {  // one cluster launch per period
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(h->cs);
+        lc.blockDim = dim3(512);
+        lc.dynamicSmemBytes = h->csmem;
+        lc.stream = h->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = h->cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        for (int p = period0; p < period0 + n_periods; p++) {
+            fb::FbClusterParams C = h->CP;
+            C.period0 = p;
+            C.n_periods = 1;
+            if (cudaLaunchKernelEx(&lc, fb::rk4_cluster, C) != cudaSuccess) return QJX_ERR_CUDA;
+        }
+    } else {
+        for (int p = period0; p < period0 + n_periods; p++) {
+            for (int s = 0; s < h->num_steps; s++) {
+                const double t = double(p) * h->T + double(s) * step;  // calcODE.cpp:280
+                for (int stage = 1; stage <= 4; stage++)
+                    fb::rk_stage<<<rblocks, warps * 32, 0, h->stream>>>(P, stage, t, step);
+                fb::rk_update<<<ublocks, 256, 0, h->stream>>>(P);
+            }
         }
     }
     cudaEventRecord(h->e1, h->stream);
@@ -192,6 +431,13 @@ extern "C" qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods)
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->e0, h->e1);
     h->last_ms = ms;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_fb_info(qjx_fb *h, int *cluster_size)
+{
+    if (!h || !cluster_size) return QJX_ERR_INVALID_ARG;
+    *cluster_size = h->cluster ? h->cs : 0;
     return QJX_OK;
 }
 

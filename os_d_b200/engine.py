@@ -160,6 +160,12 @@ class FBasis:
     def run(self, period0, n_periods):
         N.check(N.lib().qjx_fb_run(self.h, period0, n_periods), what="qjx_fb_run")
 
+    def cluster_size(self):
+        """CTAs of the cluster-resident RK4 path (0: per-stage kernels)."""
+        cs = C.c_int()
+        N.check(N.lib().qjx_fb_info(self.h, C.byref(cs)), what="qjx_fb_info")
+        return cs.value
+
     def get(self):
         x = np.zeros(self.n)
         ms = C.c_double()

@@ -136,3 +136,28 @@ def test_gpu_qj_ensemble_within_statistical_error_of_gpu_fbasis():
         pops_f = np.real(np.diag(O.fb_rho(N, x)))
         err = adr[p].std(axis=0) / np.sqrt(n)
         assert np.all(np.abs(adr[p].mean(axis=0) - pops_f) < 4.5 * err + 2e-3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", [20, 50])
+def test_gpu_cluster_rk4_matches_oracle_and_stage_kernels(N, monkeypatch):
+    import os_d_b200 as q
+
+    Gs, Qs, Ks = O.fb_dense(N, 1.0, 0.5, 1.0, 0.1)
+    Gc, Qc = O.fb_csr(Gs), O.fb_csr(Qs)
+    rho0 = np.zeros((N + 1, N + 1), complex)
+    rho0[0, 0] = 1
+    x0 = O.fb_x_from_rho(N, rho0)
+    steps = 200 if N == 20 else 2000  # RK4 stability: h times the spectral radius of Gs stays < 2.5
+    fb = q.FBasis(Gc, Qc, Ks, x0, 1.5, drv_type=0, T=T2PI, num_steps=steps)
+    assert fb.cluster_size() > 0  # the cluster-resident path is taken
+    fb.run(0, 2)
+    x_c, _ = fb.get()
+    monkeypatch.setenv("QJX_FB_PATH", "stages")
+    fs = q.FBasis(Gc, Qc, Ks, x0, 1.5, drv_type=0, T=T2PI, num_steps=steps)
+    assert fs.cluster_size() == 0
+    fs.run(0, 2)
+    x_s, _ = fs.get()
+    assert np.all(np.isfinite(x_c)) and np.array_equal(x_c, x_s)
+    x_o = O.fb_rk4(Gc, Qc, Ks, x0, 1.5, drv_type=0, T=T2PI, num_steps=steps, n_periods=2)
+    assert np.array_equal(x_c, x_o)
