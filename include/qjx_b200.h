@@ -111,6 +111,12 @@ qjx_status qjx_observe(qjx_engine *h, int dump, int is_start);
 qjx_status qjx_get_observables(qjx_engine *h, int dump0, int n_dumps, double *norm, double *mean,
                                double *dispersion, double *m2, double *energy, double *robs, double *adr);
 qjx_status qjx_get_mean_start(qjx_engine *h, double *mean_start);
+/* Ensemble purity Tr(rho^2) of the current states, rho = (1/n_traj) sum |psi_hat><psi_hat|
+ * with psi_hat = psi/||psi||.  QJX has no ensemble purity; the formula is calc_purity's
+ * (source/cpp/CQdiss/CQdiss/CalcTraseRO2.cpp:57-75) for the density matrix the trajectories
+ * sample.  rho (optional, NULL skips) receives the d x d matrix row-major, complex interleaved.
+ * Sharded ensembles combine rho_total = sum_r n_r rho_r / sum_r n_r before squaring. */
+qjx_status qjx_purity(qjx_engine *h, double *purity, double *rho);
 /* Current states [n_traj][d] complex, times, etas, jump counts (any pointer may be NULL). */
 qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, int *jumps_counts);
 /* Jump records of one trajectory accumulated since qjx_set_states. */

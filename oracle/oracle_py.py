@@ -52,6 +52,8 @@ def lib():
         L.orc_matvec.argtypes = [C.c_int, c_double_p, c_double_p, c_double_p]
         L.orc_norm_square.argtypes = [C.c_int, c_double_p]
         L.orc_norm_square.restype = C.c_double
+        L.orc_purity.argtypes = [C.c_int, C.c_int, c_double_p, c_double_p]
+        L.orc_purity.restype = C.c_double
     return _lib
 
 
@@ -109,6 +111,14 @@ def matvec(M, x):
 def norm_square(x):
     x = np.ascontiguousarray(x, dtype=np.complex128)
     return lib().orc_norm_square(x.shape[0], _dp(x))
+
+
+def purity(psi):
+    """Ensemble purity of states psi [n][d] and the trajectory-averaged rho (orc_purity)."""
+    psi = np.ascontiguousarray(psi, dtype=np.complex128)
+    n, d = psi.shape
+    rho = np.zeros((d, d), np.complex128)
+    return lib().orc_purity(d, n, _dp(psi), _dp(rho)), rho
 
 
 def dump_periods(dump_type, dump_num, num_obs_periods):

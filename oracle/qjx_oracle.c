@@ -463,6 +463,37 @@ double orc_norm_square(int d, const double *x)
     return lanes_finish(p);
 }
 
+/* Ensemble purity.  Order of operations: psi_hat = psi / sqrt(p) per element with the canonical
+ * norm p; rho_ij accumulates trajectories in ascending order (re += a_r b_r, re += a_i b_i,
+ * im += a_i b_r, im += -a_r b_i, each one fma) and is divided by n; purity = canonical squared
+ * norm of rho flattened row-major.  calc_purity (CalcTraseRO2.cpp:57-75) computes Tr(rho rho)
+ * of the f-basis density matrix; here rho is the trajectory average. */
+double orc_purity(int d, int n, const double *psi, double *rho)
+{
+    double *acc = (double *)calloc((size_t)2 * d * d, sizeof(double));
+    double *hat = (double *)malloc(sizeof(double) * 2 * (size_t)d);
+    for (int tr = 0; tr < n; tr++) {
+        const double *x = psi + (size_t)2 * d * tr;
+        const double q = sqrt(orc_norm_square(d, x));
+        for (int k = 0; k < 2 * d; k++) hat[k] = x[k] / q;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double *z = acc + 2 * ((size_t)i * d + j);
+                const double ar = hat[2 * i], ai = hat[2 * i + 1], br = hat[2 * j], bi = hat[2 * j + 1];
+                z[0] = fma(ar, br, z[0]);
+                z[0] = fma(ai, bi, z[0]);
+                z[1] = fma(ai, br, z[1]);
+                z[1] = fma(-ar, bi, z[1]);
+            }
+    }
+    for (size_t e = 0; e < (size_t)2 * d * d; e++) acc[e] = acc[e] / (double)n;
+    const double pur = orc_norm_square(d * d, acc);
+    if (rho) memcpy(rho, acc, sizeof(double) * 2 * (size_t)d * d);
+    free(acc);
+    free(hat);
+    return pur;
+}
+
 /* ------------------------------------------------------------------ QJ engine */
 
 typedef struct {

@@ -123,6 +123,10 @@ int orc_dump_periods(int dump_type, int dump_num, int num_obs_periods, int *peri
 /* Canonical kernels, exported for unit tests. */
 void orc_matvec(int d, const double *M, const double *x, double *out);
 double orc_norm_square(int d, const double *x);
+/* Ensemble purity Tr(rho^2), rho = (1/n) sum_tr psi_hat psi_hat^dagger (psi [n][d] complex
+ * interleaved); the formula of calc_purity (source/cpp/CQdiss/CQdiss/CalcTraseRO2.cpp:57-75).
+ * rho (d x d complex, may be NULL) receives the matrix. */
+double orc_purity(int d, int n, const double *psi, double *rho);
 
 #ifdef __cplusplus
 }

@@ -19,7 +19,7 @@ c_i64_p = C.POINTER(C.c_int64)
 EXPORTS = [
     "qjx_create", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
-    "qjx_get_mean_start", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
+    "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
     "qjx_random_observables", "qjx_fb_rk4_noalloc", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
@@ -70,6 +70,7 @@ def lib():
         L.qjx_observe.argtypes = [vp, C.c_int, C.c_int]
         L.qjx_get_observables.argtypes = [vp, C.c_int, C.c_int] + [c_double_p] * 7
         L.qjx_get_mean_start.argtypes = [vp, c_double_p]
+        L.qjx_purity.argtypes = [vp, c_double_p, c_double_p]
         L.qjx_get_states.argtypes = [vp, c_double_p, c_double_p, c_double_p, c_int_p]
         L.qjx_jump_count.argtypes = [vp, C.c_int, c_i64_p]
         L.qjx_get_jumps.argtypes = [vp, C.c_int, c_double_p, c_int_p, c_double_p, c_double_p]

@@ -20,6 +20,7 @@ size_t step_smem_bytes(int MD);
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st);
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st);
 cudaError_t launch_init_state(const Params &P, cudaStream_t st);
+cudaError_t launch_purity(const Params &P, double2 *hat, double2 *rho, double *out, cudaStream_t st);
 cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
 cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
 cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
@@ -42,6 +43,9 @@ struct qjx_engine {
     long long *d_inj_off = nullptr;
     int *d_dump_at = nullptr;
     int dump_cap = 0;
+    // ensemble purity scratch (allocated on the first qjx_purity call)
+    double2 *d_hat = nullptr, *d_rho = nullptr;
+    double *d_purity = nullptr;
     // host mirrors
     int *h_cnt = nullptr;   // pinned [G]
     int *h_ctrl = nullptr;  // pinned [8]
@@ -530,6 +534,30 @@ extern "C" qjx_status qjx_get_observables(qjx_engine *h, int dump0, int n_dumps,
         else
             CK(cudaMemcpy(adr, P.o_adr, (size_t)P.n * P.d * sizeof(double), cudaMemcpyDeviceToHost));
     }
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_purity(qjx_engine *h, double *purity, double *rho)
+{
+    if (!h || !purity) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    CK(cudaSetDevice(h->cfg.device));
+    Params &P = h->P;
+    if (!h->d_hat) {
+        h->d_hat = (double2 *)dalloc(h, (size_t)P.n * P.MD * sizeof(double2));
+        h->d_rho = (double2 *)dalloc(h, (size_t)P.d * P.d * sizeof(double2));
+        h->d_purity = (double *)dalloc(h, sizeof(double));
+        if (!h->d_hat || !h->d_rho || !h->d_purity) {
+            h->d_hat = nullptr;
+            return fail(h, QJX_ERR_OOM, "purity scratch");
+        }
+    }
+    CK(launch_purity(P, h->d_hat, h->d_rho, h->d_purity, h->stream));
+    h->stats.launches += 3;
+    CK(cudaMemcpyAsync(purity, h->d_purity, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (rho)
+        CK(cudaMemcpyAsync(rho, h->d_rho, (size_t)P.d * P.d * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return QJX_OK;
 }
 

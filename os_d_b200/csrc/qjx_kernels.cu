@@ -673,6 +673,67 @@ __global__ void observe_kernel(const Params P, int dump, int is_start)
     }
 }
 
+// ---------------------------------------------------------------- ensemble purity
+// rho = (1/n) sum_tr psi_hat psi_hat^dagger over the current states, purity = ||rho||_F^2 (the
+// formula of calc_purity, source/cpp/CQdiss/CQdiss/CalcTraseRO2.cpp:57-75, applied to the
+// trajectory ensemble).  Canonical order, shared bit-for-bit with the CPU oracle: psi_hat =
+// psi / sqrt(p) with the canonical 32-lane norm p; rho_ij accumulates trajectories in ascending
+// order with fma (re += a_r b_r, re += a_i b_i, im += a_i b_r, im += -a_r b_i) and is divided by n;
+// the purity is the canonical 32-lane squared norm of rho flattened row-major.
+__global__ void normalize_kernel(const Params P, double2 *hat)
+{
+    const int lane = threadIdx.x & 31;
+    const int tr = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tr >= P.n) return;
+    const double2 *src = slot_ptr(P, P.st[tr].cur, tr);
+    const double q = __dsqrt_rn(warp_norm(src, P.d, lane));
+    double2 *dst = hat + (size_t)tr * P.MD;
+    for (int k = lane; k < P.d; k += 32) {
+        const double2 v = src[k];
+        dst[k] = make_double2(__ddiv_rn(v.x, q), __ddiv_rn(v.y, q));
+    }
+}
+
+// one 16 x 16 tile of rho per block (256 threads), trajectories staged 32 at a time
+__global__ void __launch_bounds__(256) rho_kernel(const Params P, const double2 *hat, double2 *rho)
+{
+    __shared__ double2 a[32][16], b[32][16];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int i0 = blockIdx.y * 16, j0 = blockIdx.x * 16;
+    double re = 0.0, im = 0.0;
+    for (int c = 0; c < P.n; c += 32) {
+        for (int e = threadIdx.x; e < 32 * 16; e += 256) {
+            const int t = e >> 4, k = e & 15, tr = c + t;
+            double2 za = make_double2(0.0, 0.0), zb = za;
+            if (tr < P.n) {
+                if (i0 + k < P.d) za = hat[(size_t)tr * P.MD + i0 + k];
+                if (j0 + k < P.d) zb = hat[(size_t)tr * P.MD + j0 + k];
+            }
+            a[t][k] = za;
+            b[t][k] = zb;
+        }
+        __syncthreads();
+        const int m = min(32, P.n - c);
+        for (int t = 0; t < m; t++) {
+            const double2 x = a[t][ty], y = b[t][tx];
+            re = __fma_rn(x.x, y.x, re);
+            re = __fma_rn(x.y, y.y, re);
+            im = __fma_rn(x.y, y.x, im);
+            im = __fma_rn(-x.x, y.y, im);
+        }
+        __syncthreads();
+    }
+    const int i = i0 + ty, j = j0 + tx;
+    if (i < P.d && j < P.d)
+        rho[(size_t)i * P.d + j] = make_double2(__ddiv_rn(re, (double)P.n), __ddiv_rn(im, (double)P.n));
+}
+
+__global__ void purity_kernel(const double2 *rho, int dd, double *out)
+{
+    const double s = warp_norm(rho, dd, threadIdx.x & 31);
+    if (threadIdx.x == 0) *out = s;
+}
+
 __global__ void init_state_kernel(const Params P)
 {
     const int tr = blockIdx.x * blockDim.x + threadIdx.x;
@@ -785,6 +846,15 @@ cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t
         attr_set = true;
     }
     observe_kernel<<<(P.n + 7) / 8, 256, smem, st>>>(P, dump, is_start);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_purity(const Params &P, double2 *hat, double2 *rho, double *out, cudaStream_t st)
+{
+    normalize_kernel<<<(P.n + 7) / 8, 256, 0, st>>>(P, hat);
+    const int tiles = (P.d + 15) / 16;
+    rho_kernel<<<dim3(tiles, tiles), 256, 0, st>>>(P, hat, rho);
+    purity_kernel<<<1, 32, 0, st>>>(rho, P.d * P.d, out);
     return cudaGetLastError();
 }
 

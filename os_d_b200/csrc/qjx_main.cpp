@@ -96,6 +96,8 @@ int main(int argc, char **argv)
         const int dump_adr_avg_on = int(param(cp, "dump_adr_avg"));
         const int dump_phi_on = int(param(cp, "dump_phi")), dump_phi_evo_on = int(param(cp, "dump_phi_evo"));
         const int jumps_counts_lim = int(param(cp, "jumps_counts"));
+        // optional key (no counterpart in QJX): ensemble purity per dump into purity_evo
+        const int dump_purity = int(param_or(cp, "dump_purity", 0));
         const int num_robs = int(param(cp, "num_random_obs"));
         const int robs_seed = int(param_or(cp, "random_obs_seed", 0));
         if (n < 1 || N < 1) die("num_trajectories and N must be positive");
@@ -194,6 +196,14 @@ int main(int argc, char **argv)
             for (int tr = 0; tr < n; tr++)
                 save_complex_data(path + prefix + std::to_string(tr) + sfx, psi.data() + 2 * (size_t)tr * d, d, 16, append);
         };
+        std::vector<double> purity_evo;
+        auto take_purity = [&]() {
+            if (dump_purity != 1) return;
+            double p = 0.0;
+            check(qjx_purity(h, &p, nullptr), h, "qjx_purity");
+            purity_evo.push_back(p);
+        };
+        take_purity();
         write_adr_single(0, false);
         if (dump_evo_avg == 1) write_adr_avg(0, false);
 
@@ -201,7 +211,8 @@ int main(int argc, char **argv)
         if (dump_phi_evo_on == 1) write_phi("phi_evo_", false);
         int last_dump = 0;
         const bool per_interval = jumps_counts_lim > 0 || !increasing || dump_phi_evo_on == 1 ||
-                                  (dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1 || rp.is_pp == 1;
+                                  (dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1 || rp.is_pp == 1 ||
+                                  dump_purity == 1;
         if (!per_interval) {
             // one call: every trajectory runs all observation periods, observables at each dump
             std::vector<int> at(dp.begin() + 1, dp.end());
@@ -232,12 +243,14 @@ int main(int argc, char **argv)
                     check(qjx_observe(h, dump_id, 0), h, "qjx_observe");
                 }
                 last_dump = dump_id;
+                take_purity();
                 write_adr_single(dump_id, true);
                 if (dump_phi_evo_on == 1) write_phi("phi_evo_", true);
                 if (dump_evo_avg == 1) write_adr_avg(dump_id, true);
             }
         }
         const int nrec = last_dump + 1;
+        if (dump_purity == 1) save_double_data(path + "purity_evo" + sfx, purity_evo.data(), purity_evo.size(), 16, false);
 
         // collect observables of the recorded dumps
         Dumps D;

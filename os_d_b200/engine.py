@@ -93,6 +93,13 @@ class Engine:
         self._chk(N.lib().qjx_get_mean_start(self.h, N.dp(ms)), "qjx_get_mean_start")
         return ms
 
+    def purity(self, want_rho=False):
+        """Ensemble purity Tr(rho^2) of the current states (and rho itself with want_rho)."""
+        p = np.zeros(1)
+        rho = np.zeros((self.d, self.d), np.complex128) if want_rho else None
+        self._chk(N.lib().qjx_purity(self.h, N.dp(p), N.dp(rho)), "qjx_purity")
+        return (p[0], rho) if want_rho else p[0]
+
     def states(self):
         psi = np.zeros((self.n, self.d), np.complex128)
         t = np.zeros(self.n)

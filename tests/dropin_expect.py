@@ -99,6 +99,8 @@ def expected_outputs(cfg, prm, R=None):
     evo_avg, adr_avg_on = int(prm["dump_evo_avg"]), int(prm["dump_adr_avg"])
     phi_evo_on, phi_on = int(prm["dump_phi_evo"]), int(prm["dump_phi"])
     lim = int(prm["jumps_counts"])
+    dump_purity = int(prm.get("dump_purity", 0))  # optional key of the drop-in (not in QJX)
+    purity = [O.purity(ens.phi)[0]] if dump_purity == 1 else []
 
     def adr_avg(adr):
         avg = np.zeros(d)
@@ -132,6 +134,8 @@ def expected_outputs(cfg, prm, R=None):
         elif span > 0:
             assert ens.run_periods(span, is_obs=1) == 0
         obs.append(ens.observables(want_adr=True))
+        if dump_purity == 1:
+            purity.append(O.purity(ens.phi)[0])
         if evo_sep == 1 and adr_sep == 1:
             for tr in range(n):
                 emit("adr_%d" % tr + sfx, f_double_data(obs[-1]["adr"][tr]), True)
@@ -143,6 +147,8 @@ def expected_outputs(cfg, prm, R=None):
         if finished:
             break
     last = obs[-1]
+    if dump_purity == 1:
+        emit("purity_evo" + sfx, f_double_data(purity), False)
     if int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)

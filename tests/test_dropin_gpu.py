@@ -59,3 +59,11 @@ def test_dims_101_sample(tmp_path):
     cfg = dict(BASE_CONFIG, num_trajectories=16, num_tp_periods=1, num_obs_periods=2, seed=42)
     prm = dict(BASE_PARAMS, N=100, dump_num=2, jump=2)
     run_case(tmp_path, cfg, prm)
+
+
+def test_purity_per_dump(tmp_path):
+    cfg = dict(BASE_CONFIG, num_obs_periods=6, num_trajectories=24)
+    prm = dict(BASE_PARAMS, dump_num=3, dump_purity=1)
+    exp = run_case(tmp_path, cfg, prm)
+    vals = [float(v) for k, t in exp.items() if k.startswith("purity_evo") for v in t.split()]
+    assert len(vals) == 4 and vals[0] == 1.0 and 0.0 < min(vals[1:]) < 1.0
