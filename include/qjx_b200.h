@@ -72,6 +72,11 @@ typedef struct {
     int device;        /* CUDA device ordinal */
     int64_t tr_base;   /* global index of trajectory 0 (Philox stream id = tr_base + local index), so
                           an ensemble sharded over GPUs draws exactly the numbers of one big run */
+    int precision;     /* 0: complex FP64 end to end (the reference's arithmetic, bit-exact with the
+                          oracle); 1: split precision: every d x d matvec runs on the tcgen05 tensor
+                          cores as bf16 hi/lo planes with FP32 accumulation (products hi*hi + hi*lo +
+                          lo*hi), states, norms, thresholds, jump times and renormalisation stay
+                          FP64.  Needs d <= 256.  QJX has no such mode (its zgemv is FP64). */
 } qjx_config;
 
 typedef struct {

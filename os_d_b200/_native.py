@@ -29,7 +29,7 @@ class QjxConfig(C.Structure):
     _fields_ = [("d", C.c_int), ("n_traj", C.c_int), ("deep", C.c_int), ("num_branches", C.c_int),
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
-                ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64)]
+                ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("precision", C.c_int)]
 
 
 class QjxStats(C.Structure):

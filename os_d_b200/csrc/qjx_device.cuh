@@ -8,6 +8,7 @@
 //     intended fused operations are written as __fma_rn.
 #pragma once
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace qjx {
@@ -19,6 +20,7 @@ constexpr int kKB = 16;                // k rows per propagator slab (8 k pairs)
 constexpr int kStages = 2;             // slab pipeline depth
 constexpr int kMaxGroups = 256;        // distinct matrices in one engine
 constexpr int kMaxMD = 256;            // d <= 256
+constexpr double kSplitNormSlack = 1e-4;  // split precision: tolerated norm excess over 1
 // Thread layouts of a sub-tile (rows ty + TY i, columns tx + TX j, TY * TX = 256):
 //   TY = 32: MD = 32 * MT padded rows, TX = 8 column threads, up to 4 columns each
 //   TY = 16: MD = 16 * MT padded rows, TX = 16 column threads, up to 2 columns each
@@ -91,6 +93,11 @@ struct Params {
     // optional per-CTA trace, accumulated over micro-steps: [grid][kTraceFields] clock64 cycles
     // and counts (null: tracing off)
     long long *trace;
+    // split-precision form: bf16 planes of the real block form [[Re M, -Im M], [Im M, Re M]] of
+    // every matrix, rows/columns interleaved (2r + re/im), in tcgen05 core-matrix order
+    int split;                    // 0 FP64 plain form, 1 split bf16x3
+    int MDs, KS;                  // complex rows padded to 16 (one MMA N-half), k-steps of 8 complex
+    const unsigned char *usplit;  // [G][KS][kPlanes][2 MDs rows x 16 k] bf16
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns

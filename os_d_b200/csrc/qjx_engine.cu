@@ -2,6 +2,7 @@
 // loop (CUDA graphs of 6 micro-steps, bounded host polling), jump-record draining, and the
 // C ABI declared in include/qjx_b200.h.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -25,6 +26,7 @@ cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
 cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
 cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
 cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st);
+size_t split_smem_bytes(int MDs);
 }  // namespace qjx
 
 using namespace qjx;
@@ -112,6 +114,49 @@ static void pack_transposed(const double *M, int d, int MD, double *out)
         }
 }
 
+// bf16 nearest (ties to even) of x with 8 significant bits; *val receives the rounded value.
+static uint16_t bf16_round(double x, double *val)
+{
+    if (x == 0.0 || !std::isfinite(x)) {
+        *val = 0.0;
+        return 0;
+    }
+    const int e = std::ilogb(x);
+    const double q = std::ldexp(std::nearbyint(std::ldexp(x, 7 - e)), e - 7);
+    const float f = (float)q;  // exact: 8 significant bits
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    *val = q;
+    return (uint16_t)(b >> 16);
+}
+
+// bf16 hi/lo planes of the real block form of a row-major complex d x d matrix, in the order the
+// split-precision kernel loads them: out[ks][plane][2 MDs rows x 16 k] with row n = 2 r + (Re, Im
+// of output r), k index kk = 2 k + (Re, Im of input k), core matrices of 8 rows x 8 k (16 bytes
+// a row), K-halves 64 elements apart and 8-row groups 128 elements apart.
+static void pack_split(const double *M, int d, int MDs, int KS, uint16_t *out)
+{
+    const int NP = 2 * MDs;
+    const size_t plane = (size_t)NP * 16;
+    for (int ks = 0; ks < KS; ks++)
+        for (int n = 0; n < NP; n++)
+            for (int j = 0; j < 16; j++) {
+                const int kk = 16 * ks + j, k = kk >> 1, r = n >> 1;
+                double a = 0.0;
+                if (r < d && k < d) {
+                    const double mr = M[2 * ((size_t)r * d + k)], mi = M[2 * ((size_t)r * d + k) + 1];
+                    if ((n & 1) == 0) a = (kk & 1) ? -mi : mr;
+                    else a = (kk & 1) ? mr : mi;
+                }
+                double hv = 0.0, lv = 0.0;
+                const uint16_t hb = bf16_round(a, &hv);
+                const uint16_t lb = bf16_round(a - hv, &lv);
+                const size_t off = (size_t)(n & 7) * 8 + (size_t)(n >> 3) * 128 + (size_t)(j >> 3) * 64 + (j & 7);
+                out[(size_t)ks * 2 * plane + off] = hb;
+                out[(size_t)ks * 2 * plane + plane + off] = lb;
+            }
+}
+
 extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, const double *g,
                                  const double *HE, const double *R, qjx_engine **out)
 {
@@ -123,6 +168,7 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
         return QJX_ERR_INVALID_ARG;
     const int G = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;
     if (c.d > kMaxMD || G > kMaxGroups) return QJX_ERR_UNSUPPORTED;
+    if (c.precision != 0 && c.precision != 1) return QJX_ERR_INVALID_ARG;
 
     qjx_engine *h = new (std::nothrow) qjx_engine();
     if (!h) return QJX_ERR_OOM;
@@ -180,6 +226,27 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     if (!mats) return bail(QJX_ERR_OOM);
     cudaMemcpy(mats, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
     P.mats = mats;
+
+    if (c.precision == 1) {  // split precision: bf16 planes of every matrix in the tcgen05 order
+        P.split = 1;
+        P.MDs = 16 * ((d + 15) / 16);
+        P.KS = (d + 7) / 8;
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
+        if (split_smem_bytes(P.MDs) + 4096 > (size_t)optin) return bail(QJX_ERR_UNSUPPORTED);
+        const size_t per_s = (size_t)P.KS * 2 * (2 * P.MDs) * 16;
+        std::vector<uint16_t> hs((size_t)G * per_s, 0);
+        for (int b = 0; b < c.num_branches; b++)
+            for (int l = 0; l < c.deep; l++)
+                pack_split(U + dd2 * ((size_t)b * c.deep + l), d, P.MDs, P.KS, hs.data() + per_s * (b * c.deep + l));
+        for (int i = 0; i < c.num_diss; i++) pack_split(L + dd2 * i, d, P.MDs, P.KS, hs.data() + per_s * (P.gL0 + i));
+        pack_split(HE, d, P.MDs, P.KS, hs.data() + per_s * P.gHE);
+        for (int i = 0; i < c.num_robs; i++) pack_split(R + dd2 * i, d, P.MDs, P.KS, hs.data() + per_s * (P.gR0 + i));
+        unsigned char *us = (unsigned char *)dalloc(h, hs.size() * sizeof(uint16_t));
+        if (!us) return bail(QJX_ERR_OOM);
+        cudaMemcpy(us, hs.data(), hs.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+        P.usplit = us;
+    }
 
     // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24)
     std::vector<double> dts(c.deep);

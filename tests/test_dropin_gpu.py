@@ -66,4 +66,4 @@ def test_purity_per_dump(tmp_path):
     prm = dict(BASE_PARAMS, dump_num=3, dump_purity=1)
     exp = run_case(tmp_path, cfg, prm)
     vals = [float(v) for k, t in exp.items() if k.startswith("purity_evo") for v in t.split()]
-    assert len(vals) == 4 and vals[0] == 1.0 and 0.0 < min(vals[1:]) < 1.0
+    assert len(vals) == 4 and 0.0 < min(vals) <= max(vals) < 1.0  # dump 0 follows the transient periods

@@ -1,0 +1,51 @@
+"""Split-precision form (precision 1: bf16x3 tcgen05 matvecs, FP64 norms and state) against the
+complex FP64 plain form on the same inputs.  The split form is not bit-exact: its tolerances are
+stated per test.  Trajectories whose norm crosses its threshold in a different bisection bin
+diverge, so trajectory-level comparisons use the trajectories whose jump counts agree."""
+import numpy as np
+import pytest
+
+from tests.helpers import dimer_problem, start_states
+
+pytestmark = pytest.mark.gpu
+
+
+def run(P, n, periods, precision, seed=3):
+    import os_d_b200 as q
+
+    eng = q.Engine(P["U"], P["L"], [1.0], P["HE"], None, P["T"], n, seed=seed, record=1, max_dumps=2, rec_cap=4096,
+                   keep_adr=1, precision=precision)
+    eng.set_states(start_states(n, P["d"], 0, 0))
+    eng.init_thresholds()
+    eng.observe(0, is_start=True)
+    eng.run_periods(periods, dump_at=[periods], dump_base=1)
+    psi, t, eta, jc = eng.states()
+    obs = eng.observables(1, 1)
+    eng.close()
+    return psi, jc, obs
+
+
+def test_split_unitary_dynamics_matches_fp64():
+    # g = 0: no dissipation, no jumps; 2 periods = 8 matvecs per trajectory
+    P = dimer_problem(20, g=0.0)
+    psi_s, jc_s, _ = run(P, 64, 2, 1)
+    psi_d, jc_d, _ = run(P, 64, 2, 0)
+    assert jc_s.sum() == 0 and jc_d.sum() == 0
+    assert np.abs(psi_s - psi_d).max() < 1e-4  # bf16x3 with FP32 accumulation: ~1e-6 per matvec
+    assert np.abs(np.linalg.norm(psi_s, axis=1) - 1).max() < 1e-4
+
+
+@pytest.mark.parametrize("N,n,periods", [(20, 256, 2), (200, 512, 1)])
+def test_split_dissipative_ensemble_close_to_fp64(N, n, periods):
+    P = dimer_problem(N)
+    psi_s, jc_s, o_s = run(P, n, periods, 1)
+    psi_d, jc_d, o_d = run(P, n, periods, 0)
+    assert jc_d.sum() > 0
+    same = jc_s == jc_d
+    assert same.mean() > 0.8, same.mean()
+    # trajectories with the same jump sequence stay close to the FP64 ones
+    dev = np.abs(psi_s[same] - psi_d[same]).max(axis=1)
+    assert np.median(dev) < 1e-3, np.median(dev)
+    # the ensemble mean of <n1 - n2> agrees within the split-form tolerance of this short run
+    m_s, m_d = o_s["mean"][0].mean(), o_d["mean"][0].mean()
+    assert abs(m_s - m_d) < 0.02 * N, (m_s, m_d)
