@@ -76,7 +76,8 @@ typedef struct {
                           oracle); 1: split precision: every d x d matvec runs on the tcgen05 tensor
                           cores as bf16 hi/lo planes with FP32 accumulation (products hi*hi + hi*lo +
                           lo*hi), states, norms, thresholds, jump times and renormalisation stay
-                          FP64.  Needs d <= 256.  QJX has no such mode (its zgemv is FP64). */
+                          FP64.  Needs d <= 256.  QJX has no such mode
+                          (its zgemv is FP64). */
 } qjx_config;
 
 typedef struct {

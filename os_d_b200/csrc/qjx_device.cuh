@@ -93,11 +93,12 @@ struct Params {
     // optional per-CTA trace, accumulated over micro-steps: [grid][kTraceFields] clock64 cycles
     // and counts (null: tracing off)
     long long *trace;
-    // split-precision form: bf16 planes of the real block form [[Re M, -Im M], [Im M, Re M]] of
-    // every matrix, rows/columns interleaved (2r + re/im), in tcgen05 core-matrix order
+    // split-precision form: bf16 hi/lo planes of Re M and Im M of every matrix in tcgen05
+    // core-matrix order
     int split;                    // 0 FP64 plain form, 1 split bf16x3
-    int MDs, KS;                  // complex rows padded to 16 (one MMA N-half), k-steps of 8 complex
-    const unsigned char *usplit;  // [G][KS][kPlanes][2 MDs rows x 16 k] bf16
+    int MDs, KS;                  // rows padded to 16 (MMA N), k-steps of 16 complex components
+    int sstages;                  // depth of the split kernel's operand ring
+    const unsigned char *usplit;  // [G][KS][4 planes: Re hi, Re lo, Im hi, Im lo][MDs rows x 16 k] bf16
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns

@@ -26,7 +26,8 @@ cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
 cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
 cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
 cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st);
-size_t split_smem_bytes(int MDs);
+size_t split_smem_bytes(int MDs, int MD, int stages);
+size_t split_stage_bytes(int MDs);
 }  // namespace qjx
 
 using namespace qjx;
@@ -130,30 +131,29 @@ static uint16_t bf16_round(double x, double *val)
     return (uint16_t)(b >> 16);
 }
 
-// bf16 hi/lo planes of the real block form of a row-major complex d x d matrix, in the order the
-// split-precision kernel loads them: out[ks][plane][2 MDs rows x 16 k] with row n = 2 r + (Re, Im
-// of output r), k index kk = 2 k + (Re, Im of input k), core matrices of 8 rows x 8 k (16 bytes
-// a row), K-halves 64 elements apart and 8-row groups 128 elements apart.
+// bf16 planes of a row-major complex d x d matrix in the order the split-precision kernel loads
+// them: out[ks][plane][MDs rows x 16 k], planes Re hi, Re lo, Im hi, Im lo, k-step ks covering
+// k = 16 ks .. 16 ks + 15; core matrices of 8 rows x 8 k (16 bytes a row), K-halves 64 elements
+// apart and 8-row groups 128 elements apart (zero padded beyond d).
 static void pack_split(const double *M, int d, int MDs, int KS, uint16_t *out)
 {
-    const int NP = 2 * MDs;
-    const size_t plane = (size_t)NP * 16;
+    const size_t plane = (size_t)MDs * 16;
     for (int ks = 0; ks < KS; ks++)
-        for (int n = 0; n < NP; n++)
+        for (int r = 0; r < MDs; r++)
             for (int j = 0; j < 16; j++) {
-                const int kk = 16 * ks + j, k = kk >> 1, r = n >> 1;
-                double a = 0.0;
+                const int k = 16 * ks + j;
+                double re = 0.0, im = 0.0;
                 if (r < d && k < d) {
-                    const double mr = M[2 * ((size_t)r * d + k)], mi = M[2 * ((size_t)r * d + k) + 1];
-                    if ((n & 1) == 0) a = (kk & 1) ? -mi : mr;
-                    else a = (kk & 1) ? mr : mi;
+                    re = M[2 * ((size_t)r * d + k)];
+                    im = M[2 * ((size_t)r * d + k) + 1];
                 }
                 double hv = 0.0, lv = 0.0;
-                const uint16_t hb = bf16_round(a, &hv);
-                const uint16_t lb = bf16_round(a - hv, &lv);
-                const size_t off = (size_t)(n & 7) * 8 + (size_t)(n >> 3) * 128 + (size_t)(j >> 3) * 64 + (j & 7);
-                out[(size_t)ks * 2 * plane + off] = hb;
-                out[(size_t)ks * 2 * plane + plane + off] = lb;
+                const size_t off = (size_t)(r & 7) * 8 + (size_t)(r >> 3) * 128 + (size_t)(j >> 3) * 64 + (j & 7);
+                uint16_t *o = out + (size_t)ks * 4 * plane + off;
+                o[0] = bf16_round(re, &hv);
+                o[plane] = bf16_round(re - hv, &lv);
+                o[2 * plane] = bf16_round(im, &hv);
+                o[3 * plane] = bf16_round(im - hv, &lv);
             }
 }
 
@@ -230,11 +230,15 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     if (c.precision == 1) {  // split precision: bf16 planes of every matrix in the tcgen05 order
         P.split = 1;
         P.MDs = 16 * ((d + 15) / 16);
-        P.KS = (d + 7) / 8;
+        P.KS = (d + 15) / 16;
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
-        if (split_smem_bytes(P.MDs) + 4096 > (size_t)optin) return bail(QJX_ERR_UNSUPPORTED);
-        const size_t per_s = (size_t)P.KS * 2 * (2 * P.MDs) * 16;
+        // deepest operand ring (2..8 stages) that fits next to 4 KB of static shared memory
+        P.sstages = 0;
+        for (int st = 8; st >= 2 && !P.sstages; st--)
+            if (split_smem_bytes(P.MDs, MD, st) + 4096 <= (size_t)optin) P.sstages = st;
+        if (!P.sstages) return bail(QJX_ERR_UNSUPPORTED);
+        const size_t per_s = (size_t)P.KS * 4 * P.MDs * 16;
         std::vector<uint16_t> hs((size_t)G * per_s, 0);
         for (int b = 0; b < c.num_branches; b++)
             for (int l = 0; l < c.deep; l++)

@@ -512,13 +512,15 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = P.G, n = P.n, d = P.d;
-    const int *cnt_cur = P.cnt + (s % 3) * G;
+    __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
     const int *list_cur = P.lists + (size_t)(s & 1) * G * n;
     int *list_next = P.lists + (size_t)((s + 1) & 1) * G * n;
 
+    for (int i = tid; i < G; i += kThreads) cnt_cur[i] = P.cnt[(s % 3) * G + i];
     if (blockIdx.x == 0)
         for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
+    __syncthreads();
     if (tid == 0) {
         int acc = 0, kacc = 0;
         for (int g = 0; g < G; g++) {
@@ -936,7 +938,7 @@ cudaError_t launch_clear_records(const Params &P, cudaStream_t st)
 
 cudaError_t launch_split_step(const Params &P, int s, int grid, cudaStream_t st)
 {
-    const size_t smem = split_smem_bytes(P.MDs);
+    const size_t smem = split_smem_bytes(P.MDs, P.MD, P.sstages);
     static int attr_bytes = 0;
     if (attr_bytes < (int)smem) {
         cudaError_t e = cudaFuncSetAttribute(split_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -2,39 +2,44 @@
 //
 // Same lock-step micro-steps, buckets and trajectory state machine as the FP64 plain form;
 // only the d x d complex matvec changes.  Roles are transposed against the FP64 kernel so that
-// the trajectory, not the matrix row, is the MMA M dimension:
+// the trajectory, not the matrix row, is the MMA M dimension, and the complex product is four
+// real GEMMs sharing operands:
 //
-//   D[m][n] = sum_kk A[m][kk] B[n][kk]      m: trajectory of the tile (128 = TMEM lanes)
-//                                           n: 2 r + {0, 1}  (Re, Im of output row r)
-//                                          kk: 2 k + {0, 1}  (Re, Im of input component k)
-//   A = the tile's states as bf16 planes (written by the CTA from the FP64 states),
-//   B = the real block form [[Re M, -Im M], [Im M, Re M]] of the bucket's matrix, rows and
-//       columns interleaved, as bf16 planes prepared once by the host,
-//   D = FP32 accumulator in tensor memory, 2 MDs columns (two MMA N-halves of MDs each).
+//   Re y[m][r] = sum_k Xr[m][k] Ur[r][k] - Xi[m][k] Ui[r][k]     m: trajectory (128 TMEM lanes)
+//   Im y[m][r] = sum_k Xr[m][k] Ui[r][k] + Xi[m][k] Ur[r][k]     r: output row (MMA N = MDs)
+//
+//   A = the tile's states (Xr, Xi) as bf16 planes, written by the CTA from the FP64 states,
+//   B = Re M and Im M as bf16 planes prepared once by the host,
+//   D = two FP32 accumulators in tensor memory, Re in columns [0, MDs), Im in [MDs, 2 MDs);
+//       the minus sign is the instruction descriptor's negate-A bit.
 //
 // Every operand x is split x = hi + lo with hi = bf16(x), lo = bf16(x - hi); the MMAs add
 // hi*hi + hi*lo + lo*hi in FP32 ("bf16x3"), which leaves about 2^-16 of relative error per
 // product and the FP32 accumulation error (measured about 4e-6 of max|y| per matvec at
-// d = 201).  The accumulator is read back to FP64 and the FP64 epilogue of the plain form runs
-// unchanged (norm test, jump, renormalisation, observables).
+// d = 201).  The accumulators are read back to FP64 and the FP64 epilogue of the plain form
+// runs unchanged (norm test, jump, renormalisation, observables).
 //
 // Shared-memory operands use the K-major no-swizzle canonical layout: a core matrix is
 // 8 rows x 16 bytes (8 bf16 along K) stored contiguously; within one k-step (16 bf16 of K)
 // the two K-halves of a row group are 128 bytes apart (leading byte offset) and consecutive
 // 8-row groups 256 bytes apart (stride byte offset).  The host writes B in exactly this
-// order, so one k-step of all planes is one contiguous TMA bulk copy.
+// order, so one k-step of all four B planes is one contiguous TMA bulk copy.
 //
-// Per tile (one matrix, up to 128 trajectories) and k-step, a 3-stage ring:
-//   warps 0-3   one thread per trajectory row: FP64 state -> bf16 planes of A (generic
+// Per tile (one matrix, up to 128 trajectories) a ring of S stages (as many as shared memory
+// holds, 5 at d = 201), one k-step of A and B planes each:
+//   warps 0-3, 6-9, 10-13   three producer groups, one thread per trajectory row; group p
+//               converts the k-steps ks = p (mod 3): FP64 state -> bf16 planes of A (generic
 //               stores, then fence.proxy.async and an arrive on fullA)
 //   warp 4      one thread issues the bulk copy of the B planes (complete_tx on fullB)
-//   warp 5      one thread issues the 2 x 3 tcgen05.mma and commits them to empty[stage]
-// then the accumulator (commit to accf) is read by the warps whose TMEM lane quarter holds
-// each group of 32 trajectories, staged as FP64 columns, and run through column_epilogue.
+//   warp 5      one thread issues the 12 tcgen05.mma of a k-step and commits them to empty[stage]
+// then the accumulators (commit to accf) are read by the warps whose TMEM lane quarter holds
+// each group of 32 trajectories, staged as FP64 columns in the (now idle) ring, and run
+// through column_epilogue.  Rows per tile are chosen per micro-step so that the tiles fit
+// one wave of CTAs.
 
-constexpr int kPlanes = 2;                   // bf16 hi, lo
-constexpr int kTileM = 128;                  // trajectories per tile (TMEM lanes, MMA M)
-constexpr int kSStages = 3;                  // operand ring depth
+constexpr int kAPlanes = 4;                  // A and B planes: Re hi, Re lo, Im hi, Im lo
+constexpr int kTileM = 128;                  // MMA M = TMEM lanes (a tile holds up to 128 trajectories)
+constexpr int kMaxSStages = 8;               // operand ring depth (runtime: as deep as shared memory allows)
 constexpr int kABytes = kTileM * 32;         // one plane of one k-step of A: 128 rows x 16 bf16
 constexpr int kTmemCols = 512;
 constexpr long long kSplitWait = 1ll << 20;  // bounded mbarrier polls (normal waits end within microseconds)
@@ -96,75 +101,86 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
     v[7] = __uint_as_float(r7);
 }
 
-// bf16 round-to-nearest-even of a double (through the exact FP32 value when it is exact,
-// else rounding the double once to bf16 precision); returns the 16-bit pattern.
-__device__ __forceinline__ uint32_t bf16_bits(double x)
-{
-    return (uint32_t)__bfloat16_as_ushort(__double2bfloat16(x));
-}
-
-__device__ __forceinline__ double bf16_value(uint32_t b)
-{
-    return (double)__uint_as_float(b << 16);
-}
-
-// hi/lo planes of one (re, im) pair packed as two bf16 (re in the low half: lower address).
+// hi/lo planes of one (re, im) pair packed as two bf16 (re in the low half: lower address):
+// hi = bf16(f), lo = bf16(f - hi) with f the FP32 rounding of the FP64 value (f - hi is exact in
+// FP32; the FP32 rounding, 2^-24, is far below the 2^-17 the two planes resolve).
 __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo)
 {
-    const uint32_t hr = bf16_bits(v.x), hm = bf16_bits(v.y);
-    const uint32_t lr = bf16_bits(v.x - bf16_value(hr)), lm = bf16_bits(v.y - bf16_value(hm));
-    hi = hr | (hm << 16);
-    lo = lr | (lm << 16);
+    const float fr = __double2float_rn(v.x), fi = __double2float_rn(v.y);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(fr, fi);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(fr - hf.x, fi - hf.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-size_t split_smem_bytes(int MDs)
+// Dynamic shared memory: a ring of `stages` operand stages, each [A planes][B planes] of one
+// k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs+1))
+// followed by the per-warp epilogue scratch (16 x MD).
+size_t split_stage_bytes(int MDs) { return (size_t)kAPlanes * (kABytes + (size_t)MDs * 32); }
+
+size_t split_smem_bytes(int MDs, int MD, int stages)
 {
-    const size_t bbytes = (size_t)2 * MDs * 32;
-    return (size_t)kSStages * kPlanes * (kABytes + bbytes) + (size_t)32 * (MDs + 1) * sizeof(double2);
+    const size_t ring = (size_t)stages * split_stage_bytes(MDs);
+    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2) + (size_t)(kThreads / 32) * MD * sizeof(double2);
+    return ring > epi ? ring : epi;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P, int s)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int MDs = P.MDs, KS = P.KS, NP = 2 * MDs;
-    const int bbytes = NP * 32;  // one plane of one k-step of B
-    unsigned char *As = smem;                                          // [stage][plane][kABytes]
-    unsigned char *Bs = As + kSStages * kPlanes * kABytes;            // [stage][plane][bbytes]
+    const int MDs = P.MDs, KS = P.KS, S = P.sstages;
+    const int bbytes = MDs * 32;                               // one plane of one k-step of B
+    const size_t stage_bytes = (size_t)kAPlanes * (kABytes + bbytes);
     const int S16 = MDs + 1;
-    double2 *Bt = reinterpret_cast<double2 *>(Bs + (size_t)kSStages * kPlanes * bbytes);  // [32][S16]
-    __shared__ __align__(8) uint64_t fullA[kSStages], fullB[kSStages], empty[kSStages], accf;
+    double2 *Bt = reinterpret_cast<double2 *>(smem);          // epilogue: [32][S16] FP64 columns
+    double2 *wscr = Bt + 32 * S16 + (size_t)(threadIdx.x >> 5) * P.MD;
+    __shared__ __align__(8) uint64_t fullA[kMaxSStages], fullB[kMaxSStages], empty[kMaxSStages], accf;
     __shared__ uint32_t s_tmem;
     __shared__ int s_tstart[kMaxGroups + 1];
     __shared__ int s_tr[kTileM];
     __shared__ long long s_src[kTileM];
     __shared__ int s_fail;
+    __shared__ int s_rows;  // trajectories per tile in this micro-step
+    __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = P.G, n = P.n, d = P.d;
-    const int *cnt_cur = P.cnt + (s % 3) * G;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
     const int *list_cur = P.lists + (size_t)(s & 1) * G * n;
     int *list_next = P.lists + (size_t)((s + 1) & 1) * G * n;
 
+    for (int i = tid; i < G; i += kThreads) cnt_cur[i] = P.cnt[(s % 3) * G + i];
     if (blockIdx.x == 0)
         for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
-    if (tid == 0) {
-        int acc = 0;
-        for (int g = 0; g < G; g++) {
-            s_tstart[g] = acc;
-            acc += (cnt_cur[g] + kTileM - 1) / kTileM;
+    __syncthreads();
+    if (warp == 0) {
+        // rows per tile: the smallest multiple of 8 (<= 128) whose tiles fit one wave of CTAs, so
+        // the trajectories (and their epilogues) spread over all SMs; 128 when none does
+        int tiles = 0;
+        if (lane < 16)
+            for (int g = 0; g < G; g++) tiles += (cnt_cur[g] + 8 * lane + 7) / (8 * lane + 8);
+        const unsigned fit = __ballot_sync(0xffffffffu, lane < 16 && tiles <= (int)gridDim.x);
+        const int R = fit ? 8 * (__ffs(fit)) : kTileM;
+        if (lane == 0) {
+            s_rows = R;
+            int acc = 0;
+            for (int g = 0; g < G; g++) {
+                s_tstart[g] = acc;
+                acc += (cnt_cur[g] + R - 1) / R;
+            }
+            s_tstart[G] = acc;
+            for (int q = 0; q < S; q++) {
+                mbar_init(&fullA[q], kTileM);
+                mbar_init(&fullB[q], 1);
+                mbar_init(&empty[q], 1);
+            }
+            mbar_init(&accf, 1);
+            s_fail = 0;
+            fence_proxy_async();
         }
-        s_tstart[G] = acc;
-        for (int q = 0; q < kSStages; q++) {
-            mbar_init(&fullA[q], kTileM);
-            mbar_init(&fullB[q], 1);
-            mbar_init(&empty[q], 1);
-        }
-        mbar_init(&accf, 1);
-        s_fail = 0;
-        fence_proxy_async();
-    }
-    if (warp == 0) {  // the whole tensor memory of the SM (one CTA per SM)
+        __syncwarp();
+        // the whole tensor memory of the SM (one CTA per SM)
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"((uint32_t)kTmemCols)
                      : "memory");
@@ -176,11 +192,15 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const uint32_t tmem = s_tmem;
     const int T = s_tstart[G];
     const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
+    const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
     long long work = 0;
     uint32_t ntile = 0;
     bool ok = true;
+    long long tr_setup = 0, tr_mma = 0, tr_stage = 0, tr_epi = 0;
+    const long long t_begin = clock64();
 
     for (int t = blockIdx.x; t < T && ok; t += gridDim.x, ntile++) {
+        const long long t0 = clock64();
         int lo = 0, hi = G;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -188,8 +208,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             else hi = mid;
         }
         const int g = lo;
-        const int base = (t - s_tstart[g]) * kTileM;
-        const int rows = min(kTileM, cnt_cur[g] - base);
+        const int base = (t - s_tstart[g]) * s_rows;
+        const int rows = min(s_rows, cnt_cur[g] - base);
         if (tid < kTileM) {
             if (tid < rows) {
                 const int tr = list_cur[(size_t)g * n + base + tid];
@@ -203,74 +223,95 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             }
         }
         __syncthreads();
+        const long long t1 = clock64();
         const uint32_t it0 = ntile * (uint32_t)KS;  // k-steps issued before this tile
 
-        if (warp < 4) {
-            // A producer: thread m writes row m of every k-step
-            const int m = tid;
+        const int agrp = (warp < 4) ? 0 : (warp >= 6 && warp < 10) ? 1 : (warp >= 10 && warp < 14) ? 2 : -1;
+        if (agrp >= 0) {
+            // A producers: group p (4 warps, thread m = row m) handles the k-steps ks = p (mod 3), so
+            // three independent load-convert chains run in parallel; each thread issues its loads
+            // before waiting for the stage to drain
+            const int m = tid - (agrp == 0 ? 0 : (agrp == 1 ? 192 : 320));
             const double2 *src = (s_src[m] >= 0) ? P.psi + s_src[m] : nullptr;
             const int off = (m & 7) * 16 + (m >> 3) * 256;
-            for (int ks = 0; ks < KS && ok; ks++) {
-                const uint32_t it = it0 + ks, q = it % kSStages;
-                if (it >= kSStages && !mbar_wait_bounded(&empty[q], ((it / kSStages) - 1) & 1u, kSplitWait)) ok = false;
-                uint32_t h[8], l[8];
+            for (int ks = agrp; ks < KS && ok; ks += 3) {
+                const uint32_t it = it0 + ks, q = it % S;
+                unsigned char *As = smem + q * stage_bytes + off;
+                for (int hh = 0; hh < 2; hh++) {  // K-halves: components 16 ks + 8 hh .. + 7
+                    double2 v[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const int k = 8 * ks + i;
-                    const double2 v = (src && k < d) ? src[k] : make_double2(0.0, 0.0);
-                    split_pair(v, h[i], l[i]);
+                    for (int i = 0; i < 8; i++) {
+                        const int k = 16 * ks + 8 * hh + i;
+                        v[i] = (src && k < d) ? src[k] : make_double2(0.0, 0.0);
+                    }
+                    if (hh == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
+                        ok = false;
+                    uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        split_pair(make_double2(v[2 * j].x, v[2 * j + 1].x), rh[j], rl[j]);
+                        split_pair(make_double2(v[2 * j].y, v[2 * j + 1].y), ih[j], il[j]);
+                    }
+                    *reinterpret_cast<uint4 *>(As + 128 * hh) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                    *reinterpret_cast<uint4 *>(As + kABytes + 128 * hh) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                    *reinterpret_cast<uint4 *>(As + 2 * kABytes + 128 * hh) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                    *reinterpret_cast<uint4 *>(As + 3 * kABytes + 128 * hh) = make_uint4(il[0], il[1], il[2], il[3]);
                 }
-                uint4 *ah = reinterpret_cast<uint4 *>(As + (q * kPlanes + 0) * kABytes + off);
-                uint4 *al = reinterpret_cast<uint4 *>(As + (q * kPlanes + 1) * kABytes + off);
-                ah[0] = make_uint4(h[0], h[1], h[2], h[3]);
-                ah[8] = make_uint4(h[4], h[5], h[6], h[7]);  // +128 bytes: second K-half
-                al[0] = make_uint4(l[0], l[1], l[2], l[3]);
-                al[8] = make_uint4(l[4], l[5], l[6], l[7]);
                 fence_proxy_async();
                 mbar_arrive(&fullA[q]);
             }
         } else if (warp == 4) {
             if (lane == 0) {  // B producer
-                const unsigned char *ug = P.usplit + (size_t)g * KS * kPlanes * bbytes;
+                const unsigned char *ug = P.usplit + (size_t)g * KS * kAPlanes * bbytes;
                 for (int ks = 0; ks < KS && ok; ks++) {
-                    const uint32_t it = it0 + ks, q = it % kSStages;
-                    if (it >= kSStages && !mbar_wait_bounded(&empty[q], ((it / kSStages) - 1) & 1u, kSplitWait)) {
+                    const uint32_t it = it0 + ks, q = it % S;
+                    if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait)) {
                         ok = false;
                         break;
                     }
-                    mbar_expect_tx(&fullB[q], (uint32_t)(kPlanes * bbytes));
-                    bulk_g2s(Bs + (size_t)q * kPlanes * bbytes, ug + (size_t)ks * kPlanes * bbytes,
-                             (uint32_t)(kPlanes * bbytes), &fullB[q]);
+                    mbar_expect_tx(&fullB[q], (uint32_t)(kAPlanes * bbytes));
+                    bulk_g2s(smem + q * stage_bytes + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes,
+                             (uint32_t)(kAPlanes * bbytes), &fullB[q]);
                 }
             }
         } else if (warp == 5) {
             if (lane == 0) {  // MMA issuer
                 for (int ks = 0; ks < KS && ok; ks++) {
-                    const uint32_t it = it0 + ks, q = it % kSStages, par = (it / kSStages) & 1u;
+                    const uint32_t it = it0 + ks, q = it % S, par = (it / S) & 1u;
                     if (!mbar_wait_bounded(&fullA[q], par, kSplitWait) || !mbar_wait_bounded(&fullB[q], par, kSplitWait)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t a0 = smem_u32(As + (q * kPlanes + 0) * kABytes);
-                    const uint32_t a1 = smem_u32(As + (q * kPlanes + 1) * kABytes);
-                    const uint32_t b0 = smem_u32(Bs + (size_t)(q * kPlanes + 0) * bbytes);
-                    const uint32_t b1 = smem_u32(Bs + (size_t)(q * kPlanes + 1) * bbytes);
-#pragma unroll
-                    for (int hn = 0; hn < 2; hn++) {
-                        const uint32_t bo = (uint32_t)hn * (uint32_t)(MDs / 8) * 256u;  // N-half: MDs rows
-                        const uint32_t dcol = tmem + (uint32_t)(hn * MDs);
-                        umma_bf16(dcol, umma_desc_kmajor(a0), umma_desc_kmajor(b0 + bo), idesc, ks > 0 ? 1u : 0u);
-                        umma_bf16(dcol, umma_desc_kmajor(a0), umma_desc_kmajor(b1 + bo), idesc, 1u);
-                        umma_bf16(dcol, umma_desc_kmajor(a1), umma_desc_kmajor(b0 + bo), idesc, 1u);
-                    }
+                    const uint32_t a = smem_u32(smem + q * stage_bytes);
+                    const uint64_t xrh = umma_desc_kmajor(a), xrl = umma_desc_kmajor(a + kABytes);
+                    const uint64_t xih = umma_desc_kmajor(a + 2 * kABytes), xil = umma_desc_kmajor(a + 3 * kABytes);
+                    const uint32_t b = a + kAPlanes * kABytes;
+                    const uint64_t urh = umma_desc_kmajor(b), url = umma_desc_kmajor(b + bbytes);
+                    const uint64_t uih = umma_desc_kmajor(b + 2 * bbytes), uil = umma_desc_kmajor(b + 3 * bbytes);
+                    const uint32_t acc = ks > 0 ? 1u : 0u;
+                    const uint32_t dre = tmem, dim = tmem + (uint32_t)MDs;
+                    // Re y += Xr Ur - Xi Ui
+                    umma_bf16(dre, xrh, urh, idesc, acc);
+                    umma_bf16(dre, xrh, url, idesc, 1u);
+                    umma_bf16(dre, xrl, urh, idesc, 1u);
+                    umma_bf16(dre, xih, uih, idesc_neg, 1u);
+                    umma_bf16(dre, xih, uil, idesc_neg, 1u);
+                    umma_bf16(dre, xil, uih, idesc_neg, 1u);
+                    // Im y += Xr Ui + Xi Ur
+                    umma_bf16(dim, xrh, uih, idesc, acc);
+                    umma_bf16(dim, xrh, uil, idesc, 1u);
+                    umma_bf16(dim, xrl, uih, idesc, 1u);
+                    umma_bf16(dim, xih, urh, idesc, 1u);
+                    umma_bf16(dim, xih, url, idesc, 1u);
+                    umma_bf16(dim, xil, urh, idesc, 1u);
                     umma_commit(&empty[q]);  // frees the stage once these MMAs have read it
                 }
                 umma_commit(&accf);
             }
         }
         if (!ok) atomicExch(&s_fail, 1);
-        // accumulator complete (every thread waits on the commit)
+        // accumulator complete (every thread waits on the commit); the ring is free afterwards
         if (!mbar_wait_bounded(&accf, ntile & 1u, kSplitWait)) atomicExch(&s_fail, 1);
         tc_fence_after();
         __syncthreads();
@@ -278,28 +319,35 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             ok = false;
             break;
         }
-        double2 *wscr = reinterpret_cast<double2 *>(Bs) + (size_t)warp * P.MD;  // B ring is free now
+        const long long t2 = clock64();
         for (int c = 0; c < 4 && 32 * c < rows; c++) {
+            const long long ts = clock64();
             if ((warp & 3) == c) {  // TMEM lanes 32c..32c+31 belong to warps c, c+4, c+8, c+12
-                const int part = warp >> 2, ncol = NP / 4;
-                for (int col = part * ncol; col < (part + 1) * ncol; col += 8) {
-                    float v[8];
-                    tmem_ld8(tmem + ((uint32_t)(32 * c) << 16) + (uint32_t)col, v);
-                    double2 *dst = Bt + (size_t)lane * S16 + col / 2;
+                const uint32_t lanes = tmem + ((uint32_t)(32 * c) << 16);
+                for (int r0 = 8 * (warp >> 2); r0 < MDs; r0 += 32) {  // 8 output rows at a time
+                    float vr[8], vi[8];
+                    tmem_ld8(lanes + (uint32_t)r0, vr);
+                    tmem_ld8(lanes + (uint32_t)(MDs + r0), vi);
+                    double2 *dst = Bt + (size_t)lane * S16 + r0;
 #pragma unroll
-                    for (int i = 0; i < 4; i++) dst[i] = make_double2((double)v[2 * i], (double)v[2 * i + 1]);
+                    for (int i = 0; i < 8; i++) dst[i] = make_double2((double)vr[i], (double)vi[i]);
                 }
             }
             tc_fence_before();
             __syncthreads();
+            tr_stage += clock64() - ts;
             for (int cc = warp; cc < 32; cc += kThreads / 32) {
                 const int m = 32 * c + cc;
                 if (m < rows) column_epilogue(P, Bt + (size_t)cc * S16, wscr, s_tr[m], cnt_next, list_next, lane);
             }
-            fence_proxy_async();
+            fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
             __syncthreads();
         }
         work += rows;
+        const long long t3 = clock64();
+        tr_setup += t1 - t0;
+        tr_mma += t2 - t1;
+        tr_epi += t3 - t2;
     }
 
     if (!ok) {
@@ -309,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             mbar_wait_bounded(&accf, ntile & 1u, kSplitWait);
         }
         if (warp == 4 && lane == 0)
-            for (int q = 0; q < kSStages; q++) {
+            for (int q = 0; q < S; q++) {
                 mbar_wait_bounded(&fullB[q], 0u, 1024);
                 mbar_wait_bounded(&fullB[q], 1u, 1024);
             }
@@ -326,4 +374,14 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                      : "memory");
     }
     if (tid == 0 && work) atomicAdd((unsigned long long *)P.work, (unsigned long long)work);
+    if (P.trace && tid == 0) {  // fields: total, setup, -, MMA phase, epilogue, tiles, TMEM staging, rows
+        long long *tr = P.trace + (size_t)blockIdx.x * kTraceFields;
+        tr[0] += clock64() - t_begin;
+        tr[1] += tr_setup;
+        tr[3] += tr_mma;
+        tr[4] += tr_epi;
+        tr[5] += ntile;
+        tr[6] += tr_stage;
+        tr[7] += work;
+    }
 }
