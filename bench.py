@@ -13,6 +13,10 @@ job).  Metric: trajectory-periods per second over all GPUs.
 Multi-GPU: one process per GPU (torchrun); trajectories are sharded (rank r owns global
 trajectories r*n .. r*n+n-1, so the ensemble is the one a single GPU would run), the
 ensemble sums of the observables are all-reduced over NCCL once per step.
+
+The same protocol then times the split-precision form (bf16x3 matvecs on the tcgen05 tensor
+cores, FP64 states and norms) on the same inputs; it is reported beside the plain form as
+"split_form" with its speed-up and its deviation from the plain form's ensemble <n1 - n2>.
 """
 import argparse
 import json
@@ -47,6 +51,7 @@ def parse():
     ap.add_argument("--periods-per-step", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision form")
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
     return ap.parse_args()
 
@@ -210,46 +215,58 @@ def run_ours(args):
     M = model()
     n, d, P = args.n_traj, M["d"], args.periods_per_step
     steps_total = args.warmup + args.steps
-    eng = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, record=0, rec_cap=16,
-                   keep_adr=0, max_dumps=steps_total + 1, device=local, tr_base=rank * n)
     psi0 = start_states(n, d)
-    eng.set_states(psi0)
-    eng.init_thresholds()
-    eng.reset_times()
-    eng.observe(0, is_start=True)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def new_engine(precision):
+        e = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, record=0, rec_cap=16,
+                     keep_adr=0, max_dumps=steps_total + 1, device=local, tr_base=rank * n, precision=precision)
+        e.set_states(psi0)
+        e.init_thresholds()
+        e.reset_times()
+        e.observe(0, is_start=True)
+        return e
+
+    def timed_run(eng, clocks=None):
+        """W untimed + K timed steps of P periods; device time of the K steps (max over ranks),
+        stats before/after, and the ensemble <n1 - n2> with its standard error after every step."""
+        def one_step(slot):
+            eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=slot)
+            x = N_BOSONS - 2.0 * eng.observables(slot, 1)["mean"][0]
+            # ensemble sums reduced over ranks (the one exchange of the path)
+            s = allreduce([float(np.sum(x)), float(np.sum(x * x)), float(n)])
+            m = s[0] / s[2]
+            return m, float(np.sqrt(max(s[1] / s[2] - m * m, 0.0) / s[2]))
+
+        ens = [one_step(1 + w) for w in range(args.warmup)]
+        st0 = eng.stats()
+        barrier()
+        if clocks:
+            clocks.start()
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps
+            torch.cuda.synchronize()
+            ens.append(one_step(1 + args.warmup + k))
+            dev_ms += eng.stats()["last_call_ms"]
+        barrier()
+        wall = time.perf_counter() - t0
+        clk = clocks.stop() if clocks else None
+        return float(allreduce([dev_ms], "max")[0]), wall, clk, st0, eng.stats(), ens
+
+    eng = new_engine(0)
     if args.profile:
+        if os.environ.get("QJX_BENCH_PRECISION") == "split":
+            eng.close()
+            eng = new_engine(1)
         eng.run_periods(1, is_obs=1)
         eng.close()
         return
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-
-    def one_step(slot):
-        eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=slot)
-        ob = eng.observables(slot, 1)
-        # ensemble <n1 - n2> = N - 2 mean, reduced over ranks (the one exchange of the path)
-        return allreduce([float(np.sum(N_BOSONS - 2.0 * ob["mean"][0])), float(n)])
-
-    for w in range(args.warmup):
-        one_step(1 + w)
-    st0 = eng.stats()
-    clocks = ClockSampler(local)
-    barrier()
-    clocks.start()
-    t0 = time.perf_counter()
-    dev_ms = 0.0
-    ens_sum = None
-    for k in range(args.steps):
-        flush.zero_()  # L2 flush between timed steps
-        torch.cuda.synchronize()
-        ens_sum = one_step(1 + args.warmup + k)
-        dev_ms += eng.stats()["last_call_ms"]
-    barrier()
-    wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    st1 = eng.stats()
-    dev_ms_max = float(allreduce([dev_ms], "max")[0])
+    dev_ms_max, wall, clk, st0, st1, ens_plain = timed_run(eng, ClockSampler(local))
     value = world * n * P * args.steps / (dev_ms_max * 1e-3)
     ms_per_step = dev_ms_max / args.steps
+    ens_sum = ens_plain[-1]
 
     # roofline of the dominant kernel (step_kernel, grouped FP64 complex GEMM + fused epilogue)
     matvecs = st1["matvecs"] - st0["matvecs"]
@@ -283,8 +300,40 @@ def run_ours(args):
                    "l2": "flushed between timed steps (256 MB write)"},
         "wall_s": wall, "roofline": roofline, "clocks": clk,
         "gpu_launches": int(st1["launches"] - st0["launches"]),
-        "ensemble_n1_minus_n2": float(ens_sum[0] / ens_sum[1]) if ens_sum is not None else None,
+        "ensemble_n1_minus_n2": ens_sum[0], "ensemble_n1_minus_n2_stderr": ens_sum[1],
     }
+
+    # split-precision form on the same inputs and protocol
+    if not args.no_split:
+        eng_s = new_engine(1)
+        ms_s, _, _, s0, s1, ens_split = timed_run(eng_s)
+        eng_s.close()
+        v_s = world * n * P * args.steps / (ms_s * 1e-3)
+        tiles = s1["mma_tiles"] - s0["mma_tiles"]
+        mds, ks = 16 * ((d + 15) // 16), (d + 15) // 16
+        exec_flops = tiles * ks * 12 * 2.0 * 128 * mds * 16
+        kern_s = (s1["step_kernel_ms"] - s0["step_kernel_ms"]) * 1e-3
+        peaks = {}
+        pk_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(pk_file):
+            with open(pk_file) as f:
+                peaks = json.load(f)
+        bf16_peak = peaks.get("bf16_tflops", 1590.0)
+        diffs = [abs(a[0] - b[0]) for a, b in zip(ens_split, ens_plain)]
+        line["split_form"] = {
+            "metric": METRIC, "value": v_s, "unit": METRIC, "ms_per_step": ms_s / args.steps,
+            "speedup_vs_plain": v_s / value, "dtype": "bf16x3 matvec (FP32 accumulate), FP64 state and norms",
+            "n1_minus_n2_abs_diff_vs_plain_per_step": diffs,
+            "n1_minus_n2_stderr_per_step": [b[1] for b in ens_plain],
+            "periods_per_step": P,
+            "roofline": {"bound": "tensor", "kernel": "qjx::split_step_kernel",
+                         "achieved": exec_flops / kern_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
+                         "frac": exec_flops / kern_s / 1e12 / bf16_peak,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)" if peaks else "fallback 1590",
+                         "flops": "executed tcgen05 bf16 flops: 12 MMAs of 128 x MDs x 16 per k-step and tile",
+                         "algorithmic_tflops": 8.0 * d * d * (s1["matvecs"] - s0["matvecs"]) / kern_s / 1e12},
+            "gpu_launches": int(s1["launches"] - s0["launches"]),
+        }
 
     # e2e through the public C ABI with host buffers, copies inside the timed region
     if not args.no_e2e:
@@ -307,7 +356,7 @@ def run_ours(args):
                                "qjx_get_states per step"}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample = 8 * threads  # ~10-30 s of CPU work
+        sample = 128 * threads  # about 15 s of CPU work
         rate, dt, mv = cpu_rate(M, sample, 1, threads)
         line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
                                 "sample": f"{sample} trajectories x 1 period at dim 201 ({dt:.1f} s), "

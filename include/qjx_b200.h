@@ -88,6 +88,7 @@ typedef struct {
     double last_call_ms;     /* device time of the last run/observe call */
     double step_kernel_ms;   /* device time of the micro-step kernel batches alone (CUDA events) */
     int64_t launches;        /* kernels launched by the engine */
+    int64_t mma_tiles;       /* split form: 128-row tcgen05 tiles (12 MMAs of 128 x MDs x 16 per k-step) */
 } qjx_stats;
 
 /* U: [num_branches][deep][d][d] split propagators exp(K_b dt_l), dt_l = T 2^-(l+2).

@@ -35,7 +35,7 @@ class QjxConfig(C.Structure):
 class QjxStats(C.Structure):
     _fields_ = [("micro_steps", C.c_int64), ("matvecs", C.c_int64), ("jumps", C.c_int64),
                 ("kernel_ms", C.c_double), ("last_call_ms", C.c_double), ("step_kernel_ms", C.c_double),
-                ("launches", C.c_int64)]
+                ("launches", C.c_int64), ("mma_tiles", C.c_int64)]
 
 
 _lib = None

@@ -466,8 +466,8 @@ static qjx_status run_until_idle(qjx_engine *h)
     FILE *bucket_log = nullptr;
     if (const char *fn = getenv("QJX_TRACE_BUCKETS")) bucket_log = fopen(fn, "a");
     int64_t steps = 0;
-    long long work0 = 0;
-    cudaMemcpy(&work0, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
+    long long work0[2] = {0, 0};
+    cudaMemcpy(work0, P.work, 2 * sizeof(long long), cudaMemcpyDeviceToHost);
     cudaEventRecord(h->ev0, h->stream);
     while (true) {
         cudaEventRecord(h->eb0, h->stream);
@@ -526,9 +526,10 @@ static qjx_status run_until_idle(qjx_engine *h)
     h->stats.last_call_ms = ms;
     h->stats.micro_steps += steps;
     h->stats.launches += steps;
-    long long work1 = 0;
-    cudaMemcpy(&work1, P.work, sizeof(long long), cudaMemcpyDeviceToHost);
-    h->stats.matvecs += work1 - work0;
+    long long work1[2] = {0, 0};
+    cudaMemcpy(work1, P.work, 2 * sizeof(long long), cudaMemcpyDeviceToHost);
+    h->stats.matvecs += work1[0] - work0[0];
+    h->stats.mma_tiles += work1[1] - work0[1];
     cudaGraphExecDestroy(exec);
     return rs;
 }

@@ -374,6 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                      : "memory");
     }
     if (tid == 0 && work) atomicAdd((unsigned long long *)P.work, (unsigned long long)work);
+    if (tid == 0 && ntile) atomicAdd((unsigned long long *)(P.work + 1), (unsigned long long)ntile);
     if (P.trace && tid == 0) {  // fields: total, setup, -, MMA phase, epilogue, tiles, TMEM staging, rows
         long long *tr = P.trace + (size_t)blockIdx.x * kTraceFields;
         tr[0] += clock64() - t_begin;
