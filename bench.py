@@ -52,7 +52,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision form")
+    ap.add_argument("--no-fbasis", action="store_true", help="skip the f-basis Lindblad RK4 measurement")
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
+    ap.add_argument("--profile-target", default="plain", choices=["plain", "split", "fbasis"],
+                    help="what --profile runs: one period of the plain or split form, or one f-basis period")
     return ap.parse_args()
 
 
@@ -135,6 +138,64 @@ def run_reference(args):
         "matvecs_per_traj_period": mv,
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- f-basis Lindblad RK4 (configuration 3)
+FB_N, FB_DT, FB_A = 50, 1e-3, 1.5
+
+
+def fbasis_bench(args, local):
+    """The density-matrix oracle path: dimer N = 50 (f-vector of 2600), RK4 with dt = 1e-3
+    (6284 steps per period), one period per step; device time of qjx_fb_run."""
+    import math
+
+    import scipy.sparse as sp
+
+    import os_d_b200 as q
+    from os_d_b200 import _native as Nt
+
+    (gr, gc, gv), (qr, qc, qv), ks = Nt.fb_build_dimer(FB_N, PRM["J"], PRM["U"], PRM["E"], PRM["g"])
+    n = ks.size
+    Gs = sp.csr_matrix((gv, gc, gr), shape=(n, n))
+    Qs = sp.csr_matrix((qv, qc, qr), shape=(n, n))
+    T = 2.0 * math.pi
+    steps = math.ceil(T / FB_DT)
+    fb = q.FBasis(Gs, Qs, ks, q.fbasis_pure_state(FB_N, 0), FB_A, T=T, num_steps=steps, device=local)
+    for w in range(args.warmup):
+        fb.run(w, 1)
+    ms = []
+    for k in range(args.steps):
+        fb.run(args.warmup + k, 1)
+        ms.append(fb.get()[1])
+    x = fb.get()[0]
+    cs = fb.cluster_size()
+    fb.close()
+    per = float(np.mean(ms))
+    nnz = Gs.nnz + Qs.nnz
+    step_bytes = 4 * (12.0 * nnz + 24.0 * n)  # CSR operands + stage vectors, 4 stages
+    achieved = step_bytes * steps / (per * 1e-3) / 1e9
+    smem_peak = (cs if cs else 1) * 128 * 1.965e9 / 1e9
+    out = {"workload": f"f-basis Lindblad RK4, dimer N={FB_N} (f-vector {n}), dt={FB_DT} ({steps} steps/period), "
+                       f"Gs nnz {Gs.nnz}, Qs nnz {Qs.nnz}",
+           "metric": "periods/s", "value": 1e3 / per, "ms_per_period": per, "us_per_rk4_step": 1e3 * per / steps,
+           "kernel": "fb::rk4_cluster" if cs else "fb::rk_stage + fb::rk_update", "cluster_size": cs,
+           "roofline": {"bound": "shared memory / cluster barrier latency (operands resident in the cluster's shared "
+                                 "memory, no HBM traffic after the first load)",
+                        "achieved": achieved, "unit": "GB/s", "peak": smem_peak,
+                        "peak_source": "shared-memory bandwidth of the cluster's SMs, 128 B/clk at 1965 MHz",
+                        "frac": achieved / smem_peak, "algorithmic_bytes_per_rk4_step": step_bytes},
+           "purity": float(1.0 / (FB_N + 1) + x @ x)}
+    if not args.no_cpu_baseline:
+        from oracle import oracle_py as O
+
+        csteps = 200
+        t0 = time.perf_counter()
+        O.fb_rk4(Gs, Qs, ks, q.fbasis_pure_state(FB_N, 0), FB_A, T=T, num_steps=csteps, n_periods=1)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / (dt * steps / csteps), "unit": "periods/s", "cores": 1, "kind": "port",
+                               "sample": f"{csteps} RK4 steps of the same system ({dt:.2f} s), "
+                                         f"oracle/fbasis_oracle.c, scaled to {steps} steps per period"}
+    return out
 
 
 # ---------------------------------------------------------------- clocks
@@ -255,11 +316,12 @@ def run_ours(args):
         clk = clocks.stop() if clocks else None
         return float(allreduce([dev_ms], "max")[0]), wall, clk, st0, eng.stats(), ens
 
-    eng = new_engine(0)
+    if args.profile and args.profile_target == "fbasis":
+        args.warmup, args.steps, args.no_cpu_baseline = 0, 1, True
+        fbasis_bench(args, local)
+        return
+    eng = new_engine(1 if args.profile and args.profile_target == "split" else 0)
     if args.profile:
-        if os.environ.get("QJX_BENCH_PRECISION") == "split":
-            eng.close()
-            eng = new_engine(1)
         eng.run_periods(1, is_obs=1)
         eng.close()
         return
@@ -354,6 +416,8 @@ def run_ours(args):
                        "h2d_bytes_per_step": int(n * d * 16), "d2h_bytes_per_step": int(n * d * 16 + 5 * n * 8 + n * 16),
                        "path": "qjx_set_states + qjx_init_thresholds + qjx_run_periods + qjx_get_observables + "
                                "qjx_get_states per step"}
+    if rank == 0 and not args.no_fbasis:
+        line["fbasis"] = fbasis_bench(args, local)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 128 * threads  # about 15 s of CPU work

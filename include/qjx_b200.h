@@ -157,6 +157,14 @@ qjx_status qjx_random_observables(int d, int num, int seed, int mns, int type, d
 
 /* ---- f-basis Lindblad RK4 (density-matrix oracle of the ensemble) ---- */
 typedef struct qjx_fb qjx_fb;
+/* f-basis Liouvillian of the dimer (Gs, Qs_drv in CSR with sorted columns, Ks), the matrices the
+ * reference assembles from structure constants (source/cpp/CQdiss_os_dimer/CQdiss/CalcQs.cpp:141-173,
+ * CalcRs.cpp:385-468, CalcKs.cpp:82-135, CalcGs.cpp:3-11) for the f-basis operators of InitH.cpp:227-342
+ * and Init_a1_a2.cpp:54-122 with gamma = g / N (data.cpp:11).  Call with null arrays to get the
+ * nonzero counts, then with arrays of those sizes (row pointers n + 1, n = (N+1)^2 - 1). */
+qjx_status qjx_fb_build_dimer(int N, double J, double U, double E, double g, int *gs_nnz, int *qs_nnz,
+                              int *gs_rowptr, int *gs_col, double *gs_val, int *qs_rowptr, int *qs_col,
+                              double *qs_val, double *Ks);
 /* CSR (0-based) Gs and Qs_drv of size n x n, Ks [n]; x0 [n] initial f-vector.
  * drv_type 0: E(t) = -A sign(sin(w t + phase)), 1: -A sin(w t + phase) (calcODE.cpp:91-117). */
 qjx_status qjx_fb_create(int n, const int *gs_rowptr, const int *gs_col, const double *gs_val,

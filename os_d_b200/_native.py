@@ -21,7 +21,7 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_fb_rk4_noalloc", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
+    "qjx_random_observables", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
 
@@ -80,6 +80,9 @@ def lib():
         L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int), c_int_p, c_int_p, c_double_p,
+                                         c_int_p, c_int_p, c_double_p, c_double_p]
         L.qjx_random_observables.argtypes = [C.c_int] * 5 + [c_double_p]
         L.qjx_fb_create.argtypes = ([C.c_int, c_int_p, c_int_p, c_double_p, c_int_p, c_int_p, c_double_p,
                                      c_double_p, c_double_p, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -142,6 +145,21 @@ def random_observables(d, num, seed, mns, rtype):
     out = np.zeros((num, d, d), np.complex128)
     check(lib().qjx_random_observables(d, num, seed, mns, rtype, dp(out)), what="qjx_random_observables")
     return out
+
+
+def fb_build_dimer(N, J, U, E, g):
+    """f-basis Liouvillian of the dimer: (Gs, Qs) as (indptr, indices, data) CSR triples and Ks."""
+    L = lib()
+    gn, qn = C.c_int(0), C.c_int(0)
+    check(L.qjx_fb_build_dimer(N, J, U, E, g, C.byref(gn), C.byref(qn), None, None, None, None, None, None, None),
+          what="qjx_fb_build_dimer")
+    n = (N + 1) ** 2 - 1
+    gr, gc, gv = np.zeros(n + 1, np.int32), np.zeros(gn.value, np.int32), np.zeros(gn.value)
+    qr, qc, qv = np.zeros(n + 1, np.int32), np.zeros(qn.value, np.int32), np.zeros(qn.value)
+    ks = np.zeros(n)
+    check(L.qjx_fb_build_dimer(N, J, U, E, g, C.byref(gn), C.byref(qn), ip(gr), ip(gc), dp(gv), ip(qr), ip(qc),
+                               dp(qv), dp(ks)), what="qjx_fb_build_dimer")
+    return (gr, gc, gv), (qr, qc, qv), ks
 
 
 def expm(A):

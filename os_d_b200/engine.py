@@ -138,6 +138,18 @@ class Engine:
         return {k: getattr(s, k) for k, _ in N.QjxStats._fields_}
 
 
+def fbasis_pure_state(N, k):
+    """f-vector of rho = |k><k| (initRhoODE, source/cpp/CQdiss_os_dimer/CQdiss/calcODE.cpp:120-167):
+    only the diagonal generalised Gell-Mann coordinates are nonzero."""
+    d = N + 1
+    x = np.zeros(d * d - 1)
+    base = d * (d - 1)
+    for m in range(N):
+        w = 1.0 / np.sqrt((m + 1) * (m + 2))
+        x[base + m] = w * (1.0 if k <= m else 0.0) - w * (m + 1) * (1.0 if k == m + 1 else 0.0)
+    return x
+
+
 class FBasis:
     """f-basis RK4 of dx/dt = Gs x + E(t) Qs_drv x - Ks on a GPU."""
 
