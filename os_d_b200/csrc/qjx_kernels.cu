@@ -14,13 +14,15 @@
 //   * a tile is one matrix x 32 trajectory columns, full height (all d rows), so the
 //     column norm needed by the jump test stays inside the CTA;
 //   * the gathered state columns and the propagator K-slabs are moved by the TMA engine
-//     (cp.async.bulk + mbarrier, 3-stage slab pipeline), so the FP64 pipe is fed while
-//     the next slab streams from L2;
+//     (cp.async.bulk + mbarrier, 2-stage slab pipeline of 16 k-rows), so the tensor pipe is
+//     fed while the next slab streams from L2;
 //   * the epilogue is the whole trajectory state machine: norm test, descend / accept,
 //     jump record, renormalisation, channel choice, threshold redraw, time bookkeeping,
 //     period and dump accounting, the observables, and re-bucketing for the next step.
-// FP64 has no tcgen05 kind, so the contraction runs on the FP64 FMA pipe; it is written
-// so that every output keeps the oracle's k-ascending fma chain (bit-identical results).
+// FP64 has no tcgen05 kind, so the plain form's contraction runs on the FP64 tensor core
+// (mma.sync m8n8k4 f64), laid out so that every output keeps the oracle's k-ascending fma
+// chain (bit-identical results).  The split-precision form (qjx_split.cuh, included at the
+// end) runs the same micro-steps with bf16x3 products on the tcgen05 tensor cores.
 #include "qjx_device.cuh"
 
 namespace qjx {
