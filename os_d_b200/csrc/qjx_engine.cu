@@ -233,10 +233,10 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
         P.KS = (d + 15) / 16;
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
-        // deepest operand ring (2..8 stages) that fits next to 4 KB of static shared memory
+        // deepest operand ring (2..8 stages) that fits next to 8 KB of static shared memory
         P.sstages = 0;
         for (int st = 8; st >= 2 && !P.sstages; st--)
-            if (split_smem_bytes(P.MDs, MD, st) + 4096 <= (size_t)optin) P.sstages = st;
+            if (split_smem_bytes(P.MDs, MD, st) + 8192 <= (size_t)optin) P.sstages = st;
         if (!P.sstages) return bail(QJX_ERR_UNSUPPORTED);
         const size_t per_s = (size_t)P.KS * 4 * P.MDs * 16;
         std::vector<uint16_t> hs((size_t)G * per_s, 0);

@@ -190,13 +190,15 @@ __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, d
     return after_step(P, s, tr, col, wscr, lane);
 }
 
-// Warp-cooperative epilogue of one trajectory column: `col` holds M_g * psi in shared memory.
-__device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, int tr, int *cnt_next,
-                                int *list_next, int lane)
+// Warp-cooperative epilogue of one trajectory column: `col` holds M_g * psi in shared memory,
+// `s_in` the trajectory's state record (loaded by the caller).  Returns the bucket of the
+// trajectory's next micro-step, or -1 (done, paused or failed); the caller appends it.
+__device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, int tr, const TrajState &s_in,
+                               int lane)
 {
     const int d = P.d;
     double *wscr = reinterpret_cast<double *>(wscr_c);
-    TrajState s = P.st[tr];
+    TrajState s = s_in;
     int g2 = -1;
     int err = 0;
     bool paused = false;
@@ -341,6 +343,7 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
     default: break;
     }
 
+    if (err || paused) g2 = -1;
     if (lane == 0) {
         if (err) {
             s.err = err;
@@ -349,12 +352,39 @@ __device__ void column_epilogue(const Params &P, double2 *col, double2 *wscr_c, 
         } else if (paused) {
             s.paused = 1;
             atomicAdd(&P.ctrl[2], 1);
-        } else if (g2 >= 0) {
-            enqueue(P, cnt_next, list_next, g2, tr);
         }
         P.st[tr] = s;
     }
     __syncwarp();
+    return g2;
+}
+
+// Appends trajectories trs[c] to their next buckets g2s[c] (c < ncol, -1 skips) with one global
+// atomic per bucket: ranks and counts in shared memory, one reservation per bucket, then the
+// list writes.  Block-wide (contains barriers).
+__device__ void enqueue_batch(const Params &P, int *cnt_next, int *list_next, const int *trs, const int *g2s, int ncol,
+                              int *s_gcnt, int *s_gbase, int *s_rank)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < P.G; i += nt) s_gcnt[i] = 0;
+    __syncthreads();
+    for (int c = tid; c < ncol; c += nt)
+        if (g2s[c] >= 0) s_rank[c] = atomicAdd(&s_gcnt[g2s[c]], 1);
+    __syncthreads();
+    for (int i = tid; i < P.G; i += nt)
+        if (s_gcnt[i]) s_gbase[i] = atomicAdd(&cnt_next[i], s_gcnt[i]);
+    __syncthreads();
+    for (int c = tid; c < ncol; c += nt)
+        if (g2s[c] >= 0) list_next[(size_t)g2s[c] * P.n + s_gbase[g2s[c]] + s_rank[c]] = trs[c];
+}
+
+// Copies a 96-byte trajectory record with 16-byte accesses.
+__device__ __forceinline__ void load_state(TrajState *dst, const TrajState *src)
+{
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    uint4 *t = reinterpret_cast<uint4 *>(dst);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(TrajState) / 16); i++) t[i] = s[i];
 }
 
 // Accumulates M_g * B for one sub-tile of NTE x TX columns (all rows), streaming the
@@ -511,6 +541,8 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
     __shared__ int s_kc[kMaxGroups + 1];
     __shared__ int s_tr[kNC];
     __shared__ long long s_src[kNC];
+    __shared__ __align__(16) TrajState s_st[kNC];
+    __shared__ int s_g2[kNC], s_rank[kNC], s_gcnt[kMaxGroups], s_gbase[kMaxGroups];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = P.G, n = P.n, d = P.d;
@@ -565,7 +597,8 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
         if (tid < kNC) {
             if (tid < ncol) {
                 const int tr = list_cur[(size_t)g * n + idx + tid];
-                const int ph = P.st[tr].phase, cur = P.st[tr].cur;
+                load_state(&s_st[tid], &P.st[tr]);
+                const int ph = s_st[tid].phase, cur = s_st[tid].cur;
                 const int slot = (ph >= PH_OBS_E) ? (cur ^ 1) : cur;
                 s_tr[tid] = tr;
                 s_src[tid] = ((long long)slot * n + tr) * MD;
@@ -602,8 +635,12 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
         }
         const long long t2 = clock64();
         double2 *wscr = Us + warp * MD;
-        for (int c = warp; c < ncol; c += kThreads / 32)
-            column_epilogue(P, Bt + c * S16, wscr, s_tr[c], cnt_next, list_next, lane);
+        for (int c = warp; c < ncol; c += kThreads / 32) {
+            const int g2 = column_epilogue(P, Bt + c * S16, wscr, s_tr[c], s_st[c], lane);
+            if (lane == 0) s_g2[c] = g2;
+        }
+        __syncthreads();
+        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, ncol, s_gcnt, s_gbase, s_rank);
         work += ncol;
         pos += ncol;
         fence_proxy_async();

@@ -115,14 +115,15 @@ __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo
 }
 
 // Dynamic shared memory: a ring of `stages` operand stages, each [A planes][B planes] of one
-// k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs+1))
-// followed by the per-warp epilogue scratch (16 x MD).
+// k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs+1)),
+// the per-warp epilogue scratch (16 x MD) and the tile's 128 trajectory records.
 size_t split_stage_bytes(int MDs) { return (size_t)kAPlanes * (kABytes + (size_t)MDs * 32); }
 
 size_t split_smem_bytes(int MDs, int MD, int stages)
 {
     const size_t ring = (size_t)stages * split_stage_bytes(MDs);
-    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2) + (size_t)(kThreads / 32) * MD * sizeof(double2);
+    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2) + (size_t)(kThreads / 32) * MD * sizeof(double2) +
+                       (size_t)kTileM * sizeof(TrajState);
     return ring > epi ? ring : epi;
 }
 
@@ -135,6 +136,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const int S16 = MDs + 1;
     double2 *Bt = reinterpret_cast<double2 *>(smem);          // epilogue: [32][S16] FP64 columns
     double2 *wscr = Bt + 32 * S16 + (size_t)(threadIdx.x >> 5) * P.MD;
+    TrajState *s_st = reinterpret_cast<TrajState *>(Bt + 32 * S16 + (size_t)(kThreads / 32) * P.MD);  // [128]
     __shared__ __align__(8) uint64_t fullA[kMaxSStages], fullB[kMaxSStages], empty[kMaxSStages], accf;
     __shared__ uint32_t s_tmem;
     __shared__ int s_tstart[kMaxGroups + 1];
@@ -143,6 +145,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     __shared__ int s_fail;
     __shared__ int s_rows;  // trajectories per tile in this micro-step
     __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
+    __shared__ int s_g2[kTileM], s_rank[kTileM], s_gcnt[kMaxGroups], s_gbase[kMaxGroups];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = P.G, n = P.n, d = P.d;
@@ -319,6 +322,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             ok = false;
             break;
         }
+        // the tile's state records, all loaded at once (one L2 round trip for the whole tile)
+        for (int m = tid; m < rows; m += kThreads) load_state(&s_st[m], &P.st[s_tr[m]]);
         const long long t2 = clock64();
         for (int c = 0; c < 4 && 32 * c < rows; c++) {
             const long long ts = clock64();
@@ -338,11 +343,16 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             tr_stage += clock64() - ts;
             for (int cc = warp; cc < 32; cc += kThreads / 32) {
                 const int m = 32 * c + cc;
-                if (m < rows) column_epilogue(P, Bt + (size_t)cc * S16, wscr, s_tr[m], cnt_next, list_next, lane);
+                if (m < rows) {
+                    const int g2 = column_epilogue(P, Bt + (size_t)cc * S16, wscr, s_tr[m], s_st[m], lane);
+                    if (lane == 0) s_g2[m] = g2;
+                }
             }
             fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
             __syncthreads();
         }
+        __syncthreads();
+        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, rows, s_gcnt, s_gbase, s_rank);
         work += rows;
         const long long t3 = clock64();
         tr_setup += t1 - t0;
