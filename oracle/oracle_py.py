@@ -32,6 +32,11 @@ class OrcState(C.Structure):
                 ("diss_types", c_int_p), ("error", c_int_p)]
 
 
+class OrcRk(C.Structure):
+    _fields_ = [("ND", c_double_p), ("DR", c_double_p), ("E0", C.c_double), ("A", C.c_double), ("freq", C.c_double),
+                ("phase", C.c_double), ("drv_type", C.c_int), ("rk_ns", C.c_int)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -45,6 +50,8 @@ def lib():
         L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
         L.orc_philox_uniform.restype = C.c_double
         L.orc_init.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int, C.c_int]
+        L.orc_run_periods_rk.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcRk), C.POINTER(OrcState), C.c_int,
+                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_run_periods.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_int]
         L.orc_observables.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int] + [c_double_p] * 8
@@ -184,6 +191,18 @@ class Ensemble:
     def run_periods(self, n_periods, is_obs=1, tr0=0, tr1=None, n_threads=0):
         tr1 = self.n if tr1 is None else tr1
         return lib().orc_run_periods(C.byref(self.p), C.byref(self.s), tr0, tr1, n_periods, is_obs, n_threads)
+
+    def run_periods_rk(self, n_periods, ND, DR, E0, A, rk_ns, period0=0, drv_type=0, freq=1.0, phase=0.0, is_obs=1,
+                       tr0=0, tr1=None, n_threads=0):
+        """RK propagator (prop_id 1) for n_periods periods numbered from period0."""
+        tr1 = self.n if tr1 is None else tr1
+        self._nd = np.ascontiguousarray(ND, dtype=np.complex128)
+        self._dr = np.ascontiguousarray(DR, dtype=np.complex128)
+        rk = OrcRk()
+        rk.ND, rk.DR = _dp(self._nd), _dp(self._dr)
+        rk.E0, rk.A, rk.freq, rk.phase, rk.drv_type, rk.rk_ns = E0, A, freq, phase, drv_type, rk_ns
+        return lib().orc_run_periods_rk(C.byref(self.p), C.byref(rk), C.byref(self.s), tr0, tr1, n_periods, period0,
+                                        is_obs, n_threads)
 
     def observables(self, is_start=False, want_adr=False):
         n, d = self.n, self.d

@@ -681,6 +681,148 @@ int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_
     return bad;
 }
 
+/* ------------------------------------------------------------------ RK propagator */
+
+/* E(t) of rk_right_part_dimer (core.cpp:11073-11103) */
+static double rk_drive(const orc_rk *rk, double T, double t)
+{
+    if (rk->drv_type == 1) return rk->E0 + rk->A * sin(rk->freq * t + rk->phase);
+    const double mod_time = fmod(t, T), half_T = T * 0.5;
+    return (mod_time < half_T) ? rk->E0 + rk->A : rk->E0 - rk->A;
+}
+
+typedef struct {
+    traj_ctx *c;
+    const orc_rk *rk;
+    const tmat *tND, *tDR;
+    double rk_step;
+    double *prev, *args, *k1, *k2, *k3, *k4, *nd, *dr;
+} rk_ctx;
+
+/* k = -i (ND arg + E DR arg) (core.cpp:11106-11112) */
+static void rk_right_part(rk_ctx *r, const double *arg, double t, double *k)
+{
+    traj_ctx *c = r->c;
+    const int d = c->p->d;
+    matvec_t(d, r->tND->ld, r->tND->r, r->tND->i, arg, r->nd);
+    matvec_t(d, r->tDR->ld, r->tDR->r, r->tDR->i, arg, r->dr);
+    c->s->matvecs[c->tr] += 2;
+    const double E = rk_drive(r->rk, c->p->T, t);
+    for (int st = 0; st < d; st++) {
+        k[2 * st] = +(r->nd[2 * st + 1] + E * r->dr[2 * st + 1]);
+        k[2 * st + 1] = -(r->nd[2 * st] + E * r->dr[2 * st]);
+    }
+}
+
+/* rk_int_dimer (core.cpp:11592-11619) on c->phi with step h */
+static void rk_int(rk_ctx *r, double h)
+{
+    traj_ctx *c = r->c;
+    const int d = c->p->d;
+    double *phi = c->phi, *t = &c->s->t[c->tr];
+    const double rs = r->rk_step;
+    memcpy(r->args, phi, 2 * (size_t)d * sizeof(double));
+    rk_right_part(r, r->args, *t, r->k1);
+    for (int e = 0; e < 2 * d; e++) r->args[e] = phi[e] + 0.5 * rs * r->k1[e];
+    *t += h * 0.5;
+    rk_right_part(r, r->args, *t, r->k2);
+    for (int e = 0; e < 2 * d; e++) r->args[e] = phi[e] + 0.5 * rs * r->k2[e];
+    rk_right_part(r, r->args, *t, r->k3);
+    for (int e = 0; e < 2 * d; e++) r->args[e] = phi[e] + 1.0 * rs * r->k3[e];
+    *t += h * 0.5;
+    rk_right_part(r, r->args, *t, r->k4);
+    for (int e = 0; e < 2 * d; e++) phi[e] += (r->k1[e] + 2.0 * r->k2[e] + 2.0 * r->k3[e] + r->k4[e]) * h / 6.0;
+}
+
+/* rk_step_dimer (core.cpp:11886-11948); its tail recursion on the end part is a loop here */
+static void rk_step(rk_ctx *r, double h)
+{
+    traj_ctx *c = r->c;
+    const orc_problem *p = c->p;
+    orc_state *s = c->s;
+    const int d = p->d;
+    double *phi = c->phi, *t = &s->t[c->tr], *eta = &s->eta[c->tr];
+    while (1) {
+        memcpy(r->prev, phi, 2 * (size_t)d * sizeof(double));
+        const double prev_norm = orc_norm_square(d, phi);
+        rk_int(r, h);
+        const double curr_norm = orc_norm_square(d, phi);
+        if (curr_norm > 1.0) { c->err = 1; return; }
+        if (curr_norm > *eta) return; /* not crossed */
+        const double norm_diff = prev_norm - curr_norm;
+        const double begin_part = (prev_norm - *eta) / norm_diff;
+        const double end_part = 1.0 - begin_part;
+        const double begin_step = h * begin_part, end_step = h * end_part;
+        memcpy(phi, r->prev, 2 * (size_t)d * sizeof(double));
+        *t -= h;
+        rk_int(r, begin_step);
+        if (p->record > 0 && c->is_obs == 1) {
+            const int rr = s->n_rec[c->tr];
+            if (rr >= s->rec_cap) { c->err = 4; return; }
+            const size_t o = (size_t)c->tr * s->rec_cap + rr;
+            s->jump_times[o] = *t;
+            s->jump_norms[o] = orc_norm_square(d, phi);
+            s->jump_etas[o] = *eta;
+            s->diss_types[o] = -1;
+            s->n_rec[c->tr] = rr + 1;
+            s->jumps_counts[c->tr]++;
+        }
+        memcpy(c->aux, phi, 2 * (size_t)d * sizeof(double));
+        recovery(c); /* rk_recovery (rk_proc.cpp:198-305): same steps as recovery */
+        if (c->err) return;
+        memcpy(phi, c->aux, 2 * (size_t)d * sizeof(double));
+        *eta = draw(c);
+        while (*eta == 0.0 && !c->err) *eta = draw(c);
+        if (c->err) return;
+        h = end_step;
+    }
+}
+
+int orc_run_periods_rk(const orc_problem *p, const orc_rk *rk, orc_state *s, int tr0, int tr1, int n_periods,
+                       int period0, int is_obs, int n_threads)
+{
+    if (rk->rk_ns < 1) return 1;
+    int bad = 0;
+    tmat tND, tDR, tL;
+    if (tmat_make(p->d, 1, rk->ND, &tND) || tmat_make(p->d, 1, rk->DR, &tDR) || tmat_make(p->d, p->num_diss, p->L, &tL))
+        return 2;
+#ifdef _OPENMP
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads) reduction(+ : bad)
+#endif
+    for (int tr = tr0; tr < tr1; tr++) {
+        if (s->error[tr]) { bad++; continue; }
+        const int d = p->d;
+        traj_ctx c = {0};
+        c.p = p; c.s = s; c.tr = tr; c.is_obs = is_obs;
+        c.tL = &tL;
+        c.phi = s->phi + 2 * (size_t)tr * d;
+        const size_t v = 2 * (size_t)d;
+        double *buf = (double *)calloc(v * 11, sizeof(double));
+        c.aux = buf;
+        c.res = buf + v;
+        c.gn = (double *)calloc((size_t)p->num_diss + 1, sizeof(double));
+        rk_ctx r = {0};
+        r.c = &c; r.rk = rk; r.tND = &tND; r.tDR = &tDR;
+        r.rk_step = p->T / (double)rk->rk_ns;
+        r.prev = buf + 2 * v; r.args = buf + 3 * v; r.k1 = buf + 4 * v; r.k2 = buf + 5 * v; r.k3 = buf + 6 * v;
+        r.k4 = buf + 7 * v; r.nd = buf + 8 * v; r.dr = buf + 9 * v;
+        for (int per = 0; per < n_periods && !c.err; per++)
+            for (int sid = 0; sid < rk->rk_ns && !c.err; sid++) {
+                s->t[tr] = (double)(period0 + per) * p->T + (double)sid * r.rk_step;
+                rk_step(&r, r.rk_step);
+            }
+        s->error[tr] = c.err;
+        if (c.err) bad++;
+        free(buf); free(c.gn);
+    }
+    (void)n_threads;
+    tmat_free(&tND);
+    tmat_free(&tDR);
+    tmat_free(&tL);
+    return bad;
+}
+
 int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
                     double *mean_start, double *norm_o, double *mean_o, double *disp_o,
                     double *m2_o, double *energy_o, double *robs, double *adr_o)

@@ -109,6 +109,27 @@ int orc_init(const orc_problem *p, orc_state *s, int start_type, int start_state
  * exactly like ed->is_obs (qj_proc.cpp:296).  OpenMP over trajectories. */
 int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_periods, int is_obs, int n_threads);
 
+/* RK propagator (prop_id 1): dpsi/dt = -i (H_eff + E(t) H_drv) psi by classic RK4 with rk_ns
+ * steps per period and a jump located by linear interpolation of the norm inside a step.
+ *   rk_period          source/cpp/QJX/QJX/core.cpp:439-450 (t = period T + step rk_step)
+ *   rk_step_dimer      core.cpp:11886-11948 (crossing, begin / end parts, recursion)
+ *   rk_int_dimer       core.cpp:11592-11619; rk_right_part_dimer core.cpp:11033-11115
+ *   arg_upd / rk_final / rk_recovery / save / restore   rk_proc.cpp:124-341 (arg_upd always
+ *                      uses the full rk_step, also inside begin and end parts)
+ * ND = non_drv_part (H_eff), DR = drv_part (H_drv) (newdel.cpp:2354-2366). */
+typedef struct {
+    const double *ND;   /* [d][d] complex */
+    const double *DR;   /* [d][d] complex */
+    double E0, A, freq, phase;
+    int drv_type;       /* 1: E0 + A sin(freq t + phase); otherwise E0 +/- A on the half periods */
+    int rk_ns;          /* steps per period */
+} orc_rk;
+
+/* Advance trajectories [tr0, tr1) by n_periods periods with the RK propagator; the periods are
+ * numbered period0, period0 + 1, ... (the reference's period_id). */
+int orc_run_periods_rk(const orc_problem *p, const orc_rk *rk, orc_state *s, int tr0, int tr1, int n_periods,
+                       int period0, int is_obs, int n_threads);
+
 /* Observables of every trajectory (calc_chars_std[_start], core.cpp:665-725).
  * mean_start is written when is_start != 0 and read otherwise.  adr may be NULL. */
 int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
