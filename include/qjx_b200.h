@@ -96,6 +96,17 @@ typedef struct {
  * HE: [d][d] energy operator H + E0 * H_drv (experiment.cpp:1440).  R: [num_robs][d][d]. */
 qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, const double *g,
                       const double *HE, const double *R, qjx_engine **out);
+/* The RK propagator (prop_id 1): RKPropagateBehavior::one_period -> rk_period / rk_step_dimer
+ * (source/cpp/QJX/QJX/propagator.cpp:67-129, core.cpp:439-450, 11033-11115, 11592-11619,
+ * 11886-11948, rk_proc.cpp:124-341): classic RK4 of dpsi/dt = -i (H_eff + E(t) H_drv) psi with
+ * rk_ns steps per period, E(t) = E0 +/- A on the half periods (drv_type 0) or
+ * E0 + A sin(drv_freq t + drv_phase) (drv_type 1), the jump time located by linear
+ * interpolation of the norm inside the crossing step.  H_eff = non_drv_part, H_drv = drv_part
+ * (newdel.cpp:2354-2366).  cfg's deep / num_branches are ignored; precision must be 0.  Periods
+ * are numbered from the last qjx_reset_times (or creation), like the reference's period_id. */
+qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, const double *H_drv, double E0, double A,
+                         int drv_type, double drv_freq, double drv_phase, int rk_ns, const double *L,
+                         const double *g, const double *HE, const double *R, qjx_engine **out);
 void qjx_destroy(qjx_engine *h);
 const char *qjx_last_error(const qjx_engine *h);
 const char *qjx_status_string(qjx_status s);

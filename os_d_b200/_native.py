@@ -17,7 +17,7 @@ c_i64_p = C.POINTER(C.c_int64)
 
 # every entry point declared in include/qjx_b200.h
 EXPORTS = [
-    "qjx_create", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
+    "qjx_create", "qjx_create_rk", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
@@ -56,6 +56,8 @@ def lib():
                 raise QjxError(f"native library lacks {name}")
         vp = C.c_void_p
         L.qjx_create.argtypes = [C.POINTER(QjxConfig)] + [c_double_p] * 5 + [C.POINTER(vp)]
+        L.qjx_create_rk.argtypes = ([C.POINTER(QjxConfig), c_double_p, c_double_p, C.c_double, C.c_double, C.c_int,
+                                     C.c_double, C.c_double, C.c_int] + [c_double_p] * 4 + [C.POINTER(vp)])
         L.qjx_destroy.argtypes = [vp]
         L.qjx_destroy.restype = None
         L.qjx_last_error.argtypes = [vp]

@@ -34,12 +34,16 @@ enum Phase : int {
     PH_OBS_E = 3,   // energy <psi_hat| H + E0 Hd |psi_hat>
     PH_OBS_R = 4,   // random observable sub
     PH_DONE = 5,
-    PH_ERROR = 6
+    PH_ERROR = 6,
+    PH_RK = 7       // RK propagator: right-hand side of stage rk_stage, matrix rk_part
 };
+
+// state slots of the RK propagator (psi slots 0 and 1 hold psi and the spare copy)
+constexpr int kSlotArgs = 2, kSlotK1 = 3, kSlotND = 6, kRkSlots = 7;
 
 enum ErrCode : int { ERR_NONE = 0, ERR_NORM = 1, ERR_ZERO_W = 2, ERR_RNG = 3, ERR_TIMEOUT = 6 };
 
-// Per-trajectory state (one 96-byte record per trajectory).
+// Per-trajectory state (one 144-byte record per trajectory).
 struct __align__(16) TrajState {
     double t;          // times_all
     double eta;        // etas_all
@@ -50,8 +54,17 @@ struct __align__(16) TrajState {
     int lvl, b, phase, cur;   // level, branch, phase, slot holding psi
     int sub, pc, di, jumps;   // channel / observable index, periods done, next dump, jumps_counts
     int nrec, err, paused, pad;
+    // RK propagator (prop_id 1)
+    double rk_h;       // step being integrated: rk_step, or the begin / end part around a jump
+    double rk_prev;    // norm of psi before the step
+    double rk_end;     // end part still to integrate after a located jump
+    int rk_sid;        // step index within the period
+    int rk_stage;      // 1..4: right-hand side being evaluated
+    int rk_part;       // 0: H_eff arg, 1: H_drv arg
+    int rk_ctx;        // 0: step checked for a crossing; 1: begin part of a located jump
+    int rk_pad[2];
 };
-static_assert(sizeof(TrajState) == 96, "TrajState layout");
+static_assert(sizeof(TrajState) == 144, "TrajState layout");
 
 struct Params {
     int d, MD, n, deep, nb, nd, nr, G;
@@ -99,6 +112,10 @@ struct Params {
     int MDs, KS;                  // rows padded to 16 (MMA N), k-steps of 16 complex components
     int sstages;                  // depth of the split kernel's operand ring
     const unsigned char *usplit;  // [G][KS][4 planes: Re hi, Re lo, Im hi, Im lo][MDs rows x 16 k] bf16
+    // RK propagator (prop 1): groups 0 and 1 are H_eff and H_drv; psi has kRkSlots slots
+    int prop;                     // 0 QJ split tree, 1 RK
+    int rk_ns, period0, drv_type;
+    double rk_step, T, E0, A, drv_freq, drv_phase;
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns

@@ -21,6 +21,7 @@ size_t step_smem_bytes(int MD);
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st);
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st);
 cudaError_t launch_init_state(const Params &P, cudaStream_t st);
+cudaError_t launch_rk_schedule(const Params &P, cudaStream_t st);
 cudaError_t launch_purity(const Params &P, double2 *hat, double2 *rho, double *out, cudaStream_t st);
 cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
 cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
@@ -56,6 +57,7 @@ struct qjx_engine {
     std::vector<std::vector<int>> jtype;
     qjx_stats stats{};
     bool states_set = false;
+    int period_base = 0;  // periods run since the last time reset (the RK propagator's period_id)
 };
 
 static void *dalloc(qjx_engine *h, size_t bytes)
@@ -157,8 +159,8 @@ static void pack_split(const double *M, int d, int MDs, int KS, uint16_t *out)
             }
 }
 
-extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, const double *g,
-                                 const double *HE, const double *R, qjx_engine **out)
+static qjx_status create_engine(const qjx_config *cfg, const double *U, const double *L, const double *g,
+                                const double *HE, const double *R, int psi_slots, qjx_engine **out)
 {
     if (!cfg || !out || !U || !L || !g || !HE) return QJX_ERR_INVALID_ARG;
     *out = nullptr;
@@ -267,7 +269,7 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
     P.dt = d_dt;
     P.g = d_g;
 
-    P.psi = (double2 *)dalloc(h, (size_t)2 * n * MD * sizeof(double2));
+    P.psi = (double2 *)dalloc(h, (size_t)psi_slots * n * MD * sizeof(double2));
     P.st = (TrajState *)dalloc(h, (size_t)n * sizeof(TrajState));
     P.gn = (double *)dalloc(h, (size_t)n * c.num_diss * sizeof(double));
     P.cnt = (int *)dalloc(h, (size_t)3 * G * sizeof(int));
@@ -401,6 +403,7 @@ extern "C" qjx_status qjx_reset_times(qjx_engine *h)
     CK(cudaSetDevice(h->cfg.device));
     CK(launch_reset_times(h->P, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->period_base = 0;
     return QJX_OK;
 }
 
@@ -534,6 +537,41 @@ static qjx_status run_until_idle(qjx_engine *h)
     return rs;
 }
 
+extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, const double *g,
+                                 const double *HE, const double *R, qjx_engine **out)
+{
+    return create_engine(cfg, U, L, g, HE, R, 2, out);
+}
+
+extern "C" qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, const double *H_drv, double E0,
+                                    double A, int drv_type, double drv_freq, double drv_phase, int rk_ns,
+                                    const double *L, const double *g, const double *HE, const double *R,
+                                    qjx_engine **out)
+{
+    if (!cfg || !out || !H_eff || !H_drv || rk_ns < 1) return QJX_ERR_INVALID_ARG;
+    if (cfg->precision != 0) return QJX_ERR_UNSUPPORTED;  // the RK propagator runs the FP64 plain form
+    qjx_config c = *cfg;
+    c.num_branches = 1;  // groups 0 and 1: H_eff and H_drv
+    c.deep = 2;
+    const size_t dd2 = (size_t)2 * c.d * c.d;
+    std::vector<double> M(2 * dd2);
+    std::memcpy(M.data(), H_eff, dd2 * sizeof(double));
+    std::memcpy(M.data() + dd2, H_drv, dd2 * sizeof(double));
+    qjx_status st = create_engine(&c, M.data(), L, g, HE, R, kRkSlots, out);
+    if (st != QJX_OK) return st;
+    Params &P = (*out)->P;
+    P.prop = 1;
+    P.rk_ns = rk_ns;
+    P.T = c.T;
+    P.rk_step = c.T / double(rk_ns);  // init_rk (rk_proc.cpp:62)
+    P.E0 = E0;
+    P.A = A;
+    P.drv_type = drv_type;
+    P.drv_freq = drv_freq;
+    P.drv_phase = drv_phase;
+    return QJX_OK;
+}
+
 extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, const int *dump_at, int n_dumps,
                                       int dump_base)
 {
@@ -561,10 +599,13 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
     P.record = (is_obs == 1 && h->cfg.record > 0) ? 1 : 0;
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
-    CK(launch_schedule(P, 0, h->stream));
+    P.period0 = h->period_base;
+    if (P.prop == 1) CK(launch_rk_schedule(P, h->stream));
+    else CK(launch_schedule(P, 0, h->stream));
     h->stats.launches += 1;
     qjx_status s = run_until_idle(h);
     if (s != QJX_OK) return s;
+    h->period_base += n_periods;
     return drain_records(h);
 }
 

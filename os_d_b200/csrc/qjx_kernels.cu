@@ -42,8 +42,45 @@ __device__ __forceinline__ int group_of(const Params &P, const TrajState &s)
     case PH_REC_A: return P.gL0 + s.sub;
     case PH_OBS_E: return P.gHE;
     case PH_OBS_R: return P.gR0 + s.sub;
+    case PH_RK: return s.rk_part;  // group 0 H_eff, group 1 H_drv
     default: return -1;
     }
+}
+
+// Slot holding the input vector of a trajectory's next matvec: psi, the normalised copy for
+// the observables, or the RK stage argument.
+__device__ __forceinline__ int src_slot(int phase, int cur, int rk_stage)
+{
+    if (phase == PH_RK) return rk_stage == 1 ? cur : kSlotArgs;
+    return (phase == PH_OBS_E || phase == PH_OBS_R) ? (cur ^ 1) : cur;
+}
+
+// ---------------------------------------------------------------- RK propagator helpers
+// E(t) of rk_right_part_dimer (core.cpp:11073-11103)
+__device__ __forceinline__ double rk_drive(const Params &P, double t)
+{
+    if (P.drv_type == 1)
+        return __dadd_rn(P.E0, __dmul_rn(P.A, sin(__dadd_rn(__dmul_rn(P.drv_freq, t), P.drv_phase))));
+    const double mod_time = fmod(t, P.T), half_T = __dmul_rn(P.T, 0.5);
+    return (mod_time < half_T) ? __dadd_rn(P.E0, P.A) : __dsub_rn(P.E0, P.A);
+}
+
+// Start time of step rk_sid of the current period (rk_period, core.cpp:446)
+__device__ __forceinline__ double rk_step_time(const Params &P, const TrajState &s)
+{
+    return __dadd_rn(__dmul_rn((double)(P.period0 + s.pc), P.T), __dmul_rn((double)s.rk_sid, P.rk_step));
+}
+
+// Begin an RK step of size h from psi (slot cur) with norm prev; returns its first matvec's group.
+__device__ __forceinline__ int rk_begin(TrajState &s, double h, double prev, int ctx)
+{
+    s.phase = PH_RK;
+    s.rk_h = h;
+    s.rk_prev = prev;
+    s.rk_stage = 1;
+    s.rk_part = 0;
+    s.rk_ctx = ctx;
+    return 0;
 }
 
 __device__ __forceinline__ void enqueue(const Params &P, int *cnt, int *list, int g, int tr)
@@ -160,8 +197,36 @@ __device__ int finish_obs(const Params &P, TrajState &s)
         s.phase = PH_DONE;
         return -1;
     }
+    if (P.prop == 1) {  // next RK step of the period
+        s.t = rk_step_time(P, s);
+        return rk_begin(s, P.rk_step, s.rk_prev, 0);
+    }
     s.phase = PH_STEP;
     return s.b * P.deep + s.lvl;
+}
+
+// An RK step finished without crossing (rk_period, core.cpp:443-449): next step, period and dump
+// bookkeeping.  `col` holds psi, nrm its norm.
+__device__ int rk_after_step(const Params &P, TrajState &s, int tr, const double2 *col, double *wscr, int lane,
+                             double nrm)
+{
+    s.rk_prev = nrm;
+    s.rk_sid += 1;
+    if (s.rk_sid == P.rk_ns) {
+        s.rk_sid = 0;
+        s.pc += 1;
+        if (s.di < P.n_dumps && s.pc == P.dump_at[s.di]) {
+            obs_prep(P, s, tr, col, wscr, lane, P.dump_base + s.di, 0);
+            s.phase = PH_OBS_E;
+            return P.gHE;
+        }
+        if (s.pc >= P.target) {
+            s.phase = PH_DONE;
+            return -1;
+        }
+    }
+    s.t = rk_step_time(P, s);
+    return rk_begin(s, P.rk_step, nrm, 0);
 }
 
 // Apply the chosen jump channel: psi = (L_idx psi_hat) / sqrt(w_idx / g_idx)
@@ -185,6 +250,10 @@ __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, d
     s.eta = draw(P, tr, s, err);
     while (s.eta == 0.0 && *err == 0) s.eta = draw(P, tr, s, err);
     if (*err) return -1;
+    if (P.prop == 1) {  // the end part of the interrupted RK step (rk_step_dimer, core.cpp:11946)
+        const double nrm = warp_norm(col, d, lane);
+        return rk_begin(s, s.rk_end, nrm, 0);
+    }
     s.phase = PH_STEP;
     s.t = __dadd_rn(s.t, P.dt[P.deep - 1]);
     return after_step(P, s, tr, col, wscr, lane);
@@ -298,6 +367,98 @@ __device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, i
     case PH_REC_A: {
         const double w = P.gn[(size_t)tr * P.nd + s.sub];
         g2 = apply_jump(P, s, tr, col, wscr, lane, s.sub, w, &err);
+    } break;
+
+    case PH_RK: {  // one right-hand side of rk_int_dimer (core.cpp:11592-11619), col = M arg
+        if (s.rk_part == 0) {  // H_eff arg, kept for the drive part
+            double2 *dst = slot_ptr(P, kSlotND, tr);
+            for (int k = lane; k < d; k += 32) dst[k] = col[k];
+            s.rk_part = 1;
+            g2 = 1;
+            break;
+        }
+        // k = -i (H_eff arg + E H_drv arg)  (core.cpp:11106-11112)
+        const double E = rk_drive(P, s.t);
+        const double2 *nd = slot_ptr(P, kSlotND, tr);
+        const double2 *phi = slot_ptr(P, s.cur, tr);
+        const double h = s.rk_h;
+        if (s.rk_stage < 4) {
+            // arg_upd (rk_proc.cpp:146-185) uses the full rk_step, also inside a begin or end part
+            const double c = (s.rk_stage == 3) ? __dmul_rn(1.0, P.rk_step) : __dmul_rn(0.5, P.rk_step);
+            double2 *kd = slot_ptr(P, kSlotK1 + s.rk_stage - 1, tr);
+            double2 *args = slot_ptr(P, kSlotArgs, tr);
+            for (int k = lane; k < d; k += 32) {
+                const double2 a = nd[k], b = col[k], x = phi[k];
+                const double kr = __dadd_rn(a.y, __dmul_rn(E, b.y)), ki = -__dadd_rn(a.x, __dmul_rn(E, b.x));
+                kd[k] = make_double2(kr, ki);
+                args[k] = make_double2(__dadd_rn(x.x, __dmul_rn(c, kr)), __dadd_rn(x.y, __dmul_rn(c, ki)));
+            }
+            if (s.rk_stage != 2) s.t = __dadd_rn(s.t, __dmul_rn(h, 0.5));
+            s.rk_stage += 1;
+            s.rk_part = 0;
+            g2 = 0;
+            break;
+        }
+        if (s.rk_ctx == 1 && P.record && s.nrec >= P.rec_cap) {  // record buffer full: hold here
+            paused = true;
+            break;
+        }
+        // rk_final (rk_proc.cpp:187-196): psi + (k1 + 2 k2 + 2 k3 + k4) h / 6, into col
+        const double2 *k1 = slot_ptr(P, kSlotK1, tr), *k2 = slot_ptr(P, kSlotK1 + 1, tr);
+        const double2 *k3 = slot_ptr(P, kSlotK1 + 2, tr);
+        for (int k = lane; k < d; k += 32) {
+            const double2 a = nd[k], b = col[k], x = phi[k], p1 = k1[k], p2 = k2[k], p3 = k3[k];
+            const double kr = __dadd_rn(a.y, __dmul_rn(E, b.y)), ki = -__dadd_rn(a.x, __dmul_rn(E, b.x));
+            const double sr = __dadd_rn(__dadd_rn(__dadd_rn(p1.x, __dmul_rn(2.0, p2.x)), __dmul_rn(2.0, p3.x)), kr);
+            const double si = __dadd_rn(__dadd_rn(__dadd_rn(p1.y, __dmul_rn(2.0, p2.y)), __dmul_rn(2.0, p3.y)), ki);
+            col[k] = make_double2(__dadd_rn(x.x, __ddiv_rn(__dmul_rn(sr, h), 6.0)),
+                                  __dadd_rn(x.y, __ddiv_rn(__dmul_rn(si, h), 6.0)));
+        }
+        __syncwarp();
+        const double nrm = warp_norm(col, d, lane);
+        if (s.rk_ctx == 0) {
+            if (nrm > 1.0) {  // is_norm_crossed throws (experiment.cpp:1247-1251)
+                err = ERR_NORM;
+                break;
+            }
+            if (nrm > s.eta) {  // not crossed: accept psi in place
+                double2 *dst = slot_ptr(P, s.cur, tr);
+                for (int k = lane; k < d; k += 32) dst[k] = col[k];
+                g2 = rk_after_step(P, s, tr, col, wscr, lane, nrm);
+            } else {  // crossed: integrate the begin part from psi, still in its slot (core.cpp:11913-11922)
+                const double norm_diff = __dsub_rn(s.rk_prev, nrm);
+                const double begin_part = __ddiv_rn(__dsub_rn(s.rk_prev, s.eta), norm_diff);
+                const double end_part = __dsub_rn(1.0, begin_part);
+                s.rk_end = __dmul_rn(h, end_part);
+                s.t = __dsub_rn(s.t, h);
+                g2 = rk_begin(s, __dmul_rn(h, begin_part), s.rk_prev, 1);
+            }
+        } else {  // begin part done: record the jump, rk_recovery (rk_proc.cpp:198-305)
+            if (P.record) {
+                if (lane == 0) {
+                    const size_t o = (size_t)s.nrec * P.n + tr;
+                    P.r_time[o] = s.t;
+                    P.r_norm[o] = nrm;
+                    P.r_eta[o] = s.eta;
+                    P.r_type[o] = -1;
+                }
+                s.nrec += 1;
+                s.jumps += 1;
+            }
+            const double sq = __dsqrt_rn(nrm);
+            double2 *dst = slot_ptr(P, s.cur ^ 1, tr);
+            for (int k = lane; k < d; k += 32) {
+                const double2 v = col[k];
+                dst[k] = make_double2(__ddiv_rn(v.x, sq), __ddiv_rn(v.y, sq));
+            }
+            s.cur ^= 1;
+            s.ran = draw(P, tr, s, &err);
+            if (err) break;
+            s.tmpw = 0.0;
+            s.phase = PH_REC_W;
+            s.sub = 0;
+            g2 = P.gL0;
+        }
     } break;
 
     case PH_OBS_E: {  // energy <psi_hat| H + E0 Hd |psi_hat>  (experiment.cpp:1423-1469)
@@ -598,8 +759,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             if (tid < ncol) {
                 const int tr = list_cur[(size_t)g * n + idx + tid];
                 load_state(&s_st[tid], &P.st[tr]);
-                const int ph = s_st[tid].phase, cur = s_st[tid].cur;
-                const int slot = (ph >= PH_OBS_E) ? (cur ^ 1) : cur;
+                const int slot = src_slot(s_st[tid].phase, s_st[tid].cur, s_st[tid].rk_stage);
                 s_tr[tid] = tr;
                 s_src[tid] = ((long long)slot * n + tr) * MD;
             } else {
@@ -800,6 +960,14 @@ __global__ void init_state_kernel(const Params P)
     s.err = 0;
     s.paused = 0;
     s.pad = 0;
+    s.rk_h = 0.0;
+    s.rk_prev = 0.0;
+    s.rk_end = 0.0;
+    s.rk_sid = 0;
+    s.rk_stage = 0;
+    s.rk_part = 0;
+    s.rk_ctx = 0;
+    s.rk_pad[0] = s.rk_pad[1] = 0;
     P.st[tr] = s;
 }
 
@@ -901,6 +1069,35 @@ cudaError_t launch_purity(const Params &P, double2 *hat, double2 *rho, double *o
     const int tiles = (P.d + 15) / 16;
     rho_kernel<<<dim3(tiles, tiles), 256, 0, st>>>(P, hat, rho);
     purity_kernel<<<1, 32, 0, st>>>(rho, P.d * P.d, out);
+    return cudaGetLastError();
+}
+
+// Start of a run with the RK propagator: step 0 of the first period from psi (warp per trajectory).
+__global__ void rk_schedule_kernel(const Params P)
+{
+    const int lane = threadIdx.x & 31;
+    const int tr = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tr >= P.n) return;
+    TrajState s = P.st[tr];
+    if (s.phase == PH_ERROR) return;
+    const double nrm = warp_norm(slot_ptr(P, s.cur, tr), P.d, lane);
+    s.pc = 0;
+    s.di = 0;
+    s.paused = 0;
+    s.rk_sid = 0;
+    if (P.target > 0) {
+        s.t = rk_step_time(P, s);
+        rk_begin(s, P.rk_step, nrm, 0);
+        if (lane == 0) enqueue(P, P.cnt, P.lists, 0, tr);
+    } else {
+        s.phase = PH_DONE;
+    }
+    if (lane == 0) P.st[tr] = s;
+}
+
+cudaError_t launch_rk_schedule(const Params &P, cudaStream_t st)
+{
+    rk_schedule_kernel<<<(P.n + 7) / 8, 256, 0, st>>>(P);
     return cudaGetLastError();
 }
 

@@ -216,8 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         if (tid < kTileM) {
             if (tid < rows) {
                 const int tr = list_cur[(size_t)g * n + base + tid];
-                const int ph = P.st[tr].phase, cur = P.st[tr].cur;
-                const int slot = (ph >= PH_OBS_E) ? (cur ^ 1) : cur;
+                const int slot = src_slot(P.st[tr].phase, P.st[tr].cur, P.st[tr].rk_stage);
                 s_tr[tid] = tr;
                 s_src[tid] = ((long long)slot * n + tr) * P.MD;
             } else {

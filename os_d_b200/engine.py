@@ -36,6 +36,35 @@ class Engine:
                                    C.byref(h)), what="qjx_create")
         self.h = h
 
+    @classmethod
+    def rk(cls, H_eff, H_drv, L, g, HE, R=None, T=2 * np.pi, n_traj=1, E0=1.0, A=0.0, rk_ns=1000, drv_type=0,
+           drv_freq=1.0, drv_phase=0.0, seed=0, record=0, rng_kind=0, rec_cap=1024, keep_adr=0, max_dumps=1,
+           device=0, tr_base=0):
+        """Engine with the RK propagator (prop_id 1): RK4 of -i (H_eff + E(t) H_drv) with rk_ns steps
+        per period and linear interpolation of the jump time."""
+        H_eff = np.ascontiguousarray(H_eff, np.complex128)
+        d = H_eff.shape[0]
+        H_drv = np.ascontiguousarray(H_drv, np.complex128)
+        self = cls.__new__(cls)
+        L = np.ascontiguousarray(L, np.complex128).reshape(-1, d, d)
+        g = np.ascontiguousarray(np.atleast_1d(g), np.float64)
+        HE = np.ascontiguousarray(HE, np.complex128)
+        R = np.zeros((0, d, d), np.complex128) if R is None else np.ascontiguousarray(R, np.complex128).reshape(-1, d, d)
+        cfg = N.QjxConfig()
+        cfg.d, cfg.n_traj, cfg.deep, cfg.num_branches = d, n_traj, 2, 1
+        cfg.num_diss, cfg.num_robs, cfg.T, cfg.record = L.shape[0], R.shape[0], T, record
+        cfg.rng_kind, cfg.seed, cfg.rec_cap, cfg.keep_adr = rng_kind, seed, rec_cap, keep_adr
+        cfg.max_dumps, cfg.device, cfg.tr_base, cfg.precision = max_dumps, device, tr_base, 0
+        self.cfg = cfg
+        self.d, self.n, self.nr = d, n_traj, R.shape[0]
+        self.keep_adr = keep_adr
+        h = C.c_void_p()
+        N.check(N.lib().qjx_create_rk(C.byref(cfg), N.dp(H_eff), N.dp(H_drv), E0, A, drv_type, drv_freq, drv_phase,
+                                      rk_ns, N.dp(L), N.dp(g), N.dp(HE), N.dp(R) if R.size else None, C.byref(h)),
+                what="qjx_create_rk")
+        self.h = h
+        return self
+
     def _chk(self, st, what):
         N.check(st, self.h, what)
 
