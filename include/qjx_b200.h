@@ -157,6 +157,9 @@ qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_t
  * T = 2 pi / omega.  Any output may be NULL. */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
                            double *H, double *Hd, double *L, double *K, double *Utree);
+/* Operators of the RK propagator: H_eff = H - (i/2)(g/N) L^H L (non_drv_part) and H_drv
+ * (drv_part), built by DimerNewDelBehaviour::init_hamiltonians_qj (newdel.cpp:2285-2366). */
+qjx_status qjx_build_dimer_rk(int N, double J, double U, double E, double g, double *H_eff, double *H_drv);
 /* exp(A) of a complex n x n matrix, Higham (2005) scaling and squaring. */
 qjx_status qjx_expm(int n, const double *A, double *out);
 /* Random observables of init_random_obs (source/cpp/QJX/QJX/newdel.cpp:3652-3750): for

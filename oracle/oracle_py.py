@@ -45,6 +45,7 @@ def lib():
         L = _lib
         L.orc_dimer_operators.argtypes = [C.c_int] + [C.c_double] * 5 + [c_double_p] * 5
         L.orc_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.orc_dimer_heff.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p]
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
@@ -78,6 +79,13 @@ def dimer_operators(N, J, U, E, A, g):
     rc = lib().orc_dimer_operators(N, J, U, E, A, g, _dp(H), _dp(Hd), _dp(L), _dp(K0), _dp(K1))
     assert rc == 0
     return H, Hd, L, K0, K1
+
+
+def dimer_heff(N, J, U, E, g):
+    """H_eff = H - (i/2) (g/N) L^H L of the dimer (the RK propagator's non-drive part)."""
+    out = _cplx((N + 1, N + 1))
+    assert lib().orc_dimer_heff(N, J, U, E, g, _dp(out)) == 0
+    return out
 
 
 def expm(A):

@@ -82,6 +82,33 @@ int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
     return 0;
 }
 
+/* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
+int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
+{
+    const int d = N + 1;
+    const size_t dd = (size_t)d * d;
+    double *H = malloc(2 * dd * sizeof(double)), *Hd = malloc(2 * dd * sizeof(double));
+    double *L = malloc(2 * dd * sizeof(double)), *K = malloc(4 * dd * sizeof(double));
+    if (!H || !Hd || !L || !K) return 2;
+    int rc = orc_dimer_operators(N, J, U, E, 0.0, g, H, Hd, L, K, K + 2 * dd);
+    const double gamma = g / (double)(d - 1);
+    for (int i = 0; i < d && !rc; i++)
+        for (int j = 0; j < d; j++) {
+            double sr = 0.0, si = 0.0;
+            for (int k = 0; k < d; k++) {
+                const double ar = L[2 * ((size_t)k * d + i)], ai = L[2 * ((size_t)k * d + i) + 1];
+                const double br = L[2 * ((size_t)k * d + j)], bi = L[2 * ((size_t)k * d + j) + 1];
+                sr = sr + (ar * br + ai * bi);
+                si = si + (ar * bi - ai * br);
+            }
+            const size_t idx = (size_t)i * d + j;
+            Heff[2 * idx] = H[2 * idx] + 0.5 * (gamma * si);
+            Heff[2 * idx + 1] = 0.0 - 0.5 * (gamma * sr);
+        }
+    free(H); free(Hd); free(L); free(K);
+    return rc;
+}
+
 /* ------------------------------------------------------------------ expm */
 
 static void cmatmul(int n, const double *A, const double *B, double *C)

@@ -48,6 +48,10 @@ extern "C" {
 int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
                         double *H, double *Hd, double *L, double *K0, double *K1);
 
+/* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
+ * propagator (newdel.cpp:2354-2366), complex d x d. */
+int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);
+
 /* Matrix exponential exp(A), complex n x n, Higham (2005) scaling and squaring with
  * Pade [m/m], m in {3,5,7,9,13}.  Replaces Eigen MatrixXcd::exp() (qj_proc.cpp:55,98). */
 int orc_expm(int n, const double *A, double *out);

@@ -17,7 +17,7 @@ c_i64_p = C.POINTER(C.c_int64)
 
 # every entry point declared in include/qjx_b200.h
 EXPORTS = [
-    "qjx_create", "qjx_create_rk", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
+    "qjx_create", "qjx_create_rk", "qjx_build_dimer_rk", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
@@ -82,6 +82,7 @@ def lib():
         L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_build_dimer_rk.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 2
         L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.POINTER(C.c_int), C.POINTER(C.c_int), c_int_p, c_int_p, c_double_p,
                                          c_int_p, c_int_p, c_double_p, c_double_p]
@@ -126,6 +127,15 @@ def build_dimer(N, J, U, E, A, g, omega, deep):
     check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(Lm), None, dp(Ut)),
           what="qjx_build_dimer")
     return H, Hd, Lm, Ut
+
+
+def build_dimer_rk(N, J, U, E, g):
+    """Operators of the RK propagator: H_eff = H - (i/2)(g/N) L^H L and H_drv."""
+    d = N + 1
+    He = np.zeros((d, d), np.complex128)
+    Hd = np.zeros_like(He)
+    check(lib().qjx_build_dimer_rk(N, J, U, E, g, dp(He), dp(Hd)), what="qjx_build_dimer_rk")
+    return He, Hd
 
 
 def dimer_generators(N, J, U, E, A, g):

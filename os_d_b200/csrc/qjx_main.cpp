@@ -1,5 +1,5 @@
 // qjx_main.cpp -- qjx_b200: process-level drop-in for the reference's qjx executable on the
-// Std task with the QJ propagator (sys_id 0, task_id 1, prop_id 0).
+// Std task with the QJ propagator (sys_id 0, task_id 1, prop_id 0) or the RK propagator (prop_id 1).
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -71,7 +71,8 @@ int main(int argc, char **argv)
 
     if (rp.sys_id != 0) die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer, sys_id 0)");
     if (rp.task_id != 1) die("Wrong task_id: " + std::to_string(rp.task_id) + " (this engine runs the Std task, task_id 1)");
-    if (rp.prop_id != 0) die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ propagator, prop_id 0)");
+    if (rp.prop_id != 0 && rp.prop_id != 1)
+        die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
 
     try {
         cp.fn_suffix = dimer_suffix(rp, cp, 4);
@@ -117,8 +118,9 @@ int main(int argc, char **argv)
             save_complex_data(path + "dissipator_0" + sfx, L.data(), dd, 16, false);
             for (int b = 0; b < 2; b++) {
                 save_complex_data(path + "hamiltonians_qj_" + std::to_string(b) + sfx, K.data() + 2 * dd * b, dd, 16, false);
-                save_complex_data(path + "exp_mtx_" + std::to_string(b) + sfx, Ut.data() + 2 * dd * ((size_t)b * deep + deep - 1),
-                                  dd, 16, false);
+                if (rp.prop_id == 0)  // the split tree exists for the QJ propagator only (qj_proc.cpp:115-119)
+                    save_complex_data(path + "exp_mtx_" + std::to_string(b) + sfx,
+                                      Ut.data() + 2 * dd * ((size_t)b * deep + deep - 1), dd, 16, false);
             }
         }
         std::vector<double> HE(2 * dd);
@@ -151,8 +153,17 @@ int main(int argc, char **argv)
         cfg.device = device;
         const double gr[1] = {1.0};  // head->g (core.cpp:9905)
         qjx_engine *h = nullptr;
-        check(qjx_create(&cfg, Ut.data(), L.data(), gr, HE.data(), num_robs ? R.data() : nullptr, &h), nullptr,
-              "qjx_create");
+        if (rp.prop_id == 0) {
+            check(qjx_create(&cfg, Ut.data(), L.data(), gr, HE.data(), num_robs ? R.data() : nullptr, &h), nullptr,
+                  "qjx_create");
+        } else {  // RK propagator: rk_right_part_dimer's drive keys (core.cpp:11048-11051)
+            std::vector<double> He(2 * dd), Hdr(2 * dd);
+            check(qjx_build_dimer_rk(N, J, U, E, g, He.data(), Hdr.data()), nullptr, "qjx_build_dimer_rk");
+            check(qjx_create_rk(&cfg, He.data(), Hdr.data(), E, A, int(param_or(cp, "dimer_drv_type", 0)), omega,
+                                param_or(cp, "dimer_drv_phase", 0.0), cp.rk_ns, L.data(), gr, HE.data(),
+                                num_robs ? R.data() : nullptr, &h),
+                  nullptr, "qjx_create_rk");
+        }
 
         // init_data: start states (newdel_exp.cpp:656-679)
         std::vector<double> psi(2 * (size_t)n * d, 0.0);

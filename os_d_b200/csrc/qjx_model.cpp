@@ -198,6 +198,21 @@ extern "C" qjx_status qjx_expm(int n, const double *A, double *out)
     return expm(n, A, out) ? QJX_OK : QJX_ERR_INVALID_ARG;
 }
 
+// H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352) of real L; returns (hr, hi) of element (i, j)
+static void heff_element(int d, const cvec &h, const cvec &l, double gamma, int i, int j, double &hr, double &hi)
+{
+    double sr = 0.0, si = 0.0;
+    for (int k = 0; k < d; k++) {
+        const double ar = l[2 * ((size_t)k * d + i)], ai = l[2 * ((size_t)k * d + i) + 1];
+        const double br = l[2 * ((size_t)k * d + j)], bi = l[2 * ((size_t)k * d + j) + 1];
+        sr = sr + (ar * br + ai * bi);
+        si = si + (ar * bi - ai * br);
+    }
+    const size_t idx = (size_t)i * d + j;
+    hr = h[2 * idx] + 0.5 * (gamma * si);
+    hi = 0.0 - 0.5 * (gamma * sr);
+}
+
 extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega,
                                       int deep, double *H, double *Hd, double *L, double *Kout, double *Utree)
 {
@@ -231,16 +246,9 @@ extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, doubl
     const double Eb[2] = {E + A, E - A};
     for (int i = 0; i < d; i++)
         for (int j = 0; j < d; j++) {
-            double sr = 0.0, si = 0.0;
-            for (int k = 0; k < d; k++) {
-                const double ar = l[2 * ((size_t)k * d + i)], ai = l[2 * ((size_t)k * d + i) + 1];
-                const double br = l[2 * ((size_t)k * d + j)], bi = l[2 * ((size_t)k * d + j) + 1];
-                sr = sr + (ar * br + ai * bi);
-                si = si + (ar * bi - ai * br);
-            }
             const size_t idx = (size_t)i * d + j;
-            const double hr = h[2 * idx] + 0.5 * (gamma * si);
-            const double hi = 0.0 - 0.5 * (gamma * sr);
+            double hr, hi;
+            heff_element(d, h, l, gamma, i, j, hr, hi);
             for (int b = 0; b < 2; b++) {
                 K[b][2 * idx] = 0.0 + (hi + Eb[b] * 0.0);
                 K[b][2 * idx + 1] = 0.0 - (hr + Eb[b] * hd[2 * idx]);
@@ -270,4 +278,23 @@ extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, doubl
             ok = expm(d, scaled.data(), Utree + e2 * ((size_t)b * deep + lv)) && ok;
         }
     return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}
+
+// Operators of the RK propagator: H_eff = non_drv_part and H_drv = drv_part (newdel.cpp:2354-2366).
+extern "C" qjx_status qjx_build_dimer_rk(int N, double J, double U, double E, double g, double *H_eff, double *H_drv)
+{
+    if (N < 1 || !H_eff || !H_drv) return QJX_ERR_INVALID_ARG;
+    const int d = N + 1;
+    const size_t e2 = 2 * (size_t)d * d;
+    cvec h(e2), hd(e2), l(e2);
+    const qjx_status st = qjx_build_dimer(N, J, U, E, 0.0, g, 1.0, 1, h.data(), hd.data(), l.data(), nullptr, nullptr);
+    if (st != QJX_OK) return st;
+    const double gamma = g / double(d - 1);
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            const size_t idx = (size_t)i * d + j;
+            heff_element(d, h, l, gamma, i, j, H_eff[2 * idx], H_eff[2 * idx + 1]);
+        }
+    std::memcpy(H_drv, hd.data(), e2 * sizeof(double));
+    return QJX_OK;
 }

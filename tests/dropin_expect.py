@@ -82,18 +82,33 @@ def expected_outputs(cfg, prm, R=None):
     nr = int(prm["num_random_obs"])
     ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
     ens.init(int(prm["start_type"]), int(prm["start_state"]))
+    prop = cfg.get("prop_id", 0)
+    period = [0]  # the RK propagator's period_id, reset with the times after the transient
+
+    def advance(k, is_obs=1):
+        if prop == 0:
+            return ens.run_periods(k, is_obs=is_obs)
+        Heff = O.dimer_heff(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"], prm["diss_gamma"])
+        rc = ens.run_periods_rk(k, Heff, Hd, prm["dimer_prm_E"], prm["dimer_drv_ampl"], cfg.get("rk_ns", 1000),
+                                period0=period[0], drv_type=int(prm.get("dimer_drv_type", 0)),
+                                freq=prm["dimer_drv_freq"], phase=prm.get("dimer_drv_phase", 0.0), is_obs=is_obs)
+        period[0] += k
+        return rc
+
     files = {}
     if cfg.get("is_debug", 0):
         files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
         files[path + "dissipator_0" + sfx] = f_complex_data(L.reshape(-1))
         files[path + "hamiltonians_qj_0" + sfx] = f_complex_data(K0.reshape(-1))
         files[path + "hamiltonians_qj_1" + sfx] = f_complex_data(K1.reshape(-1))
-        files[path + "exp_mtx_0" + sfx] = f_complex_data(U[0, -1].reshape(-1))
-        files[path + "exp_mtx_1" + sfx] = f_complex_data(U[1, -1].reshape(-1))
+        if cfg.get("prop_id", 0) == 0:
+            files[path + "exp_mtx_0" + sfx] = f_complex_data(U[0, -1].reshape(-1))
+            files[path + "exp_mtx_1" + sfx] = f_complex_data(U[1, -1].reshape(-1))
     dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
     ndt = len(dp)
-    assert ens.run_periods(cfg.get("num_tp_periods", 0), is_obs=0) == 0
+    assert advance(cfg.get("num_tp_periods", 0), is_obs=0) == 0
     ens.t[:] = 0.0
+    period[0] = 0
     obs = [ens.observables(is_start=True, want_adr=True)]
     evo_sep, adr_sep = int(prm["dump_evo_sep"]), int(prm["dump_adr_sep"])
     evo_avg, adr_avg_on = int(prm["dump_evo_avg"]), int(prm["dump_adr_avg"])
@@ -127,12 +142,12 @@ def expected_outputs(cfg, prm, R=None):
         span = dp[dump_id] - dp[dump_id - 1]
         if lim > 0:
             for _ in range(span):
-                assert ens.run_periods(1, is_obs=1) == 0
+                assert advance(1) == 0
                 if np.all(ens.jumps_counts >= lim):
                     finished = True
                     break
         elif span > 0:
-            assert ens.run_periods(span, is_obs=1) == 0
+            assert advance(span) == 0
         obs.append(ens.observables(want_adr=True))
         if dump_purity == 1:
             purity.append(O.purity(ens.phi)[0])

@@ -45,7 +45,7 @@ def test_params_echo_format(tmp_path):
     assert "diss_gamma: 0.1\n" in r.stdout and "N: 16\n" in r.stdout
 
 
-@pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 7), ("prop_id", 1)])
+@pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 7), ("prop_id", 2)])
 def test_unsupported_ids_exit_with_error(tmp_path, key, val):
     r = check(tmp_path, dict(BASE_CONFIG, **{key: val}), BASE_PARAMS)
     assert r.returncode != 0 and "Error: Wrong " + key in r.stdout

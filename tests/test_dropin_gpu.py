@@ -67,3 +67,11 @@ def test_purity_per_dump(tmp_path):
     exp = run_case(tmp_path, cfg, prm)
     vals = [float(v) for k, t in exp.items() if k.startswith("purity_evo") for v in t.split()]
     assert len(vals) == 4 and 0.0 < min(vals) <= max(vals) < 1.0  # dump 0 follows the transient periods
+
+
+def test_rk_propagator_files_match(tmp_path):
+    cfg = dict(BASE_CONFIG, prop_id=1, rk_ns=400, num_tp_periods=1, num_obs_periods=3, num_trajectories=12,
+               is_debug=1)
+    prm = dict(BASE_PARAMS, dump_num=3, jump=2)
+    exp = run_case(tmp_path, cfg, prm)
+    assert any(k.startswith("jump_times_") and exp[k] for k in exp)

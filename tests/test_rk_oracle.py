@@ -75,3 +75,12 @@ def test_rk_ensemble_within_statistical_error_of_fbasis_rho():
     adr = ens.observables(want_adr=True)["adr"]
     err = adr.std(axis=0) / np.sqrt(n)
     assert np.all(np.abs(adr.mean(axis=0) - pops_f) < 4.5 * err + 2e-3), (adr.mean(axis=0), pops_f)
+
+
+@pytest.mark.parametrize("N", [5, 100])
+def test_library_rk_operators_equal_oracle(N):
+    import os_d_b200 as q
+
+    He, Hd = q.build_dimer_rk(N, 1.0, 0.5, 1.0, 0.1)
+    assert np.array_equal(He, O.dimer_heff(N, 1.0, 0.5, 1.0, 0.1))
+    assert np.array_equal(Hd, O.dimer_operators(N, 1.0, 0.5, 1.0, 1.5, 0.1)[1])
