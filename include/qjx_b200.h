@@ -72,6 +72,12 @@ typedef struct {
     int device;        /* CUDA device ordinal */
     int64_t tr_base;   /* global index of trajectory 0 (Philox stream id = tr_base + local index), so
                           an ensemble sharded over GPUs draws exactly the numbers of one big run */
+    int deep_num_steps; /* 0: Std task.  > 0: StdDeep task (task_id 4): every branch runs as
+                          2 deep_num_steps units of the split tree of T_sub = T / (2 deep_num_steps)
+                          (give U from qjx_build_dimer_deep), and observation runs (is_obs 1) take
+                          the observables after every sub-period into consecutive dump slots from
+                          dump_base, num_branches deep_num_steps per period (ex_period_obs_deep,
+                          core.cpp:114-153); dump_at must then be empty. */
     int precision;     /* 0: complex FP64 end to end (the reference's arithmetic, bit-exact with the
                           oracle); 1: split precision: every d x d matvec runs on the tcgen05 tensor
                           cores as bf16 hi/lo planes with FP32 accumulation (products hi*hi + hi*lo +
@@ -157,6 +163,10 @@ qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_t
  * T = 2 pi / omega.  Any output may be NULL. */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
                            double *H, double *Hd, double *L, double *K, double *Utree);
+/* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)
+ * (init_split_structure_dimer_deep, core.cpp:9928-9981). */
+qjx_status qjx_build_dimer_deep(int N, double J, double U, double E, double A, double g, double omega, int deep,
+                                int deep_num_steps, double *H, double *Hd, double *L, double *K, double *Utree);
 /* Operators of the RK propagator: H_eff = H - (i/2)(g/N) L^H L (non_drv_part) and H_drv
  * (drv_part), built by DimerNewDelBehaviour::init_hamiltonians_qj (newdel.cpp:2285-2366). */
 qjx_status qjx_build_dimer_rk(int N, double J, double U, double E, double g, double *H_eff, double *H_drv);

@@ -51,6 +51,7 @@ def lib():
         L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
         L.orc_philox_uniform.restype = C.c_double
         L.orc_init.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int, C.c_int]
+        L.orc_run_branch_units.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState)] + [C.c_int] * 6
         L.orc_run_periods_rk.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcRk), C.POINTER(OrcState), C.c_int,
                                          C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_run_periods.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int, C.c_int, C.c_int,
@@ -199,6 +200,11 @@ class Ensemble:
     def run_periods(self, n_periods, is_obs=1, tr0=0, tr1=None, n_threads=0):
         tr1 = self.n if tr1 is None else tr1
         return lib().orc_run_periods(C.byref(self.p), C.byref(self.s), tr0, tr1, n_periods, is_obs, n_threads)
+
+    def run_branch_units(self, b, n_units, is_obs=1, tr0=0, tr1=None, n_threads=0):
+        """n_units runs of branch b from level 0 (deep tasks: a sub-period is two units)."""
+        tr1 = self.n if tr1 is None else tr1
+        return lib().orc_run_branch_units(C.byref(self.p), C.byref(self.s), tr0, tr1, b, n_units, is_obs, n_threads)
 
     def run_periods_rk(self, n_periods, ND, DR, E0, A, rk_ns, period0=0, drv_type=0, freq=1.0, phase=0.0, is_obs=1,
                        tr0=0, tr1=None, n_threads=0):

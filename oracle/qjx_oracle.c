@@ -708,6 +708,43 @@ int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_
     return bad;
 }
 
+/* n_units units of branch b (one_period_branch from level 0): the deep tasks' building block,
+ * one sub-period being two units (one_sub_period_deep, qj_proc.cpp:345-359); p->T is the tree
+ * head's dt, T / (2 deep_num_steps) for the deep tasks (core.cpp:9934). */
+int orc_run_branch_units(const orc_problem *p, orc_state *s, int tr0, int tr1, int b, int n_units, int is_obs,
+                         int n_threads)
+{
+    if (p->deep < 1 || p->deep > 60 || b < 0 || b >= p->num_branches) return 1;
+    int bad = 0;
+    tmat tU, tL;
+    if (tmat_make(p->d, p->num_branches * p->deep, p->U, &tU) || tmat_make(p->d, p->num_diss, p->L, &tL)) return 2;
+#ifdef _OPENMP
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads) reduction(+ : bad)
+#endif
+    for (int tr = tr0; tr < tr1; tr++) {
+        if (s->error[tr]) { bad++; continue; }
+        const int d = p->d;
+        traj_ctx c = {0};
+        c.p = p; c.s = s; c.tr = tr; c.is_obs = is_obs;
+        c.tU = &tU; c.tL = &tL;
+        c.phi = s->phi + 2 * (size_t)tr * d;
+        c.aux = (double *)calloc(2 * (size_t)d, sizeof(double));
+        c.res = (double *)calloc(2 * (size_t)d, sizeof(double));
+        c.gn = (double *)calloc((size_t)p->num_diss + 1, sizeof(double));
+        double dt = p->T * 0.5;
+        for (int l = 0; l < p->deep; l++) { dt *= 0.5; c.dt[l] = dt; }
+        for (int u = 0; u < n_units && !c.err; u++) one_period_branch(&c, b, 0);
+        s->error[tr] = c.err;
+        if (c.err) bad++;
+        free(c.aux); free(c.res); free(c.gn);
+    }
+    (void)n_threads;
+    tmat_free(&tU);
+    tmat_free(&tL);
+    return bad;
+}
+
 /* ------------------------------------------------------------------ RK propagator */
 
 /* E(t) of rk_right_part_dimer (core.cpp:11073-11103) */

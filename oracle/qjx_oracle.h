@@ -113,6 +113,12 @@ int orc_init(const orc_problem *p, orc_state *s, int start_type, int start_state
  * exactly like ed->is_obs (qj_proc.cpp:296).  OpenMP over trajectories. */
 int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_periods, int is_obs, int n_threads);
 
+/* Deep tasks (task_id 4, StdDeep): n_units runs of branch b from split level 0; a sub-period is
+ * two units (one_sub_period_deep, qj_proc.cpp:345-359; ex_period_obs_deep, core.cpp:114-153).
+ * The problem's T must be the tree head's dt, T_period / (2 deep_num_steps). */
+int orc_run_branch_units(const orc_problem *p, orc_state *s, int tr0, int tr1, int b, int n_units, int is_obs,
+                         int n_threads);
+
 /* RK propagator (prop_id 1): dpsi/dt = -i (H_eff + E(t) H_drv) psi by classic RK4 with rk_ns
  * steps per period and a jump located by linear interpolation of the norm inside a step.
  *   rk_period          source/cpp/QJX/QJX/core.cpp:439-450 (t = period T + step rk_step)

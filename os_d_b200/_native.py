@@ -17,7 +17,7 @@ c_i64_p = C.POINTER(C.c_int64)
 
 # every entry point declared in include/qjx_b200.h
 EXPORTS = [
-    "qjx_create", "qjx_create_rk", "qjx_build_dimer_rk", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
+    "qjx_create", "qjx_create_rk", "qjx_build_dimer_rk", "qjx_build_dimer_deep", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
@@ -29,7 +29,8 @@ class QjxConfig(C.Structure):
     _fields_ = [("d", C.c_int), ("n_traj", C.c_int), ("deep", C.c_int), ("num_branches", C.c_int),
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
-                ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("precision", C.c_int)]
+                ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("deep_num_steps", C.c_int),
+                ("precision", C.c_int)]
 
 
 class QjxStats(C.Structure):
@@ -81,6 +82,7 @@ def lib():
         L.qjx_get_trace.argtypes = [vp, c_i64_p, c_int_p, c_int_p]
         L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
+        L.qjx_build_dimer_deep.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int, C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_build_dimer_rk.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 2
         L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -126,6 +128,18 @@ def build_dimer(N, J, U, E, A, g, omega, deep):
     Ut = np.zeros((2, deep, d, d), np.complex128)
     check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(Lm), None, dp(Ut)),
           what="qjx_build_dimer")
+    return H, Hd, Lm, Ut
+
+
+def build_dimer_deep(N, J, U, E, A, g, omega, deep, deep_num_steps):
+    """build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)."""
+    d = N + 1
+    H = np.zeros((d, d), np.complex128)
+    Hd = np.zeros_like(H)
+    Lm = np.zeros_like(H)
+    Ut = np.zeros((2, deep, d, d), np.complex128)
+    check(lib().qjx_build_dimer_deep(N, J, U, E, A, g, omega, deep, deep_num_steps, dp(H), dp(Hd), dp(Lm), None,
+                                     dp(Ut)), what="qjx_build_dimer_deep")
     return H, Hd, Lm, Ut
 
 

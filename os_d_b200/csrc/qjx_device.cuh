@@ -58,7 +58,7 @@ struct __align__(16) TrajState {
     double rk_h;       // step being integrated: rk_step, or the begin / end part around a jump
     double rk_prev;    // norm of psi before the step
     double rk_end;     // end part still to integrate after a located jump
-    int rk_sid;        // step index within the period
+    int rk_sid;        // RK: step index within the period; QJ: units done in the current branch
     int rk_stage;      // 1..4: right-hand side being evaluated
     int rk_part;       // 0: H_eff arg, 1: H_drv arg
     int rk_ctx;        // 0: step checked for a crossing; 1: begin part of a located jump
@@ -116,6 +116,9 @@ struct Params {
     int prop;                     // 0 QJ split tree, 1 RK
     int rk_ns, period0, drv_type;
     double rk_step, T, E0, A, drv_freq, drv_phase;
+    // deep tasks (StdDeep): each branch runs brep = 2 deep_num_steps units of two level-0 steps;
+    // with subdump the observables are taken after every sub-period (two units)
+    int brep, subdump;
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns

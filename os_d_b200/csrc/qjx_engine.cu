@@ -254,9 +254,13 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
         P.usplit = us;
     }
 
-    // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24)
+    // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24); the deep tasks'
+    // tree head is the sub-period T / (2 deep_num_steps) (core.cpp:9934)
+    if (c.deep_num_steps < 0) return bail(QJX_ERR_INVALID_ARG);
+    P.brep = c.deep_num_steps > 0 ? 2 * c.deep_num_steps : 1;
+    const double t_head = c.deep_num_steps > 0 ? 0.5 * c.T / double(c.deep_num_steps) : c.T;
     std::vector<double> dts(c.deep);
-    double dt = c.T * 0.5;
+    double dt = t_head * 0.5;
     for (int l = 0; l < c.deep; l++) {
         dt *= 0.5;
         dts[l] = dt;
@@ -553,6 +557,7 @@ extern "C" qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, 
     qjx_config c = *cfg;
     c.num_branches = 1;  // groups 0 and 1: H_eff and H_drv
     c.deep = 2;
+    c.deep_num_steps = 0;
     const size_t dd2 = (size_t)2 * c.d * c.d;
     std::vector<double> M(2 * dd2);
     std::memcpy(M.data(), H_eff, dd2 * sizeof(double));
@@ -579,6 +584,10 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
     if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
     if (dump_base < 0 || dump_base + n_dumps > h->cfg.max_dumps)
         return fail(h, QJX_ERR_INVALID_ARG, "dump slots exceed max_dumps");
+    const int subdump = (h->cfg.deep_num_steps > 0 && is_obs == 1) ? 1 : 0;
+    if (subdump && (n_dumps > 0 ||
+                    dump_base + (long long)n_periods * h->cfg.num_branches * h->cfg.deep_num_steps > h->cfg.max_dumps))
+        return fail(h, QJX_ERR_INVALID_ARG, "deep task: dump_at must be empty and every sub-period needs a dump slot");
     for (int i = 0; i < n_dumps; i++)
         if (dump_at[i] < 1 || dump_at[i] > n_periods || (i > 0 && dump_at[i] <= dump_at[i - 1]))
             return fail(h, QJX_ERR_INVALID_ARG, "dump_at must be ascending within 1..n_periods");
@@ -596,6 +605,7 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
     P.n_dumps = n_dumps;
     P.dump_base = dump_base;
     P.target = n_periods;
+    P.subdump = subdump;
     P.record = (is_obs == 1 && h->cfg.record > 0) ? 1 : 0;
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
@@ -619,6 +629,7 @@ extern "C" qjx_status qjx_observe(qjx_engine *h, int dump, int is_start)
     P.n_dumps = 1;
     P.dump_base = dump;
     P.record = 0;
+    P.subdump = 0;
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
     CK(launch_observe(P, dump, is_start, h->stream));

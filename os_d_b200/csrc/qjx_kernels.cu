@@ -100,8 +100,10 @@ __device__ __forceinline__ void report_error(const Params &P, int tr, int code)
 // Counter bookkeeping after a completed step at level s.lvl (qj_proc.cpp:317-320, 330-338):
 // advance the level's counter; a level that finished both steps returns to its parent,
 // which undoes and redoes its own time advance (t -= dt; t += dt) and counts its step.
-// Returns true when the last branch of a period finished.
-__device__ __forceinline__ bool advance(TrajState &s, const double *dt, int nb)
+// Returns 0 inside a unit (two level-0 steps), 1 when a unit finished, 2 when the last unit
+// of the last branch of a period finished.  A branch has brep units (1, or 2 deep_num_steps
+// for the deep tasks, whose sub-period is two units: one_sub_period_deep, qj_proc.cpp:345-359).
+__device__ __forceinline__ int advance(TrajState &s, const double *dt, int nb, int brep)
 {
     int l = s.lvl;
     unsigned long long m = s.mask;
@@ -110,18 +112,20 @@ __device__ __forceinline__ bool advance(TrajState &s, const double *dt, int nb)
             m |= (1ull << l);
             s.lvl = l;
             s.mask = m;
-            return false;
+            return 0;
         }
         m &= ~(1ull << l);
         if (l == 0) {
             s.mask = m;
             s.lvl = 0;
+            if (++s.rk_sid < brep) return 1;
+            s.rk_sid = 0;
             s.b += 1;
             if (s.b == nb) {
                 s.b = 0;
-                return true;
+                return 2;
             }
-            return false;
+            return 1;
         }
         l -= 1;
         s.t = __dadd_rn(__dsub_rn(s.t, dt[l]), dt[l]);
@@ -175,8 +179,14 @@ __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const doub
 // next group, or -1 when the trajectory is done for this call.
 __device__ int after_step(const Params &P, TrajState &s, int tr, const double2 *col, double *wscr, int lane)
 {
-    if (advance(s, P.dt, P.nb)) {
-        s.pc += 1;
+    const int a = advance(s, P.dt, P.nb, P.brep);
+    if (a == 2) s.pc += 1;
+    if (a >= 1 && P.subdump && (s.rk_sid & 1) == 0) {  // deep task: a sub-period ended
+        obs_prep(P, s, tr, col, wscr, lane, P.dump_base + s.di, 0);
+        s.phase = PH_OBS_E;
+        return P.gHE;
+    }
+    if (a == 2) {
         if (s.di < P.n_dumps && s.pc == P.dump_at[s.di]) {
             obs_prep(P, s, tr, col, wscr, lane, P.dump_base + s.di, 0);
             s.phase = PH_OBS_E;
@@ -840,6 +850,7 @@ __global__ void schedule_kernel(const Params P, int mode)
         s.b = 0;
         s.lvl = 0;
         s.mask = 0;
+        s.rk_sid = 0;
         s.paused = 0;
         s.phase = (P.target > 0) ? PH_STEP : PH_DONE;
     } else {

@@ -213,8 +213,27 @@ static void heff_element(int d, const cvec &h, const cvec &l, double gamma, int 
     hi = 0.0 - 0.5 * (gamma * sr);
 }
 
+static qjx_status build_dimer_impl(int N, double J, double U, double E, double A, double g, double omega, int deep,
+                                   int deep_num_steps, double *H, double *Hd, double *L, double *Kout, double *Utree);
+
 extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega,
                                       int deep, double *H, double *Hd, double *L, double *Kout, double *Utree)
+{
+    return build_dimer_impl(N, J, U, E, A, g, omega, deep, 0, H, Hd, L, Kout, Utree);
+}
+
+// Deep tasks: the split tree of a sub-period T_sub = T / (2 deep_num_steps)
+// (init_split_structure_dimer_deep, core.cpp:9928-9940).
+extern "C" qjx_status qjx_build_dimer_deep(int N, double J, double U, double E, double A, double g, double omega,
+                                           int deep, int deep_num_steps, double *H, double *Hd, double *L,
+                                           double *Kout, double *Utree)
+{
+    if (deep_num_steps < 1) return QJX_ERR_INVALID_ARG;
+    return build_dimer_impl(N, J, U, E, A, g, omega, deep, deep_num_steps, H, Hd, L, Kout, Utree);
+}
+
+static qjx_status build_dimer_impl(int N, double J, double U, double E, double A, double g, double omega, int deep,
+                                   int deep_num_steps, double *H, double *Hd, double *L, double *Kout, double *Utree)
 {
     if (N < 1 || deep < 1 || !(omega > 0.0)) return QJX_ERR_INVALID_ARG;
     const int d = N + 1;
@@ -259,7 +278,8 @@ extern "C" qjx_status qjx_build_dimer(int N, double J, double U, double E, doubl
         std::memcpy(Kout + e2, K[1].data(), e2 * sizeof(double));
     }
     if (!Utree) return QJX_OK;
-    const double T = 2.0 * 3.1415926535897932384626433832795 / omega;
+    const double Tp = 2.0 * 3.1415926535897932384626433832795 / omega;
+    const double T = deep_num_steps > 0 ? 0.5 * Tp / double(deep_num_steps) : Tp;  // the tree head's dt
     std::vector<double> dts(deep);
     double dt = T * 0.5;
     for (int lv = 0; lv < deep; lv++) {
