@@ -1,5 +1,6 @@
 // qjx_main.cpp -- qjx_b200: process-level drop-in for the reference's qjx executable on the
-// Std task with the QJ propagator (sys_id 0, task_id 1, prop_id 0) or the RK propagator (prop_id 1).
+// Std task (task_id 1) with the QJ propagator (prop_id 0) or the RK propagator (prop_id 1), and the
+// StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0).
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -70,7 +71,9 @@ int main(int argc, char **argv)
     std::cout << params_echo(rp, cp);
 
     if (rp.sys_id != 0) die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer, sys_id 0)");
-    if (rp.task_id != 1) die("Wrong task_id: " + std::to_string(rp.task_id) + " (this engine runs the Std task, task_id 1)");
+    if (rp.task_id != 1 && rp.task_id != 4)
+        die("Wrong task_id: " + std::to_string(rp.task_id) + " (this engine runs the Std (1) and StdDeep (4) tasks)");
+    if (rp.task_id == 4 && rp.prop_id != 0) die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (StdDeep runs the QJ propagator)");
     if (rp.prop_id != 0 && rp.prop_id != 1)
         die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
 
@@ -109,8 +112,17 @@ int main(int argc, char **argv)
 
         // model (newdel.cpp init_*), debug dumps (debugger.cpp:142-168, qj_proc.cpp:115-119)
         std::vector<double> H(2 * dd), Hd(2 * dd), L(2 * dd), K(4 * dd), Ut(4 * dd * deep);
-        check(qjx_build_dimer(N, J, U, E, A, g, omega, deep, H.data(), Hd.data(), L.data(), K.data(), Ut.data()),
-              nullptr, "qjx_build_dimer");
+        // StdDeep (task_id 4): the split tree of the sub-period T / (2 deep_num_steps)
+        const bool deep_task = rp.task_id == 4;
+        const int nsub = deep_task ? int(param(cp, "deep_num_steps")) : 0;
+        if (deep_task && nsub < 1) die("deep_num_steps must be positive");
+        if (deep_task)
+            check(qjx_build_dimer_deep(N, J, U, E, A, g, omega, deep, nsub, H.data(), Hd.data(), L.data(), K.data(),
+                                       Ut.data()),
+                  nullptr, "qjx_build_dimer_deep");
+        else
+            check(qjx_build_dimer(N, J, U, E, A, g, omega, deep, H.data(), Hd.data(), L.data(), K.data(), Ut.data()),
+                  nullptr, "qjx_build_dimer");
         std::cout << "init_sizes" << std::endl << "init_hamiltonians" << std::endl << "init_dissipators" << std::endl
                   << "init_hamiltonians_qj" << std::endl;
         if (rp.is_debug) {
@@ -130,7 +142,16 @@ int main(int argc, char **argv)
                                int(param_or(cp, "random_obs_type", 0)));
 
         // dump schedule (init_dump_periods)
-        const std::vector<int> dp = dump_periods(int(param(cp, "dump_type")), int(param(cp, "dump_num")), cp.num_obs_periods);
+        // StdDeep: a dump after every sub-period, labelled with its period (init_dump_periods_deep,
+        // newdel_exp.cpp:377-406)
+        std::vector<int> dp;
+        if (deep_task) {
+            dp.push_back(0);
+            for (int p = 0; p < cp.num_obs_periods; p++)
+                for (int k = 0; k < 2 * nsub; k++) dp.push_back(p);
+        } else {
+            dp = dump_periods(int(param(cp, "dump_type")), int(param(cp, "dump_num")), cp.num_obs_periods);
+        }
         if (dp.empty()) die("Wrong dump_type");
         const int ndt = (int)dp.size();
         bool increasing = true;
@@ -150,6 +171,7 @@ int main(int argc, char **argv)
         cfg.rec_cap = 1024;
         cfg.keep_adr = ((dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1) ? 1 : 0;
         cfg.max_dumps = ndt;
+        cfg.deep_num_steps = nsub;
         cfg.device = device;
         const double gr[1] = {1.0};  // head->g (core.cpp:9905)
         qjx_engine *h = nullptr;
@@ -219,12 +241,23 @@ int main(int argc, char **argv)
         if (dump_evo_avg == 1) write_adr_avg(0, false);
 
         // obser_process (experiment.cpp:448-542)
-        if (dump_phi_evo_on == 1) write_phi("phi_evo_", false);
+        if (dump_phi_evo_on == 1 && !deep_task) write_phi("phi_evo_", false);
         int last_dump = 0;
         const bool per_interval = jumps_counts_lim > 0 || !increasing || dump_phi_evo_on == 1 ||
                                   (dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1 || rp.is_pp == 1 ||
                                   dump_purity == 1;
-        if (!per_interval) {
+        if (deep_task) {
+            // StdDeep obser_process (experiment.cpp:806-845): a period per step, observables after
+            // every sub-period inside it, adr files per sub-period, adr_avg per period
+            const int per_period = 2 * nsub;
+            for (int p = 0; p < cp.num_obs_periods; p++) {
+                if (rp.is_pp == 1) std::cout << "dump_id: " << p + 1 << std::endl;
+                check(qjx_run_periods(h, 1, 1, nullptr, 0, 1 + p * per_period), h, "qjx_run_periods");
+                for (int k = 0; k < per_period; k++) write_adr_single(1 + p * per_period + k, true);
+                if (dump_evo_avg == 1) write_adr_avg(per_period * (p + 1), true);
+            }
+            last_dump = ndt - 1;
+        } else if (!per_interval) {
             // one call: every trajectory runs all observation periods, observables at each dump
             std::vector<int> at(dp.begin() + 1, dp.end());
             if (ndt > 1) check(qjx_run_periods(h, dp[ndt - 1], 1, at.data(), ndt - 1, 1), h, "qjx_run_periods");
@@ -288,8 +321,8 @@ int main(int argc, char **argv)
             save_double_data(path + "m2" + sfx, D.m2.data() + o, n, 16, false);
             save_double_data(path + "energy" + sfx, D.energy.data() + o, n, 16, false);
         }
-        if (dump_phi_on == 1) write_phi("phi_", false);
-        if (dump_phi_evo_on == 1) write_phi("phi_evo_", true);
+        if (dump_phi_on == 1 && !deep_task) write_phi("phi_", false);
+        if (dump_phi_evo_on == 1 && !deep_task) write_phi("phi_evo_", true);
 
         // dump_std_evo (core.cpp:1008-1084): rows = dumps, columns = trajectories
         if (dump_evo_sep == 1 && dump_obs == 1) {

@@ -77,15 +77,20 @@ def expected_outputs(cfg, prm, R=None):
     H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
                                          prm["dimer_drv_ampl"], prm["diss_gamma"])
     T = TWO_PI / prm["dimer_drv_freq"]
-    U = np.stack([O.split_tree(K0, T, deep), O.split_tree(K1, T, deep)])
+    deep_task = cfg.get("task_id", 1) == 4
+    nsub = int(prm.get("deep_num_steps", 0)) if deep_task else 0
+    t_head = 0.5 * T / nsub if deep_task else T  # init_split_structure_dimer_deep's branch dt
+    U = np.stack([O.split_tree(K0, t_head, deep), O.split_tree(K1, t_head, deep)])
     HE = H + prm["dimer_prm_E"] * Hd
     nr = int(prm["num_random_obs"])
-    ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
+    ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, t_head, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
     ens.init(int(prm["start_type"]), int(prm["start_state"]))
     prop = cfg.get("prop_id", 0)
     period = [0]  # the RK propagator's period_id, reset with the times after the transient
 
     def advance(k, is_obs=1):
+        if deep_task:
+            return sum(ens.run_branch_units(b, 2 * nsub, is_obs=is_obs) for _ in range(k) for b in range(2))
         if prop == 0:
             return ens.run_periods(k, is_obs=is_obs)
         Heff = O.dimer_heff(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"], prm["diss_gamma"])
@@ -104,7 +109,10 @@ def expected_outputs(cfg, prm, R=None):
         if cfg.get("prop_id", 0) == 0:
             files[path + "exp_mtx_0" + sfx] = f_complex_data(U[0, -1].reshape(-1))
             files[path + "exp_mtx_1" + sfx] = f_complex_data(U[1, -1].reshape(-1))
-    dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
+    if deep_task:
+        dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(2 * nsub)]
+    else:
+        dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
     ndt = len(dp)
     assert advance(cfg.get("num_tp_periods", 0), is_obs=0) == 0
     ens.t[:] = 0.0
@@ -113,6 +121,8 @@ def expected_outputs(cfg, prm, R=None):
     evo_sep, adr_sep = int(prm["dump_evo_sep"]), int(prm["dump_adr_sep"])
     evo_avg, adr_avg_on = int(prm["dump_evo_avg"]), int(prm["dump_adr_avg"])
     phi_evo_on, phi_on = int(prm["dump_phi_evo"]), int(prm["dump_phi"])
+    if deep_task:  # StdDeep writes no phi files (experiment.cpp:806-845)
+        phi_evo_on = phi_on = 0
     lim = int(prm["jumps_counts"])
     dump_purity = int(prm.get("dump_purity", 0))  # optional key of the drop-in (not in QJX)
     purity = [O.purity(ens.phi)[0]] if dump_purity == 1 else []
@@ -138,7 +148,18 @@ def expected_outputs(cfg, prm, R=None):
         for tr in range(n):
             emit("phi_evo_%d" % tr + sfx, f_complex_data(ens.phi[tr]), False)
     finished = False
-    for dump_id in range(1, ndt):
+    if deep_task:  # StdDeep obser_process: observables after every sub-period
+        for _ in range(cfg.get("num_obs_periods", 10)):
+            for b in range(2):
+                for _ in range(nsub):
+                    assert ens.run_branch_units(b, 2) == 0
+                    obs.append(ens.observables(want_adr=True))
+                    if evo_sep == 1 and adr_sep == 1:
+                        for tr in range(n):
+                            emit("adr_%d" % tr + sfx, f_double_data(obs[-1]["adr"][tr]), True)
+            if evo_avg == 1 and adr_avg_on == 1:
+                emit("adr_avg" + sfx, f_double_data(adr_avg(obs[-1]["adr"])), True)
+    for dump_id in range(1, ndt if not deep_task else 1):
         span = dp[dump_id] - dp[dump_id - 1]
         if lim > 0:
             for _ in range(span):

@@ -75,3 +75,10 @@ def test_rk_propagator_files_match(tmp_path):
     prm = dict(BASE_PARAMS, dump_num=3, jump=2)
     exp = run_case(tmp_path, cfg, prm)
     assert any(k.startswith("jump_times_") and exp[k] for k in exp)
+
+
+def test_std_deep_task_files_match(tmp_path):
+    cfg = dict(BASE_CONFIG, task_id=4, num_tp_periods=1, num_obs_periods=2, num_trajectories=10, is_debug=1)
+    prm = dict(BASE_PARAMS, deep_num_steps=2, dump_adr_sep=1, dump_adr_avg=1, dump_evo_avg=1, jump=2)
+    exp = run_case(tmp_path, cfg, prm)
+    assert any(k.startswith("adr_0") for k in exp)
