@@ -147,6 +147,45 @@ qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, in
 qjx_status qjx_jump_count(qjx_engine *h, int tr, int64_t *count);
 qjx_status qjx_get_jumps(qjx_engine *h, int tr, double *times, int *types, double *norms, double *etas);
 qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats);
+/* Later qjx_run_periods calls advance trajectories [0, n_active) only (the others keep their
+ * states); the Lyapunov task runs its transient on the bases alone (LpnMultExperimentBehaviour::
+ * trans_process, experiment.cpp:147-155).  n_active = n_traj restores the default. */
+qjx_status qjx_set_active(qjx_engine *h, int n_active);
+
+/* Lyapunov paired trajectories (task_id 7, LpnMult; experiment.cpp:138-286).  n_traj is even;
+ * trajectories [0, n/2) are the bases and n/2 + b is the variation of base b. */
+typedef struct {
+    int lpn_type;         /* -1 mean, -2 energy, k >= 0 random observable k (calc_delta_s, core.cpp:839-901) */
+    int eps_deep;         /* lpn_eps_deep: bisection halvings at most */
+    int per_period;       /* lambda_per_periods: 0 lambda_lpn (renormalise on the thresholds), 1
+                             lambda_lpn_now (every period) */
+    int pad;
+    double eps_low, eps_high;  /* lpn_eps_low / lpn_eps_high: log10 bounds of the perturbation size */
+    double eps_error;     /* lpn_eps_error: tolerance on delta_s */
+    double delta_s;       /* lpn_delta_s: target distance after a perturbation */
+    double delta_f_high, delta_f_low;  /* lpn_delta_f_high / lpn_delta_f_low */
+    double max_energy;    /* max |Re H_ii| of the hamiltonian (init_obs_lpn, newdel_exp.cpp:540-550) */
+} qjx_lpn_config;
+/* After the bases' transient (trans_process, experiment.cpp:138-183): copy every base into its
+ * variation (psi, eta and jump stream: copy_trajectory_lpn, experiment.cpp:2221-2244), perturb
+ * it (var_trajectory_lpn, experiment.cpp:2278-2397; the direction is drawn from a per-trajectory
+ * variation stream) and set the Lyapunov characteristics (calc_chars_lpn_start, core.cpp:727-761).
+ * Follow with qjx_reset_times and qjx_observe(h, 0, 1). */
+qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *cfg);
+/* After one observation period (obser_process, experiment.cpp:209-240): calc_chars_lpn of the
+ * bases and lambda_lpn / lambda_lpn_now of the variations with curr_time = (period_id + 1) T.
+ * adr_dump >= 0: this period carried dump slot adr_dump, whose |psi_i|^2/|psi|^2 of the variations
+ * is replaced by the value after the update (abs_diag_rho_all after lambda_lpn); -1 otherwise. */
+qjx_status qjx_lpn_period(qjx_engine *h, double curr_time, int adr_dump);
+/* Current Lyapunov values per trajectory [n_traj] (robs_lpn [n_traj][num_robs] complex); any
+ * pointer may be NULL.  lambda_now is what lambda / lambda_evo dump (core.cpp:959-1000). */
+qjx_status qjx_lpn_get(qjx_engine *h, double *lambda_now, double *lambda, double *delta_s, double *mean_lpn,
+                       double *energy_lpn, double *robs_lpn, int *num_renorms);
+/* Renormalisations of the last qjx_lpn_start / qjx_lpn_period per trajectory: renormed (0/1),
+ * delta_f / delta_s, delta_s, delta_f (the save_lambdas records, experiment.cpp:3082-3088), the
+ * bisection halvings and the perturbation size eps; any pointer may be NULL. */
+qjx_status qjx_lpn_get_last(qjx_engine *h, int *renormed, double *ratio, double *delta_s, double *delta_f,
+                            int *eps_iters, double *eps);
 /* Per-CTA trace of the micro-step kernel (profiling aid, off by default): enabling clears
  * and starts accumulating, per persistent CTA, clock64 cycles {total, setup, (reserved),
  * MMA loop, epilogue} and counts {sub-tiles, 8-column blocks, columns}.  qjx_get_trace

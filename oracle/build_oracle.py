@@ -1,6 +1,6 @@
 """Build recipe for the CPU oracle (test infrastructure).
 
-Compiles oracle/qjx_oracle.c and oracle/fbasis_oracle.c into oracle/_build/liboracle.so.
+Compiles oracle/qjx_oracle.c, oracle/fbasis_oracle.c and oracle/lpn_oracle.c into oracle/_build/liboracle.so.
 The flags are part of the arithmetic contract shared with the CUDA engine:
 -ffp-contract=off keeps every expression literal, so only explicit fma() calls fuse.
 x86-64-v3 (AVX2 + FMA) keeps the library portable to the GPU box's host CPU.
@@ -11,7 +11,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "liboracle.so")
-SOURCES = ["qjx_oracle.c", "fbasis_oracle.c"]
+SOURCES = ["qjx_oracle.c", "fbasis_oracle.c", "lpn_oracle.c"]
 
 
 def build(force: bool = False) -> str:

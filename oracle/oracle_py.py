@@ -29,7 +29,21 @@ class OrcState(C.Structure):
     _fields_ = [("phi", c_double_p), ("eta", c_double_p), ("t", c_double_p), ("rng_pos", c_i64_p),
                 ("jumps_counts", c_int_p), ("matvecs", c_i64_p), ("rec_cap", C.c_int), ("n_rec", c_int_p),
                 ("jump_times", c_double_p), ("jump_norms", c_double_p), ("jump_etas", c_double_p),
-                ("diss_types", c_int_p), ("error", c_int_p)]
+                ("diss_types", c_int_p), ("error", c_int_p), ("rng_src", c_int_p)]
+
+
+class OrcLpnConfig(C.Structure):
+    _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
+                ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
+                ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
+                ("max_energy", C.c_double)]
+
+
+class OrcLpn(C.Structure):
+    _fields_ = [("lambda_", c_double_p), ("lambda_now", c_double_p), ("delta_s", c_double_p),
+                ("mean_lpn", c_double_p), ("energy_lpn", c_double_p), ("robs_lpn", c_double_p),
+                ("num_renorms", c_int_p), ("var_pos", c_i64_p), ("renormed", c_int_p), ("ratio", c_double_p),
+                ("ds_rec", c_double_p), ("df_rec", c_double_p), ("eps_iters", c_int_p), ("eps", c_double_p)]
 
 
 class OrcRk(C.Structure):
@@ -58,6 +72,14 @@ def lib():
                                       C.c_int, C.c_int]
         L.orc_observables.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.c_int] + [c_double_p] * 8
         L.orc_dump_periods.argtypes = [C.c_int, C.c_int, C.c_int, c_int_p]
+        L.orc_lpn_start.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.POINTER(OrcLpnConfig),
+                                    C.POINTER(OrcLpn)]
+        L.orc_lpn_period.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.POINTER(OrcLpnConfig),
+                                     C.POINTER(OrcLpn), C.c_double]
+        L.orc_lpn_exp10.argtypes = [C.c_double]
+        L.orc_lpn_exp10.restype = C.c_double
+        L.orc_lpn_log.argtypes = [C.c_double]
+        L.orc_lpn_log.restype = C.c_double
         L.orc_matvec.argtypes = [C.c_int, c_double_p, c_double_p, c_double_p]
         L.orc_norm_square.argtypes = [C.c_int, c_double_p]
         L.orc_norm_square.restype = C.c_double
@@ -191,6 +213,8 @@ class Ensemble:
         s.jump_times, s.jump_norms, s.jump_etas = _dp(self.jump_times), _dp(self.jump_norms), _dp(self.jump_etas)
         s.diss_types = self.diss_types.ctypes.data_as(c_int_p)
         s.error = self.error.ctypes.data_as(c_int_p)
+        self.rng_src = np.arange(n, dtype=np.int32)
+        s.rng_src = self.rng_src.ctypes.data_as(c_int_p)
         self.s = s
         self.mean_start = np.zeros(n)
 
@@ -235,6 +259,63 @@ class Ensemble:
         k = int(self.n_rec[tr])
         return (self.jump_times[tr, :k].copy(), self.diss_types[tr, :k].copy(),
                 self.jump_norms[tr, :k].copy(), self.jump_etas[tr, :k].copy())
+
+
+class Lpn:
+    """Lyapunov paired trajectories (task_id 7, LpnMult) over an Ensemble: bases [0, n/2),
+    variation n/2 + b of base b (orc_lpn_start / orc_lpn_period in lpn_oracle.c)."""
+
+    def __init__(self, ens, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10,
+                 delta_s=1e-3, delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0):
+        self.ens = ens
+        n = ens.n
+        self.cfg = OrcLpnConfig(lpn_type=lpn_type, eps_deep=eps_deep, per_period=int(per_period), eps_low=eps_low,
+                                eps_high=eps_high, eps_error=eps_error, delta_s=delta_s,
+                                delta_f_high=delta_f_high, delta_f_low=delta_f_low, max_energy=max_energy)
+        self.a = {k: np.zeros(n) for k in ("lambda", "lambda_now", "delta_s", "mean_lpn", "energy_lpn", "ratio",
+                                           "ds_rec", "df_rec", "eps")}
+        self.robs_lpn = np.zeros((n, max(ens.R.shape[0], 1)), np.complex128)
+        self.num_renorms = np.zeros(n, np.int32)
+        self.renormed = np.zeros(n, np.int32)
+        self.eps_iters = np.zeros(n, np.int32)
+        self.var_pos = np.zeros(n, np.int64)
+        s = OrcLpn()
+        s.lambda_, s.lambda_now, s.delta_s = _dp(self.a["lambda"]), _dp(self.a["lambda_now"]), _dp(self.a["delta_s"])
+        s.mean_lpn, s.energy_lpn = _dp(self.a["mean_lpn"]), _dp(self.a["energy_lpn"])
+        s.robs_lpn = _dp(self.robs_lpn)
+        s.num_renorms, s.renormed = self.num_renorms.ctypes.data_as(c_int_p), self.renormed.ctypes.data_as(c_int_p)
+        s.var_pos = self.var_pos.ctypes.data_as(c_i64_p)
+        s.ratio, s.ds_rec, s.df_rec, s.eps = _dp(self.a["ratio"]), _dp(self.a["ds_rec"]), _dp(self.a["df_rec"]), \
+            _dp(self.a["eps"])
+        s.eps_iters = self.eps_iters.ctypes.data_as(c_int_p)
+        self.s = s
+
+    def start(self):
+        st = lib().orc_lpn_start(C.byref(self.ens.p), C.byref(self.ens.s), C.byref(self.cfg), C.byref(self.s))
+        assert st == 0, st
+
+    def period(self, curr_time):
+        st = lib().orc_lpn_period(C.byref(self.ens.p), C.byref(self.ens.s), C.byref(self.cfg), C.byref(self.s),
+                                  float(curr_time))
+        assert st == 0, st
+
+    def values(self):
+        out = {k: self.a[k].copy() for k in ("lambda_now", "lambda", "delta_s", "mean_lpn", "energy_lpn")}
+        out["robs_lpn"] = self.robs_lpn[:, : self.ens.R.shape[0]].copy()
+        out["num_renorms"] = self.num_renorms.copy()
+        return out
+
+    def last(self):
+        return {"renormed": self.renormed.copy(), "ratio": self.a["ratio"].copy(), "delta_s": self.a["ds_rec"].copy(),
+                "delta_f": self.a["df_rec"].copy(), "eps_iters": self.eps_iters.copy(), "eps": self.a["eps"].copy()}
+
+
+def lpn_exp10(x):
+    return lib().orc_lpn_exp10(float(x))
+
+
+def lpn_log(x):
+    return lib().orc_lpn_log(float(x))
 
 
 # ---------------------------------------------------------------- f-basis

@@ -538,8 +538,11 @@ static double draw(traj_ctx *c)
 {
     const orc_problem *p = c->p;
     int64_t *pos = &c->s->rng_pos[c->tr];
-    if (p->rng_kind == 0) return orc_philox_uniform(p->seed, p->tr_base + (uint64_t)c->tr, (uint64_t)(*pos)++);
-    const int64_t lo = p->inj_off[c->tr], hi = p->inj_off[c->tr + 1];
+    /* the jump stream of trajectory tr, or the one it was copied from (vslCopyStream of the
+     * Lyapunov tasks, experiment.cpp:2228-2246) */
+    const int src = c->s->rng_src ? c->s->rng_src[c->tr] : c->tr;
+    if (p->rng_kind == 0) return orc_philox_uniform(p->seed, p->tr_base + (uint64_t)src, (uint64_t)(*pos)++);
+    const int64_t lo = p->inj_off[src], hi = p->inj_off[src + 1];
     if (lo + *pos >= hi) { c->err = 3; return 0.5; }
     return p->inj_u[lo + (*pos)++];
 }

@@ -103,6 +103,7 @@ typedef struct {
     double *jump_etas;
     int *diss_types;
     int *error;         /* [n_traj] 0 ok; 1 norm>1; 2 all jump weights zero; 3 rng exhausted; 4 record overflow */
+    int *rng_src;       /* [n_traj] jump stream each trajectory draws from (NULL: its own) */
 } orc_state;
 
 /* Initial state: start_type 0 -> |start_state>, else uniform sqrt(1/d) (newdel_exp.cpp:656-679);
@@ -150,6 +151,43 @@ int orc_observables(const orc_problem *p, const orc_state *s, int is_start,
 /* Dump schedule (newdel_exp.cpp:408-455).  Returns dump_num_total, fills periods
  * (caller provides dump_num + 2 ints). */
 int orc_dump_periods(int dump_type, int dump_num, int num_obs_periods, int *periods);
+
+/* Lyapunov paired trajectories (task_id 7, LpnMult; lpn_oracle.c).  n_traj is even; [0, n/2) are the
+ * bases and n/2 + b the variation of base b.  s->rng_src must be set (a variation draws the jump
+ * stream of its base after every copy). */
+typedef struct {
+    int lpn_type;        /* -1 mean, -2 energy, k >= 0 random observable k */
+    int eps_deep;        /* lpn_eps_deep: bisection halvings at most */
+    int per_period;      /* lambda_per_periods: 0 renormalise on the thresholds, 1 every period */
+    int pad;
+    double eps_low, eps_high, eps_error;  /* log10 bounds of eps, tolerance on delta_s */
+    double delta_s;      /* lpn_delta_s */
+    double delta_f_high, delta_f_low;
+    double max_energy;   /* max |Re H_ii| (lpn_type -2) */
+} orc_lpn_config;
+
+typedef struct {
+    double *lambda, *lambda_now, *delta_s;   /* [n_traj] */
+    double *mean_lpn, *energy_lpn;            /* [n_traj] */
+    double *robs_lpn;                         /* [n_traj][num_robs] complex */
+    int *num_renorms;                         /* [n_traj] */
+    int64_t *var_pos;                         /* [n_traj] draws taken from the variation stream */
+    /* last call: renormalised?, delta_f / delta_s, delta_s, delta_f (save_lambdas records) */
+    int *renormed;
+    double *ratio, *ds_rec, *df_rec;
+    int *eps_iters;                           /* halvings of the last bisection */
+    double *eps;                              /* eps of the last bisection */
+} orc_lpn;
+
+/* After the bases' transient periods: copy every base into its variation (phi, eta, jump stream),
+ * perturb it (var_trajectory_lpn) and set the Lyapunov characteristics (calc_chars_lpn_start). */
+int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg, orc_lpn *lp);
+/* After one observation period: calc_chars_lpn of the bases and lambda_lpn (per_period 0) or
+ * lambda_lpn_now (1) of the variations, curr_time = (period_id + 1) T. */
+int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg, orc_lpn *lp, double curr_time);
+/* pow(10, x) and log(x) of the Lyapunov task, shared operation for operation with the engine. */
+double orc_lpn_exp10(double x);
+double orc_lpn_log(double x);
 
 /* Canonical kernels, exported for unit tests. */
 void orc_matvec(int d, const double *M, const double *x, double *out);

@@ -21,7 +21,8 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
+    "qjx_random_observables", "qjx_set_active", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
+    "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
 
@@ -31,6 +32,13 @@ class QjxConfig(C.Structure):
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
                 ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("deep_num_steps", C.c_int),
                 ("precision", C.c_int)]
+
+
+class QjxLpnConfig(C.Structure):
+    _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
+                ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
+                ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
+                ("max_energy", C.c_double)]
 
 
 class QjxStats(C.Structure):
@@ -79,6 +87,11 @@ def lib():
         L.qjx_get_jumps.argtypes = [vp, C.c_int, c_double_p, c_int_p, c_double_p, c_double_p]
         L.qjx_get_stats.argtypes = [vp, C.POINTER(QjxStats)]
         L.qjx_set_trace.argtypes = [vp, C.c_int]
+        L.qjx_set_active.argtypes = [vp, C.c_int]
+        L.qjx_lpn_start.argtypes = [vp, C.POINTER(QjxLpnConfig)]
+        L.qjx_lpn_period.argtypes = [vp, C.c_double, C.c_int]
+        L.qjx_lpn_get.argtypes = [vp] + [c_double_p] * 6 + [c_int_p]
+        L.qjx_lpn_get_last.argtypes = [vp, c_int_p, c_double_p, c_double_p, c_double_p, c_int_p, c_double_p]
         L.qjx_get_trace.argtypes = [vp, c_i64_p, c_int_p, c_int_p]
         L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5

@@ -129,6 +129,12 @@ std::string dimer_suffix(const RunParam &rp, const ConfigParam &cp, int precisio
       << std::setprecision(precision) << std::fixed << param(cp, "dimer_prm_U") << "_"
       << std::setprecision(precision) << std::fixed << param(cp, "dimer_prm_J") << ")";
     p << "_start(" << int(param(cp, "start_type")) << "_" << int(param(cp, "start_state")) << ")";
+    if (rp.task_id == 7 || rp.task_id == 8) {  // LpnMult / LpnMultDeep: suffix_lpn (outputter.cpp:371-381)
+        p << "_lpn(" << std::defaultfloat << std::setprecision(6) << param(cp, "lpn_type") << "_"
+          << std::setprecision(4) << std::fixed << std::log10(param(cp, "lpn_delta_s")) << "_"
+          << std::setprecision(4) << std::fixed << std::log10(param(cp, "lpn_delta_f_high")) << "_"
+          << std::setprecision(4) << std::fixed << std::log10(param(cp, "lpn_delta_f_low")) << ")";
+    }
     return s.str() + p.str() + ".txt";
 }
 

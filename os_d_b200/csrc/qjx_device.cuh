@@ -53,7 +53,9 @@ struct __align__(16) TrajState {
     unsigned long long mask;  // bit l = step counter of split level l (0 or 1)
     int lvl, b, phase, cur;   // level, branch, phase, slot holding psi
     int sub, pc, di, jumps;   // channel / observable index, periods done, next dump, jumps_counts
-    int nrec, err, paused, pad;
+    int nrec, err, paused;
+    int rng_src;       // trajectory whose jump stream this one draws (itself, or the base it was
+                       // copied from by the Lyapunov task: vslCopyStream, experiment.cpp:2228-2256)
     // RK propagator (prop_id 1)
     double rk_h;       // step being integrated: rk_step, or the begin / end part around a jump
     double rk_prev;    // norm of psi before the step
@@ -119,6 +121,25 @@ struct Params {
     // deep tasks (StdDeep): each branch runs brep = 2 deep_num_steps units of two level-0 steps;
     // with subdump the observables are taken after every sub-period (two units)
     int brep, subdump;
+    // run_periods advances trajectories [0, n_active) only (the Lyapunov task's transient runs
+    // the bases alone)
+    int n_active;
+};
+
+// Lyapunov paired trajectories (task_id 7, LpnMult): [0, n/2) bases, n/2 + b the variation of b.
+struct LpnParams {
+    int lpn_type;        // -1 mean, -2 energy, k >= 0 random observable k
+    int eps_deep;        // bisection halvings at most
+    int per_period;      // lambda_per_periods
+    double eps_low, eps_high, eps_error, delta_s, delta_f_high, delta_f_low, max_energy;
+    double *lambda, *lambda_now, *delta_s_v, *mean_lpn, *energy_lpn;  // [n]
+    double2 *robs_lpn;                                                // [n][nr]
+    int *num_renorms;                                                 // [n]
+    long long *var_pos;                                               // [n] variation-stream draws
+    int *renormed;                                                    // [n] last call
+    double *ratio, *ds_rec, *df_rec;                                  // [n] last call
+    int *eps_iters;                                                   // [n] last bisection
+    double *eps;                                                      // [n] last bisection
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns
@@ -154,9 +175,10 @@ __device__ __forceinline__ double philox_uniform(unsigned long long seed, unsign
 // Next uniform of a trajectory; sets *err on an exhausted injected sequence.
 __device__ __forceinline__ double draw(const Params &P, int tr, TrajState &s, int *err)
 {
+    (void)tr;
     if (P.rng_kind == 0)
-        return philox_uniform(P.seed, (unsigned long long)(P.tr_base + tr), (unsigned long long)(s.rng_pos++));
-    const long long lo = P.inj_off[tr], hi = P.inj_off[tr + 1];
+        return philox_uniform(P.seed, (unsigned long long)(P.tr_base + s.rng_src), (unsigned long long)(s.rng_pos++));
+    const long long lo = P.inj_off[s.rng_src], hi = P.inj_off[s.rng_src + 1];
     if (lo + s.rng_pos >= hi) { *err = ERR_RNG; return 0.5; }
     return P.inj_u[lo + (s.rng_pos++)];
 }

@@ -29,6 +29,8 @@ cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
 cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st);
 size_t split_smem_bytes(int MDs, int MD, int stages);
 size_t split_stage_bytes(int MDs);
+cudaError_t launch_lpn(const Params &P, const LpnParams &L, int mode, double curr_time, int adr_dump,
+                       cudaStream_t st);
 }  // namespace qjx
 
 using namespace qjx;
@@ -58,6 +60,9 @@ struct qjx_engine {
     qjx_stats stats{};
     bool states_set = false;
     int period_base = 0;  // periods run since the last time reset (the RK propagator's period_id)
+    // Lyapunov task (allocated by the first qjx_lpn_start)
+    LpnParams L{};
+    bool lpn_alloc = false, lpn_started = false;
 };
 
 static void *dalloc(qjx_engine *h, size_t bytes)
@@ -213,6 +218,7 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
     P.tr_base = c.tr_base;
     P.keep_adr = c.keep_adr;
     P.rec_cap = h->cfg.rec_cap;
+    P.n_active = n;
 
     // matrices in the transposed padded layout mats[g][k][row], k < kp, row < MD (zero padded)
     const size_t per = (size_t)kp * MD * 2;
@@ -740,6 +746,117 @@ extern "C" qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats)
     for (auto &v : h->jt) jumps += (int64_t)v.size();
     h->stats.jumps = jumps;
     *stats = h->stats;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_set_active(qjx_engine *h, int n_active)
+{
+    if (!h || n_active < 0 || n_active > h->P.n) return QJX_ERR_INVALID_ARG;
+    h->P.n_active = n_active;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
+{
+    if (!h || !c) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    const Params &P = h->P;
+    if (P.n < 2 || (P.n & 1)) return fail(h, QJX_ERR_INVALID_ARG, "the Lyapunov task needs an even n_traj >= 2");
+    if (!(c->lpn_type == -1 || c->lpn_type == -2 || (c->lpn_type >= 0 && c->lpn_type < P.nr)))
+        return fail(h, QJX_ERR_INVALID_ARG, "lpn_type must be -1, -2 or a random observable index");
+    if (P.nr > 64) return fail(h, QJX_ERR_UNSUPPORTED, "the Lyapunov task takes at most 64 random observables");
+    if (c->eps_deep < 0) return fail(h, QJX_ERR_INVALID_ARG, "eps_deep must be >= 0");
+    CK(cudaSetDevice(h->cfg.device));
+    LpnParams &L = h->L;
+    const size_t n = P.n;
+    if (!h->lpn_alloc) {
+        L.lambda = (double *)dalloc(h, n * sizeof(double));
+        L.lambda_now = (double *)dalloc(h, n * sizeof(double));
+        L.delta_s_v = (double *)dalloc(h, n * sizeof(double));
+        L.mean_lpn = (double *)dalloc(h, n * sizeof(double));
+        L.energy_lpn = (double *)dalloc(h, n * sizeof(double));
+        L.robs_lpn = (double2 *)dalloc(h, n * std::max(1, P.nr) * sizeof(double2));
+        L.num_renorms = (int *)dalloc(h, n * sizeof(int));
+        L.var_pos = (long long *)dalloc(h, n * sizeof(long long));
+        L.renormed = (int *)dalloc(h, n * sizeof(int));
+        L.ratio = (double *)dalloc(h, n * sizeof(double));
+        L.ds_rec = (double *)dalloc(h, n * sizeof(double));
+        L.df_rec = (double *)dalloc(h, n * sizeof(double));
+        L.eps_iters = (int *)dalloc(h, n * sizeof(int));
+        L.eps = (double *)dalloc(h, n * sizeof(double));
+        if (!L.lambda || !L.lambda_now || !L.delta_s_v || !L.mean_lpn || !L.energy_lpn || !L.robs_lpn ||
+            !L.num_renorms || !L.var_pos || !L.renormed || !L.ratio || !L.ds_rec || !L.df_rec || !L.eps_iters || !L.eps)
+            return fail(h, QJX_ERR_OOM, "Lyapunov arrays");
+        h->lpn_alloc = true;
+    }
+    L.lpn_type = c->lpn_type;
+    L.eps_deep = c->eps_deep;
+    L.per_period = c->per_period ? 1 : 0;
+    L.eps_low = c->eps_low;
+    L.eps_high = c->eps_high;
+    L.eps_error = c->eps_error;
+    L.delta_s = c->delta_s;
+    L.delta_f_high = c->delta_f_high;
+    L.delta_f_low = c->delta_f_low;
+    L.max_energy = c->max_energy;
+    CK(cudaMemsetAsync(L.var_pos, 0, n * sizeof(long long), h->stream));
+    CK(cudaMemsetAsync(L.ratio, 0, n * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(L.ds_rec, 0, n * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(L.df_rec, 0, n * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(L.eps_iters, 0, n * sizeof(int), h->stream));
+    CK(cudaMemsetAsync(L.eps, 0, n * sizeof(double), h->stream));
+    CK(launch_lpn(P, L, 0, 0.0, -1, h->stream));
+    h->stats.launches += 1;
+    CK(cudaStreamSynchronize(h->stream));
+    h->lpn_started = true;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_lpn_period(qjx_engine *h, double curr_time, int adr_dump)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (!h->lpn_started) return fail(h, QJX_ERR_STATE, "qjx_lpn_start first");
+    if (adr_dump < -1 || adr_dump >= h->cfg.max_dumps) return fail(h, QJX_ERR_INVALID_ARG, "adr_dump out of range");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(launch_lpn(h->P, h->L, 1, curr_time, adr_dump, h->stream));
+    h->stats.launches += 1;
+    CK(cudaStreamSynchronize(h->stream));
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_lpn_get(qjx_engine *h, double *lambda_now, double *lambda, double *delta_s,
+                                  double *mean_lpn, double *energy_lpn, double *robs_lpn, int *num_renorms)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (!h->lpn_started) return fail(h, QJX_ERR_STATE, "qjx_lpn_start first");
+    CK(cudaSetDevice(h->cfg.device));
+    const LpnParams &L = h->L;
+    const size_t n = h->P.n;
+    if (lambda_now) CK(cudaMemcpy(lambda_now, L.lambda_now, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (lambda) CK(cudaMemcpy(lambda, L.lambda, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (delta_s) CK(cudaMemcpy(delta_s, L.delta_s_v, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (mean_lpn) CK(cudaMemcpy(mean_lpn, L.mean_lpn, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (energy_lpn) CK(cudaMemcpy(energy_lpn, L.energy_lpn, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (robs_lpn && h->P.nr > 0)
+        CK(cudaMemcpy(robs_lpn, L.robs_lpn, n * h->P.nr * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (num_renorms) CK(cudaMemcpy(num_renorms, L.num_renorms, n * sizeof(int), cudaMemcpyDeviceToHost));
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_lpn_get_last(qjx_engine *h, int *renormed, double *ratio, double *delta_s,
+                                       double *delta_f, int *eps_iters, double *eps)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (!h->lpn_started) return fail(h, QJX_ERR_STATE, "qjx_lpn_start first");
+    CK(cudaSetDevice(h->cfg.device));
+    const LpnParams &L = h->L;
+    const size_t n = h->P.n;
+    if (renormed) CK(cudaMemcpy(renormed, L.renormed, n * sizeof(int), cudaMemcpyDeviceToHost));
+    if (ratio) CK(cudaMemcpy(ratio, L.ratio, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (delta_s) CK(cudaMemcpy(delta_s, L.ds_rec, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (delta_f) CK(cudaMemcpy(delta_f, L.df_rec, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (eps_iters) CK(cudaMemcpy(eps_iters, L.eps_iters, n * sizeof(int), cudaMemcpyDeviceToHost));
+    if (eps) CK(cudaMemcpy(eps, L.eps, n * sizeof(double), cudaMemcpyDeviceToHost));
     return QJX_OK;
 }
 

@@ -852,7 +852,7 @@ __global__ void schedule_kernel(const Params P, int mode)
         s.mask = 0;
         s.rk_sid = 0;
         s.paused = 0;
-        s.phase = (P.target > 0) ? PH_STEP : PH_DONE;
+        s.phase = (P.target > 0 && tr < P.n_active) ? PH_STEP : PH_DONE;
     } else {
         if (!s.paused) return;
         s.paused = 0;
@@ -970,7 +970,7 @@ __global__ void init_state_kernel(const Params P)
     s.nrec = 0;
     s.err = 0;
     s.paused = 0;
-    s.pad = 0;
+    s.rng_src = tr;
     s.rk_h = 0.0;
     s.rk_prev = 0.0;
     s.rk_end = 0.0;
@@ -1096,7 +1096,7 @@ __global__ void rk_schedule_kernel(const Params P)
     s.di = 0;
     s.paused = 0;
     s.rk_sid = 0;
-    if (P.target > 0) {
+    if (P.target > 0 && tr < P.n_active) {
         s.t = rk_step_time(P, s);
         rk_begin(s, P.rk_step, nrm, 0);
         if (lane == 0) enqueue(P, P.cnt, P.lists, 0, tr);

@@ -1,6 +1,6 @@
 // qjx_main.cpp -- qjx_b200: process-level drop-in for the reference's qjx executable on the
-// Std task (task_id 1) with the QJ propagator (prop_id 0) or the RK propagator (prop_id 1), and the
-// StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0).
+// Std task (task_id 1) and the LpnMult task (task_id 7) with the QJ propagator (prop_id 0) or the
+// RK propagator (prop_id 1), and the StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0).
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -12,6 +12,8 @@
 //   qjx_b200 [--config FILE] [--params FILE] [--device N] [--check]
 // --check parses both files, prints the parameter echo and the file-name suffix, and exits
 // without touching a GPU.
+#include <algorithm>
+#include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -47,6 +49,227 @@ struct Dumps {
     std::vector<std::complex<double>> robs;           // [dump][tr][nr]
 };
 
+void write_2d_inv(const std::string &fn, const std::vector<double> &v, int nrec, int ndt, int n)
+{
+    std::vector<double> inv((size_t)ndt * n, 0.0);  // [tr][dump] like ed->*_evo
+    for (int dmp = 0; dmp < nrec; dmp++)
+        for (int tr = 0; tr < n; tr++) inv[(size_t)tr * ndt + dmp] = v[(size_t)dmp * n + tr];
+    save_2d_inv_double_data(fn, inv.data(), ndt, n, 16, false);
+}
+
+// LpnMult (task_id 7): LpnMultExperimentBehaviour::trans_process / obser_process
+// (experiment.cpp:138-286).  The bases [0, n/2) run the transient alone, every variation
+// n/2 + b starts as its base perturbed to delta_s, and after every observation period the
+// variations' Lyapunov sums are updated (lambda_lpn / lambda_lpn_now).  Files: dump_std,
+// dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127), adr files (dump.cpp:3-98).
+void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, const qjx_config &cfg,
+                  const std::vector<double> &H, int d, int num_robs, int robs_seed)
+{
+    const int n = cp.num_trajectories, half = n / 2;
+    if (n < 2 || (n & 1)) die("LpnMult needs an even num_trajectories >= 2");
+    const std::string &sfx = cp.fn_suffix;
+    const std::string path = rp.path;
+    const int dump_obs = int(param(cp, "dump_obs")), dump_evo_sep = int(param(cp, "dump_evo_sep"));
+    const int dump_evo_avg = int(param(cp, "dump_evo_avg")), dump_adr_sep = int(param(cp, "dump_adr_sep"));
+    const int dump_adr_avg_on = int(param(cp, "dump_adr_avg"));
+    const int jump = int(param(cp, "jump"));
+    qjx_lpn_config lc{};
+    lc.lpn_type = int(param(cp, "lpn_type"));
+    lc.eps_deep = int(param(cp, "lpn_eps_deep"));
+    lc.per_period = int(param(cp, "lambda_per_periods")) == 0 ? 0 : 1;
+    lc.eps_low = param(cp, "lpn_eps_low");
+    lc.eps_high = param(cp, "lpn_eps_high");
+    lc.eps_error = param(cp, "lpn_eps_error");
+    lc.delta_s = param(cp, "lpn_delta_s");
+    lc.delta_f_high = param(cp, "lpn_delta_f_high");
+    lc.delta_f_low = param(cp, "lpn_delta_f_low");
+    const int save_lambdas = int(param(cp, "save_lambdas"));
+    lc.max_energy = 0.0;  // init_obs_lpn (newdel_exp.cpp:540-550)
+    for (int st = 0; st < d; st++) {
+        const double v = std::fabs(H[2 * ((size_t)st * d + st)]);
+        if (v > lc.max_energy) lc.max_energy = v;
+    }
+    const std::vector<int> dp = dump_periods(int(param(cp, "dump_type")), int(param(cp, "dump_num")), cp.num_obs_periods);
+    if (dp.empty()) die("Wrong dump_type");
+    const int ndt = (int)dp.size();
+
+    // per-dump records: std observables live in the engine's dump slots; Lyapunov values here
+    std::vector<double> lam_evo, mean_lpn_evo, energy_lpn_evo;
+    std::vector<std::complex<double>> robs_lpn_evo;
+    std::vector<double> lam(n), mean_l(n), energy_l(n);
+    std::vector<std::complex<double>> robs_l((size_t)n * (num_robs ? num_robs : 1));
+    std::vector<int> renorms(n);
+    auto take_lpn = [&]() {
+        check(qjx_lpn_get(h, lam.data(), nullptr, nullptr, mean_l.data(), energy_l.data(),
+                          num_robs ? reinterpret_cast<double *>(robs_l.data()) : nullptr, renorms.data()),
+              h, "qjx_lpn_get");
+        lam_evo.insert(lam_evo.end(), lam.begin(), lam.end());
+        mean_lpn_evo.insert(mean_lpn_evo.end(), mean_l.begin(), mean_l.end());
+        energy_lpn_evo.insert(energy_lpn_evo.end(), energy_l.begin(), energy_l.end());
+        robs_lpn_evo.insert(robs_lpn_evo.end(), robs_l.begin(), robs_l.begin() + (size_t)n * num_robs);
+    };
+    // save_lambdas: delta_f / delta_s, delta_s, delta_f of every renormalisation per trajectory
+    std::vector<std::vector<double>> rec_ratio(n), rec_ds(n), rec_df(n);
+    std::vector<int> ren(n), iters(n);
+    std::vector<double> ratio(n), rds(n), rdf(n), eps(n);
+    auto after_lpn = [&](bool start) {
+        if (save_lambdas <= 0 && rp.is_pp != 1) return;
+        check(qjx_lpn_get_last(h, ren.data(), ratio.data(), rds.data(), rdf.data(), iters.data(), eps.data()), h,
+              "qjx_lpn_get_last");
+        std::vector<double> ds_now(n);
+        if (rp.is_pp == 1)
+            check(qjx_lpn_get(h, nullptr, nullptr, ds_now.data(), nullptr, nullptr, nullptr, nullptr), h, "qjx_lpn_get");
+        for (int v = half; v < n; v++) {
+            if (!start && !ren[v]) continue;
+            if (!start && save_lambdas > 0) {
+                rec_ratio[v].push_back(ratio[v]);
+                rec_ds[v].push_back(rds[v]);
+                rec_df[v].push_back(rdf[v]);
+            }
+            if (rp.is_pp == 1)  // var_trajectory_lpn's progress lines (experiment.cpp:2385-2392)
+                std::cout << "lpn: " << v + 1 << std::endl
+                          << "curr_lpn_eps: " << std::log10(eps[v]) << std::endl
+                          << "lpn_deep: " << iters[v] << std::endl
+                          << "delta_s: " << ds_now[v] << std::endl
+                          << std::endl;
+        }
+    };
+    auto get_adr = [&](int dump) {
+        std::vector<double> adr((size_t)n * d);
+        check(qjx_get_observables(h, cfg.keep_adr ? dump : 0, 1, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                  adr.data()),
+              h, "qjx_get_observables");
+        return adr;
+    };
+    auto write_adr_single = [&](int dump, bool append) {
+        if (!(dump_evo_sep == 1 && dump_adr_sep == 1)) return;
+        const std::vector<double> adr = get_adr(dump);
+        for (int tr = 0; tr < n; tr++)
+            save_double_data(path + "adr_" + std::to_string(tr) + sfx, adr.data() + (size_t)tr * d, d, 16, append);
+    };
+    auto write_adr_avg = [&](int dump, int tr1, bool append) {  // dump_adr_avg / dump_adr_avg_mult
+        if (dump_adr_avg_on != 1) return;
+        const std::vector<double> adr = get_adr(dump);
+        std::vector<double> avg(d, 0.0);
+        for (int tr = 0; tr < tr1; tr++)
+            for (int st = 0; st < d; st++) avg[st] += adr[(size_t)tr * d + st] / double(tr1);
+        save_double_data(path + "adr_avg" + sfx, avg.data(), d, 16, append);
+    };
+
+    // trans_process: the bases' transient, then copy + perturb, refresh times, dump 0
+    check(qjx_init_thresholds(h), h, "qjx_init_thresholds");
+    check(qjx_set_active(h, half), h, "qjx_set_active");
+    check(qjx_run_periods(h, cp.num_tp_periods, 0, nullptr, 0, 0), h, "qjx_run_periods");
+    check(qjx_set_active(h, n), h, "qjx_set_active");
+    check(qjx_lpn_start(h, &lc), h, "qjx_lpn_start");
+    after_lpn(true);
+    check(qjx_reset_times(h), h, "qjx_reset_times");
+    check(qjx_observe(h, 0, 1), h, "qjx_observe");
+    take_lpn();
+    write_adr_single(0, false);
+    if (dump_evo_avg == 1) write_adr_avg(0, n, false);
+
+    // obser_process: period by period (the Lyapunov update follows every period)
+    std::vector<bool> zero_span(ndt, false);
+    for (int dump_id = 1; dump_id < ndt; dump_id++) {
+        if (rp.is_pp == 1) std::cout << "dump_id: " << dump_id << std::endl;
+        for (int period_id = dp[dump_id - 1]; period_id < dp[dump_id]; period_id++) {
+            const bool at_dump = period_id + 1 == dp[dump_id];
+            const int one = 1;
+            check(qjx_run_periods(h, 1, 1, at_dump ? &one : nullptr, at_dump ? 1 : 0, dump_id), h, "qjx_run_periods");
+            check(qjx_lpn_period(h, double(period_id + 1) * cfg.T, at_dump ? dump_id : -1), h, "qjx_lpn_period");
+            after_lpn(false);
+        }
+        if (dp[dump_id] == dp[dump_id - 1]) {  // no period ran: adr of the current states (abs_diag_rho_all)
+            check(qjx_observe(h, dump_id, 0), h, "qjx_observe");
+            zero_span[dump_id] = true;
+        }
+        take_lpn();
+        write_adr_single(dump_id, true);
+        if (dump_evo_avg == 1) write_adr_avg(dump_id, half, true);
+    }
+    const int last_dump = ndt - 1;
+
+    std::vector<double> norm_((size_t)ndt * n), mean_((size_t)ndt * n), disp_((size_t)ndt * n), m2_((size_t)ndt * n),
+        energy_((size_t)ndt * n);
+    std::vector<std::complex<double>> robs_((size_t)ndt * n * (num_robs ? num_robs : 1));
+    check(qjx_get_observables(h, 0, ndt, norm_.data(), mean_.data(), disp_.data(), m2_.data(), energy_.data(),
+                              num_robs ? reinterpret_cast<double *>(robs_.data()) : nullptr, nullptr),
+          h, "qjx_get_observables");
+    // a dump with no period since the previous one repeats the previous std characteristics
+    // (calc_chars_std runs once per period; a renormalised variation keeps its pre-renormalisation values)
+    for (int dmp = 1; dmp < ndt; dmp++) {
+        if (!zero_span[dmp]) continue;
+        const size_t a = (size_t)(dmp - 1) * n, b = (size_t)dmp * n;
+        for (auto *v : {&norm_, &mean_, &disp_, &m2_, &energy_}) std::copy(v->begin() + a, v->begin() + a + n, v->begin() + b);
+        std::copy(robs_.begin() + a * num_robs, robs_.begin() + (a + n) * num_robs, robs_.begin() + b * num_robs);
+    }
+    std::vector<double> mean_start(n);
+    check(qjx_get_mean_start(h, mean_start.data()), h, "qjx_get_mean_start");
+    if (dump_obs == 1) {
+        const size_t o = (size_t)last_dump * n;
+        save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);  // dump_std
+        save_double_data(path + "mean_start" + sfx, mean_start.data(), n, 16, false);
+        save_double_data(path + "mean" + sfx, mean_.data() + o, n, 16, false);
+        save_double_data(path + "dispersion" + sfx, disp_.data() + o, n, 16, false);
+        save_double_data(path + "m2" + sfx, m2_.data() + o, n, 16, false);
+        save_double_data(path + "energy" + sfx, energy_.data() + o, n, 16, false);
+        const size_t ol = (size_t)last_dump * n;  // dump_lpn
+        save_double_data(path + "lambda" + sfx, lam_evo.data() + ol, n, 16, false);
+        save_int_data(path + "num_renorms" + sfx, renorms.data(), n, false);
+        save_double_data(path + "mean_lpn" + sfx, mean_lpn_evo.data() + ol, n, 16, false);
+        save_double_data(path + "energy_lpn" + sfx, energy_lpn_evo.data() + ol, n, 16, false);
+        if (save_lambdas > 0)
+            for (int tr = 0; tr < n; tr++) {
+                save_double_vector(path + "delta_f_by_delta_s_" + std::to_string(tr) + sfx, rec_ratio[tr], 16, false);
+                save_double_vector(path + "deltas_s_" + std::to_string(tr) + sfx, rec_ds[tr], 16, false);
+                save_double_vector(path + "deltas_f_" + std::to_string(tr) + sfx, rec_df[tr], 16, false);
+            }
+    }
+    if (dump_evo_sep == 1 && dump_obs == 1) {
+        save_int_data(path + "periods" + sfx, dp.data(), ndt, false);  // dump_std_evo
+        write_2d_inv(path + "norm_evo" + sfx, norm_, ndt, ndt, n);
+        write_2d_inv(path + "mean_evo" + sfx, mean_, ndt, ndt, n);
+        write_2d_inv(path + "dispersion_evo" + sfx, disp_, ndt, ndt, n);
+        write_2d_inv(path + "m2_evo" + sfx, m2_, ndt, ndt, n);
+        write_2d_inv(path + "energy_evo" + sfx, energy_, ndt, ndt, n);
+        auto robs_file = [&](const std::string &name, const std::vector<std::complex<double>> &src) {
+            for (int o = 0; o < num_robs; o++) {
+                std::vector<std::vector<std::complex<double>>> v(n, std::vector<std::complex<double>>(ndt));
+                for (int tr = 0; tr < n; tr++)
+                    for (int dmp = 0; dmp < ndt; dmp++) v[tr][dmp] = src[((size_t)dmp * n + tr) * num_robs + o];
+                save_2d_complex_vector(path + name + std::to_string(robs_seed + o) + sfx, v, 16);
+            }
+        };
+        robs_file("random_obs_evo_", robs_);
+        if (jump > 0) {
+            for (int tr = 0; tr < n; tr++) {
+                int64_t k = 0;
+                check(qjx_jump_count(h, tr, &k), h, "qjx_jump_count");
+                std::vector<double> t(k), nr(k), et(k);
+                std::vector<int> ty(k);
+                check(qjx_get_jumps(h, tr, t.data(), ty.data(), nr.data(), et.data()), h, "qjx_get_jumps");
+                save_double_vector(path + "jump_times_" + std::to_string(tr) + sfx, t, 16, false);
+                save_int_vector(path + "diss_types_" + std::to_string(tr) + sfx, ty, false);
+                if (jump > 1) {
+                    save_double_vector(path + "jump_norms_" + std::to_string(tr) + sfx, nr, 16, false);
+                    save_double_vector(path + "jump_etas_" + std::to_string(tr) + sfx, et, 16, false);
+                }
+            }
+        }
+        write_2d_inv(path + "lambda_evo" + sfx, lam_evo, ndt, ndt, n);  // dump_lpn_evo
+        write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
+        write_2d_inv(path + "energy_lpn_evo" + sfx, energy_lpn_evo, ndt, ndt, n);
+        robs_file("random_obs_lpn_evo_", robs_lpn_evo);
+    }
+    if (dump_evo_avg == 0) write_adr_avg(last_dump, half, true);
+
+    qjx_stats st{};
+    qjx_get_stats(h, &st);
+    std::cout << "micro-steps: " << st.micro_steps << ", matvecs: " << st.matvecs
+              << ", device time (ms): " << st.kernel_ms << std::endl;
+}
+
 }  // namespace
 
 int main(int argc, char **argv)
@@ -71,8 +294,9 @@ int main(int argc, char **argv)
     std::cout << params_echo(rp, cp);
 
     if (rp.sys_id != 0) die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer, sys_id 0)");
-    if (rp.task_id != 1 && rp.task_id != 4)
-        die("Wrong task_id: " + std::to_string(rp.task_id) + " (this engine runs the Std (1) and StdDeep (4) tasks)");
+    if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7)
+        die("Wrong task_id: " + std::to_string(rp.task_id) +
+            " (this engine runs the Std (1), StdDeep (4) and LpnMult (7) tasks)");
     if (rp.task_id == 4 && rp.prop_id != 0) die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (StdDeep runs the QJ propagator)");
     if (rp.prop_id != 0 && rp.prop_id != 1)
         die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
@@ -195,6 +419,12 @@ int main(int argc, char **argv)
                 else psi[2 * ((size_t)tr * d + i)] = std::sqrt(1.0 / double(d));
         check(qjx_set_states(h, psi.data()), h, "qjx_set_states");
         std::cout << "init_data" << std::endl;
+
+        if (rp.task_id == 7) {
+            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed);
+            qjx_destroy(h);
+            return 0;
+        }
 
         // trans_process (experiment.cpp:411-446)
         check(qjx_init_thresholds(h), h, "qjx_init_thresholds");

@@ -149,6 +149,46 @@ class Engine:
                   "qjx_get_jumps")
         return times, types, norms, etas
 
+    def set_active(self, n_active):
+        """Later run_periods calls advance trajectories [0, n_active) only."""
+        self._chk(N.lib().qjx_set_active(self.h, int(n_active)), "qjx_set_active")
+
+    # ---------------------------------------------------------- Lyapunov task (task_id 7)
+    def lpn_start(self, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10, delta_s=1e-3,
+                  delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0):
+        """Copy every base [0, n/2) into its variation n/2 + b and perturb it (LpnMult trans_process);
+        keyword names follow the reference's lpn_* params."""
+        c = N.QjxLpnConfig(lpn_type=lpn_type, eps_deep=eps_deep, per_period=int(per_period), eps_low=eps_low,
+                           eps_high=eps_high, eps_error=eps_error, delta_s=delta_s, delta_f_high=delta_f_high,
+                           delta_f_low=delta_f_low, max_energy=max_energy)
+        self._chk(N.lib().qjx_lpn_start(self.h, C.byref(c)), "qjx_lpn_start")
+
+    def lpn_period(self, curr_time, adr_dump=-1):
+        """calc_chars_lpn of the bases and lambda_lpn of the variations after one period."""
+        self._chk(N.lib().qjx_lpn_period(self.h, float(curr_time), int(adr_dump)), "qjx_lpn_period")
+
+    def lpn_values(self):
+        n = self.n
+        out = {k: np.zeros(n) for k in ("lambda_now", "lambda", "delta_s", "mean_lpn", "energy_lpn")}
+        robs = np.zeros((n, max(self.nr, 1)), np.complex128)
+        nr = np.zeros(n, np.int32)
+        self._chk(N.lib().qjx_lpn_get(self.h, N.dp(out["lambda_now"]), N.dp(out["lambda"]), N.dp(out["delta_s"]),
+                                      N.dp(out["mean_lpn"]), N.dp(out["energy_lpn"]), N.dp(robs), N.ip(nr)),
+                  "qjx_lpn_get")
+        out["robs_lpn"] = robs[:, : self.nr]
+        out["num_renorms"] = nr
+        return out
+
+    def lpn_last(self):
+        n = self.n
+        ren, it = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        out = {k: np.zeros(n) for k in ("ratio", "delta_s", "delta_f", "eps")}
+        self._chk(N.lib().qjx_lpn_get_last(self.h, N.ip(ren), N.dp(out["ratio"]), N.dp(out["delta_s"]),
+                                           N.dp(out["delta_f"]), N.ip(it), N.dp(out["eps"])), "qjx_lpn_get_last")
+        out["renormed"] = ren
+        out["eps_iters"] = it
+        return out
+
     def set_trace(self, enable=True):
         self._chk(N.lib().qjx_set_trace(self.h, int(enable)), "qjx_set_trace")
 

@@ -62,11 +62,20 @@ def suffix(cfg, prm):
             + "_drv(%d_%s_%s_%s)" % (int(prm["dimer_drv_type"]), f4(prm["dimer_drv_ampl"]),
                                      f4(prm["dimer_drv_freq"]), f4(prm["dimer_drv_phase"]))
             + "_prm(%s_%s_%s)" % (f4(prm["dimer_prm_E"]), f4(prm["dimer_prm_U"]), f4(prm["dimer_prm_J"]))
-            + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"])) + ".txt")
+            + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"]))
+            + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
+
+
+def lpn_suffix(prm):
+    """suffix_lpn (outputter.cpp:371-381)."""
+    return "_lpn(%g_%.4f_%.4f_%.4f)" % (float(prm["lpn_type"]), np.log10(prm["lpn_delta_s"]),
+                                        np.log10(prm["lpn_delta_f_high"]), np.log10(prm["lpn_delta_f_low"]))
 
 
 def expected_outputs(cfg, prm, R=None):
     """All files the drop-in writes, as {relative file name: text}."""
+    if cfg.get("task_id", 1) == 7:
+        return expected_lpn_outputs(cfg, prm, R)
     N = int(prm["N"])
     d = N + 1
     n = cfg["num_trajectories"]
@@ -222,6 +231,143 @@ def expected_outputs(cfg, prm, R=None):
     files.update(acc)
     return files
 
+
+def expected_lpn_outputs(cfg, prm, R=None):
+    """LpnMult (task_id 7): LpnMultExperimentBehaviour::trans_process / obser_process
+    (experiment.cpp:138-286) with dump_std, dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127)
+    and the adr files (dump.cpp:3-98)."""
+    N = int(prm["N"])
+    d = N + 1
+    n = cfg["num_trajectories"]
+    half = n // 2
+    deep = cfg.get("ex_deep", 16)
+    seed = cfg.get("seed", 0)
+    path = cfg.get("path", "")
+    sfx = suffix(cfg, prm)
+    H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
+                                         prm["dimer_drv_ampl"], prm["diss_gamma"])
+    T = TWO_PI / prm["dimer_drv_freq"]
+    U = np.stack([O.split_tree(K0, T, deep), O.split_tree(K1, T, deep)])
+    HE = H + prm["dimer_prm_E"] * Hd
+    nr = int(prm["num_random_obs"])
+    ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
+    ens.init(int(prm["start_type"]), int(prm["start_state"]))
+    prop = cfg.get("prop_id", 0)
+    period = [0]
+
+    def advance(k, is_obs=1, tr1=None):
+        if prop == 0:
+            return ens.run_periods(k, is_obs=is_obs, tr1=tr1)
+        Heff = O.dimer_heff(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"], prm["diss_gamma"])
+        rc = ens.run_periods_rk(k, Heff, Hd, prm["dimer_prm_E"], prm["dimer_drv_ampl"], cfg.get("rk_ns", 1000),
+                                period0=period[0], drv_type=int(prm.get("dimer_drv_type", 0)),
+                                freq=prm["dimer_drv_freq"], phase=prm.get("dimer_drv_phase", 0.0), is_obs=is_obs,
+                                tr1=tr1)
+        period[0] += k
+        return rc
+
+    max_energy = float(np.max(np.abs(np.diag(H).real)))
+    lp = O.Lpn(ens, lpn_type=int(prm["lpn_type"]), eps_deep=int(prm["lpn_eps_deep"]),
+               eps_low=float(prm["lpn_eps_low"]), eps_high=float(prm["lpn_eps_high"]),
+               eps_error=float(prm["lpn_eps_error"]), delta_s=float(prm["lpn_delta_s"]),
+               delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
+               per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy)
+    dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
+    ndt = len(dp)
+    assert advance(cfg.get("num_tp_periods", 0), is_obs=0, tr1=half) == 0
+    lp.start()
+    ens.t[:] = 0.0
+    period[0] = 0
+    obs = [ens.observables(is_start=True, want_adr=True)]
+    lpn = [lp.values()]
+    save_lambdas = int(prm["save_lambdas"])
+    recs = {k: [[] for _ in range(n)] for k in ("ratio", "delta_s", "delta_f")}
+    evo_sep, adr_sep = int(prm["dump_evo_sep"]), int(prm["dump_adr_sep"])
+    evo_avg, adr_avg_on = int(prm["dump_evo_avg"]), int(prm["dump_adr_avg"])
+    acc = {}
+
+    def emit(name, text, append):
+        key = path + name
+        acc[key] = (acc.get(key, "") if append else "") + text
+
+    def adr_avg(adr, m):
+        avg = np.zeros(d)
+        for tr in range(m):
+            avg += adr[tr] / float(m)
+        return avg
+
+    if evo_sep == 1 and adr_sep == 1:
+        for tr in range(n):
+            emit("adr_%d" % tr + sfx, f_double_data(obs[0]["adr"][tr]), False)
+    if evo_avg == 1 and adr_avg_on == 1:
+        emit("adr_avg" + sfx, f_double_data(adr_avg(obs[0]["adr"], n)), False)
+    for dump_id in range(1, ndt):
+        o = {k: v.copy() for k, v in obs[-1].items()}
+        for period_id in range(dp[dump_id - 1], dp[dump_id]):
+            assert advance(1) == 0
+            o = ens.observables(want_adr=True)
+            lp.period((period_id + 1) * T)
+            o["adr"][half:] = ens.observables(want_adr=True)["adr"][half:]
+            last = lp.last()
+            for v in range(half, n):
+                if save_lambdas > 0 and last["renormed"][v]:
+                    for k in recs:
+                        recs[k][v].append(last[k][v])
+        obs.append(o)
+        lpn.append(lp.values())
+        if evo_sep == 1 and adr_sep == 1:
+            for tr in range(n):
+                emit("adr_%d" % tr + sfx, f_double_data(o["adr"][tr]), True)
+        if evo_avg == 1 and adr_avg_on == 1:
+            emit("adr_avg" + sfx, f_double_data(adr_avg(o["adr"], half)), True)
+    last = obs[-1]
+    if int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
+        emit("mean" + sfx, f_double_data(last["mean"]), False)
+        emit("dispersion" + sfx, f_double_data(last["dispersion"]), False)
+        emit("m2" + sfx, f_double_data(last["m2"]), False)
+        emit("energy" + sfx, f_double_data(last["energy"]), False)
+        emit("lambda" + sfx, f_double_data(lpn[-1]["lambda_now"]), False)
+        emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
+        emit("mean_lpn" + sfx, f_double_data(lpn[-1]["mean_lpn"]), False)
+        emit("energy_lpn" + sfx, f_double_data(lpn[-1]["energy_lpn"]), False)
+        if save_lambdas > 0:
+            for tr in range(n):
+                emit("delta_f_by_delta_s_%d" % tr + sfx, f_double_data(recs["ratio"][tr]), False)
+                emit("deltas_s_%d" % tr + sfx, f_double_data(recs["delta_s"][tr]), False)
+                emit("deltas_f_%d" % tr + sfx, f_double_data(recs["delta_f"][tr]), False)
+    if evo_sep == 1 and int(prm["dump_obs"]) == 1:
+        emit("periods" + sfx, f_int_data(dp), False)
+        for key, name in (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"),
+                          ("m2", "m2_evo"), ("energy", "energy_evo")):
+            emit(name + sfx, f_2d_inv(np.array([o[key] for o in obs])), False)
+        for o_id in range(nr):
+            rows = [o["random_obs"][:, o_id] for o in obs]
+            emit("random_obs_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
+        if int(prm["jump"]) > 0:
+            for tr in range(n):
+                t, ty, nm, et = ens.jumps(tr)
+                emit("jump_times_%d" % tr + sfx, f_double_data(t), False)
+                emit("diss_types_%d" % tr + sfx, f_int_data(ty), False)
+                if int(prm["jump"]) > 1:
+                    emit("jump_norms_%d" % tr + sfx, f_double_data(nm), False)
+                    emit("jump_etas_%d" % tr + sfx, f_double_data(et), False)
+        for key, name in (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo"), ("energy_lpn", "energy_lpn_evo")):
+            emit(name + sfx, f_2d_inv(np.array([v[key] for v in lpn])), False)
+        for o_id in range(nr):
+            rows = [v["robs_lpn"][:, o_id] for v in lpn]
+            emit("random_obs_lpn_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
+    if evo_avg == 0 and adr_avg_on == 1:
+        emit("adr_avg" + sfx, f_double_data(adr_avg(last["adr"], half)), False)
+    return acc
+
+
+LPN_PARAMS = {
+    "lpn_type": 0, "lpn_eps_deep": 100, "lpn_eps_error": 1.0e-10, "lpn_eps_high": 10, "lpn_eps_low": -10,
+    "lpn_delta_s": 1.0e-3, "lpn_delta_f_high": 1.0e-1, "lpn_delta_f_low": 1.0e-5, "lambda_per_periods": 0,
+    "save_lambdas": 0,
+}
 
 BASE_PARAMS = {
     "num_random_obs": 1, "random_obs_seed": 100, "random_obs_mns": 1000000, "random_obs_type": 2,

@@ -5,7 +5,7 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, config_text, params_text, suffix
+from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, LPN_PARAMS, config_text, params_text, suffix
 
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
 
@@ -45,7 +45,19 @@ def test_params_echo_format(tmp_path):
     assert "diss_gamma: 0.1\n" in r.stdout and "N: 16\n" in r.stdout
 
 
-@pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 7), ("prop_id", 2)])
+@pytest.mark.parametrize("over", [{}, {"lpn_type": -1, "lpn_delta_s": 2.5e-4, "lpn_delta_f_high": 0.3,
+                                      "lpn_delta_f_low": 3e-6}, {"lpn_type": -2}])
+def test_lpn_suffix_matches_reference_rule(tmp_path, over):
+    """LpnMult appends suffix_lpn (outputter.cpp:34-38, 371-381)."""
+    cfg = dict(BASE_CONFIG, task_id=7)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **over}
+    r = check(tmp_path, cfg, prm)
+    assert r.returncode == 0, r.stdout
+    line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
+    assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_lpn(" in line
+
+
+@pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 9), ("prop_id", 2)])
 def test_unsupported_ids_exit_with_error(tmp_path, key, val):
     r = check(tmp_path, dict(BASE_CONFIG, **{key: val}), BASE_PARAMS)
     assert r.returncode != 0 and "Error: Wrong " + key in r.stdout

@@ -7,7 +7,7 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, config_text, expected_outputs, params_text
+from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, LPN_PARAMS, config_text, expected_outputs, params_text
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -82,3 +82,24 @@ def test_std_deep_task_files_match(tmp_path):
     prm = dict(BASE_PARAMS, deep_num_steps=2, dump_adr_sep=1, dump_adr_avg=1, dump_evo_avg=1, jump=2)
     exp = run_case(tmp_path, cfg, prm)
     assert any(k.startswith("adr_0") for k in exp)
+
+
+def test_lpn_mult_task_files_match(tmp_path):
+    """LpnMult (task_id 7), random-observable distance, renormalisation on the thresholds, the
+    save_lambdas records and the adr files."""
+    cfg = dict(BASE_CONFIG, task_id=7, num_trajectories=12, num_tp_periods=2, num_obs_periods=6)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, "dump_num": 3, "lpn_delta_f_high": 5e-3, "lpn_delta_f_low": 5e-4,
+           "save_lambdas": 1, "dump_adr_sep": 1, "dump_adr_avg": 1}
+    exp = run_case(tmp_path, cfg, prm)
+    assert any(k.startswith("deltas_s_") and exp[k] for k in exp)
+    assert any(k.startswith("lambda_evo") for k in exp)
+
+
+def test_lpn_mult_every_period_rk(tmp_path):
+    """LpnMult with lambda_lpn_now (every period), the mean distance, the RK propagator,
+    logarithmic dumps and the per-dump adr average over the bases."""
+    cfg = dict(BASE_CONFIG, task_id=7, prop_id=1, rk_ns=400, num_trajectories=8, num_tp_periods=1,
+               num_obs_periods=5, is_pp=1)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, "lpn_type": -1, "lambda_per_periods": 1, "dump_type": 1, "dump_num": 2,
+           "dump_evo_avg": 1, "dump_adr_avg": 1, "num_random_obs": 2}
+    run_case(tmp_path, cfg, prm)
