@@ -19,7 +19,7 @@ constexpr int kNC = 32;                // trajectory columns per sub-tile (max)
 constexpr int kKB = 16;                // k rows per propagator slab (8 k pairs)
 constexpr int kStages = 2;             // slab pipeline depth
 constexpr int kMaxGroups = 256;        // distinct matrices in one engine
-constexpr int kMaxMD = 256;            // d <= 256
+constexpr int kMaxMD = 1024;           // d <= 1024 (plain form; the split form takes d <= 256)
 constexpr double kSplitNormSlack = 1e-4;  // split precision: tolerated norm excess over 1
 // Thread layouts of a sub-tile (rows ty + TY i, columns tx + TX j, TY * TX = 256):
 //   TY = 32: MD = 32 * MT padded rows, TX = 8 column threads, up to 4 columns each
@@ -124,6 +124,9 @@ struct Params {
     // run_periods advances trajectories [0, n_active) only (the Lyapunov task's transient runs
     // the bases alone)
     int n_active;
+    // plain step kernel tiling (chosen from MD and the shared memory): columns per sub-tile
+    // (32, 16 or 8) and k rows per propagator slab
+    int nc, kb;
 };
 
 // Lyapunov paired trajectories (task_id 7, LpnMult): [0, n/2) bases, n/2 + b the variation of b.

@@ -17,7 +17,9 @@ namespace qjx {
 cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st);
 int pick_layout(int d, int *rows_per_block);
 cudaError_t launch_dmma_peak(double *out, int blocks, int iters, cudaStream_t st);
-size_t step_smem_bytes(int MD);
+size_t step_smem_bytes(int MD, int nc, int kb);
+bool pick_step_tiles(int MD, size_t budget, int *nc, int *kb);
+size_t step_static_smem();
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st);
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st);
 cudaError_t launch_init_state(const Params &P, cudaStream_t st);
@@ -176,6 +178,7 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
     const int G = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;
     if (c.d > kMaxMD || G > kMaxGroups) return QJX_ERR_UNSUPPORTED;
     if (c.precision != 0 && c.precision != 1) return QJX_ERR_INVALID_ARG;
+    if (c.precision == 1 && c.d > 256) return QJX_ERR_UNSUPPORTED;  // the split kernel's N = MDs <= 256
 
     qjx_engine *h = new (std::nothrow) qjx_engine();
     if (!h) return QJX_ERR_OOM;
@@ -202,6 +205,13 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
     const int kp = (d + 1) & ~1;  // k rows padded to whole pairs for the m8n8k4 MMA
     h->MD = MD;
     Params &P = h->P;
+    {  // plain step kernel tiling for this dimension
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
+        const size_t fixed = step_static_smem() + 1024;
+        if ((size_t)optin <= fixed || !pick_step_tiles(MD, (size_t)optin - fixed, &P.nc, &P.kb))
+            return bail(QJX_ERR_UNSUPPORTED);
+    }
     P.d = d;
     P.MD = MD;
     P.n = n;

@@ -23,6 +23,8 @@
 // (mma.sync m8n8k4 f64), laid out so that every output keeps the oracle's k-ascending fma
 // chain (bit-identical results).  The split-precision form (qjx_split.cuh, included at the
 // end) runs the same micro-steps with bf16x3 products on the tcgen05 tensor cores.
+#include <algorithm>
+
 #include "qjx_device.cuh"
 
 namespace qjx {
@@ -132,12 +134,19 @@ __device__ __forceinline__ int advance(TrajState &s, const double *dt, int nb, i
     }
 }
 
+// |psi_k|^2 / norm as mult_scalar_double(mult_scalar_complex(phi, phi, 1), 1/norm).real
+// (core.cpp:665-725), recomputed wherever it is needed (no scratch array)
+__device__ __forceinline__ double adr_of(double2 v, double inv)
+{
+    return __dmul_rn(__dadd_rn(0.0, __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y))), inv);
+}
+
 // Observables of the state held in `col` (calc_chars_std[_start], core.cpp:665-725) and
 // the normalised state psi / sqrt(norm) written to the spare slot for the energy and
 // random-observable micro-steps.  Warp-cooperative; every lane computes the sequential
 // sums identically.
-__device__ void obs_prep(const Params &P, const TrajState &s, int tr, const double2 *col, double *wscr,
-                         int lane, int dump, int is_start)
+__device__ void obs_prep(const Params &P, const TrajState &s, int tr, const double2 *col, int lane, int dump,
+                         int is_start)
 {
     const int d = P.d;
     const double nrm = warp_norm(col, d, lane);
@@ -149,19 +158,17 @@ __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const doub
     for (int k = lane; k < d; k += 32) {
         const double2 v = col[k];
         hat[k] = make_double2(__ddiv_rn(v.x, sq), __ddiv_rn(v.y, sq));
-        const double a = __dmul_rn(__dadd_rn(0.0, __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y))), inv);
-        wscr[k] = a;
-        if (adr_out) adr_out[k] = a;
+        if (adr_out) adr_out[k] = adr_of(v, inv);
     }
     double mean = 0.0;
-    for (int k = lane; k < d; k += 32) mean = __dadd_rn(mean, __dmul_rn((double)k, wscr[k]));
+    for (int k = lane; k < d; k += 32) mean = __dadd_rn(mean, __dmul_rn((double)k, adr_of(col[k], inv)));
     mean = warp_allsum(mean);
     const double ms = is_start ? mean : P.mean_start[tr];
     const double disp = __dmul_rn(__dsub_rn(mean, ms), __dsub_rn(mean, ms));
     double m2 = 0.0;
     for (int k = lane; k < d; k += 32) {
         const double dk = __dsub_rn((double)k, mean);
-        m2 = __dadd_rn(m2, __dmul_rn(__dmul_rn(dk, dk), wscr[k]));
+        m2 = __dadd_rn(m2, __dmul_rn(__dmul_rn(dk, dk), adr_of(col[k], inv)));
     }
     m2 = warp_allsum(m2);
     if (lane == 0) {
@@ -177,18 +184,18 @@ __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const doub
 
 // Continue after a completed split step: period / dump / target bookkeeping.  Returns the
 // next group, or -1 when the trajectory is done for this call.
-__device__ int after_step(const Params &P, TrajState &s, int tr, const double2 *col, double *wscr, int lane)
+__device__ int after_step(const Params &P, TrajState &s, int tr, const double2 *col, int lane)
 {
     const int a = advance(s, P.dt, P.nb, P.brep);
     if (a == 2) s.pc += 1;
     if (a >= 1 && P.subdump && (s.rk_sid & 1) == 0) {  // deep task: a sub-period ended
-        obs_prep(P, s, tr, col, wscr, lane, P.dump_base + s.di, 0);
+        obs_prep(P, s, tr, col, lane, P.dump_base + s.di, 0);
         s.phase = PH_OBS_E;
         return P.gHE;
     }
     if (a == 2) {
         if (s.di < P.n_dumps && s.pc == P.dump_at[s.di]) {
-            obs_prep(P, s, tr, col, wscr, lane, P.dump_base + s.di, 0);
+            obs_prep(P, s, tr, col, lane, P.dump_base + s.di, 0);
             s.phase = PH_OBS_E;
             return P.gHE;
         }
@@ -217,7 +224,7 @@ __device__ int finish_obs(const Params &P, TrajState &s)
 
 // An RK step finished without crossing (rk_period, core.cpp:443-449): next step, period and dump
 // bookkeeping.  `col` holds psi, nrm its norm.
-__device__ int rk_after_step(const Params &P, TrajState &s, int tr, const double2 *col, double *wscr, int lane,
+__device__ int rk_after_step(const Params &P, TrajState &s, int tr, const double2 *col, int lane,
                              double nrm)
 {
     s.rk_prev = nrm;
@@ -226,7 +233,7 @@ __device__ int rk_after_step(const Params &P, TrajState &s, int tr, const double
         s.rk_sid = 0;
         s.pc += 1;
         if (s.di < P.n_dumps && s.pc == P.dump_at[s.di]) {
-            obs_prep(P, s, tr, col, wscr, lane, P.dump_base + s.di, 0);
+            obs_prep(P, s, tr, col, lane, P.dump_base + s.di, 0);
             s.phase = PH_OBS_E;
             return P.gHE;
         }
@@ -242,7 +249,7 @@ __device__ int rk_after_step(const Params &P, TrajState &s, int tr, const double
 // Apply the chosen jump channel: psi = (L_idx psi_hat) / sqrt(w_idx / g_idx)
 // (experiment.cpp:1346-1369), record the channel, redraw eta (qj_proc.cpp:310-314) and
 // count the finest-level step.
-__device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, double *wscr, int lane, int idx,
+__device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, int lane, int idx,
                           double w_idx, int *err)
 {
     const int d = P.d;
@@ -266,17 +273,15 @@ __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, d
     }
     s.phase = PH_STEP;
     s.t = __dadd_rn(s.t, P.dt[P.deep - 1]);
-    return after_step(P, s, tr, col, wscr, lane);
+    return after_step(P, s, tr, col, lane);
 }
 
 // Warp-cooperative epilogue of one trajectory column: `col` holds M_g * psi in shared memory,
 // `s_in` the trajectory's state record (loaded by the caller).  Returns the bucket of the
 // trajectory's next micro-step, or -1 (done, paused or failed); the caller appends it.
-__device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, int tr, const TrajState &s_in,
-                               int lane)
+__device__ int column_epilogue(const Params &P, double2 *col, int tr, const TrajState &s_in, int lane)
 {
     const int d = P.d;
-    double *wscr = reinterpret_cast<double *>(wscr_c);
     TrajState s = s_in;
     int g2 = -1;
     int err = 0;
@@ -297,7 +302,7 @@ __device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, i
             for (int k = lane; k < d; k += 32) dst[k] = col[k];
             s.cur ^= 1;
             s.t = __dadd_rn(s.t, dt);
-            g2 = after_step(P, s, tr, col, wscr, lane);
+            g2 = after_step(P, s, tr, col, lane);
         } else if (s.lvl < P.deep - 1) {  // crossed on a coarse level: bisect from psi (qj_proc.cpp:328-331)
             s.lvl += 1;
             g2 = s.b * P.deep + s.lvl;
@@ -366,7 +371,7 @@ __device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, i
         }
         if (err) break;
         if (P.nd == 1) {
-            g2 = apply_jump(P, s, tr, col, wscr, lane, index, w, &err);
+            g2 = apply_jump(P, s, tr, col, lane, index, w, &err);
         } else {
             s.phase = PH_REC_A;
             s.sub = index;
@@ -376,7 +381,7 @@ __device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, i
 
     case PH_REC_A: {
         const double w = P.gn[(size_t)tr * P.nd + s.sub];
-        g2 = apply_jump(P, s, tr, col, wscr, lane, s.sub, w, &err);
+        g2 = apply_jump(P, s, tr, col, lane, s.sub, w, &err);
     } break;
 
     case PH_RK: {  // one right-hand side of rk_int_dimer (core.cpp:11592-11619), col = M arg
@@ -434,7 +439,7 @@ __device__ int column_epilogue(const Params &P, double2 *col, double2 *wscr_c, i
             if (nrm > s.eta) {  // not crossed: accept psi in place
                 double2 *dst = slot_ptr(P, s.cur, tr);
                 for (int k = lane; k < d; k += 32) dst[k] = col[k];
-                g2 = rk_after_step(P, s, tr, col, wscr, lane, nrm);
+                g2 = rk_after_step(P, s, tr, col, lane, nrm);
             } else {  // crossed: integrate the begin part from psi, still in its slot (core.cpp:11913-11922)
                 const double norm_diff = __dsub_rn(s.rk_prev, nrm);
                 const double begin_part = __ddiv_rn(__dsub_rn(s.rk_prev, s.eta), norm_diff);
@@ -587,7 +592,7 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
 // WPC warps share one column block; warp `sub` of them owns row blocks sub, sub + WPC, ...
 template <int NRB, int WPC>
 __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, double2 *Us, uint64_t *bar,
-                                          int *released, uint32_t &phase, int d, int kp, int RB, int MD,
+                                          int *released, uint32_t &phase, int d, int kp, int KB, int RB, int MD,
                                           int warp, int lane, int tid)
 {
     const int S16 = MD + 1;
@@ -596,7 +601,7 @@ __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, doubl
     // each scheduler the same number of row blocks
     const int cb = warp / WPC, sub = (warp % WPC + cb * (WPC / 4)) % WPC;
     const int th = t >> 1, todd = t & 1;
-    const int nslab = (kp + kKB - 1) / kKB;
+    const int nslab = (kp + KB - 1) / KB;
     bool ok = true;
     double re[NRB][2], im[NRB][2];
 #pragma unroll
@@ -609,9 +614,9 @@ __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, doubl
         const int q = sl % kStages;
         if (!mbar_wait_bounded(&bar[q], (phase >> q) & 1u, kWaitLimit)) ok = false;
         phase ^= 1u << q;
-        const int k0 = sl * kKB;
-        const int kc = min(kKB, kp - k0);  // even
-        const double *Uq = reinterpret_cast<const double *>(Us + q * kKB * MD);
+        const int k0 = sl * KB;
+        const int kc = min(KB, kp - k0);  // even
+        const double *Uq = reinterpret_cast<const double *>(Us + q * KB * MD);
 #pragma unroll 2
         for (int kk = 0; kk < kc; kk += 2) {
             const double2 xb = bcol[k0 + kk + th];
@@ -636,10 +641,10 @@ __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, doubl
             if (atomicAdd(&released[q], 1) == kThreads / 32 - 1) {
                 released[q] = 0;
                 const int sn = sl + kStages;
-                const int kn = min(kKB, kp - sn * kKB);
+                const int kn = min(KB, kp - sn * KB);
                 fence_proxy_async();
                 mbar_expect_tx(&bar[q], (uint32_t)(kn * MD * 16));
-                bulk_g2s(Us + q * kKB * MD, mat + (size_t)sn * kKB * MD, (uint32_t)(kn * MD * 16), &bar[q]);
+                bulk_g2s(Us + q * KB * MD, mat + (size_t)sn * KB * MD, (uint32_t)(kn * MD * 16), &bar[q]);
             }
         }
     }
@@ -662,11 +667,20 @@ __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, doubl
 // sub-tile (gather, epilogue), 6 per active 8-column block (MMA loop), and 3 more per
 // sub-tile of the jump-operator and observable buckets, whose epilogues renormalise, draw
 // and reduce.
-__device__ __forceinline__ int subtile_cost(int m, bool heavy_epilogue)
+// Columns of the next sub-tile of a bucket piece of m columns: with 32-column sub-tiles a rest
+// of 17..24 columns is cut as 16 + rest (no sub-tile of 3 column blocks); narrower sub-tiles
+// (large d) take min(m, NC).
+__device__ __forceinline__ int subtile_cols(int m, int NC)
+{
+    if (NC == kNC) return (m > 24) ? min(m, kNC) : (m > 16 ? 16 : m);
+    return min(m, NC);
+}
+
+__device__ __forceinline__ int subtile_cost(int m, bool heavy_epilogue, int NC)
 {
     int c = 0;
     while (m > 0) {
-        const int s = (m > 24) ? min(m, kNC) : (m > 16 ? 16 : m);
+        const int s = subtile_cols(m, NC);
         const int cb = (s + 7) / 8;
         c += 2 + 6 * ((cb == 3) ? 4 : cb) + (heavy_epilogue ? 3 : 0);
         m -= s;
@@ -696,7 +710,9 @@ __device__ __forceinline__ int cost_to_column(const int *cstart, const int *kc, 
 // into equal column ranges, one per persistent CTA; each range is processed as sub-tiles of
 // at most 32 columns of one matrix, and a sub-tile costs in proportion to its active 8-column
 // blocks (1, 2 or 4): the warps are spread over the row blocks of the active column blocks.
-template <int NRB>
+// NRB: row blocks per warp when a sub-tile has its widest CBMAX column blocks (16 / CBMAX warps
+// per column block); CBMAX = P.nc / 8 (4 for d <= ~208, 2 up to 512, 1 up to 1024).
+template <int NRB, int CBMAX>
 __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -704,8 +720,9 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
     const int RB = MD / 8;
     const int S16 = MD + 1;       // odd column stride: conflict-free column reads
     const int kp = (P.d + 1) & ~1;  // k rows padded to pairs (the matrices carry a zero row)
+    const int KB = P.kb;           // k rows per propagator slab
     double2 *Bt = reinterpret_cast<double2 *>(smem);
-    double2 *Us = Bt + kNC * S16;
+    double2 *Us = Bt + P.nc * S16;
     __shared__ __align__(8) uint64_t bar[kStages + 1];
     __shared__ int released[kStages];
     __shared__ int s_cstart[kMaxGroups + 1];
@@ -732,7 +749,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             s_cstart[g] = acc;
             s_kc[g] = kacc;
             acc += cnt_cur[g];
-            kacc += subtile_cost(cnt_cur[g], g >= P.gL0);
+            kacc += subtile_cost(cnt_cur[g], g >= P.gL0, P.nc);
         }
         s_cstart[G] = acc;
         s_kc[G] = kacc;
@@ -745,7 +762,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
     const long long K = s_kc[G];
     const int c_lo = cost_to_column(s_cstart, s_kc, cnt_cur, G, K * blockIdx.x / gridDim.x);
     const int c_hi = cost_to_column(s_cstart, s_kc, cnt_cur, G, K * (blockIdx.x + 1) / gridDim.x);
-    const int nslab = (kp + kKB - 1) / kKB;
+    const int nslab = (kp + KB - 1) / KB;
     uint32_t phase = 0;
     long long work = 0;
     long long tr_setup = 0, tr_loop = 0, tr_epi = 0, tr_sub = 0, tr_cb = 0;
@@ -763,7 +780,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
         const int idx = pos - s_cstart[g];
         // piece of this group left in the range, cut so that no sub-tile has 3 column blocks
         const int m = min(c_hi - pos, cnt_cur[g] - idx);
-        const int ncol = (m > 24) ? min(m, kNC) : (m > 16 ? 16 : m);
+        const int ncol = subtile_cols(m, P.nc);
         const int ncb = (ncol + 7) / 8;
         if (tid < kNC) {
             if (tid < ncol) {
@@ -783,19 +800,25 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             mbar_expect_tx(&bar[kStages], (uint32_t)(ncol * kp * 16));
             for (int c = 0; c < ncol; c++) bulk_g2s(Bt + c * S16, P.psi + s_src[c], (uint32_t)(kp * 16), &bar[kStages]);
             for (int q = 0; q < kStages && q < nslab; q++) {
-                const int kc = min(kKB, kp - q * kKB);
+                const int kc = min(KB, kp - q * KB);
                 mbar_expect_tx(&bar[q], (uint32_t)(kc * MD * 16));
-                bulk_g2s(Us + q * kKB * MD, mat + (size_t)q * kKB * MD, (uint32_t)(kc * MD * 16), &bar[q]);
+                bulk_g2s(Us + q * KB * MD, mat + (size_t)q * KB * MD, (uint32_t)(kc * MD * 16), &bar[q]);
             }
         }
         const long long t1 = clock64();
-        bool ok;
-        if (ncb == 1)
-            ok = tile_dmma<(NRB + 3) / 4, 16>(mat, Bt, Us, bar, released, phase, d, kp, RB, MD, warp, lane, tid);
-        else if (ncb == 2)
-            ok = tile_dmma<(NRB + 1) / 2, 8>(mat, Bt, Us, bar, released, phase, d, kp, RB, MD, warp, lane, tid);
-        else
-            ok = tile_dmma<NRB, 4>(mat, Bt, Us, bar, released, phase, d, kp, RB, MD, warp, lane, tid);
+        bool ok = false;
+        constexpr int W1 = 16 / CBMAX;  // warps per column block of the widest sub-tile
+        if (ncb == 1) {
+            ok = tile_dmma<(NRB * W1 + 15) / 16, 16>(mat, Bt, Us, bar, released, phase, d, kp, KB, RB, MD, warp,
+                                                     lane, tid);
+        } else if constexpr (CBMAX >= 2) {
+            if (ncb == 2) {
+                ok = tile_dmma<(NRB * W1 + 7) / 8, 8>(mat, Bt, Us, bar, released, phase, d, kp, KB, RB, MD, warp,
+                                                      lane, tid);
+            } else if constexpr (CBMAX == 4) {
+                ok = tile_dmma<NRB, 4>(mat, Bt, Us, bar, released, phase, d, kp, KB, RB, MD, warp, lane, tid);
+            }
+        }
         if (!__syncthreads_and(ok ? 1 : 0)) {  // a bounded wait gave up: report and stop
             if (tid == 0) {
                 atomicAdd(&P.ctrl[4], 1);
@@ -804,9 +827,8 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             return;
         }
         const long long t2 = clock64();
-        double2 *wscr = Us + warp * MD;
         for (int c = warp; c < ncol; c += kThreads / 32) {
-            const int g2 = column_epilogue(P, Bt + c * S16, wscr, s_tr[c], s_st[c], lane);
+            const int g2 = column_epilogue(P, Bt + c * S16, s_tr[c], s_st[c], lane);
             if (lane == 0) s_g2[c] = g2;
         }
         __syncthreads();
@@ -870,14 +892,13 @@ __global__ void observe_kernel(const Params P, int dump, int is_start)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tr = blockIdx.x * (blockDim.x / 32) + warp;
     if (tr >= P.n) return;
-    double2 *col = reinterpret_cast<double2 *>(smem) + (size_t)warp * 2 * P.MD;
-    double *wscr = reinterpret_cast<double *>(col + P.MD);
+    double2 *col = reinterpret_cast<double2 *>(smem) + (size_t)warp * P.MD;
     TrajState s = P.st[tr];
     if (s.phase == PH_ERROR) return;
     const double2 *src = slot_ptr(P, s.cur, tr);
     for (int k = lane; k < P.d; k += 32) col[k] = src[k];
     __syncwarp();
-    obs_prep(P, s, tr, col, wscr, lane, dump, is_start);
+    obs_prep(P, s, tr, col, lane, dump, is_start);
     if (lane == 0) {
         s.pc = 0;
         s.di = 0;
@@ -1012,18 +1033,38 @@ __global__ void clear_records_kernel(const Params P)
 }
 
 // ---------------------------------------------------------------- host-side launchers
-template <int NRB>
+size_t step_smem_bytes(int MD, int nc, int kb);
+
+template <int NRB, int CBMAX>
 static cudaError_t launch_step_t(const Params &P, int s, int grid, cudaStream_t st)
 {
-    const size_t smem = (size_t)(kNC * (P.MD + 1) + kStages * kKB * P.MD) * sizeof(double2);
+    const size_t smem = step_smem_bytes(P.MD, P.nc, P.kb);
     static int attr_bytes = 0;
     if (attr_bytes < (int)smem) {
-        cudaError_t e = cudaFuncSetAttribute(step_kernel<NRB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(step_kernel<NRB, CBMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_bytes = (int)smem;
     }
-    step_kernel<NRB><<<grid, kThreads, smem, st>>>(P, s);
+    step_kernel<NRB, CBMAX><<<grid, kThreads, smem, st>>>(P, s);
     return cudaGetLastError();
+}
+
+template <int CBMAX>
+static cudaError_t launch_step_cb(const Params &P, int s, int grid, cudaStream_t st)
+{
+    const int RB = P.MD / 8, W1 = 16 / CBMAX;
+    switch ((RB + W1 - 1) / W1) {  // row blocks per warp at the widest sub-tile
+    case 1: return launch_step_t<1, CBMAX>(P, s, grid, st);
+    case 2: return launch_step_t<2, CBMAX>(P, s, grid, st);
+    case 3: return launch_step_t<3, CBMAX>(P, s, grid, st);
+    case 4: return launch_step_t<4, CBMAX>(P, s, grid, st);
+    case 5: return launch_step_t<5, CBMAX>(P, s, grid, st);
+    case 6: return launch_step_t<6, CBMAX>(P, s, grid, st);
+    case 7: return launch_step_t<7, CBMAX>(P, s, grid, st);
+    case 8: return launch_step_t<8, CBMAX>(P, s, grid, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 // Padded rows for dimension d: whole 8-row blocks (the m8n8k4 row block).
@@ -1038,21 +1079,51 @@ cudaError_t launch_split_step(const Params &P, int s, int grid, cudaStream_t st)
 cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st)
 {
     if (P.split) return launch_split_step(P, s, grid, st);
-    const int RB = P.MD / 8;
-    switch ((RB + 3) / 4) {  // row blocks per warp with 4 warps per column block
-    case 1: return launch_step_t<1>(P, s, grid, st);
-    case 2: return launch_step_t<2>(P, s, grid, st);
-    case 3: return launch_step_t<3>(P, s, grid, st);
-    case 4: return launch_step_t<4>(P, s, grid, st);
-    case 5: return launch_step_t<5>(P, s, grid, st);
-    case 6: return launch_step_t<6>(P, s, grid, st);
-    case 7: return launch_step_t<7>(P, s, grid, st);
-    case 8: return launch_step_t<8>(P, s, grid, st);
+    switch (P.nc) {
+    case 32: return launch_step_cb<4>(P, s, grid, st);
+    case 16: return launch_step_cb<2>(P, s, grid, st);
+    case 8: return launch_step_cb<1>(P, s, grid, st);
     default: return cudaErrorInvalidValue;
     }
 }
 
-size_t step_smem_bytes(int MD) { return (size_t)(kNC * (MD + 1) + kStages * kKB * MD) * sizeof(double2); }
+// Shared memory of the step kernel: nc staged columns of MD + 1 (odd stride) and kStages
+// propagator slabs of kb k rows.
+size_t step_smem_bytes(int MD, int nc, int kb)
+{
+    return (size_t)(nc * (MD + 1) + kStages * kb * MD) * sizeof(double2);
+}
+
+// Static shared memory of the step kernel (the same for every instantiation).
+size_t step_static_smem()
+{
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, step_kernel<1, 4>) != cudaSuccess) return 16384;
+    return a.sharedSizeBytes;
+}
+
+// Widest sub-tile (32, 16 or 8 columns) whose staged columns leave room for slabs of at least
+// 8 k rows (at most 16, even) in `budget` bytes of dynamic shared memory, with at most 8 row
+// blocks per warp; failing that, the widest with 2-row slabs.  Returns false when none fits.
+bool pick_step_tiles(int MD, size_t budget, int *nc, int *kb)
+{
+    const int RB = MD / 8;
+    for (int min_kb = 8; min_kb >= 2; min_kb -= 6) {
+        for (int c = kNC; c >= 8; c /= 2) {
+            const int W1 = 16 / (c / 8);
+            if ((RB + W1 - 1) / W1 > 8) continue;
+            const size_t bt = (size_t)c * (MD + 1) * sizeof(double2);
+            if (bt >= budget) continue;
+            int k = (int)((budget - bt) / ((size_t)kStages * MD * sizeof(double2)));
+            k = std::min(k, kKB) & ~1;
+            if (k < min_kb) continue;
+            *nc = c;
+            *kb = k;
+            return true;
+        }
+    }
+    return false;
+}
 
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st)
 {
@@ -1062,11 +1133,11 @@ cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st)
 
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st)
 {
-    const size_t smem = (size_t)8 * 2 * P.MD * sizeof(double2);
+    const size_t smem = (size_t)8 * P.MD * sizeof(double2);
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(observe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(8 * 2 * kMaxMD * sizeof(double2)));
+                                             (int)(8 * kMaxMD * sizeof(double2)));
         if (e != cudaSuccess) return e;
         attr_set = true;
     }

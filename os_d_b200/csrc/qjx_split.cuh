@@ -122,8 +122,8 @@ size_t split_stage_bytes(int MDs) { return (size_t)kAPlanes * (kABytes + (size_t
 size_t split_smem_bytes(int MDs, int MD, int stages)
 {
     const size_t ring = (size_t)stages * split_stage_bytes(MDs);
-    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2) + (size_t)(kThreads / 32) * MD * sizeof(double2) +
-                       (size_t)kTileM * sizeof(TrajState);
+    (void)MD;
+    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2) + (size_t)kTileM * sizeof(TrajState);
     return ring > epi ? ring : epi;
 }
 
@@ -135,8 +135,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const size_t stage_bytes = (size_t)kAPlanes * (kABytes + bbytes);
     const int S16 = MDs + 1;
     double2 *Bt = reinterpret_cast<double2 *>(smem);          // epilogue: [32][S16] FP64 columns
-    double2 *wscr = Bt + 32 * S16 + (size_t)(threadIdx.x >> 5) * P.MD;
-    TrajState *s_st = reinterpret_cast<TrajState *>(Bt + 32 * S16 + (size_t)(kThreads / 32) * P.MD);  // [128]
+    TrajState *s_st = reinterpret_cast<TrajState *>(Bt + 32 * S16);  // [128]
     __shared__ __align__(8) uint64_t fullA[kMaxSStages], fullB[kMaxSStages], empty[kMaxSStages], accf;
     __shared__ uint32_t s_tmem;
     __shared__ int s_tstart[kMaxGroups + 1];
@@ -343,7 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             for (int cc = warp; cc < 32; cc += kThreads / 32) {
                 const int m = 32 * c + cc;
                 if (m < rows) {
-                    const int g2 = column_epilogue(P, Bt + (size_t)cc * S16, wscr, s_tr[m], s_st[m], lane);
+                    const int g2 = column_epilogue(P, Bt + (size_t)cc * S16, s_tr[m], s_st[m], lane);
                     if (lane == 0) s_g2[m] = g2;
                 }
             }

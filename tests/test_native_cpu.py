@@ -103,7 +103,8 @@ def test_create_rejects_bad_arguments_before_touching_a_gpu():
     assert create(n_traj=0) == 1
     assert create(T=0.0) == 1
     assert create(num_robs=1) == 1    # R missing
-    assert create(d=300) == 8         # QJX_ERR_UNSUPPORTED: d > 256
+    assert create(d=1025) == 8        # QJX_ERR_UNSUPPORTED: d > 1024
+    assert create(d=300, precision=1) == 8  # the split form takes d <= 256
     assert lib.qjx_create(None, None, None, None, None, None, C.byref(h)) == 1
 
 
