@@ -113,6 +113,27 @@ qjx_status qjx_create(const qjx_config *cfg, const double *U, const double *L, c
 qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, const double *H_drv, double E0, double A,
                          int drv_type, double drv_freq, double drv_phase, int rk_ns, const double *L,
                          const double *g, const double *HE, const double *R, qjx_engine **out);
+/* One ensemble of a batched engine: its own dimension, trajectories, period, Philox key and first
+ * stream (the thresholds it would draw in an engine of its own with seed = seed and
+ * tr_base = tr_base), and its operators with the layouts of qjx_create at this d. */
+typedef struct {
+    int d;
+    int n_traj;
+    double T;
+    uint64_t seed;
+    int64_t tr_base;
+    const double *U, *L, *g, *HE, *R;
+} qjx_ensemble;
+/* Batched engine: n_ens ensembles of uneven Hilbert dimension (d <= 1024) advanced together by
+ * the same persistent micro-step launches (every (ensemble, matrix) pair is a bucket of the
+ * grouped GEMM; a sub-tile multiplies only its ensemble's d x d block).  cfg supplies what the
+ * ensembles share: deep, num_branches, num_diss, num_robs, record, rng_kind, rec_cap, keep_adr,
+ * max_dumps, device, deep_num_steps; cfg's d, n_traj, T, seed and tr_base are ignored and
+ * precision must be 0.  Trajectories are numbered ensemble after ensemble; states and
+ * observables use the largest dimension as row length (qjx_set_states: rows zero-padded past
+ * each ensemble's d).  Every trajectory is bit-identical to its run in an engine of its own.
+ * The Lyapunov entry points, qjx_purity and the RK propagator take single-ensemble engines. */
+qjx_status qjx_create_batch(const qjx_config *cfg, int n_ens, const qjx_ensemble *ens, qjx_engine **out);
 void qjx_destroy(qjx_engine *h);
 const char *qjx_last_error(const qjx_engine *h);
 const char *qjx_status_string(qjx_status s);

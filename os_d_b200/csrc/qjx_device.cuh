@@ -64,7 +64,8 @@ struct __align__(16) TrajState {
     int rk_stage;      // 1..4: right-hand side being evaluated
     int rk_part;       // 0: H_eff arg, 1: H_drv arg
     int rk_ctx;        // 0: step checked for a crossing; 1: begin part of a located jump
-    int rk_pad[2];
+    int ens;           // ensemble of the trajectory (batched engines; 0 otherwise)
+    int rk_pad;
 };
 static_assert(sizeof(TrajState) == 144, "TrajState layout");
 
@@ -127,7 +128,39 @@ struct Params {
     // plain step kernel tiling (chosen from MD and the shared memory): columns per sub-tile
     // (32, 16 or 8) and k rows per propagator slab
     int nc, kb;
+    // ensembles (a batched engine holds E ensembles of their own dimension, operators, seed and
+    // period; an ordinary engine is the batch of one).  Trajectories [e_tr0[e], e_tr0[e+1]) form
+    // ensemble e; its groups are e_g0[e] + the local group (branch * deep + level, gL0 + channel,
+    // gHE, gR0 + observable).  d and MD above are the largest dimension and its padded rows.
+    int E;
+    const int *e_d;                   // [E] dimension
+    const int *e_tr0;                 // [E + 1] first trajectory
+    const int *e_g0;                  // [E] first group
+    const double *e_dt;               // [E][deep] split-level steps
+    const double *e_rate;             // [E][nd] jump rates
+    const unsigned long long *e_seed; // [E] Philox key
+    const long long *e_sbase;         // [E] Philox stream of the ensemble's first trajectory
+    const long long *g_off;           // [G] offset of the group's matrix in mats (double2 units)
+    const int *g_ens;                 // [G] ensemble of the group
+    const long long *g_loff;          // [G] start of the group's bucket list (capacity: the
+                                      // ensemble's trajectories); lists hold 2 x ltot entries
+    long long ltot;
+    // plain step kernel plan of the next micro-step: [0, G] bucket starts, [G + 1, 2G + 1] cost
+    // prefix; written by the last CTA of a micro-step (or plan_kernel after a host call)
+    int *plan;
+    unsigned int *plan_sync;          // [1] CTAs finished in the current micro-step
 };
+
+// Dimension, split-level steps and jump rates of a trajectory's ensemble.
+__device__ __forceinline__ int dim_of(const Params &P, const TrajState &s) { return P.e_d[s.ens]; }
+__device__ __forceinline__ const double *dt_of(const Params &P, const TrajState &s)
+{
+    return P.e_dt + (size_t)s.ens * P.deep;
+}
+__device__ __forceinline__ double rate_of(const Params &P, const TrajState &s, int i)
+{
+    return P.e_rate[(size_t)s.ens * P.nd + i];
+}
 
 // Lyapunov paired trajectories (task_id 7, LpnMult): [0, n/2) bases, n/2 + b the variation of b.
 struct LpnParams {
@@ -175,12 +208,15 @@ __device__ __forceinline__ double philox_uniform(unsigned long long seed, unsign
     return __dmul_rn((double)(m + 1), 0x1p-53);
 }
 
-// Next uniform of a trajectory; sets *err on an exhausted injected sequence.
+// Next uniform of a trajectory; sets *err on an exhausted injected sequence.  The Philox
+// stream of local trajectory i of ensemble e is e_sbase[e] + i under the key e_seed[e], so an
+// ensemble draws the same numbers alone and inside a batch.
 __device__ __forceinline__ double draw(const Params &P, int tr, TrajState &s, int *err)
 {
     (void)tr;
     if (P.rng_kind == 0)
-        return philox_uniform(P.seed, (unsigned long long)(P.tr_base + s.rng_src), (unsigned long long)(s.rng_pos++));
+        return philox_uniform(P.e_seed[s.ens], (unsigned long long)(P.e_sbase[s.ens] + (s.rng_src - P.e_tr0[s.ens])),
+                              (unsigned long long)(s.rng_pos++));
     const long long lo = P.inj_off[s.rng_src], hi = P.inj_off[s.rng_src + 1];
     if (lo + s.rng_pos >= hi) { *err = ERR_RNG; return 0.5; }
     return P.inj_u[lo + (s.rng_pos++)];

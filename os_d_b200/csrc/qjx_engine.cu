@@ -62,6 +62,7 @@ struct qjx_engine {
     qjx_stats stats{};
     bool states_set = false;
     int period_base = 0;  // periods run since the last time reset (the RK propagator's period_id)
+    int n_ens = 1;        // ensembles (qjx_create_batch)
     // Lyapunov task (allocated by the first qjx_lpn_start)
     LpnParams L{};
     bool lpn_alloc = false, lpn_started = false;
@@ -166,23 +167,59 @@ static void pack_split(const double *M, int d, int MDs, int KS, uint16_t *out)
             }
 }
 
-static qjx_status create_engine(const qjx_config *cfg, const double *U, const double *L, const double *g,
-                                const double *HE, const double *R, int psi_slots, qjx_engine **out)
+// One ensemble of an engine: its dimension, trajectories, period, Philox key and first stream,
+// and operators (U: [num_branches][deep][d][d], L: [num_diss][d][d], g: [num_diss], HE, R).
+struct EnsDesc {
+    int d, n;
+    double T;
+    uint64_t seed;
+    int64_t sbase;
+    const double *U, *L, *g, *HE, *R;
+};
+
+template <class T>
+static T *upload(qjx_engine *h, const std::vector<T> &v)
 {
-    if (!cfg || !out || !U || !L || !g || !HE) return QJX_ERR_INVALID_ARG;
+    T *p = (T *)dalloc(h, std::max<size_t>(1, v.size()) * sizeof(T));
+    if (p && !v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return p;
+}
+
+// Engine over E ensembles (E = 1: an ordinary engine).  cfg supplies what the ensembles share:
+// deep, num_branches, num_diss, num_robs, record, rng_kind, rec_cap, keep_adr, max_dumps,
+// device, precision, deep_num_steps.
+static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc> &ens, int psi_slots,
+                                qjx_engine **out)
+{
+    if (!cfg || !out || ens.empty()) return QJX_ERR_INVALID_ARG;
     *out = nullptr;
     const qjx_config &c = *cfg;
-    if (c.d < 2 || c.n_traj < 1 || c.deep < 1 || c.deep > 62 || c.num_branches < 1 || c.num_diss < 1 ||
-        c.num_robs < 0 || !(c.T > 0.0) || (c.num_robs > 0 && !R))
+    if (c.deep < 1 || c.deep > 62 || c.num_branches < 1 || c.num_diss < 1 || c.num_robs < 0 || c.deep_num_steps < 0)
         return QJX_ERR_INVALID_ARG;
-    const int G = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;
-    if (c.d > kMaxMD || G > kMaxGroups) return QJX_ERR_UNSUPPORTED;
+    const int E = (int)ens.size();
+    int dmax = 0;
+    long long ntot = 0;
+    for (const EnsDesc &e : ens) {
+        if (e.d < 2 || e.n < 1 || !(e.T > 0.0) || !e.U || !e.L || !e.g || !e.HE || (c.num_robs > 0 && !e.R))
+            return QJX_ERR_INVALID_ARG;
+        dmax = std::max(dmax, e.d);
+        ntot += e.n;
+    }
+    const int Ge = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;  // groups per ensemble
+    const long long Gl = (long long)E * Ge;
+    if (dmax > kMaxMD || Ge > kMaxGroups || Gl > (1 << 24) || ntot > (1 << 30)) return QJX_ERR_UNSUPPORTED;
     if (c.precision != 0 && c.precision != 1) return QJX_ERR_INVALID_ARG;
-    if (c.precision == 1 && c.d > 256) return QJX_ERR_UNSUPPORTED;  // the split kernel's N = MDs <= 256
+    // the split kernel's N = MDs <= 256 and its bucket tables hold one ensemble
+    if (c.precision == 1 && (dmax > 256 || E > 1)) return QJX_ERR_UNSUPPORTED;
+    const int G = (int)Gl;
+    const int n = (int)ntot;
 
     qjx_engine *h = new (std::nothrow) qjx_engine();
     if (!h) return QJX_ERR_OOM;
     h->cfg = c;
+    h->cfg.d = dmax;
+    h->cfg.n_traj = n;
+    h->n_ens = E;
     if (h->cfg.rec_cap <= 0) h->cfg.rec_cap = 1024;
     if (h->cfg.max_dumps <= 0) h->cfg.max_dumps = 1;
     auto bail = [&](qjx_status s) {
@@ -199,13 +236,12 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
     cudaEventCreate(&h->eb0);
     cudaEventCreate(&h->eb1);
 
-    const int d = c.d, n = c.n_traj;
+    const int d = dmax;
     int rows_per_block = 0;
     const int MD = pick_layout(d, &rows_per_block);
-    const int kp = (d + 1) & ~1;  // k rows padded to whole pairs for the m8n8k4 MMA
     h->MD = MD;
     Params &P = h->P;
-    {  // plain step kernel tiling for this dimension
+    {  // plain step kernel tiling for the largest dimension
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
         const size_t fixed = step_static_smem() + 1024;
@@ -220,32 +256,92 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
     P.nd = c.num_diss;
     P.nr = c.num_robs;
     P.G = G;
-    P.gL0 = c.num_branches * c.deep;
+    P.E = E;
+    P.gL0 = c.num_branches * c.deep;  // local group offsets, the same in every ensemble
     P.gHE = P.gL0 + c.num_diss;
     P.gR0 = P.gHE + 1;
     P.rng_kind = c.rng_kind;
-    P.seed = c.seed;
-    P.tr_base = c.tr_base;
+    P.seed = ens[0].seed;
+    P.tr_base = ens[0].sbase;
     P.keep_adr = c.keep_adr;
     P.rec_cap = h->cfg.rec_cap;
     P.n_active = n;
 
-    // matrices in the transposed padded layout mats[g][k][row], k < kp, row < MD (zero padded)
-    const size_t per = (size_t)kp * MD * 2;
-    std::vector<double> host((size_t)G * per, 0.0);
-    const size_t dd2 = (size_t)d * d * 2;
-    for (int b = 0; b < c.num_branches; b++)
-        for (int l = 0; l < c.deep; l++)
-            pack_transposed(U + dd2 * ((size_t)b * c.deep + l), d, MD, host.data() + per * (b * c.deep + l));
-    for (int i = 0; i < c.num_diss; i++) pack_transposed(L + dd2 * i, d, MD, host.data() + per * (P.gL0 + i));
-    pack_transposed(HE, d, MD, host.data() + per * P.gHE);
-    for (int i = 0; i < c.num_robs; i++) pack_transposed(R + dd2 * i, d, MD, host.data() + per * (P.gR0 + i));
+    // ensemble tables; matrices of ensemble e in its own transposed padded layout
+    // [k < kp_e][row < MD_e] (zero padded), one after another
+    std::vector<int> e_d(E), e_tr0(E + 1), e_g0(E), g_ens(G);
+    std::vector<double> e_dt((size_t)E * c.deep), e_rate((size_t)E * c.num_diss);
+    std::vector<unsigned long long> e_seed(E);
+    std::vector<long long> e_sbase(E), g_off(G), g_loff(G);
+    long long moff = 0, loff = 0;
+    e_tr0[0] = 0;
+    for (int e = 0; e < E; e++) {
+        const EnsDesc &x = ens[e];
+        e_d[e] = x.d;
+        e_tr0[e + 1] = e_tr0[e] + x.n;
+        e_g0[e] = e * Ge;
+        e_seed[e] = x.seed;
+        e_sbase[e] = x.sbase;
+        // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24); the deep tasks'
+        // tree head is the sub-period T / (2 deep_num_steps) (core.cpp:9934)
+        const double t_head = c.deep_num_steps > 0 ? 0.5 * x.T / double(c.deep_num_steps) : x.T;
+        double dt = t_head * 0.5;
+        for (int l = 0; l < c.deep; l++) {
+            dt *= 0.5;
+            e_dt[(size_t)e * c.deep + l] = dt;
+        }
+        for (int i = 0; i < c.num_diss; i++) e_rate[(size_t)e * c.num_diss + i] = x.g[i];
+        const long long per = (long long)((x.d + 1) & ~1) * (8 * ((x.d + 7) / 8));
+        for (int l = 0; l < Ge; l++) {
+            g_ens[e * Ge + l] = e;
+            g_off[e * Ge + l] = moff;
+            g_loff[e * Ge + l] = loff;
+            moff += per;
+            loff += x.n;
+        }
+    }
+    std::vector<double> host((size_t)moff * 2, 0.0);
+    for (int e = 0; e < E; e++) {
+        const EnsDesc &x = ens[e];
+        const int MDe = 8 * ((x.d + 7) / 8);
+        const size_t dd2 = (size_t)x.d * x.d * 2;
+        auto dst = [&](int l) { return host.data() + 2 * (size_t)g_off[e * Ge + l]; };
+        for (int b = 0; b < c.num_branches; b++)
+            for (int l = 0; l < c.deep; l++)
+                pack_transposed(x.U + dd2 * ((size_t)b * c.deep + l), x.d, MDe, dst(b * c.deep + l));
+        for (int i = 0; i < c.num_diss; i++) pack_transposed(x.L + dd2 * i, x.d, MDe, dst(P.gL0 + i));
+        pack_transposed(x.HE, x.d, MDe, dst(P.gHE));
+        for (int i = 0; i < c.num_robs; i++) pack_transposed(x.R + dd2 * i, x.d, MDe, dst(P.gR0 + i));
+    }
     double2 *mats = (double2 *)dalloc(h, host.size() * sizeof(double));
     if (!mats) return bail(QJX_ERR_OOM);
     cudaMemcpy(mats, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
     P.mats = mats;
+    P.e_d = upload(h, e_d);
+    P.e_tr0 = upload(h, e_tr0);
+    P.e_g0 = upload(h, e_g0);
+    P.e_dt = upload(h, e_dt);
+    P.e_rate = upload(h, e_rate);
+    P.e_seed = upload(h, e_seed);
+    P.e_sbase = upload(h, e_sbase);
+    P.g_off = upload(h, g_off);
+    P.g_ens = upload(h, g_ens);
+    P.g_loff = upload(h, g_loff);
+    P.ltot = loff;
+    P.dt = P.e_dt;
+    P.g = P.e_rate;
+    P.plan = (int *)dalloc(h, (size_t)(2 * G + 2) * sizeof(int));
+    P.plan_sync = (unsigned int *)dalloc(h, sizeof(unsigned int));
+    if (!P.e_d || !P.e_tr0 || !P.e_g0 || !P.e_dt || !P.e_rate || !P.e_seed || !P.e_sbase || !P.g_off || !P.g_ens ||
+        !P.g_loff || !P.plan || !P.plan_sync)
+        return bail(QJX_ERR_OOM);
+    cudaMemset(P.plan, 0, (size_t)(2 * G + 2) * sizeof(int));
+    cudaMemset(P.plan_sync, 0, sizeof(unsigned int));
 
     if (c.precision == 1) {  // split precision: bf16 planes of every matrix in the tcgen05 order
+        const EnsDesc &x = ens[0];
+        const double *U = x.U, *L = x.L, *HE = x.HE, *R = x.R;
+        const size_t dd2 = (size_t)d * d * 2;
         P.split = 1;
         P.MDs = 16 * ((d + 15) / 16);
         P.KS = (d + 15) / 16;
@@ -269,31 +365,13 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
         cudaMemcpy(us, hs.data(), hs.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
         P.usplit = us;
     }
-
-    // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24); the deep tasks'
-    // tree head is the sub-period T / (2 deep_num_steps) (core.cpp:9934)
-    if (c.deep_num_steps < 0) return bail(QJX_ERR_INVALID_ARG);
     P.brep = c.deep_num_steps > 0 ? 2 * c.deep_num_steps : 1;
-    const double t_head = c.deep_num_steps > 0 ? 0.5 * c.T / double(c.deep_num_steps) : c.T;
-    std::vector<double> dts(c.deep);
-    double dt = t_head * 0.5;
-    for (int l = 0; l < c.deep; l++) {
-        dt *= 0.5;
-        dts[l] = dt;
-    }
-    double *d_dt = (double *)dalloc(h, sizeof(double) * c.deep);
-    double *d_g = (double *)dalloc(h, sizeof(double) * c.num_diss);
-    if (!d_dt || !d_g) return bail(QJX_ERR_OOM);
-    cudaMemcpy(d_dt, dts.data(), sizeof(double) * c.deep, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_g, g, sizeof(double) * c.num_diss, cudaMemcpyHostToDevice);
-    P.dt = d_dt;
-    P.g = d_g;
 
     P.psi = (double2 *)dalloc(h, (size_t)psi_slots * n * MD * sizeof(double2));
     P.st = (TrajState *)dalloc(h, (size_t)n * sizeof(TrajState));
     P.gn = (double *)dalloc(h, (size_t)n * c.num_diss * sizeof(double));
     P.cnt = (int *)dalloc(h, (size_t)3 * G * sizeof(int));
-    P.lists = (int *)dalloc(h, (size_t)2 * G * n * sizeof(int));
+    P.lists = (int *)dalloc(h, (size_t)2 * P.ltot * sizeof(int));
     const size_t nd_ = (size_t)h->cfg.max_dumps * n;
     P.o_norm = (double *)dalloc(h, nd_ * sizeof(double));
     P.o_mean = (double *)dalloc(h, nd_ * sizeof(double));
@@ -328,6 +406,18 @@ static qjx_status create_engine(const qjx_config *cfg, const double *U, const do
     return QJX_OK;
 }
 
+// The ordinary engine: one ensemble described by cfg.
+static qjx_status create_engine(const qjx_config *cfg, const double *U, const double *L, const double *g,
+                                const double *HE, const double *R, int psi_slots, qjx_engine **out)
+{
+    if (!cfg || !out || !U || !L || !g || !HE) return QJX_ERR_INVALID_ARG;
+    const qjx_config &c = *cfg;
+    if (c.d < 2 || c.n_traj < 1 || !(c.T > 0.0) || (c.num_robs > 0 && !R)) return QJX_ERR_INVALID_ARG;
+    if (c.d > kMaxMD) return QJX_ERR_UNSUPPORTED;
+    const EnsDesc e{c.d, c.n_traj, c.T, c.seed, c.tr_base, U, L, g, HE, R};
+    return create_engine(cfg, std::vector<EnsDesc>{e}, psi_slots, out);
+}
+
 extern "C" void qjx_destroy(qjx_engine *h)
 {
     if (!h) return;
@@ -351,7 +441,9 @@ extern "C" qjx_status qjx_set_states(qjx_engine *h, const double *psi)
     if (!h || !psi) return QJX_ERR_INVALID_ARG;
     const Params &P = h->P;
     CK(cudaSetDevice(h->cfg.device));
-    CK(cudaMemsetAsync(P.psi, 0, (size_t)2 * P.n * P.MD * sizeof(double2), h->stream));
+    // every slot, so the rows past d that the gathers of odd d read are zero
+    const int slots = P.prop == 1 ? kRkSlots : 2;
+    CK(cudaMemsetAsync(P.psi, 0, (size_t)slots * P.n * P.MD * sizeof(double2), h->stream));
     CK(cudaMemcpy2DAsync(P.psi, (size_t)P.MD * sizeof(double2), psi, (size_t)P.d * sizeof(double2),
                          (size_t)P.d * sizeof(double2), P.n, cudaMemcpyHostToDevice, h->stream));
     CK(launch_init_state(P, h->stream));
@@ -504,7 +596,11 @@ static qjx_status run_until_idle(qjx_engine *h)
         if (rs != QJX_OK) break;
         steps += 6 * batch;
         cudaEventRecord(h->eb1, h->stream);
-        cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
+        // the next micro-step's bucket sizes (split form, bucket log) or the plain kernel's plan
+        // total, which the last micro-step computed
+        const bool all_counts = P.split || bucket_log;
+        if (all_counts) cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
+        else cudaMemcpyAsync(h->h_cnt, P.plan + P.G, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
         cudaMemcpyAsync(h->h_ctrl, P.ctrl, sizeof(int) * 16, cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
@@ -516,8 +612,9 @@ static qjx_status run_until_idle(qjx_engine *h)
         h->stats.step_kernel_ms += bms;
         rs = check_ctrl(h);
         if (rs != QJX_OK) break;
-        long long active = 0;
-        for (int g = 0; g < P.G; g++) active += h->h_cnt[g];
+        long long active = all_counts ? 0 : h->h_cnt[0];
+        if (all_counts)
+            for (int g = 0; g < P.G; g++) active += h->h_cnt[g];
         if (bucket_log) {
             for (int g = 0; g < P.G; g++) fprintf(bucket_log, g ? " %d" : "%d", h->h_cnt[g]);
             fprintf(bucket_log, "\n");
@@ -561,6 +658,19 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
                                  const double *HE, const double *R, qjx_engine **out)
 {
     return create_engine(cfg, U, L, g, HE, R, 2, out);
+}
+
+extern "C" qjx_status qjx_create_batch(const qjx_config *cfg, int n_ens, const qjx_ensemble *ens, qjx_engine **out)
+{
+    if (!cfg || !out || n_ens < 1 || !ens) return QJX_ERR_INVALID_ARG;
+    if (cfg->precision != 0) return QJX_ERR_UNSUPPORTED;
+    std::vector<EnsDesc> v(n_ens);
+    for (int e = 0; e < n_ens; e++) {
+        const qjx_ensemble &x = ens[e];
+        if (x.d > kMaxMD) return QJX_ERR_UNSUPPORTED;
+        v[e] = EnsDesc{x.d, x.n_traj, x.T, x.seed, x.tr_base, x.U, x.L, x.g, x.HE, x.R};
+    }
+    return create_engine(cfg, v, 2, out);
 }
 
 extern "C" qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, const double *H_drv, double E0,
@@ -681,6 +791,7 @@ extern "C" qjx_status qjx_purity(qjx_engine *h, double *purity, double *rho)
 {
     if (!h || !purity) return QJX_ERR_INVALID_ARG;
     if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    if (h->n_ens != 1) return fail(h, QJX_ERR_UNSUPPORTED, "qjx_purity takes a single-ensemble engine");
     CK(cudaSetDevice(h->cfg.device));
     Params &P = h->P;
     if (!h->d_hat) {
@@ -771,6 +882,7 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
     if (!h || !c) return QJX_ERR_INVALID_ARG;
     if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
     const Params &P = h->P;
+    if (h->n_ens != 1) return fail(h, QJX_ERR_UNSUPPORTED, "the Lyapunov task takes a single-ensemble engine");
     if (P.n < 2 || (P.n & 1)) return fail(h, QJX_ERR_INVALID_ARG, "the Lyapunov task needs an even n_traj >= 2");
     if (!(c->lpn_type == -1 || c->lpn_type == -2 || (c->lpn_type >= 0 && c->lpn_type < P.nr)))
         return fail(h, QJX_ERR_INVALID_ARG, "lpn_type must be -1, -2 or a random observable index");

@@ -36,17 +36,20 @@ __device__ __forceinline__ double2 *slot_ptr(const Params &P, int slot, int tr)
     return P.psi + ((size_t)slot * P.n + tr) * P.MD;
 }
 
+// Bucket (global group) of a trajectory's next matvec, or -1.
 __device__ __forceinline__ int group_of(const Params &P, const TrajState &s)
 {
+    int g;
     switch (s.phase) {
-    case PH_STEP: return s.b * P.deep + s.lvl;
+    case PH_STEP: g = s.b * P.deep + s.lvl; break;
     case PH_REC_W:
-    case PH_REC_A: return P.gL0 + s.sub;
-    case PH_OBS_E: return P.gHE;
-    case PH_OBS_R: return P.gR0 + s.sub;
-    case PH_RK: return s.rk_part;  // group 0 H_eff, group 1 H_drv
+    case PH_REC_A: g = P.gL0 + s.sub; break;
+    case PH_OBS_E: g = P.gHE; break;
+    case PH_OBS_R: g = P.gR0 + s.sub; break;
+    case PH_RK: g = s.rk_part; break;  // group 0 H_eff, group 1 H_drv
     default: return -1;
     }
+    return P.e_g0[s.ens] + g;
 }
 
 // Slot holding the input vector of a trajectory's next matvec: psi, the normalised copy for
@@ -88,7 +91,7 @@ __device__ __forceinline__ int rk_begin(TrajState &s, double h, double prev, int
 __device__ __forceinline__ void enqueue(const Params &P, int *cnt, int *list, int g, int tr)
 {
     const int pos = atomicAdd(&cnt[g], 1);
-    list[(size_t)g * P.n + pos] = tr;
+    list[P.g_loff[g] + pos] = tr;
 }
 
 __device__ __forceinline__ void report_error(const Params &P, int tr, int code)
@@ -148,13 +151,13 @@ __device__ __forceinline__ double adr_of(double2 v, double inv)
 __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const double2 *col, int lane, int dump,
                          int is_start)
 {
-    const int d = P.d;
+    const int d = dim_of(P, s);
     const double nrm = warp_norm(col, d, lane);
     const double sq = __dsqrt_rn(nrm);
     const double inv = __ddiv_rn(1.0, nrm);
     double2 *hat = slot_ptr(P, s.cur ^ 1, tr);
     double *adr_out = !P.o_adr ? nullptr
-                      : (P.keep_adr ? P.o_adr + ((size_t)dump * P.n + tr) * d : P.o_adr + (size_t)tr * d);
+                      : (P.keep_adr ? P.o_adr + ((size_t)dump * P.n + tr) * P.d : P.o_adr + (size_t)tr * P.d);
     for (int k = lane; k < d; k += 32) {
         const double2 v = col[k];
         hat[k] = make_double2(__ddiv_rn(v.x, sq), __ddiv_rn(v.y, sq));
@@ -186,7 +189,7 @@ __device__ void obs_prep(const Params &P, const TrajState &s, int tr, const doub
 // next group, or -1 when the trajectory is done for this call.
 __device__ int after_step(const Params &P, TrajState &s, int tr, const double2 *col, int lane)
 {
-    const int a = advance(s, P.dt, P.nb, P.brep);
+    const int a = advance(s, dt_of(P, s), P.nb, P.brep);
     if (a == 2) s.pc += 1;
     if (a >= 1 && P.subdump && (s.rk_sid & 1) == 0) {  // deep task: a sub-period ended
         obs_prep(P, s, tr, col, lane, P.dump_base + s.di, 0);
@@ -252,8 +255,8 @@ __device__ int rk_after_step(const Params &P, TrajState &s, int tr, const double
 __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, int lane, int idx,
                           double w_idx, int *err)
 {
-    const int d = P.d;
-    const double q = __dsqrt_rn(__ddiv_rn(w_idx, P.g[idx]));
+    const int d = dim_of(P, s);
+    const double q = __dsqrt_rn(__ddiv_rn(w_idx, rate_of(P, s, idx)));
     double2 *dst = slot_ptr(P, s.cur ^ 1, tr);
     for (int k = lane; k < d; k += 32) {
         const double2 v = col[k];
@@ -272,7 +275,7 @@ __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, i
         return rk_begin(s, s.rk_end, nrm, 0);
     }
     s.phase = PH_STEP;
-    s.t = __dadd_rn(s.t, P.dt[P.deep - 1]);
+    s.t = __dadd_rn(s.t, dt_of(P, s)[P.deep - 1]);
     return after_step(P, s, tr, col, lane);
 }
 
@@ -281,7 +284,7 @@ __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, i
 // trajectory's next micro-step, or -1 (done, paused or failed); the caller appends it.
 __device__ int column_epilogue(const Params &P, double2 *col, int tr, const TrajState &s_in, int lane)
 {
-    const int d = P.d;
+    const int d = dim_of(P, s_in);
     TrajState s = s_in;
     int g2 = -1;
     int err = 0;
@@ -296,7 +299,7 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
             err = ERR_NORM;
             break;
         }
-        const double dt = P.dt[s.lvl];
+        const double dt = dt_of(P, s)[s.lvl];
         if (nrm > s.eta) {  // not crossed: accept psi' (qj_proc.cpp:317, 335)
             double2 *dst = slot_ptr(P, s.cur ^ 1, tr);
             for (int k = lane; k < d; k += 32) dst[k] = col[k];
@@ -341,7 +344,7 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
 
     case PH_REC_W: {  // gnorms[i] = norm_square(L_i psi_hat) * g[i]  (experiment.cpp:1301-1322)
         double w = warp_norm(col, d, lane);
-        w = __dmul_rn(w, P.g[s.sub]);
+        w = __dmul_rn(w, rate_of(P, s, s.sub));
         if (lane == 0) P.gn[(size_t)tr * P.nd + s.sub] = w;
         s.tmpw = __dadd_rn(s.tmpw, w);
         if (s.sub + 1 < P.nd) {
@@ -532,26 +535,26 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
         P.st[tr] = s;
     }
     __syncwarp();
-    return g2;
+    return g2 >= 0 ? P.e_g0[s.ens] + g2 : -1;  // local group -> the ensemble's bucket
 }
 
 // Appends trajectories trs[c] to their next buckets g2s[c] (c < ncol, -1 skips) with one global
-// atomic per bucket: ranks and counts in shared memory, one reservation per bucket, then the
-// list writes.  Block-wide (contains barriers).
-__device__ void enqueue_batch(const Params &P, int *cnt_next, int *list_next, const int *trs, const int *g2s, int ncol,
-                              int *s_gcnt, int *s_gbase, int *s_rank)
+// atomic per distinct bucket of each 32 columns: warp w takes columns 32w .. 32w + 31, lanes
+// with the same bucket find each other with __match_any_sync, the lowest reserves the run and
+// the others take consecutive slots in lane order.  Independent of the number of groups.
+__device__ void enqueue_batch(const Params &P, int *cnt_next, int *list_next, const int *trs, const int *g2s, int ncol)
 {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int i = tid; i < P.G; i += nt) s_gcnt[i] = 0;
-    __syncthreads();
-    for (int c = tid; c < ncol; c += nt)
-        if (g2s[c] >= 0) s_rank[c] = atomicAdd(&s_gcnt[g2s[c]], 1);
-    __syncthreads();
-    for (int i = tid; i < P.G; i += nt)
-        if (s_gcnt[i]) s_gbase[i] = atomicAdd(&cnt_next[i], s_gcnt[i]);
-    __syncthreads();
-    for (int c = tid; c < ncol; c += nt)
-        if (g2s[c] >= 0) list_next[(size_t)g2s[c] * P.n + s_gbase[g2s[c]] + s_rank[c]] = trs[c];
+    const int lane = threadIdx.x & 31;
+    for (int c0 = (threadIdx.x >> 5) * 32; c0 < ncol; c0 += blockDim.x) {
+        const int c = c0 + lane;
+        const int g = (c < ncol) ? g2s[c] : -1;
+        const unsigned m = __match_any_sync(0xffffffffu, g);
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (g >= 0 && lane == leader) base = atomicAdd(&cnt_next[g], __popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (g >= 0) list_next[P.g_loff[g] + base + __popc(m & ((1u << lane) - 1u))] = trs[c];
+    }
 }
 
 // Copies a 96-byte trajectory record with 16-byte accesses.
@@ -593,9 +596,8 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
 template <int NRB, int WPC>
 __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, double2 *Us, uint64_t *bar,
                                           int *released, uint32_t &phase, int d, int kp, int KB, int RB, int MD,
-                                          int warp, int lane, int tid)
+                                          int S16, int warp, int lane, int tid)
 {
-    const int S16 = MD + 1;
     const int g = lane >> 2, t = lane & 3;
     // warp w runs on scheduler w % 4; rotating the row-block index by column block gives
     // each scheduler the same number of row blocks
@@ -676,20 +678,95 @@ __device__ __forceinline__ int subtile_cols(int m, int NC)
     return min(m, NC);
 }
 
-__device__ __forceinline__ int subtile_cost(int m, bool heavy_epilogue, int NC)
+__device__ __forceinline__ int subtile_cost(int m, int NC, int u_epi, int u_mma)
 {
     int c = 0;
     while (m > 0) {
         const int s = subtile_cols(m, NC);
         const int cb = (s + 7) / 8;
-        c += 2 + 6 * ((cb == 3) ? 4 : cb) + (heavy_epilogue ? 3 : 0);
+        c += u_epi + u_mma * ((cb == 3) ? 4 : cb);
         m -= s;
     }
     return c;
 }
 
-// Column position of cost offset k (monotone in k).
-__device__ __forceinline__ int cost_to_column(const int *cstart, const int *kc, const int *cnt, int G, long long k)
+// Estimated cost of group g's bucket of m columns, in units of ~5k cycles at d = 201: per
+// sub-tile 2 (gather, epilogue; 3 more for the jump-operator and observable buckets, whose
+// epilogues renormalise, draw and reduce), per active 8-column block 6 (MMA loop), scaled to
+// the group's dimension (epilogue ~ d, MMA ~ row blocks x k rows).
+__device__ __forceinline__ int group_cost(const Params &P, int g, int m)
+{
+    if (m == 0) return 0;
+    const int e = P.g_ens[g], d = P.e_d[e];
+    const bool heavy = g - P.e_g0[e] >= P.gL0;
+    const int u_epi = max(1, ((heavy ? 5 : 2) * d + 100) / 201);
+    const int u_mma = max(1, (((d + 7) >> 3) * ((d + 1) & ~1) + 437) / 875);
+    return subtile_cost(m, P.nc, u_epi, u_mma);
+}
+
+// Plan of a micro-step from its bucket sizes cnt[G]: bucket starts plan[0..G] and cost prefix
+// plan[G+1..2G+1].  Block-wide (any multiple of 32 threads); reads cnt past L1 (its atomics
+// were made by other CTAs).
+__device__ void plan_scan(const Params &P, const int *cnt)
+{
+    __shared__ int w_c[32], w_k[32];
+    const int G = P.G, nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (G + nt - 1) / nt;
+    const int g0 = min(G, tid * per), g1 = min(G, g0 + per);
+    int c = 0, k = 0;
+    for (int g = g0; g < g1; g++) {
+        const int m = __ldcg(cnt + g);
+        c += m;
+        k += group_cost(P, g, m);
+    }
+    int ic = c, ik = k;  // inclusive warp scans
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int yc = __shfl_up_sync(0xffffffffu, ic, off), yk = __shfl_up_sync(0xffffffffu, ik, off);
+        if (lane >= off) {
+            ic += yc;
+            ik += yk;
+        }
+    }
+    if (lane == 31) {
+        w_c[warp] = ic;
+        w_k[warp] = ik;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = nt >> 5;
+        int vc = lane < nw ? w_c[lane] : 0, vk = lane < nw ? w_k[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int yc = __shfl_up_sync(0xffffffffu, vc, off), yk = __shfl_up_sync(0xffffffffu, vk, off);
+            if (lane >= off) {
+                vc += yc;
+                vk += yk;
+            }
+        }
+        if (lane < nw) {
+            w_c[lane] = vc;  // inclusive totals through warp `lane`
+            w_k[lane] = vk;
+        }
+    }
+    __syncthreads();
+    int cs = ic - c + (warp ? w_c[warp - 1] : 0), ks = ik - k + (warp ? w_k[warp - 1] : 0);
+    for (int g = g0; g < g1; g++) {
+        const int m = __ldcg(cnt + g);
+        P.plan[g] = cs;
+        P.plan[G + 1 + g] = ks;
+        cs += m;
+        ks += group_cost(P, g, m);
+    }
+    if (tid == nt - 1) {
+        P.plan[G] = cs;
+        P.plan[2 * G + 1] = ks;
+    }
+    __syncthreads();
+}
+
+// Column position of cost offset k (monotone in k) in a plan.
+__device__ __forceinline__ int cost_to_column(const int *cstart, const int *kc, int G, long long k)
 {
     if (k >= kc[G]) return cstart[G];
     int lo = 0, hi = G;
@@ -698,10 +775,11 @@ __device__ __forceinline__ int cost_to_column(const int *cstart, const int *kc, 
         if (kc[mid] <= k) lo = mid;
         else hi = mid;
     }
+    const int cnt = cstart[lo + 1] - cstart[lo];
     const int cost = kc[lo + 1] - kc[lo];
     if (cost <= 0) return cstart[lo];
-    const long long off = (k - kc[lo]) * (long long)cnt[lo] / cost;
-    const int col = (int)min((long long)cnt[lo], ((off + 4) / 8) * 8);
+    const long long off = (k - kc[lo]) * (long long)cnt / cost;
+    const int col = (int)min((long long)cnt, ((off + 4) / 8) * 8);
     return cstart[lo] + col;
 }
 
@@ -716,53 +794,37 @@ template <int NRB, int CBMAX>
 __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int MD = P.MD;          // 8 * RB padded rows
-    const int RB = MD / 8;
-    const int S16 = MD + 1;       // odd column stride: conflict-free column reads
-    const int kp = (P.d + 1) & ~1;  // k rows padded to pairs (the matrices carry a zero row)
+    const int S16 = P.MD + 1;     // odd column stride: conflict-free column reads
     const int KB = P.kb;           // k rows per propagator slab
     double2 *Bt = reinterpret_cast<double2 *>(smem);
     double2 *Us = Bt + P.nc * S16;
     __shared__ __align__(8) uint64_t bar[kStages + 1];
     __shared__ int released[kStages];
-    __shared__ int s_cstart[kMaxGroups + 1];
-    __shared__ int s_kc[kMaxGroups + 1];
     __shared__ int s_tr[kNC];
     __shared__ long long s_src[kNC];
     __shared__ __align__(16) TrajState s_st[kNC];
-    __shared__ int s_g2[kNC], s_rank[kNC], s_gcnt[kMaxGroups], s_gbase[kMaxGroups];
+    __shared__ int s_g2[kNC];
+    __shared__ int s_last;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int G = P.G, n = P.n, d = P.d;
-    __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
+    const int G = P.G, n = P.n;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
-    const int *list_cur = P.lists + (size_t)(s & 1) * G * n;
-    int *list_next = P.lists + (size_t)((s + 1) & 1) * G * n;
+    const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
+    int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
+    const int *cstart = P.plan, *kc = P.plan + G + 1;  // this step's plan
 
-    for (int i = tid; i < G; i += kThreads) cnt_cur[i] = P.cnt[(s % 3) * G + i];
     if (blockIdx.x == 0)
         for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
-    __syncthreads();
     if (tid == 0) {
-        int acc = 0, kacc = 0;
-        for (int g = 0; g < G; g++) {
-            s_cstart[g] = acc;
-            s_kc[g] = kacc;
-            acc += cnt_cur[g];
-            kacc += subtile_cost(cnt_cur[g], g >= P.gL0, P.nc);
-        }
-        s_cstart[G] = acc;
-        s_kc[G] = kacc;
         for (int q = 0; q <= kStages; q++) mbar_init(&bar[q], 1);
         for (int q = 0; q < kStages; q++) released[q] = 0;
     }
     __syncthreads();
     // equal shares of the estimated cost, mapped back to column positions (8-column aligned
     // inside each bucket): buckets that split into many narrow sub-tiles get shorter ranges
-    const long long K = s_kc[G];
-    const int c_lo = cost_to_column(s_cstart, s_kc, cnt_cur, G, K * blockIdx.x / gridDim.x);
-    const int c_hi = cost_to_column(s_cstart, s_kc, cnt_cur, G, K * (blockIdx.x + 1) / gridDim.x);
-    const int nslab = (kp + KB - 1) / KB;
+    const long long K = kc[G];
+    const int c_lo = cost_to_column(cstart, kc, G, K * blockIdx.x / gridDim.x);
+    const int c_hi = cost_to_column(cstart, kc, G, K * (blockIdx.x + 1) / gridDim.x);
     uint32_t phase = 0;
     long long work = 0;
     long long tr_setup = 0, tr_loop = 0, tr_epi = 0, tr_sub = 0, tr_cb = 0;
@@ -773,50 +835,54 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
         int lo = 0, hi = G;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (s_cstart[mid] <= pos) lo = mid;
+            if (cstart[mid] <= pos) lo = mid;
             else hi = mid;
         }
         const int g = lo;
-        const int idx = pos - s_cstart[g];
+        const int idx = pos - cstart[g];
+        // the group's matrix: its ensemble's dimension, padded rows and k rows
+        const int dg = P.e_d[P.g_ens[g]];
+        const int MD = 8 * ((dg + 7) / 8), RB = MD / 8, kp = (dg + 1) & ~1;
+        const int nslab = (kp + KB - 1) / KB;
         // piece of this group left in the range, cut so that no sub-tile has 3 column blocks
-        const int m = min(c_hi - pos, cnt_cur[g] - idx);
+        const int m = min(c_hi - pos, cstart[g + 1] - pos);
         const int ncol = subtile_cols(m, P.nc);
         const int ncb = (ncol + 7) / 8;
         if (tid < kNC) {
             if (tid < ncol) {
-                const int tr = list_cur[(size_t)g * n + idx + tid];
+                const int tr = list_cur[P.g_loff[g] + idx + tid];
                 load_state(&s_st[tid], &P.st[tr]);
                 const int slot = src_slot(s_st[tid].phase, s_st[tid].cur, s_st[tid].rk_stage);
                 s_tr[tid] = tr;
-                s_src[tid] = ((long long)slot * n + tr) * MD;
+                s_src[tid] = ((long long)slot * n + tr) * P.MD;
             } else {
                 s_tr[tid] = -1;
             }
         }
         __syncthreads();
-        const double2 *mat = P.mats + (size_t)g * kp * MD;
+        const double2 *mat = P.mats + P.g_off[g];
         if (tid == 0) {
             fence_proxy_async();
             mbar_expect_tx(&bar[kStages], (uint32_t)(ncol * kp * 16));
             for (int c = 0; c < ncol; c++) bulk_g2s(Bt + c * S16, P.psi + s_src[c], (uint32_t)(kp * 16), &bar[kStages]);
             for (int q = 0; q < kStages && q < nslab; q++) {
-                const int kc = min(KB, kp - q * KB);
-                mbar_expect_tx(&bar[q], (uint32_t)(kc * MD * 16));
-                bulk_g2s(Us + q * KB * MD, mat + (size_t)q * KB * MD, (uint32_t)(kc * MD * 16), &bar[q]);
+                const int kcq = min(KB, kp - q * KB);
+                mbar_expect_tx(&bar[q], (uint32_t)(kcq * MD * 16));
+                bulk_g2s(Us + q * KB * MD, mat + (size_t)q * KB * MD, (uint32_t)(kcq * MD * 16), &bar[q]);
             }
         }
         const long long t1 = clock64();
         bool ok = false;
         constexpr int W1 = 16 / CBMAX;  // warps per column block of the widest sub-tile
         if (ncb == 1) {
-            ok = tile_dmma<(NRB * W1 + 15) / 16, 16>(mat, Bt, Us, bar, released, phase, d, kp, KB, RB, MD, warp,
-                                                     lane, tid);
+            ok = tile_dmma<(NRB * W1 + 15) / 16, 16>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16,
+                                                     warp, lane, tid);
         } else if constexpr (CBMAX >= 2) {
             if (ncb == 2) {
-                ok = tile_dmma<(NRB * W1 + 7) / 8, 8>(mat, Bt, Us, bar, released, phase, d, kp, KB, RB, MD, warp,
-                                                      lane, tid);
+                ok = tile_dmma<(NRB * W1 + 7) / 8, 8>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16,
+                                                      warp, lane, tid);
             } else if constexpr (CBMAX == 4) {
-                ok = tile_dmma<NRB, 4>(mat, Bt, Us, bar, released, phase, d, kp, KB, RB, MD, warp, lane, tid);
+                ok = tile_dmma<NRB, 4>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16, warp, lane, tid);
             }
         }
         if (!__syncthreads_and(ok ? 1 : 0)) {  // a bounded wait gave up: report and stop
@@ -824,7 +890,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
                 atomicAdd(&P.ctrl[4], 1);
                 report_error(P, -1, ERR_TIMEOUT);
             }
-            return;
+            break;
         }
         const long long t2 = clock64();
         for (int c = warp; c < ncol; c += kThreads / 32) {
@@ -832,7 +898,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             if (lane == 0) s_g2[c] = g2;
         }
         __syncthreads();
-        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, ncol, s_gcnt, s_gbase, s_rank);
+        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, ncol);
         work += ncol;
         pos += ncol;
         fence_proxy_async();
@@ -856,6 +922,24 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
         t[6] += tr_cb;
         t[7] += work;
     }
+    // the last CTA to finish plans the next micro-step from the buckets all CTAs filled
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(P.plan_sync, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        plan_scan(P, cnt_next);
+        if (tid == 0) *P.plan_sync = 0u;
+    }
+}
+
+// Plan of step 0 after a host-side enqueue (schedule, observe, resume): one block.
+__global__ void __launch_bounds__(1024) plan_kernel(const Params P)
+{
+    plan_scan(P, P.cnt);
 }
 
 // Bucket trajectories for step 0 of a call.  mode 0: start of a run of P.target periods;
@@ -896,14 +980,14 @@ __global__ void observe_kernel(const Params P, int dump, int is_start)
     TrajState s = P.st[tr];
     if (s.phase == PH_ERROR) return;
     const double2 *src = slot_ptr(P, s.cur, tr);
-    for (int k = lane; k < P.d; k += 32) col[k] = src[k];
+    for (int k = lane; k < dim_of(P, s); k += 32) col[k] = src[k];
     __syncwarp();
     obs_prep(P, s, tr, col, lane, dump, is_start);
     if (lane == 0) {
         s.pc = 0;
         s.di = 0;
         s.phase = PH_OBS_E;
-        enqueue(P, P.cnt, P.lists, P.gHE, tr);
+        enqueue(P, P.cnt, P.lists, P.e_g0[s.ens] + P.gHE, tr);
         P.st[tr] = s;
     }
 }
@@ -999,7 +1083,17 @@ __global__ void init_state_kernel(const Params P)
     s.rk_stage = 0;
     s.rk_part = 0;
     s.rk_ctx = 0;
-    s.rk_pad[0] = s.rk_pad[1] = 0;
+    int lo = 0, hi = P.E;  // ensemble e with e_tr0[e] <= tr < e_tr0[e + 1]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (P.e_tr0[mid] <= tr) lo = mid;
+        else hi = mid;
+    }
+    s.ens = lo;
+    s.rk_pad = 0;
+    // rows past the ensemble's dimension stay zero (they meet the zero rows of its matrices)
+    double2 *psi0 = P.psi + (size_t)tr * P.MD;
+    for (int k = P.e_d[lo]; k < P.MD; k++) psi0[k] = make_double2(0.0, 0.0);
     P.st[tr] = s;
 }
 
@@ -1125,10 +1219,18 @@ bool pick_step_tiles(int MD, size_t budget, int *nc, int *kb)
     return false;
 }
 
+// The plain step kernel's first micro-step after a host-side enqueue needs its plan.
+static cudaError_t launch_plan(const Params &P, cudaStream_t st)
+{
+    if (P.split) return cudaGetLastError();
+    plan_kernel<<<1, 1024, 0, st>>>(P);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st)
 {
     schedule_kernel<<<(P.n + 255) / 256, 256, 0, st>>>(P, mode);
-    return cudaGetLastError();
+    return launch_plan(P, st);
 }
 
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st)
@@ -1142,7 +1244,7 @@ cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t
         attr_set = true;
     }
     observe_kernel<<<(P.n + 7) / 8, 256, smem, st>>>(P, dump, is_start);
-    return cudaGetLastError();
+    return launch_plan(P, st);
 }
 
 cudaError_t launch_purity(const Params &P, double2 *hat, double2 *rho, double *out, cudaStream_t st)
@@ -1170,7 +1272,7 @@ __global__ void rk_schedule_kernel(const Params P)
     if (P.target > 0 && tr < P.n_active) {
         s.t = rk_step_time(P, s);
         rk_begin(s, P.rk_step, nrm, 0);
-        if (lane == 0) enqueue(P, P.cnt, P.lists, 0, tr);
+        if (lane == 0) enqueue(P, P.cnt, P.lists, P.e_g0[s.ens], tr);
     } else {
         s.phase = PH_DONE;
     }
@@ -1180,7 +1282,7 @@ __global__ void rk_schedule_kernel(const Params P)
 cudaError_t launch_rk_schedule(const Params &P, cudaStream_t st)
 {
     rk_schedule_kernel<<<(P.n + 7) / 8, 256, 0, st>>>(P);
-    return cudaGetLastError();
+    return launch_plan(P, st);
 }
 
 cudaError_t launch_init_state(const Params &P, cudaStream_t st)

@@ -144,13 +144,13 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     __shared__ int s_fail;
     __shared__ int s_rows;  // trajectories per tile in this micro-step
     __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
-    __shared__ int s_g2[kTileM], s_rank[kTileM], s_gcnt[kMaxGroups], s_gbase[kMaxGroups];
+    __shared__ int s_g2[kTileM];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int G = P.G, n = P.n, d = P.d;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
-    const int *list_cur = P.lists + (size_t)(s & 1) * G * n;
-    int *list_next = P.lists + (size_t)((s + 1) & 1) * G * n;
+    const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
+    int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
 
     for (int i = tid; i < G; i += kThreads) cnt_cur[i] = P.cnt[(s % 3) * G + i];
     if (blockIdx.x == 0)
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         const int rows = min(s_rows, cnt_cur[g] - base);
         if (tid < kTileM) {
             if (tid < rows) {
-                const int tr = list_cur[(size_t)g * n + base + tid];
+                const int tr = list_cur[P.g_loff[g] + base + tid];
                 const int slot = src_slot(P.st[tr].phase, P.st[tr].cur, P.st[tr].rk_stage);
                 s_tr[tid] = tr;
                 s_src[tid] = ((long long)slot * n + tr) * P.MD;
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             __syncthreads();
         }
         __syncthreads();
-        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, rows, s_gcnt, s_gbase, s_rank);
+        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, rows);
         work += rows;
         const long long t3 = clock64();
         tr_setup += t1 - t0;

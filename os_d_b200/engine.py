@@ -66,6 +66,44 @@ class Engine:
         self.h = h
         return self
 
+    @classmethod
+    def batch(cls, ensembles, deep=16, num_branches=2, record=0, rng_kind=0, rec_cap=1024, keep_adr=0, max_dumps=1,
+              device=0, deep_num_steps=0):
+        """Batched engine over ensembles of uneven dimension: each item is a dict with U
+        ([nb][deep][d][d]), L, g, HE, optional R, n_traj, T, seed, tr_base.  Trajectories are numbered
+        ensemble after ensemble (`ranges` gives each ensemble's slice); state rows have the largest d."""
+        self = cls.__new__(cls)
+        keep, arr = [], (N.QjxEnsemble * len(ensembles))()
+        nr = None
+        for i, e in enumerate(ensembles):
+            U = np.ascontiguousarray(e["U"], np.complex128)
+            d = U.shape[-1]
+            L = np.ascontiguousarray(e["L"], np.complex128).reshape(-1, d, d)
+            g = np.ascontiguousarray(np.atleast_1d(e.get("g", [1.0])), np.float64)
+            HE = np.ascontiguousarray(e["HE"], np.complex128)
+            R = e.get("R")
+            R = np.zeros((0, d, d), np.complex128) if R is None else np.ascontiguousarray(R, np.complex128).reshape(-1, d, d)
+            nr = R.shape[0] if nr is None else nr
+            keep += [U, L, g, HE, R]
+            arr[i] = N.QjxEnsemble(d=d, n_traj=int(e["n_traj"]), T=float(e.get("T", 2 * np.pi)),
+                                   seed=int(e.get("seed", 0)), tr_base=int(e.get("tr_base", 0)), U=N.dp(U), L=N.dp(L),
+                                   g=N.dp(g), HE=N.dp(HE), R=N.dp(R) if R.size else None)
+        cfg = N.QjxConfig()
+        cfg.deep, cfg.num_branches, cfg.num_diss, cfg.num_robs = deep, num_branches, keep[1].shape[0], nr
+        cfg.record, cfg.rng_kind, cfg.rec_cap, cfg.keep_adr = record, rng_kind, rec_cap, keep_adr
+        cfg.max_dumps, cfg.device, cfg.deep_num_steps, cfg.precision = max_dumps, device, deep_num_steps, 0
+        h = C.c_void_p()
+        N.check(N.lib().qjx_create_batch(C.byref(cfg), len(ensembles), arr, C.byref(h)), what="qjx_create_batch")
+        self.h = h
+        self.cfg = cfg
+        dims = [a.d for a in arr]
+        self.d, self.n, self.nr = max(dims), sum(a.n_traj for a in arr), nr
+        self.keep_adr = keep_adr
+        starts = np.cumsum([0] + [a.n_traj for a in arr])
+        self.ranges = [slice(int(starts[i]), int(starts[i + 1])) for i in range(len(arr))]
+        self.dims = dims
+        return self
+
     def _chk(self, st, what):
         N.check(st, self.h, what)
 
