@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision form")
     ap.add_argument("--no-fbasis", action="store_true", help="skip the f-basis Lindblad RK4 measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-ensembles measurement")
+    ap.add_argument("--batch-ensembles", type=int, default=32,
+                    help="ensembles of configuration 4 in the batched measurement (of 256)")
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
     ap.add_argument("--profile-target", default="plain", choices=["plain", "split", "fbasis"],
                     help="what --profile runs: one period of the plain or split form, or one f-basis period")
@@ -81,9 +84,10 @@ def model():
 
 
 def kernel_name(d):
-    """Instantiation of qjx::step_kernel<NRB> the library picks for dimension d."""
+    """Instantiation qjx::step_kernel<NRB, CBMAX> the library picks for dimension d <= 208
+    (32-column sub-tiles: CBMAX 4, NRB row blocks per warp at 4 warps per column block)."""
     rb = (d + 7) // 8
-    return f"qjx::step_kernel<{(rb + 3) // 4}>"
+    return f"qjx::step_kernel<{(rb + 3) // 4}, 4>"
 
 
 def start_states(n, d):
@@ -196,6 +200,93 @@ def fbasis_bench(args, local):
                                "sample": f"{csteps} RK4 steps of the same system ({dt:.2f} s), "
                                          f"oracle/fbasis_oracle.c, scaled to {steps} steps per period"}
     return out
+
+
+# ---------------------------------------------------------------- batched uneven ensembles (configuration 4)
+BATCH_SEED, BATCH_TRAJ = 11, 1000
+
+
+def batch_draw(count):
+    """Configuration 4's ensembles: N ~ U[50, 400], E0 ~ U[0, 2], g log-uniform in [0.01, 1], seed 11
+    (the first `count` of the 256 draws)."""
+    rng = np.random.default_rng(BATCH_SEED)
+    Ns = rng.integers(50, 401, size=256)
+    E0 = rng.uniform(0.0, 2.0, size=256)
+    g = 10.0 ** rng.uniform(-2.0, 0.0, size=256)
+    return [(int(Ns[i]), float(E0[i]), float(g[i])) for i in range(count)]
+
+
+def batched_bench(args, local):
+    """Chosen form 2: ensembles of uneven dimension advanced together by one engine (one set of
+    persistent micro-step launches, CUDA graphs of 6 micro-steps), one period per step, against
+    the same ensembles solved one after another by single-ensemble engines (serial plain FP64)."""
+    import torch
+
+    import os_d_b200 as q
+
+    ens = []
+    t_build = time.perf_counter()
+    for i, (N, E0, g) in enumerate(batch_draw(args.batch_ensembles)):
+        H, Hd, L, Ut = q.build_dimer(N, PRM["J"], PRM["U"], E0, PRM["A"], g, PRM["omega"], DEEP)
+        ens.append(dict(U=Ut, L=L, g=[1.0], HE=H + E0 * Hd, n_traj=BATCH_TRAJ, T=2.0 * np.pi / PRM["omega"],
+                        seed=BATCH_SEED, tr_base=i * BATCH_TRAJ))
+    t_build = time.perf_counter() - t_build
+    dims = [x["U"].shape[-1] for x in ens]
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def prepare(eng, n, rows):
+        psi = np.zeros((n, rows), np.complex128)
+        psi[:, 0] = 1.0
+        eng.set_states(psi)
+        eng.init_thresholds()
+        eng.reset_times()
+        return eng
+
+    B = prepare(q.Engine.batch(ens, deep=DEEP, device=local), BATCH_TRAJ * len(ens), max(dims))
+    for _ in range(args.warmup):
+        B.run_periods(1, is_obs=1)
+    ms, m0 = 0.0, B.stats()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        B.run_periods(1, is_obs=1)
+        ms += B.stats()["last_call_ms"]
+    m1 = B.stats()
+    B.close()
+    # serial: each ensemble alone for the same periods; its matvecs give the algorithmic flops
+    ms_serial, flops = 0.0, 0.0
+    for x in ens:
+        d = x["U"].shape[-1]
+        A = prepare(q.Engine(x["U"], x["L"], x["g"], x["HE"], None, x["T"], BATCH_TRAJ, seed=x["seed"],
+                             tr_base=x["tr_base"], device=local), BATCH_TRAJ, d)
+        for _ in range(args.warmup):
+            A.run_periods(1, is_obs=1)
+        a0 = A.stats()
+        for _ in range(args.steps):
+            A.run_periods(1, is_obs=1)
+            ms_serial += A.stats()["last_call_ms"]
+        flops += 8.0 * d * d * (A.stats()["matvecs"] - a0["matvecs"])
+        A.close()
+    n_tot = BATCH_TRAJ * len(ens)
+    kern_s = (m1["step_kernel_ms"] - m0["step_kernel_ms"]) * 1e-3
+    peak_ffma, peak_dmma = q.measure_fp64_peak(local)
+    peak = max(peak_ffma, peak_dmma)
+    return {
+        "workload": (f"{len(ens)} of configuration 4's 256 dimer ensembles (N ~ U[50,400], E0 ~ U[0,2], g log-uniform "
+                     f"[0.01,1], seed {BATCH_SEED}; dims {min(dims)}-{max(dims)}), {BATCH_TRAJ} trajectories each, "
+                     f"ex_deep {DEEP}, complex FP64, one period per step"),
+        "metric": METRIC, "value": n_tot * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+        "serial_single_ensemble_engines": {"value": n_tot * args.steps / (ms_serial * 1e-3),
+                                           "ms_per_step": ms_serial / args.steps},
+        "speedup_vs_serial": ms_serial / ms,
+        "roofline": {"bound": "tensor", "kernel": "qjx::step_kernel (per-(ensemble, matrix) buckets)",
+                     "achieved": flops / kern_s / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": flops / kern_s / 1e12 / peak,
+                     "flops": "8 d_e^2 per executed matvec, summed over the ensembles (matvecs counted by the "
+                              "same ensembles run alone, whose trajectories are bit-identical)"},
+        "gpu_launches": int(m1["launches"] - m0["launches"]),
+        "host_build_s": t_build,
+    }
 
 
 # ---------------------------------------------------------------- clocks
@@ -418,6 +509,8 @@ def run_ours(args):
                                "qjx_get_states per step"}
     if rank == 0 and not args.no_fbasis:
         line["fbasis"] = fbasis_bench(args, local)
+    if rank == 0 and world == 1 and not args.no_batch:  # a single-GPU measurement
+        line["batched"] = batched_bench(args, local)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 128 * threads  # about 15 s of CPU work

@@ -125,9 +125,11 @@ struct Params {
     // run_periods advances trajectories [0, n_active) only (the Lyapunov task's transient runs
     // the bases alone)
     int n_active;
-    // plain step kernel tiling (chosen from MD and the shared memory): columns per sub-tile
-    // (32, 16 or 8) and k rows per propagator slab
-    int nc, kb;
+    // plain step kernel tiling, per ensemble (chosen from its padded rows and the shared memory):
+    // columns per sub-tile (32, 16 or 8) and k rows per propagator slab; step_smem is the
+    // kernel's dynamic shared memory (the largest ensemble layout)
+    const int *e_nc, *e_kb;
+    int step_smem;
     // ensembles (a batched engine holds E ensembles of their own dimension, operators, seed and
     // period; an ordinary engine is the batch of one).  Trajectories [e_tr0[e], e_tr0[e+1]) form
     // ensemble e; its groups are e_g0[e] + the local group (branch * deep + level, gL0 + channel,

@@ -241,12 +241,19 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     const int MD = pick_layout(d, &rows_per_block);
     h->MD = MD;
     Params &P = h->P;
-    {  // plain step kernel tiling for the largest dimension
+    std::vector<int> e_nc(E), e_kb(E);
+    {  // plain step kernel tiling of every ensemble within the shared memory
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
         const size_t fixed = step_static_smem() + 1024;
-        if ((size_t)optin <= fixed || !pick_step_tiles(MD, (size_t)optin - fixed, &P.nc, &P.kb))
-            return bail(QJX_ERR_UNSUPPORTED);
+        if ((size_t)optin <= fixed) return bail(QJX_ERR_UNSUPPORTED);
+        size_t smem = 0;
+        for (int e = 0; e < E; e++) {
+            const int MDe = 8 * ((ens[e].d + 7) / 8);
+            if (!pick_step_tiles(MDe, (size_t)optin - fixed, &e_nc[e], &e_kb[e])) return bail(QJX_ERR_UNSUPPORTED);
+            smem = std::max(smem, step_smem_bytes(MDe, e_nc[e], e_kb[e]));
+        }
+        P.step_smem = (int)smem;
     }
     P.d = d;
     P.MD = MD;
@@ -318,6 +325,8 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     cudaMemcpy(mats, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
     P.mats = mats;
     P.e_d = upload(h, e_d);
+    P.e_nc = upload(h, e_nc);
+    P.e_kb = upload(h, e_kb);
     P.e_tr0 = upload(h, e_tr0);
     P.e_g0 = upload(h, e_g0);
     P.e_dt = upload(h, e_dt);
@@ -332,7 +341,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     P.g = P.e_rate;
     P.plan = (int *)dalloc(h, (size_t)(2 * G + 2) * sizeof(int));
     P.plan_sync = (unsigned int *)dalloc(h, sizeof(unsigned int));
-    if (!P.e_d || !P.e_tr0 || !P.e_g0 || !P.e_dt || !P.e_rate || !P.e_seed || !P.e_sbase || !P.g_off || !P.g_ens ||
+    if (!P.e_d || !P.e_nc || !P.e_kb || !P.e_tr0 || !P.e_g0 || !P.e_dt || !P.e_rate || !P.e_seed || !P.e_sbase || !P.g_off || !P.g_ens ||
         !P.g_loff || !P.plan || !P.plan_sync)
         return bail(QJX_ERR_OOM);
     cudaMemset(P.plan, 0, (size_t)(2 * G + 2) * sizeof(int));

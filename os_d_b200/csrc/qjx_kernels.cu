@@ -701,7 +701,7 @@ __device__ __forceinline__ int group_cost(const Params &P, int g, int m)
     const bool heavy = g - P.e_g0[e] >= P.gL0;
     const int u_epi = max(1, ((heavy ? 5 : 2) * d + 100) / 201);
     const int u_mma = max(1, (((d + 7) >> 3) * ((d + 1) & ~1) + 437) / 875);
-    return subtile_cost(m, P.nc, u_epi, u_mma);
+    return subtile_cost(m, P.e_nc[e], u_epi, u_mma);
 }
 
 // Plan of a micro-step from its bucket sizes cnt[G]: bucket starts plan[0..G] and cost prefix
@@ -788,16 +788,16 @@ __device__ __forceinline__ int cost_to_column(const int *cstart, const int *kc, 
 // into equal column ranges, one per persistent CTA; each range is processed as sub-tiles of
 // at most 32 columns of one matrix, and a sub-tile costs in proportion to its active 8-column
 // blocks (1, 2 or 4): the warps are spread over the row blocks of the active column blocks.
-// NRB: row blocks per warp when a sub-tile has its widest CBMAX column blocks (16 / CBMAX warps
-// per column block); CBMAX = P.nc / 8 (4 for d <= ~208, 2 up to 512, 1 up to 1024).
-template <int NRB, int CBMAX>
+// Each ensemble has its own sub-tile width (32, 16 or 8 columns) and slab height; the shared
+// memory holds the staged columns (stride MD + 1, odd: conflict-free column reads) followed by
+// the propagator slabs, laid out per sub-tile.  R4, R2, R1: row blocks per warp of the sub-tiles
+// with 4, 2 and 1 column blocks (4, 8 and 16 warps per column block), large enough for every
+// ensemble that uses them.
+template <int R4, int R2, int R1>
 __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int S16 = P.MD + 1;     // odd column stride: conflict-free column reads
-    const int KB = P.kb;           // k rows per propagator slab
     double2 *Bt = reinterpret_cast<double2 *>(smem);
-    double2 *Us = Bt + P.nc * S16;
     __shared__ __align__(8) uint64_t bar[kStages + 1];
     __shared__ int released[kStages];
     __shared__ int s_tr[kNC];
@@ -840,13 +840,16 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
         }
         const int g = lo;
         const int idx = pos - cstart[g];
-        // the group's matrix: its ensemble's dimension, padded rows and k rows
-        const int dg = P.e_d[P.g_ens[g]];
+        // the group's matrix: its ensemble's dimension, padded rows, k rows and tiling
+        const int eg = P.g_ens[g];
+        const int dg = P.e_d[eg];
         const int MD = 8 * ((dg + 7) / 8), RB = MD / 8, kp = (dg + 1) & ~1;
+        const int S16 = MD + 1, KB = P.e_kb[eg], NC = P.e_nc[eg];
+        double2 *Us = Bt + NC * S16;
         const int nslab = (kp + KB - 1) / KB;
         // piece of this group left in the range, cut so that no sub-tile has 3 column blocks
         const int m = min(c_hi - pos, cstart[g + 1] - pos);
-        const int ncol = subtile_cols(m, P.nc);
+        const int ncol = subtile_cols(m, NC);
         const int ncb = (ncol + 7) / 8;
         if (tid < kNC) {
             if (tid < ncol) {
@@ -872,19 +875,13 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
             }
         }
         const long long t1 = clock64();
-        bool ok = false;
-        constexpr int W1 = 16 / CBMAX;  // warps per column block of the widest sub-tile
-        if (ncb == 1) {
-            ok = tile_dmma<(NRB * W1 + 15) / 16, 16>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16,
-                                                     warp, lane, tid);
-        } else if constexpr (CBMAX >= 2) {
-            if (ncb == 2) {
-                ok = tile_dmma<(NRB * W1 + 7) / 8, 8>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16,
-                                                      warp, lane, tid);
-            } else if constexpr (CBMAX == 4) {
-                ok = tile_dmma<NRB, 4>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16, warp, lane, tid);
-            }
-        }
+        bool ok;
+        if (ncb == 1)
+            ok = tile_dmma<R1, 16>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16, warp, lane, tid);
+        else if (ncb == 2)
+            ok = tile_dmma<R2, 8>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16, warp, lane, tid);
+        else
+            ok = tile_dmma<R4, 4>(mat, Bt, Us, bar, released, phase, dg, kp, KB, RB, MD, S16, warp, lane, tid);
         if (!__syncthreads_and(ok ? 1 : 0)) {  // a bounded wait gave up: report and stop
             if (tid == 0) {
                 atomicAdd(&P.ctrl[4], 1);
@@ -1129,34 +1126,54 @@ __global__ void clear_records_kernel(const Params P)
 // ---------------------------------------------------------------- host-side launchers
 size_t step_smem_bytes(int MD, int nc, int kb);
 
-template <int NRB, int CBMAX>
+template <int R4, int R2, int R1>
 static cudaError_t launch_step_t(const Params &P, int s, int grid, cudaStream_t st)
 {
-    const size_t smem = step_smem_bytes(P.MD, P.nc, P.kb);
     static int attr_bytes = 0;
-    if (attr_bytes < (int)smem) {
+    if (attr_bytes < P.step_smem) {
         cudaError_t e =
-            cudaFuncSetAttribute(step_kernel<NRB, CBMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(step_kernel<R4, R2, R1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.step_smem);
         if (e != cudaSuccess) return e;
-        attr_bytes = (int)smem;
+        attr_bytes = P.step_smem;
     }
-    step_kernel<NRB, CBMAX><<<grid, kThreads, smem, st>>>(P, s);
+    step_kernel<R4, R2, R1><<<grid, kThreads, P.step_smem, st>>>(P, s);
     return cudaGetLastError();
 }
 
-template <int CBMAX>
-static cudaError_t launch_step_cb(const Params &P, int s, int grid, cudaStream_t st)
+cudaError_t launch_split_step(const Params &P, int s, int grid, cudaStream_t st);
+
+// Instantiation for the largest padded rows MD: up to 256 rows every sub-tile width may occur
+// (R4 = ceil(RB / 4)); up to 512 the 32-column sub-tiles belong to ensembles of at most 256 rows
+// (R4 = 8) and R2 = ceil(RB / 8); up to 1024 also R2 = 8 and R1 = ceil(RB / 16).
+cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st)
 {
-    const int RB = P.MD / 8, W1 = 16 / CBMAX;
-    switch ((RB + W1 - 1) / W1) {  // row blocks per warp at the widest sub-tile
-    case 1: return launch_step_t<1, CBMAX>(P, s, grid, st);
-    case 2: return launch_step_t<2, CBMAX>(P, s, grid, st);
-    case 3: return launch_step_t<3, CBMAX>(P, s, grid, st);
-    case 4: return launch_step_t<4, CBMAX>(P, s, grid, st);
-    case 5: return launch_step_t<5, CBMAX>(P, s, grid, st);
-    case 6: return launch_step_t<6, CBMAX>(P, s, grid, st);
-    case 7: return launch_step_t<7, CBMAX>(P, s, grid, st);
-    case 8: return launch_step_t<8, CBMAX>(P, s, grid, st);
+    if (P.split) return launch_split_step(P, s, grid, st);
+    const int RB = P.MD / 8;
+    if (RB <= 32) {
+        switch ((RB + 3) / 4) {
+        case 1: return launch_step_t<1, 1, 1>(P, s, grid, st);
+        case 2: return launch_step_t<2, 1, 1>(P, s, grid, st);
+        case 3: return launch_step_t<3, 2, 1>(P, s, grid, st);
+        case 4: return launch_step_t<4, 2, 1>(P, s, grid, st);
+        case 5: return launch_step_t<5, 3, 2>(P, s, grid, st);
+        case 6: return launch_step_t<6, 3, 2>(P, s, grid, st);
+        case 7: return launch_step_t<7, 4, 2>(P, s, grid, st);
+        default: return launch_step_t<8, 4, 2>(P, s, grid, st);
+        }
+    }
+    if (RB <= 64) {
+        switch ((RB + 7) / 8) {
+        case 5: return launch_step_t<8, 5, 3>(P, s, grid, st);
+        case 6: return launch_step_t<8, 6, 3>(P, s, grid, st);
+        case 7: return launch_step_t<8, 7, 4>(P, s, grid, st);
+        default: return launch_step_t<8, 8, 4>(P, s, grid, st);
+        }
+    }
+    switch ((RB + 15) / 16) {
+    case 5: return launch_step_t<8, 8, 5>(P, s, grid, st);
+    case 6: return launch_step_t<8, 8, 6>(P, s, grid, st);
+    case 7: return launch_step_t<8, 8, 7>(P, s, grid, st);
+    case 8: return launch_step_t<8, 8, 8>(P, s, grid, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1166,19 +1183,6 @@ int pick_layout(int d, int *rows_per_block)
 {
     *rows_per_block = 8;
     return 8 * ((d + 7) / 8);
-}
-
-cudaError_t launch_split_step(const Params &P, int s, int grid, cudaStream_t st);
-
-cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st)
-{
-    if (P.split) return launch_split_step(P, s, grid, st);
-    switch (P.nc) {
-    case 32: return launch_step_cb<4>(P, s, grid, st);
-    case 16: return launch_step_cb<2>(P, s, grid, st);
-    case 8: return launch_step_cb<1>(P, s, grid, st);
-    default: return cudaErrorInvalidValue;
-    }
 }
 
 // Shared memory of the step kernel: nc staged columns of MD + 1 (odd stride) and kStages
@@ -1192,7 +1196,7 @@ size_t step_smem_bytes(int MD, int nc, int kb)
 size_t step_static_smem()
 {
     cudaFuncAttributes a{};
-    if (cudaFuncGetAttributes(&a, step_kernel<1, 4>) != cudaSuccess) return 16384;
+    if (cudaFuncGetAttributes(&a, step_kernel<1, 1, 1>) != cudaSuccess) return 16384;
     return a.sharedSizeBytes;
 }
 
