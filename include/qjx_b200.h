@@ -134,6 +134,18 @@ typedef struct {
  * each ensemble's d).  Every trajectory is bit-identical to its run in an engine of its own.
  * The Lyapunov entry points, qjx_purity and the RK propagator take single-ensemble engines. */
 qjx_status qjx_create_batch(const qjx_config *cfg, int n_ens, const qjx_ensemble *ens, qjx_engine **out);
+/* Serving engine: n_slots resident ensemble slots, each with room for dimension <= d_cap and
+ * n_cap trajectories (slot s owns trajectories s * n_cap ...); all slots start free.  Run calls
+ * advance the loaded slots together (qjx_create_batch's launches); loading or releasing a slot
+ * between run calls leaves the others' states, streams and records untouched, so requests join
+ * and leave a running batch (continuous batching).  cfg as for qjx_create_batch. */
+qjx_status qjx_create_slots(const qjx_config *cfg, int n_slots, int d_cap, int n_cap, qjx_engine **out);
+/* Load an ensemble into a free slot: its operators into the slot's resident matrix region, its
+ * e->n_traj trajectories from psi ([n_traj][e->d] complex; NULL: |0>), fresh times, records and
+ * thresholds (its own Philox stream), then the slot runs with the next run call. */
+qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble *e, const double *psi);
+/* Stop advancing and observing a slot; its states stay readable until it is loaded again. */
+qjx_status qjx_slot_release(qjx_engine *h, int slot);
 void qjx_destroy(qjx_engine *h);
 const char *qjx_last_error(const qjx_engine *h);
 const char *qjx_status_string(qjx_status s);

@@ -21,7 +21,8 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_create_batch", "qjx_set_active", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
+    "qjx_random_observables", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
+    "qjx_set_active", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
@@ -95,6 +96,9 @@ def lib():
         L.qjx_set_trace.argtypes = [vp, C.c_int]
         L.qjx_set_active.argtypes = [vp, C.c_int]
         L.qjx_create_batch.argtypes = [C.POINTER(QjxConfig), C.c_int, C.POINTER(QjxEnsemble), C.POINTER(vp)]
+        L.qjx_create_slots.argtypes = [C.POINTER(QjxConfig), C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
+        L.qjx_slot_load.argtypes = [vp, C.c_int, C.POINTER(QjxEnsemble), c_double_p]
+        L.qjx_slot_release.argtypes = [vp, C.c_int]
         L.qjx_lpn_start.argtypes = [vp, C.POINTER(QjxLpnConfig)]
         L.qjx_lpn_period.argtypes = [vp, C.c_double, C.c_int]
         L.qjx_lpn_get.argtypes = [vp] + [c_double_p] * 6 + [c_int_p]

@@ -123,8 +123,10 @@ struct Params {
     // with subdump the observables are taken after every sub-period (two units)
     int brep, subdump;
     // run_periods advances trajectories [0, n_active) only (the Lyapunov task's transient runs
-    // the bases alone)
+    // the bases alone), and of those only the ones with active[tr] != 0 when `active` is set
+    // (the ensemble slots of a serving engine)
     int n_active;
+    const unsigned char *active;
     // plain step kernel tiling, per ensemble (chosen from its padded rows and the shared memory):
     // columns per sub-tile (32, 16 or 8) and k rows per propagator slab; step_smem is the
     // kernel's dynamic shared memory (the largest ensemble layout)

@@ -22,10 +22,10 @@ bool pick_step_tiles(int MD, size_t budget, int *nc, int *kb);
 size_t step_static_smem();
 cudaError_t launch_schedule(const Params &P, int mode, cudaStream_t st);
 cudaError_t launch_observe(const Params &P, int dump, int is_start, cudaStream_t st);
-cudaError_t launch_init_state(const Params &P, cudaStream_t st);
+cudaError_t launch_init_state(const Params &P, cudaStream_t st, int tr0 = 0, int tr1 = -1);
 cudaError_t launch_rk_schedule(const Params &P, cudaStream_t st);
 cudaError_t launch_purity(const Params &P, double2 *hat, double2 *rho, double *out, cudaStream_t st);
-cudaError_t launch_thresholds(const Params &P, cudaStream_t st);
+cudaError_t launch_thresholds(const Params &P, cudaStream_t st, int tr0 = 0, int tr1 = -1);
 cudaError_t launch_reset_times(const Params &P, cudaStream_t st);
 cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
 cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st);
@@ -63,6 +63,10 @@ struct qjx_engine {
     bool states_set = false;
     int period_base = 0;  // periods run since the last time reset (the RK propagator's period_id)
     int n_ens = 1;        // ensembles (qjx_create_batch)
+    // serving engines (qjx_create_slots): every ensemble is a slot with room for d_cap and n_cap
+    int slot_dcap = 0, slot_ncap = 0;
+    std::vector<int> slot_n;          // trajectories of the loaded ensemble (0: free)
+    unsigned char *d_active = nullptr;
     // Lyapunov task (allocated by the first qjx_lpn_start)
     LpnParams L{};
     bool lpn_alloc = false, lpn_started = false;
@@ -680,6 +684,118 @@ extern "C" qjx_status qjx_create_batch(const qjx_config *cfg, int n_ens, const q
         v[e] = EnsDesc{x.d, x.n_traj, x.T, x.seed, x.tr_base, x.U, x.L, x.g, x.HE, x.R};
     }
     return create_engine(cfg, v, 2, out);
+}
+
+extern "C" qjx_status qjx_create_slots(const qjx_config *cfg, int n_slots, int d_cap, int n_cap, qjx_engine **out)
+{
+    if (!cfg || !out || n_slots < 1 || d_cap < 2 || n_cap < 1) return QJX_ERR_INVALID_ARG;
+    if (cfg->precision != 0 || d_cap > kMaxMD) return QJX_ERR_UNSUPPORTED;
+    const qjx_config &c = *cfg;
+    // placeholder operators (zero) until a slot is loaded
+    const size_t dd2 = (size_t)2 * d_cap * d_cap;
+    std::vector<double> U(dd2 * c.num_branches * std::max(1, c.deep)), L(dd2 * std::max(1, c.num_diss)), HE(dd2),
+        R(dd2 * std::max(1, c.num_robs)), g(std::max(1, c.num_diss), 1.0);
+    std::vector<EnsDesc> v(n_slots, EnsDesc{d_cap, n_cap, 1.0, 0, 0, U.data(), L.data(), g.data(), HE.data(),
+                                            c.num_robs ? R.data() : nullptr});
+    qjx_status st = create_engine(cfg, v, 2, out);
+    if (st != QJX_OK) return st;
+    qjx_engine *h = *out;
+    h->slot_dcap = d_cap;
+    h->slot_ncap = n_cap;
+    h->slot_n.assign(n_slots, 0);
+    h->d_active = (unsigned char *)dalloc(h, (size_t)h->P.n);
+    if (!h->d_active) {
+        qjx_destroy(h);
+        *out = nullptr;
+        return QJX_ERR_OOM;
+    }
+    cudaMemset(h->d_active, 0, (size_t)h->P.n);
+    h->P.active = h->d_active;
+    h->states_set = true;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble *e, const double *psi)
+{
+    if (!h || !e) return QJX_ERR_INVALID_ARG;
+    if (!h->d_active || slot < 0 || slot >= h->n_ens) return fail(h, QJX_ERR_INVALID_ARG, "not a slot of a serving engine");
+    if (h->slot_n[slot]) return fail(h, QJX_ERR_STATE, "slot in use: release it first");
+    Params &P = h->P;
+    const int d = e->d, n = e->n_traj;
+    if (d < 2 || d > h->slot_dcap || n < 1 || n > h->slot_ncap || !(e->T > 0.0) || !e->U || !e->L || !e->g || !e->HE ||
+        (P.nr > 0 && !e->R))
+        return fail(h, QJX_ERR_INVALID_ARG, "ensemble does not fit the slot");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaStreamSynchronize(h->stream));
+    const int MDe = 8 * ((d + 7) / 8), kpe = (d + 1) & ~1;
+    int nc = 0, kb = 0;
+    if (!pick_step_tiles(MDe, (size_t)P.step_smem, &nc, &kb)) return fail(h, QJX_ERR_UNSUPPORTED, "no tiling");
+    // operators into the slot's resident matrix region
+    const int Ge = P.G / h->n_ens;
+    const size_t per = (size_t)kpe * MDe * 2, dd2 = (size_t)2 * d * d;
+    std::vector<double> host(per * Ge, 0.0);
+    for (int b = 0; b < P.nb; b++)
+        for (int l = 0; l < P.deep; l++)
+            pack_transposed(e->U + dd2 * ((size_t)b * P.deep + l), d, MDe, host.data() + per * (b * P.deep + l));
+    for (int i = 0; i < P.nd; i++) pack_transposed(e->L + dd2 * i, d, MDe, host.data() + per * (P.gL0 + i));
+    pack_transposed(e->HE, d, MDe, host.data() + per * P.gHE);
+    for (int i = 0; i < P.nr; i++) pack_transposed(e->R + dd2 * i, d, MDe, host.data() + per * (P.gR0 + i));
+    std::vector<long long> goff(Ge);
+    CK(cudaMemcpy(goff.data(), P.g_off + (size_t)slot * Ge, Ge * sizeof(long long), cudaMemcpyDeviceToHost));
+    for (int l = 0; l < Ge; l++)
+        CK(cudaMemcpy(const_cast<double2 *>(P.mats) + goff[l], host.data() + per * l, per * sizeof(double),
+                      cudaMemcpyHostToDevice));
+    // the slot's ensemble table entries
+    std::vector<double> dts(P.deep);
+    double dt = (h->cfg.deep_num_steps > 0 ? 0.5 * e->T / double(h->cfg.deep_num_steps) : e->T) * 0.5;
+    for (int l = 0; l < P.deep; l++) {
+        dt *= 0.5;
+        dts[l] = dt;
+    }
+    const unsigned long long seed = e->seed;
+    const long long sbase = e->tr_base;
+    CK(cudaMemcpy(const_cast<int *>(P.e_d) + slot, &d, sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<int *>(P.e_nc) + slot, &nc, sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<int *>(P.e_kb) + slot, &kb, sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<double *>(P.e_dt) + (size_t)slot * P.deep, dts.data(), P.deep * sizeof(double),
+                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<double *>(P.e_rate) + (size_t)slot * P.nd, e->g, P.nd * sizeof(double),
+                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<unsigned long long *>(P.e_seed) + slot, &seed, sizeof(seed), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<long long *>(P.e_sbase) + slot, &sbase, sizeof(sbase), cudaMemcpyHostToDevice));
+    // states: psi (or |0>) in rows of the largest dimension, fresh records, thresholds
+    const int t0 = slot * h->slot_ncap;
+    CK(cudaMemset(P.psi + (size_t)t0 * P.MD, 0, (size_t)h->slot_ncap * P.MD * sizeof(double2)));
+    CK(cudaMemset(P.psi + ((size_t)P.n + t0) * P.MD, 0, (size_t)h->slot_ncap * P.MD * sizeof(double2)));
+    if (psi) {
+        CK(cudaMemcpy2D(P.psi + (size_t)t0 * P.MD, (size_t)P.MD * sizeof(double2), psi, (size_t)d * sizeof(double2),
+                        (size_t)d * sizeof(double2), n, cudaMemcpyHostToDevice));
+    } else {
+        const double2 one = make_double2(1.0, 0.0);
+        for (int i = 0; i < n; i++) CK(cudaMemcpy(P.psi + ((size_t)t0 + i) * P.MD, &one, sizeof(one), cudaMemcpyHostToDevice));
+    }
+    CK(launch_init_state(P, h->stream, t0, t0 + h->slot_ncap));
+    CK(launch_thresholds(P, h->stream, t0, t0 + n));
+    CK(cudaMemsetAsync(h->d_active + t0, 1, (size_t)n, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int i = t0; i < t0 + h->slot_ncap; i++) {
+        h->jt[i].clear();
+        h->jn[i].clear();
+        h->je[i].clear();
+        h->jtype[i].clear();
+    }
+    h->slot_n[slot] = n;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_slot_release(qjx_engine *h, int slot)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (!h->d_active || slot < 0 || slot >= h->n_ens) return fail(h, QJX_ERR_INVALID_ARG, "not a slot of a serving engine");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaMemset(h->d_active + (size_t)slot * h->slot_ncap, 0, (size_t)h->slot_ncap));
+    h->slot_n[slot] = 0;
+    return QJX_OK;
 }
 
 extern "C" qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, const double *H_drv, double E0,

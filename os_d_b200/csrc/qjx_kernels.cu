@@ -36,6 +36,12 @@ __device__ __forceinline__ double2 *slot_ptr(const Params &P, int slot, int tr)
     return P.psi + ((size_t)slot * P.n + tr) * P.MD;
 }
 
+// Whether run calls advance trajectory tr.
+__device__ __forceinline__ bool runs(const Params &P, int tr)
+{
+    return tr < P.n_active && (!P.active || P.active[tr]);
+}
+
 // Bucket (global group) of a trajectory's next matvec, or -1.
 __device__ __forceinline__ int group_of(const Params &P, const TrajState &s)
 {
@@ -955,7 +961,7 @@ __global__ void schedule_kernel(const Params P, int mode)
         s.mask = 0;
         s.rk_sid = 0;
         s.paused = 0;
-        s.phase = (P.target > 0 && tr < P.n_active) ? PH_STEP : PH_DONE;
+        s.phase = (P.target > 0 && runs(P, tr)) ? PH_STEP : PH_DONE;
     } else {
         if (!s.paused) return;
         s.paused = 0;
@@ -972,7 +978,7 @@ __global__ void observe_kernel(const Params P, int dump, int is_start)
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tr = blockIdx.x * (blockDim.x / 32) + warp;
-    if (tr >= P.n) return;
+    if (tr >= P.n || (P.active && !P.active[tr])) return;
     double2 *col = reinterpret_cast<double2 *>(smem) + (size_t)warp * P.MD;
     TrajState s = P.st[tr];
     if (s.phase == PH_ERROR) return;
@@ -1050,10 +1056,10 @@ __global__ void purity_kernel(const double2 *rho, int dd, double *out)
     if (threadIdx.x == 0) *out = s;
 }
 
-__global__ void init_state_kernel(const Params P)
+__global__ void init_state_kernel(const Params P, int tr0, int tr1)
 {
-    const int tr = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tr >= P.n) return;
+    const int tr = tr0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (tr >= tr1) return;
     TrajState s;
     s.t = 0.0;
     s.eta = 0.0;
@@ -1095,10 +1101,10 @@ __global__ void init_state_kernel(const Params P)
 }
 
 // eta_0 draw of trans_process_single (experiment.cpp:3260-3265)
-__global__ void thresholds_kernel(const Params P)
+__global__ void thresholds_kernel(const Params P, int tr0, int tr1)
 {
-    const int tr = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tr >= P.n) return;
+    const int tr = tr0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (tr >= tr1) return;
     TrajState s = P.st[tr];
     int err = 0;
     s.eta = 0.0;
@@ -1273,7 +1279,7 @@ __global__ void rk_schedule_kernel(const Params P)
     s.di = 0;
     s.paused = 0;
     s.rk_sid = 0;
-    if (P.target > 0 && tr < P.n_active) {
+    if (P.target > 0 && runs(P, tr)) {
         s.t = rk_step_time(P, s);
         rk_begin(s, P.rk_step, nrm, 0);
         if (lane == 0) enqueue(P, P.cnt, P.lists, P.e_g0[s.ens], tr);
@@ -1289,15 +1295,19 @@ cudaError_t launch_rk_schedule(const Params &P, cudaStream_t st)
     return launch_plan(P, st);
 }
 
-cudaError_t launch_init_state(const Params &P, cudaStream_t st)
+cudaError_t launch_init_state(const Params &P, cudaStream_t st, int tr0, int tr1)
 {
-    init_state_kernel<<<(P.n + 255) / 256, 256, 0, st>>>(P);
+    if (tr1 < 0) tr1 = P.n;
+    if (tr1 <= tr0) return cudaSuccess;
+    init_state_kernel<<<(tr1 - tr0 + 255) / 256, 256, 0, st>>>(P, tr0, tr1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_thresholds(const Params &P, cudaStream_t st)
+cudaError_t launch_thresholds(const Params &P, cudaStream_t st, int tr0, int tr1)
 {
-    thresholds_kernel<<<(P.n + 255) / 256, 256, 0, st>>>(P);
+    if (tr1 < 0) tr1 = P.n;
+    if (tr1 <= tr0) return cudaSuccess;
+    thresholds_kernel<<<(tr1 - tr0 + 255) / 256, 256, 0, st>>>(P, tr0, tr1);
     return cudaGetLastError();
 }
 

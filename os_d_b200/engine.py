@@ -104,6 +104,47 @@ class Engine:
         self.dims = dims
         return self
 
+    @staticmethod
+    def _ensemble_struct(e, keep):
+        U = np.ascontiguousarray(e["U"], np.complex128)
+        d = U.shape[-1]
+        L = np.ascontiguousarray(e["L"], np.complex128).reshape(-1, d, d)
+        g = np.ascontiguousarray(np.atleast_1d(e.get("g", [1.0])), np.float64)
+        HE = np.ascontiguousarray(e["HE"], np.complex128)
+        R = e.get("R")
+        R = np.zeros((0, d, d), np.complex128) if R is None else np.ascontiguousarray(R, np.complex128).reshape(-1, d, d)
+        keep += [U, L, g, HE, R]
+        return N.QjxEnsemble(d=d, n_traj=int(e["n_traj"]), T=float(e.get("T", 2 * np.pi)), seed=int(e.get("seed", 0)),
+                             tr_base=int(e.get("tr_base", 0)), U=N.dp(U), L=N.dp(L), g=N.dp(g), HE=N.dp(HE),
+                             R=N.dp(R) if R.size else None)
+
+    @classmethod
+    def slots(cls, n_slots, d_cap, n_cap, deep=16, num_branches=2, num_diss=1, num_robs=0, record=0, rng_kind=0,
+              rec_cap=1024, keep_adr=0, max_dumps=1, device=0):
+        """Serving engine: n_slots resident ensemble slots (dimension <= d_cap, n_cap trajectories
+        each; slot s owns trajectories s * n_cap ...), loaded and released between run calls."""
+        self = cls.__new__(cls)
+        cfg = N.QjxConfig()
+        cfg.deep, cfg.num_branches, cfg.num_diss, cfg.num_robs = deep, num_branches, num_diss, num_robs
+        cfg.record, cfg.rng_kind, cfg.rec_cap, cfg.keep_adr = record, rng_kind, rec_cap, keep_adr
+        cfg.max_dumps, cfg.device, cfg.precision = max_dumps, device, 0
+        h = C.c_void_p()
+        N.check(N.lib().qjx_create_slots(C.byref(cfg), n_slots, d_cap, n_cap, C.byref(h)), what="qjx_create_slots")
+        self.h, self.cfg = h, cfg
+        self.d, self.n, self.nr, self.keep_adr = d_cap, n_slots * n_cap, num_robs, keep_adr
+        self.n_cap = n_cap
+        return self
+
+    def slot_load(self, slot, ensemble, psi=None):
+        """Load an ensemble (dict as for Engine.batch) into a free slot; psi [n_traj][d] or None (|0>)."""
+        keep = []
+        st = self._ensemble_struct(ensemble, keep)
+        p = None if psi is None else np.ascontiguousarray(psi, np.complex128)
+        self._chk(N.lib().qjx_slot_load(self.h, slot, C.byref(st), N.dp(p)), "qjx_slot_load")
+
+    def slot_release(self, slot):
+        self._chk(N.lib().qjx_slot_release(self.h, slot), "qjx_slot_release")
+
     def _chk(self, st, what):
         N.check(st, self.h, what)
 
