@@ -54,10 +54,12 @@ def parse():
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision form")
     ap.add_argument("--no-fbasis", action="store_true", help="skip the f-basis Lindblad RK4 measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-ensembles measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--serve-window", type=float, default=1.0, help="seconds of Poisson arrivals at 50/s")
     ap.add_argument("--batch-ensembles", type=int, default=32,
                     help="ensembles of configuration 4 in the batched measurement (of 256)")
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
-    ap.add_argument("--profile-target", default="plain", choices=["plain", "split", "fbasis"],
+    ap.add_argument("--profile-target", default="plain", choices=["plain", "split", "fbasis", "lpn"],
                     help="what --profile runs: one period of the plain or split form, or one f-basis period")
     return ap.parse_args()
 
@@ -289,6 +291,87 @@ def batched_bench(args, local):
     }
 
 
+# ---------------------------------------------------------------- Lyapunov pair kernel (profiling case)
+def lpn_profile_case(local):
+    """LpnMult on the headline dimer (dim 201): 2000 trajectories (1000 base/variation pairs), the
+    bases' transient period, the start (copy + perturbation bisection) and two observation periods
+    with lambda_lpn (random-observable distance, renormalisation thresholds of the production sweep
+    but delta_f_high = 5e-3 so that pairs renormalise)."""
+    import os_d_b200 as q
+
+    M = model()
+    n, d = 2000, M["d"]
+    eng = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, max_dumps=1, device=local)
+    eng.set_states(start_states(n, d))
+    eng.init_thresholds()
+    eng.set_active(n // 2)
+    eng.run_periods(1, is_obs=0)
+    eng.set_active(n)
+    eng.lpn_start(lpn_type=0, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10, delta_s=1e-3,
+                  delta_f_high=5e-3, delta_f_low=1e-5)
+    eng.reset_times()
+    for p in range(2):
+        eng.run_periods(1, is_obs=1)
+        eng.lpn_period((p + 1) * M["T"])
+    v = eng.lpn_values()
+    print(json.dumps({"pairs": n // 2, "renormalisations": int(v["num_renorms"].sum()),
+                      "bisection_steps_last": int(eng.lpn_last()["eps_iters"][n // 2:].sum())}), flush=True)
+    eng.close()
+
+
+# ---------------------------------------------------------------- serving loop (configuration 5, sampled)
+def serving_bench(args, local):
+    """Continuous batching (os_d_b200.serve): Poisson arrivals at 50/s over a short window, each
+    request a dimer ensemble with N log-uniform in [31, 255], E0 ~ U[0, 2], g log-uniform in
+    [0.01, 1], seed 23; latency from arrival to result on the wall clock; the same requests then
+    solved one after another by single-ensemble engines (serial plain FP64)."""
+    import os_d_b200 as q
+    from os_d_b200.serve import Server, dimer_ensemble
+
+    rng = np.random.default_rng(23)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / 50.0)
+        if t > args.serve_window:
+            break
+        N = int(round(10 ** rng.uniform(np.log10(31), np.log10(255))))
+        arrivals.append((t, dict(N=N, n_traj=int(rng.integers(100, 501)), periods=int(rng.integers(5, 21)),
+                                 E0=float(rng.uniform(0, 2)), g=float(10 ** rng.uniform(-2, 0)), seed=23,
+                                 tr_base=1000 * len(arrivals))))
+    srv = Server(n_slots=64, d_cap=256, n_cap=500, deep=DEEP, hbm_budget=40 << 30, device=local)
+    t0 = time.perf_counter()
+    res = srv.run(arrivals)
+    wall = time.perf_counter() - t0
+    dev_ms = srv.device_ms
+    srv.close()
+    lat = np.array([r["t_done"] - r["t_submit"] for r in res])
+    work = float(sum(r["n_traj"] * r["periods"] for r in res))
+    # serial plain FP64 solves of the same requests (device time of each alone)
+    ser_ms = 0.0
+    for _, r in arrivals:
+        e = dimer_ensemble(r, DEEP)
+        d, n = e["U"].shape[-1], e["n_traj"]
+        A = q.Engine(e["U"], e["L"], e["g"], e["HE"], None, e["T"], n, seed=e["seed"], tr_base=e["tr_base"],
+                     max_dumps=1, device=local)
+        psi = np.zeros((n, d), np.complex128)
+        psi[:, 0] = 1.0
+        A.set_states(psi)
+        A.init_thresholds()
+        A.run_periods(int(r["periods"]), is_obs=1, dump_at=[int(r["periods"])], dump_base=0)
+        ser_ms += A.stats()["kernel_ms"]
+        A.close()
+    return {
+        "workload": (f"{len(arrivals)} requests, Poisson 50/s over {args.serve_window:g} s; dimer N log-uniform [31,255], "
+                     f"trajectories U[100,500], periods U[5,20], E0 ~ U[0,2], g log-uniform [0.01,1], seed 23; "
+                     f"64 resident slots (d <= 256, 500 trajectories), one period per tick"),
+        "metric": METRIC, "value": work / wall, "device_value": work / (dev_ms * 1e-3),
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "serial_single_ensemble_engines": {"value": work / (ser_ms * 1e-3), "device_s": ser_ms * 1e-3},
+        "speedup_vs_serial_device": ser_ms / dev_ms, "ticks": srv.ticks, "wall_s": wall,
+    }
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -407,6 +490,9 @@ def run_ours(args):
         clk = clocks.stop() if clocks else None
         return float(allreduce([dev_ms], "max")[0]), wall, clk, st0, eng.stats(), ens
 
+    if args.profile and args.profile_target == "lpn":
+        lpn_profile_case(local)
+        return
     if args.profile and args.profile_target == "fbasis":
         args.warmup, args.steps, args.no_cpu_baseline = 0, 1, True
         fbasis_bench(args, local)
@@ -509,8 +595,10 @@ def run_ours(args):
                                "qjx_get_states per step"}
     if rank == 0 and not args.no_fbasis:
         line["fbasis"] = fbasis_bench(args, local)
-    if rank == 0 and world == 1 and not args.no_batch:  # a single-GPU measurement
+    if rank == 0 and world == 1 and not args.no_batch:  # single-GPU measurements
         line["batched"] = batched_bench(args, local)
+    if rank == 0 and world == 1 and not args.no_serve:
+        line["serving"] = serving_bench(args, local)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 128 * threads  # about 15 s of CPU work
