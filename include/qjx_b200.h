@@ -84,6 +84,11 @@ typedef struct {
                           lo*hi), states, norms, thresholds, jump times and renormalisation stay
                           FP64.  Needs d <= 256.  QJX has no such mode
                           (its zgemv is FP64). */
+    const double *branch_len; /* [num_branches] durations of the branches of a period (NULL: T / 2
+                          each, the dimer's half periods); systems with unequal parts (the JCS kick
+                          and free evolution, init_split_structure_jcs, core.cpp:10086-10124) give
+                          them here.  Level l of branch b steps 2 len_b / brep 2^-(l+2), brep = 1
+                          or 2 deep_num_steps. */
 } qjx_config;
 
 typedef struct {

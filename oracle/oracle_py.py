@@ -22,7 +22,7 @@ class OrcProblem(C.Structure):
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("record", C.c_int), ("rng_kind", C.c_int),
                 ("T", C.c_double), ("seed", C.c_uint64),
                 ("U", c_double_p), ("L", c_double_p), ("g", c_double_p), ("HE", c_double_p), ("R", c_double_p),
-                ("inj_u", c_double_p), ("inj_off", c_i64_p), ("tr_base", C.c_uint64)]
+                ("inj_u", c_double_p), ("inj_off", c_i64_p), ("tr_base", C.c_uint64), ("branch_len", c_double_p)]
 
 
 class OrcState(C.Structure):
@@ -170,7 +170,7 @@ class Ensemble:
     """One QJ ensemble run by the oracle, mirroring the Std task flow."""
 
     def __init__(self, U, L, g, HE, R, T, n_traj, seed=0, record=2, rng_kind=0, inj_u=None, inj_off=None,
-                 rec_cap=4096, tr_base=0):
+                 rec_cap=4096, tr_base=0, branch_len=None):
         self.U = np.ascontiguousarray(U, dtype=np.complex128)  # [nb, deep, d, d]
         nb, deep, d, _ = self.U.shape
         self.L = np.ascontiguousarray(L, dtype=np.complex128).reshape(-1, d, d)
@@ -188,6 +188,8 @@ class Ensemble:
         p.R = _dp(self.R) if self.R.size else None
         p.inj_u = _dp(self.inj_u)
         p.inj_off = self.inj_off.ctypes.data_as(c_i64_p) if self.inj_off is not None else None
+        self.branch_len = None if branch_len is None else np.ascontiguousarray(branch_len, np.float64)
+        p.branch_len = _dp(self.branch_len)
         self.p = p
         n = n_traj
         self.phi = _cplx((n, d))

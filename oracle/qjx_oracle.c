@@ -530,7 +530,7 @@ typedef struct {
     int is_obs;
     double *phi, *aux, *res, *gn;
     const tmat *tU, *tL;
-    double dt[64];
+    const double *dt;   /* [num_branches][deep] split-level steps */
     int err;
 } traj_ctx;
 
@@ -607,7 +607,7 @@ static void one_period_branch(traj_ctx *c, int b, int level)
     (void)dd;
     double *t = &s->t[c->tr];
     double *eta = &s->eta[c->tr];
-    const double dt = c->dt[level];
+    const double dt = c->dt[b * p->deep + level];
 
     if (level == p->deep - 1) {
         for (int counter = 0; counter != 2; counter++) {
@@ -677,12 +677,30 @@ int orc_init(const orc_problem *p, orc_state *s, int start_type, int start_state
     return 0;
 }
 
+/* Split-level steps of every branch: level 0 steps half of the branch head H_b, every level
+ * halves it (init_split_branches, qj_proc.cpp:15-24); H_b = 2 len_b, len_b = T / 2 by default. */
+static double *dt_table(const orc_problem *p)
+{
+    double *t = (double *)malloc(sizeof(double) * (size_t)p->num_branches * p->deep);
+    if (!t) return NULL;
+    for (int b = 0; b < p->num_branches; b++) {
+        double dt = (p->branch_len ? 2.0 * p->branch_len[b] : p->T) * 0.5;
+        for (int l = 0; l < p->deep; l++) {
+            dt *= 0.5;
+            t[b * p->deep + l] = dt;
+        }
+    }
+    return t;
+}
+
 int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_periods, int is_obs, int n_threads)
 {
     if (p->deep < 1 || p->deep > 60) return 1;
     int bad = 0;
     tmat tU, tL;
     if (tmat_make(p->d, p->num_branches * p->deep, p->U, &tU) || tmat_make(p->d, p->num_diss, p->L, &tL)) return 2;
+    double *dtab = dt_table(p);
+    if (!dtab) return 2;
 #ifdef _OPENMP
     if (n_threads <= 0) n_threads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads) reduction(+ : bad)
@@ -697,8 +715,7 @@ int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_
         c.aux = (double *)calloc(2 * (size_t)d, sizeof(double));
         c.res = (double *)calloc(2 * (size_t)d, sizeof(double));
         c.gn = (double *)calloc((size_t)p->num_diss + 1, sizeof(double));
-        double dt = p->T * 0.5;
-        for (int l = 0; l < p->deep; l++) { dt *= 0.5; c.dt[l] = dt; }
+        c.dt = dtab;
         for (int per = 0; per < n_periods && !c.err; per++)
             for (int b = 0; b < p->num_branches && !c.err; b++) one_period_branch(&c, b, 0);
         s->error[tr] = c.err;
@@ -706,6 +723,7 @@ int orc_run_periods(const orc_problem *p, orc_state *s, int tr0, int tr1, int n_
         free(c.aux); free(c.res); free(c.gn);
     }
     (void)n_threads;
+    free(dtab);
     tmat_free(&tU);
     tmat_free(&tL);
     return bad;
@@ -721,6 +739,8 @@ int orc_run_branch_units(const orc_problem *p, orc_state *s, int tr0, int tr1, i
     int bad = 0;
     tmat tU, tL;
     if (tmat_make(p->d, p->num_branches * p->deep, p->U, &tU) || tmat_make(p->d, p->num_diss, p->L, &tL)) return 2;
+    double *dtab = dt_table(p);
+    if (!dtab) return 2;
 #ifdef _OPENMP
     if (n_threads <= 0) n_threads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads) reduction(+ : bad)
@@ -735,14 +755,14 @@ int orc_run_branch_units(const orc_problem *p, orc_state *s, int tr0, int tr1, i
         c.aux = (double *)calloc(2 * (size_t)d, sizeof(double));
         c.res = (double *)calloc(2 * (size_t)d, sizeof(double));
         c.gn = (double *)calloc((size_t)p->num_diss + 1, sizeof(double));
-        double dt = p->T * 0.5;
-        for (int l = 0; l < p->deep; l++) { dt *= 0.5; c.dt[l] = dt; }
+        c.dt = dtab;
         for (int u = 0; u < n_units && !c.err; u++) one_period_branch(&c, b, 0);
         s->error[tr] = c.err;
         if (c.err) bad++;
         free(c.aux); free(c.res); free(c.gn);
     }
     (void)n_threads;
+    free(dtab);
     tmat_free(&tU);
     tmat_free(&tL);
     return bad;

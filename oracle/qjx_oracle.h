@@ -85,6 +85,8 @@ typedef struct {
     const double *inj_u;      /* rng_kind 1: concatenated uniforms */
     const int64_t *inj_off;   /* rng_kind 1: [n_traj + 1] offsets into inj_u */
     uint64_t tr_base;         /* Philox stream of local trajectory tr is tr_base + tr (sharding) */
+    const double *branch_len; /* [num_branches] branch durations (NULL: T / 2 each, the dimer's
+                                 half periods); level l of branch b steps 2 len_b 2^-(l+2) */
 } orc_problem;
 
 /* Mutable per-run state and outputs. */

@@ -32,7 +32,7 @@ class QjxConfig(C.Structure):
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
                 ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("deep_num_steps", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("branch_len", c_double_p)]
 
 
 class QjxEnsemble(C.Structure):

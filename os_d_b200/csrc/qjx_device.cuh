@@ -140,7 +140,7 @@ struct Params {
     const int *e_d;                   // [E] dimension
     const int *e_tr0;                 // [E + 1] first trajectory
     const int *e_g0;                  // [E] first group
-    const double *e_dt;               // [E][deep] split-level steps
+    const double *e_dt;               // [E][nb][deep] split-level steps
     const double *e_rate;             // [E][nd] jump rates
     const unsigned long long *e_seed; // [E] Philox key
     const long long *e_sbase;         // [E] Philox stream of the ensemble's first trajectory
@@ -159,7 +159,7 @@ struct Params {
 __device__ __forceinline__ int dim_of(const Params &P, const TrajState &s) { return P.e_d[s.ens]; }
 __device__ __forceinline__ const double *dt_of(const Params &P, const TrajState &s)
 {
-    return P.e_dt + (size_t)s.ens * P.deep;
+    return P.e_dt + ((size_t)s.ens * P.nb + s.b) * P.deep;
 }
 __device__ __forceinline__ double rate_of(const Params &P, const TrajState &s, int i)
 {

@@ -63,6 +63,7 @@ struct qjx_engine {
     bool states_set = false;
     int period_base = 0;  // periods run since the last time reset (the RK propagator's period_id)
     int n_ens = 1;        // ensembles (qjx_create_batch)
+    std::vector<double> branch_len;   // copy of qjx_config.branch_len
     // serving engines (qjx_create_slots): every ensemble is a slot with room for d_cap and n_cap
     int slot_dcap = 0, slot_ncap = 0;
     std::vector<int> slot_n;          // trajectories of the loaded ensemble (0: free)
@@ -171,6 +172,24 @@ static void pack_split(const double *M, int d, int MDs, int KS, uint16_t *out)
             }
 }
 
+// Split-level steps of every branch of one ensemble: level 0 steps half of the branch head,
+// every level halves it (qj_proc.cpp:15-24).  The head is T (a branch is half a period) or, for
+// the deep tasks, the sub-period T / (2 deep_num_steps) (core.cpp:9934); with explicit branch
+// durations it is 2 len_b / brep.
+static void fill_dt(const qjx_config &c, double T, double *out)
+{
+    const int brep = c.deep_num_steps > 0 ? 2 * c.deep_num_steps : 1;
+    for (int b = 0; b < c.num_branches; b++) {
+        const double head = c.branch_len ? 2.0 * c.branch_len[b] / double(brep)
+                                         : (c.deep_num_steps > 0 ? 0.5 * T / double(c.deep_num_steps) : T);
+        double dt = head * 0.5;
+        for (int l = 0; l < c.deep; l++) {
+            dt *= 0.5;
+            out[(size_t)b * c.deep + l] = dt;
+        }
+    }
+}
+
 // One ensemble of an engine: its dimension, trajectories, period, Philox key and first stream,
 // and operators (U: [num_branches][deep][d][d], L: [num_diss][d][d], g: [num_diss], HE, R).
 struct EnsDesc {
@@ -211,16 +230,26 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     }
     const int Ge = c.num_branches * c.deep + c.num_diss + 1 + c.num_robs;  // groups per ensemble
     const long long Gl = (long long)E * Ge;
-    if (dmax > kMaxMD || Ge > kMaxGroups || Gl > (1 << 24) || ntot > (1 << 30)) return QJX_ERR_UNSUPPORTED;
+    if (dmax > kMaxMD || Gl > (1 << 24) || ntot > (1 << 30)) return QJX_ERR_UNSUPPORTED;
     if (c.precision != 0 && c.precision != 1) return QJX_ERR_INVALID_ARG;
-    // the split kernel's N = MDs <= 256 and its bucket tables hold one ensemble
-    if (c.precision == 1 && (dmax > 256 || E > 1)) return QJX_ERR_UNSUPPORTED;
+    // the split kernel's N = MDs <= 256 and its shared-memory bucket tables hold one ensemble of
+    // at most kMaxGroups matrices
+    if (c.precision == 1 && (dmax > 256 || E > 1 || Ge > kMaxGroups)) return QJX_ERR_UNSUPPORTED;
     const int G = (int)Gl;
     const int n = (int)ntot;
 
     qjx_engine *h = new (std::nothrow) qjx_engine();
     if (!h) return QJX_ERR_OOM;
     h->cfg = c;
+    if (c.branch_len) {  // keep a copy: the caller's array need not outlive the call
+        for (int b = 0; b < c.num_branches; b++)
+            if (!(c.branch_len[b] > 0.0)) {
+                delete h;
+                return QJX_ERR_INVALID_ARG;
+            }
+        h->branch_len.assign(c.branch_len, c.branch_len + c.num_branches);
+        h->cfg.branch_len = h->branch_len.data();
+    }
     h->cfg.d = dmax;
     h->cfg.n_traj = n;
     h->n_ens = E;
@@ -281,7 +310,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     // ensemble tables; matrices of ensemble e in its own transposed padded layout
     // [k < kp_e][row < MD_e] (zero padded), one after another
     std::vector<int> e_d(E), e_tr0(E + 1), e_g0(E), g_ens(G);
-    std::vector<double> e_dt((size_t)E * c.deep), e_rate((size_t)E * c.num_diss);
+    std::vector<double> e_dt((size_t)E * c.num_branches * c.deep), e_rate((size_t)E * c.num_diss);
     std::vector<unsigned long long> e_seed(E);
     std::vector<long long> e_sbase(E), g_off(G), g_loff(G);
     long long moff = 0, loff = 0;
@@ -293,14 +322,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
         e_g0[e] = e * Ge;
         e_seed[e] = x.seed;
         e_sbase[e] = x.sbase;
-        // split-step sizes: dt = T/2, then halved per level (qj_proc.cpp:15-24); the deep tasks'
-        // tree head is the sub-period T / (2 deep_num_steps) (core.cpp:9934)
-        const double t_head = c.deep_num_steps > 0 ? 0.5 * x.T / double(c.deep_num_steps) : x.T;
-        double dt = t_head * 0.5;
-        for (int l = 0; l < c.deep; l++) {
-            dt *= 0.5;
-            e_dt[(size_t)e * c.deep + l] = dt;
-        }
+        fill_dt(h->cfg, x.T, e_dt.data() + (size_t)e * c.num_branches * c.deep);
         for (int i = 0; i < c.num_diss; i++) e_rate[(size_t)e * c.num_diss + i] = x.g[i];
         const long long per = (long long)((x.d + 1) & ~1) * (8 * ((x.d + 7) / 8));
         for (int l = 0; l < Ge; l++) {
@@ -746,19 +768,15 @@ extern "C" qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble 
         CK(cudaMemcpy(const_cast<double2 *>(P.mats) + goff[l], host.data() + per * l, per * sizeof(double),
                       cudaMemcpyHostToDevice));
     // the slot's ensemble table entries
-    std::vector<double> dts(P.deep);
-    double dt = (h->cfg.deep_num_steps > 0 ? 0.5 * e->T / double(h->cfg.deep_num_steps) : e->T) * 0.5;
-    for (int l = 0; l < P.deep; l++) {
-        dt *= 0.5;
-        dts[l] = dt;
-    }
+    std::vector<double> dts((size_t)P.nb * P.deep);
+    fill_dt(h->cfg, e->T, dts.data());
     const unsigned long long seed = e->seed;
     const long long sbase = e->tr_base;
     CK(cudaMemcpy(const_cast<int *>(P.e_d) + slot, &d, sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(const_cast<int *>(P.e_nc) + slot, &nc, sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(const_cast<int *>(P.e_kb) + slot, &kb, sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(const_cast<double *>(P.e_dt) + (size_t)slot * P.deep, dts.data(), P.deep * sizeof(double),
-                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<double *>(P.e_dt) + (size_t)slot * P.nb * P.deep, dts.data(),
+                  dts.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(const_cast<double *>(P.e_rate) + (size_t)slot * P.nd, e->g, P.nd * sizeof(double),
                   cudaMemcpyHostToDevice));
     CK(cudaMemcpy(const_cast<unsigned long long *>(P.e_seed) + slot, &seed, sizeof(seed), cudaMemcpyHostToDevice));
@@ -809,6 +827,7 @@ extern "C" qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, 
     c.num_branches = 1;  // groups 0 and 1: H_eff and H_drv
     c.deep = 2;
     c.deep_num_steps = 0;
+    c.branch_len = nullptr;
     const size_t dd2 = (size_t)2 * c.d * c.d;
     std::vector<double> M(2 * dd2);
     std::memcpy(M.data(), H_eff, dd2 * sizeof(double));

@@ -15,7 +15,7 @@ class Engine:
     """One ensemble of trajectories resident on a GPU."""
 
     def __init__(self, U, L, g, HE, R=None, T=2 * np.pi, n_traj=1, seed=0, record=0, rng_kind=0, rec_cap=1024,
-                 keep_adr=0, max_dumps=1, device=0, tr_base=0, precision=0, deep_num_steps=0):
+                 keep_adr=0, max_dumps=1, device=0, tr_base=0, precision=0, deep_num_steps=0, branch_len=None):
         U = np.ascontiguousarray(U, np.complex128)
         nb, deep, d, _ = U.shape
         L = np.ascontiguousarray(L, np.complex128).reshape(-1, d, d)
@@ -29,6 +29,8 @@ class Engine:
         cfg.max_dumps, cfg.device, cfg.tr_base = max_dumps, device, tr_base
         cfg.precision = precision  # 0 complex FP64, 1 split bf16x3 on tcgen05
         cfg.deep_num_steps = deep_num_steps  # > 0: StdDeep task (U from build_dimer_deep)
+        self._branch_len = None if branch_len is None else np.ascontiguousarray(branch_len, np.float64)
+        cfg.branch_len = N.dp(self._branch_len)  # per-branch durations (None: T / 2 each)
         self.cfg = cfg
         self.d, self.n, self.nr = d, n_traj, R.shape[0]
         self.keep_adr = keep_adr
