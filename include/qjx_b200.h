@@ -240,6 +240,14 @@ qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_t
  * T = 2 pi / omega.  Any output may be NULL. */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
                            double *H, double *Hd, double *L, double *K, double *Utree);
+/* The JCS system (sys_id 1; newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601; split structure
+ * core.cpp:10086-10124): d = N, H = 0.5/alpha^3 a^+a^+aa, H_drv = a^+ - a, L = a, the number
+ * operator Nop = a^+ a and the observable `special` A_op = a; K_0 = -i H_eff + E0 H_drv (the kick),
+ * K_1 = -i H_eff with gamma = 1/(4 alpha); Utree [2][deep][d][d] = exp(K_b head_b 2^-(l+2)) with
+ * head_b = part_b alpha (branch b lasts head_b / 2: qjx_config.branch_len = head_b / 2).  Any
+ * output pointer may be NULL. */
+qjx_status qjx_build_jcs(int N, double alpha, double drv_ampl, double part_1, double part_2, int deep, double *H,
+                         double *Hd, double *L, double *Nop, double *A_op, double *Kout, double *Utree);
 /* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)
  * (init_split_structure_dimer_deep, core.cpp:9928-9981). */
 qjx_status qjx_build_dimer_deep(int N, double J, double U, double E, double A, double g, double omega, int deep,

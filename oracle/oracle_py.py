@@ -60,6 +60,7 @@ def lib():
         L.orc_dimer_operators.argtypes = [C.c_int] + [C.c_double] * 5 + [c_double_p] * 5
         L.orc_expm.argtypes = [C.c_int, c_double_p, c_double_p]
         L.orc_dimer_heff.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p]
+        L.orc_jcs_operators.argtypes = [C.c_int, C.c_double, C.c_double] + [c_double_p] * 6
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
@@ -102,6 +103,14 @@ def dimer_operators(N, J, U, E, A, g):
     rc = lib().orc_dimer_operators(N, J, U, E, A, g, _dp(H), _dp(Hd), _dp(L), _dp(K0), _dp(K1))
     assert rc == 0
     return H, Hd, L, K0, K1
+
+
+def jcs_operators(N, alpha, drv_ampl):
+    """JCS (sys_id 1): H, H_drv, L = a, Nop = a^+ a, K0, K1 (d = N)."""
+    d = N
+    out = [_cplx((d, d)) for _ in range(6)]
+    assert lib().orc_jcs_operators(N, alpha, drv_ampl, *[_dp(x) for x in out]) == 0
+    return tuple(out)
 
 
 def dimer_heff(N, J, U, E, g):

@@ -82,6 +82,71 @@ int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
     return 0;
 }
 
+/* JCS (sys_id 1): d = N; a = sum sqrt(k+1) |k><k+1| (newdel.cpp:608-614); H = 0.5 / alpha^3 ((a^+ a^+) a) a
+ * (dgemm order, newdel.cpp:617-631); H_drv = a^+ - a; L = a (newdel.cpp:1571-1576); Nop = a^+ a
+ * (experiment.cpp:2127-2135); gamma = 1 / (4 alpha), H_eff = H - (i/2) gamma L^H L,
+ * K0 = -i H_eff + E0 H_drv, K1 = -i H_eff (newdel.cpp:2508-2597). */
+static void rmatmul(int d, const double *A, const double *B, double *C)
+{
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            double s = 0.0;
+            for (int k = 0; k < d; k++) s = s + A[(size_t)i * d + k] * B[(size_t)k * d + j];
+            C[(size_t)i * d + j] = s;
+        }
+}
+
+int orc_jcs_operators(int N, double alpha, double drv_ampl, double *H, double *Hd, double *L, double *Nop,
+                      double *K0, double *K1)
+{
+    if (N < 2) return 1;
+    const int d = N;
+    const size_t dd = (size_t)d * d;
+    double *a = (double *)calloc(dd, sizeof(double)), *ad = (double *)calloc(dd, sizeof(double));
+    double *m1 = (double *)malloc(dd * sizeof(double)), *m2 = (double *)malloc(dd * sizeof(double));
+    double *m3 = (double *)malloc(dd * sizeof(double)), *nop = (double *)malloc(dd * sizeof(double));
+    if (!a || !ad || !m1 || !m2 || !m3 || !nop) return 2;
+    for (int k = 0; k < d - 1; k++) {
+        a[(size_t)k * d + (k + 1)] = sqrt((double)(k + 1));
+        ad[(size_t)(k + 1) * d + k] = sqrt((double)(k + 1));
+    }
+    rmatmul(d, ad, ad, m1);
+    rmatmul(d, m1, a, m2);
+    rmatmul(d, m2, a, m3);
+    rmatmul(d, ad, a, nop);
+    const double hs = 0.5 / pow(alpha, 3);
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(Hd, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 2 * dd * sizeof(double));
+    memset(Nop, 0, 2 * dd * sizeof(double));
+    for (size_t e = 0; e < dd; e++) {
+        H[2 * e] = hs * m3[e];
+        Hd[2 * e] = ad[e] - a[e];
+        L[2 * e] = a[e];
+        Nop[2 * e] = nop[e];
+    }
+    const double gamma = 1.0 / (4.0 * alpha);
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            double sr = 0.0, si = 0.0;
+            for (int k = 0; k < d; k++) {
+                const double ar = L[2 * ((size_t)k * d + i)], ai = L[2 * ((size_t)k * d + i) + 1];
+                const double br = L[2 * ((size_t)k * d + j)], bi = L[2 * ((size_t)k * d + j) + 1];
+                sr = sr + (ar * br + ai * bi);
+                si = si + (ar * bi - ai * br);
+            }
+            const size_t idx = (size_t)i * d + j;
+            const double hr = H[2 * idx] + 0.5 * (gamma * si);
+            const double hi = 0.0 - 0.5 * (gamma * sr);
+            K0[2 * idx] = 0.0 + (hi + drv_ampl * Hd[2 * idx]);
+            K0[2 * idx + 1] = 0.0 - (hr + drv_ampl * 0.0);
+            K1[2 * idx] = 0.0 + (hi + 0.0 * Hd[2 * idx]);
+            K1[2 * idx + 1] = 0.0 - (hr + 0.0 * 0.0);
+        }
+    free(a); free(ad); free(m1); free(m2); free(m3); free(nop);
+    return 0;
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

@@ -48,6 +48,11 @@ extern "C" {
 int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
                         double *H, double *Hd, double *L, double *K0, double *K1);
 
+/* JCS operators (sys_id 1, newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601): d = N; H, H_drv,
+ * L = a, the number operator Nop = a^+ a, K0 = -i H_eff + E0 H_drv, K1 = -i H_eff, all complex d x d. */
+int orc_jcs_operators(int N, double alpha, double drv_ampl, double *H, double *Hd, double *L, double *Nop,
+                      double *K0, double *K1);
+
 /* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
  * propagator (newdel.cpp:2354-2366), complex d x d. */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);

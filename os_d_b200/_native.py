@@ -21,7 +21,7 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
+    "qjx_random_observables", "qjx_build_jcs", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
     "qjx_set_active", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
@@ -108,6 +108,7 @@ def lib():
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
         L.qjx_build_dimer_deep.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int, C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_build_jcs.argtypes = [C.c_int] + [C.c_double] * 4 + [C.c_int] + [c_double_p] * 7
         L.qjx_build_dimer_rk.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 2
         L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.POINTER(C.c_int), C.POINTER(C.c_int), c_int_p, c_int_p, c_double_p,
@@ -165,6 +166,17 @@ def build_dimer_deep(N, J, U, E, A, g, omega, deep, deep_num_steps):
     check(lib().qjx_build_dimer_deep(N, J, U, E, A, g, omega, deep, deep_num_steps, dp(H), dp(Hd), dp(Lm), None,
                                      dp(Ut)), what="qjx_build_dimer_deep")
     return H, Hd, Lm, Ut
+
+
+def build_jcs(N, alpha, drv_ampl, part_1, part_2, deep):
+    """JCS system (sys_id 1): H, H_drv, L = a, Nop = a^+ a, A = a and the split tree [2][deep][N][N];
+    branch b lasts part_b * alpha / 2 (pass branch_len to the engine)."""
+    d = N
+    H, Hd, L, Nop, A = (np.zeros((d, d), np.complex128) for _ in range(5))
+    U = np.zeros((2, deep, d, d), np.complex128)
+    check(lib().qjx_build_jcs(N, alpha, drv_ampl, part_1, part_2, deep, dp(H), dp(Hd), dp(L), dp(Nop), dp(A), None,
+                              dp(U)), what="qjx_build_jcs")
+    return H, Hd, L, Nop, A, U
 
 
 def build_dimer_rk(N, J, U, E, g):

@@ -111,6 +111,17 @@ double param_or(const ConfigParam &cp, const std::string &key, double dflt)
     return it == cp.params.end() ? dflt : it->second;
 }
 
+static std::string lpn_suffix(const RunParam &rp, const ConfigParam &cp)
+{
+    if (rp.task_id != 7 && rp.task_id != 8) return "";
+    std::stringstream p;  // suffix_lpn (outputter.cpp:371-381)
+    p << "_lpn(" << std::defaultfloat << std::setprecision(6) << param(cp, "lpn_type") << "_" << std::setprecision(4)
+      << std::fixed << std::log10(param(cp, "lpn_delta_s")) << "_" << std::setprecision(4) << std::fixed
+      << std::log10(param(cp, "lpn_delta_f_high")) << "_" << std::setprecision(4) << std::fixed
+      << std::log10(param(cp, "lpn_delta_f_low")) << ")";
+    return p.str();
+}
+
 std::string dimer_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
 {
     std::stringstream s;
@@ -129,13 +140,23 @@ std::string dimer_suffix(const RunParam &rp, const ConfigParam &cp, int precisio
       << std::setprecision(precision) << std::fixed << param(cp, "dimer_prm_U") << "_"
       << std::setprecision(precision) << std::fixed << param(cp, "dimer_prm_J") << ")";
     p << "_start(" << int(param(cp, "start_type")) << "_" << int(param(cp, "start_state")) << ")";
-    if (rp.task_id == 7 || rp.task_id == 8) {  // LpnMult / LpnMultDeep: suffix_lpn (outputter.cpp:371-381)
-        p << "_lpn(" << std::defaultfloat << std::setprecision(6) << param(cp, "lpn_type") << "_"
-          << std::setprecision(4) << std::fixed << std::log10(param(cp, "lpn_delta_s")) << "_"
-          << std::setprecision(4) << std::fixed << std::log10(param(cp, "lpn_delta_f_high")) << "_"
-          << std::setprecision(4) << std::fixed << std::log10(param(cp, "lpn_delta_f_low")) << ")";
-    }
-    return s.str() + p.str() + ".txt";
+    return s.str() + p.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
+std::string jcs_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_N(" << int(param(cp, "N")) << ")";
+    s << "_diss(" << int(param(cp, "diss_type")) << "_" << std::setprecision(precision) << std::fixed
+      << param(cp, "diss_gamma") << "_" << std::setprecision(precision) << std::fixed << param(cp, "diss_phase") << ")";
+    s << "_drv(" << std::setprecision(precision) << std::fixed << param(cp, "jcs_drv_part_1") << "_"
+      << std::setprecision(precision) << std::fixed << param(cp, "jcs_drv_part_2") << "_"
+      << std::setprecision(precision) << std::fixed << param(cp, "jcs_drv_ampl") << ")";
+    s << "_prm(" << std::setprecision(precision) << std::fixed << param(cp, "jcs_prm_alpha") << ")";
+    s << "_start(" << int(param(cp, "start_type")) << "_" << int(param(cp, "start_state")) << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
@@ -193,6 +214,20 @@ void save_2d_inv_double_data(const std::string &fn, const double *data, int rows
     ofs << std::setprecision(precision) << std::scientific;
     for (int r = 0; r < rows; r++) {
         for (int c = 0; c < cols; c++) ofs << data[(size_t)c * rows + r] << " ";
+        ofs << std::endl;
+    }
+}
+
+void save_2d_inv_complex_data(const std::string &fn, const double *data, int rows, int cols, int precision,
+                              bool append)
+{
+    std::ofstream ofs = open_out(fn, append);
+    ofs << std::setprecision(precision) << std::scientific;
+    for (int r = 0; r < rows; r++) {
+        for (int c = 0; c < cols; c++) {
+            const size_t i = (size_t)c * rows + r;
+            ofs << data[2 * i] << " " << data[2 * i + 1] << " ";
+        }
         ofs << std::endl;
     }
 }

@@ -45,6 +45,8 @@ double param_or(const ConfigParam &cp, const std::string &key, double dflt);
 // DimerOutputBehavior::suffix_param with precision 4 (source/cpp/QJX/QJX/outputter.cpp:3-44,
 // 353-388): _setup(s_t_p)_rnd(seed_mns)_N(..)_diss(..)_drv(..)_prm(..)_start(..).txt
 std::string dimer_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
+// JCSOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:95-133)
+std::string jcs_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 
 // init_dump_periods (source/cpp/QJX/QJX/newdel_exp.cpp:408-455); empty on a bad dump_type.
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods);
@@ -55,6 +57,10 @@ std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods);
 void save_double_data(const std::string &fn, const double *data, size_t n, int precision, bool append);
 void save_int_data(const std::string &fn, const int *data, size_t n, bool append);
 void save_complex_data(const std::string &fn, const double *data, size_t n, int precision, bool append);
+// complex data[col * rows + row] (interleaved re, im) printed as rows lines of "re im " pairs
+// (save_2d_inv_complex_data, utils.cpp:228-282, the non-append branch)
+void save_2d_inv_complex_data(const std::string &fn, const double *data, int rows, int cols, int precision,
+                              bool append);
 // data[col * rows + row] printed as rows lines of cols values (save_2d_inv_double_data)
 void save_2d_inv_double_data(const std::string &fn, const double *data, int rows, int cols, int precision,
                              bool append);

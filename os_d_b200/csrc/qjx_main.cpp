@@ -293,7 +293,11 @@ int main(int argc, char **argv)
     if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
     std::cout << params_echo(rp, cp);
 
-    if (rp.sys_id != 0) die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer, sys_id 0)");
+    if (rp.sys_id != 0 && rp.sys_id != 1)
+        die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer (0) and JCS (1) systems)");
+    const bool jcs = rp.sys_id == 1;  // JCS: the Std task with the QJ propagator
+    if (jcs && (rp.task_id != 1 || rp.prop_id != 0))
+        die("Wrong task_id / prop_id for sys_id 1 (this engine runs JCS with the Std task and the QJ propagator)");
     if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7)
         die("Wrong task_id: " + std::to_string(rp.task_id) +
             " (this engine runs the Std (1), StdDeep (4) and LpnMult (7) tasks)");
@@ -302,7 +306,7 @@ int main(int argc, char **argv)
         die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
 
     try {
-        cp.fn_suffix = dimer_suffix(rp, cp, 4);
+        cp.fn_suffix = jcs ? jcs_suffix(rp, cp, 4) : dimer_suffix(rp, cp, 4);
     } catch (const std::exception &e) {
         die(e.what());
     }
@@ -313,10 +317,15 @@ int main(int argc, char **argv)
 
     try {
         const int N = int(param(cp, "N"));
-        const int d = N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
-        const double J = param(cp, "dimer_prm_J"), U = param(cp, "dimer_prm_U"), E = param(cp, "dimer_prm_E");
-        const double A = param(cp, "dimer_drv_ampl"), omega = param(cp, "dimer_drv_freq");
+        // the dimer has N + 1 Fock states; the JCS oscillator is truncated at N states (newdel.cpp:110)
+        const int d = jcs ? N : N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
+        const double J = jcs ? 0.0 : param(cp, "dimer_prm_J"), U = jcs ? 0.0 : param(cp, "dimer_prm_U");
+        const double E = jcs ? 0.0 : param(cp, "dimer_prm_E");
+        const double A = jcs ? 0.0 : param(cp, "dimer_drv_ampl"), omega = jcs ? 1.0 : param(cp, "dimer_drv_freq");
         const double g = param(cp, "diss_gamma");
+        const double jcs_alpha = jcs ? param(cp, "jcs_prm_alpha") : 0.0;
+        const double jcs_ampl = jcs ? param(cp, "jcs_drv_ampl") : 0.0;
+        const double jcs_p1 = jcs ? param(cp, "jcs_drv_part_1") : 0.0, jcs_p2 = jcs ? param(cp, "jcs_drv_part_2") : 0.0;
         const int start_type = int(param(cp, "start_type")), start_state = int(param(cp, "start_state"));
         const int jump = int(param(cp, "jump"));
         const int dump_obs = int(param(cp, "dump_obs")), dump_evo_sep = int(param(cp, "dump_evo_sep"));
@@ -328,7 +337,7 @@ int main(int argc, char **argv)
         const int dump_purity = int(param_or(cp, "dump_purity", 0));
         const int num_robs = int(param(cp, "num_random_obs"));
         const int robs_seed = int(param_or(cp, "random_obs_seed", 0));
-        if (n < 1 || N < 1) die("num_trajectories and N must be positive");
+        if (n < 1 || N < 1 || (jcs && N < 2)) die("num_trajectories and N must be positive (N >= 2 for JCS)");
         if (start_type == 0 && (start_state < 0 || start_state >= d)) die("start_state out of range");
         const std::string &sfx = cp.fn_suffix;
         const std::string path = rp.path;
@@ -340,7 +349,13 @@ int main(int argc, char **argv)
         const bool deep_task = rp.task_id == 4;
         const int nsub = deep_task ? int(param(cp, "deep_num_steps")) : 0;
         if (deep_task && nsub < 1) die("deep_num_steps must be positive");
-        if (deep_task)
+        // JCS: the number operator (energy slot) and a = special (first random-observable slot)
+        std::vector<double> Nop(jcs ? 2 * dd : 0), Aop(jcs ? 2 * dd : 0);
+        if (jcs)
+            check(qjx_build_jcs(N, jcs_alpha, jcs_ampl, jcs_p1, jcs_p2, deep, H.data(), Hd.data(), L.data(), Nop.data(),
+                                Aop.data(), K.data(), Ut.data()),
+                  nullptr, "qjx_build_jcs");
+        else if (deep_task)
             check(qjx_build_dimer_deep(N, J, U, E, A, g, omega, deep, nsub, H.data(), Hd.data(), L.data(), K.data(),
                                        Ut.data()),
                   nullptr, "qjx_build_dimer_deep");
@@ -360,10 +375,13 @@ int main(int argc, char **argv)
             }
         }
         std::vector<double> HE(2 * dd);
-        for (size_t e = 0; e < 2 * dd; e++) HE[e] = H[e] + E * Hd[e];
-        const std::vector<double> R =
+        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : H[e] + E * Hd[e];
+        std::vector<double> R =
             random_observables(d, num_robs, robs_seed, int(param_or(cp, "random_obs_mns", 1000000)),
                                int(param_or(cp, "random_obs_type", 0)));
+        const int robs_off = jcs ? 1 : 0;  // JCS: spec = <a> / alpha rides in observable slot 0
+        if (jcs) R.insert(R.begin(), Aop.begin(), Aop.end());
+        const int nr_eng = num_robs + robs_off;
 
         // dump schedule (init_dump_periods)
         // StdDeep: a dump after every sub-period, labelled with its period (init_dump_periods_deep,
@@ -387,8 +405,12 @@ int main(int argc, char **argv)
         cfg.deep = deep;
         cfg.num_branches = 2;
         cfg.num_diss = 1;
-        cfg.num_robs = num_robs;
-        cfg.T = 2.0 * 3.1415926535897932384626433832795 / omega;
+        cfg.num_robs = nr_eng;
+        cfg.T = jcs ? jcs_alpha : 2.0 * 3.1415926535897932384626433832795 / omega;
+        // JCS: branch b's head is jcs_drv_part_b * alpha and the branch lasts half of it
+        // (init_split_structure_jcs, core.cpp:10086-10124)
+        const double jcs_len[2] = {0.5 * (jcs_p1 * jcs_alpha), 0.5 * (jcs_p2 * jcs_alpha)};
+        cfg.branch_len = jcs ? jcs_len : nullptr;
         cfg.record = jump;
         cfg.rng_kind = int(param_or(cp, "rng_kind", 0));
         cfg.seed = (uint64_t)(uint32_t)cp.seed;
@@ -400,7 +422,7 @@ int main(int argc, char **argv)
         const double gr[1] = {1.0};  // head->g (core.cpp:9905)
         qjx_engine *h = nullptr;
         if (rp.prop_id == 0) {
-            check(qjx_create(&cfg, Ut.data(), L.data(), gr, HE.data(), num_robs ? R.data() : nullptr, &h), nullptr,
+            check(qjx_create(&cfg, Ut.data(), L.data(), gr, HE.data(), nr_eng ? R.data() : nullptr, &h), nullptr,
                   "qjx_create");
         } else {  // RK propagator: rk_right_part_dimer's drive keys (core.cpp:11048-11051)
             std::vector<double> He(2 * dd), Hdr(2 * dd);
@@ -534,15 +556,27 @@ int main(int argc, char **argv)
         D.disp.assign(nd_, 0.0);
         D.m2.assign(nd_, 0.0);
         D.energy.assign(nd_, 0.0);
-        D.robs.assign(nd_ * (num_robs ? num_robs : 1), 0.0);
+        D.robs.assign(nd_ * (nr_eng ? nr_eng : 1), 0.0);
         check(qjx_get_observables(h, 0, nrec, D.norm.data(), D.mean.data(), D.disp.data(), D.m2.data(), D.energy.data(),
-                                  num_robs ? reinterpret_cast<double *>(D.robs.data()) : nullptr, nullptr),
+                                  nr_eng ? reinterpret_cast<double *>(D.robs.data()) : nullptr, nullptr),
               h, "qjx_get_observables");
+        // JCS: spec = <a> / alpha (get_spec_jcs, experiment.cpp:1520-1562), mean = <a^+ a>
+        // (get_num_photons_jcs, experiment.cpp:2080-2160) from the energy slot
+        std::vector<std::complex<double>> spec(jcs ? nd_ : 0);
+        for (size_t i = 0; i < spec.size(); i++) {
+            const std::complex<double> a = D.robs[i * nr_eng];
+            spec[i] = std::complex<double>(a.real() / jcs_alpha, a.imag() / jcs_alpha);
+        }
         std::vector<double> mean_start(n);
         check(qjx_get_mean_start(h, mean_start.data()), h, "qjx_get_mean_start");
 
+        if (jcs && dump_obs == 1) {  // JCSCoreBehaviour::dump_std (core.cpp:2976-2999)
+            const size_t o = (size_t)last_dump * n;
+            save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
+            save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec.data() + o), n, 16, false);
+        }
         // dump_std (core.cpp:918-957): values of the last dump
-        if (dump_obs == 1) {
+        if (!jcs && dump_obs == 1) {
             const size_t o = (size_t)last_dump * n;
             save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
             save_double_data(path + "mean_start" + sfx, mean_start.data(), n, 16, false);
@@ -564,14 +598,24 @@ int main(int argc, char **argv)
                 save_2d_inv_double_data(path + name + sfx, inv.data(), ndt, n, 16, false);
             };
             evo(D.norm, "norm_evo");
-            evo(D.mean, "mean_evo");
-            evo(D.disp, "dispersion_evo");
-            evo(D.m2, "m2_evo");
-            evo(D.energy, "energy_evo");
+            if (jcs) {  // JCSCoreBehaviour::dump_std_evo (core.cpp:3034-3102)
+                std::vector<std::complex<double>> cinv((size_t)ndt * n);
+                for (int dmp = 0; dmp < nrec; dmp++)
+                    for (int tr = 0; tr < n; tr++) cinv[(size_t)tr * ndt + dmp] = spec[(size_t)dmp * n + tr];
+                save_2d_inv_complex_data(path + "spec_evo" + sfx, reinterpret_cast<const double *>(cinv.data()), ndt, n,
+                                         16, false);
+                evo(D.energy, "mean_evo");
+            } else {
+                evo(D.mean, "mean_evo");
+                evo(D.disp, "dispersion_evo");
+                evo(D.m2, "m2_evo");
+                evo(D.energy, "energy_evo");
+            }
             for (int o = 0; o < num_robs; o++) {
                 std::vector<std::vector<std::complex<double>>> v(n, std::vector<std::complex<double>>(nrec));
                 for (int tr = 0; tr < n; tr++)
-                    for (int dmp = 0; dmp < nrec; dmp++) v[tr][dmp] = D.robs[((size_t)dmp * n + tr) * num_robs + o];
+                    for (int dmp = 0; dmp < nrec; dmp++)
+                        v[tr][dmp] = D.robs[((size_t)dmp * n + tr) * nr_eng + robs_off + o];
                 save_2d_complex_vector(path + "random_obs_evo_" + std::to_string(robs_seed + o) + sfx, v, 16);
             }
             if (jump > 0) {

@@ -318,3 +318,92 @@ extern "C" qjx_status qjx_build_dimer_rk(int N, double J, double U, double E, do
     std::memcpy(H_drv, hd.data(), e2 * sizeof(double));
     return QJX_OK;
 }
+
+// JCS (sys_id 1): JCSNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp)
+//   init_sizes            :96-130   d = N, T = jcs_prm_alpha, one jump operator, two branches
+//   init_hamiltonians     :564-649  H = 0.5 / alpha^3 a^+ a^+ a a, H_drv = a^+ - a, special = a
+//   init_dissipators      :1546-1580 L = a
+//   init_hamiltonians_qj  :2499-2601 gamma = 1 / (4 alpha); H_eff = H - i/2 gamma L^H L;
+//                                     K_0 = -i H_eff + E0 H_drv (kick), K_1 = -i H_eff
+// init_split_structure_jcs (core.cpp:10086-10124): branch b's head is jcs_drv_part_b * T, so
+// U_{b,l} = exp(K_b head_b 2^-(l+2)) and branch b lasts head_b / 2.
+// Products of the ladder matrices follow the reference's dgemm order ((a^+ a^+) a) a; each entry
+// has a single nonzero term, so the order of the zero terms does not matter.
+static void real_matmul(int d, const std::vector<double> &A, const std::vector<double> &B, std::vector<double> &C)
+{
+    C.assign((size_t)d * d, 0.0);
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            double s = 0.0;
+            for (int k = 0; k < d; k++) s = s + A[(size_t)i * d + k] * B[(size_t)k * d + j];
+            C[(size_t)i * d + j] = s;
+        }
+}
+
+extern "C" qjx_status qjx_build_jcs(int N, double alpha, double drv_ampl, double part_1, double part_2, int deep,
+                                    double *H, double *Hd, double *L, double *Nop, double *A_op, double *Kout,
+                                    double *Utree)
+{
+    if (N < 2 || !(alpha > 0.0) || deep < 1 || !(part_1 > 0.0) || !(part_2 > 0.0)) return QJX_ERR_INVALID_ARG;
+    const int d = N;
+    const size_t dd = (size_t)d * d, e2 = 2 * dd;
+    std::vector<double> a(dd, 0.0), ad(dd, 0.0), m1, m2, m3, nop;
+    for (int k = 0; k < d - 1; k++) {
+        a[(size_t)k * d + (k + 1)] = std::sqrt(double(k + 1));
+        ad[(size_t)(k + 1) * d + k] = std::sqrt(double(k + 1));
+    }
+    real_matmul(d, ad, ad, m1);
+    real_matmul(d, m1, a, m2);
+    real_matmul(d, m2, a, m3);
+    real_matmul(d, ad, a, nop);  // get_num_photons_jcs (experiment.cpp:2080-2160)
+    cvec h(e2, 0.0), hd(e2, 0.0), l(e2, 0.0);
+    const double hs = 0.5 / std::pow(alpha, 3);
+    for (size_t e = 0; e < dd; e++) {
+        h[2 * e] = hs * m3[e];
+        hd[2 * e] = ad[e] - a[e];
+        l[2 * e] = a[e];
+    }
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (Hd) std::memcpy(Hd, hd.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), e2 * sizeof(double));
+    if (Nop)
+        for (size_t e = 0; e < dd; e++) {
+            Nop[2 * e] = nop[e];
+            Nop[2 * e + 1] = 0.0;
+        }
+    if (A_op) std::memcpy(A_op, l.data(), e2 * sizeof(double));
+    if (!Utree && !Kout) return QJX_OK;
+    const double gamma = 1.0 / (4.0 * alpha);
+    cvec K[2] = {cvec(e2), cvec(e2)};
+    const double Eb[2] = {drv_ampl, 0.0};
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            const size_t idx = (size_t)i * d + j;
+            double hr, hi;
+            heff_element(d, h, l, gamma, i, j, hr, hi);
+            for (int b = 0; b < 2; b++) {
+                K[b][2 * idx] = 0.0 + (hi + Eb[b] * hd[2 * idx]);
+                K[b][2 * idx + 1] = 0.0 - (hr + Eb[b] * 0.0);
+            }
+        }
+    if (Kout) {
+        std::memcpy(Kout, K[0].data(), e2 * sizeof(double));
+        std::memcpy(Kout + e2, K[1].data(), e2 * sizeof(double));
+    }
+    if (!Utree) return QJX_OK;
+    const double head[2] = {part_1 * alpha, part_2 * alpha};
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) collapse(2) reduction(&& : ok)
+    for (int b = 0; b < 2; b++)
+        for (int lv = 0; lv < deep; lv++) {
+            double dt = head[b] * 0.5;
+            for (int q = 0; q <= lv; q++) dt *= 0.5;
+            cvec scaled(e2);
+            for (size_t e = 0; e < dd; e++) {
+                scaled[2 * e] = K[b][2 * e] * dt;
+                scaled[2 * e + 1] = K[b][2 * e + 1] * dt;
+            }
+            ok = expm(d, scaled.data(), Utree + e2 * ((size_t)b * deep + lv)) && ok;
+        }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

@@ -53,8 +53,18 @@ def f_2d_complex(rows_by_cols):
 
 
 def suffix(cfg, prm):
-    """DimerOutputBehavior::suffix_param with precision 4 (outputter.cpp:3-44, 353-388)."""
+    """DimerOutputBehavior::suffix_param with precision 4 (outputter.cpp:3-44, 353-388);
+    JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 1:
+        return ("_setup(%d_%d_%d)" % (1, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_N(%d)" % int(prm["N"])
+                + "_diss(%d_%s_%s)" % (int(prm["diss_type"]), f4(prm["diss_gamma"]), f4(prm["diss_phase"]))
+                + "_drv(%s_%s_%s)" % (f4(prm["jcs_drv_part_1"]), f4(prm["jcs_drv_part_2"]), f4(prm["jcs_drv_ampl"]))
+                + "_prm(%s)" % f4(prm["jcs_prm_alpha"])
+                + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"]))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     return ("_setup(%d_%d_%d)" % (cfg.get("sys_id", 0), cfg.get("task_id", 0), cfg.get("prop_id", 0))
             + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
             + "_N(%d)" % int(prm["N"])
@@ -77,22 +87,35 @@ def expected_outputs(cfg, prm, R=None):
     if cfg.get("task_id", 1) == 7:
         return expected_lpn_outputs(cfg, prm, R)
     N = int(prm["N"])
-    d = N + 1
+    jcs = cfg.get("sys_id", 0) == 1
+    d = N if jcs else N + 1
     n = cfg["num_trajectories"]
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
     path = cfg.get("path", "")
     sfx = suffix(cfg, prm)
-    H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
-                                         prm["dimer_drv_ampl"], prm["diss_gamma"])
-    T = TWO_PI / prm["dimer_drv_freq"]
+    nr = int(prm["num_random_obs"])
     deep_task = cfg.get("task_id", 1) == 4
     nsub = int(prm.get("deep_num_steps", 0)) if deep_task else 0
-    t_head = 0.5 * T / nsub if deep_task else T  # init_split_structure_dimer_deep's branch dt
-    U = np.stack([O.split_tree(K0, t_head, deep), O.split_tree(K1, t_head, deep)])
-    HE = H + prm["dimer_prm_E"] * Hd
-    nr = int(prm["num_random_obs"])
-    ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, t_head, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
+    if jcs:  # JCS: kick and free evolution of heads part_b * alpha, spec = <a> / alpha, mean = <a^+ a>
+        alpha = prm["jcs_prm_alpha"]
+        H, Hd, L, Nop, K0, K1 = O.jcs_operators(N, alpha, prm["jcs_drv_ampl"])
+        heads = [prm["jcs_drv_part_1"] * alpha, prm["jcs_drv_part_2"] * alpha]
+        U = np.stack([O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)])
+        HE = Nop
+        Rs = np.concatenate([L[None], R]) if nr else L[None]
+        T = t_head = alpha
+        ens = O.Ensemble(U, L, [1.0], HE, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
+                         branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+    else:
+        H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
+                                             prm["dimer_drv_ampl"], prm["diss_gamma"])
+        T = TWO_PI / prm["dimer_drv_freq"]
+        t_head = 0.5 * T / nsub if deep_task else T  # init_split_structure_dimer_deep's branch dt
+        U = np.stack([O.split_tree(K0, t_head, deep), O.split_tree(K1, t_head, deep)])
+        HE = H + prm["dimer_prm_E"] * Hd
+        ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, t_head, n, seed=seed, record=int(prm["jump"]),
+                         rec_cap=100000)
     ens.init(int(prm["start_type"]), int(prm["start_state"]))
     prop = cfg.get("prop_id", 0)
     period = [0]  # the RK propagator's period_id, reset with the times after the transient
@@ -194,7 +217,15 @@ def expected_outputs(cfg, prm, R=None):
     last = obs[-1]
     if dump_purity == 1:
         emit("purity_evo" + sfx, f_double_data(purity), False)
-    if int(prm["dump_obs"]) == 1:
+    if jcs:
+        for o in obs:
+            z = o["random_obs"][:, 0]  # result.real /= alpha; result.imag /= alpha (real divisions)
+            o["spec"] = z.real / alpha + 1j * (z.imag / alpha)
+            o["random_obs"] = o["random_obs"][:, 1:]
+    if jcs and int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("spec" + sfx, f_complex_data(last["spec"]), False)
+    if not jcs and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
         emit("mean" + sfx, f_double_data(last["mean"]), False)
@@ -209,12 +240,20 @@ def expected_outputs(cfg, prm, R=None):
             emit("phi_evo_%d" % tr + sfx, f_complex_data(ens.phi[tr]), True)
     if evo_sep == 1 and int(prm["dump_obs"]) == 1:
         emit("periods" + sfx, f_int_data(dp), False)
-        for key, name in (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"),
-                          ("m2", "m2_evo"), ("energy", "energy_evo")):
+        keys = ((("norm", "norm_evo"), ("energy", "mean_evo")) if jcs else
+                (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
+                 ("energy", "energy_evo")))
+        for key, name in keys:
             grid = np.zeros((ndt, n))
             for i, o in enumerate(obs):
                 grid[i] = o[key]
             emit(name + sfx, f_2d_inv(grid), False)
+        if jcs:
+            grid = np.zeros((ndt, n), complex)
+            for i, o in enumerate(obs):
+                grid[i] = o["spec"]
+            emit("spec_evo" + sfx, "".join("".join(fmt_double(z.real) + " " + fmt_double(z.imag) + " " for z in row)
+                                           + "\n" for row in grid), False)
         for o_id in range(nr):
             rows = [o["random_obs"][:, o_id] for o in obs]
             emit("random_obs_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
@@ -362,6 +401,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
         emit("adr_avg" + sfx, f_double_data(adr_avg(last["adr"], half)), False)
     return acc
 
+
+JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_1": 0.5, "jcs_drv_part_2": 1.5}
 
 LPN_PARAMS = {
     "lpn_type": 0, "lpn_eps_deep": 100, "lpn_eps_error": 1.0e-10, "lpn_eps_high": 10, "lpn_eps_low": -10,

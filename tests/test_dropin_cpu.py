@@ -5,7 +5,7 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, LPN_PARAMS, config_text, params_text, suffix
+from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, config_text, params_text, suffix
 
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
 
@@ -55,6 +55,17 @@ def test_lpn_suffix_matches_reference_rule(tmp_path, over):
     assert r.returncode == 0, r.stdout
     line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
     assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_lpn(" in line
+
+
+@pytest.mark.parametrize("over", [{}, {"jcs_drv_part_1": 1.25, "jcs_drv_ampl": 0.05, "diss_type": 1}])
+def test_jcs_suffix_matches_reference_rule(tmp_path, over):
+    """JCSOutputBehavior::suffix_param (outputter.cpp:95-133)."""
+    cfg = dict(BASE_CONFIG, sys_id=1)
+    prm = {**BASE_PARAMS, **JCS_PARAMS, **over}
+    r = check(tmp_path, cfg, prm)
+    assert r.returncode == 0, r.stdout
+    line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
+    assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_prm(5.0000)" in line
 
 
 @pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 9), ("prop_id", 2)])

@@ -7,7 +7,8 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, LPN_PARAMS, config_text, expected_outputs, params_text
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, config_text, expected_outputs,
+                                 params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -21,6 +22,7 @@ def run_case(tmp_path, cfg, prm):
     r = subprocess.run([EXE], cwd=tmp_path, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     d = int(prm["N"]) + 1
+    d = int(prm["N"]) if cfg.get("sys_id", 0) == 1 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -103,3 +105,12 @@ def test_lpn_mult_every_period_rk(tmp_path):
     prm = {**BASE_PARAMS, **LPN_PARAMS, "lpn_type": -1, "lambda_per_periods": 1, "dump_type": 1, "dump_num": 2,
            "dump_evo_avg": 1, "dump_adr_avg": 1, "num_random_obs": 2}
     run_case(tmp_path, cfg, prm)
+
+
+def test_jcs_system_files_match(tmp_path):
+    """The JCS system (sys_id 1): kick and free evolution of unequal duration, spec = <a> / alpha,
+    mean = <a^+ a> (newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601; core.cpp:2739-3102)."""
+    cfg = dict(BASE_CONFIG, sys_id=1, num_trajectories=16, num_tp_periods=1, num_obs_periods=4, is_debug=1)
+    prm = {**BASE_PARAMS, **JCS_PARAMS, "dump_num": 2, "jump": 2, "dump_adr_sep": 1, "dump_adr_avg": 1}
+    exp = run_case(tmp_path, cfg, prm)
+    assert any(k.startswith("spec_evo") for k in exp) and any(k.startswith("jump_times_") and exp[k] for k in exp)
