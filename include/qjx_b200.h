@@ -224,6 +224,15 @@ qjx_status qjx_lpn_get(qjx_engine *h, double *lambda_now, double *lambda, double
  * bisection halvings and the perturbation size eps; any pointer may be NULL. */
 qjx_status qjx_lpn_get_last(qjx_engine *h, int *renormed, double *ratio, double *delta_s, double *delta_f,
                             int *eps_iters, double *eps);
+/* Checkpoint / resume (preemption): the complete trajectory state between run calls -- every
+ * state slot, the per-trajectory records (times, thresholds, RNG cursors, branch / level,
+ * jump counters), channel weights, mean_start, the period counter and, when started, the
+ * Lyapunov arrays -- as one host blob.  Loading it into an engine created with the same
+ * configuration continues the run bit for bit (jump records already drained to the host are
+ * not part of the blob).  QJX has no checkpoint (its only resume is skipping finished jobs). */
+qjx_status qjx_checkpoint_size(qjx_engine *h, size_t *bytes);
+qjx_status qjx_checkpoint_save(qjx_engine *h, void *buf, size_t bytes);
+qjx_status qjx_checkpoint_load(qjx_engine *h, const void *buf, size_t bytes);
 /* Per-CTA trace of the micro-step kernel (profiling aid, off by default): enabling clears
  * and starts accumulating, per persistent CTA, clock64 cycles {total, setup, (reserved),
  * MMA loop, epilogue} and counts {sub-tiles, 8-column blocks, columns}.  qjx_get_trace

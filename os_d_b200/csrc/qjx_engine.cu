@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/qjx_b200.h"
 #include "qjx_device.cuh"
 
@@ -34,6 +36,12 @@ size_t split_stage_bytes(int MDs);
 cudaError_t launch_lpn(const Params &P, const LpnParams &L, int mode, double curr_time, int adr_dump,
                        cudaStream_t st);
 }  // namespace qjx
+
+// NVTX range around a host call (visible in Nsight Systems timelines; free when no tool is attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 using namespace qjx;
 
@@ -739,6 +747,7 @@ extern "C" qjx_status qjx_create_slots(const qjx_config *cfg, int n_slots, int d
 
 extern "C" qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble *e, const double *psi)
 {
+    NvtxRange range("qjx_slot_load");
     if (!h || !e) return QJX_ERR_INVALID_ARG;
     if (!h->d_active || slot < 0 || slot >= h->n_ens) return fail(h, QJX_ERR_INVALID_ARG, "not a slot of a serving engine");
     if (h->slot_n[slot]) return fail(h, QJX_ERR_STATE, "slot in use: release it first");
@@ -850,6 +859,7 @@ extern "C" qjx_status qjx_create_rk(const qjx_config *cfg, const double *H_eff, 
 extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, const int *dump_at, int n_dumps,
                                       int dump_base)
 {
+    NvtxRange range("qjx_run_periods");
     if (!h || n_periods < 0 || n_dumps < 0 || (n_dumps > 0 && !dump_at)) return QJX_ERR_INVALID_ARG;
     if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
     if (dump_base < 0 || dump_base + n_dumps > h->cfg.max_dumps)
@@ -891,6 +901,7 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
 
 extern "C" qjx_status qjx_observe(qjx_engine *h, int dump, int is_start)
 {
+    NvtxRange range("qjx_observe");
     if (!h || dump < 0 || dump >= h->cfg.max_dumps) return QJX_ERR_INVALID_ARG;
     if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
     CK(cudaSetDevice(h->cfg.device));
@@ -1080,6 +1091,7 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
 
 extern "C" qjx_status qjx_lpn_period(qjx_engine *h, double curr_time, int adr_dump)
 {
+    NvtxRange range("qjx_lpn_period");
     if (!h) return QJX_ERR_INVALID_ARG;
     if (!h->lpn_started) return fail(h, QJX_ERR_STATE, "qjx_lpn_start first");
     if (adr_dump < -1 || adr_dump >= h->cfg.max_dumps) return fail(h, QJX_ERR_INVALID_ARG, "adr_dump out of range");
@@ -1123,6 +1135,108 @@ extern "C" qjx_status qjx_lpn_get_last(qjx_engine *h, int *renormed, double *rat
     if (delta_f) CK(cudaMemcpy(delta_f, L.df_rec, n * sizeof(double), cudaMemcpyDeviceToHost));
     if (eps_iters) CK(cudaMemcpy(eps_iters, L.eps_iters, n * sizeof(int), cudaMemcpyDeviceToHost));
     if (eps) CK(cudaMemcpy(eps, L.eps, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return QJX_OK;
+}
+
+// ---------------------------------------------------------------- checkpoint / resume
+namespace {
+struct CkptHeader {
+    uint64_t magic;  // 'QJXCKPT1'
+    int n, MD, slots, nd, E, lpn, nr, period_base;
+};
+constexpr uint64_t kCkptMagic = 0x3154504b43584a51ULL;
+
+// (device pointer, bytes) of every array a checkpoint carries, in blob order
+std::vector<std::pair<void *, size_t>> ckpt_parts(qjx_engine *h)
+{
+    const Params &P = h->P;
+    const size_t n = P.n;
+    const int slots = P.prop == 1 ? kRkSlots : 2;
+    std::vector<std::pair<void *, size_t>> v = {
+        {P.psi, (size_t)slots * n * P.MD * sizeof(double2)},
+        {P.st, n * sizeof(TrajState)},
+        {P.gn, n * P.nd * sizeof(double)},
+        {P.mean_start, n * sizeof(double)},
+    };
+    if (h->lpn_alloc) {
+        const LpnParams &L = h->L;
+        v.push_back({L.lambda, n * sizeof(double)});
+        v.push_back({L.lambda_now, n * sizeof(double)});
+        v.push_back({L.delta_s_v, n * sizeof(double)});
+        v.push_back({L.mean_lpn, n * sizeof(double)});
+        v.push_back({L.energy_lpn, n * sizeof(double)});
+        v.push_back({L.robs_lpn, n * std::max(1, P.nr) * sizeof(double2)});
+        v.push_back({L.num_renorms, n * sizeof(int)});
+        v.push_back({L.var_pos, n * sizeof(long long)});
+    }
+    if (h->d_active) v.push_back({h->d_active, n});
+    return v;
+}
+}  // namespace
+
+extern "C" qjx_status qjx_checkpoint_size(qjx_engine *h, size_t *bytes)
+{
+    if (!h || !bytes) return QJX_ERR_INVALID_ARG;
+    size_t b = sizeof(CkptHeader);
+    for (const auto &p : ckpt_parts(h)) b += p.second;
+    *bytes = b;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_checkpoint_save(qjx_engine *h, void *buf, size_t bytes)
+{
+    size_t need = 0;
+    if (!h || !buf || qjx_checkpoint_size(h, &need) != QJX_OK || bytes < need) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "nothing to checkpoint: qjx_set_states first");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaStreamSynchronize(h->stream));
+    const Params &P = h->P;
+    CkptHeader hd{kCkptMagic, P.n, P.MD, P.prop == 1 ? kRkSlots : 2, P.nd, P.E, h->lpn_alloc ? 1 : 0, P.nr,
+                  h->period_base};
+    unsigned char *o = static_cast<unsigned char *>(buf);
+    std::memcpy(o, &hd, sizeof(hd));
+    o += sizeof(hd);
+    for (const auto &p : ckpt_parts(h)) {
+        CK(cudaMemcpy(o, p.first, p.second, cudaMemcpyDeviceToHost));
+        o += p.second;
+    }
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_checkpoint_load(qjx_engine *h, const void *buf, size_t bytes)
+{
+    if (!h || !buf || bytes < sizeof(CkptHeader)) return QJX_ERR_INVALID_ARG;
+    CkptHeader hd;
+    std::memcpy(&hd, buf, sizeof(hd));
+    const Params &P = h->P;
+    if (hd.magic != kCkptMagic || hd.n != P.n || hd.MD != P.MD || hd.slots != (P.prop == 1 ? kRkSlots : 2) ||
+        hd.nd != P.nd || hd.E != P.E || hd.nr != P.nr)
+        return fail(h, QJX_ERR_INVALID_ARG, "checkpoint of a different engine configuration");
+    if (hd.lpn && !h->lpn_alloc)
+        return fail(h, QJX_ERR_STATE, "checkpoint carries the Lyapunov task: qjx_lpn_start this engine first");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaStreamSynchronize(h->stream));
+    const unsigned char *in = static_cast<const unsigned char *>(buf) + sizeof(hd);
+    const unsigned char *end = static_cast<const unsigned char *>(buf) + bytes;
+    for (const auto &p : ckpt_parts(h)) {
+        const bool lpn_part = h->lpn_alloc && (p.first == h->L.lambda || p.first == h->L.lambda_now ||
+                                               p.first == h->L.delta_s_v || p.first == h->L.mean_lpn ||
+                                               p.first == h->L.energy_lpn || p.first == h->L.robs_lpn ||
+                                               p.first == h->L.num_renorms || p.first == h->L.var_pos);
+        if (lpn_part && !hd.lpn) continue;
+        if (in + p.second > end) return fail(h, QJX_ERR_INVALID_ARG, "truncated checkpoint");
+        CK(cudaMemcpy(p.first, in, p.second, cudaMemcpyHostToDevice));
+        in += p.second;
+    }
+    h->period_base = hd.period_base;
+    h->states_set = true;
+    if (hd.lpn) h->lpn_started = true;
+    for (int i = 0; i < P.n; i++) {
+        h->jt[i].clear();
+        h->jn[i].clear();
+        h->je[i].clear();
+        h->jtype[i].clear();
+    }
     return QJX_OK;
 }
 

@@ -270,6 +270,19 @@ class Engine:
         out["eps_iters"] = it
         return out
 
+    def checkpoint(self):
+        """The engine's complete trajectory state as bytes (qjx_checkpoint_save)."""
+        size = C.c_size_t()
+        self._chk(N.lib().qjx_checkpoint_size(self.h, C.byref(size)), "qjx_checkpoint_size")
+        buf = C.create_string_buffer(size.value)
+        self._chk(N.lib().qjx_checkpoint_save(self.h, buf, size.value), "qjx_checkpoint_save")
+        return buf.raw
+
+    def restore(self, blob):
+        """Continue from a checkpoint of an engine with the same configuration."""
+        buf = C.create_string_buffer(blob, len(blob))
+        self._chk(N.lib().qjx_checkpoint_load(self.h, buf, len(blob)), "qjx_checkpoint_load")
+
     def set_trace(self, enable=True):
         self._chk(N.lib().qjx_set_trace(self.h, int(enable)), "qjx_set_trace")
 
