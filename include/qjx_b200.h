@@ -191,7 +191,11 @@ qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats);
 qjx_status qjx_set_active(qjx_engine *h, int n_active);
 
 /* Lyapunov paired trajectories (task_id 7, LpnMult; experiment.cpp:138-286).  n_traj is even;
- * trajectories [0, n/2) are the bases and n/2 + b is the variation of base b. */
+ * trajectories [0, n/2) are the bases and n/2 + b is the variation of base b -- in a batched engine
+ * within every ensemble (each with an even n_traj), so a whole parameter sweep runs as one batch.
+ * qjx_set_bases_only(h, 1): later run calls advance the bases of every ensemble only (the
+ * transient); 0 restores all. */
+qjx_status qjx_set_bases_only(qjx_engine *h, int on);
 typedef struct {
     int lpn_type;         /* -1 mean, -2 energy, k >= 0 random observable k (calc_delta_s, core.cpp:839-901) */
     int eps_deep;         /* lpn_eps_deep: bisection halvings at most */

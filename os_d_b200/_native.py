@@ -22,7 +22,7 @@ EXPORTS = [
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
     "qjx_random_observables", "qjx_build_jcs", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
-    "qjx_set_active", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
+    "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
@@ -95,6 +95,7 @@ def lib():
         L.qjx_get_stats.argtypes = [vp, C.POINTER(QjxStats)]
         L.qjx_set_trace.argtypes = [vp, C.c_int]
         L.qjx_set_active.argtypes = [vp, C.c_int]
+        L.qjx_set_bases_only.argtypes = [vp, C.c_int]
         L.qjx_checkpoint_size.argtypes = [vp, C.POINTER(C.c_size_t)]
         L.qjx_checkpoint_save.argtypes = [vp, vp, C.c_size_t]
         L.qjx_checkpoint_load.argtypes = [vp, vp, C.c_size_t]

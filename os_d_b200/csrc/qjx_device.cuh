@@ -180,6 +180,8 @@ struct LpnParams {
     double *ratio, *ds_rec, *df_rec;                                  // [n] last call
     int *eps_iters;                                                   // [n] last bisection
     double *eps;                                                      // [n] last bisection
+    const int *pair0;                                                 // [E + 1] first pair of each ensemble
+    int pairs;                                                        // sum over ensembles of n_e / 2
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns

@@ -72,6 +72,8 @@ struct qjx_engine {
     int period_base = 0;  // periods run since the last time reset (the RK propagator's period_id)
     int n_ens = 1;        // ensembles (qjx_create_batch)
     std::vector<double> branch_len;   // copy of qjx_config.branch_len
+    std::vector<int> e_tr0;           // host copy of the ensembles' first trajectories [E + 1]
+    unsigned char *d_bases = nullptr; // Lyapunov transient mask (bases of every ensemble)
     // serving engines (qjx_create_slots): every ensemble is a slot with room for d_cap and n_cap
     int slot_dcap = 0, slot_ncap = 0;
     std::vector<int> slot_n;          // trajectories of the loaded ensemble (0: free)
@@ -358,6 +360,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     if (!mats) return bail(QJX_ERR_OOM);
     cudaMemcpy(mats, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
     P.mats = mats;
+    h->e_tr0 = e_tr0;
     P.e_d = upload(h, e_d);
     P.e_nc = upload(h, e_nc);
     P.e_kb = upload(h, e_kb);
@@ -1032,13 +1035,39 @@ extern "C" qjx_status qjx_set_active(qjx_engine *h, int n_active)
     return QJX_OK;
 }
 
+extern "C" qjx_status qjx_set_bases_only(qjx_engine *h, int on)
+{
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (h->d_active) return fail(h, QJX_ERR_UNSUPPORTED, "serving engines keep their slot mask");
+    CK(cudaSetDevice(h->cfg.device));
+    if (!on) {
+        h->P.active = nullptr;
+        return QJX_OK;
+    }
+    if (!h->d_bases) {
+        std::vector<unsigned char> m(h->P.n, 0);
+        for (int e = 0; e < h->n_ens; e++) {
+            const int t0 = h->e_tr0[e], half = (h->e_tr0[e + 1] - t0) / 2;
+            for (int i = 0; i < half; i++) m[t0 + i] = 1;
+        }
+        h->d_bases = upload(h, m);
+        if (!h->d_bases) return fail(h, QJX_ERR_OOM, "bases mask");
+    }
+    h->P.active = h->d_bases;
+    return QJX_OK;
+}
+
 extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
 {
     if (!h || !c) return QJX_ERR_INVALID_ARG;
     if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
     const Params &P = h->P;
-    if (h->n_ens != 1) return fail(h, QJX_ERR_UNSUPPORTED, "the Lyapunov task takes a single-ensemble engine");
-    if (P.n < 2 || (P.n & 1)) return fail(h, QJX_ERR_INVALID_ARG, "the Lyapunov task needs an even n_traj >= 2");
+    if (h->d_active) return fail(h, QJX_ERR_UNSUPPORTED, "the Lyapunov task does not run on serving slots");
+    for (int e = 0; e < h->n_ens; e++) {
+        const int ne = h->e_tr0[e + 1] - h->e_tr0[e];
+        if (ne < 2 || (ne & 1))
+            return fail(h, QJX_ERR_INVALID_ARG, "the Lyapunov task needs an even n_traj >= 2 in every ensemble");
+    }
     if (!(c->lpn_type == -1 || c->lpn_type == -2 || (c->lpn_type >= 0 && c->lpn_type < P.nr)))
         return fail(h, QJX_ERR_INVALID_ARG, "lpn_type must be -1, -2 or a random observable index");
     if (P.nr > 64) return fail(h, QJX_ERR_UNSUPPORTED, "the Lyapunov task takes at most 64 random observables");
@@ -1061,8 +1090,13 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
         L.df_rec = (double *)dalloc(h, n * sizeof(double));
         L.eps_iters = (int *)dalloc(h, n * sizeof(int));
         L.eps = (double *)dalloc(h, n * sizeof(double));
+        std::vector<int> pair0(h->n_ens + 1, 0);
+        for (int e = 0; e < h->n_ens; e++) pair0[e + 1] = pair0[e] + (h->e_tr0[e + 1] - h->e_tr0[e]) / 2;
+        L.pair0 = upload(h, pair0);
+        L.pairs = pair0[h->n_ens];
         if (!L.lambda || !L.lambda_now || !L.delta_s_v || !L.mean_lpn || !L.energy_lpn || !L.robs_lpn ||
-            !L.num_renorms || !L.var_pos || !L.renormed || !L.ratio || !L.ds_rec || !L.df_rec || !L.eps_iters || !L.eps)
+            !L.num_renorms || !L.var_pos || !L.renormed || !L.ratio || !L.ds_rec || !L.df_rec || !L.eps_iters || !L.eps ||
+            !L.pair0)
             return fail(h, QJX_ERR_OOM, "Lyapunov arrays");
         h->lpn_alloc = true;
     }

@@ -105,10 +105,17 @@ struct LpnShared {
     double red[4];  // [0] norm of the state under study, [1] |w|^2, [2] |base|^2
 };
 
-__device__ __forceinline__ void cta_matvec(const Params &P, int g, const double2 *x, double2 *y)
+// The pair's ensemble: dimension, padded rows of its matrices, first group and the offset from a
+// trajectory index to its Philox stream.
+struct EnsCtx {
+    int d, MD, g0;
+    long long sbase;
+};
+
+__device__ __forceinline__ void cta_matvec(const Params &P, const EnsCtx &E, int g, const double2 *x, double2 *y)
 {
-    const int d = P.d, MD = P.MD, kp = (d + 1) & ~1;
-    const double2 *mat = P.mats + (size_t)g * kp * MD;
+    const int d = E.d, MD = E.MD;
+    const double2 *mat = P.mats + P.g_off[E.g0 + g];
     for (int r = threadIdx.x; r < d; r += blockDim.x) {
         double re = 0.0, im = 0.0;
         for (int k = 0; k < d; k++) {
@@ -126,10 +133,10 @@ __device__ __forceinline__ void cta_matvec(const Params &P, int g, const double2
 // calc_chars_lpn / calc_chars_std of `phi` (core.cpp:697-785) for the parts in `want` (robs_one
 // >= 0: that random observable only) into `c`; the canonical norm is left in sh.red[0].  Ends
 // with a barrier, so every thread may read `c` afterwards.
-__device__ void cta_chars(const Params &P, const double2 *phi, int want, int robs_one, double2 *xh, double2 *y,
-                          LpnShared &sh, LpnChars &c, double *adr_out)
+__device__ void cta_chars(const Params &P, const EnsCtx &E, const double2 *phi, int want, int robs_one, double2 *xh,
+                          double2 *y, LpnShared &sh, LpnChars &c, double *adr_out)
 {
-    const int d = P.d, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int d = E.d, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (warp == 0) {
         const double nrm = warp_norm(phi, d, lane);
         if (lane == 0) sh.red[0] = nrm;
@@ -155,7 +162,7 @@ __device__ void cta_chars(const Params &P, const double2 *phi, int want, int rob
     }
     __syncthreads();
     if (want & CH_ENERGY) {
-        cta_matvec(P, P.gHE, xh, y);
+        cta_matvec(P, E, P.gHE, xh, y);
         __syncthreads();
         if (warp == 0) {
             double es = 0.0;
@@ -170,7 +177,7 @@ __device__ void cta_chars(const Params &P, const double2 *phi, int want, int rob
     }
     for (int o = 0; o < P.nr; o++) {
         if (!(want & CH_ROBS_ALL) && o != robs_one) continue;
-        cta_matvec(P, P.gR0 + o, xh, y);
+        cta_matvec(P, E, P.gR0 + o, xh, y);
         __syncthreads();
         if (warp == 0) {
             double pr = 0.0, pi = 0.0;
@@ -194,10 +201,10 @@ __device__ __forceinline__ int delta_want(int lpn_type)
 }
 
 // calc_delta_s / calc_delta_f (core.cpp:839-901), variation v against base b
-__device__ __forceinline__ double lpn_delta(const Params &P, const LpnParams &L, const LpnChars &v,
+__device__ __forceinline__ double lpn_delta(const EnsCtx &E, const LpnParams &L, const LpnChars &v,
                                             const LpnChars &b)
 {
-    if (L.lpn_type == -1) return __ddiv_rn(fabs(__dsub_rn(v.mean, b.mean)), (double)P.d);
+    if (L.lpn_type == -1) return __ddiv_rn(fabs(__dsub_rn(v.mean, b.mean)), (double)E.d);
     if (L.lpn_type == -2) return __ddiv_rn(fabs(__dsub_rn(v.energy, b.energy)), L.max_energy);
     const double2 bb = b.robs[L.lpn_type], vv = v.robs[L.lpn_type];
     const double dr = __dsub_rn(bb.x, vv.x), di = __dsub_rn(bb.y, vv.y);
@@ -209,12 +216,12 @@ __device__ __forceinline__ double lpn_delta(const Params &P, const LpnParams &L,
 // parts), |w| = 1, and eps = 10^m bisected in m until |delta_s - target| < eps_error or
 // eps_deep halvings; a delta_s that is neither above nor below the target ends the search.
 // Leaves the perturbed state in pv.
-__device__ void var_trajectory(const Params &P, const LpnParams &L, int v, const double2 *pb, double2 *pv,
-                               double2 *w, double2 *xh, double2 *y, LpnShared &sh)
+__device__ void var_trajectory(const Params &P, const EnsCtx &E, const LpnParams &L, int v, const double2 *pb,
+                               double2 *pv, double2 *w, double2 *xh, double2 *y, LpnShared &sh)
 {
-    const int d = P.d, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int d = E.d, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long pos0 = L.var_pos[v];
-    const unsigned long long stream = (1ULL << 63) | (unsigned long long)(P.tr_base + v);
+    const unsigned long long stream = (1ULL << 63) | (unsigned long long)(E.sbase + v);
     for (int st = threadIdx.x; st < d; st += blockDim.x) {
         const double ur = philox_uniform(777ULL, stream, (unsigned long long)(pos0 + st));
         const double ui = philox_uniform(777ULL, stream, (unsigned long long)(pos0 + d + st));
@@ -259,8 +266,8 @@ __device__ void var_trajectory(const Params &P, const LpnParams &L, int v, const
             pv[st] = make_double2(__dmul_rn(__ddiv_rn(a.x, sm), s2), __dmul_rn(__ddiv_rn(a.y, sm), s2));
         }
         __syncthreads();
-        cta_chars(P, pv, want, one, xh, y, sh, sh.vc, nullptr);
-        const double ds = lpn_delta(P, L, sh.vc, sh.bc);
+        cta_chars(P, E, pv, want, one, xh, y, sh, sh.vc, nullptr);
+        const double ds = lpn_delta(E, L, sh.vc, sh.bc);
         if (fabs(__dsub_rn(ds, L.delta_s)) < L.eps_error) break;
         if (ds > L.delta_s) {
             hi = __dsub_rn(hi, __dmul_rn(0.5, diff));
@@ -300,8 +307,18 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
     double2 *pb = reinterpret_cast<double2 *>(smem + ((sizeof(LpnShared) + 15) & ~(size_t)15));
     double2 *pv = pb + P.MD, *w = pv + P.MD, *xh = w + P.MD, *y = xh + P.MD;
     double *adr = reinterpret_cast<double *>(y + P.MD);
-    const int d = P.d, half = P.n / 2;
-    const int b = blockIdx.x, v = half + b;
+    // pair -> its ensemble e (pairs of ensemble e are pair0[e] .. pair0[e + 1] - 1): base b and
+    // variation v = b + n_e / 2 of that ensemble
+    int lo = 0, hi = P.E;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (L.pair0[mid] <= (int)blockIdx.x) lo = mid;
+        else hi = mid;
+    }
+    const int t0 = P.e_tr0[lo], half = (P.e_tr0[lo + 1] - t0) / 2;
+    const int b = t0 + (int)blockIdx.x - L.pair0[lo], v = b + half;
+    const EnsCtx E{P.e_d[lo], 8 * ((P.e_d[lo] + 7) / 8), P.e_g0[lo], P.e_sbase[lo] - t0};
+    const int d = E.d;
     const TrajState sb = P.st[b];
     TrajState sv = P.st[v];
     if (sb.phase == PH_ERROR || sv.phase == PH_ERROR) return;
@@ -313,7 +330,7 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
     }
     __syncthreads();
     const int full = CH_MEAN | CH_ENERGY | CH_ROBS_ALL;
-    cta_chars(P, pb, full, -1, xh, y, sh, sh.bc, nullptr);  // calc_chars_lpn of the base
+    cta_chars(P, E, pb, full, -1, xh, y, sh, sh.bc, nullptr);  // calc_chars_lpn of the base
     store_chars(P, L, b, sh.bc);
     bool moved = false;
     if (mode == 0) {
@@ -323,12 +340,12 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
         sv.eta = sb.eta;
         for (int st = threadIdx.x; st < d; st += blockDim.x) pv[st] = pb[st];
         __syncthreads();
-        var_trajectory(P, L, v, pb, pv, w, xh, y, sh);
+        var_trajectory(P, E, L, v, pb, pv, w, xh, y, sh);
         moved = true;
-        cta_chars(P, pv, full, -1, xh, y, sh, sh.vc, nullptr);
+        cta_chars(P, E, pv, full, -1, xh, y, sh, sh.vc, nullptr);
         store_chars(P, L, v, sh.vc);
         if (threadIdx.x == 0) {
-            L.delta_s_v[v] = lpn_delta(P, L, sh.vc, sh.bc);
+            L.delta_s_v[v] = lpn_delta(E, L, sh.vc, sh.bc);
             L.delta_s_v[b] = 0.0;
             L.lambda[b] = L.lambda[v] = 0.0;
             L.lambda_now[b] = L.lambda_now[v] = 0.0;
@@ -337,8 +354,8 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
         }
     } else {
         const int want = delta_want(L.lpn_type), one = L.lpn_type >= 0 ? L.lpn_type : -1;
-        cta_chars(P, pv, want, one, xh, y, sh, sh.vc, nullptr);
-        const double df = lpn_delta(P, L, sh.vc, sh.bc);
+        cta_chars(P, E, pv, want, one, xh, y, sh, sh.vc, nullptr);
+        const double df = lpn_delta(E, L, sh.vc, sh.bc);
         const double ds = L.delta_s_v[v];
         const double ds10 = __dmul_rn(ds, 10.0);
         const double lim = (L.delta_f_high < ds10) ? ds10 : L.delta_f_high;  // std::max
@@ -349,9 +366,9 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
             sv.rng_src = sb.rng_src;  // copy_stream_lpn
             sv.rng_pos = sb.rng_pos;
             sv.eta = sb.eta;
-            var_trajectory(P, L, v, pb, pv, w, xh, y, sh);
+            var_trajectory(P, E, L, v, pb, pv, w, xh, y, sh);
             moved = true;
-            cta_chars(P, pv, full, -1, xh, y, sh, sh.vc, nullptr);
+            cta_chars(P, E, pv, full, -1, xh, y, sh, sh.vc, nullptr);
             store_chars(P, L, v, sh.vc);
             if (threadIdx.x == 0) {
                 L.lambda[v] = lam;
@@ -360,11 +377,11 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
                 L.ratio[v] = ratio;
                 L.ds_rec[v] = ds;
                 L.df_rec[v] = df;
-                L.delta_s_v[v] = lpn_delta(P, L, sh.vc, sh.bc);
+                L.delta_s_v[v] = lpn_delta(E, L, sh.vc, sh.bc);
                 L.lambda_now[v] = __ddiv_rn(lam, curr_time);
             }
         } else {
-            cta_chars(P, pv, full, -1, xh, y, sh, sh.vc, nullptr);
+            cta_chars(P, E, pv, full, -1, xh, y, sh, sh.vc, nullptr);
             store_chars(P, L, v, sh.vc);
             if (threadIdx.x == 0) {
                 L.renormed[v] = 0;
@@ -378,8 +395,8 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
         if (threadIdx.x == 0) P.st[v] = sv;
     }
     if (adr_dump >= 0 && P.o_adr) {
-        double *dst = P.keep_adr ? P.o_adr + ((size_t)adr_dump * P.n + v) * d : P.o_adr + (size_t)v * d;
-        cta_chars(P, pv, CH_MEAN, -1, xh, y, sh, sh.vc, adr);
+        double *dst = P.keep_adr ? P.o_adr + ((size_t)adr_dump * P.n + v) * P.d : P.o_adr + (size_t)v * P.d;
+        cta_chars(P, E, pv, CH_MEAN, -1, xh, y, sh, sh.vc, adr);
         for (int st = threadIdx.x; st < d; st += blockDim.x) dst[st] = adr[st];
     }
 }
@@ -392,7 +409,7 @@ size_t lpn_smem_bytes(int MD)
 cudaError_t launch_lpn(const Params &P, const LpnParams &L, int mode, double curr_time, int adr_dump,
                        cudaStream_t st)
 {
-    const int pairs = P.n / 2;
+    const int pairs = L.pairs;
     if (pairs == 0) return cudaSuccess;
     const size_t smem = lpn_smem_bytes(P.MD);
     if (smem > 48 * 1024) {

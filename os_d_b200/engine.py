@@ -234,6 +234,10 @@ class Engine:
         """Later run_periods calls advance trajectories [0, n_active) only."""
         self._chk(N.lib().qjx_set_active(self.h, int(n_active)), "qjx_set_active")
 
+    def set_bases_only(self, on=True):
+        """Later run_periods calls advance the Lyapunov bases of every ensemble only."""
+        self._chk(N.lib().qjx_set_bases_only(self.h, int(on)), "qjx_set_bases_only")
+
     # ---------------------------------------------------------- Lyapunov task (task_id 7)
     def lpn_start(self, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10, delta_s=1e-3,
                   delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0):

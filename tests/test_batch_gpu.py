@@ -88,3 +88,44 @@ def test_batch_of_one_is_the_ordinary_engine():
     for x1, x2 in zip(ob, oa):
         for k in x1:
             assert np.array_equal(x1[k], x2[k]), k
+
+
+def test_batched_lyapunov_sweep_equals_single_runs():
+    """LpnMult over a batch of parameter points (the production sweep as one launch): every
+    ensemble's states and Lyapunov values equal its own single-ensemble run, bit for bit."""
+    import os_d_b200 as q
+    from tests.test_lpn_cpu import CFGS
+
+    cfg = dict(CFGS[1])
+    deep = 10
+    specs = [(20, 1.0, 0.1, 3, 10, 0), (33, 1.0, 0.3, 4, 14, 50), (12, 0.5, 0.05, 5, 8, 7)]
+    ens = [ensemble(N, E0, gm, sd, n, deep, tb, U=0.3 + 0.1 * i) for i, (N, E0, gm, sd, n, tb) in enumerate(specs)]
+
+    def flow(eng, rows):
+        psi = np.zeros((eng.n, rows), complex)
+        psi[:, 0] = 1.0
+        eng.set_states(psi)
+        eng.init_thresholds()
+        eng.set_bases_only(True)
+        eng.run_periods(1, is_obs=0)
+        eng.set_bases_only(False)
+        eng.lpn_start(**cfg)
+        eng.reset_times()
+        for p in range(3):
+            eng.run_periods(1)
+            eng.lpn_period((p + 1) * T2PI)
+        return eng.states(), eng.lpn_values()
+
+    B = q.Engine.batch(ens, deep=deep, record=1, max_dumps=1)
+    (psi_b, t_b, eta_b, jc_b), lv_b = flow(B, B.d)
+    renorms = 0
+    for e, x in enumerate(ens):
+        r, d = B.ranges[e], x["U"].shape[-1]
+        A = q.Engine(x["U"], x["L"], x["g"], x["HE"], x["R"], x["T"], x["n_traj"], seed=x["seed"],
+                     tr_base=x["tr_base"], record=1, max_dumps=1)
+        (psi_a, t_a, eta_a, jc_a), lv_a = flow(A, d)
+        assert np.array_equal(psi_b[r, :d], psi_a) and np.array_equal(t_b[r], t_a) and np.array_equal(eta_b[r], eta_a)
+        for k in lv_a:
+            assert np.array_equal(lv_b[k][r], lv_a[k]), (e, k)
+        renorms += int(lv_a["num_renorms"].sum())
+    assert renorms > 0
