@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-fbasis", action="store_true", help="skip the f-basis Lindblad RK4 measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-ensembles measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--production-sweep", type=int, default=0,
+                    help="only time this many points of the N=500 LpnMult production sweep (separate JSON line)")
     ap.add_argument("--serve-window", type=float, default=1.0, help="seconds of Poisson arrivals at 50/s")
     ap.add_argument("--batch-ensembles", type=int, default=32,
                     help="ensembles of configuration 4 in the batched measurement (of 256)")
@@ -319,6 +321,80 @@ def lpn_profile_case(local):
     eng.close()
 
 
+# ---------------------------------------------------------------- production Lyapunov sweep (sampled)
+def production_sweep(args, local):
+    """The reference's production dimer workload (submit/qjx/submit_dimer.py): LpnMult (task_id 7) at
+    N = 500 (dim 501), 20 trajectories (10 base/variation pairs) per parameter point, U = 0.01,
+    0.02, ..., A = 1.5, E = 1, J = 1, g = 0.1, one random observable (lpn_type 0), ex_deep 16.  The
+    first `count` U values run as one batched engine, one observation period (with the Lyapunov
+    update) per step, against the same points solved one after another by single-ensemble engines,
+    and against the CPU restatement on the host cores."""
+    import os_d_b200 as q
+
+    count, n, N = args.production_sweep, 20, 500
+    d = N + 1
+    R = q.random_observables(d, 1, 100, 1000000, 2)
+    cfg = dict(lpn_type=0, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10, delta_s=1e-3,
+               delta_f_high=1e-1, delta_f_low=1e-5)
+    t_build = time.perf_counter()
+    ens = []
+    for i in range(count):
+        U = 0.01 * (i + 1)
+        H, Hd, L, Ut = q.build_dimer(N, 1.0, U, 1.0, 1.5, 0.1, 1.0, DEEP)
+        ens.append(dict(U=Ut, L=L, g=[1.0], HE=H + Hd, R=R, n_traj=n, T=2.0 * np.pi, seed=0, tr_base=0))
+    t_build = time.perf_counter() - t_build
+
+    def flow(eng, rows, steps):
+        psi = np.zeros((eng.n, rows), np.complex128)
+        psi[:, 0] = 1.0
+        eng.set_states(psi)
+        eng.init_thresholds()
+        eng.set_bases_only(True)
+        eng.run_periods(1, is_obs=0)  # (a sample of) the bases' transient
+        eng.set_bases_only(False)
+        eng.lpn_start(**cfg)
+        eng.reset_times()
+        ms = 0.0
+        for p in range(steps):
+            eng.run_periods(1, is_obs=1)
+            eng.lpn_period((p + 1) * 2.0 * np.pi)
+            ms += eng.stats()["last_call_ms"]
+        return ms, eng.stats()
+
+    B = q.Engine.batch(ens, deep=DEEP, max_dumps=1, device=local)
+    ms_b, st_b = flow(B, d, args.steps)
+    v = B.lpn_values()
+    B.close()
+    ms_s = 0.0
+    for x in ens:
+        A = q.Engine(x["U"], x["L"], x["g"], x["HE"], x["R"], x["T"], n, seed=0, max_dumps=1, device=local)
+        m, _ = flow(A, d, args.steps)
+        ms_s += m
+        A.close()
+    out = {"workload": (f"LpnMult (task_id 7) production sweep sample: {count} parameter points U = 0.01..{0.01 * count:.2f} "
+                        f"of submit_dimer.py, dimer N={N} (dim {d}), {n} trajectories each, ex_deep {DEEP}, "
+                        f"lpn_type 0, one observation period + Lyapunov update per step"),
+           "metric": METRIC, "value": count * n * args.steps / (ms_b * 1e-3), "ms_per_step": ms_b / args.steps,
+           "serial_single_ensemble_engines": {"value": count * n * args.steps / (ms_s * 1e-3),
+                                              "ms_per_step": ms_s / args.steps},
+           "speedup_vs_serial": ms_s / ms_b, "renormalisations": int(v["num_renorms"].sum()),
+           "matvecs_per_traj_period": (st_b["matvecs"]) / (count * n * (args.steps + 1)),
+           "host_build_s": t_build}
+    if not args.no_cpu_baseline:
+        from oracle import oracle_py as O
+
+        threads = os.cpu_count() or 1
+        x = ens[0]
+        o = O.Ensemble(x["U"], x["L"], x["g"], x["HE"], x["R"], x["T"], threads, seed=0, record=0)
+        o.init(0, 0)
+        t0 = time.perf_counter()
+        assert o.run_periods(1, is_obs=1, n_threads=threads) == 0
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": threads / dt, "unit": METRIC, "cores": threads, "kind": "port",
+                               "sample": f"{threads} trajectories x 1 period at dim {d} ({dt:.1f} s), oracle/qjx_oracle.c"}
+    return out
+
+
 # ---------------------------------------------------------------- serving loop (configuration 5, sampled)
 def serving_bench(args, local):
     """Continuous batching (os_d_b200.serve): Poisson arrivals at 50/s over a short window, each
@@ -490,6 +566,10 @@ def run_ours(args):
         clk = clocks.stop() if clocks else None
         return float(allreduce([dev_ms], "max")[0]), wall, clk, st0, eng.stats(), ens
 
+    if args.production_sweep > 0:
+        if rank == 0:
+            print(json.dumps({"production_sweep": production_sweep(args, local)}), flush=True)
+        return
     if args.profile and args.profile_target == "lpn":
         lpn_profile_case(local)
         return
