@@ -207,6 +207,13 @@ typedef struct {
     double delta_s;       /* lpn_delta_s: target distance after a perturbation */
     double delta_f_high, delta_f_low;  /* lpn_delta_f_high / lpn_delta_f_low */
     double max_energy;    /* max |Re H_ii| of the hamiltonian (init_obs_lpn, newdel_exp.cpp:540-550) */
+    /* MBL characteristics (MBLCoreBehaviour, core.cpp:4729-4902) when mbl_Nc > 0: every ensemble
+     * has d = C(mbl_Nc, mbl_Nc/2), random-observable slot 0 holds H and spec = slot 0 / spec_div (W);
+     * mean_lpn is the imbalance; lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v - imbalance_b|,
+     * k >= 0 = random observable slot k + 1.  0 = the dimer's characteristics. */
+    int mbl_Nc;
+    int pad2;
+    double spec_div;
 } qjx_lpn_config;
 /* After the bases' transient (trans_process, experiment.cpp:138-183): copy every base into its
  * variation (psi, eta and jump stream: copy_trajectory_lpn, experiment.cpp:2221-2244), perturb
@@ -261,6 +268,21 @@ qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double
  * output pointer may be NULL. */
 qjx_status qjx_build_jcs(int N, double alpha, double drv_ampl, double part_1, double part_2, int deep, double *H,
                          double *Hd, double *L, double *Nop, double *A_op, double *Kout, double *Utree);
+/* The MBL system (sys_id 3; MBLNewDelBehaviour, newdel.cpp:182-271, 868-958, 1699-1815, 2751-2838):
+ * Nc cells (even, <= 24) holding Nc/2 hard-core particles, basis = the Nc-bit words with Nc/2 bits
+ * set in ascending order (id_to_x [d], d = C(Nc, Nc/2)); energies [Nc] = uniform(-1, 1) disorder
+ * from the MCG31 stream seed 77778888 leapfrogged (mbl_seed, mbl_mns); H = W sum_c n_c e_c +
+ * U sum_c n_c n_{c+1} - J (nearest-neighbour hops); L [num_diss][d][d]: diss_type 0 n_c (num_diss
+ * = Nc), diss_type 1 n_c - n_{c+1} plus the hop c <-> c+1 with phase diss_phase (num_diss = Nc - 1);
+ * K = -i (H - i/2 gamma sum_c L_c^H L_c); jump rates 1.  Utree [deep][d][d] = exp(K T 2^-(l+2)):
+ * one branch, run twice per period of duration T (init_split_structure_mbl, core.cpp:10382-10432).
+ * Any output pointer may be NULL (Utree also skips the exponentials). */
+qjx_status qjx_mbl_size(int Nc, int diss_type, int *d, int *num_diss);
+qjx_status qjx_build_mbl(int Nc, double W, double U, double J, int mbl_seed, int mbl_mns, int diss_type,
+                         double diss_phase, double gamma, double T, int deep, double *energies, int *id_to_x,
+                         double *H, double *L, double *K, double *Utree);
+/* The MBL imbalance of n probability rows adr [n][d] (get_imbalance_mbl, experiment.cpp:1753-1800). */
+qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double *out);
 /* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)
  * (init_split_structure_dimer_deep, core.cpp:9928-9981). */
 qjx_status qjx_build_dimer_deep(int N, double J, double U, double E, double A, double g, double omega, int deep,

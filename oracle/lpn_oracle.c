@@ -125,10 +125,28 @@ typedef struct {
     double robs[2 * 64];
 } chars_t;
 
+/* MBL: the imbalance of an adr row (get_imbalance_mbl, experiment.cpp:1753-1800): cell
+ * occupations summed over the basis words in order, then (even cells - odd cells) / all. */
+static double mbl_imbalance_row(int Nc, int d, const int *words, const double *adr)
+{
+    double occ[32];
+    for (int c = 0; c < Nc; c++) occ[c] = 0.0;
+    for (int s = 0; s < d; s++)
+        for (int c = 0; c < Nc; c++) occ[c] = occ[c] + adr[s] * (double)((words[s] >> (Nc - 1 - c)) & 1);
+    double even = 0.0, odd = 0.0;
+    for (int c = 0; c < Nc; c++) {
+        if (c % 2 == 0) even = even + occ[c];
+        else odd = odd + occ[c];
+    }
+    return (even - odd) / (odd + even);
+}
+
 /* calc_chars_lpn / calc_chars_std of one state (core.cpp:697-785): the operations of
- * orc_observables for the parts in `want`; `robs_one` >= 0 asks for that random observable only. */
+ * orc_observables for the parts in `want`; `robs_one` >= 0 asks for that random observable only.
+ * With MBL words (mbl_Nc > 0) the mean is the imbalance (MBLCoreBehaviour::calc_chars_lpn,
+ * core.cpp:4753-4775). */
 static void lpn_chars(const orc_problem *p, const double *phi, int want, int robs_one, double *xh, double *sm,
-                      chars_t *c)
+                      chars_t *c, int mbl_Nc, const int *words)
 {
     const int d = p->d;
     const double norm = orc_norm_square(d, phi);
@@ -139,8 +157,9 @@ static void lpn_chars(const orc_problem *p, const double *phi, int want, int rob
             const double a = phi[2 * st] * phi[2 * st], b = phi[2 * st + 1] * phi[2 * st + 1];
             const double adr = (0.0 + (a + b)) * inv;
             ps[st & 31] = ps[st & 31] + (double)st * adr;
+            sm[st] = adr;
         }
-        c->mean = lanes_sum(ps);
+        c->mean = mbl_Nc > 0 ? mbl_imbalance_row(mbl_Nc, d, words, sm) : lanes_sum(ps);
     }
     if (!(want & (CH_ENERGY | CH_ROBS_ALL)) && robs_one < 0) return;
     const double sq = sqrt(norm);
@@ -171,22 +190,52 @@ static void lpn_chars(const orc_problem *p, const double *phi, int want, int rob
     }
 }
 
-/* what calc_delta_s / calc_delta_f need of a state */
-static int delta_want(int lpn_type) { return lpn_type == -1 ? CH_MEAN : lpn_type == -2 ? CH_ENERGY : 0; }
+/* what calc_delta_s / calc_delta_f need of a state: a CH_ part (delta_want) and / or one random
+ * observable slot (delta_one, -1 none) */
+static int delta_want(const orc_lpn_config *cfg)
+{
+    if (cfg->mbl_Nc > 0) return cfg->lpn_type == -2 ? CH_MEAN : 0;
+    return cfg->lpn_type == -1 ? CH_MEAN : cfg->lpn_type == -2 ? CH_ENERGY : 0;
+}
 
-/* calc_delta_s / calc_delta_f (core.cpp:839-901): var against base */
+static int delta_one(const orc_lpn_config *cfg)
+{
+    if (cfg->mbl_Nc > 0) return cfg->lpn_type == -1 ? 0 : cfg->lpn_type >= 0 ? cfg->lpn_type + 1 : -1;
+    return cfg->lpn_type >= 0 ? cfg->lpn_type : -1;
+}
+
+/* calc_delta_s / calc_delta_f (dimer core.cpp:839-901; MBL core.cpp:4823-4901): var against base */
 static double lpn_delta(const orc_problem *p, const orc_lpn_config *cfg, const chars_t *v, const chars_t *b)
 {
+    if (cfg->mbl_Nc > 0 && cfg->lpn_type == -1) { /* spec = <H> / W, real divisions */
+        const double dr = b->robs[0] / cfg->spec_div - v->robs[0] / cfg->spec_div;
+        const double di = b->robs[1] / cfg->spec_div - v->robs[1] / cfg->spec_div;
+        return sqrt(dr * dr + di * di);
+    }
+    if (cfg->mbl_Nc > 0 && cfg->lpn_type == -2) return fabs(v->mean - b->mean);
     if (cfg->lpn_type == -1) return fabs(v->mean - b->mean) / (double)p->d;
     if (cfg->lpn_type == -2) return fabs(v->energy - b->energy) / cfg->max_energy;
-    const int o = cfg->lpn_type;
+    const int o = delta_one(cfg);
     const double dr = b->robs[2 * o] - v->robs[2 * o], di = b->robs[2 * o + 1] - v->robs[2 * o + 1];
     return sqrt(dr * dr + di * di);
 }
 
 static int lpn_type_ok(const orc_problem *p, const orc_lpn_config *cfg)
 {
-    return cfg->lpn_type == -1 || cfg->lpn_type == -2 || (cfg->lpn_type >= 0 && cfg->lpn_type < p->num_robs);
+    if (cfg->mbl_Nc > 0 && (orc_mbl_basis(cfg->mbl_Nc, NULL) != p->d || cfg->mbl_Nc > 24 || p->num_robs < 1))
+        return 0;
+    const int shift = cfg->mbl_Nc > 0 ? 1 : 0;
+    return cfg->lpn_type == -1 || cfg->lpn_type == -2 ||
+           (cfg->lpn_type >= 0 && cfg->lpn_type + shift < p->num_robs);
+}
+
+/* the MBL basis words of cfg (NULL for the dimer); the caller frees */
+static int *lpn_words(const orc_lpn_config *cfg)
+{
+    if (cfg->mbl_Nc <= 0) return NULL;
+    int *w = (int *)malloc(sizeof(int) * (size_t)orc_mbl_basis(cfg->mbl_Nc, NULL));
+    if (w) orc_mbl_basis(cfg->mbl_Nc, w);
+    return w;
 }
 
 static double var_uniform(const orc_problem *p, int tr, int64_t *pos)
@@ -201,7 +250,8 @@ static double var_uniform(const orc_problem *p, int tr, int64_t *pos)
  * below the target (NaN, or equal with eps_error <= 0) ends the search (the reference would not
  * terminate).  Returns the halvings done; *eps_out gets the last eps. */
 static int var_trajectory(const orc_problem *p, const orc_lpn_config *cfg, orc_lpn *lp, const double *base_phi,
-                          double *phi, int v, const chars_t *bc, double *w, double *xh, double *sm, double *eps_out)
+                          double *phi, int v, const chars_t *bc, double *w, double *xh, double *sm, double *eps_out,
+                          const int *words)
 {
     const int d = p->d;
     for (int st = 0; st < d; st++) w[2 * st] = var_uniform(p, v, &lp->var_pos[v]);
@@ -215,14 +265,14 @@ static int var_trajectory(const orc_problem *p, const orc_lpn_config *cfg, orc_l
     double lo = cfg->eps_low, hi = cfg->eps_high, diff = hi - lo;
     int deep = 0;
     double eps = orc_lpn_exp10((lo + hi) * 0.5);
-    const int want = delta_want(cfg->lpn_type);
+    const int want = delta_want(cfg), one = delta_one(cfg);
     while (deep < cfg->eps_deep) {
         for (int st = 0; st < 2 * d; st++) phi[st] = base_phi[st] + eps * w[st];
         const double nm = orc_norm_square(d, phi);
         for (int st = 0; st < 2 * d; st++) phi[st] = phi[st] / sqrt(nm);
         for (int st = 0; st < 2 * d; st++) phi[st] = phi[st] * sqrt(norm_2);
         chars_t vc;
-        lpn_chars(p, phi, want, cfg->lpn_type >= 0 ? cfg->lpn_type : -1, xh, sm, &vc);
+        lpn_chars(p, phi, want, one, xh, sm, &vc, cfg->mbl_Nc, words);
         const double ds = lpn_delta(p, cfg, &vc, bc);
         if (fabs(ds - cfg->delta_s) < cfg->eps_error) break;
         if (ds > cfg->delta_s) {
@@ -262,6 +312,8 @@ int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg,
     const int d = p->d, n = p->n_traj, half = n / 2;
     if (!lpn_type_ok(p, cfg) || p->num_robs > 64 || !s->rng_src || (n & 1)) return 2;
     const int full = CH_MEAN | CH_ENERGY | CH_ROBS_ALL;
+    int *words = lpn_words(cfg);
+    if (cfg->mbl_Nc > 0 && !words) return 1;
     int bad = 0;
 #pragma omp parallel
     {
@@ -277,14 +329,14 @@ int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg,
                 const int v = half + b;
                 double *pb = s->phi + 2 * (size_t)b * d, *pv = s->phi + 2 * (size_t)v * d;
                 chars_t bc, vc;
-                lpn_chars(p, pb, full, -1, xh, sm, &bc);
+                lpn_chars(p, pb, full, -1, xh, sm, &bc, cfg->mbl_Nc, words);
                 store_chars(p, lp, b, &bc);
                 /* copy_trajectory_lpn + var_trajectory_lpn */
                 memcpy(pv, pb, sizeof(double) * 2 * d);
                 copy_stream(s, v, b);
-                lp->eps_iters[v] = var_trajectory(p, cfg, lp, pb, pv, v, &bc, w, xh, sm, &lp->eps[v]);
+                lp->eps_iters[v] = var_trajectory(p, cfg, lp, pb, pv, v, &bc, w, xh, sm, &lp->eps[v], words);
                 /* calc_chars_lpn_start: delta_s from the std characteristics (calc_delta_f) */
-                lpn_chars(p, pv, full, -1, xh, sm, &vc);
+                lpn_chars(p, pv, full, -1, xh, sm, &vc, cfg->mbl_Nc, words);
                 store_chars(p, lp, v, &vc);
                 lp->delta_s[v] = lpn_delta(p, cfg, &vc, &bc);
                 lp->delta_s[b] = 0.0;
@@ -298,6 +350,7 @@ int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg,
         free(xh);
         free(sm);
     }
+    free(words);
     return bad;
 }
 
@@ -306,7 +359,9 @@ int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg
     const int d = p->d, n = p->n_traj, half = n / 2;
     if (!lpn_type_ok(p, cfg) || p->num_robs > 64 || !s->rng_src || (n & 1)) return 2;
     const int full = CH_MEAN | CH_ENERGY | CH_ROBS_ALL;
-    const int want = delta_want(cfg->lpn_type), one = cfg->lpn_type >= 0 ? cfg->lpn_type : -1;
+    const int want = delta_want(cfg), one = delta_one(cfg);
+    int *words = lpn_words(cfg);
+    if (cfg->mbl_Nc > 0 && !words) return 1;
     int bad = 0;
 #pragma omp parallel
     {
@@ -323,10 +378,10 @@ int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg
                 double *pb = s->phi + 2 * (size_t)b * d, *pv = s->phi + 2 * (size_t)v * d;
                 chars_t bc, vf, vc;
                 /* calc_chars_lpn of the base (its std characteristics are the same numbers) */
-                lpn_chars(p, pb, full, -1, xh, sm, &bc);
+                lpn_chars(p, pb, full, -1, xh, sm, &bc, cfg->mbl_Nc, words);
                 store_chars(p, lp, b, &bc);
                 /* calc_delta_f from the variation's std characteristics */
-                lpn_chars(p, pv, want, one, xh, sm, &vf);
+                lpn_chars(p, pv, want, one, xh, sm, &vf, cfg->mbl_Nc, words);
                 const double df = lpn_delta(p, cfg, &vf, &bc);
                 const double ds = lp->delta_s[v];
                 const double ds10 = ds * 10.0;
@@ -341,13 +396,13 @@ int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg
                     lp->ds_rec[v] = ds;
                     lp->df_rec[v] = df;
                     copy_stream(s, v, b);
-                    lp->eps_iters[v] = var_trajectory(p, cfg, lp, pb, pv, v, &bc, w, xh, sm, &lp->eps[v]);
-                    lpn_chars(p, pv, full, -1, xh, sm, &vc);
+                    lp->eps_iters[v] = var_trajectory(p, cfg, lp, pb, pv, v, &bc, w, xh, sm, &lp->eps[v], words);
+                    lpn_chars(p, pv, full, -1, xh, sm, &vc, cfg->mbl_Nc, words);
                     store_chars(p, lp, v, &vc);
                     lp->delta_s[v] = lpn_delta(p, cfg, &vc, &bc);
                     lp->lambda_now[v] = lp->lambda[v] / curr_time;
                 } else {
-                    lpn_chars(p, pv, full, -1, xh, sm, &vc);
+                    lpn_chars(p, pv, full, -1, xh, sm, &vc, cfg->mbl_Nc, words);
                     store_chars(p, lp, v, &vc);
                     lp->lambda_now[v] = (lp->lambda[v] + orc_lpn_log(df / ds + 1.0e-16)) / curr_time;
                 }
@@ -357,5 +412,6 @@ int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg
         free(xh);
         free(sm);
     }
+    free(words);
     return bad;
 }

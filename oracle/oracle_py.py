@@ -36,7 +36,7 @@ class OrcLpnConfig(C.Structure):
     _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
                 ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
                 ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
-                ("max_energy", C.c_double)]
+                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("pad2", C.c_int), ("spec_div", C.c_double)]
 
 
 class OrcLpn(C.Structure):
@@ -61,6 +61,11 @@ def lib():
         L.orc_expm.argtypes = [C.c_int, c_double_p, c_double_p]
         L.orc_dimer_heff.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p]
         L.orc_jcs_operators.argtypes = [C.c_int, C.c_double, C.c_double] + [c_double_p] * 6
+        L.orc_mbl_basis.argtypes = [C.c_int, c_int_p]
+        L.orc_mcg31_uniform.argtypes = [C.c_ulonglong] * 3 + [C.c_int, C.c_double, C.c_double, c_double_p]
+        L.orc_mbl_operators.argtypes = ([C.c_int] + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_double] * 2
+                                        + [c_double_p] * 4)
+        L.orc_mbl_imbalance.argtypes = [C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
@@ -111,6 +116,41 @@ def jcs_operators(N, alpha, drv_ampl):
     out = [_cplx((d, d)) for _ in range(6)]
     assert lib().orc_jcs_operators(N, alpha, drv_ampl, *[_dp(x) for x in out]) == 0
     return tuple(out)
+
+
+def mbl_basis(Nc):
+    """The MBL basis words (Nc/2 of Nc bits set, ascending)."""
+    d = lib().orc_mbl_basis(Nc, None)
+    assert d > 0
+    xs = np.zeros(d, dtype=np.int32)
+    lib().orc_mbl_basis(Nc, xs.ctypes.data_as(c_int_p))
+    return xs
+
+
+def mcg31_uniform(seed, k, s, count, a, b):
+    out = np.zeros(count)
+    lib().orc_mcg31_uniform(seed, k, s, count, a, b, _dp(out))
+    return out
+
+
+def mbl_operators(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma):
+    """MBL (sys_id 3): energies [Nc], H, L [num_diss], K = hamiltonians_qj[0] (d = C(Nc, Nc/2))."""
+    d = len(mbl_basis(Nc))
+    nd = Nc if diss_type == 0 else Nc - 1
+    en = np.zeros(Nc)
+    H, K = _cplx((d, d)), _cplx((d, d))
+    L = _cplx((nd, d, d))
+    assert lib().orc_mbl_operators(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, _dp(en), _dp(H),
+                                   _dp(L), _dp(K)) == 0
+    return en, H, L, K
+
+
+def mbl_imbalance(Nc, adr):
+    """get_imbalance_mbl of each row of adr [n][d]."""
+    adr = np.ascontiguousarray(adr, dtype=np.float64)
+    out = np.zeros(adr.shape[0])
+    lib().orc_mbl_imbalance(Nc, adr.shape[1], adr.shape[0], _dp(adr), _dp(out))
+    return out
 
 
 def dimer_heff(N, J, U, E, g):
@@ -277,12 +317,14 @@ class Lpn:
     variation n/2 + b of base b (orc_lpn_start / orc_lpn_period in lpn_oracle.c)."""
 
     def __init__(self, ens, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10,
-                 delta_s=1e-3, delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0):
+                 delta_s=1e-3, delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0, mbl_Nc=0,
+                 spec_div=1.0):
         self.ens = ens
         n = ens.n
         self.cfg = OrcLpnConfig(lpn_type=lpn_type, eps_deep=eps_deep, per_period=int(per_period), eps_low=eps_low,
                                 eps_high=eps_high, eps_error=eps_error, delta_s=delta_s,
-                                delta_f_high=delta_f_high, delta_f_low=delta_f_low, max_energy=max_energy)
+                                delta_f_high=delta_f_high, delta_f_low=delta_f_low, max_energy=max_energy,
+                                mbl_Nc=mbl_Nc, spec_div=spec_div)
         self.a = {k: np.zeros(n) for k in ("lambda", "lambda_now", "delta_s", "mean_lpn", "energy_lpn", "ratio",
                                            "ds_rec", "df_rec", "eps")}
         self.robs_lpn = np.zeros((n, max(ens.R.shape[0], 1)), np.complex128)

@@ -147,6 +147,174 @@ int orc_jcs_operators(int N, double alpha, double drv_ampl, double *H, double *H
     return 0;
 }
 
+/* MBL (sys_id 3): Nc cells holding Nc/2 hard-core particles; the basis is every Nc-bit word with
+ * Nc/2 bits set, in ascending order (MBLNewDelBehaviour::init_sizes, newdel.cpp:209-257). */
+static int popcount_int(int v)
+{
+    int c = 0;
+    while (v > 0) {
+        c += v & 1;
+        v >>= 1;
+    }
+    return c;
+}
+
+static int mbl_adjacent(int g) /* two set bits, neighbours (newdel.cpp:229-236) */
+{
+    return popcount_int(g) == 2 && popcount_int(g & (g << 1)) == 1;
+}
+
+int orc_mbl_basis(int Nc, int *id_to_x)
+{
+    if (Nc < 2 || Nc > 24 || Nc % 2) return -1;
+    int n = 0;
+    for (int x = 0; x < (1 << Nc); x++)
+        if (popcount_int(x) == Nc / 2) {
+            if (id_to_x) id_to_x[n] = x;
+            n++;
+        }
+    return n;
+}
+
+/* MCG31m1 leapfrog stream (seed, k, s): u_i = x_{k+1+i s} / (2^31 - 1), x_n = 1132489760 x_{n-1}
+ * mod 2^31 - 1 (the published MCG31m1 definition), mapped to [a, b) as a + (b - a) u. */
+void orc_mcg31_uniform(unsigned long long seed, unsigned long long k, unsigned long long s, int count, double a,
+                       double b, double *out)
+{
+    const unsigned long long m = 2147483647ull, mult = 1132489760ull;
+    unsigned long long x = seed % m, p = 1, q = mult, e = k + 1, step = 1;
+    if (x == 0) x = 1;
+    while (e) { /* mult^(k+1) */
+        if (e & 1) p = p * q % m;
+        q = q * q % m;
+        e >>= 1;
+    }
+    x = p * x % m;
+    q = mult;
+    e = s;
+    while (e) { /* mult^s */
+        if (e & 1) step = step * q % m;
+        q = q * q % m;
+        e >>= 1;
+    }
+    for (int i = 0; i < count; i++) {
+        const double u = (double)x / (double)m;
+        out[i] = a + (b - a) * u;
+        x = x * step % m;
+    }
+}
+
+/* MBL operators (newdel.cpp:868-958, 1699-1815, 2751-2838), d = C(Nc, Nc/2), basis words x_s:
+ *   energies[c] : uniform(-1, 1) from MCG31 seed 77778888 leapfrogged (mbl_seed, mbl_mns)
+ *   H  : diagonal W sum_c vb_c(x_s) energies[c] (vb_c = bit Nc-1-c), + U popcount(x & x << 1),
+ *        then every element -= J [x_s ^ x_t holds two neighbouring bits]
+ *   L_c: diss_type 0: diag(bit c of x_s), c < Nc; diss_type 1 (c < Nc-1): diag(bit c - bit c+1)
+ *        plus the hop between the words that differ in bits c, c+1: -e^{-i phi} from the word
+ *        with bit c set, e^{i phi} from the word with bit c+1 set
+ *   K  : hamiltonians_qj[0] = -i (H - (i/2) sum_c gamma L_c^H L_c), jump rates g_c = 1.
+ * L holds num_diss complex d x d matrices. */
+int orc_mbl_operators(int Nc, double W, double U, double J, int mbl_seed, int mbl_mns, int diss_type, double diss_phase,
+                      double gamma, double *energies, double *H, double *L, double *K)
+{
+    const int d = orc_mbl_basis(Nc, NULL);
+    if (d < 2 || (diss_type != 0 && diss_type != 1)) return 1;
+    const int nd = diss_type == 0 ? Nc : Nc - 1;
+    const size_t dd = (size_t)d * d;
+    int *xs = (int *)malloc((size_t)d * sizeof(int));
+    double *hp = (double *)malloc(2 * dd * sizeof(double));
+    if (!xs || !hp) return 2;
+    orc_mbl_basis(Nc, xs);
+    orc_mcg31_uniform(77778888ull, (unsigned long long)mbl_seed, (unsigned long long)mbl_mns, Nc, -1.0, 1.0, energies);
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 2 * dd * (size_t)nd * sizeof(double));
+    for (int s = 0; s < d; s++) {
+        double sum = 0.0;
+        for (int c = 0; c < Nc; c++) sum += (double)((xs[s] >> (Nc - 1 - c)) & 1) * energies[c];
+        sum *= 1.0 * W;
+        H[2 * ((size_t)s * d + s)] += sum;
+    }
+    for (int s = 0; s < d; s++) H[2 * ((size_t)s * d + s)] += U * popcount_int(xs[s] & (xs[s] << 1));
+    for (int s = 0; s < d; s++)
+        for (int t = 0; t < d; t++) H[2 * ((size_t)s * d + t)] -= J * mbl_adjacent(xs[s] ^ xs[t]);
+    for (int c = 0; c < nd; c++) {
+        double *Lc = L + 2 * dd * (size_t)c;
+        for (int s = 0; s < d; s++) {
+            const int bc = (xs[s] >> c) & 1;
+            Lc[2 * ((size_t)s * d + s)] = diss_type == 0 ? (double)bc : (double)bc - (double)((xs[s] >> (c + 1)) & 1);
+        }
+        if (diss_type == 0) continue;
+        for (int s = 0; s < d; s++) {
+            const int bc = (xs[s] >> c) & 1, bc1 = (xs[s] >> (c + 1)) & 1;
+            if (bc == bc1) continue;
+            for (int t = 0; t < d; t++) {
+                const int g = xs[s] ^ xs[t];
+                if (!mbl_adjacent(g) || (g & -g) != (1 << c)) continue; /* lower hop cell == c */
+                double *e = Lc + 2 * ((size_t)s * d + t);
+                if (bc) {
+                    e[0] = -cos(-diss_phase);
+                    e[1] = -sin(-diss_phase);
+                } else {
+                    e[0] = cos(diss_phase);
+                    e[1] = sin(diss_phase);
+                }
+            }
+        }
+    }
+    /* hamitlonian_part accumulates -(i/2) gamma L_c^H L_c channel by channel (newdel.cpp:2772-2828) */
+    for (size_t e = 0; e < dd; e++) {
+        hp[2 * e] = H[2 * e];
+        hp[2 * e + 1] = 0.0;
+    }
+    for (int c = 0; c < nd; c++) {
+        const double *Lc = L + 2 * dd * (size_t)c;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int k = 0; k < d; k++) {
+                    const double ar = Lc[2 * ((size_t)k * d + i)], ai = Lc[2 * ((size_t)k * d + i) + 1];
+                    const double br = Lc[2 * ((size_t)k * d + j)], bi = Lc[2 * ((size_t)k * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (gamma * si);
+                hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        K[2 * e] = 0.0 + hp[2 * e + 1];
+        K[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    free(xs);
+    free(hp);
+    return 0;
+}
+
+/* get_imbalance_mbl (experiment.cpp:1753-1800) for n trajectories' adr rows [n][d]:
+ * n_c = sum_s adr_s vb_c(x_s) (s ascending), (sum_{c even} n_c - sum_{c odd} n_c) / total. */
+void orc_mbl_imbalance(int Nc, int d, int n, const double *adr, double *out)
+{
+    int *xs = (int *)malloc((size_t)d * sizeof(int));
+    double *np_ = (double *)malloc((size_t)Nc * sizeof(double));
+    if (!xs || !np_) return;
+    orc_mbl_basis(Nc, xs);
+    for (int tr = 0; tr < n; tr++) {
+        const double *a = adr + (size_t)tr * d;
+        for (int c = 0; c < Nc; c++) np_[c] = 0.0;
+        for (int s = 0; s < d; s++)
+            for (int c = 0; c < Nc; c++) np_[c] += a[s] * (double)((xs[s] >> (Nc - 1 - c)) & 1);
+        double so = 0.0, se = 0.0;
+        for (int c = 0; c < Nc; c++) {
+            if (c % 2 == 0) so += np_[c];
+            else se += np_[c];
+        }
+        const double all = se + so;
+        out[tr] = (so - se) / all;
+    }
+    free(xs);
+    free(np_);
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

@@ -53,6 +53,18 @@ int orc_dimer_operators(int N, double J, double U, double E, double A, double g,
 int orc_jcs_operators(int N, double alpha, double drv_ampl, double *H, double *Hd, double *L, double *Nop,
                       double *K0, double *K1);
 
+/* MBL (sys_id 3, newdel.cpp:182-271, 868-958, 1699-1815, 2751-2838).  orc_mbl_basis: the words with
+ * Nc/2 of Nc bits set, ascending (returns their number d = C(Nc, Nc/2); id_to_x may be NULL).
+ * orc_mbl_operators: energies[Nc], H, L [num_diss][d][d] (num_diss = Nc for diss_type 0, Nc - 1 for
+ * diss_type 1), K = hamiltonians_qj[0]; jump rates are 1.  orc_mbl_imbalance: get_imbalance_mbl
+ * (experiment.cpp:1753-1800) of n adr rows [n][d]. */
+int orc_mbl_basis(int Nc, int *id_to_x);
+void orc_mcg31_uniform(unsigned long long seed, unsigned long long k, unsigned long long s, int count, double a,
+                       double b, double *out);
+int orc_mbl_operators(int Nc, double W, double U, double J, int mbl_seed, int mbl_mns, int diss_type, double diss_phase,
+                      double gamma, double *energies, double *H, double *L, double *K);
+void orc_mbl_imbalance(int Nc, int d, int n, const double *adr, double *out);
+
 /* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
  * propagator (newdel.cpp:2354-2366), complex d x d. */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);
@@ -171,6 +183,12 @@ typedef struct {
     double delta_s;      /* lpn_delta_s */
     double delta_f_high, delta_f_low;
     double max_energy;   /* max |Re H_ii| (lpn_type -2) */
+    /* MBL characteristics (MBLCoreBehaviour, core.cpp:4729-4902) when mbl_Nc > 0: random-observable
+     * slot 0 holds H and spec = slot 0 / spec_div (W); mean = the imbalance of the adr row;
+     * lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v - imbalance_b|, k >= 0 = slot k + 1. */
+    int mbl_Nc;
+    int pad2;
+    double spec_div;
 } orc_lpn_config;
 
 typedef struct {

@@ -159,6 +159,22 @@ std::string jcs_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string mbl_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_Nc(" << int(param(cp, "mbl_Nc")) << ")";
+    s << "_rnd(" << int(param(cp, "mbl_seed")) << "_" << int(param(cp, "mbl_mns")) << ")";
+    s << "_diss(" << int(param(cp, "diss_type")) << "_" << std::setprecision(precision) << std::fixed
+      << param(cp, "diss_phase") << "_" << std::setprecision(precision) << std::fixed << param(cp, "diss_gamma") << ")";
+    s << "_prm(" << std::setprecision(precision) << std::fixed << param(cp, "mbl_prm_W") << "_"
+      << std::setprecision(precision) << std::fixed << param(cp, "mbl_prm_U") << "_"
+      << std::setprecision(precision) << std::fixed << param(cp, "mbl_prm_J") << ")";
+    s << "_start(" << int(param(cp, "start_type")) << "_" << int(param(cp, "start_state")) << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

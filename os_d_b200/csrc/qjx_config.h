@@ -47,6 +47,8 @@ double param_or(const ConfigParam &cp, const std::string &key, double dflt);
 std::string dimer_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 // JCSOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:95-133)
 std::string jcs_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
+// MBLOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:176-212)
+std::string mbl_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 
 // init_dump_periods (source/cpp/QJX/QJX/newdel_exp.cpp:408-455); empty on a bad dump_type.
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods);

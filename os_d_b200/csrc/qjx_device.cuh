@@ -182,6 +182,9 @@ struct LpnParams {
     double *eps;                                                      // [n] last bisection
     const int *pair0;                                                 // [E + 1] first pair of each ensemble
     int pairs;                                                        // sum over ensembles of n_e / 2
+    int mbl_Nc;                                                       // > 0: MBL characteristics
+    double spec_div;                                                  // MBL: spec = robs slot 0 / W
+    const int *words;                                                 // MBL: [d] basis words
 };
 // trace fields: total, setup (bucket scan + gather), operand wait, MMA loop, epilogue,
 // sub-tiles, 8-column blocks, columns

@@ -73,6 +73,7 @@ struct qjx_engine {
     int n_ens = 1;        // ensembles (qjx_create_batch)
     std::vector<double> branch_len;   // copy of qjx_config.branch_len
     std::vector<int> e_tr0;           // host copy of the ensembles' first trajectories [E + 1]
+    std::vector<int> e_d_host;        // host copy of the ensembles' dimensions [E]
     unsigned char *d_bases = nullptr; // Lyapunov transient mask (bases of every ensemble)
     // serving engines (qjx_create_slots): every ensemble is a slot with room for d_cap and n_cap
     int slot_dcap = 0, slot_ncap = 0;
@@ -361,6 +362,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     cudaMemcpy(mats, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
     P.mats = mats;
     h->e_tr0 = e_tr0;
+    h->e_d_host = e_d;
     P.e_d = upload(h, e_d);
     P.e_nc = upload(h, e_nc);
     P.e_kb = upload(h, e_kb);
@@ -785,6 +787,7 @@ extern "C" qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble 
     const unsigned long long seed = e->seed;
     const long long sbase = e->tr_base;
     CK(cudaMemcpy(const_cast<int *>(P.e_d) + slot, &d, sizeof(int), cudaMemcpyHostToDevice));
+    h->e_d_host[slot] = d;
     CK(cudaMemcpy(const_cast<int *>(P.e_nc) + slot, &nc, sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(const_cast<int *>(P.e_kb) + slot, &kb, sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(const_cast<double *>(P.e_dt) + (size_t)slot * P.nb * P.deep, dts.data(),
@@ -1068,8 +1071,19 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
         if (ne < 2 || (ne & 1))
             return fail(h, QJX_ERR_INVALID_ARG, "the Lyapunov task needs an even n_traj >= 2 in every ensemble");
     }
-    if (!(c->lpn_type == -1 || c->lpn_type == -2 || (c->lpn_type >= 0 && c->lpn_type < P.nr)))
+    const int shift = c->mbl_Nc > 0 ? 1 : 0;  // MBL: slot 0 holds H (spec)
+    if (!(c->lpn_type == -1 || c->lpn_type == -2 || (c->lpn_type >= 0 && c->lpn_type + shift < P.nr)))
         return fail(h, QJX_ERR_INVALID_ARG, "lpn_type must be -1, -2 or a random observable index");
+    std::vector<int> words;
+    if (c->mbl_Nc != 0) {
+        int dm = 0;
+        if (qjx_mbl_size(c->mbl_Nc, 0, &dm, nullptr) != QJX_OK || P.nr < 1 || !(c->spec_div != 0.0))
+            return fail(h, QJX_ERR_INVALID_ARG, "mbl_Nc must be even in [2, 24] with H in observable slot 0");
+        for (int e = 0; e < h->n_ens; e++)
+            if (h->e_d_host[e] != dm) return fail(h, QJX_ERR_INVALID_ARG, "mbl_Nc does not match the dimension");
+        for (int x = 0; x < (1 << c->mbl_Nc); x++)
+            if (__builtin_popcount(x) == c->mbl_Nc / 2) words.push_back(x);
+    }
     if (P.nr > 64) return fail(h, QJX_ERR_UNSUPPORTED, "the Lyapunov task takes at most 64 random observables");
     if (c->eps_deep < 0) return fail(h, QJX_ERR_INVALID_ARG, "eps_deep must be >= 0");
     CK(cudaSetDevice(h->cfg.device));
@@ -1110,6 +1124,12 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
     L.delta_f_high = c->delta_f_high;
     L.delta_f_low = c->delta_f_low;
     L.max_energy = c->max_energy;
+    L.mbl_Nc = c->mbl_Nc;
+    L.spec_div = c->spec_div;
+    if (!words.empty()) {
+        L.words = upload(h, words);
+        if (!L.words) return fail(h, QJX_ERR_OOM, "MBL words");
+    }
     CK(cudaMemsetAsync(L.var_pos, 0, n * sizeof(long long), h->stream));
     CK(cudaMemsetAsync(L.ratio, 0, n * sizeof(double), h->stream));
     CK(cudaMemsetAsync(L.ds_rec, 0, n * sizeof(double), h->stream));

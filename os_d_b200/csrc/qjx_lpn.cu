@@ -103,6 +103,7 @@ struct LpnChars {
 struct LpnShared {
     LpnChars bc, vc;
     double red[4];  // [0] norm of the state under study, [1] |w|^2, [2] |base|^2
+    double occ[24];  // MBL: cell occupations of the state under study
 };
 
 // The pair's ensemble: dimension, padded rows of its matrices, first group and the offset from a
@@ -131,10 +132,13 @@ __device__ __forceinline__ void cta_matvec(const Params &P, const EnsCtx &E, int
 }
 
 // calc_chars_lpn / calc_chars_std of `phi` (core.cpp:697-785) for the parts in `want` (robs_one
-// >= 0: that random observable only) into `c`; the canonical norm is left in sh.red[0].  Ends
-// with a barrier, so every thread may read `c` afterwards.
-__device__ void cta_chars(const Params &P, const EnsCtx &E, const double2 *phi, int want, int robs_one, double2 *xh,
-                          double2 *y, LpnShared &sh, LpnChars &c, double *adr_out)
+// >= 0: that random observable only) into `c`; the canonical norm is left in sh.red[0] and, with
+// CH_MEAN, |phi_i|^2 / |phi|^2 in adr.  With MBL characteristics the mean is the imbalance
+// (MBLCoreBehaviour::calc_chars_lpn, core.cpp:4753-4775; get_imbalance_mbl,
+// experiment.cpp:1753-1800): one thread per cell sums its occupation over the basis words in
+// order.  Ends with a barrier, so every thread may read `c` afterwards.
+__device__ void cta_chars(const Params &P, const LpnParams &L, const EnsCtx &E, const double2 *phi, int want,
+                          int robs_one, double2 *xh, double2 *y, LpnShared &sh, LpnChars &c, double *adr)
 {
     const int d = E.d, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (warp == 0) {
@@ -146,7 +150,7 @@ __device__ void cta_chars(const Params &P, const EnsCtx &E, const double2 *phi, 
             for (int st = lane; st < d; st += 32) {
                 const double2 v = phi[st];
                 const double a = __dmul_rn(__dadd_rn(0.0, __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y))), inv);
-                if (adr_out) adr_out[st] = a;
+                adr[st] = a;
                 ms = __dadd_rn(ms, __dmul_rn((double)st, a));
             }
             ms = warp_allsum(ms);
@@ -154,6 +158,25 @@ __device__ void cta_chars(const Params &P, const EnsCtx &E, const double2 *phi, 
         }
     }
     __syncthreads();
+    if ((want & CH_MEAN) && L.mbl_Nc > 0) {
+        const int Nc = L.mbl_Nc;
+        if ((int)threadIdx.x < Nc) {
+            const int sh_bits = Nc - 1 - (int)threadIdx.x;  // cell c is bit Nc-1-c of a word
+            double o = 0.0;
+            for (int st = 0; st < d; st++) o = __dadd_rn(o, __dmul_rn(adr[st], (double)((L.words[st] >> sh_bits) & 1)));
+            sh.occ[threadIdx.x] = o;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double even = 0.0, odd = 0.0;
+            for (int cc = 0; cc < Nc; cc++) {
+                if (cc % 2 == 0) even = __dadd_rn(even, sh.occ[cc]);
+                else odd = __dadd_rn(odd, sh.occ[cc]);
+            }
+            c.mean = __ddiv_rn(__dsub_rn(even, odd), __dadd_rn(odd, even));
+        }
+        __syncthreads();
+    }
     if (!(want & (CH_ENERGY | CH_ROBS_ALL)) && robs_one < 0) return;
     const double sq = __dsqrt_rn(sh.red[0]);
     for (int st = threadIdx.x; st < d; st += blockDim.x) {
@@ -195,18 +218,36 @@ __device__ void cta_chars(const Params &P, const EnsCtx &E, const double2 *phi, 
     }
 }
 
-__device__ __forceinline__ int delta_want(int lpn_type)
+// What calc_delta_s / calc_delta_f need of a state: CH_ parts and one random-observable slot
+// (-1: none).  MBL: -1 the spec (slot 0), -2 the imbalance, k >= 0 slot k + 1.
+__device__ __forceinline__ int delta_want(const LpnParams &L)
 {
-    return lpn_type == -1 ? CH_MEAN : lpn_type == -2 ? CH_ENERGY : 0;
+    if (L.mbl_Nc > 0) return L.lpn_type == -2 ? CH_MEAN : 0;
+    return L.lpn_type == -1 ? CH_MEAN : L.lpn_type == -2 ? CH_ENERGY : 0;
 }
 
-// calc_delta_s / calc_delta_f (core.cpp:839-901), variation v against base b
+__device__ __forceinline__ int delta_one(const LpnParams &L)
+{
+    if (L.mbl_Nc > 0) return L.lpn_type == -1 ? 0 : L.lpn_type >= 0 ? L.lpn_type + 1 : -1;
+    return L.lpn_type >= 0 ? L.lpn_type : -1;
+}
+
+// calc_delta_s / calc_delta_f (dimer core.cpp:839-901, MBL core.cpp:4823-4901), variation v
+// against base b
 __device__ __forceinline__ double lpn_delta(const EnsCtx &E, const LpnParams &L, const LpnChars &v,
                                             const LpnChars &b)
 {
+    if (L.mbl_Nc > 0 && L.lpn_type == -1) {  // spec = <H> / W, real divisions
+        const double2 bb = b.robs[0], vv = v.robs[0];
+        const double dr = __dsub_rn(__ddiv_rn(bb.x, L.spec_div), __ddiv_rn(vv.x, L.spec_div));
+        const double di = __dsub_rn(__ddiv_rn(bb.y, L.spec_div), __ddiv_rn(vv.y, L.spec_div));
+        return __dsqrt_rn(__dadd_rn(__dmul_rn(dr, dr), __dmul_rn(di, di)));
+    }
+    if (L.mbl_Nc > 0 && L.lpn_type == -2) return fabs(__dsub_rn(v.mean, b.mean));
     if (L.lpn_type == -1) return __ddiv_rn(fabs(__dsub_rn(v.mean, b.mean)), (double)E.d);
     if (L.lpn_type == -2) return __ddiv_rn(fabs(__dsub_rn(v.energy, b.energy)), L.max_energy);
-    const double2 bb = b.robs[L.lpn_type], vv = v.robs[L.lpn_type];
+    const int o = delta_one(L);
+    const double2 bb = b.robs[o], vv = v.robs[o];
     const double dr = __dsub_rn(bb.x, vv.x), di = __dsub_rn(bb.y, vv.y);
     return __dsqrt_rn(__dadd_rn(__dmul_rn(dr, dr), __dmul_rn(di, di)));
 }
@@ -217,7 +258,7 @@ __device__ __forceinline__ double lpn_delta(const EnsCtx &E, const LpnParams &L,
 // eps_deep halvings; a delta_s that is neither above nor below the target ends the search.
 // Leaves the perturbed state in pv.
 __device__ void var_trajectory(const Params &P, const EnsCtx &E, const LpnParams &L, int v, const double2 *pb,
-                               double2 *pv, double2 *w, double2 *xh, double2 *y, LpnShared &sh)
+                               double2 *pv, double2 *w, double2 *xh, double2 *y, LpnShared &sh, double *adr)
 {
     const int d = E.d, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long pos0 = L.var_pos[v];
@@ -247,7 +288,7 @@ __device__ void var_trajectory(const Params &P, const EnsCtx &E, const LpnParams
     double lo = L.eps_low, hi = L.eps_high, diff = __dsub_rn(hi, lo);
     int deep = 0;
     double eps = lpn_exp10(__dmul_rn(__dadd_rn(lo, hi), 0.5));
-    const int want = delta_want(L.lpn_type), one = L.lpn_type >= 0 ? L.lpn_type : -1;
+    const int want = delta_want(L), one = delta_one(L);
     __syncthreads();
     while (deep < L.eps_deep) {
         for (int st = threadIdx.x; st < d; st += blockDim.x) {
@@ -266,7 +307,7 @@ __device__ void var_trajectory(const Params &P, const EnsCtx &E, const LpnParams
             pv[st] = make_double2(__dmul_rn(__ddiv_rn(a.x, sm), s2), __dmul_rn(__ddiv_rn(a.y, sm), s2));
         }
         __syncthreads();
-        cta_chars(P, E, pv, want, one, xh, y, sh, sh.vc, nullptr);
+        cta_chars(P, L, E, pv, want, one, xh, y, sh, sh.vc, adr);
         const double ds = lpn_delta(E, L, sh.vc, sh.bc);
         if (fabs(__dsub_rn(ds, L.delta_s)) < L.eps_error) break;
         if (ds > L.delta_s) {
@@ -330,7 +371,7 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
     }
     __syncthreads();
     const int full = CH_MEAN | CH_ENERGY | CH_ROBS_ALL;
-    cta_chars(P, E, pb, full, -1, xh, y, sh, sh.bc, nullptr);  // calc_chars_lpn of the base
+    cta_chars(P, L, E, pb, full, -1, xh, y, sh, sh.bc, adr);  // calc_chars_lpn of the base
     store_chars(P, L, b, sh.bc);
     bool moved = false;
     if (mode == 0) {
@@ -340,9 +381,9 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
         sv.eta = sb.eta;
         for (int st = threadIdx.x; st < d; st += blockDim.x) pv[st] = pb[st];
         __syncthreads();
-        var_trajectory(P, E, L, v, pb, pv, w, xh, y, sh);
+        var_trajectory(P, E, L, v, pb, pv, w, xh, y, sh, adr);
         moved = true;
-        cta_chars(P, E, pv, full, -1, xh, y, sh, sh.vc, nullptr);
+        cta_chars(P, L, E, pv, full, -1, xh, y, sh, sh.vc, adr);
         store_chars(P, L, v, sh.vc);
         if (threadIdx.x == 0) {
             L.delta_s_v[v] = lpn_delta(E, L, sh.vc, sh.bc);
@@ -353,8 +394,8 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
             L.renormed[b] = L.renormed[v] = 0;
         }
     } else {
-        const int want = delta_want(L.lpn_type), one = L.lpn_type >= 0 ? L.lpn_type : -1;
-        cta_chars(P, E, pv, want, one, xh, y, sh, sh.vc, nullptr);
+        const int want = delta_want(L), one = delta_one(L);
+        cta_chars(P, L, E, pv, want, one, xh, y, sh, sh.vc, adr);
         const double df = lpn_delta(E, L, sh.vc, sh.bc);
         const double ds = L.delta_s_v[v];
         const double ds10 = __dmul_rn(ds, 10.0);
@@ -366,9 +407,9 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
             sv.rng_src = sb.rng_src;  // copy_stream_lpn
             sv.rng_pos = sb.rng_pos;
             sv.eta = sb.eta;
-            var_trajectory(P, E, L, v, pb, pv, w, xh, y, sh);
+            var_trajectory(P, E, L, v, pb, pv, w, xh, y, sh, adr);
             moved = true;
-            cta_chars(P, E, pv, full, -1, xh, y, sh, sh.vc, nullptr);
+            cta_chars(P, L, E, pv, full, -1, xh, y, sh, sh.vc, adr);
             store_chars(P, L, v, sh.vc);
             if (threadIdx.x == 0) {
                 L.lambda[v] = lam;
@@ -381,7 +422,7 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
                 L.lambda_now[v] = __ddiv_rn(lam, curr_time);
             }
         } else {
-            cta_chars(P, E, pv, full, -1, xh, y, sh, sh.vc, nullptr);
+            cta_chars(P, L, E, pv, full, -1, xh, y, sh, sh.vc, adr);
             store_chars(P, L, v, sh.vc);
             if (threadIdx.x == 0) {
                 L.renormed[v] = 0;
@@ -396,7 +437,7 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
     }
     if (adr_dump >= 0 && P.o_adr) {
         double *dst = P.keep_adr ? P.o_adr + ((size_t)adr_dump * P.n + v) * P.d : P.o_adr + (size_t)v * P.d;
-        cta_chars(P, E, pv, CH_MEAN, -1, xh, y, sh, sh.vc, adr);
+        cta_chars(P, L, E, pv, CH_MEAN, -1, xh, y, sh, sh.vc, adr);
         for (int st = threadIdx.x; st < d; st += blockDim.x) dst[st] = adr[st];
     }
 }

@@ -1,6 +1,7 @@
 // qjx_main.cpp -- qjx_b200: process-level drop-in for the reference's qjx executable on the
 // Std task (task_id 1) and the LpnMult task (task_id 7) with the QJ propagator (prop_id 0) or the
-// RK propagator (prop_id 1), and the StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0).
+// RK propagator (prop_id 1), and the StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0);
+// the Std task with the QJ propagator for the JCS (sys_id 1) and MBL (sys_id 3) systems.
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -62,9 +63,13 @@ void write_2d_inv(const std::string &fn, const std::vector<double> &v, int nrec,
 // n/2 + b starts as its base perturbed to delta_s, and after every observation period the
 // variations' Lyapunov sums are updated (lambda_lpn / lambda_lpn_now).  Files: dump_std,
 // dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127), adr files (dump.cpp:3-98).
+// MBL (Nc > 0; MBLCoreBehaviour, core.cpp:4677-5105): H rides in random-observable slot 0, spec
+// = slot 0 / W, the mean characteristics are imbalances, and the file set is MBL's.
 void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, const qjx_config &cfg,
-                  const std::vector<double> &H, int d, int num_robs, int robs_seed)
+                  const std::vector<double> &H, int d, int num_robs, int robs_seed, int Nc = 0, double W = 1.0)
 {
+    const bool mbl = Nc > 0;
+    const int ro = mbl ? 1 : 0, nr = num_robs + ro;  // engine slots: [spec,] random observables
     const int n = cp.num_trajectories, half = n / 2;
     if (n < 2 || (n & 1)) die("LpnMult needs an even num_trajectories >= 2");
     const std::string &sfx = cp.fn_suffix;
@@ -84,6 +89,8 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     lc.delta_f_high = param(cp, "lpn_delta_f_high");
     lc.delta_f_low = param(cp, "lpn_delta_f_low");
     const int save_lambdas = int(param(cp, "save_lambdas"));
+    lc.mbl_Nc = Nc;
+    lc.spec_div = W;
     lc.max_energy = 0.0;  // init_obs_lpn (newdel_exp.cpp:540-550)
     for (int st = 0; st < d; st++) {
         const double v = std::fabs(H[2 * ((size_t)st * d + st)]);
@@ -97,16 +104,26 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     std::vector<double> lam_evo, mean_lpn_evo, energy_lpn_evo;
     std::vector<std::complex<double>> robs_lpn_evo;
     std::vector<double> lam(n), mean_l(n), energy_l(n);
-    std::vector<std::complex<double>> robs_l((size_t)n * (num_robs ? num_robs : 1));
+    std::vector<std::complex<double>> robs_l((size_t)n * (nr ? nr : 1));
     std::vector<int> renorms(n);
     auto take_lpn = [&]() {
         check(qjx_lpn_get(h, lam.data(), nullptr, nullptr, mean_l.data(), energy_l.data(),
-                          num_robs ? reinterpret_cast<double *>(robs_l.data()) : nullptr, renorms.data()),
+                          nr ? reinterpret_cast<double *>(robs_l.data()) : nullptr, renorms.data()),
               h, "qjx_lpn_get");
         lam_evo.insert(lam_evo.end(), lam.begin(), lam.end());
         mean_lpn_evo.insert(mean_lpn_evo.end(), mean_l.begin(), mean_l.end());
         energy_lpn_evo.insert(energy_lpn_evo.end(), energy_l.begin(), energy_l.end());
-        robs_lpn_evo.insert(robs_lpn_evo.end(), robs_l.begin(), robs_l.begin() + (size_t)n * num_robs);
+        robs_lpn_evo.insert(robs_lpn_evo.end(), robs_l.begin(), robs_l.begin() + (size_t)n * nr);
+    };
+    // MBL: the std imbalance of a dump comes from its adr rows before the Lyapunov update rewrites
+    // the variations' rows (calc_chars_std runs before lambda_lpn, experiment.cpp:226-252)
+    std::vector<double> imb_std(mbl ? (size_t)ndt * n : 0);
+    auto take_imbalance = [&](int dump) {
+        if (!mbl) return;
+        std::vector<double> adr((size_t)n * d);
+        check(qjx_get_observables(h, dump, 1, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, adr.data()), h,
+              "qjx_get_observables");
+        check(qjx_mbl_imbalance(Nc, n, adr.data(), imb_std.data() + (size_t)dump * n), h, "qjx_mbl_imbalance");
     };
     // save_lambdas: delta_f / delta_s, delta_s, delta_f of every renormalisation per trajectory
     std::vector<std::vector<double>> rec_ratio(n), rec_ds(n), rec_df(n);
@@ -165,6 +182,7 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     after_lpn(true);
     check(qjx_reset_times(h), h, "qjx_reset_times");
     check(qjx_observe(h, 0, 1), h, "qjx_observe");
+    take_imbalance(0);
     take_lpn();
     write_adr_single(0, false);
     if (dump_evo_avg == 1) write_adr_avg(0, n, false);
@@ -177,6 +195,7 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
             const bool at_dump = period_id + 1 == dp[dump_id];
             const int one = 1;
             check(qjx_run_periods(h, 1, 1, at_dump ? &one : nullptr, at_dump ? 1 : 0, dump_id), h, "qjx_run_periods");
+            if (at_dump) take_imbalance(dump_id);
             check(qjx_lpn_period(h, double(period_id + 1) * cfg.T, at_dump ? dump_id : -1), h, "qjx_lpn_period");
             after_lpn(false);
         }
@@ -192,9 +211,9 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
 
     std::vector<double> norm_((size_t)ndt * n), mean_((size_t)ndt * n), disp_((size_t)ndt * n), m2_((size_t)ndt * n),
         energy_((size_t)ndt * n);
-    std::vector<std::complex<double>> robs_((size_t)ndt * n * (num_robs ? num_robs : 1));
+    std::vector<std::complex<double>> robs_((size_t)ndt * n * (nr ? nr : 1));
     check(qjx_get_observables(h, 0, ndt, norm_.data(), mean_.data(), disp_.data(), m2_.data(), energy_.data(),
-                              num_robs ? reinterpret_cast<double *>(robs_.data()) : nullptr, nullptr),
+                              nr ? reinterpret_cast<double *>(robs_.data()) : nullptr, nullptr),
           h, "qjx_get_observables");
     // a dump with no period since the previous one repeats the previous std characteristics
     // (calc_chars_std runs once per period; a renormalised variation keeps its pre-renormalisation values)
@@ -202,11 +221,36 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         if (!zero_span[dmp]) continue;
         const size_t a = (size_t)(dmp - 1) * n, b = (size_t)dmp * n;
         for (auto *v : {&norm_, &mean_, &disp_, &m2_, &energy_}) std::copy(v->begin() + a, v->begin() + a + n, v->begin() + b);
-        std::copy(robs_.begin() + a * num_robs, robs_.begin() + (a + n) * num_robs, robs_.begin() + b * num_robs);
+        if (mbl) std::copy(imb_std.begin() + a, imb_std.begin() + a + n, imb_std.begin() + b);
+        std::copy(robs_.begin() + a * nr, robs_.begin() + (a + n) * nr, robs_.begin() + b * nr);
     }
+    // MBL spec = <H> / W per trajectory (get_spec_mbl, experiment.cpp:1705-1751): std [dump][tr], lpn
+    auto spec_of = [&](const std::vector<std::complex<double>> &src) {
+        std::vector<std::complex<double>> out(src.size() / (nr ? nr : 1));
+        for (size_t i = 0; i < out.size() && mbl; i++)
+            out[i] = std::complex<double>(src[i * nr].real() / W, src[i * nr].imag() / W);
+        return out;
+    };
+    const std::vector<std::complex<double>> spec_std = spec_of(robs_), spec_lpn = spec_of(robs_lpn_evo);
+    auto write_2d_inv_c = [&](const std::string &fn, const std::vector<std::complex<double>> &v) {
+        std::vector<std::complex<double>> inv((size_t)ndt * n);
+        for (int dmp = 0; dmp < ndt; dmp++)
+            for (int tr = 0; tr < n; tr++) inv[(size_t)tr * ndt + dmp] = v[(size_t)dmp * n + tr];
+        save_2d_inv_complex_data(fn, reinterpret_cast<const double *>(inv.data()), ndt, n, 16, false);
+    };
     std::vector<double> mean_start(n);
     check(qjx_get_mean_start(h, mean_start.data()), h, "qjx_get_mean_start");
-    if (dump_obs == 1) {
+    if (dump_obs == 1 && mbl) {  // MBLCoreBehaviour::dump_std / dump_lpn (core.cpp:4910-4987)
+        const size_t o = (size_t)last_dump * n;
+        save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);
+        save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec_std.data() + o), n, 16, false);
+        save_double_data(path + "imbalance" + sfx, imb_std.data() + o, n, 16, false);
+        save_double_data(path + "lambda" + sfx, lam_evo.data() + o, n, 16, false);
+        save_int_data(path + "num_renorms" + sfx, renorms.data(), n, false);
+        save_complex_data(path + "spec_lpn" + sfx, reinterpret_cast<const double *>(spec_lpn.data() + o), n, 16, false);
+        save_double_data(path + "imbalance_lpn" + sfx, mean_lpn_evo.data() + o, n, 16, false);
+    }
+    if (dump_obs == 1 && !mbl) {
         const size_t o = (size_t)last_dump * n;
         save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);  // dump_std
         save_double_data(path + "mean_start" + sfx, mean_start.data(), n, 16, false);
@@ -219,6 +263,8 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         save_int_data(path + "num_renorms" + sfx, renorms.data(), n, false);
         save_double_data(path + "mean_lpn" + sfx, mean_lpn_evo.data() + ol, n, 16, false);
         save_double_data(path + "energy_lpn" + sfx, energy_lpn_evo.data() + ol, n, 16, false);
+    }
+    if (dump_obs == 1) {
         if (save_lambdas > 0)
             for (int tr = 0; tr < n; tr++) {
                 save_double_vector(path + "delta_f_by_delta_s_" + std::to_string(tr) + sfx, rec_ratio[tr], 16, false);
@@ -229,15 +275,20 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     if (dump_evo_sep == 1 && dump_obs == 1) {
         save_int_data(path + "periods" + sfx, dp.data(), ndt, false);  // dump_std_evo
         write_2d_inv(path + "norm_evo" + sfx, norm_, ndt, ndt, n);
-        write_2d_inv(path + "mean_evo" + sfx, mean_, ndt, ndt, n);
-        write_2d_inv(path + "dispersion_evo" + sfx, disp_, ndt, ndt, n);
-        write_2d_inv(path + "m2_evo" + sfx, m2_, ndt, ndt, n);
-        write_2d_inv(path + "energy_evo" + sfx, energy_, ndt, ndt, n);
+        if (mbl) {  // MBLCoreBehaviour::dump_std_evo (core.cpp:4988-5056)
+            write_2d_inv_c(path + "spec_evo" + sfx, spec_std);
+            write_2d_inv(path + "imbalance_evo" + sfx, imb_std, ndt, ndt, n);
+        } else {
+            write_2d_inv(path + "mean_evo" + sfx, mean_, ndt, ndt, n);
+            write_2d_inv(path + "dispersion_evo" + sfx, disp_, ndt, ndt, n);
+            write_2d_inv(path + "m2_evo" + sfx, m2_, ndt, ndt, n);
+            write_2d_inv(path + "energy_evo" + sfx, energy_, ndt, ndt, n);
+        }
         auto robs_file = [&](const std::string &name, const std::vector<std::complex<double>> &src) {
             for (int o = 0; o < num_robs; o++) {
                 std::vector<std::vector<std::complex<double>>> v(n, std::vector<std::complex<double>>(ndt));
                 for (int tr = 0; tr < n; tr++)
-                    for (int dmp = 0; dmp < ndt; dmp++) v[tr][dmp] = src[((size_t)dmp * n + tr) * num_robs + o];
+                    for (int dmp = 0; dmp < ndt; dmp++) v[tr][dmp] = src[((size_t)dmp * n + tr) * nr + ro + o];
                 save_2d_complex_vector(path + name + std::to_string(robs_seed + o) + sfx, v, 16);
             }
         };
@@ -258,8 +309,13 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
             }
         }
         write_2d_inv(path + "lambda_evo" + sfx, lam_evo, ndt, ndt, n);  // dump_lpn_evo
-        write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
-        write_2d_inv(path + "energy_lpn_evo" + sfx, energy_lpn_evo, ndt, ndt, n);
+        if (mbl) {  // MBLCoreBehaviour::dump_lpn_evo (core.cpp:5058-5096)
+            write_2d_inv_c(path + "spec_lpn_evo" + sfx, spec_lpn);
+            write_2d_inv(path + "imbalance_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
+        } else {
+            write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
+            write_2d_inv(path + "energy_lpn_evo" + sfx, energy_lpn_evo, ndt, ndt, n);
+        }
         robs_file("random_obs_lpn_evo_", robs_lpn_evo);
     }
     if (dump_evo_avg == 0) write_adr_avg(last_dump, half, true);
@@ -293,11 +349,15 @@ int main(int argc, char **argv)
     if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
     std::cout << params_echo(rp, cp);
 
-    if (rp.sys_id != 0 && rp.sys_id != 1)
-        die("Wrong sys_id: " + std::to_string(rp.sys_id) + " (this engine runs the dimer (0) and JCS (1) systems)");
-    const bool jcs = rp.sys_id == 1;  // JCS: the Std task with the QJ propagator
-    if (jcs && (rp.task_id != 1 || rp.prop_id != 0))
-        die("Wrong task_id / prop_id for sys_id 1 (this engine runs JCS with the Std task and the QJ propagator)");
+    if (rp.sys_id != 0 && rp.sys_id != 1 && rp.sys_id != 3)
+        die("Wrong sys_id: " + std::to_string(rp.sys_id) +
+            " (this engine runs the dimer (0), JCS (1) and MBL (3) systems)");
+    const bool jcs = rp.sys_id == 1;  // JCS and MBL: the Std task with the QJ propagator
+    const bool mbl = rp.sys_id == 3;
+    if ((jcs && (rp.task_id != 1 || rp.prop_id != 0)) || (mbl && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0)))
+        die("Wrong task_id / prop_id for sys_id " + std::to_string(rp.sys_id) +
+            " (this engine runs JCS with the Std task, MBL with the Std and LpnMult tasks, both with the QJ "
+            "propagator)");
     if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7)
         die("Wrong task_id: " + std::to_string(rp.task_id) +
             " (this engine runs the Std (1), StdDeep (4) and LpnMult (7) tasks)");
@@ -306,7 +366,7 @@ int main(int argc, char **argv)
         die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
 
     try {
-        cp.fn_suffix = jcs ? jcs_suffix(rp, cp, 4) : dimer_suffix(rp, cp, 4);
+        cp.fn_suffix = jcs ? jcs_suffix(rp, cp, 4) : mbl ? mbl_suffix(rp, cp, 4) : dimer_suffix(rp, cp, 4);
     } catch (const std::exception &e) {
         die(e.what());
     }
@@ -316,12 +376,20 @@ int main(int argc, char **argv)
     }
 
     try {
-        const int N = int(param(cp, "N"));
+        const bool dimer = !jcs && !mbl;
+        const int N = mbl ? 0 : int(param(cp, "N"));
+        // MBL: C(Nc, Nc/2) basis words and Nc (diss_type 0) or Nc - 1 (diss_type 1) jump channels
+        const int Nc = mbl ? int(param(cp, "mbl_Nc")) : 0, mbl_dt = mbl ? int(param(cp, "diss_type")) : 0;
+        int d_mbl = 0, nd_mbl = 0;
+        if (mbl && qjx_mbl_size(Nc, mbl_dt, &d_mbl, &nd_mbl) != QJX_OK)
+            die("mbl_Nc must be even and in [2, 24], diss_type 0 or 1");
         // the dimer has N + 1 Fock states; the JCS oscillator is truncated at N states (newdel.cpp:110)
-        const int d = jcs ? N : N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
-        const double J = jcs ? 0.0 : param(cp, "dimer_prm_J"), U = jcs ? 0.0 : param(cp, "dimer_prm_U");
-        const double E = jcs ? 0.0 : param(cp, "dimer_prm_E");
-        const double A = jcs ? 0.0 : param(cp, "dimer_drv_ampl"), omega = jcs ? 1.0 : param(cp, "dimer_drv_freq");
+        const int d = mbl ? d_mbl : jcs ? N : N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
+        const int num_diss = mbl ? nd_mbl : 1;
+        const double J = dimer ? param(cp, "dimer_prm_J") : 0.0, U = dimer ? param(cp, "dimer_prm_U") : 0.0;
+        const double E = dimer ? param(cp, "dimer_prm_E") : 0.0;
+        const double A = dimer ? param(cp, "dimer_drv_ampl") : 0.0, omega = dimer ? param(cp, "dimer_drv_freq") : 1.0;
+        const double mbl_W = mbl ? param(cp, "mbl_prm_W") : 1.0;
         const double g = param(cp, "diss_gamma");
         const double jcs_alpha = jcs ? param(cp, "jcs_prm_alpha") : 0.0;
         const double jcs_ampl = jcs ? param(cp, "jcs_drv_ampl") : 0.0;
@@ -337,14 +405,14 @@ int main(int argc, char **argv)
         const int dump_purity = int(param_or(cp, "dump_purity", 0));
         const int num_robs = int(param(cp, "num_random_obs"));
         const int robs_seed = int(param_or(cp, "random_obs_seed", 0));
-        if (n < 1 || N < 1 || (jcs && N < 2)) die("num_trajectories and N must be positive (N >= 2 for JCS)");
+        if (n < 1 || (!mbl && N < 1) || (jcs && N < 2)) die("num_trajectories and N must be positive (N >= 2 for JCS)");
         if (start_type == 0 && (start_state < 0 || start_state >= d)) die("start_state out of range");
         const std::string &sfx = cp.fn_suffix;
         const std::string path = rp.path;
         const size_t dd = (size_t)d * d;
 
         // model (newdel.cpp init_*), debug dumps (debugger.cpp:142-168, qj_proc.cpp:115-119)
-        std::vector<double> H(2 * dd), Hd(2 * dd), L(2 * dd), K(4 * dd), Ut(4 * dd * deep);
+        std::vector<double> H(2 * dd), Hd(2 * dd), L(2 * dd * num_diss), K(4 * dd), Ut(4 * dd * deep);
         // StdDeep (task_id 4): the split tree of the sub-period T / (2 deep_num_steps)
         const bool deep_task = rp.task_id == 4;
         const int nsub = deep_task ? int(param(cp, "deep_num_steps")) : 0;
@@ -355,6 +423,19 @@ int main(int argc, char **argv)
             check(qjx_build_jcs(N, jcs_alpha, jcs_ampl, jcs_p1, jcs_p2, deep, H.data(), Hd.data(), L.data(), Nop.data(),
                                 Aop.data(), K.data(), Ut.data()),
                   nullptr, "qjx_build_jcs");
+        else if (mbl) {
+            // one branch head of duration mbl_T with two children of the same split tree
+            // (init_split_structure_mbl, core.cpp:10382-10432): the engine's two branches
+            std::vector<double> en(Nc);
+            check(qjx_build_mbl(Nc, mbl_W, param(cp, "mbl_prm_U"), param(cp, "mbl_prm_J"), int(param(cp, "mbl_seed")),
+                                int(param(cp, "mbl_mns")), mbl_dt, param(cp, "diss_phase"), g, param(cp, "mbl_T"),
+                                deep, en.data(), nullptr, H.data(), L.data(), K.data(), Ut.data()),
+                  nullptr, "qjx_build_mbl");
+            std::copy(Ut.begin(), Ut.begin() + 2 * dd * deep, Ut.begin() + 2 * dd * deep);
+            std::copy(K.begin(), K.begin() + 2 * dd, K.begin() + 2 * dd);
+            // written to the working directory, without `path` (newdel.cpp:903-905)
+            save_double_data("energies" + cp.fn_suffix, en.data(), Nc, 16, false);
+        }
         else if (deep_task)
             check(qjx_build_dimer_deep(N, J, U, E, A, g, omega, deep, nsub, H.data(), Hd.data(), L.data(), K.data(),
                                        Ut.data()),
@@ -364,7 +445,14 @@ int main(int argc, char **argv)
                   nullptr, "qjx_build_dimer");
         std::cout << "init_sizes" << std::endl << "init_hamiltonians" << std::endl << "init_dissipators" << std::endl
                   << "init_hamiltonians_qj" << std::endl;
-        if (rp.is_debug) {
+        if (rp.is_debug && mbl) {  // MBLDebugBehaviour::save (debugger.cpp:55-68), qj_proc.cpp:115-119
+            save_complex_data(path + "hamiltonian" + sfx, H.data(), dd, 16, false);
+            for (int c = 0; c < num_diss; c++)
+                save_complex_data(path + "dissipator_" + std::to_string(c) + sfx, L.data() + 2 * dd * c, dd, 16, false);
+            save_complex_data(path + "hamiltonians_qj_0" + sfx, K.data(), dd, 16, false);
+            save_complex_data(path + "spec_mtx" + sfx, H.data(), dd, 16, false);
+            save_complex_data(path + "exp_mtx_0" + sfx, Ut.data() + 2 * dd * (deep - 1), dd, 16, false);
+        } else if (rp.is_debug) {
             save_complex_data(path + "hamiltonian" + sfx, H.data(), dd, 16, false);
             save_complex_data(path + "dissipator_0" + sfx, L.data(), dd, 16, false);
             for (int b = 0; b < 2; b++) {
@@ -375,12 +463,14 @@ int main(int argc, char **argv)
             }
         }
         std::vector<double> HE(2 * dd);
-        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : H[e] + E * Hd[e];
+        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : mbl ? H[e] : H[e] + E * Hd[e];
         std::vector<double> R =
             random_observables(d, num_robs, robs_seed, int(param_or(cp, "random_obs_mns", 1000000)),
                                int(param_or(cp, "random_obs_type", 0)));
-        const int robs_off = jcs ? 1 : 0;  // JCS: spec = <a> / alpha rides in observable slot 0
+        // JCS: spec = <a> / alpha, MBL: spec = <H> / W ride in observable slot 0
+        const int robs_off = (jcs || mbl) ? 1 : 0;
         if (jcs) R.insert(R.begin(), Aop.begin(), Aop.end());
+        if (mbl) R.insert(R.begin(), H.begin(), H.end());
         const int nr_eng = num_robs + robs_off;
 
         // dump schedule (init_dump_periods)
@@ -404,9 +494,9 @@ int main(int argc, char **argv)
         cfg.n_traj = n;
         cfg.deep = deep;
         cfg.num_branches = 2;
-        cfg.num_diss = 1;
+        cfg.num_diss = num_diss;
         cfg.num_robs = nr_eng;
-        cfg.T = jcs ? jcs_alpha : 2.0 * 3.1415926535897932384626433832795 / omega;
+        cfg.T = jcs ? jcs_alpha : mbl ? param(cp, "mbl_T") : 2.0 * 3.1415926535897932384626433832795 / omega;
         // JCS: branch b's head is jcs_drv_part_b * alpha and the branch lasts half of it
         // (init_split_structure_jcs, core.cpp:10086-10124)
         const double jcs_len[2] = {0.5 * (jcs_p1 * jcs_alpha), 0.5 * (jcs_p2 * jcs_alpha)};
@@ -415,20 +505,21 @@ int main(int argc, char **argv)
         cfg.rng_kind = int(param_or(cp, "rng_kind", 0));
         cfg.seed = (uint64_t)(uint32_t)cp.seed;
         cfg.rec_cap = 1024;
-        cfg.keep_adr = ((dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1) ? 1 : 0;
+        // MBL: the imbalance of every recorded dump comes from its adr rows
+        cfg.keep_adr = ((dump_evo_sep == 1 && dump_adr_sep == 1) || dump_evo_avg == 1 || mbl) ? 1 : 0;
         cfg.max_dumps = ndt;
         cfg.deep_num_steps = nsub;
         cfg.device = device;
-        const double gr[1] = {1.0};  // head->g (core.cpp:9905)
+        const std::vector<double> gr(num_diss, 1.0);  // head->g (core.cpp:9905, 10418)
         qjx_engine *h = nullptr;
         if (rp.prop_id == 0) {
-            check(qjx_create(&cfg, Ut.data(), L.data(), gr, HE.data(), nr_eng ? R.data() : nullptr, &h), nullptr,
+            check(qjx_create(&cfg, Ut.data(), L.data(), gr.data(), HE.data(), nr_eng ? R.data() : nullptr, &h), nullptr,
                   "qjx_create");
         } else {  // RK propagator: rk_right_part_dimer's drive keys (core.cpp:11048-11051)
             std::vector<double> He(2 * dd), Hdr(2 * dd);
             check(qjx_build_dimer_rk(N, J, U, E, g, He.data(), Hdr.data()), nullptr, "qjx_build_dimer_rk");
             check(qjx_create_rk(&cfg, He.data(), Hdr.data(), E, A, int(param_or(cp, "dimer_drv_type", 0)), omega,
-                                param_or(cp, "dimer_drv_phase", 0.0), cp.rk_ns, L.data(), gr, HE.data(),
+                                param_or(cp, "dimer_drv_phase", 0.0), cp.rk_ns, L.data(), gr.data(), HE.data(),
                                 num_robs ? R.data() : nullptr, &h),
                   nullptr, "qjx_create_rk");
         }
@@ -443,7 +534,7 @@ int main(int argc, char **argv)
         std::cout << "init_data" << std::endl;
 
         if (rp.task_id == 7) {
-            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed);
+            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, mbl ? Nc : 0, mbl_W);
             qjx_destroy(h);
             return 0;
         }
@@ -562,21 +653,37 @@ int main(int argc, char **argv)
               h, "qjx_get_observables");
         // JCS: spec = <a> / alpha (get_spec_jcs, experiment.cpp:1520-1562), mean = <a^+ a>
         // (get_num_photons_jcs, experiment.cpp:2080-2160) from the energy slot
-        std::vector<std::complex<double>> spec(jcs ? nd_ : 0);
+        // MBL: spec = <H> / W (get_spec_mbl, experiment.cpp:1705-1751), imbalance from the adr rows
+        // (get_imbalance_mbl, experiment.cpp:1753-1800)
+        std::vector<std::complex<double>> spec((jcs || mbl) ? nd_ : 0);
+        const double spec_div = jcs ? jcs_alpha : mbl_W;
         for (size_t i = 0; i < spec.size(); i++) {
             const std::complex<double> a = D.robs[i * nr_eng];
-            spec[i] = std::complex<double>(a.real() / jcs_alpha, a.imag() / jcs_alpha);
+            spec[i] = std::complex<double>(a.real() / spec_div, a.imag() / spec_div);
+        }
+        std::vector<double> imbalance(mbl ? nd_ : 0);
+        if (mbl) {
+            std::vector<double> adr(nd_ * d);
+            check(qjx_get_observables(h, 0, nrec, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, adr.data()), h,
+                  "qjx_get_observables");
+            check(qjx_mbl_imbalance(Nc, int(nd_), adr.data(), imbalance.data()), h, "qjx_mbl_imbalance");
         }
         std::vector<double> mean_start(n);
         check(qjx_get_mean_start(h, mean_start.data()), h, "qjx_get_mean_start");
 
+        if (mbl && dump_obs == 1) {  // MBLCoreBehaviour::dump_std (core.cpp:4910-4937)
+            const size_t o = (size_t)last_dump * n;
+            save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
+            save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec.data() + o), n, 16, false);
+            save_double_data(path + "imbalance" + sfx, imbalance.data() + o, n, 16, false);
+        }
         if (jcs && dump_obs == 1) {  // JCSCoreBehaviour::dump_std (core.cpp:2976-2999)
             const size_t o = (size_t)last_dump * n;
             save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
             save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec.data() + o), n, 16, false);
         }
         // dump_std (core.cpp:918-957): values of the last dump
-        if (!jcs && dump_obs == 1) {
+        if (dimer && dump_obs == 1) {
             const size_t o = (size_t)last_dump * n;
             save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
             save_double_data(path + "mean_start" + sfx, mean_start.data(), n, 16, false);
@@ -598,13 +705,14 @@ int main(int argc, char **argv)
                 save_2d_inv_double_data(path + name + sfx, inv.data(), ndt, n, 16, false);
             };
             evo(D.norm, "norm_evo");
-            if (jcs) {  // JCSCoreBehaviour::dump_std_evo (core.cpp:3034-3102)
+            if (jcs || mbl) {  // JCS / MBL CoreBehaviour::dump_std_evo (core.cpp:3034-3102, 4988-5056)
                 std::vector<std::complex<double>> cinv((size_t)ndt * n);
                 for (int dmp = 0; dmp < nrec; dmp++)
                     for (int tr = 0; tr < n; tr++) cinv[(size_t)tr * ndt + dmp] = spec[(size_t)dmp * n + tr];
                 save_2d_inv_complex_data(path + "spec_evo" + sfx, reinterpret_cast<const double *>(cinv.data()), ndt, n,
                                          16, false);
-                evo(D.energy, "mean_evo");
+                if (jcs) evo(D.energy, "mean_evo");
+                else evo(imbalance, "imbalance_evo");
             } else {
                 evo(D.mean, "mean_evo");
                 evo(D.disp, "dispersion_evo");

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/qjx_b200.h"
+#include "qjx_config.h"
 
 namespace {
 
@@ -406,4 +407,145 @@ extern "C" qjx_status qjx_build_jcs(int N, double alpha, double drv_ampl, double
             ok = expm(d, scaled.data(), Utree + e2 * ((size_t)b * deep + lv)) && ok;
         }
     return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}
+
+// ---------------------------------------------------------------------------------------- MBL
+// MBLNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp): Nc cells, Nc/2 hard-core particles; the
+// basis is every Nc-bit word with Nc/2 bits set, ascending (init_sizes :209-257).
+
+static int bits_set(int v)
+{
+    int c = 0;
+    for (; v > 0; v >>= 1) c += v & 1;
+    return c;
+}
+
+// Two set bits that are neighbours: the words x, y are one hop apart iff x ^ y is such a pair.
+static bool one_hop(int g) { return bits_set(g) == 2 && bits_set(g & (g << 1)) == 1; }
+
+static std::vector<int> mbl_words(int Nc)
+{
+    std::vector<int> xs;
+    for (int x = 0; x < (1 << Nc); x++)
+        if (bits_set(x) == Nc / 2) xs.push_back(x);
+    return xs;
+}
+
+extern "C" qjx_status qjx_mbl_size(int Nc, int diss_type, int *d, int *num_diss)
+{
+    if (Nc < 2 || Nc > 24 || Nc % 2 || (diss_type != 0 && diss_type != 1)) return QJX_ERR_INVALID_ARG;
+    // C(Nc, Nc/2) by the multiplicative formula, exact in integers at every step
+    long long c = 1;
+    for (int i = 0; i < Nc / 2; i++) c = c * (Nc - i) / (i + 1);
+    if (d) *d = int(c);
+    if (num_diss) *num_diss = diss_type == 0 ? Nc : Nc - 1;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_build_mbl(int Nc, double W, double U, double J, int mbl_seed, int mbl_mns, int diss_type,
+                                    double diss_phase, double gamma, double T, int deep, double *energies,
+                                    int *id_to_x, double *H, double *L, double *Kout, double *Utree)
+{
+    int d = 0, nd = 0;
+    if (qjx_mbl_size(Nc, diss_type, &d, &nd) != QJX_OK || mbl_mns < 1 || mbl_seed < 0) return QJX_ERR_INVALID_ARG;
+    if (Utree && (deep < 1 || !(T > 0.0))) return QJX_ERR_INVALID_ARG;
+    const std::vector<int> xs = mbl_words(Nc);
+    const size_t dd = (size_t)d * d, e2 = 2 * dd;
+    // disorder (init_hamiltonians :891-905): uniform(-1, 1) from MCG31 seed 77778888, leapfrog
+    // stream (mbl_seed, mbl_mns), as a + (b - a) u
+    std::vector<double> en(Nc);
+    qjxio::LeapfrogLCG st = qjxio::LeapfrogLCG::mcg31(77778888ull, (unsigned long long)mbl_seed,
+                                                        (unsigned long long)mbl_mns);
+    for (int c = 0; c < Nc; c++) en[c] = -1.0 + (1.0 - -1.0) * st.next();
+    cvec h(e2, 0.0), l(e2 * nd, 0.0);
+    for (int s = 0; s < d; s++) {  // W sum_c n_c e_c, cell c = bit Nc-1-c (:907-918)
+        double sum = 0.0;
+        for (int c = 0; c < Nc; c++) sum += double((xs[s] >> (Nc - 1 - c)) & 1) * en[c];
+        sum *= 1.0 * W;
+        h[2 * ((size_t)s * d + s)] += sum;
+    }
+    for (int s = 0; s < d; s++)  // U n_c n_{c+1} (:924-928)
+        h[2 * ((size_t)s * d + s)] += U * bits_set(xs[s] & (xs[s] << 1));
+    for (int s = 0; s < d; s++)  // -J hops (:932-939)
+        for (int t = 0; t < d; t++) h[2 * ((size_t)s * d + t)] -= J * int(one_hop(xs[s] ^ xs[t]));
+    // dissipators (init_dissipators :1699-1795)
+    for (int c = 0; c < nd; c++) {
+        double *lc = l.data() + e2 * c;
+        for (int s = 0; s < d; s++) {
+            const int b0 = (xs[s] >> c) & 1, b1 = (xs[s] >> (c + 1)) & 1;
+            lc[2 * ((size_t)s * d + s)] = diss_type == 0 ? double(b0) : double(b0) - double(b1);
+            if (diss_type == 0 || b0 == b1) continue;
+            for (int t = 0; t < d; t++) {
+                const int g = xs[s] ^ xs[t];
+                if (!one_hop(g) || (g & -g) != (1 << c)) continue;  // the pair (c, c+1)
+                double *e = lc + 2 * ((size_t)s * d + t);
+                e[0] = b0 ? -std::cos(-diss_phase) : std::cos(diss_phase);
+                e[1] = b0 ? -std::sin(-diss_phase) : std::sin(diss_phase);
+            }
+        }
+    }
+    if (energies) std::memcpy(energies, en.data(), Nc * sizeof(double));
+    if (id_to_x) std::memcpy(id_to_x, xs.data(), d * sizeof(int));
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), e2 * nd * sizeof(double));
+    if (!Kout && !Utree) return QJX_OK;
+    // init_hamiltonians_qj (:2751-2838): H - (i/2) gamma L_c^H L_c added channel by channel, K = -i H_eff
+    cvec hp(e2, 0.0), k(e2);
+    for (size_t e = 0; e < dd; e++) hp[2 * e] = h[2 * e];
+    for (int c = 0; c < nd; c++) {
+        const double *lc = l.data() + e2 * c;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int q = 0; q < d; q++) {
+                    const double ar = lc[2 * ((size_t)q * d + i)], ai = lc[2 * ((size_t)q * d + i) + 1];
+                    const double br = lc[2 * ((size_t)q * d + j)], bi = lc[2 * ((size_t)q * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (gamma * si);
+                hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        k[2 * e] = 0.0 + hp[2 * e + 1];
+        k[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    if (Kout) std::memcpy(Kout, k.data(), e2 * sizeof(double));
+    if (!Utree) return QJX_OK;
+    // init_split_structure_mbl (core.cpp:10382-10432): a branch head of duration T whose two
+    // children each run the split tree of T (so a period is two T/2 halves of the same K)
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
+    for (int lv = 0; lv < deep; lv++) {
+        double dt = T * 0.5;
+        for (int q = 0; q <= lv; q++) dt *= 0.5;
+        cvec scaled(e2);
+        for (size_t e = 0; e < e2; e++) scaled[e] = k[e] * dt;
+        ok = expm(d, scaled.data(), Utree + e2 * (size_t)lv) && ok;
+    }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}
+
+// get_imbalance_mbl (source/cpp/QJX/QJX/experiment.cpp:1753-1800) for n rows adr [n][d]: the
+// cell occupations n_c = sum_s adr_s n_c(x_s) (s ascending), then (even cells - odd cells) / all.
+extern "C" qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double *out)
+{
+    int d = 0;
+    if (qjx_mbl_size(Nc, 0, &d, nullptr) != QJX_OK || n < 0 || (n > 0 && (!adr || !out))) return QJX_ERR_INVALID_ARG;
+    const std::vector<int> xs = mbl_words(Nc);
+#pragma omp parallel for schedule(static)
+    for (int tr = 0; tr < n; tr++) {
+        const double *a = adr + (size_t)tr * d;
+        std::vector<double> occ(Nc, 0.0);
+        for (int s = 0; s < d; s++)
+            for (int c = 0; c < Nc; c++) occ[c] += a[s] * double((xs[s] >> (Nc - 1 - c)) & 1);
+        double even = 0.0, odd = 0.0;
+        for (int c = 0; c < Nc; c++) (c % 2 == 0 ? even : odd) += occ[c];
+        const double all = odd + even;
+        out[tr] = (even - odd) / all;
+    }
+    return QJX_OK;
 }

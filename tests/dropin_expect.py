@@ -47,6 +47,11 @@ def f_2d_inv(rows_by_cols):  # array [rows][cols]
     return "".join("".join(fmt_double(x) + " " for x in row) + "\n" for row in rows_by_cols)
 
 
+def f_2d_inv_complex(rows_by_cols):  # save_2d_inv_complex_data: "re im " pairs, rows = dumps
+    return "".join("".join(fmt_double(z.real) + " " + fmt_double(z.imag) + " " for z in row) + "\n"
+                   for row in rows_by_cols)
+
+
 def f_2d_complex(rows_by_cols):
     return "".join("\t".join("(%s,%s)" % (fmt_double(z.real), fmt_double(z.imag)) for z in row) + "\n"
                    for row in rows_by_cols)
@@ -54,8 +59,18 @@ def f_2d_complex(rows_by_cols):
 
 def suffix(cfg, prm):
     """DimerOutputBehavior::suffix_param with precision 4 (outputter.cpp:3-44, 353-388);
-    JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133)."""
+    JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
+    for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 3:
+        return ("_setup(%d_%d_%d)" % (3, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_Nc(%d)" % int(prm["mbl_Nc"])
+                + "_rnd(%d_%d)" % (int(prm["mbl_seed"]), int(prm["mbl_mns"]))
+                + "_diss(%d_%s_%s)" % (int(prm["diss_type"]), f4(prm["diss_phase"]), f4(prm["diss_gamma"]))
+                + "_prm(%s_%s_%s)" % (f4(prm["mbl_prm_W"]), f4(prm["mbl_prm_U"]), f4(prm["mbl_prm_J"]))
+                + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"]))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 1:
         return ("_setup(%d_%d_%d)" % (1, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -86,9 +101,13 @@ def expected_outputs(cfg, prm, R=None):
     """All files the drop-in writes, as {relative file name: text}."""
     if cfg.get("task_id", 1) == 7:
         return expected_lpn_outputs(cfg, prm, R)
-    N = int(prm["N"])
     jcs = cfg.get("sys_id", 0) == 1
+    mbl = cfg.get("sys_id", 0) == 3
+    N = 0 if mbl else int(prm["N"])
     d = N if jcs else N + 1
+    if mbl:
+        Nc = int(prm["mbl_Nc"])
+        d = len(O.mbl_basis(Nc))
     n = cfg["num_trajectories"]
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
@@ -107,6 +126,16 @@ def expected_outputs(cfg, prm, R=None):
         T = t_head = alpha
         ens = O.Ensemble(U, L, [1.0], HE, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
                          branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+    elif mbl:  # MBL: one head of duration mbl_T, two children of the same tree; spec = <H> / W
+        en, H, Ls, K = O.mbl_operators(Nc, prm["mbl_prm_W"], prm["mbl_prm_U"], prm["mbl_prm_J"], int(prm["mbl_seed"]),
+                                       int(prm["mbl_mns"]), int(prm["diss_type"]), prm["diss_phase"],
+                                       prm["diss_gamma"])
+        T = prm["mbl_T"]
+        Ut = O.split_tree(K, T, deep)
+        U = np.stack([Ut, Ut])
+        HE = H
+        Rs = np.concatenate([H[None], R]) if nr else H[None]
+        ens = O.Ensemble(U, Ls, [1.0] * Ls.shape[0], HE, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
     else:
         H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
                                              prm["dimer_drv_ampl"], prm["diss_gamma"])
@@ -133,7 +162,16 @@ def expected_outputs(cfg, prm, R=None):
         return rc
 
     files = {}
-    if cfg.get("is_debug", 0):
+    if mbl:  # newdel.cpp:903-905: written to the working directory
+        files["energies" + sfx] = f_double_data(en)
+    if mbl and cfg.get("is_debug", 0):
+        files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
+        for c in range(Ls.shape[0]):
+            files[path + "dissipator_%d" % c + sfx] = f_complex_data(Ls[c].reshape(-1))
+        files[path + "hamiltonians_qj_0" + sfx] = f_complex_data(K.reshape(-1))
+        files[path + "spec_mtx" + sfx] = f_complex_data(H.reshape(-1))
+        files[path + "exp_mtx_0" + sfx] = f_complex_data(Ut[-1].reshape(-1))
+    elif cfg.get("is_debug", 0):
         files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
         files[path + "dissipator_0" + sfx] = f_complex_data(L.reshape(-1))
         files[path + "hamiltonians_qj_0" + sfx] = f_complex_data(K0.reshape(-1))
@@ -217,15 +255,22 @@ def expected_outputs(cfg, prm, R=None):
     last = obs[-1]
     if dump_purity == 1:
         emit("purity_evo" + sfx, f_double_data(purity), False)
-    if jcs:
+    if jcs or mbl:
+        div = alpha if jcs else prm["mbl_prm_W"]
         for o in obs:
-            z = o["random_obs"][:, 0]  # result.real /= alpha; result.imag /= alpha (real divisions)
-            o["spec"] = z.real / alpha + 1j * (z.imag / alpha)
+            z = o["random_obs"][:, 0]  # result.real /= div; result.imag /= div (real divisions)
+            o["spec"] = z.real / div + 1j * (z.imag / div)
             o["random_obs"] = o["random_obs"][:, 1:]
+            if mbl:
+                o["imbalance"] = O.mbl_imbalance(Nc, o["adr"])
+    if mbl and int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("spec" + sfx, f_complex_data(last["spec"]), False)
+        emit("imbalance" + sfx, f_double_data(last["imbalance"]), False)
     if jcs and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("spec" + sfx, f_complex_data(last["spec"]), False)
-    if not jcs and int(prm["dump_obs"]) == 1:
+    if not jcs and not mbl and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
         emit("mean" + sfx, f_double_data(last["mean"]), False)
@@ -241,6 +286,7 @@ def expected_outputs(cfg, prm, R=None):
     if evo_sep == 1 and int(prm["dump_obs"]) == 1:
         emit("periods" + sfx, f_int_data(dp), False)
         keys = ((("norm", "norm_evo"), ("energy", "mean_evo")) if jcs else
+                (("norm", "norm_evo"), ("imbalance", "imbalance_evo")) if mbl else
                 (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
                  ("energy", "energy_evo")))
         for key, name in keys:
@@ -248,7 +294,7 @@ def expected_outputs(cfg, prm, R=None):
             for i, o in enumerate(obs):
                 grid[i] = o[key]
             emit(name + sfx, f_2d_inv(grid), False)
-        if jcs:
+        if jcs or mbl:
             grid = np.zeros((ndt, n), complex)
             for i, o in enumerate(obs):
                 grid[i] = o["spec"]
@@ -275,21 +321,35 @@ def expected_lpn_outputs(cfg, prm, R=None):
     """LpnMult (task_id 7): LpnMultExperimentBehaviour::trans_process / obser_process
     (experiment.cpp:138-286) with dump_std, dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127)
     and the adr files (dump.cpp:3-98)."""
-    N = int(prm["N"])
+    mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
+    N = 0 if mbl else int(prm["N"])
     d = N + 1
+    if mbl:
+        Nc, W = int(prm["mbl_Nc"]), float(prm["mbl_prm_W"])
+        d = len(O.mbl_basis(Nc))
     n = cfg["num_trajectories"]
     half = n // 2
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
     path = cfg.get("path", "")
     sfx = suffix(cfg, prm)
-    H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
-                                         prm["dimer_drv_ampl"], prm["diss_gamma"])
-    T = TWO_PI / prm["dimer_drv_freq"]
-    U = np.stack([O.split_tree(K0, T, deep), O.split_tree(K1, T, deep)])
-    HE = H + prm["dimer_prm_E"] * Hd
     nr = int(prm["num_random_obs"])
-    ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
+    if mbl:
+        en, H, L, K = O.mbl_operators(Nc, W, prm["mbl_prm_U"], prm["mbl_prm_J"], int(prm["mbl_seed"]),
+                                      int(prm["mbl_mns"]), int(prm["diss_type"]), prm["diss_phase"], prm["diss_gamma"])
+        T = prm["mbl_T"]
+        Ut = O.split_tree(K, T, deep)
+        Rs = np.concatenate([H[None], R]) if nr else H[None]
+        ens = O.Ensemble(np.stack([Ut, Ut]), L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]),
+                         rec_cap=100000)
+    else:
+        H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
+                                             prm["dimer_drv_ampl"], prm["diss_gamma"])
+        T = TWO_PI / prm["dimer_drv_freq"]
+        U = np.stack([O.split_tree(K0, T, deep), O.split_tree(K1, T, deep)])
+        HE = H + prm["dimer_prm_E"] * Hd
+        ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]),
+                         rec_cap=100000)
     ens.init(int(prm["start_type"]), int(prm["start_state"]))
     prop = cfg.get("prop_id", 0)
     period = [0]
@@ -310,7 +370,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
                eps_low=float(prm["lpn_eps_low"]), eps_high=float(prm["lpn_eps_high"]),
                eps_error=float(prm["lpn_eps_error"]), delta_s=float(prm["lpn_delta_s"]),
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
-               per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy)
+               per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
+               mbl_Nc=Nc if mbl else 0, spec_div=W if mbl else 1.0)
     dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
     ndt = len(dp)
     assert advance(cfg.get("num_tp_periods", 0), is_obs=0, tr1=half) == 0
@@ -318,6 +379,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
     ens.t[:] = 0.0
     period[0] = 0
     obs = [ens.observables(is_start=True, want_adr=True)]
+    if mbl:
+        obs[0]["imbalance"] = O.mbl_imbalance(Nc, obs[0]["adr"])
     lpn = [lp.values()]
     save_lambdas = int(prm["save_lambdas"])
     recs = {k: [[] for _ in range(n)] for k in ("ratio", "delta_s", "delta_f")}
@@ -345,6 +408,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
         for period_id in range(dp[dump_id - 1], dp[dump_id]):
             assert advance(1) == 0
             o = ens.observables(want_adr=True)
+            if mbl:  # calc_chars_std before lambda_lpn: the pre-update adr rows
+                o["imbalance"] = O.mbl_imbalance(Nc, o["adr"])
             lp.period((period_id + 1) * T)
             o["adr"][half:] = ens.observables(want_adr=True)["adr"][half:]
             last = lp.last()
@@ -360,7 +425,23 @@ def expected_lpn_outputs(cfg, prm, R=None):
         if evo_avg == 1 and adr_avg_on == 1:
             emit("adr_avg" + sfx, f_double_data(adr_avg(o["adr"], half)), True)
     last = obs[-1]
-    if int(prm["dump_obs"]) == 1:
+    ro = 1 if mbl else 0
+    if mbl:
+        for o in obs:
+            z = o["random_obs"][:, 0]
+            o["spec"] = z.real / W + 1j * (z.imag / W)
+        for v in lpn:
+            z = v["robs_lpn"][:, 0]
+            v["spec_lpn"] = z.real / W + 1j * (z.imag / W)
+    if mbl and int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("spec" + sfx, f_complex_data(last["spec"]), False)
+        emit("imbalance" + sfx, f_double_data(last["imbalance"]), False)
+        emit("lambda" + sfx, f_double_data(lpn[-1]["lambda_now"]), False)
+        emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
+        emit("spec_lpn" + sfx, f_complex_data(lpn[-1]["spec_lpn"]), False)
+        emit("imbalance_lpn" + sfx, f_double_data(lpn[-1]["mean_lpn"]), False)
+    if int(prm["dump_obs"]) == 1 and not mbl:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
         emit("mean" + sfx, f_double_data(last["mean"]), False)
@@ -371,6 +452,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
         emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
         emit("mean_lpn" + sfx, f_double_data(lpn[-1]["mean_lpn"]), False)
         emit("energy_lpn" + sfx, f_double_data(lpn[-1]["energy_lpn"]), False)
+    if int(prm["dump_obs"]) == 1:
         if save_lambdas > 0:
             for tr in range(n):
                 emit("delta_f_by_delta_s_%d" % tr + sfx, f_double_data(recs["ratio"][tr]), False)
@@ -378,11 +460,15 @@ def expected_lpn_outputs(cfg, prm, R=None):
                 emit("deltas_f_%d" % tr + sfx, f_double_data(recs["delta_f"][tr]), False)
     if evo_sep == 1 and int(prm["dump_obs"]) == 1:
         emit("periods" + sfx, f_int_data(dp), False)
-        for key, name in (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"),
-                          ("m2", "m2_evo"), ("energy", "energy_evo")):
+        keys = ((("norm", "norm_evo"), ("imbalance", "imbalance_evo")) if mbl else
+                (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
+                 ("energy", "energy_evo")))
+        for key, name in keys:
             emit(name + sfx, f_2d_inv(np.array([o[key] for o in obs])), False)
+        if mbl:
+            emit("spec_evo" + sfx, f_2d_inv_complex(np.array([o["spec"] for o in obs])), False)
         for o_id in range(nr):
-            rows = [o["random_obs"][:, o_id] for o in obs]
+            rows = [o["random_obs"][:, ro + o_id] for o in obs]
             emit("random_obs_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
         if int(prm["jump"]) > 0:
             for tr in range(n):
@@ -392,17 +478,27 @@ def expected_lpn_outputs(cfg, prm, R=None):
                 if int(prm["jump"]) > 1:
                     emit("jump_norms_%d" % tr + sfx, f_double_data(nm), False)
                     emit("jump_etas_%d" % tr + sfx, f_double_data(et), False)
-        for key, name in (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo"), ("energy_lpn", "energy_lpn_evo")):
+        keys = ((("lambda_now", "lambda_evo"), ("mean_lpn", "imbalance_lpn_evo")) if mbl else
+                (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo"), ("energy_lpn", "energy_lpn_evo")))
+        for key, name in keys:
             emit(name + sfx, f_2d_inv(np.array([v[key] for v in lpn])), False)
+        if mbl:
+            emit("spec_lpn_evo" + sfx, f_2d_inv_complex(np.array([v["spec_lpn"] for v in lpn])), False)
         for o_id in range(nr):
-            rows = [v["robs_lpn"][:, o_id] for v in lpn]
+            rows = [v["robs_lpn"][:, ro + o_id] for v in lpn]
             emit("random_obs_lpn_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
     if evo_avg == 0 and adr_avg_on == 1:
         emit("adr_avg" + sfx, f_double_data(adr_avg(last["adr"], half)), False)
+    if mbl:  # newdel.cpp:903-905: written to the working directory
+        acc["energies" + sfx] = f_double_data(en)
     return acc
 
 
 JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_1": 0.5, "jcs_drv_part_2": 1.5}
+
+# the production MBL sweeps' values (Nc 8, diss_type 1, gamma 0.1, J 1, T 10), one disorder seed
+MBL_PARAMS = {"mbl_Nc": 8, "mbl_seed": 3, "mbl_mns": 1000000, "mbl_prm_W": 2.5, "mbl_prm_U": 1.0, "mbl_prm_J": 1.0,
+              "mbl_T": 10.0, "diss_type": 1, "diss_gamma": 0.1, "diss_phase": 0.0}
 
 LPN_PARAMS = {
     "lpn_type": 0, "lpn_eps_deep": 100, "lpn_eps_error": 1.0e-10, "lpn_eps_high": 10, "lpn_eps_low": -10,

@@ -5,7 +5,8 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, config_text, params_text, suffix
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS, config_text, params_text,
+                                 suffix)
 
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
 
@@ -68,7 +69,24 @@ def test_jcs_suffix_matches_reference_rule(tmp_path, over):
     assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_prm(5.0000)" in line
 
 
-@pytest.mark.parametrize("key,val", [("sys_id", 3), ("task_id", 9), ("prop_id", 2)])
+@pytest.mark.parametrize("over", [{}, {"diss_type": 0, "diss_phase": 0.125, "mbl_seed": 17, "mbl_prm_W": 12.0}])
+def test_mbl_suffix_matches_reference_rule(tmp_path, over):
+    """MBLOutputBehavior::suffix_param (outputter.cpp:176-212): a second _rnd() with the disorder
+    stream, and diss() in the order type, phase, gamma."""
+    cfg = dict(BASE_CONFIG, sys_id=3)
+    prm = {**BASE_PARAMS, **MBL_PARAMS, **over}
+    r = check(tmp_path, cfg, prm)
+    assert r.returncode == 0, r.stdout
+    line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
+    assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_Nc(8)_rnd(" in line
+
+
+def test_mbl_other_tasks_exit_with_error(tmp_path):
+    r = check(tmp_path, dict(BASE_CONFIG, sys_id=3, task_id=4), {**BASE_PARAMS, **MBL_PARAMS})
+    assert r.returncode != 0 and "Error: Wrong task_id / prop_id for sys_id 3" in r.stdout
+
+
+@pytest.mark.parametrize("key,val", [("sys_id", 5), ("task_id", 9), ("prop_id", 2)])
 def test_unsupported_ids_exit_with_error(tmp_path, key, val):
     r = check(tmp_path, dict(BASE_CONFIG, **{key: val}), BASE_PARAMS)
     assert r.returncode != 0 and "Error: Wrong " + key in r.stdout

@@ -1,14 +1,15 @@
 """The drop-in executable (os_d_b200/qjx_b200) on a GPU, compared file by file with the
 reference's Std-task outputs computed by the CPU oracle on the same inputs."""
 import copy
+import math
 import os
 import subprocess
 
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, config_text, expected_outputs,
-                                 params_text)
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS, config_text,
+                                 expected_outputs, params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -23,6 +24,7 @@ def run_case(tmp_path, cfg, prm):
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     d = int(prm["N"]) + 1
     d = int(prm["N"]) if cfg.get("sys_id", 0) == 1 else d
+    d = math.comb(int(prm["mbl_Nc"]), int(prm["mbl_Nc"]) // 2) if cfg.get("sys_id", 0) == 3 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -105,6 +107,36 @@ def test_lpn_mult_every_period_rk(tmp_path):
     prm = {**BASE_PARAMS, **LPN_PARAMS, "lpn_type": -1, "lambda_per_periods": 1, "dump_type": 1, "dump_num": 2,
            "dump_evo_avg": 1, "dump_adr_avg": 1, "num_random_obs": 2}
     run_case(tmp_path, cfg, prm)
+
+
+@pytest.mark.parametrize("diss_type", [1, 0])
+def test_mbl_system_files_match(tmp_path, diss_type):
+    """The MBL system (sys_id 3): 70 basis words of 8 cells, 7 hop-dissipators (diss_type 1) or 8
+    occupation dissipators (diss_type 0), spec = <H> / W and the imbalance from the adr rows
+    (newdel.cpp:182-271, 868-958, 1699-1815, 2751-2838; experiment.cpp:1705-1800; core.cpp:4190-5056)."""
+    cfg = dict(BASE_CONFIG, sys_id=3, num_trajectories=16, num_tp_periods=1, num_obs_periods=4, is_debug=1)
+    prm = {**BASE_PARAMS, **MBL_PARAMS, "diss_type": diss_type, "dump_num": 2, "jump": 2, "dump_adr_sep": 1,
+           "dump_adr_avg": 1, "start_state": 5}
+    exp = run_case(tmp_path, cfg, prm)
+    assert any(k.startswith("imbalance_evo") for k in exp) and any(k.startswith("energies") for k in exp)
+    types = set()
+    for k, v in exp.items():
+        if k.startswith("diss_types_"):
+            types.update(int(x) for x in v.split())
+    assert len(types) > 3  # several channels chosen
+
+
+@pytest.mark.parametrize("lpn_type", [-1, -2, 0])
+def test_mbl_lpn_mult_files_match(tmp_path, lpn_type):
+    """MBL LpnMult (sys_id 3, task_id 7; the production MBL sweeps, submit_mbl.py): spec, imbalance
+    and random-observable distances, the MBL file set (core.cpp:4910-5096) incl. save_lambdas."""
+    cfg = dict(BASE_CONFIG, sys_id=3, task_id=7, num_trajectories=16, num_tp_periods=2, num_obs_periods=5)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **MBL_PARAMS, "lpn_type": lpn_type, "dump_num": 5, "jump": 1,
+           "dump_adr_sep": 1, "dump_adr_avg": 1, "save_lambdas": 1, "lpn_delta_f_high": 1e-2}
+    exp = run_case(tmp_path, cfg, prm)
+    k = [k for k in exp if k.startswith("num_renorms")][0]
+    assert sum(int(x) for x in exp[k].split()) > 0  # renormalisations happened
+    assert any(k.startswith("imbalance_lpn_evo") for k in exp) and any(k.startswith("spec_lpn_evo") for k in exp)
 
 
 def test_jcs_system_files_match(tmp_path):
