@@ -207,12 +207,15 @@ typedef struct {
     double delta_s;       /* lpn_delta_s: target distance after a perturbation */
     double delta_f_high, delta_f_low;  /* lpn_delta_f_high / lpn_delta_f_low */
     double max_energy;    /* max |Re H_ii| of the hamiltonian (init_obs_lpn, newdel_exp.cpp:540-550) */
-    /* MBL characteristics (MBLCoreBehaviour, core.cpp:4729-4902) when mbl_Nc > 0: every ensemble
-     * has d = C(mbl_Nc, mbl_Nc/2), random-observable slot 0 holds H and spec = slot 0 / spec_div (W);
-     * mean_lpn is the imbalance; lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v - imbalance_b|,
-     * k >= 0 = random observable slot k + 1.  0 = the dimer's characteristics. */
+    /* System characteristics (0 / 0: the dimer's).  MBL (MBLCoreBehaviour, core.cpp:4729-4902)
+     * when mbl_Nc > 0: every ensemble has d = C(mbl_Nc, mbl_Nc/2), random-observable slot 0 holds H,
+     * spec = slot 0 / spec_div (W), mean_lpn is the imbalance, lpn_type -1 = |spec_b - spec_v|, -2 =
+     * |imbalance_v - imbalance_b|.  JCS (JCSCoreBehaviour, core.cpp:2739-2975) when jcs = 1: slot 0
+     * holds a, spec = slot 0 / spec_div (alpha), mean_lpn is <a^+ a> (the energy observable with
+     * Nop), lpn_type -1 = |spec_b - spec_v|, -2 = |n_v - n_b| / d.  For both, k >= 0 = random
+     * observable slot k + 1. */
     int mbl_Nc;
-    int pad2;
+    int jcs;
     double spec_div;
 } qjx_lpn_config;
 /* After the bases' transient (trans_process, experiment.cpp:138-183): copy every base into its

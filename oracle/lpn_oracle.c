@@ -192,27 +192,31 @@ static void lpn_chars(const orc_problem *p, const double *phi, int want, int rob
 
 /* what calc_delta_s / calc_delta_f need of a state: a CH_ part (delta_want) and / or one random
  * observable slot (delta_one, -1 none) */
+static int spec_sys(const orc_lpn_config *cfg) { return cfg->mbl_Nc > 0 || cfg->jcs; }
+
 static int delta_want(const orc_lpn_config *cfg)
 {
     if (cfg->mbl_Nc > 0) return cfg->lpn_type == -2 ? CH_MEAN : 0;
+    if (cfg->jcs) return cfg->lpn_type == -2 ? CH_ENERGY : 0;
     return cfg->lpn_type == -1 ? CH_MEAN : cfg->lpn_type == -2 ? CH_ENERGY : 0;
 }
 
 static int delta_one(const orc_lpn_config *cfg)
 {
-    if (cfg->mbl_Nc > 0) return cfg->lpn_type == -1 ? 0 : cfg->lpn_type >= 0 ? cfg->lpn_type + 1 : -1;
+    if (spec_sys(cfg)) return cfg->lpn_type == -1 ? 0 : cfg->lpn_type >= 0 ? cfg->lpn_type + 1 : -1;
     return cfg->lpn_type >= 0 ? cfg->lpn_type : -1;
 }
 
 /* calc_delta_s / calc_delta_f (dimer core.cpp:839-901; MBL core.cpp:4823-4901): var against base */
 static double lpn_delta(const orc_problem *p, const orc_lpn_config *cfg, const chars_t *v, const chars_t *b)
 {
-    if (cfg->mbl_Nc > 0 && cfg->lpn_type == -1) { /* spec = <H> / W, real divisions */
+    if (spec_sys(cfg) && cfg->lpn_type == -1) { /* spec = <H> / W or <a> / alpha, real divisions */
         const double dr = b->robs[0] / cfg->spec_div - v->robs[0] / cfg->spec_div;
         const double di = b->robs[1] / cfg->spec_div - v->robs[1] / cfg->spec_div;
         return sqrt(dr * dr + di * di);
     }
     if (cfg->mbl_Nc > 0 && cfg->lpn_type == -2) return fabs(v->mean - b->mean);
+    if (cfg->jcs && cfg->lpn_type == -2) return fabs(v->energy - b->energy) / (double)p->d;
     if (cfg->lpn_type == -1) return fabs(v->mean - b->mean) / (double)p->d;
     if (cfg->lpn_type == -2) return fabs(v->energy - b->energy) / cfg->max_energy;
     const int o = delta_one(cfg);
@@ -224,7 +228,8 @@ static int lpn_type_ok(const orc_problem *p, const orc_lpn_config *cfg)
 {
     if (cfg->mbl_Nc > 0 && (orc_mbl_basis(cfg->mbl_Nc, NULL) != p->d || cfg->mbl_Nc > 24 || p->num_robs < 1))
         return 0;
-    const int shift = cfg->mbl_Nc > 0 ? 1 : 0;
+    if (cfg->jcs && p->num_robs < 1) return 0;
+    const int shift = spec_sys(cfg) ? 1 : 0;
     return cfg->lpn_type == -1 || cfg->lpn_type == -2 ||
            (cfg->lpn_type >= 0 && cfg->lpn_type + shift < p->num_robs);
 }
@@ -290,9 +295,9 @@ static int var_trajectory(const orc_problem *p, const orc_lpn_config *cfg, orc_l
     return deep;
 }
 
-static void store_chars(const orc_problem *p, orc_lpn *lp, int tr, const chars_t *c)
+static void store_chars(const orc_problem *p, const orc_lpn_config *cfg, orc_lpn *lp, int tr, const chars_t *c)
 {
-    lp->mean_lpn[tr] = c->mean;
+    lp->mean_lpn[tr] = cfg->jcs ? c->energy : c->mean; /* JCS: get_num_photons_jcs */
     lp->energy_lpn[tr] = c->energy;
     for (int o = 0; o < p->num_robs; o++) {
         lp->robs_lpn[2 * ((size_t)tr * p->num_robs + o)] = c->robs[2 * o];
@@ -330,14 +335,14 @@ int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg,
                 double *pb = s->phi + 2 * (size_t)b * d, *pv = s->phi + 2 * (size_t)v * d;
                 chars_t bc, vc;
                 lpn_chars(p, pb, full, -1, xh, sm, &bc, cfg->mbl_Nc, words);
-                store_chars(p, lp, b, &bc);
+                store_chars(p, cfg, lp, b, &bc);
                 /* copy_trajectory_lpn + var_trajectory_lpn */
                 memcpy(pv, pb, sizeof(double) * 2 * d);
                 copy_stream(s, v, b);
                 lp->eps_iters[v] = var_trajectory(p, cfg, lp, pb, pv, v, &bc, w, xh, sm, &lp->eps[v], words);
                 /* calc_chars_lpn_start: delta_s from the std characteristics (calc_delta_f) */
                 lpn_chars(p, pv, full, -1, xh, sm, &vc, cfg->mbl_Nc, words);
-                store_chars(p, lp, v, &vc);
+                store_chars(p, cfg, lp, v, &vc);
                 lp->delta_s[v] = lpn_delta(p, cfg, &vc, &bc);
                 lp->delta_s[b] = 0.0;
                 lp->lambda[b] = lp->lambda[v] = 0.0;
@@ -379,7 +384,7 @@ int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg
                 chars_t bc, vf, vc;
                 /* calc_chars_lpn of the base (its std characteristics are the same numbers) */
                 lpn_chars(p, pb, full, -1, xh, sm, &bc, cfg->mbl_Nc, words);
-                store_chars(p, lp, b, &bc);
+                store_chars(p, cfg, lp, b, &bc);
                 /* calc_delta_f from the variation's std characteristics */
                 lpn_chars(p, pv, want, one, xh, sm, &vf, cfg->mbl_Nc, words);
                 const double df = lpn_delta(p, cfg, &vf, &bc);
@@ -398,12 +403,12 @@ int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg
                     copy_stream(s, v, b);
                     lp->eps_iters[v] = var_trajectory(p, cfg, lp, pb, pv, v, &bc, w, xh, sm, &lp->eps[v], words);
                     lpn_chars(p, pv, full, -1, xh, sm, &vc, cfg->mbl_Nc, words);
-                    store_chars(p, lp, v, &vc);
+                    store_chars(p, cfg, lp, v, &vc);
                     lp->delta_s[v] = lpn_delta(p, cfg, &vc, &bc);
                     lp->lambda_now[v] = lp->lambda[v] / curr_time;
                 } else {
                     lpn_chars(p, pv, full, -1, xh, sm, &vc, cfg->mbl_Nc, words);
-                    store_chars(p, lp, v, &vc);
+                    store_chars(p, cfg, lp, v, &vc);
                     lp->lambda_now[v] = (lp->lambda[v] + orc_lpn_log(df / ds + 1.0e-16)) / curr_time;
                 }
             }

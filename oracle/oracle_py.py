@@ -36,7 +36,7 @@ class OrcLpnConfig(C.Structure):
     _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
                 ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
                 ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
-                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("pad2", C.c_int), ("spec_div", C.c_double)]
+                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("jcs", C.c_int), ("spec_div", C.c_double)]
 
 
 class OrcLpn(C.Structure):
@@ -318,13 +318,13 @@ class Lpn:
 
     def __init__(self, ens, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10,
                  delta_s=1e-3, delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0, mbl_Nc=0,
-                 spec_div=1.0):
+                 spec_div=1.0, jcs=0):
         self.ens = ens
         n = ens.n
         self.cfg = OrcLpnConfig(lpn_type=lpn_type, eps_deep=eps_deep, per_period=int(per_period), eps_low=eps_low,
                                 eps_high=eps_high, eps_error=eps_error, delta_s=delta_s,
                                 delta_f_high=delta_f_high, delta_f_low=delta_f_low, max_energy=max_energy,
-                                mbl_Nc=mbl_Nc, spec_div=spec_div)
+                                mbl_Nc=mbl_Nc, spec_div=spec_div, jcs=int(jcs))
         self.a = {k: np.zeros(n) for k in ("lambda", "lambda_now", "delta_s", "mean_lpn", "energy_lpn", "ratio",
                                            "ds_rec", "df_rec", "eps")}
         self.robs_lpn = np.zeros((n, max(ens.R.shape[0], 1)), np.complex128)

@@ -185,9 +185,11 @@ typedef struct {
     double max_energy;   /* max |Re H_ii| (lpn_type -2) */
     /* MBL characteristics (MBLCoreBehaviour, core.cpp:4729-4902) when mbl_Nc > 0: random-observable
      * slot 0 holds H and spec = slot 0 / spec_div (W); mean = the imbalance of the adr row;
-     * lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v - imbalance_b|, k >= 0 = slot k + 1. */
+     * lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v - imbalance_b|, k >= 0 = slot k + 1.
+     * JCS (JCSCoreBehaviour, core.cpp:2739-2975) when jcs = 1: slot 0 holds a, spec = slot 0 / alpha,
+     * mean_lpn = <a^+ a> (the energy observable), -1 = |spec_b - spec_v|, -2 = |n_v - n_b| / d. */
     int mbl_Nc;
-    int pad2;
+    int jcs;
     double spec_div;
 } orc_lpn_config;
 

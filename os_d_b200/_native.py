@@ -45,7 +45,7 @@ class QjxLpnConfig(C.Structure):
     _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
                 ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
                 ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
-                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("pad2", C.c_int), ("spec_div", C.c_double)]
+                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("jcs", C.c_int), ("spec_div", C.c_double)]
 
 
 class QjxStats(C.Structure):

@@ -63,13 +63,18 @@ void write_2d_inv(const std::string &fn, const std::vector<double> &v, int nrec,
 // n/2 + b starts as its base perturbed to delta_s, and after every observation period the
 // variations' Lyapunov sums are updated (lambda_lpn / lambda_lpn_now).  Files: dump_std,
 // dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127), adr files (dump.cpp:3-98).
-// MBL (Nc > 0; MBLCoreBehaviour, core.cpp:4677-5105): H rides in random-observable slot 0, spec
-// = slot 0 / W, the mean characteristics are imbalances, and the file set is MBL's.
+// JCS (sys_id 1; JCSCoreBehaviour, core.cpp:2739-3150) and MBL (sys_id 3; MBLCoreBehaviour,
+// core.cpp:4677-5105): the spec operator (a or H) rides in random-observable slot 0, spec = slot 0
+// / spec_div (alpha or W); the mean characteristics are <a^+ a> (JCS) or imbalances (MBL); each
+// system writes its own file set.  calc_T is the period of the Lyapunov time (calc_T: JCS
+// part_1 alpha + part_2 alpha, core.cpp:2833-2845).
 void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, const qjx_config &cfg,
-                  const std::vector<double> &H, int d, int num_robs, int robs_seed, int Nc = 0, double W = 1.0)
+                  const std::vector<double> &H, int d, int num_robs, int robs_seed, int sys, int Nc, double spec_div,
+                  double calc_T)
 {
-    const bool mbl = Nc > 0;
-    const int ro = mbl ? 1 : 0, nr = num_robs + ro;  // engine slots: [spec,] random observables
+    const bool mbl = sys == 3, jcs = sys == 1, spec = mbl || jcs;
+    const double W = spec_div;
+    const int ro = spec ? 1 : 0, nr = num_robs + ro;  // engine slots: [spec,] random observables
     const int n = cp.num_trajectories, half = n / 2;
     if (n < 2 || (n & 1)) die("LpnMult needs an even num_trajectories >= 2");
     const std::string &sfx = cp.fn_suffix;
@@ -89,8 +94,9 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     lc.delta_f_high = param(cp, "lpn_delta_f_high");
     lc.delta_f_low = param(cp, "lpn_delta_f_low");
     const int save_lambdas = int(param(cp, "save_lambdas"));
-    lc.mbl_Nc = Nc;
-    lc.spec_div = W;
+    lc.mbl_Nc = mbl ? Nc : 0;
+    lc.jcs = jcs ? 1 : 0;
+    lc.spec_div = spec_div;
     lc.max_energy = 0.0;  // init_obs_lpn (newdel_exp.cpp:540-550)
     for (int st = 0; st < d; st++) {
         const double v = std::fabs(H[2 * ((size_t)st * d + st)]);
@@ -196,7 +202,9 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
             const int one = 1;
             check(qjx_run_periods(h, 1, 1, at_dump ? &one : nullptr, at_dump ? 1 : 0, dump_id), h, "qjx_run_periods");
             if (at_dump) take_imbalance(dump_id);
-            check(qjx_lpn_period(h, double(period_id + 1) * cfg.T, at_dump ? dump_id : -1), h, "qjx_lpn_period");
+            // JCS's calc_chars_lpn leaves abs_diag_rho_all alone: its adr rows stay the std ones
+            check(qjx_lpn_period(h, double(period_id + 1) * calc_T, (at_dump && !jcs) ? dump_id : -1), h,
+                  "qjx_lpn_period");
             after_lpn(false);
         }
         if (dp[dump_id] == dp[dump_id - 1]) {  // no period ran: adr of the current states (abs_diag_rho_all)
@@ -227,7 +235,7 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     // MBL spec = <H> / W per trajectory (get_spec_mbl, experiment.cpp:1705-1751): std [dump][tr], lpn
     auto spec_of = [&](const std::vector<std::complex<double>> &src) {
         std::vector<std::complex<double>> out(src.size() / (nr ? nr : 1));
-        for (size_t i = 0; i < out.size() && mbl; i++)
+        for (size_t i = 0; i < out.size() && spec; i++)
             out[i] = std::complex<double>(src[i * nr].real() / W, src[i * nr].imag() / W);
         return out;
     };
@@ -250,7 +258,16 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         save_complex_data(path + "spec_lpn" + sfx, reinterpret_cast<const double *>(spec_lpn.data() + o), n, 16, false);
         save_double_data(path + "imbalance_lpn" + sfx, mean_lpn_evo.data() + o, n, 16, false);
     }
-    if (dump_obs == 1 && !mbl) {
+    if (dump_obs == 1 && jcs) {  // JCSCoreBehaviour::dump_std / dump_lpn (core.cpp:2976-3033)
+        const size_t o = (size_t)last_dump * n;
+        save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);
+        save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec_std.data() + o), n, 16, false);
+        save_double_data(path + "lambda" + sfx, lam_evo.data() + o, n, 16, false);
+        save_int_data(path + "num_renorms" + sfx, renorms.data(), n, false);
+        save_complex_data(path + "spec_lpn" + sfx, reinterpret_cast<const double *>(spec_lpn.data() + o), n, 16, false);
+        save_double_data(path + "mean" + sfx, mean_lpn_evo.data() + o, n, 16, false);
+    }
+    if (dump_obs == 1 && !spec) {
         const size_t o = (size_t)last_dump * n;
         save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);  // dump_std
         save_double_data(path + "mean_start" + sfx, mean_start.data(), n, 16, false);
@@ -278,6 +295,9 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         if (mbl) {  // MBLCoreBehaviour::dump_std_evo (core.cpp:4988-5056)
             write_2d_inv_c(path + "spec_evo" + sfx, spec_std);
             write_2d_inv(path + "imbalance_evo" + sfx, imb_std, ndt, ndt, n);
+        } else if (jcs) {  // JCSCoreBehaviour::dump_std_evo (core.cpp:3034-3102): mean = <a^+ a>
+            write_2d_inv_c(path + "spec_evo" + sfx, spec_std);
+            write_2d_inv(path + "mean_evo" + sfx, energy_, ndt, ndt, n);
         } else {
             write_2d_inv(path + "mean_evo" + sfx, mean_, ndt, ndt, n);
             write_2d_inv(path + "dispersion_evo" + sfx, disp_, ndt, ndt, n);
@@ -312,6 +332,9 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         if (mbl) {  // MBLCoreBehaviour::dump_lpn_evo (core.cpp:5058-5096)
             write_2d_inv_c(path + "spec_lpn_evo" + sfx, spec_lpn);
             write_2d_inv(path + "imbalance_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
+        } else if (jcs) {  // JCSCoreBehaviour::dump_lpn_evo (core.cpp:3104-3150)
+            write_2d_inv_c(path + "spec_lpn_evo" + sfx, spec_lpn);
+            write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
         } else {
             write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
             write_2d_inv(path + "energy_lpn_evo" + sfx, energy_lpn_evo, ndt, ndt, n);
@@ -354,10 +377,9 @@ int main(int argc, char **argv)
             " (this engine runs the dimer (0), JCS (1) and MBL (3) systems)");
     const bool jcs = rp.sys_id == 1;  // JCS and MBL: the Std task with the QJ propagator
     const bool mbl = rp.sys_id == 3;
-    if ((jcs && (rp.task_id != 1 || rp.prop_id != 0)) || (mbl && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0)))
+    if ((jcs || mbl) && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
         die("Wrong task_id / prop_id for sys_id " + std::to_string(rp.sys_id) +
-            " (this engine runs JCS with the Std task, MBL with the Std and LpnMult tasks, both with the QJ "
-            "propagator)");
+            " (this engine runs JCS and MBL with the Std and LpnMult tasks and the QJ propagator)");
     if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7)
         die("Wrong task_id: " + std::to_string(rp.task_id) +
             " (this engine runs the Std (1), StdDeep (4) and LpnMult (7) tasks)");
@@ -534,7 +556,8 @@ int main(int argc, char **argv)
         std::cout << "init_data" << std::endl;
 
         if (rp.task_id == 7) {
-            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, mbl ? Nc : 0, mbl_W);
+            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, rp.sys_id, Nc, jcs ? jcs_alpha : mbl_W,
+                         jcs ? jcs_p1 * jcs_alpha + jcs_p2 * jcs_alpha : cfg.T);
             qjx_destroy(h);
             return 0;
         }

@@ -322,11 +322,15 @@ def expected_lpn_outputs(cfg, prm, R=None):
     (experiment.cpp:138-286) with dump_std, dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127)
     and the adr files (dump.cpp:3-98)."""
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
+    jcs = cfg.get("sys_id", 0) == 1  # JCS: a in observable slot 0, <a^+ a>, JCS file set
+    spec = mbl or jcs
     N = 0 if mbl else int(prm["N"])
-    d = N + 1
+    d = N if jcs else N + 1
     if mbl:
         Nc, W = int(prm["mbl_Nc"]), float(prm["mbl_prm_W"])
         d = len(O.mbl_basis(Nc))
+    if jcs:
+        W = float(prm["jcs_prm_alpha"])  # the spec divisor
     n = cfg["num_trajectories"]
     half = n // 2
     deep = cfg.get("ex_deep", 16)
@@ -334,7 +338,17 @@ def expected_lpn_outputs(cfg, prm, R=None):
     path = cfg.get("path", "")
     sfx = suffix(cfg, prm)
     nr = int(prm["num_random_obs"])
-    if mbl:
+    if jcs:
+        alpha = W
+        H, Hd, L, Nop, K0, K1 = O.jcs_operators(N, alpha, prm["jcs_drv_ampl"])
+        heads = [prm["jcs_drv_part_1"] * alpha, prm["jcs_drv_part_2"] * alpha]
+        U = np.stack([O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)])
+        Rs = np.concatenate([L[None], R]) if nr else L[None]
+        T = alpha
+        calc_T = heads[0] + heads[1]  # JCSCoreBehaviour::calc_T (core.cpp:2833-2845)
+        ens = O.Ensemble(U, L, [1.0], Nop, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
+                         branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+    elif mbl:
         en, H, L, K = O.mbl_operators(Nc, W, prm["mbl_prm_U"], prm["mbl_prm_J"], int(prm["mbl_seed"]),
                                       int(prm["mbl_mns"]), int(prm["diss_type"]), prm["diss_phase"], prm["diss_gamma"])
         T = prm["mbl_T"]
@@ -342,6 +356,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
         Rs = np.concatenate([H[None], R]) if nr else H[None]
         ens = O.Ensemble(np.stack([Ut, Ut]), L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]),
                          rec_cap=100000)
+        calc_T = T
     else:
         H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
                                              prm["dimer_drv_ampl"], prm["diss_gamma"])
@@ -350,6 +365,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
         HE = H + prm["dimer_prm_E"] * Hd
         ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]),
                          rec_cap=100000)
+        calc_T = T
     ens.init(int(prm["start_type"]), int(prm["start_state"]))
     prop = cfg.get("prop_id", 0)
     period = [0]
@@ -371,7 +387,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
                eps_error=float(prm["lpn_eps_error"]), delta_s=float(prm["lpn_delta_s"]),
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
-               mbl_Nc=Nc if mbl else 0, spec_div=W if mbl else 1.0)
+               mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0, jcs=jcs)
     dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
     ndt = len(dp)
     assert advance(cfg.get("num_tp_periods", 0), is_obs=0, tr1=half) == 0
@@ -410,8 +426,9 @@ def expected_lpn_outputs(cfg, prm, R=None):
             o = ens.observables(want_adr=True)
             if mbl:  # calc_chars_std before lambda_lpn: the pre-update adr rows
                 o["imbalance"] = O.mbl_imbalance(Nc, o["adr"])
-            lp.period((period_id + 1) * T)
-            o["adr"][half:] = ens.observables(want_adr=True)["adr"][half:]
+            lp.period((period_id + 1) * calc_T)
+            if not jcs:  # JCS's calc_chars_lpn does not rewrite abs_diag_rho_all
+                o["adr"][half:] = ens.observables(want_adr=True)["adr"][half:]
             last = lp.last()
             for v in range(half, n):
                 if save_lambdas > 0 and last["renormed"][v]:
@@ -425,8 +442,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
         if evo_avg == 1 and adr_avg_on == 1:
             emit("adr_avg" + sfx, f_double_data(adr_avg(o["adr"], half)), True)
     last = obs[-1]
-    ro = 1 if mbl else 0
-    if mbl:
+    ro = 1 if spec else 0
+    if spec:
         for o in obs:
             z = o["random_obs"][:, 0]
             o["spec"] = z.real / W + 1j * (z.imag / W)
@@ -441,7 +458,14 @@ def expected_lpn_outputs(cfg, prm, R=None):
         emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
         emit("spec_lpn" + sfx, f_complex_data(lpn[-1]["spec_lpn"]), False)
         emit("imbalance_lpn" + sfx, f_double_data(lpn[-1]["mean_lpn"]), False)
-    if int(prm["dump_obs"]) == 1 and not mbl:
+    if jcs and int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("spec" + sfx, f_complex_data(last["spec"]), False)
+        emit("lambda" + sfx, f_double_data(lpn[-1]["lambda_now"]), False)
+        emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
+        emit("spec_lpn" + sfx, f_complex_data(lpn[-1]["spec_lpn"]), False)
+        emit("mean" + sfx, f_double_data(lpn[-1]["mean_lpn"]), False)
+    if int(prm["dump_obs"]) == 1 and not spec:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
         emit("mean" + sfx, f_double_data(last["mean"]), False)
@@ -461,11 +485,12 @@ def expected_lpn_outputs(cfg, prm, R=None):
     if evo_sep == 1 and int(prm["dump_obs"]) == 1:
         emit("periods" + sfx, f_int_data(dp), False)
         keys = ((("norm", "norm_evo"), ("imbalance", "imbalance_evo")) if mbl else
+                (("norm", "norm_evo"), ("energy", "mean_evo")) if jcs else
                 (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
                  ("energy", "energy_evo")))
         for key, name in keys:
             emit(name + sfx, f_2d_inv(np.array([o[key] for o in obs])), False)
-        if mbl:
+        if spec:
             emit("spec_evo" + sfx, f_2d_inv_complex(np.array([o["spec"] for o in obs])), False)
         for o_id in range(nr):
             rows = [o["random_obs"][:, ro + o_id] for o in obs]
@@ -479,10 +504,11 @@ def expected_lpn_outputs(cfg, prm, R=None):
                     emit("jump_norms_%d" % tr + sfx, f_double_data(nm), False)
                     emit("jump_etas_%d" % tr + sfx, f_double_data(et), False)
         keys = ((("lambda_now", "lambda_evo"), ("mean_lpn", "imbalance_lpn_evo")) if mbl else
+                (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo")) if jcs else
                 (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo"), ("energy_lpn", "energy_lpn_evo")))
         for key, name in keys:
             emit(name + sfx, f_2d_inv(np.array([v[key] for v in lpn])), False)
-        if mbl:
+        if spec:
             emit("spec_lpn_evo" + sfx, f_2d_inv_complex(np.array([v["spec_lpn"] for v in lpn])), False)
         for o_id in range(nr):
             rows = [v["robs_lpn"][:, ro + o_id] for v in lpn]

@@ -81,9 +81,22 @@ def test_mbl_suffix_matches_reference_rule(tmp_path, over):
     assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_Nc(8)_rnd(" in line
 
 
-def test_mbl_other_tasks_exit_with_error(tmp_path):
-    r = check(tmp_path, dict(BASE_CONFIG, sys_id=3, task_id=4), {**BASE_PARAMS, **MBL_PARAMS})
-    assert r.returncode != 0 and "Error: Wrong task_id / prop_id for sys_id 3" in r.stdout
+@pytest.mark.parametrize("sys_id,task_id,prop_id", [(3, 4, 0), (1, 4, 0), (3, 7, 1), (1, 1, 1)])
+def test_jcs_mbl_other_tasks_exit_with_error(tmp_path, sys_id, task_id, prop_id):
+    prm = {**BASE_PARAMS, **(MBL_PARAMS if sys_id == 3 else JCS_PARAMS)}
+    r = check(tmp_path, dict(BASE_CONFIG, sys_id=sys_id, task_id=task_id, prop_id=prop_id), prm)
+    assert r.returncode != 0 and "Error: Wrong task_id / prop_id for sys_id %d" % sys_id in r.stdout
+
+
+@pytest.mark.parametrize("sys_id", [1, 3])
+def test_jcs_mbl_lpn_suffix(tmp_path, sys_id):
+    """suffix_param + suffix_lpn for the LpnMult task of JCS and MBL (outputter.cpp:95-212, 371-381)."""
+    cfg = dict(BASE_CONFIG, sys_id=sys_id, task_id=7)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **(MBL_PARAMS if sys_id == 3 else JCS_PARAMS)}
+    r = check(tmp_path, cfg, prm)
+    assert r.returncode == 0, r.stdout
+    line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
+    assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_lpn(" in line
 
 
 @pytest.mark.parametrize("key,val", [("sys_id", 5), ("task_id", 9), ("prop_id", 2)])

@@ -139,6 +139,21 @@ def test_mbl_lpn_mult_files_match(tmp_path, lpn_type):
     assert any(k.startswith("imbalance_lpn_evo") for k in exp) and any(k.startswith("spec_lpn_evo") for k in exp)
 
 
+@pytest.mark.parametrize("lpn_type", [-1, -2, 0])
+def test_jcs_lpn_mult_files_match(tmp_path, lpn_type):
+    """JCS LpnMult (sys_id 1, task_id 7; submit_jcs.py): spec = <a> / alpha, <a^+ a> / d and
+    random-observable distances, Lyapunov time in units of calc_T = (part_1 + part_2) alpha, adr rows
+    left as the std ones (JCS's calc_chars_lpn does not rewrite them), the JCS file set
+    (core.cpp:2976-3150)."""
+    cfg = dict(BASE_CONFIG, sys_id=1, task_id=7, num_trajectories=16, num_tp_periods=2, num_obs_periods=5)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **JCS_PARAMS, "lpn_type": lpn_type, "dump_num": 5, "jump": 1,
+           "dump_adr_sep": 1, "dump_adr_avg": 1, "save_lambdas": 1, "lpn_delta_f_high": 1e-2}
+    exp = run_case(tmp_path, cfg, prm)
+    k = [k for k in exp if k.startswith("num_renorms")][0]
+    assert sum(int(x) for x in exp[k].split()) > 0
+    assert any(k.startswith("mean_lpn_evo") for k in exp) and any(k.startswith("spec_lpn_evo") for k in exp)
+
+
 def test_jcs_system_files_match(tmp_path):
     """The JCS system (sys_id 1): kick and free evolution of unequal duration, spec = <a> / alpha,
     mean = <a^+ a> (newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601; core.cpp:2739-3102)."""
