@@ -207,15 +207,17 @@ typedef struct {
     double delta_s;       /* lpn_delta_s: target distance after a perturbation */
     double delta_f_high, delta_f_low;  /* lpn_delta_f_high / lpn_delta_f_low */
     double max_energy;    /* max |Re H_ii| of the hamiltonian (init_obs_lpn, newdel_exp.cpp:540-550) */
-    /* System characteristics (0 / 0: the dimer's).  MBL (MBLCoreBehaviour, core.cpp:4729-4902)
-     * when mbl_Nc > 0: every ensemble has d = C(mbl_Nc, mbl_Nc/2), random-observable slot 0 holds H,
-     * spec = slot 0 / spec_div (W), mean_lpn is the imbalance, lpn_type -1 = |spec_b - spec_v|, -2 =
-     * |imbalance_v - imbalance_b|.  JCS (JCSCoreBehaviour, core.cpp:2739-2975) when jcs = 1: slot 0
-     * holds a, spec = slot 0 / spec_div (alpha), mean_lpn is <a^+ a> (the energy observable with
-     * Nop), lpn_type -1 = |spec_b - spec_v|, -2 = |n_v - n_b| / d.  For both, k >= 0 = random
+    /* Whose Lyapunov characteristics (chars_sys = the reference's sys_id; 0: the dimer's).
+     * 3 MBL (MBLCoreBehaviour, core.cpp:4729-4902) with mbl_Nc (every ensemble has d =
+     * C(mbl_Nc, mbl_Nc/2); 0 otherwise): random-observable slot 0 holds H, spec = slot 0 / spec_div
+     * (W), mean_lpn is the imbalance, lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v -
+     * imbalance_b|.  1 JCS (JCSCoreBehaviour, core.cpp:2739-2975): slot 0 holds a, spec = slot 0 /
+     * spec_div (alpha), mean_lpn is <a^+ a> (the energy observable with Nop), -1 = |spec_b - spec_v|,
+     * -2 = |n_v - n_b| / d.  5 Integrable (IntegrableCoreBehaviour, core.cpp:6470-6676): slot 0 holds
+     * the special matrix, spec_div 1, -1 = |spec_b - spec_v|, no -2.  For all three, k >= 0 = random
      * observable slot k + 1. */
     int mbl_Nc;
-    int jcs;
+    int chars_sys;
     double spec_div;
 } qjx_lpn_config;
 /* After the bases' transient (trans_process, experiment.cpp:138-183): copy every base into its
@@ -284,6 +286,15 @@ qjx_status qjx_mbl_size(int Nc, int diss_type, int *d, int *num_diss);
 qjx_status qjx_build_mbl(int Nc, double W, double U, double J, int mbl_seed, int mbl_mns, int diss_type,
                          double diss_phase, double gamma, double T, int deep, double *energies, int *id_to_x,
                          double *H, double *L, double *K, double *Utree);
+/* The Integrable system (sys_id 5; IntegrableNewDelBehaviour, newdel.cpp:310-345, 1030-1095, 1924-2076,
+ * 2914-3004): N spins (3 <= N <= 10), d = 2^N, H = 0; L [N][d][d]: the 4 x 4 operator tau |00><00| +
+ * k |11><11| + |01><10| + |10><01| on spins (c, c+1), c < N - 1, and on the border pair (N-1, 0);
+ * special = y / sqrt(Re tr y^2) / sqrt(d), y = (X + X^H) / 2, X_ij = g_ij (1 + i) with g Box-Muller
+ * normals of the MCG31 stream seed 13371337 leapfrogged (seed, num_seeds); K = -i (-(i/2) sum_c
+ * L_c^H L_c); jump rates 1; Utree [deep][d][d] = exp(K T 2^-(l+2)), one branch run twice per period
+ * (init_split_structure_integrable, core.cpp:10610-10660).  Any output pointer may be NULL. */
+qjx_status qjx_build_integrable(int N, int seed, int num_seeds, double tau, double k, double T, int deep, double *L,
+                                double *special, double *K, double *Utree);
 /* The MBL imbalance of n probability rows adr [n][d] (get_imbalance_mbl, experiment.cpp:1753-1800). */
 qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double *out);
 /* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)

@@ -192,12 +192,13 @@ static void lpn_chars(const orc_problem *p, const double *phi, int want, int rob
 
 /* what calc_delta_s / calc_delta_f need of a state: a CH_ part (delta_want) and / or one random
  * observable slot (delta_one, -1 none) */
-static int spec_sys(const orc_lpn_config *cfg) { return cfg->mbl_Nc > 0 || cfg->jcs; }
+static int spec_sys(const orc_lpn_config *cfg) { return cfg->chars_sys != 0; }
 
 static int delta_want(const orc_lpn_config *cfg)
 {
     if (cfg->mbl_Nc > 0) return cfg->lpn_type == -2 ? CH_MEAN : 0;
-    if (cfg->jcs) return cfg->lpn_type == -2 ? CH_ENERGY : 0;
+    if (cfg->chars_sys == 1) return cfg->lpn_type == -2 ? CH_ENERGY : 0;
+    if (cfg->chars_sys == 5) return 0;
     return cfg->lpn_type == -1 ? CH_MEAN : cfg->lpn_type == -2 ? CH_ENERGY : 0;
 }
 
@@ -216,7 +217,7 @@ static double lpn_delta(const orc_problem *p, const orc_lpn_config *cfg, const c
         return sqrt(dr * dr + di * di);
     }
     if (cfg->mbl_Nc > 0 && cfg->lpn_type == -2) return fabs(v->mean - b->mean);
-    if (cfg->jcs && cfg->lpn_type == -2) return fabs(v->energy - b->energy) / (double)p->d;
+    if (cfg->chars_sys == 1 && cfg->lpn_type == -2) return fabs(v->energy - b->energy) / (double)p->d;
     if (cfg->lpn_type == -1) return fabs(v->mean - b->mean) / (double)p->d;
     if (cfg->lpn_type == -2) return fabs(v->energy - b->energy) / cfg->max_energy;
     const int o = delta_one(cfg);
@@ -228,7 +229,10 @@ static int lpn_type_ok(const orc_problem *p, const orc_lpn_config *cfg)
 {
     if (cfg->mbl_Nc > 0 && (orc_mbl_basis(cfg->mbl_Nc, NULL) != p->d || cfg->mbl_Nc > 24 || p->num_robs < 1))
         return 0;
-    if (cfg->jcs && p->num_robs < 1) return 0;
+    if (cfg->chars_sys != 0 && cfg->chars_sys != 1 && cfg->chars_sys != 3 && cfg->chars_sys != 5) return 0;
+    if ((cfg->chars_sys == 3) != (cfg->mbl_Nc > 0)) return 0;
+    if (cfg->chars_sys != 0 && p->num_robs < 1) return 0;
+    if (cfg->chars_sys == 5 && cfg->lpn_type == -2) return 0;
     const int shift = spec_sys(cfg) ? 1 : 0;
     return cfg->lpn_type == -1 || cfg->lpn_type == -2 ||
            (cfg->lpn_type >= 0 && cfg->lpn_type + shift < p->num_robs);
@@ -297,7 +301,7 @@ static int var_trajectory(const orc_problem *p, const orc_lpn_config *cfg, orc_l
 
 static void store_chars(const orc_problem *p, const orc_lpn_config *cfg, orc_lpn *lp, int tr, const chars_t *c)
 {
-    lp->mean_lpn[tr] = cfg->jcs ? c->energy : c->mean; /* JCS: get_num_photons_jcs */
+    lp->mean_lpn[tr] = cfg->chars_sys == 1 ? c->energy : c->mean; /* JCS: get_num_photons_jcs */
     lp->energy_lpn[tr] = c->energy;
     for (int o = 0; o < p->num_robs; o++) {
         lp->robs_lpn[2 * ((size_t)tr * p->num_robs + o)] = c->robs[2 * o];

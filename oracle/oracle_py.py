@@ -36,7 +36,7 @@ class OrcLpnConfig(C.Structure):
     _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
                 ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
                 ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
-                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("jcs", C.c_int), ("spec_div", C.c_double)]
+                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("chars_sys", C.c_int), ("spec_div", C.c_double)]
 
 
 class OrcLpn(C.Structure):
@@ -66,6 +66,7 @@ def lib():
         L.orc_mbl_operators.argtypes = ([C.c_int] + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_double] * 2
                                         + [c_double_p] * 4)
         L.orc_mbl_imbalance.argtypes = [C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
+        L.orc_integrable_operators.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [c_double_p] * 3
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
@@ -143,6 +144,14 @@ def mbl_operators(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma):
     assert lib().orc_mbl_operators(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, _dp(en), _dp(H),
                                    _dp(L), _dp(K)) == 0
     return en, H, L, K
+
+
+def integrable_operators(N, seed, num_seeds, tau, k):
+    """Integrable (sys_id 5): L [N], special, K = hamiltonians_qj[0] (d = 2^N, H = 0)."""
+    d = 1 << N
+    L, S, K = _cplx((N, d, d)), _cplx((d, d)), _cplx((d, d))
+    assert lib().orc_integrable_operators(N, seed, num_seeds, tau, k, _dp(L), _dp(S), _dp(K)) == 0
+    return L, S, K
 
 
 def mbl_imbalance(Nc, adr):
@@ -318,13 +327,14 @@ class Lpn:
 
     def __init__(self, ens, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10,
                  delta_s=1e-3, delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0, mbl_Nc=0,
-                 spec_div=1.0, jcs=0):
+                 spec_div=1.0, chars_sys=None):
         self.ens = ens
         n = ens.n
         self.cfg = OrcLpnConfig(lpn_type=lpn_type, eps_deep=eps_deep, per_period=int(per_period), eps_low=eps_low,
                                 eps_high=eps_high, eps_error=eps_error, delta_s=delta_s,
                                 delta_f_high=delta_f_high, delta_f_low=delta_f_low, max_energy=max_energy,
-                                mbl_Nc=mbl_Nc, spec_div=spec_div, jcs=int(jcs))
+                                mbl_Nc=mbl_Nc, spec_div=spec_div,
+                                chars_sys=(3 if mbl_Nc else 0) if chars_sys is None else chars_sys)
         self.a = {k: np.zeros(n) for k in ("lambda", "lambda_now", "delta_s", "mean_lpn", "energy_lpn", "ratio",
                                            "ds_rec", "df_rec", "eps")}
         self.robs_lpn = np.zeros((n, max(ens.R.shape[0], 1)), np.complex128)

@@ -315,6 +315,86 @@ void orc_mbl_imbalance(int Nc, int d, int n, const double *adr, double *out)
     free(np_);
 }
 
+/* Integrable (sys_id 5, newdel.cpp:310-345, 1030-1095, 1924-2076, 2914-3004): N spins, d = 2^N, H = 0.
+ * con = tau |00><00| + k |11><11| + |01><10| + |10><01| on neighbouring spins (c, c+1) for c < N-1
+ * (kron order: spin 0 is the most significant bit), and on (N-1, 0) for the border channel;
+ * special = y / sqrt(d), y = (X + X^H) / 2 normalised by sqrt(Re tr y^2), X_ij = g_ij (1 + i) with
+ * g Box-Muller normals from MCG31 seed 13371337 leapfrogged (seed, num_seeds); K = -i (0 - (i/2)
+ * sum_c L_c^H L_c), jump rates 1.  L holds N complex d x d matrices. */
+int orc_integrable_operators(int N, int seed, int num_seeds, double tau, double kk, double *L, double *special,
+                             double *K)
+{
+    if (N < 3 || N > 12) return 1;
+    const int d = 1 << N;
+    const size_t dd = (size_t)d * d;
+    memset(L, 0, 2 * dd * (size_t)N * sizeof(double));
+    /* channel c < N-1 acts on spins (c, c+1), i.e. bits (N-1-c, N-2-c); the border on (N-1, 0):
+     * bits 0 (spin N-1, first of the pair) and N-1 (spin 0) */
+    for (int c = 0; c < N; c++) {
+        double *Lc = L + 2 * dd * (size_t)c;
+        const int ba = c < N - 1 ? N - 1 - c : 0, bb = c < N - 1 ? N - 2 - c : N - 1;
+        for (int s = 0; s < d; s++) {
+            const int a = (s >> ba) & 1, b = (s >> bb) & 1;
+            if (a == b) {
+                Lc[2 * ((size_t)s * d + s)] = a ? kk : tau;
+            } else {
+                const int r = s ^ (1 << ba) ^ (1 << bb); /* |01> <-> |10> */
+                Lc[2 * ((size_t)r * d + s)] = 1.0;
+            }
+        }
+    }
+    double *u = (double *)malloc(2 * dd * sizeof(double)), *g = (double *)malloc(dd * sizeof(double));
+    double *y = (double *)malloc(2 * dd * sizeof(double)), *hp = (double *)malloc(2 * dd * sizeof(double));
+    if (!u || !g || !y || !hp) return 2;
+    orc_mcg31_uniform(13371337ull, (unsigned long long)seed, (unsigned long long)num_seeds, (int)(2 * dd), 0.0, 1.0, u);
+    const double two_pi = 2.0 * 3.1415926535897932384626433832795;
+    for (size_t e = 0; e < dd; e++) g[e] = sqrt(-2.0 * log(u[2 * e])) * sin(two_pi * u[2 * e + 1]);
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) { /* 0.5 (X + X^H), X_ij = g_ij + i g_ij */
+            const double gij = g[(size_t)i * d + j], gji = g[(size_t)j * d + i];
+            y[2 * ((size_t)i * d + j)] = 0.5 * (gij + gji);
+            y[2 * ((size_t)i * d + j) + 1] = 0.5 * (gij + -gji);
+        }
+    double tr = 0.0; /* Re tr y^2: sum_i sum_k y_ik y_ki, k ascending, then i ascending */
+    for (int i = 0; i < d; i++) {
+        double sr = 0.0;
+        for (int k = 0; k < d; k++) {
+            const double ar = y[2 * ((size_t)i * d + k)], ai = y[2 * ((size_t)i * d + k) + 1];
+            const double br = y[2 * ((size_t)k * d + i)], bi = y[2 * ((size_t)k * d + i) + 1];
+            sr = sr + (ar * br - ai * bi);
+        }
+        tr = tr + sr;
+    }
+    const double sy = sqrt(tr), sd = sqrt((double)d);
+    for (size_t e = 0; e < 2 * dd; e++) special[e] = (y[e] / sy) / sd;
+    for (size_t e = 0; e < 2 * dd; e++) hp[e] = 0.0;
+    for (int c = 0; c < N; c++) {
+        const double *Lc = L + 2 * dd * (size_t)c;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int k = 0; k < d; k++) {
+                    const double ar = Lc[2 * ((size_t)k * d + i)], ai = Lc[2 * ((size_t)k * d + i) + 1];
+                    const double br = Lc[2 * ((size_t)k * d + j)], bi = Lc[2 * ((size_t)k * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (1.0 * si);
+                hp[2 * idx + 1] -= 0.5 * (1.0 * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        K[2 * e] = 0.0 + hp[2 * e + 1];
+        K[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    free(u);
+    free(g);
+    free(y);
+    free(hp);
+    return 0;
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

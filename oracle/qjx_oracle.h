@@ -65,6 +65,11 @@ int orc_mbl_operators(int Nc, double W, double U, double J, int mbl_seed, int mb
                       double gamma, double *energies, double *H, double *L, double *K);
 void orc_mbl_imbalance(int Nc, int d, int n, const double *adr, double *out);
 
+/* Integrable (sys_id 5, newdel.cpp:310-345, 1030-1095, 1924-2076, 2914-3004): d = 2^N, H = 0, L [N][d][d]
+ * (the con 4 x 4 on neighbouring spins and on the border pair), special (the spec observable), K. */
+int orc_integrable_operators(int N, int seed, int num_seeds, double tau, double kk, double *L, double *special,
+                             double *K);
+
 /* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
  * propagator (newdel.cpp:2354-2366), complex d x d. */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);
@@ -186,10 +191,12 @@ typedef struct {
     /* MBL characteristics (MBLCoreBehaviour, core.cpp:4729-4902) when mbl_Nc > 0: random-observable
      * slot 0 holds H and spec = slot 0 / spec_div (W); mean = the imbalance of the adr row;
      * lpn_type -1 = |spec_b - spec_v|, -2 = |imbalance_v - imbalance_b|, k >= 0 = slot k + 1.
-     * JCS (JCSCoreBehaviour, core.cpp:2739-2975) when jcs = 1: slot 0 holds a, spec = slot 0 / alpha,
-     * mean_lpn = <a^+ a> (the energy observable), -1 = |spec_b - spec_v|, -2 = |n_v - n_b| / d. */
+     * chars_sys selects the system: 0 the dimer, 1 JCS (JCSCoreBehaviour, core.cpp:2739-2975: slot 0
+     * holds a, spec = slot 0 / alpha, mean_lpn = <a^+ a> (the energy observable), -1 = |spec_b -
+     * spec_v|, -2 = |n_v - n_b| / d), 3 MBL (with mbl_Nc), 5 Integrable (core.cpp:6470-6676: slot 0
+     * holds the special matrix, spec_div 1, -1 = |spec_b - spec_v|, no -2). */
     int mbl_Nc;
-    int jcs;
+    int chars_sys;
     double spec_div;
 } orc_lpn_config;
 

@@ -21,7 +21,7 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
+    "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
     "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
@@ -45,7 +45,7 @@ class QjxLpnConfig(C.Structure):
     _fields_ = [("lpn_type", C.c_int), ("eps_deep", C.c_int), ("per_period", C.c_int), ("pad", C.c_int),
                 ("eps_low", C.c_double), ("eps_high", C.c_double), ("eps_error", C.c_double),
                 ("delta_s", C.c_double), ("delta_f_high", C.c_double), ("delta_f_low", C.c_double),
-                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("jcs", C.c_int), ("spec_div", C.c_double)]
+                ("max_energy", C.c_double), ("mbl_Nc", C.c_int), ("chars_sys", C.c_int), ("spec_div", C.c_double)]
 
 
 class QjxStats(C.Structure):
@@ -117,6 +117,7 @@ def lib():
         L.qjx_build_mbl.argtypes = ([C.c_int] + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int]
                                     + [c_double_p, c_int_p] + [c_double_p] * 4)
         L.qjx_mbl_imbalance.argtypes = [C.c_int, C.c_int, c_double_p, c_double_p]
+        L.qjx_build_integrable.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int] + [c_double_p] * 4
         L.qjx_build_dimer_rk.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 2
         L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.POINTER(C.c_int), C.POINTER(C.c_int), c_int_p, c_int_p, c_double_p,
@@ -201,6 +202,18 @@ def build_mbl(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, T, d
     check(lib().qjx_build_mbl(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, T, deep, dp(en),
                               xs.ctypes.data_as(c_int_p), dp(H), dp(Lm), None, dp(Ut)), what="qjx_build_mbl")
     return en, xs, H, Lm, Ut
+
+
+def build_integrable(N, seed, num_seeds, tau, k, T, deep):
+    """Integrable system (sys_id 5): L [N], the special (spec) matrix and the split tree [deep][d][d]
+    of one branch (a period runs it twice); d = 2^N, H = 0, jump rates 1."""
+    d = 1 << N
+    Lm = np.zeros((N, d, d), np.complex128)
+    S = np.zeros((d, d), np.complex128)
+    Ut = np.zeros((deep, d, d), np.complex128)
+    check(lib().qjx_build_integrable(N, seed, num_seeds, tau, k, T, deep, dp(Lm), dp(S), None, dp(Ut)),
+          what="qjx_build_integrable")
+    return Lm, S, Ut
 
 
 def mbl_imbalance(Nc, adr):

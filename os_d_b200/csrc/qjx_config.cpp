@@ -175,6 +175,19 @@ std::string mbl_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string integrable_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_N(" << int(param(cp, "integrable_N")) << ")";
+    s << "_seed(" << int(param(cp, "integrable_seed")) << ")";
+    s << "_tau(" << int(param(cp, "integrable_tau")) << ")";
+    s << "_k(" << int(param(cp, "integrable_k")) << ")";
+    s << "_T(" << std::setprecision(precision) << std::fixed << param(cp, "integrable_T") << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

@@ -183,7 +183,7 @@ struct LpnParams {
     const int *pair0;                                                 // [E + 1] first pair of each ensemble
     int pairs;                                                        // sum over ensembles of n_e / 2
     int mbl_Nc;                                                       // > 0: MBL characteristics
-    int jcs;                                                          // 1: JCS characteristics
+    int chars_sys;                                                    // characteristics of sys_id 0 / 1 / 3 / 5
     double spec_div;                                                  // MBL: spec = robs slot 0 / W
     const int *words;                                                 // MBL: [d] basis words
 };

@@ -1071,9 +1071,14 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
         if (ne < 2 || (ne & 1))
             return fail(h, QJX_ERR_INVALID_ARG, "the Lyapunov task needs an even n_traj >= 2 in every ensemble");
     }
-    const int shift = (c->mbl_Nc > 0 || c->jcs) ? 1 : 0;  // MBL / JCS: slot 0 holds the spec operator
-    if (c->jcs && (c->mbl_Nc != 0 || P.nr < 1 || !(c->spec_div != 0.0)))
-        return fail(h, QJX_ERR_INVALID_ARG, "jcs needs a in observable slot 0 and spec_div = alpha");
+    const int cs = c->chars_sys;
+    if (cs != 0 && cs != 1 && cs != 3 && cs != 5)
+        return fail(h, QJX_ERR_INVALID_ARG, "chars_sys must be 0 (dimer), 1 (JCS), 3 (MBL) or 5 (Integrable)");
+    if ((cs == 3) != (c->mbl_Nc != 0)) return fail(h, QJX_ERR_INVALID_ARG, "mbl_Nc goes with chars_sys 3 only");
+    if (cs != 0 && (P.nr < 1 || !(c->spec_div != 0.0)))
+        return fail(h, QJX_ERR_INVALID_ARG, "the spec operator goes in observable slot 0, with spec_div != 0");
+    if (cs == 5 && c->lpn_type == -2) return fail(h, QJX_ERR_INVALID_ARG, "Integrable has no lpn_type -2");
+    const int shift = cs != 0 ? 1 : 0;  // JCS / MBL / Integrable: slot 0 holds the spec operator
     if (!(c->lpn_type == -1 || c->lpn_type == -2 || (c->lpn_type >= 0 && c->lpn_type + shift < P.nr)))
         return fail(h, QJX_ERR_INVALID_ARG, "lpn_type must be -1, -2 or a random observable index");
     std::vector<int> words;
@@ -1127,7 +1132,7 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
     L.delta_f_low = c->delta_f_low;
     L.max_energy = c->max_energy;
     L.mbl_Nc = c->mbl_Nc;
-    L.jcs = c->jcs ? 1 : 0;
+    L.chars_sys = cs;
     L.spec_div = c->spec_div;
     if (!words.empty()) {
         L.words = upload(h, words);

@@ -220,13 +220,15 @@ __device__ void cta_chars(const Params &P, const LpnParams &L, const EnsCtx &E, 
 
 // What calc_delta_s / calc_delta_f need of a state: CH_ parts and one random-observable slot
 // (-1: none).  MBL: -1 the spec (slot 0), -2 the imbalance, k >= 0 slot k + 1; JCS: -1 the spec
-// (slot 0), -2 <a^+ a> (the energy observable), k >= 0 slot k + 1.
-__device__ __forceinline__ bool spec_sys(const LpnParams &L) { return L.mbl_Nc > 0 || L.jcs; }
+// (slot 0), -2 <a^+ a> (the energy observable), k >= 0 slot k + 1; Integrable: -1 the spec (slot
+// 0), k >= 0 slot k + 1.
+__device__ __forceinline__ bool spec_sys(const LpnParams &L) { return L.chars_sys != 0; }
 
 __device__ __forceinline__ int delta_want(const LpnParams &L)
 {
     if (L.mbl_Nc > 0) return L.lpn_type == -2 ? CH_MEAN : 0;
-    if (L.jcs) return L.lpn_type == -2 ? CH_ENERGY : 0;
+    if (L.chars_sys == 1) return L.lpn_type == -2 ? CH_ENERGY : 0;
+    if (L.chars_sys == 5) return 0;
     return L.lpn_type == -1 ? CH_MEAN : L.lpn_type == -2 ? CH_ENERGY : 0;
 }
 
@@ -237,7 +239,7 @@ __device__ __forceinline__ int delta_one(const LpnParams &L)
 }
 
 // calc_delta_s / calc_delta_f (dimer core.cpp:839-901, JCS core.cpp:2870-2975, MBL
-// core.cpp:4823-4901), variation v against base b
+// core.cpp:4823-4901, Integrable core.cpp:6606-6676), variation v against base b
 __device__ __forceinline__ double lpn_delta(const EnsCtx &E, const LpnParams &L, const LpnChars &v,
                                             const LpnChars &b)
 {
@@ -248,7 +250,7 @@ __device__ __forceinline__ double lpn_delta(const EnsCtx &E, const LpnParams &L,
         return __dsqrt_rn(__dadd_rn(__dmul_rn(dr, dr), __dmul_rn(di, di)));
     }
     if (L.mbl_Nc > 0 && L.lpn_type == -2) return fabs(__dsub_rn(v.mean, b.mean));
-    if (L.jcs && L.lpn_type == -2) return __ddiv_rn(fabs(__dsub_rn(v.energy, b.energy)), (double)E.d);
+    if (L.chars_sys == 1 && L.lpn_type == -2) return __ddiv_rn(fabs(__dsub_rn(v.energy, b.energy)), (double)E.d);
     if (L.lpn_type == -1) return __ddiv_rn(fabs(__dsub_rn(v.mean, b.mean)), (double)E.d);
     if (L.lpn_type == -2) return __ddiv_rn(fabs(__dsub_rn(v.energy, b.energy)), L.max_energy);
     const int o = delta_one(L);
@@ -337,7 +339,7 @@ __device__ void var_trajectory(const Params &P, const EnsCtx &E, const LpnParams
 __device__ void store_chars(const Params &P, const LpnParams &L, int tr, const LpnChars &c)
 {
     if (threadIdx.x == 0) {
-        L.mean_lpn[tr] = L.jcs ? c.energy : c.mean;  // JCS: get_num_photons_jcs
+        L.mean_lpn[tr] = L.chars_sys == 1 ? c.energy : c.mean;  // JCS: get_num_photons_jcs
         L.energy_lpn[tr] = c.energy;
     }
     for (int o = threadIdx.x; o < P.nr; o += blockDim.x) L.robs_lpn[(size_t)tr * P.nr + o] = c.robs[o];

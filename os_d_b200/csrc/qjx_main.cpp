@@ -1,7 +1,8 @@
 // qjx_main.cpp -- qjx_b200: process-level drop-in for the reference's qjx executable on the
 // Std task (task_id 1) and the LpnMult task (task_id 7) with the QJ propagator (prop_id 0) or the
 // RK propagator (prop_id 1), and the StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0);
-// the Std task with the QJ propagator for the JCS (sys_id 1) and MBL (sys_id 3) systems.
+// the Std and LpnMult tasks with the QJ propagator for the JCS (sys_id 1), MBL (sys_id 3) and
+// Integrable (sys_id 5) systems.
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -72,7 +73,7 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
                   const std::vector<double> &H, int d, int num_robs, int robs_seed, int sys, int Nc, double spec_div,
                   double calc_T)
 {
-    const bool mbl = sys == 3, jcs = sys == 1, spec = mbl || jcs;
+    const bool mbl = sys == 3, jcs = sys == 1, integ = sys == 5, spec = mbl || jcs || integ;
     const double W = spec_div;
     const int ro = spec ? 1 : 0, nr = num_robs + ro;  // engine slots: [spec,] random observables
     const int n = cp.num_trajectories, half = n / 2;
@@ -95,7 +96,7 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     lc.delta_f_low = param(cp, "lpn_delta_f_low");
     const int save_lambdas = int(param(cp, "save_lambdas"));
     lc.mbl_Nc = mbl ? Nc : 0;
-    lc.jcs = jcs ? 1 : 0;
+    lc.chars_sys = sys;
     lc.spec_div = spec_div;
     lc.max_energy = 0.0;  // init_obs_lpn (newdel_exp.cpp:540-550)
     for (int st = 0; st < d; st++) {
@@ -258,6 +259,14 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         save_complex_data(path + "spec_lpn" + sfx, reinterpret_cast<const double *>(spec_lpn.data() + o), n, 16, false);
         save_double_data(path + "imbalance_lpn" + sfx, mean_lpn_evo.data() + o, n, 16, false);
     }
+    if (dump_obs == 1 && integ) {  // IntegrableCoreBehaviour::dump_std / dump_lpn (core.cpp:6685-6753)
+        const size_t o = (size_t)last_dump * n;
+        save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);
+        save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec_std.data() + o), n, 16, false);
+        save_double_data(path + "lambda" + sfx, lam_evo.data() + o, n, 16, false);
+        save_int_data(path + "num_renorms" + sfx, renorms.data(), n, false);
+        save_complex_data(path + "spec_lpn" + sfx, reinterpret_cast<const double *>(spec_lpn.data() + o), n, 16, false);
+    }
     if (dump_obs == 1 && jcs) {  // JCSCoreBehaviour::dump_std / dump_lpn (core.cpp:2976-3033)
         const size_t o = (size_t)last_dump * n;
         save_double_data(path + "norm" + sfx, norm_.data() + o, n, 16, false);
@@ -298,6 +307,8 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         } else if (jcs) {  // JCSCoreBehaviour::dump_std_evo (core.cpp:3034-3102): mean = <a^+ a>
             write_2d_inv_c(path + "spec_evo" + sfx, spec_std);
             write_2d_inv(path + "mean_evo" + sfx, energy_, ndt, ndt, n);
+        } else if (integ) {  // IntegrableCoreBehaviour::dump_std_evo (core.cpp:6755-6819)
+            write_2d_inv_c(path + "spec_evo" + sfx, spec_std);
         } else {
             write_2d_inv(path + "mean_evo" + sfx, mean_, ndt, ndt, n);
             write_2d_inv(path + "dispersion_evo" + sfx, disp_, ndt, ndt, n);
@@ -335,6 +346,8 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         } else if (jcs) {  // JCSCoreBehaviour::dump_lpn_evo (core.cpp:3104-3150)
             write_2d_inv_c(path + "spec_lpn_evo" + sfx, spec_lpn);
             write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
+        } else if (integ) {  // IntegrableCoreBehaviour::dump_lpn_evo (core.cpp:6821-6858)
+            write_2d_inv_c(path + "spec_lpn_evo" + sfx, spec_lpn);
         } else {
             write_2d_inv(path + "mean_lpn_evo" + sfx, mean_lpn_evo, ndt, ndt, n);
             write_2d_inv(path + "energy_lpn_evo" + sfx, energy_lpn_evo, ndt, ndt, n);
@@ -372,14 +385,15 @@ int main(int argc, char **argv)
     if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
     std::cout << params_echo(rp, cp);
 
-    if (rp.sys_id != 0 && rp.sys_id != 1 && rp.sys_id != 3)
+    if (rp.sys_id != 0 && rp.sys_id != 1 && rp.sys_id != 3 && rp.sys_id != 5)
         die("Wrong sys_id: " + std::to_string(rp.sys_id) +
-            " (this engine runs the dimer (0), JCS (1) and MBL (3) systems)");
-    const bool jcs = rp.sys_id == 1;  // JCS and MBL: the Std task with the QJ propagator
+            " (this engine runs the dimer (0), JCS (1), MBL (3) and Integrable (5) systems)");
+    const bool jcs = rp.sys_id == 1;  // JCS, MBL, Integrable: Std and LpnMult with the QJ propagator
     const bool mbl = rp.sys_id == 3;
-    if ((jcs || mbl) && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
+    const bool integ = rp.sys_id == 5;
+    if ((jcs || mbl || integ) && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
         die("Wrong task_id / prop_id for sys_id " + std::to_string(rp.sys_id) +
-            " (this engine runs JCS and MBL with the Std and LpnMult tasks and the QJ propagator)");
+            " (this engine runs JCS, MBL and Integrable with the Std and LpnMult tasks and the QJ propagator)");
     if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7)
         die("Wrong task_id: " + std::to_string(rp.task_id) +
             " (this engine runs the Std (1), StdDeep (4) and LpnMult (7) tasks)");
@@ -388,7 +402,10 @@ int main(int argc, char **argv)
         die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
 
     try {
-        cp.fn_suffix = jcs ? jcs_suffix(rp, cp, 4) : mbl ? mbl_suffix(rp, cp, 4) : dimer_suffix(rp, cp, 4);
+        cp.fn_suffix = jcs ? jcs_suffix(rp, cp, 4)
+                       : mbl ? mbl_suffix(rp, cp, 4)
+                       : integ ? integrable_suffix(rp, cp, 4)
+                               : dimer_suffix(rp, cp, 4);
     } catch (const std::exception &e) {
         die(e.what());
     }
@@ -398,16 +415,19 @@ int main(int argc, char **argv)
     }
 
     try {
-        const bool dimer = !jcs && !mbl;
-        const int N = mbl ? 0 : int(param(cp, "N"));
+        const bool dimer = !jcs && !mbl && !integ;
+        const int N = (mbl || integ) ? 0 : int(param(cp, "N"));
+        // Integrable: 2^integrable_N basis states, integrable_N jump channels
+        const int Ni = integ ? int(param(cp, "integrable_N")) : 0;
+        if (integ && (Ni < 3 || Ni > 10)) die("integrable_N must be in [3, 10]");
         // MBL: C(Nc, Nc/2) basis words and Nc (diss_type 0) or Nc - 1 (diss_type 1) jump channels
         const int Nc = mbl ? int(param(cp, "mbl_Nc")) : 0, mbl_dt = mbl ? int(param(cp, "diss_type")) : 0;
         int d_mbl = 0, nd_mbl = 0;
         if (mbl && qjx_mbl_size(Nc, mbl_dt, &d_mbl, &nd_mbl) != QJX_OK)
             die("mbl_Nc must be even and in [2, 24], diss_type 0 or 1");
         // the dimer has N + 1 Fock states; the JCS oscillator is truncated at N states (newdel.cpp:110)
-        const int d = mbl ? d_mbl : jcs ? N : N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
-        const int num_diss = mbl ? nd_mbl : 1;
+        const int d = mbl ? d_mbl : integ ? (1 << Ni) : jcs ? N : N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
+        const int num_diss = mbl ? nd_mbl : integ ? Ni : 1;
         const double J = dimer ? param(cp, "dimer_prm_J") : 0.0, U = dimer ? param(cp, "dimer_prm_U") : 0.0;
         const double E = dimer ? param(cp, "dimer_prm_E") : 0.0;
         const double A = dimer ? param(cp, "dimer_drv_ampl") : 0.0, omega = dimer ? param(cp, "dimer_drv_freq") : 1.0;
@@ -427,7 +447,7 @@ int main(int argc, char **argv)
         const int dump_purity = int(param_or(cp, "dump_purity", 0));
         const int num_robs = int(param(cp, "num_random_obs"));
         const int robs_seed = int(param_or(cp, "random_obs_seed", 0));
-        if (n < 1 || (!mbl && N < 1) || (jcs && N < 2)) die("num_trajectories and N must be positive (N >= 2 for JCS)");
+        if (n < 1 || (dimer && N < 1) || (jcs && N < 2)) die("num_trajectories and N must be positive (N >= 2 for JCS)");
         if (start_type == 0 && (start_state < 0 || start_state >= d)) die("start_state out of range");
         const std::string &sfx = cp.fn_suffix;
         const std::string path = rp.path;
@@ -457,6 +477,15 @@ int main(int argc, char **argv)
             std::copy(K.begin(), K.begin() + 2 * dd, K.begin() + 2 * dd);
             // written to the working directory, without `path` (newdel.cpp:903-905)
             save_double_data("energies" + cp.fn_suffix, en.data(), Nc, 16, false);
+        } else if (integ) {
+            // H = 0; `special` (the spec observable) into Hd's storage; one head of duration
+            // integrable_T with two children of the same split tree (init_split_structure_integrable)
+            check(qjx_build_integrable(Ni, int(param(cp, "integrable_seed")), int(param(cp, "integrable_num_seeds")),
+                                       param(cp, "integrable_tau"), param(cp, "integrable_k"), param(cp, "integrable_T"),
+                                       deep, L.data(), Hd.data(), K.data(), Ut.data()),
+                  nullptr, "qjx_build_integrable");
+            std::copy(Ut.begin(), Ut.begin() + 2 * dd * deep, Ut.begin() + 2 * dd * deep);
+            std::copy(K.begin(), K.begin() + 2 * dd, K.begin() + 2 * dd);
         }
         else if (deep_task)
             check(qjx_build_dimer_deep(N, J, U, E, A, g, omega, deep, nsub, H.data(), Hd.data(), L.data(), K.data(),
@@ -467,12 +496,12 @@ int main(int argc, char **argv)
                   nullptr, "qjx_build_dimer");
         std::cout << "init_sizes" << std::endl << "init_hamiltonians" << std::endl << "init_dissipators" << std::endl
                   << "init_hamiltonians_qj" << std::endl;
-        if (rp.is_debug && mbl) {  // MBLDebugBehaviour::save (debugger.cpp:55-68), qj_proc.cpp:115-119
+        if (rp.is_debug && (mbl || integ)) {  // MBL / IntegrableDebugBehaviour::save (debugger.cpp:55-95)
             save_complex_data(path + "hamiltonian" + sfx, H.data(), dd, 16, false);
             for (int c = 0; c < num_diss; c++)
                 save_complex_data(path + "dissipator_" + std::to_string(c) + sfx, L.data() + 2 * dd * c, dd, 16, false);
             save_complex_data(path + "hamiltonians_qj_0" + sfx, K.data(), dd, 16, false);
-            save_complex_data(path + "spec_mtx" + sfx, H.data(), dd, 16, false);
+            save_complex_data(path + "spec_mtx" + sfx, integ ? Hd.data() : H.data(), dd, 16, false);
             save_complex_data(path + "exp_mtx_0" + sfx, Ut.data() + 2 * dd * (deep - 1), dd, 16, false);
         } else if (rp.is_debug) {
             save_complex_data(path + "hamiltonian" + sfx, H.data(), dd, 16, false);
@@ -485,14 +514,16 @@ int main(int argc, char **argv)
             }
         }
         std::vector<double> HE(2 * dd);
-        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : mbl ? H[e] : H[e] + E * Hd[e];
+        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : (mbl || integ) ? H[e] : H[e] + E * Hd[e];
         std::vector<double> R =
             random_observables(d, num_robs, robs_seed, int(param_or(cp, "random_obs_mns", 1000000)),
                                int(param_or(cp, "random_obs_type", 0)));
         // JCS: spec = <a> / alpha, MBL: spec = <H> / W ride in observable slot 0
-        const int robs_off = (jcs || mbl) ? 1 : 0;
+        // Integrable: spec = <special> rides in observable slot 0 as well
+        const int robs_off = (jcs || mbl || integ) ? 1 : 0;
         if (jcs) R.insert(R.begin(), Aop.begin(), Aop.end());
         if (mbl) R.insert(R.begin(), H.begin(), H.end());
+        if (integ) R.insert(R.begin(), Hd.begin(), Hd.end());
         const int nr_eng = num_robs + robs_off;
 
         // dump schedule (init_dump_periods)
@@ -518,7 +549,10 @@ int main(int argc, char **argv)
         cfg.num_branches = 2;
         cfg.num_diss = num_diss;
         cfg.num_robs = nr_eng;
-        cfg.T = jcs ? jcs_alpha : mbl ? param(cp, "mbl_T") : 2.0 * 3.1415926535897932384626433832795 / omega;
+        cfg.T = jcs     ? jcs_alpha
+                : mbl   ? param(cp, "mbl_T")
+                : integ ? param(cp, "integrable_T")
+                        : 2.0 * 3.1415926535897932384626433832795 / omega;
         // JCS: branch b's head is jcs_drv_part_b * alpha and the branch lasts half of it
         // (init_split_structure_jcs, core.cpp:10086-10124)
         const double jcs_len[2] = {0.5 * (jcs_p1 * jcs_alpha), 0.5 * (jcs_p2 * jcs_alpha)};
@@ -556,7 +590,7 @@ int main(int argc, char **argv)
         std::cout << "init_data" << std::endl;
 
         if (rp.task_id == 7) {
-            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, rp.sys_id, Nc, jcs ? jcs_alpha : mbl_W,
+            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, rp.sys_id, Nc, jcs ? jcs_alpha : mbl ? mbl_W : 1.0,
                          jcs ? jcs_p1 * jcs_alpha + jcs_p2 * jcs_alpha : cfg.T);
             qjx_destroy(h);
             return 0;
@@ -678,8 +712,8 @@ int main(int argc, char **argv)
         // (get_num_photons_jcs, experiment.cpp:2080-2160) from the energy slot
         // MBL: spec = <H> / W (get_spec_mbl, experiment.cpp:1705-1751), imbalance from the adr rows
         // (get_imbalance_mbl, experiment.cpp:1753-1800)
-        std::vector<std::complex<double>> spec((jcs || mbl) ? nd_ : 0);
-        const double spec_div = jcs ? jcs_alpha : mbl_W;
+        std::vector<std::complex<double>> spec((jcs || mbl || integ) ? nd_ : 0);
+        const double spec_div = jcs ? jcs_alpha : mbl ? mbl_W : 1.0;  // get_spec_integrable: no division
         for (size_t i = 0; i < spec.size(); i++) {
             const std::complex<double> a = D.robs[i * nr_eng];
             spec[i] = std::complex<double>(a.real() / spec_div, a.imag() / spec_div);
@@ -700,7 +734,7 @@ int main(int argc, char **argv)
             save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec.data() + o), n, 16, false);
             save_double_data(path + "imbalance" + sfx, imbalance.data() + o, n, 16, false);
         }
-        if (jcs && dump_obs == 1) {  // JCSCoreBehaviour::dump_std (core.cpp:2976-2999)
+        if ((jcs || integ) && dump_obs == 1) {  // JCS / Integrable dump_std (core.cpp:2976-2999, 6685-6708)
             const size_t o = (size_t)last_dump * n;
             save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
             save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec.data() + o), n, 16, false);
@@ -728,14 +762,14 @@ int main(int argc, char **argv)
                 save_2d_inv_double_data(path + name + sfx, inv.data(), ndt, n, 16, false);
             };
             evo(D.norm, "norm_evo");
-            if (jcs || mbl) {  // JCS / MBL CoreBehaviour::dump_std_evo (core.cpp:3034-3102, 4988-5056)
+            if (jcs || mbl || integ) {  // JCS / MBL / Integrable dump_std_evo (core.cpp:3034-3102, 4988-5056, 6755-6819)
                 std::vector<std::complex<double>> cinv((size_t)ndt * n);
                 for (int dmp = 0; dmp < nrec; dmp++)
                     for (int tr = 0; tr < n; tr++) cinv[(size_t)tr * ndt + dmp] = spec[(size_t)dmp * n + tr];
                 save_2d_inv_complex_data(path + "spec_evo" + sfx, reinterpret_cast<const double *>(cinv.data()), ndt, n,
                                          16, false);
                 if (jcs) evo(D.energy, "mean_evo");
-                else evo(imbalance, "imbalance_evo");
+                else if (mbl) evo(imbalance, "imbalance_evo");
             } else {
                 evo(D.mean, "mean_evo");
                 evo(D.disp, "dispersion_evo");

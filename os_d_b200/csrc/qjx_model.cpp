@@ -549,3 +549,95 @@ extern "C" qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double
     }
     return QJX_OK;
 }
+
+// ---------------------------------------------------------------------------------- Integrable
+// IntegrableNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp:310-345, 1030-1095, 1924-2076,
+// 2914-3004): N spins (spin 0 the most significant bit of a basis index), d = 2^N, H = 0.
+extern "C" qjx_status qjx_build_integrable(int N, int seed, int num_seeds, double tau, double k, double T, int deep,
+                                           double *L, double *special, double *Kout, double *Utree)
+{
+    if (N < 3 || N > 10 || num_seeds < 1 || seed < 0) return QJX_ERR_INVALID_ARG;
+    if (Utree && (deep < 1 || !(T > 0.0))) return QJX_ERR_INVALID_ARG;
+    const int d = 1 << N;
+    const size_t dd = (size_t)d * d, e2 = 2 * dd;
+    // channel c < N-1: the 4 x 4 con = tau |00><00| + k |11><11| + |01><10| + |10><01| on spins
+    // (c, c+1); channel N-1: the border pair (N-1, 0)
+    cvec l(e2 * N, 0.0);
+    for (int c = 0; c < N; c++) {
+        double *lc = l.data() + e2 * c;
+        const int ba = c < N - 1 ? N - 1 - c : 0, bb = c < N - 1 ? N - 2 - c : N - 1;
+        for (int s = 0; s < d; s++) {
+            const int a = (s >> ba) & 1, b = (s >> bb) & 1;
+            if (a == b) lc[2 * ((size_t)s * d + s)] = a ? k : tau;
+            else lc[2 * ((size_t)(s ^ (1 << ba) ^ (1 << bb)) * d + s)] = 1.0;
+        }
+    }
+    if (L) std::memcpy(L, l.data(), e2 * N * sizeof(double));
+    if (special) {
+        // X_ij = g_ij (1 + i), g Box-Muller normals of MCG31 seed 13371337 leapfrogged (seed,
+        // num_seeds); y = (X + X^H) / 2, special = y / sqrt(Re tr y^2) / sqrt(d)
+        qjxio::LeapfrogLCG st = qjxio::LeapfrogLCG::mcg31(13371337ull, (unsigned long long)seed,
+                                                            (unsigned long long)num_seeds);
+        const double two_pi = 2.0 * 3.1415926535897932384626433832795;
+        std::vector<double> g(dd);
+        for (size_t e = 0; e < dd; e++) {
+            const double u1 = st.next(), u2 = st.next();
+            g[e] = std::sqrt(-2.0 * std::log(u1)) * std::sin(two_pi * u2);
+        }
+        cvec y(e2);
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                const double gij = g[(size_t)i * d + j], gji = g[(size_t)j * d + i];
+                y[2 * ((size_t)i * d + j)] = 0.5 * (gij + gji);
+                y[2 * ((size_t)i * d + j) + 1] = 0.5 * (gij + -gji);
+            }
+        double tr = 0.0;
+        for (int i = 0; i < d; i++) {
+            double sr = 0.0;
+            for (int q = 0; q < d; q++)
+                sr = sr + (y[2 * ((size_t)i * d + q)] * y[2 * ((size_t)q * d + i)] -
+                           y[2 * ((size_t)i * d + q) + 1] * y[2 * ((size_t)q * d + i) + 1]);
+            tr = tr + sr;
+        }
+        const double sy = std::sqrt(tr), sd = std::sqrt(double(d));
+        for (size_t e = 0; e < e2; e++) special[e] = (y[e] / sy) / sd;
+    }
+    if (!Kout && !Utree) return QJX_OK;
+    // init_hamiltonians_qj: H_eff = 0 - (i/2) sum_c L_c^H L_c (gamma 1), K = -i H_eff
+    cvec hp(e2, 0.0), kk(e2);
+    for (int c = 0; c < N; c++) {
+        const double *lc = l.data() + e2 * c;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int q = 0; q < d; q++) {
+                    const double ar = lc[2 * ((size_t)q * d + i)], ai = lc[2 * ((size_t)q * d + i) + 1];
+                    const double br = lc[2 * ((size_t)q * d + j)], bi = lc[2 * ((size_t)q * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (1.0 * si);
+                hp[2 * idx + 1] -= 0.5 * (1.0 * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        kk[2 * e] = 0.0 + hp[2 * e + 1];
+        kk[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    if (Kout) std::memcpy(Kout, kk.data(), e2 * sizeof(double));
+    if (!Utree) return QJX_OK;
+    // init_split_structure_integrable (core.cpp:10610-10660): like MBL, one head of duration T
+    // whose two children run the tree of T
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
+    for (int lv = 0; lv < deep; lv++) {
+        double dt = T * 0.5;
+        for (int q = 0; q <= lv; q++) dt *= 0.5;
+        cvec scaled(e2);
+        for (size_t e = 0; e < e2; e++) scaled[e] = kk[e] * dt;
+        ok = expm(d, scaled.data(), Utree + e2 * (size_t)lv) && ok;
+    }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

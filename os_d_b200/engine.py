@@ -241,15 +241,16 @@ class Engine:
     # ---------------------------------------------------------- Lyapunov task (task_id 7)
     def lpn_start(self, lpn_type=-1, eps_deep=100, eps_low=-10.0, eps_high=10.0, eps_error=1e-10, delta_s=1e-3,
                   delta_f_high=1e-1, delta_f_low=1e-5, per_period=0, max_energy=1.0, mbl_Nc=0, spec_div=1.0,
-                  jcs=0):
+                  chars_sys=None):
         """Copy every base [0, n/2) into its variation n/2 + b and perturb it (LpnMult trans_process);
         keyword names follow the reference's lpn_* params.  mbl_Nc > 0 selects the MBL
-        characteristics (H in observable slot 0, spec = slot 0 / spec_div, mean = imbalance); jcs=1 the
-        JCS ones (a in slot 0, spec = slot 0 / alpha, mean = <a^+ a> from the energy observable)."""
+        characteristics (H in observable slot 0, spec = slot 0 / spec_div, mean = imbalance); chars_sys
+        1 the JCS ones (a in slot 0, spec = slot 0 / alpha, mean = <a^+ a> from the energy
+        observable), 5 the Integrable ones (the special matrix in slot 0, spec_div 1)."""
         c = N.QjxLpnConfig(lpn_type=lpn_type, eps_deep=eps_deep, per_period=int(per_period), eps_low=eps_low,
                            eps_high=eps_high, eps_error=eps_error, delta_s=delta_s, delta_f_high=delta_f_high,
                            delta_f_low=delta_f_low, max_energy=max_energy, mbl_Nc=mbl_Nc, spec_div=spec_div,
-                           jcs=int(jcs))
+                           chars_sys=(3 if mbl_Nc else 0) if chars_sys is None else chars_sys)
         self._chk(N.lib().qjx_lpn_start(self.h, C.byref(c)), "qjx_lpn_start")
 
     def lpn_period(self, curr_time, adr_dump=-1):

@@ -62,6 +62,13 @@ def suffix(cfg, prm):
     JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
     for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 5:  # IntegrableOutputBehavior::suffix_param (outputter.cpp:244-269)
+        return ("_setup(%d_%d_%d)" % (5, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_N(%d)_seed(%d)_tau(%d)_k(%d)" % (int(prm["integrable_N"]), int(prm["integrable_seed"]),
+                                                     int(prm["integrable_tau"]), int(prm["integrable_k"]))
+                + "_T(%s)" % f4(prm["integrable_T"])
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 3:
         return ("_setup(%d_%d_%d)" % (3, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -97,17 +104,27 @@ def lpn_suffix(prm):
                                         np.log10(prm["lpn_delta_f_high"]), np.log10(prm["lpn_delta_f_low"]))
 
 
+def integrable_model(prm):
+    """The Integrable operators (L [N], special, K) of a params dict."""
+    return O.integrable_operators(int(prm["integrable_N"]), int(prm["integrable_seed"]),
+                                  int(prm["integrable_num_seeds"]), float(prm["integrable_tau"]),
+                                  float(prm["integrable_k"]))
+
+
 def expected_outputs(cfg, prm, R=None):
     """All files the drop-in writes, as {relative file name: text}."""
     if cfg.get("task_id", 1) == 7:
         return expected_lpn_outputs(cfg, prm, R)
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
-    N = 0 if mbl else int(prm["N"])
+    integ = cfg.get("sys_id", 0) == 5
+    N = 0 if (mbl or integ) else int(prm["N"])
     d = N if jcs else N + 1
     if mbl:
         Nc = int(prm["mbl_Nc"])
         d = len(O.mbl_basis(Nc))
+    if integ:
+        d = 1 << int(prm["integrable_N"])
     n = cfg["num_trajectories"]
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
@@ -126,6 +143,14 @@ def expected_outputs(cfg, prm, R=None):
         T = t_head = alpha
         ens = O.Ensemble(U, L, [1.0], HE, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
                          branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+    elif integ:  # Integrable: H = 0, one head of duration integrable_T, two children; spec = <special>
+        Ls, S, K = integrable_model(prm)
+        T = prm["integrable_T"]
+        Ut = O.split_tree(K, T, deep)
+        U = np.stack([Ut, Ut])
+        H = np.zeros_like(S)
+        Rs = np.concatenate([S[None], R]) if nr else S[None]
+        ens = O.Ensemble(U, Ls, [1.0] * Ls.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
     elif mbl:  # MBL: one head of duration mbl_T, two children of the same tree; spec = <H> / W
         en, H, Ls, K = O.mbl_operators(Nc, prm["mbl_prm_W"], prm["mbl_prm_U"], prm["mbl_prm_J"], int(prm["mbl_seed"]),
                                        int(prm["mbl_mns"]), int(prm["diss_type"]), prm["diss_phase"],
@@ -164,7 +189,14 @@ def expected_outputs(cfg, prm, R=None):
     files = {}
     if mbl:  # newdel.cpp:903-905: written to the working directory
         files["energies" + sfx] = f_double_data(en)
-    if mbl and cfg.get("is_debug", 0):
+    if integ and cfg.get("is_debug", 0):
+        files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
+        for c in range(Ls.shape[0]):
+            files[path + "dissipator_%d" % c + sfx] = f_complex_data(Ls[c].reshape(-1))
+        files[path + "hamiltonians_qj_0" + sfx] = f_complex_data(K.reshape(-1))
+        files[path + "spec_mtx" + sfx] = f_complex_data(S.reshape(-1))
+        files[path + "exp_mtx_0" + sfx] = f_complex_data(Ut[-1].reshape(-1))
+    elif mbl and cfg.get("is_debug", 0):
         files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
         for c in range(Ls.shape[0]):
             files[path + "dissipator_%d" % c + sfx] = f_complex_data(Ls[c].reshape(-1))
@@ -255,8 +287,8 @@ def expected_outputs(cfg, prm, R=None):
     last = obs[-1]
     if dump_purity == 1:
         emit("purity_evo" + sfx, f_double_data(purity), False)
-    if jcs or mbl:
-        div = alpha if jcs else prm["mbl_prm_W"]
+    if jcs or mbl or integ:
+        div = alpha if jcs else prm["mbl_prm_W"] if mbl else 1.0
         for o in obs:
             z = o["random_obs"][:, 0]  # result.real /= div; result.imag /= div (real divisions)
             o["spec"] = z.real / div + 1j * (z.imag / div)
@@ -267,10 +299,10 @@ def expected_outputs(cfg, prm, R=None):
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("spec" + sfx, f_complex_data(last["spec"]), False)
         emit("imbalance" + sfx, f_double_data(last["imbalance"]), False)
-    if jcs and int(prm["dump_obs"]) == 1:
+    if (jcs or integ) and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("spec" + sfx, f_complex_data(last["spec"]), False)
-    if not jcs and not mbl and int(prm["dump_obs"]) == 1:
+    if not jcs and not mbl and not integ and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
         emit("mean" + sfx, f_double_data(last["mean"]), False)
@@ -287,6 +319,7 @@ def expected_outputs(cfg, prm, R=None):
         emit("periods" + sfx, f_int_data(dp), False)
         keys = ((("norm", "norm_evo"), ("energy", "mean_evo")) if jcs else
                 (("norm", "norm_evo"), ("imbalance", "imbalance_evo")) if mbl else
+                (("norm", "norm_evo"),) if integ else
                 (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
                  ("energy", "energy_evo")))
         for key, name in keys:
@@ -294,7 +327,7 @@ def expected_outputs(cfg, prm, R=None):
             for i, o in enumerate(obs):
                 grid[i] = o[key]
             emit(name + sfx, f_2d_inv(grid), False)
-        if jcs or mbl:
+        if jcs or mbl or integ:
             grid = np.zeros((ndt, n), complex)
             for i, o in enumerate(obs):
                 grid[i] = o["spec"]
@@ -323,14 +356,17 @@ def expected_lpn_outputs(cfg, prm, R=None):
     and the adr files (dump.cpp:3-98)."""
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
     jcs = cfg.get("sys_id", 0) == 1  # JCS: a in observable slot 0, <a^+ a>, JCS file set
-    spec = mbl or jcs
-    N = 0 if mbl else int(prm["N"])
+    integ = cfg.get("sys_id", 0) == 5  # Integrable: the special matrix in slot 0, spec only
+    spec = mbl or jcs or integ
+    N = 0 if (mbl or integ) else int(prm["N"])
     d = N if jcs else N + 1
     if mbl:
         Nc, W = int(prm["mbl_Nc"]), float(prm["mbl_prm_W"])
         d = len(O.mbl_basis(Nc))
     if jcs:
         W = float(prm["jcs_prm_alpha"])  # the spec divisor
+    if integ:
+        d, W = 1 << int(prm["integrable_N"]), 1.0
     n = cfg["num_trajectories"]
     half = n // 2
     deep = cfg.get("ex_deep", 16)
@@ -348,6 +384,14 @@ def expected_lpn_outputs(cfg, prm, R=None):
         calc_T = heads[0] + heads[1]  # JCSCoreBehaviour::calc_T (core.cpp:2833-2845)
         ens = O.Ensemble(U, L, [1.0], Nop, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
                          branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+    elif integ:
+        L, S, K = integrable_model(prm)
+        T = calc_T = prm["integrable_T"]
+        Ut = O.split_tree(K, T, deep)
+        H = np.zeros_like(S)
+        Rs = np.concatenate([S[None], R]) if nr else S[None]
+        ens = O.Ensemble(np.stack([Ut, Ut]), L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]),
+                         rec_cap=100000)
     elif mbl:
         en, H, L, K = O.mbl_operators(Nc, W, prm["mbl_prm_U"], prm["mbl_prm_J"], int(prm["mbl_seed"]),
                                       int(prm["mbl_mns"]), int(prm["diss_type"]), prm["diss_phase"], prm["diss_gamma"])
@@ -381,13 +425,13 @@ def expected_lpn_outputs(cfg, prm, R=None):
         period[0] += k
         return rc
 
-    max_energy = float(np.max(np.abs(np.diag(H).real)))
+    max_energy = float(np.max(np.abs(np.diag(H).real))) if not integ else 0.0
     lp = O.Lpn(ens, lpn_type=int(prm["lpn_type"]), eps_deep=int(prm["lpn_eps_deep"]),
                eps_low=float(prm["lpn_eps_low"]), eps_high=float(prm["lpn_eps_high"]),
                eps_error=float(prm["lpn_eps_error"]), delta_s=float(prm["lpn_delta_s"]),
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
-               mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0, jcs=jcs)
+               mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0, chars_sys=cfg.get("sys_id", 0))
     dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
     ndt = len(dp)
     assert advance(cfg.get("num_tp_periods", 0), is_obs=0, tr1=half) == 0
@@ -458,6 +502,12 @@ def expected_lpn_outputs(cfg, prm, R=None):
         emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
         emit("spec_lpn" + sfx, f_complex_data(lpn[-1]["spec_lpn"]), False)
         emit("imbalance_lpn" + sfx, f_double_data(lpn[-1]["mean_lpn"]), False)
+    if integ and int(prm["dump_obs"]) == 1:
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("spec" + sfx, f_complex_data(last["spec"]), False)
+        emit("lambda" + sfx, f_double_data(lpn[-1]["lambda_now"]), False)
+        emit("num_renorms" + sfx, f_int_data(lpn[-1]["num_renorms"]), False)
+        emit("spec_lpn" + sfx, f_complex_data(lpn[-1]["spec_lpn"]), False)
     if jcs and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("spec" + sfx, f_complex_data(last["spec"]), False)
@@ -486,6 +536,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
         emit("periods" + sfx, f_int_data(dp), False)
         keys = ((("norm", "norm_evo"), ("imbalance", "imbalance_evo")) if mbl else
                 (("norm", "norm_evo"), ("energy", "mean_evo")) if jcs else
+                (("norm", "norm_evo"),) if integ else
                 (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
                  ("energy", "energy_evo")))
         for key, name in keys:
@@ -505,6 +556,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
                     emit("jump_etas_%d" % tr + sfx, f_double_data(et), False)
         keys = ((("lambda_now", "lambda_evo"), ("mean_lpn", "imbalance_lpn_evo")) if mbl else
                 (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo")) if jcs else
+                (("lambda_now", "lambda_evo"),) if integ else
                 (("lambda_now", "lambda_evo"), ("mean_lpn", "mean_lpn_evo"), ("energy_lpn", "energy_lpn_evo")))
         for key, name in keys:
             emit(name + sfx, f_2d_inv(np.array([v[key] for v in lpn])), False)
@@ -521,6 +573,10 @@ def expected_lpn_outputs(cfg, prm, R=None):
 
 
 JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_1": 0.5, "jcs_drv_part_2": 1.5}
+
+# submit_integrable.py's system (tau 1, k -1, integrable_N 7 there; 6 spins here), one disorder seed
+INTEGRABLE_PARAMS = {"integrable_N": 6, "integrable_seed": 2, "integrable_num_seeds": 1000000, "integrable_tau": 1.0,
+                     "integrable_k": -1.0, "integrable_T": 1.0}
 
 # the production MBL sweeps' values (Nc 8, diss_type 1, gamma 0.1, J 1, T 10), one disorder seed
 MBL_PARAMS = {"mbl_Nc": 8, "mbl_seed": 3, "mbl_mns": 1000000, "mbl_prm_W": 2.5, "mbl_prm_U": 1.0, "mbl_prm_J": 1.0,

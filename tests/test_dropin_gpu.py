@@ -8,8 +8,8 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS, config_text,
-                                 expected_outputs, params_text)
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS,
+                                 config_text, expected_outputs, params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -25,6 +25,7 @@ def run_case(tmp_path, cfg, prm):
     d = int(prm["N"]) + 1
     d = int(prm["N"]) if cfg.get("sys_id", 0) == 1 else d
     d = math.comb(int(prm["mbl_Nc"]), int(prm["mbl_Nc"]) // 2) if cfg.get("sys_id", 0) == 3 else d
+    d = 1 << int(prm["integrable_N"]) if cfg.get("sys_id", 0) == 5 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -152,6 +153,31 @@ def test_jcs_lpn_mult_files_match(tmp_path, lpn_type):
     k = [k for k in exp if k.startswith("num_renorms")][0]
     assert sum(int(x) for x in exp[k].split()) > 0
     assert any(k.startswith("mean_lpn_evo") for k in exp) and any(k.startswith("spec_lpn_evo") for k in exp)
+
+
+def test_integrable_system_files_match(tmp_path):
+    """The Integrable system (sys_id 5): 6 spins (d = 64), H = 0, 6 pair dissipators incl. the
+    border, spec = <special> (newdel.cpp:310-345, 1030-1095, 1924-2076, 2914-3004; core.cpp:6470-6819)."""
+    cfg = dict(BASE_CONFIG, sys_id=5, num_trajectories=16, num_tp_periods=1, num_obs_periods=4, is_debug=1)
+    prm = {**BASE_PARAMS, **INTEGRABLE_PARAMS, "dump_num": 2, "jump": 2, "dump_adr_sep": 1, "dump_adr_avg": 1}
+    exp = run_case(tmp_path, cfg, prm)
+    types = set()
+    for k, v in exp.items():
+        if k.startswith("diss_types_"):
+            types.update(int(x) for x in v.split())
+    assert len(types) == 6
+
+
+@pytest.mark.parametrize("lpn_type", [-1, 0])
+def test_integrable_lpn_mult_files_match(tmp_path, lpn_type):
+    """Integrable LpnMult (sys_id 5, task_id 7; submit_integrable.py): spec and random-observable
+    distances, the Integrable Lyapunov file set (core.cpp:6685-6858)."""
+    cfg = dict(BASE_CONFIG, sys_id=5, task_id=7, num_trajectories=16, num_tp_periods=2, num_obs_periods=5)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **INTEGRABLE_PARAMS, "lpn_type": lpn_type, "dump_num": 5, "jump": 1,
+           "dump_adr_sep": 1, "dump_adr_avg": 1, "save_lambdas": 1, "lpn_delta_f_high": 1e-2}
+    exp = run_case(tmp_path, cfg, prm)
+    k = [k for k in exp if k.startswith("num_renorms")][0]
+    assert sum(int(x) for x in exp[k].split()) > 0
 
 
 def test_jcs_system_files_match(tmp_path):
