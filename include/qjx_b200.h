@@ -266,11 +266,12 @@ qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_t
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
                            double *H, double *Hd, double *L, double *K, double *Utree);
 /* The JCS system (sys_id 1; newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601; split structure
- * core.cpp:10086-10124): d = N, H = 0.5/alpha^3 a^+a^+aa, H_drv = a^+ - a, L = a, the number
+ * core.cpp:10086-10157): d = N, H = 0.5/alpha^3 a^+a^+aa, H_drv = a^+ - a, L = a, the number
  * operator Nop = a^+ a and the observable `special` A_op = a; K_0 = -i H_eff + E0 H_drv (the kick),
  * K_1 = -i H_eff with gamma = 1/(4 alpha); Utree [2][deep][d][d] = exp(K_b head_b 2^-(l+2)) with
- * head_b = part_b alpha (branch b lasts head_b / 2: qjx_config.branch_len = head_b / 2).  Any
- * output pointer may be NULL. */
+ * head_b = part_b alpha.  A period runs each part as two halves (the head's two children): engine
+ * branches [U_0, U_0, U_1, U_1] with qjx_config.branch_len [head_0, head_0, head_1, head_1] / 2.
+ * Any output pointer may be NULL. */
 qjx_status qjx_build_jcs(int N, double alpha, double drv_ampl, double part_1, double part_2, int deep, double *H,
                          double *Hd, double *L, double *Nop, double *A_op, double *Kout, double *Utree);
 /* The MBL system (sys_id 3; MBLNewDelBehaviour, newdel.cpp:182-271, 868-958, 1699-1815, 2751-2838):
@@ -286,6 +287,17 @@ qjx_status qjx_mbl_size(int Nc, int diss_type, int *d, int *num_diss);
 qjx_status qjx_build_mbl(int Nc, double W, double U, double J, int mbl_seed, int mbl_mns, int diss_type,
                          double diss_phase, double gamma, double T, int deep, double *energies, int *id_to_x,
                          double *H, double *L, double *K, double *Utree);
+/* The PS system (sys_id 2; PSNewDelBehaviour, newdel.cpp:132-181, 650-866, 1582-1697, 2603-2749): ns
+ * spins times nps photon states, d = 2^ns nps (spins (x) photons, spin 0 the most significant);
+ * H = (d_prm/2) J_z + (g_prm/2)(J_- a^+ + J_+ a) + 0.5/alpha^3 a^+a^+aa, H_drv = a^+ - a; L [1 + ns
+ * for diss_type 1]: a, then sigma_- of each spin; S [4][d][d] = a, J_z, J_+, a^+a (spec, spec_2,
+ * spec_3, photons); K [2] = -i H_eff + E0 H_drv (the kick), -i H_eff with gamma 1/(4 alpha) on the
+ * cavity and diss_w on the spins; jump rates 1; Utree [2][deep][d][d] = exp(K_b head_b 2^-(l+2)),
+ * head_b = part_b alpha, each part run as two halves (init_split_structure_ps, core.cpp:10234-10305:
+ * engine branches [K_0, K_0, K_1, K_1] of durations head_b / 2).  Any output pointer may be NULL. */
+qjx_status qjx_build_ps(int ns, int nps, double alpha, double d_prm, double g_prm, double drv_ampl, int diss_type,
+                        double diss_w, double part_1, double part_2, int deep, double *H, double *Hd, double *L,
+                        double *S, double *K, double *Utree);
 /* The Integrable system (sys_id 5; IntegrableNewDelBehaviour, newdel.cpp:310-345, 1030-1095, 1924-2076,
  * 2914-3004): N spins (3 <= N <= 10), d = 2^N, H = 0; L [N][d][d]: the 4 x 4 operator tau |00><00| +
  * k |11><11| + |01><10| + |10><01| on spins (c, c+1), c < N - 1, and on the border pair (N-1, 0);

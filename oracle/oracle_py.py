@@ -66,6 +66,7 @@ def lib():
         L.orc_mbl_operators.argtypes = ([C.c_int] + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_double] * 2
                                         + [c_double_p] * 4)
         L.orc_mbl_imbalance.argtypes = [C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
+        L.orc_ps_operators.argtypes = [C.c_int] * 2 + [C.c_double] * 4 + [C.c_int, C.c_double] + [c_double_p] * 6
         L.orc_integrable_operators.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [c_double_p] * 3
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -144,6 +145,17 @@ def mbl_operators(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma):
     assert lib().orc_mbl_operators(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, _dp(en), _dp(H),
                                    _dp(L), _dp(K)) == 0
     return en, H, L, K
+
+
+def ps_operators(ns, nps, alpha, dprm, gprm, drv_ampl, diss_type, diss_w):
+    """PS (sys_id 2): H, Hd, L [1 + ns diss_type], S [4] (spec, spec_2, spec_3, photons), K0, K1."""
+    d = (1 << ns) * nps
+    nd = 1 if diss_type == 0 else 1 + ns
+    H, Hd, K0, K1 = (_cplx((d, d)) for _ in range(4))
+    L, S = _cplx((nd, d, d)), _cplx((4, d, d))
+    assert lib().orc_ps_operators(ns, nps, alpha, dprm, gprm, drv_ampl, diss_type, diss_w, _dp(H), _dp(Hd), _dp(L),
+                                  _dp(S), _dp(K0), _dp(K1)) == 0
+    return H, Hd, L, S, K0, K1
 
 
 def integrable_operators(N, seed, num_seeds, tau, k):

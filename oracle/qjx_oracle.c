@@ -395,6 +395,109 @@ int orc_integrable_operators(int N, int seed, int num_seeds, double tau, double 
     return 0;
 }
 
+/* PS (sys_id 2, newdel.cpp:132-181, 650-866, 1582-1697, 2603-2749): ns spins (index x, spin 0 the most
+ * significant bit) times nps photon states, basis index x nps + k (Kronecker order spins (x) photons).
+ *   H  = (d/2) J_z (x) 1 + (g/2)(J_- (x) a^+ + J_+ (x) a) + 1 (x) (0.5/alpha^3) a^+a^+aa, J = sum sigma / 2
+ *   Hd = 1 (x) (a^+ - a);  S = [1 (x) a, J_z (x) 1, J_+ (x) 1, 1 (x) a^+a] (spec, spec_2, spec_3, photons)
+ *   L  = [1 (x) a] (+ [sigma_-^(s) (x) 1] for diss_type 1), H_eff with gamma 1/(4 alpha) for the
+ *        cavity and diss_w for the spins; K0 = -i H_eff + E0 Hd (the kick), K1 = -i H_eff. */
+int orc_ps_operators(int ns, int nps, double alpha, double dprm, double gprm, double drv_ampl, int diss_type,
+                     double diss_w, double *H, double *Hd, double *L, double *S, double *K0, double *K1)
+{
+    if (ns < 1 || ns > 8 || nps < 2 || (diss_type != 0 && diss_type != 1)) return 1;
+    const int n2 = 1 << ns, d = n2 * nps, nd = diss_type == 0 ? 1 : 1 + ns;
+    const size_t dd = (size_t)d * d, pp = (size_t)nps * nps;
+    double *a = (double *)calloc(pp, sizeof(double)), *ad = (double *)calloc(pp, sizeof(double));
+    double *m1 = (double *)malloc(pp * sizeof(double)), *m2 = (double *)malloc(pp * sizeof(double));
+    double *m3 = (double *)malloc(pp * sizeof(double)), *nop = (double *)malloc(pp * sizeof(double));
+    double *jz = (double *)calloc((size_t)n2 * n2, sizeof(double)), *jm = (double *)calloc((size_t)n2 * n2, sizeof(double));
+    double *jp = (double *)calloc((size_t)n2 * n2, sizeof(double)), *hp = (double *)malloc(2 * dd * sizeof(double));
+    if (!a || !ad || !m1 || !m2 || !m3 || !nop || !jz || !jm || !jp || !hp) return 2;
+    for (int k = 0; k < nps - 1; k++) {
+        a[(size_t)k * nps + (k + 1)] = sqrt((double)(k + 1));
+        ad[(size_t)(k + 1) * nps + k] = sqrt((double)(k + 1));
+    }
+    rmatmul(nps, ad, ad, m1);
+    rmatmul(nps, m1, a, m2);
+    rmatmul(nps, m2, a, m3);
+    rmatmul(nps, ad, a, nop);
+    const double hs = 0.5 / pow(alpha, 3);
+    /* J_z, J_-, J_+: sums over spins of sigma_z = diag(1, -1), sigma_- = |1><0|, sigma_+ = |0><1| */
+    for (int sp = 0; sp < ns; sp++)
+        for (int x = 0; x < n2; x++) {
+            const int bit = 1 << (ns - 1 - sp), b = (x & bit) != 0;
+            jz[(size_t)x * n2 + x] += b ? -1.0 : 1.0;
+            if (!b) jm[(size_t)(x | bit) * n2 + x] += 1.0;
+            else jp[(size_t)(x & ~bit) * n2 + x] += 1.0;
+        }
+    for (size_t e = 0; e < (size_t)n2 * n2; e++) {
+        jz[e] *= 0.5;
+        jm[e] *= 0.5;
+        jp[e] *= 0.5;
+    }
+    const double sd = dprm * 0.5, sg = gprm * 0.5;
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(Hd, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 2 * dd * (size_t)nd * sizeof(double));
+    memset(S, 0, 8 * dd * sizeof(double));
+    for (int xi = 0; xi < n2; xi++)
+        for (int xj = 0; xj < n2; xj++)
+            for (int ki = 0; ki < nps; ki++)
+                for (int kj = 0; kj < nps; kj++) {
+                    const size_t I = (size_t)xi * nps + ki, J = (size_t)xj * nps + kj, e = I * d + J;
+                    const double id_s = xi == xj ? 1.0 : 0.0, id_p = ki == kj ? 1.0 : 0.0;
+                    const size_t pe = (size_t)ki * nps + kj, se = (size_t)xi * n2 + xj;
+                    const double s_ham = (sd * jz[se]) * id_p;
+                    const double s_p = sg * (ad[pe] * jm[se] + jp[se] * a[pe]);
+                    const double p_ham = id_s * (hs * m3[pe]);
+                    H[2 * e] = (s_ham + s_p) + p_ham;
+                    Hd[2 * e] = id_s * (ad[pe] - a[pe]);
+                    S[2 * e] = id_s * a[pe];
+                    S[2 * (dd + e)] = jz[se] * id_p;
+                    S[2 * (2 * dd + e)] = jp[se] * id_p;
+                    S[2 * (3 * dd + e)] = id_s * nop[pe];
+                    L[2 * e] = id_s * a[pe];
+                }
+    if (diss_type == 1)
+        for (int sp = 0; sp < ns; sp++) {
+            double *Lc = L + 2 * dd * (size_t)(1 + sp);
+            const int bit = 1 << (ns - 1 - sp);
+            for (int x = 0; x < n2; x++)
+                if (!(x & bit))
+                    for (int k = 0; k < nps; k++)
+                        Lc[2 * (((size_t)(x | bit) * nps + k) * d + (size_t)x * nps + k)] = 1.0;
+        }
+    for (size_t e = 0; e < dd; e++) {
+        hp[2 * e] = H[2 * e];
+        hp[2 * e + 1] = 0.0;
+    }
+    for (int c = 0; c < nd; c++) {
+        const double *Lc = L + 2 * dd * (size_t)c;
+        const double gamma = c == 0 ? 1.0 / (4.0 * alpha) : diss_w;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int k = 0; k < d; k++) {
+                    const double ar = Lc[2 * ((size_t)k * d + i)], ai = Lc[2 * ((size_t)k * d + i) + 1];
+                    const double br = Lc[2 * ((size_t)k * d + j)], bi = Lc[2 * ((size_t)k * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (gamma * si);
+                hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        K0[2 * e] = 0.0 + (hp[2 * e + 1] + drv_ampl * Hd[2 * e]);
+        K0[2 * e + 1] = 0.0 - (hp[2 * e] + drv_ampl * 0.0);
+        K1[2 * e] = 0.0 + (hp[2 * e + 1] + 0.0 * Hd[2 * e]);
+        K1[2 * e + 1] = 0.0 - (hp[2 * e] + 0.0 * 0.0);
+    }
+    free(a); free(ad); free(m1); free(m2); free(m3); free(nop); free(jz); free(jm); free(jp); free(hp);
+    return 0;
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

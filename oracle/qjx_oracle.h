@@ -65,6 +65,11 @@ int orc_mbl_operators(int Nc, double W, double U, double J, int mbl_seed, int mb
                       double gamma, double *energies, double *H, double *L, double *K);
 void orc_mbl_imbalance(int Nc, int d, int n, const double *adr, double *out);
 
+/* PS (sys_id 2, newdel.cpp:132-181, 650-866, 1582-1697, 2603-2749): d = 2^ns nps; H, Hd, L [1 (+ ns)],
+ * S [4] = special, special_2, special_3, special_4, K0 (kick), K1, all complex d x d. */
+int orc_ps_operators(int ns, int nps, double alpha, double dprm, double gprm, double drv_ampl, int diss_type,
+                     double diss_w, double *H, double *Hd, double *L, double *S, double *K0, double *K1);
+
 /* Integrable (sys_id 5, newdel.cpp:310-345, 1030-1095, 1924-2076, 2914-3004): d = 2^N, H = 0, L [N][d][d]
  * (the con 4 x 4 on neighbouring spins and on the border pair), special (the spec observable), K. */
 int orc_integrable_operators(int N, int seed, int num_seeds, double tau, double kk, double *L, double *special,

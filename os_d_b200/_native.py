@@ -21,7 +21,7 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
+    "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_build_ps", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
     "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
@@ -117,6 +117,8 @@ def lib():
         L.qjx_build_mbl.argtypes = ([C.c_int] + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int]
                                     + [c_double_p, c_int_p] + [c_double_p] * 4)
         L.qjx_mbl_imbalance.argtypes = [C.c_int, C.c_int, c_double_p, c_double_p]
+        L.qjx_build_ps.argtypes = ([C.c_int] * 2 + [C.c_double] * 4 + [C.c_int] + [C.c_double] * 3 + [C.c_int]
+                                   + [c_double_p] * 6)
         L.qjx_build_integrable.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int] + [c_double_p] * 4
         L.qjx_build_dimer_rk.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 2
         L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -178,8 +180,9 @@ def build_dimer_deep(N, J, U, E, A, g, omega, deep, deep_num_steps):
 
 
 def build_jcs(N, alpha, drv_ampl, part_1, part_2, deep):
-    """JCS system (sys_id 1): H, H_drv, L = a, Nop = a^+ a, A = a and the split tree [2][deep][N][N];
-    branch b lasts part_b * alpha / 2 (pass branch_len to the engine)."""
+    """JCS system (sys_id 1): H, H_drv, L = a, Nop = a^+ a, A = a and the split trees [2][deep][N][N];
+    a period runs part b (head part_b * alpha) as two halves: engine branches [U0, U0, U1, U1] with
+    branch_len [h0, h0, h1, h1] / 2."""
     d = N
     H, Hd, L, Nop, A = (np.zeros((d, d), np.complex128) for _ in range(5))
     U = np.zeros((2, deep, d, d), np.complex128)
@@ -202,6 +205,19 @@ def build_mbl(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, T, d
     check(lib().qjx_build_mbl(Nc, W, U, J, mbl_seed, mbl_mns, diss_type, diss_phase, gamma, T, deep, dp(en),
                               xs.ctypes.data_as(c_int_p), dp(H), dp(Lm), None, dp(Ut)), what="qjx_build_mbl")
     return en, xs, H, Lm, Ut
+
+
+def build_ps(ns, nps, alpha, d_prm, g_prm, drv_ampl, diss_type, diss_w, part_1, part_2, deep):
+    """PS system (sys_id 2): H, Hd, L [1 + ns diss_type], S [4] (spec, spec_2, spec_3, photons) and the
+    split trees [2][deep][d][d] (part b's head part_b alpha, run as two halves)."""
+    d = (1 << ns) * nps
+    nd = 1 if diss_type == 0 else 1 + ns
+    H, Hd = np.zeros((d, d), np.complex128), np.zeros((d, d), np.complex128)
+    Lm, S = np.zeros((nd, d, d), np.complex128), np.zeros((4, d, d), np.complex128)
+    Ut = np.zeros((2, deep, d, d), np.complex128)
+    check(lib().qjx_build_ps(ns, nps, alpha, d_prm, g_prm, drv_ampl, diss_type, diss_w, part_1, part_2, deep, dp(H),
+                             dp(Hd), dp(Lm), dp(S), None, dp(Ut)), what="qjx_build_ps")
+    return H, Hd, Lm, S, Ut
 
 
 def build_integrable(N, seed, num_seeds, tau, k, T, deep):

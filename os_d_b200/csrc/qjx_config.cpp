@@ -188,6 +188,25 @@ std::string integrable_suffix(const RunParam &rp, const ConfigParam &cp, int pre
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string ps_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    auto f = [&](const char *key) {
+        std::stringstream v;
+        v << std::setprecision(precision) << std::fixed << param(cp, key);
+        return v.str();
+    };
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_s(" << int(param(cp, "ps_num_spins")) << ")";
+    s << "_nps(" << int(param(cp, "ps_num_photons_states")) << ")";
+    s << "_diss(" << int(param(cp, "diss_type")) << "_" << f("ps_diss_w") << ")";
+    s << "_drv(" << f("ps_drv_part_1") << "_" << f("ps_drv_part_2") << "_" << f("ps_drv_ampl") << ")";
+    s << "_prm(" << f("ps_prm_alpha") << "_" << f("ps_prm_d") << "_" << f("ps_prm_g") << ")";
+    s << "_start(" << int(param(cp, "start_type")) << "_" << int(param(cp, "start_state")) << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

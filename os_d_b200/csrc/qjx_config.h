@@ -51,6 +51,8 @@ std::string jcs_suffix(const RunParam &rp, const ConfigParam &cp, int precision 
 std::string mbl_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 // IntegrableOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:244-269)
 std::string integrable_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
+// PSOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:135-174)
+std::string ps_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 
 // init_dump_periods (source/cpp/QJX/QJX/newdel_exp.cpp:408-455); empty on a bad dump_type.
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods);

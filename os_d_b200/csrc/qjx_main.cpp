@@ -2,7 +2,7 @@
 // Std task (task_id 1) and the LpnMult task (task_id 7) with the QJ propagator (prop_id 0) or the
 // RK propagator (prop_id 1), and the StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0);
 // the Std and LpnMult tasks with the QJ propagator for the JCS (sys_id 1), MBL (sys_id 3) and
-// Integrable (sys_id 5) systems.
+// Integrable (sys_id 5) systems, and the Std task with the QJ propagator for PS (sys_id 2).
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -385,12 +385,15 @@ int main(int argc, char **argv)
     if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
     std::cout << params_echo(rp, cp);
 
-    if (rp.sys_id != 0 && rp.sys_id != 1 && rp.sys_id != 3 && rp.sys_id != 5)
+    if (rp.sys_id < 0 || rp.sys_id > 5 || rp.sys_id == 4)
         die("Wrong sys_id: " + std::to_string(rp.sys_id) +
-            " (this engine runs the dimer (0), JCS (1), MBL (3) and Integrable (5) systems)");
+            " (this engine runs the dimer (0), JCS (1), PS (2), MBL (3) and Integrable (5) systems)");
     const bool jcs = rp.sys_id == 1;  // JCS, MBL, Integrable: Std and LpnMult with the QJ propagator
     const bool mbl = rp.sys_id == 3;
     const bool integ = rp.sys_id == 5;
+    const bool ps = rp.sys_id == 2;  // PS: the Std task with the QJ propagator
+    if (ps && (rp.task_id != 1 || rp.prop_id != 0))
+        die("Wrong task_id / prop_id for sys_id 2 (this engine runs PS with the Std task and the QJ propagator)");
     if ((jcs || mbl || integ) && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
         die("Wrong task_id / prop_id for sys_id " + std::to_string(rp.sys_id) +
             " (this engine runs JCS, MBL and Integrable with the Std and LpnMult tasks and the QJ propagator)");
@@ -405,6 +408,7 @@ int main(int argc, char **argv)
         cp.fn_suffix = jcs ? jcs_suffix(rp, cp, 4)
                        : mbl ? mbl_suffix(rp, cp, 4)
                        : integ ? integrable_suffix(rp, cp, 4)
+                       : ps    ? ps_suffix(rp, cp, 4)
                                : dimer_suffix(rp, cp, 4);
     } catch (const std::exception &e) {
         die(e.what());
@@ -415,8 +419,13 @@ int main(int argc, char **argv)
     }
 
     try {
-        const bool dimer = !jcs && !mbl && !integ;
-        const int N = (mbl || integ) ? 0 : int(param(cp, "N"));
+        const bool dimer = !jcs && !mbl && !integ && !ps;
+        const int N = (mbl || integ || ps) ? 0 : int(param(cp, "N"));
+        // PS: 2^ps_num_spins spin states times ps_num_photons_states photon states
+        const int ps_ns = ps ? int(param(cp, "ps_num_spins")) : 0, ps_np = ps ? int(param(cp, "ps_num_photons_states")) : 0;
+        const int ps_dt = ps ? int(param(cp, "diss_type")) : 0;
+        if (ps && (ps_ns < 1 || ps_ns > 8 || ps_np < 2 || (ps_dt != 0 && ps_dt != 1)))
+            die("ps_num_spins must be in [1, 8], ps_num_photons_states >= 2, diss_type 0 or 1");
         // Integrable: 2^integrable_N basis states, integrable_N jump channels
         const int Ni = integ ? int(param(cp, "integrable_N")) : 0;
         if (integ && (Ni < 3 || Ni > 10)) die("integrable_N must be in [3, 10]");
@@ -426,8 +435,12 @@ int main(int argc, char **argv)
         if (mbl && qjx_mbl_size(Nc, mbl_dt, &d_mbl, &nd_mbl) != QJX_OK)
             die("mbl_Nc must be even and in [2, 24], diss_type 0 or 1");
         // the dimer has N + 1 Fock states; the JCS oscillator is truncated at N states (newdel.cpp:110)
-        const int d = mbl ? d_mbl : integ ? (1 << Ni) : jcs ? N : N + 1, n = cp.num_trajectories, deep = cp.ex_deep;
-        const int num_diss = mbl ? nd_mbl : integ ? Ni : 1;
+        const int d = mbl ? d_mbl : integ ? (1 << Ni) : ps ? (1 << ps_ns) * ps_np : jcs ? N : N + 1;
+        const int n = cp.num_trajectories, deep = cp.ex_deep;
+        const int num_diss = mbl ? nd_mbl : integ ? Ni : ps ? (ps_dt == 0 ? 1 : 1 + ps_ns) : 1;
+        // JCS and PS run each drive part as two halves of its tree (init_split_structure_jcs / _ps,
+        // core.cpp:10086-10157, 10234-10305: counter 2): four engine branches [K_0, K_0, K_1, K_1]
+        const int nbr = (ps || jcs) ? 4 : 2;
         const double J = dimer ? param(cp, "dimer_prm_J") : 0.0, U = dimer ? param(cp, "dimer_prm_U") : 0.0;
         const double E = dimer ? param(cp, "dimer_prm_E") : 0.0;
         const double A = dimer ? param(cp, "dimer_drv_ampl") : 0.0, omega = dimer ? param(cp, "dimer_drv_freq") : 1.0;
@@ -454,7 +467,10 @@ int main(int argc, char **argv)
         const size_t dd = (size_t)d * d;
 
         // model (newdel.cpp init_*), debug dumps (debugger.cpp:142-168, qj_proc.cpp:115-119)
-        std::vector<double> H(2 * dd), Hd(2 * dd), L(2 * dd * num_diss), K(4 * dd), Ut(4 * dd * deep);
+        std::vector<double> H(2 * dd), Hd(2 * dd), L(2 * dd * num_diss), K(4 * dd), Ut(2 * dd * deep * nbr);
+        std::vector<double> Sps(ps ? 8 * dd : 0);  // PS: special, special_2, special_3, special_4
+        const double ps_alpha = ps ? param(cp, "ps_prm_alpha") : 0.0;
+        const double ps_p1 = ps ? param(cp, "ps_drv_part_1") : 0.0, ps_p2 = ps ? param(cp, "ps_drv_part_2") : 0.0;
         // StdDeep (task_id 4): the split tree of the sub-period T / (2 deep_num_steps)
         const bool deep_task = rp.task_id == 4;
         const int nsub = deep_task ? int(param(cp, "deep_num_steps")) : 0;
@@ -465,7 +481,12 @@ int main(int argc, char **argv)
             check(qjx_build_jcs(N, jcs_alpha, jcs_ampl, jcs_p1, jcs_p2, deep, H.data(), Hd.data(), L.data(), Nop.data(),
                                 Aop.data(), K.data(), Ut.data()),
                   nullptr, "qjx_build_jcs");
-        else if (mbl) {
+        if (jcs) {  // engine branches [U_0, U_0, U_1, U_1]
+            const size_t tree = 2 * dd * deep;
+            std::copy(Ut.begin() + tree, Ut.begin() + 2 * tree, Ut.begin() + 2 * tree);
+            std::copy(Ut.begin() + 2 * tree, Ut.begin() + 3 * tree, Ut.begin() + 3 * tree);
+            std::copy(Ut.begin(), Ut.begin() + tree, Ut.begin() + tree);
+        } else if (mbl) {
             // one branch head of duration mbl_T with two children of the same split tree
             // (init_split_structure_mbl, core.cpp:10382-10432): the engine's two branches
             std::vector<double> en(Nc);
@@ -477,6 +498,16 @@ int main(int argc, char **argv)
             std::copy(K.begin(), K.begin() + 2 * dd, K.begin() + 2 * dd);
             // written to the working directory, without `path` (newdel.cpp:903-905)
             save_double_data("energies" + cp.fn_suffix, en.data(), Nc, 16, false);
+        } else if (ps) {
+            check(qjx_build_ps(ps_ns, ps_np, ps_alpha, param(cp, "ps_prm_d"), param(cp, "ps_prm_g"),
+                               param(cp, "ps_drv_ampl"), ps_dt, param(cp, "ps_diss_w"), ps_p1, ps_p2, deep, H.data(),
+                               Hd.data(), L.data(), Sps.data(), K.data(), Ut.data()),
+                  nullptr, "qjx_build_ps");
+            // engine branches [U_0, U_0, U_1, U_1]
+            const size_t tree = 2 * dd * deep;
+            std::copy(Ut.begin() + tree, Ut.begin() + 2 * tree, Ut.begin() + 2 * tree);
+            std::copy(Ut.begin() + 2 * tree, Ut.begin() + 3 * tree, Ut.begin() + 3 * tree);
+            std::copy(Ut.begin(), Ut.begin() + tree, Ut.begin() + tree);
         } else if (integ) {
             // H = 0; `special` (the spec observable) into Hd's storage; one head of duration
             // integrable_T with two children of the same split tree (init_split_structure_integrable)
@@ -503,27 +534,36 @@ int main(int argc, char **argv)
             save_complex_data(path + "hamiltonians_qj_0" + sfx, K.data(), dd, 16, false);
             save_complex_data(path + "spec_mtx" + sfx, integ ? Hd.data() : H.data(), dd, 16, false);
             save_complex_data(path + "exp_mtx_0" + sfx, Ut.data() + 2 * dd * (deep - 1), dd, 16, false);
-        } else if (rp.is_debug) {
+        } else if (rp.is_debug) {  // Dimer / JCS / PSDebugBehaviour::save (debugger.cpp:3-53)
             save_complex_data(path + "hamiltonian" + sfx, H.data(), dd, 16, false);
-            save_complex_data(path + "dissipator_0" + sfx, L.data(), dd, 16, false);
+            for (int c = 0; c < num_diss; c++)
+                save_complex_data(path + "dissipator_" + std::to_string(c) + sfx, L.data() + 2 * dd * c, dd, 16, false);
             for (int b = 0; b < 2; b++) {
                 save_complex_data(path + "hamiltonians_qj_" + std::to_string(b) + sfx, K.data() + 2 * dd * b, dd, 16, false);
                 if (rp.prop_id == 0)  // the split tree exists for the QJ propagator only (qj_proc.cpp:115-119)
                     save_complex_data(path + "exp_mtx_" + std::to_string(b) + sfx,
-                                      Ut.data() + 2 * dd * ((size_t)b * deep + deep - 1), dd, 16, false);
+                                      Ut.data() + 2 * dd * ((size_t)((ps || jcs) ? 2 * b : b) * deep + deep - 1), dd, 16,
+                                      false);
+            }
+            if (jcs) save_complex_data(path + "spec_mtx" + sfx, Aop.data(), dd, 16, false);
+            if (ps) {
+                const char *names[4] = {"spec_mtx", "spec_2_mtx", "spec_3_mtx", "spec_4_mtx"};
+                for (int o = 0; o < 4; o++) save_complex_data(path + names[o] + sfx, Sps.data() + 2 * dd * o, dd, 16, false);
             }
         }
         std::vector<double> HE(2 * dd);
-        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : (mbl || integ) ? H[e] : H[e] + E * Hd[e];
+        for (size_t e = 0; e < 2 * dd; e++) HE[e] = jcs ? Nop[e] : (mbl || integ || ps) ? H[e] : H[e] + E * Hd[e];
         std::vector<double> R =
             random_observables(d, num_robs, robs_seed, int(param_or(cp, "random_obs_mns", 1000000)),
                                int(param_or(cp, "random_obs_type", 0)));
         // JCS: spec = <a> / alpha, MBL: spec = <H> / W ride in observable slot 0
         // Integrable: spec = <special> rides in observable slot 0 as well
-        const int robs_off = (jcs || mbl || integ) ? 1 : 0;
+        // PS: spec, spec_2, spec_3 and the photon number ride in slots 0..3
+        const int robs_off = (jcs || mbl || integ) ? 1 : ps ? 4 : 0;
         if (jcs) R.insert(R.begin(), Aop.begin(), Aop.end());
         if (mbl) R.insert(R.begin(), H.begin(), H.end());
         if (integ) R.insert(R.begin(), Hd.begin(), Hd.end());
+        if (ps) R.insert(R.begin(), Sps.begin(), Sps.end());
         const int nr_eng = num_robs + robs_off;
 
         // dump schedule (init_dump_periods)
@@ -546,17 +586,22 @@ int main(int argc, char **argv)
         cfg.d = d;
         cfg.n_traj = n;
         cfg.deep = deep;
-        cfg.num_branches = 2;
+        cfg.num_branches = nbr;
         cfg.num_diss = num_diss;
         cfg.num_robs = nr_eng;
         cfg.T = jcs     ? jcs_alpha
+                : ps    ? ps_alpha
                 : mbl   ? param(cp, "mbl_T")
                 : integ ? param(cp, "integrable_T")
                         : 2.0 * 3.1415926535897932384626433832795 / omega;
-        // JCS: branch b's head is jcs_drv_part_b * alpha and the branch lasts half of it
-        // (init_split_structure_jcs, core.cpp:10086-10124)
-        const double jcs_len[2] = {0.5 * (jcs_p1 * jcs_alpha), 0.5 * (jcs_p2 * jcs_alpha)};
-        cfg.branch_len = jcs ? jcs_len : nullptr;
+        // JCS: part b's head is jcs_drv_part_b * alpha, run as two halves (init_split_structure_jcs,
+        // core.cpp:10086-10157)
+        const double jcs_len[4] = {0.5 * (jcs_p1 * jcs_alpha), 0.5 * (jcs_p1 * jcs_alpha), 0.5 * (jcs_p2 * jcs_alpha),
+                                   0.5 * (jcs_p2 * jcs_alpha)};
+        // PS: part b (head part_b alpha) as two halves (init_split_structure_ps, core.cpp:10234-10305)
+        const double ps_len[4] = {0.5 * (ps_p1 * ps_alpha), 0.5 * (ps_p1 * ps_alpha), 0.5 * (ps_p2 * ps_alpha),
+                                  0.5 * (ps_p2 * ps_alpha)};
+        cfg.branch_len = jcs ? jcs_len : ps ? ps_len : nullptr;
         cfg.record = jump;
         cfg.rng_kind = int(param_or(cp, "rng_kind", 0));
         cfg.seed = (uint64_t)(uint32_t)cp.seed;
@@ -712,11 +757,21 @@ int main(int argc, char **argv)
         // (get_num_photons_jcs, experiment.cpp:2080-2160) from the energy slot
         // MBL: spec = <H> / W (get_spec_mbl, experiment.cpp:1705-1751), imbalance from the adr rows
         // (get_imbalance_mbl, experiment.cpp:1753-1800)
-        std::vector<std::complex<double>> spec((jcs || mbl || integ) ? nd_ : 0);
-        const double spec_div = jcs ? jcs_alpha : mbl ? mbl_W : 1.0;  // get_spec_integrable: no division
+        std::vector<std::complex<double>> spec((jcs || mbl || integ || ps) ? nd_ : 0);
+        // get_spec_integrable: no division; get_spec_ps (experiment.cpp:1568-1614): / alpha
+        const double spec_div = jcs ? jcs_alpha : mbl ? mbl_W : ps ? ps_alpha : 1.0;
         for (size_t i = 0; i < spec.size(); i++) {
             const std::complex<double> a = D.robs[i * nr_eng];
             spec[i] = std::complex<double>(a.real() / spec_div, a.imag() / spec_div);
+        }
+        // PS: spec_2 = <J_z>, spec_3 = <J_+>, mean = Re <a^+ a> (get_spec_2_ps, get_spec_3_ps,
+        // get_num_photons_ps, experiment.cpp:1616-1708, 2170-2216) from slots 1, 2, 3
+        std::vector<std::complex<double>> spec2(ps ? nd_ : 0), spec3(ps ? nd_ : 0);
+        std::vector<double> ps_mean(ps ? nd_ : 0);
+        for (size_t i = 0; i < spec2.size(); i++) {
+            spec2[i] = D.robs[i * nr_eng + 1];
+            spec3[i] = D.robs[i * nr_eng + 2];
+            ps_mean[i] = D.robs[i * nr_eng + 3].real();
         }
         std::vector<double> imbalance(mbl ? nd_ : 0);
         if (mbl) {
@@ -728,6 +783,14 @@ int main(int argc, char **argv)
         std::vector<double> mean_start(n);
         check(qjx_get_mean_start(h, mean_start.data()), h, "qjx_get_mean_start");
 
+        if (ps && dump_obs == 1) {  // PSCoreBehaviour::dump_std (core.cpp:3958-3995)
+            const size_t o = (size_t)last_dump * n;
+            save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
+            save_complex_data(path + "spec" + sfx, reinterpret_cast<const double *>(spec.data() + o), n, 16, false);
+            save_complex_data(path + "spec_2" + sfx, reinterpret_cast<const double *>(spec2.data() + o), n, 16, false);
+            save_complex_data(path + "spec_3" + sfx, reinterpret_cast<const double *>(spec3.data() + o), n, 16, false);
+            save_double_data(path + "mean" + sfx, ps_mean.data() + o, n, 16, false);
+        }
         if (mbl && dump_obs == 1) {  // MBLCoreBehaviour::dump_std (core.cpp:4910-4937)
             const size_t o = (size_t)last_dump * n;
             save_double_data(path + "norm" + sfx, D.norm.data() + o, n, 16, false);
@@ -762,12 +825,20 @@ int main(int argc, char **argv)
                 save_2d_inv_double_data(path + name + sfx, inv.data(), ndt, n, 16, false);
             };
             evo(D.norm, "norm_evo");
-            if (jcs || mbl || integ) {  // JCS / MBL / Integrable dump_std_evo (core.cpp:3034-3102, 4988-5056, 6755-6819)
-                std::vector<std::complex<double>> cinv((size_t)ndt * n);
-                for (int dmp = 0; dmp < nrec; dmp++)
-                    for (int tr = 0; tr < n; tr++) cinv[(size_t)tr * ndt + dmp] = spec[(size_t)dmp * n + tr];
-                save_2d_inv_complex_data(path + "spec_evo" + sfx, reinterpret_cast<const double *>(cinv.data()), ndt, n,
-                                         16, false);
+            if (jcs || mbl || integ || ps) {  // dump_std_evo (core.cpp:3034-3102, 4052-4130, 4988-5056, 6755-6819)
+                auto cevo = [&](const std::vector<std::complex<double>> &v, const char *name) {
+                    std::vector<std::complex<double>> cinv((size_t)ndt * n);
+                    for (int dmp = 0; dmp < nrec; dmp++)
+                        for (int tr = 0; tr < n; tr++) cinv[(size_t)tr * ndt + dmp] = v[(size_t)dmp * n + tr];
+                    save_2d_inv_complex_data(path + name + sfx, reinterpret_cast<const double *>(cinv.data()), ndt, n,
+                                             16, false);
+                };
+                cevo(spec, "spec_evo");
+                if (ps) {
+                    cevo(spec2, "spec_2_evo");
+                    cevo(spec3, "spec_3_evo");
+                    evo(ps_mean, "mean_evo");
+                }
                 if (jcs) evo(D.energy, "mean_evo");
                 else if (mbl) evo(imbalance, "imbalance_evo");
             } else {

@@ -641,3 +641,122 @@ extern "C" qjx_status qjx_build_integrable(int N, int seed, int num_seeds, doubl
     }
     return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
 }
+
+// -------------------------------------------------------------------------------------------- PS
+// PSNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp:132-181, 650-866, 1582-1697, 2603-2749): ns spins
+// (spin 0 the most significant bit of the spin index x) times nps photon states; basis index
+// x nps + k (Kronecker order spins (x) photons); J = sum of sigma / 2 over the spins.
+extern "C" qjx_status qjx_build_ps(int ns, int nps, double alpha, double dprm, double gprm, double drv_ampl,
+                                   int diss_type, double diss_w, double part_1, double part_2, int deep, double *H,
+                                   double *Hd, double *L, double *S, double *Kout, double *Utree)
+{
+    if (ns < 1 || ns > 8 || nps < 2 || (diss_type != 0 && diss_type != 1) || !(alpha > 0.0)) return QJX_ERR_INVALID_ARG;
+    const int n2 = 1 << ns, d = n2 * nps, nd = diss_type == 0 ? 1 : 1 + ns;
+    if (d > 4096) return QJX_ERR_INVALID_ARG;
+    if (Utree && (deep < 1 || !(part_1 > 0.0) || !(part_2 > 0.0))) return QJX_ERR_INVALID_ARG;
+    const size_t dd = (size_t)d * d, e2 = 2 * dd, pp = (size_t)nps * nps, ss = (size_t)n2 * n2;
+    std::vector<double> a(pp, 0.0), ad(pp, 0.0), m1, m2, m3, nop;
+    for (int k = 0; k < nps - 1; k++) {
+        a[(size_t)k * nps + (k + 1)] = std::sqrt(double(k + 1));
+        ad[(size_t)(k + 1) * nps + k] = std::sqrt(double(k + 1));
+    }
+    real_matmul(nps, ad, ad, m1);
+    real_matmul(nps, m1, a, m2);
+    real_matmul(nps, m2, a, m3);   // a^+ a^+ a a
+    real_matmul(nps, ad, a, nop);  // a^+ a (special_4)
+    const double hs = 0.5 / std::pow(alpha, 3);
+    // J_z, J_-, J_+ from sigma_z = diag(1, -1), sigma_- = |1><0|, sigma_+ = |0><1| (:700-800)
+    std::vector<double> jz(ss, 0.0), jm(ss, 0.0), jp(ss, 0.0);
+    for (int sp = 0; sp < ns; sp++)
+        for (int x = 0; x < n2; x++) {
+            const int bit = 1 << (ns - 1 - sp);
+            const bool b = (x & bit) != 0;
+            jz[(size_t)x * n2 + x] += b ? -1.0 : 1.0;
+            if (!b) jm[(size_t)(x | bit) * n2 + x] += 1.0;
+            else jp[(size_t)(x & ~bit) * n2 + x] += 1.0;
+        }
+    for (size_t e = 0; e < ss; e++) {
+        jz[e] *= 0.5;
+        jm[e] *= 0.5;
+        jp[e] *= 0.5;
+    }
+    const double sd = dprm * 0.5, sg = gprm * 0.5;
+    cvec h(e2, 0.0), hd(e2, 0.0), l(e2 * nd, 0.0), sp4(4 * e2, 0.0);
+    for (int xi = 0; xi < n2; xi++)
+        for (int xj = 0; xj < n2; xj++)
+            for (int ki = 0; ki < nps; ki++)
+                for (int kj = 0; kj < nps; kj++) {
+                    const size_t e = ((size_t)xi * nps + ki) * d + (size_t)xj * nps + kj;
+                    const double id_s = xi == xj ? 1.0 : 0.0, id_p = ki == kj ? 1.0 : 0.0;
+                    const size_t pe = (size_t)ki * nps + kj, se = (size_t)xi * n2 + xj;
+                    // H = (d/2) J_z (x) 1 + (g/2)(a^+ J_- + J_+ a) + 1 (x) H_photon (:826-833)
+                    h[2 * e] = ((sd * jz[se]) * id_p + sg * (ad[pe] * jm[se] + jp[se] * a[pe])) + id_s * (hs * m3[pe]);
+                    hd[2 * e] = id_s * (ad[pe] - a[pe]);
+                    sp4[2 * e] = id_s * a[pe];
+                    sp4[2 * (dd + e)] = jz[se] * id_p;
+                    sp4[2 * (2 * dd + e)] = jp[se] * id_p;
+                    sp4[2 * (3 * dd + e)] = id_s * nop[pe];
+                    l[2 * e] = id_s * a[pe];  // the cavity dissipator 1 (x) a (:1622-1631)
+                }
+    if (diss_type == 1)  // spin decay sigma_-^(s) (x) 1 (:1633-1695)
+        for (int sp = 0; sp < ns; sp++) {
+            double *lc = l.data() + e2 * (1 + sp);
+            const int bit = 1 << (ns - 1 - sp);
+            for (int x = 0; x < n2; x++)
+                if (!(x & bit))
+                    for (int k = 0; k < nps; k++) lc[2 * (((size_t)(x | bit) * nps + k) * d + (size_t)x * nps + k)] = 1.0;
+        }
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (Hd) std::memcpy(Hd, hd.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), e2 * nd * sizeof(double));
+    if (S) std::memcpy(S, sp4.data(), 4 * e2 * sizeof(double));
+    if (!Kout && !Utree) return QJX_OK;
+    // init_hamiltonians_qj (:2603-2749): gamma 1/(4 alpha) on the cavity, diss_w on the spins;
+    // K_0 = -i H_eff + E0 H_drv (the kick), K_1 = -i H_eff
+    cvec hp(e2, 0.0);
+    for (size_t e = 0; e < dd; e++) hp[2 * e] = h[2 * e];
+    for (int c = 0; c < nd; c++) {
+        const double *lc = l.data() + e2 * c;
+        const double gamma = c == 0 ? 1.0 / (4.0 * alpha) : diss_w;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int q = 0; q < d; q++) {
+                    const double ar = lc[2 * ((size_t)q * d + i)], ai = lc[2 * ((size_t)q * d + i) + 1];
+                    const double br = lc[2 * ((size_t)q * d + j)], bi = lc[2 * ((size_t)q * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (gamma * si);
+                hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    cvec K[2] = {cvec(e2), cvec(e2)};
+    const double Eb[2] = {drv_ampl, 0.0};
+    for (size_t e = 0; e < dd; e++)
+        for (int b = 0; b < 2; b++) {
+            K[b][2 * e] = 0.0 + (hp[2 * e + 1] + Eb[b] * hd[2 * e]);
+            K[b][2 * e + 1] = 0.0 - (hp[2 * e] + Eb[b] * 0.0);
+        }
+    if (Kout) {
+        std::memcpy(Kout, K[0].data(), e2 * sizeof(double));
+        std::memcpy(Kout + e2, K[1].data(), e2 * sizeof(double));
+    }
+    if (!Utree) return QJX_OK;
+    // init_split_structure_ps (core.cpp:10234-10305): part b's head lasts part_b alpha and runs two
+    // children of its tree, each half of it
+    const double head[2] = {part_1 * alpha, part_2 * alpha};
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) collapse(2) reduction(&& : ok)
+    for (int b = 0; b < 2; b++)
+        for (int lv = 0; lv < deep; lv++) {
+            double dt = head[b] * 0.5;
+            for (int q = 0; q <= lv; q++) dt *= 0.5;
+            cvec scaled(e2);
+            for (size_t e = 0; e < e2; e++) scaled[e] = K[b][e] * dt;
+            ok = expm(d, scaled.data(), Utree + e2 * ((size_t)b * deep + lv)) && ok;
+        }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

@@ -62,6 +62,15 @@ def suffix(cfg, prm):
     JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
     for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 2:  # PSOutputBehavior::suffix_param (outputter.cpp:135-174)
+        return ("_setup(%d_%d_%d)" % (2, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_s(%d)_nps(%d)" % (int(prm["ps_num_spins"]), int(prm["ps_num_photons_states"]))
+                + "_diss(%d_%s)" % (int(prm["diss_type"]), f4(prm["ps_diss_w"]))
+                + "_drv(%s_%s_%s)" % (f4(prm["ps_drv_part_1"]), f4(prm["ps_drv_part_2"]), f4(prm["ps_drv_ampl"]))
+                + "_prm(%s_%s_%s)" % (f4(prm["ps_prm_alpha"]), f4(prm["ps_prm_d"]), f4(prm["ps_prm_g"]))
+                + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"]))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 5:  # IntegrableOutputBehavior::suffix_param (outputter.cpp:244-269)
         return ("_setup(%d_%d_%d)" % (5, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -118,13 +127,16 @@ def expected_outputs(cfg, prm, R=None):
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
     integ = cfg.get("sys_id", 0) == 5
-    N = 0 if (mbl or integ) else int(prm["N"])
+    ps = cfg.get("sys_id", 0) == 2
+    N = 0 if (mbl or integ or ps) else int(prm["N"])
     d = N if jcs else N + 1
     if mbl:
         Nc = int(prm["mbl_Nc"])
         d = len(O.mbl_basis(Nc))
     if integ:
         d = 1 << int(prm["integrable_N"])
+    if ps:
+        d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"])
     n = cfg["num_trajectories"]
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
@@ -137,12 +149,26 @@ def expected_outputs(cfg, prm, R=None):
         alpha = prm["jcs_prm_alpha"]
         H, Hd, L, Nop, K0, K1 = O.jcs_operators(N, alpha, prm["jcs_drv_ampl"])
         heads = [prm["jcs_drv_part_1"] * alpha, prm["jcs_drv_part_2"] * alpha]
-        U = np.stack([O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)])
+        # each part runs as the head's two children (init_split_structure_jcs, core.cpp:10086-10157)
+        U0, U1 = O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)
+        U = np.stack([U0, U0, U1, U1])
         HE = Nop
         Rs = np.concatenate([L[None], R]) if nr else L[None]
         T = t_head = alpha
         ens = O.Ensemble(U, L, [1.0], HE, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
-                         branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+                         branch_len=[0.5 * heads[0], 0.5 * heads[0], 0.5 * heads[1], 0.5 * heads[1]])
+    elif ps:  # PS: like JCS with spins; spec, spec_2, spec_3, photons ride in observable slots 0..3
+        alpha = prm["ps_prm_alpha"]
+        H, Hd, L, S4, K0, K1 = O.ps_operators(int(prm["ps_num_spins"]), int(prm["ps_num_photons_states"]), alpha,
+                                              prm["ps_prm_d"], prm["ps_prm_g"], prm["ps_drv_ampl"],
+                                              int(prm["diss_type"]), prm["ps_diss_w"])
+        heads = [prm["ps_drv_part_1"] * alpha, prm["ps_drv_part_2"] * alpha]
+        U0, U1 = O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)
+        U = np.stack([U0, U0, U1, U1])
+        Rs = np.concatenate([S4, R]) if nr else S4
+        T = alpha
+        ens = O.Ensemble(U, L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
+                         branch_len=[0.5 * heads[0], 0.5 * heads[0], 0.5 * heads[1], 0.5 * heads[1]])
     elif integ:  # Integrable: H = 0, one head of duration integrable_T, two children; spec = <special>
         Ls, S, K = integrable_model(prm)
         T = prm["integrable_T"]
@@ -205,12 +231,18 @@ def expected_outputs(cfg, prm, R=None):
         files[path + "exp_mtx_0" + sfx] = f_complex_data(Ut[-1].reshape(-1))
     elif cfg.get("is_debug", 0):
         files[path + "hamiltonian" + sfx] = f_complex_data(H.reshape(-1))
-        files[path + "dissipator_0" + sfx] = f_complex_data(L.reshape(-1))
+        for c, Lc in enumerate(L.reshape(-1, d, d)):
+            files[path + "dissipator_%d" % c + sfx] = f_complex_data(Lc.reshape(-1))
         files[path + "hamiltonians_qj_0" + sfx] = f_complex_data(K0.reshape(-1))
         files[path + "hamiltonians_qj_1" + sfx] = f_complex_data(K1.reshape(-1))
-        if cfg.get("prop_id", 0) == 0:
+        if cfg.get("prop_id", 0) == 0:  # JCS / PS: part 1's tree is engine branch 2
             files[path + "exp_mtx_0" + sfx] = f_complex_data(U[0, -1].reshape(-1))
-            files[path + "exp_mtx_1" + sfx] = f_complex_data(U[1, -1].reshape(-1))
+            files[path + "exp_mtx_1" + sfx] = f_complex_data(U[2 if (jcs or ps) else 1, -1].reshape(-1))
+        if jcs:  # JCSDebugBehaviour::save (debugger.cpp:13-26): special = a
+            files[path + "spec_mtx" + sfx] = f_complex_data(L.reshape(-1))
+        if ps:  # PSDebugBehaviour::save (debugger.cpp:28-53)
+            for o, name in enumerate(("spec_mtx", "spec_2_mtx", "spec_3_mtx", "spec_4_mtx")):
+                files[path + name + sfx] = f_complex_data(S4[o].reshape(-1))
     if deep_task:
         dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(2 * nsub)]
     else:
@@ -299,10 +331,22 @@ def expected_outputs(cfg, prm, R=None):
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("spec" + sfx, f_complex_data(last["spec"]), False)
         emit("imbalance" + sfx, f_double_data(last["imbalance"]), False)
+    if ps:  # get_spec_ps (/ alpha), get_spec_2_ps, get_spec_3_ps, get_num_photons_ps (experiment.cpp:1568-1708, 2170)
+        for o in obs:
+            z = o["random_obs"]
+            o["spec"] = z[:, 0].real / alpha + 1j * (z[:, 0].imag / alpha)
+            o["spec_2"], o["spec_3"], o["mean"] = z[:, 1], z[:, 2], z[:, 3].real.copy()
+            o["random_obs"] = z[:, 4:]
+    if ps and int(prm["dump_obs"]) == 1:  # PSCoreBehaviour::dump_std (core.cpp:3958-3995)
+        emit("norm" + sfx, f_double_data(last["norm"]), False)
+        emit("spec" + sfx, f_complex_data(last["spec"]), False)
+        emit("spec_2" + sfx, f_complex_data(last["spec_2"]), False)
+        emit("spec_3" + sfx, f_complex_data(last["spec_3"]), False)
+        emit("mean" + sfx, f_double_data(last["mean"]), False)
     if (jcs or integ) and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("spec" + sfx, f_complex_data(last["spec"]), False)
-    if not jcs and not mbl and not integ and int(prm["dump_obs"]) == 1:
+    if not jcs and not mbl and not integ and not ps and int(prm["dump_obs"]) == 1:
         emit("norm" + sfx, f_double_data(last["norm"]), False)
         emit("mean_start" + sfx, f_double_data(ens.mean_start), False)
         emit("mean" + sfx, f_double_data(last["mean"]), False)
@@ -320,6 +364,7 @@ def expected_outputs(cfg, prm, R=None):
         keys = ((("norm", "norm_evo"), ("energy", "mean_evo")) if jcs else
                 (("norm", "norm_evo"), ("imbalance", "imbalance_evo")) if mbl else
                 (("norm", "norm_evo"),) if integ else
+                (("norm", "norm_evo"), ("mean", "mean_evo")) if ps else
                 (("norm", "norm_evo"), ("mean", "mean_evo"), ("dispersion", "dispersion_evo"), ("m2", "m2_evo"),
                  ("energy", "energy_evo")))
         for key, name in keys:
@@ -327,12 +372,9 @@ def expected_outputs(cfg, prm, R=None):
             for i, o in enumerate(obs):
                 grid[i] = o[key]
             emit(name + sfx, f_2d_inv(grid), False)
-        if jcs or mbl or integ:
-            grid = np.zeros((ndt, n), complex)
-            for i, o in enumerate(obs):
-                grid[i] = o["spec"]
-            emit("spec_evo" + sfx, "".join("".join(fmt_double(z.real) + " " + fmt_double(z.imag) + " " for z in row)
-                                           + "\n" for row in grid), False)
+        if jcs or mbl or integ or ps:
+            for key in (("spec", "spec_2", "spec_3") if ps else ("spec",)):
+                emit(key + "_evo" + sfx, f_2d_inv_complex(np.array([o[key] for o in obs])), False)
         for o_id in range(nr):
             rows = [o["random_obs"][:, o_id] for o in obs]
             emit("random_obs_evo_%d" % (int(prm["random_obs_seed"]) + o_id) + sfx, f_2d_complex(rows), False)
@@ -378,12 +420,13 @@ def expected_lpn_outputs(cfg, prm, R=None):
         alpha = W
         H, Hd, L, Nop, K0, K1 = O.jcs_operators(N, alpha, prm["jcs_drv_ampl"])
         heads = [prm["jcs_drv_part_1"] * alpha, prm["jcs_drv_part_2"] * alpha]
-        U = np.stack([O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)])
+        U0, U1 = O.split_tree(K0, heads[0], deep), O.split_tree(K1, heads[1], deep)
+        U = np.stack([U0, U0, U1, U1])
         Rs = np.concatenate([L[None], R]) if nr else L[None]
         T = alpha
         calc_T = heads[0] + heads[1]  # JCSCoreBehaviour::calc_T (core.cpp:2833-2845)
         ens = O.Ensemble(U, L, [1.0], Nop, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
-                         branch_len=[0.5 * heads[0], 0.5 * heads[1]])
+                         branch_len=[0.5 * heads[0], 0.5 * heads[0], 0.5 * heads[1], 0.5 * heads[1]])
     elif integ:
         L, S, K = integrable_model(prm)
         T = calc_T = prm["integrable_T"]
@@ -573,6 +616,10 @@ def expected_lpn_outputs(cfg, prm, R=None):
 
 
 JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_1": 0.5, "jcs_drv_part_2": 1.5}
+
+# submit_ps.py's system (1 spin, alpha 5, parts 1 / 1 (x T), diss_w 0.05; 300 photon states there, 24 here)
+PS_PARAMS = {"ps_num_spins": 1, "ps_num_photons_states": 24, "ps_prm_alpha": 5.0, "ps_prm_d": 1.0, "ps_prm_g": 0.5,
+             "ps_drv_ampl": 3.2, "ps_drv_part_1": 0.5, "ps_drv_part_2": 1.5, "ps_diss_w": 0.05, "diss_type": 1}
 
 # submit_integrable.py's system (tau 1, k -1, integrable_N 7 there; 6 spins here), one disorder seed
 INTEGRABLE_PARAMS = {"integrable_N": 6, "integrable_seed": 2, "integrable_num_seeds": 1000000, "integrable_tau": 1.0,

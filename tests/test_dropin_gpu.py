@@ -9,7 +9,7 @@ import pytest
 
 import os_d_b200 as q
 from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS,
-                                 config_text, expected_outputs, params_text)
+                                 PS_PARAMS, config_text, expected_outputs, params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -26,6 +26,7 @@ def run_case(tmp_path, cfg, prm):
     d = int(prm["N"]) if cfg.get("sys_id", 0) == 1 else d
     d = math.comb(int(prm["mbl_Nc"]), int(prm["mbl_Nc"]) // 2) if cfg.get("sys_id", 0) == 3 else d
     d = 1 << int(prm["integrable_N"]) if cfg.get("sys_id", 0) == 5 else d
+    d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"]) if cfg.get("sys_id", 0) == 2 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -153,6 +154,18 @@ def test_jcs_lpn_mult_files_match(tmp_path, lpn_type):
     k = [k for k in exp if k.startswith("num_renorms")][0]
     assert sum(int(x) for x in exp[k].split()) > 0
     assert any(k.startswith("mean_lpn_evo") for k in exp) and any(k.startswith("spec_lpn_evo") for k in exp)
+
+
+@pytest.mark.parametrize("diss_type,spins", [(1, 1), (0, 2)])
+def test_ps_system_files_match(tmp_path, diss_type, spins):
+    """The PS system (sys_id 2): spins x photons, kick and free evolution each run as two halves,
+    spec = <a> / alpha, spec_2 = <J_z>, spec_3 = <J_+>, mean = <a^+ a> (newdel.cpp:132-181, 650-866,
+    1582-1697, 2603-2749; core.cpp:3245-4130, 10234-10305)."""
+    cfg = dict(BASE_CONFIG, sys_id=2, num_trajectories=16, num_tp_periods=1, num_obs_periods=4, is_debug=1)
+    prm = {**BASE_PARAMS, **PS_PARAMS, "diss_type": diss_type, "ps_num_spins": spins, "dump_num": 2, "jump": 2,
+           "dump_adr_sep": 1, "dump_adr_avg": 1}
+    exp = run_case(tmp_path, cfg, prm)
+    assert any(k.startswith("spec_3_evo") for k in exp)
 
 
 def test_integrable_system_files_match(tmp_path):

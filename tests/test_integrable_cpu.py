@@ -77,3 +77,36 @@ def test_bad_sizes_rejected():
 
     assert N.lib().qjx_build_integrable(2, 1, 1, 1.0, 1.0, 1.0, 4, None, None, None, None) == 1
     assert N.lib().qjx_build_integrable(11, 1, 1, 1.0, 1.0, 1.0, 4, None, None, None, None) == 1
+
+
+def test_ps_product_builder_equals_oracle():
+    """PS (sys_id 2): qjx_build_ps against orc_ps_operators bit for bit, and the oracle against a
+    numpy Kronecker restatement of PSNewDelBehaviour (newdel.cpp:650-866, 1582-1697, 2603-2749)."""
+    import os_d_b200 as q
+
+    ns, nps, al, dp, gp, A, w = 2, 6, 5.0, 1.3, 0.7, 3.2, 0.05
+    H, Hd, L, S, K0, K1 = O.ps_operators(ns, nps, al, dp, gp, A, 1, w)
+    H2, Hd2, L2, S2, Ut = q.build_ps(ns, nps, al, dp, gp, A, 1, w, 0.5, 1.5, 8)
+    assert all(np.array_equal(x, y) for x, y in ((H, H2), (Hd, Hd2), (L, L2), (S, S2)))
+    assert np.array_equal(Ut[0], O.split_tree(K0, 0.5 * al, 8)) and np.array_equal(Ut[1], O.split_tree(K1, 1.5 * al, 8))
+    a = np.diag(np.sqrt(np.arange(1, nps)), 1)
+    sz, sm, sp, I2 = np.diag([1.0, -1.0]), np.array([[0, 0], [1, 0.0]]), np.array([[0, 1], [0, 0.0]]), np.eye(2)
+
+    def spin_op(sig, s):
+        m = sig if s == 0 else I2
+        for it in range(1, ns):
+            m = np.kron(m, sig if it == s else I2)
+        return m
+
+    Jz, Jm, Jp = (0.5 * sum(spin_op(sig, s) for s in range(ns)) for sig in (sz, sm, sp))
+    Is, Ip = np.eye(1 << ns), np.eye(nps)
+    Hn = (np.kron(dp * 0.5 * Jz, Ip) + gp * 0.5 * (np.kron(Is, a.T) @ np.kron(Jm, Ip) + np.kron(Jp, Ip) @ np.kron(Is, a))
+          + np.kron(Is, 0.5 / al ** 3 * a.T @ a.T @ a @ a))
+    assert np.allclose(H, Hn, rtol=0, atol=1e-15)
+    Ls = [np.kron(Is, a)] + [np.kron(spin_op(sm, s), Ip) for s in range(ns)]
+    assert np.array_equal(L, np.array(Ls, complex))
+    for got, want in zip(S, (np.kron(Is, a), np.kron(Jz, Ip), np.kron(Jp, Ip), np.kron(Is, a.T @ a))):
+        assert np.array_equal(got, want.astype(complex))
+    He = Hn - 0.5j * sum(g * Lc.T @ Lc for g, Lc in zip([1 / (4 * al)] + [w] * ns, Ls))
+    assert np.allclose(K0, -1j * He + A * np.kron(Is, a.T - a), atol=1e-14)
+    assert np.allclose(K1, -1j * He, atol=1e-14)
