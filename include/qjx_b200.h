@@ -166,6 +166,12 @@ qjx_status qjx_init_thresholds(qjx_engine *h);
 qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, const int *dump_at, int n_dumps,
                            int dump_base);
 qjx_status qjx_reset_times(qjx_engine *h);
+/* Deep tasks (deep_num_steps > 0, QJ propagator): continue every active trajectory for n_sub
+ * sub-periods from where the previous call left it, the observables after each sub-period going to
+ * dump slots dump_base, dump_base + 1, ... (LpnMultDeep runs the Lyapunov update between
+ * sub-periods: ex_period_obs_deep_mult_lpn, core.cpp:155-241).  Periods carry over between calls;
+ * qjx_run_periods always starts a new period. */
+qjx_status qjx_run_sub_periods(qjx_engine *h, int n_sub, int dump_base);
 /* Observables of the current states into dump slot `dump`; is_start writes mean_start. */
 qjx_status qjx_observe(qjx_engine *h, int dump, int is_start);
 /* Per-dump arrays laid out [dump][trajectory]; robs [dump][trajectory][num_robs] complex;
@@ -231,6 +237,10 @@ qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *cfg);
  * adr_dump >= 0: this period carried dump slot adr_dump, whose |psi_i|^2/|psi|^2 of the variations
  * is replaced by the value after the update (abs_diag_rho_all after lambda_lpn); -1 otherwise. */
 qjx_status qjx_lpn_period(qjx_engine *h, double curr_time, int adr_dump);
+/* LpnMultDeep (task_id 8): calc_chars_lpn of the bases only, for the sub-periods at which the
+ * variations take no Lyapunov step (lambda_per_periods 1: ex_period_obs_deep_mult_lpn,
+ * core.cpp:155-241, updates them at the last sub-period of a period only). */
+qjx_status qjx_lpn_bases(qjx_engine *h);
 /* Current Lyapunov values per trajectory [n_traj] (robs_lpn [n_traj][num_robs] complex); any
  * pointer may be NULL.  lambda_now is what lambda / lambda_evo dump (core.cpp:959-1000). */
 qjx_status qjx_lpn_get(qjx_engine *h, double *lambda_now, double *lambda, double *delta_s, double *mean_lpn,

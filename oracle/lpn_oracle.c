@@ -363,6 +363,38 @@ int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg,
     return bad;
 }
 
+/* LpnMultDeep sub-periods without a Lyapunov step: calc_chars_lpn of the bases only
+ * (ex_period_obs_deep_mult_lpn, core.cpp:155-241). */
+int orc_lpn_bases(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg, orc_lpn *lp)
+{
+    const int d = p->d, n = p->n_traj, half = n / 2;
+    if (!lpn_type_ok(p, cfg) || p->num_robs > 64 || (n & 1)) return 2;
+    const int full = CH_MEAN | CH_ENERGY | CH_ROBS_ALL;
+    int *words = lpn_words(cfg);
+    if (cfg->mbl_Nc > 0 && !words) return 1;
+    int bad = 0;
+#pragma omp parallel
+    {
+        double *xh = (double *)malloc(sizeof(double) * 2 * d);
+        double *sm = (double *)malloc(sizeof(double) * 2 * d);
+        if (!xh || !sm) {
+#pragma omp atomic write
+            bad = 1;
+        } else {
+#pragma omp for schedule(dynamic, 1)
+            for (int b = 0; b < half; b++) {
+                chars_t bc;
+                lpn_chars(p, s->phi + 2 * (size_t)b * d, full, -1, xh, sm, &bc, cfg->mbl_Nc, words);
+                store_chars(p, cfg, lp, b, &bc);
+            }
+        }
+        free(xh);
+        free(sm);
+    }
+    free(words);
+    return bad;
+}
+
 int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg, orc_lpn *lp, double curr_time)
 {
     const int d = p->d, n = p->n_traj, half = n / 2;

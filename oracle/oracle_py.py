@@ -84,6 +84,8 @@ def lib():
                                     C.POINTER(OrcLpn)]
         L.orc_lpn_period.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.POINTER(OrcLpnConfig),
                                      C.POINTER(OrcLpn), C.c_double]
+        L.orc_lpn_bases.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcState), C.POINTER(OrcLpnConfig),
+                                    C.POINTER(OrcLpn)]
         L.orc_lpn_exp10.argtypes = [C.c_double]
         L.orc_lpn_exp10.restype = C.c_double
         L.orc_lpn_log.argtypes = [C.c_double]
@@ -372,6 +374,10 @@ class Lpn:
     def period(self, curr_time):
         st = lib().orc_lpn_period(C.byref(self.ens.p), C.byref(self.ens.s), C.byref(self.cfg), C.byref(self.s),
                                   float(curr_time))
+        assert st == 0, st
+
+    def bases(self):
+        st = lib().orc_lpn_bases(C.byref(self.ens.p), C.byref(self.ens.s), C.byref(self.cfg), C.byref(self.s))
         assert st == 0, st
 
     def values(self):

@@ -224,6 +224,8 @@ int orc_lpn_start(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg,
 /* After one observation period: calc_chars_lpn of the bases and lambda_lpn (per_period 0) or
  * lambda_lpn_now (1) of the variations, curr_time = (period_id + 1) T. */
 int orc_lpn_period(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg, orc_lpn *lp, double curr_time);
+/* calc_chars_lpn of the bases only (LpnMultDeep sub-periods without a Lyapunov step). */
+int orc_lpn_bases(const orc_problem *p, orc_state *s, const orc_lpn_config *cfg, orc_lpn *lp);
 /* pow(10, x) and log(x) of the Lyapunov task, shared operation for operation with the engine. */
 double orc_lpn_exp10(double x);
 double orc_lpn_log(double x);

@@ -22,7 +22,7 @@ EXPORTS = [
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
     "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_build_ps", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
-    "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_get",
+    "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_bases", "qjx_run_sub_periods", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
 
@@ -105,6 +105,8 @@ def lib():
         L.qjx_slot_release.argtypes = [vp, C.c_int]
         L.qjx_lpn_start.argtypes = [vp, C.POINTER(QjxLpnConfig)]
         L.qjx_lpn_period.argtypes = [vp, C.c_double, C.c_int]
+        L.qjx_lpn_bases.argtypes = [vp]
+        L.qjx_run_sub_periods.argtypes = [vp, C.c_int, C.c_int]
         L.qjx_lpn_get.argtypes = [vp] + [c_double_p] * 6 + [c_int_p]
         L.qjx_lpn_get_last.argtypes = [vp, c_int_p, c_double_p, c_double_p, c_double_p, c_int_p, c_double_p]
         L.qjx_get_trace.argtypes = [vp, c_i64_p, c_int_p, c_int_p]

@@ -89,6 +89,7 @@ struct Params {
     // run
     int record;
     int target;
+    int sub_target;  // deep tasks, qjx_run_sub_periods: stop after this many sub-periods (0: off)
     const int *dump_at;
     int n_dumps;
     int dump_base;

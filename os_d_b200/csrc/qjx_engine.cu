@@ -905,6 +905,39 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
     return drain_records(h);
 }
 
+// Deep tasks: continue every trajectory for n_sub sub-periods from where it stands, with the
+// observables after each sub-period in dump slots dump_base, dump_base + 1, ... (the per-sub-period
+// loop of ex_period_obs_deep_mult_lpn, core.cpp:155-241, which runs the Lyapunov update between
+// sub-periods).  Periods continue across calls; a later qjx_run_periods starts a new period.
+extern "C" qjx_status qjx_run_sub_periods(qjx_engine *h, int n_sub, int dump_base)
+{
+    NvtxRange range("qjx_run_sub_periods");
+    if (!h || n_sub < 1 || dump_base < 0) return QJX_ERR_INVALID_ARG;
+    if (!h->states_set) return fail(h, QJX_ERR_STATE, "qjx_set_states first");
+    if (h->cfg.deep_num_steps < 1 || h->P.prop != 0)
+        return fail(h, QJX_ERR_INVALID_ARG, "sub-periods exist for the deep tasks with the QJ propagator only");
+    if ((long long)dump_base + n_sub > h->cfg.max_dumps)
+        return fail(h, QJX_ERR_INVALID_ARG, "every sub-period needs a dump slot below max_dumps");
+    CK(cudaSetDevice(h->cfg.device));
+    Params &P = h->P;
+    P.dump_at = h->d_dump_at;
+    P.n_dumps = 0;
+    P.dump_base = dump_base;
+    P.target = 0x7fffffff;  // periods do not end the call; sub_target does
+    P.sub_target = n_sub;
+    P.subdump = 1;
+    P.record = h->cfg.record > 0 ? 1 : 0;
+    CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
+    CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
+    P.period0 = h->period_base;
+    cudaError_t e = launch_schedule(P, 2, h->stream);
+    h->stats.launches += 1;
+    qjx_status st = e == cudaSuccess ? run_until_idle(h) : cuda_fail(h, e, "launch_schedule");
+    P.sub_target = 0;
+    if (st != QJX_OK) return st;
+    return drain_records(h);
+}
+
 extern "C" qjx_status qjx_observe(qjx_engine *h, int dump, int is_start)
 {
     NvtxRange range("qjx_observe");
@@ -1148,6 +1181,18 @@ extern "C" qjx_status qjx_lpn_start(qjx_engine *h, const qjx_lpn_config *c)
     h->stats.launches += 1;
     CK(cudaStreamSynchronize(h->stream));
     h->lpn_started = true;
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_lpn_bases(qjx_engine *h)
+{
+    NvtxRange range("qjx_lpn_bases");
+    if (!h) return QJX_ERR_INVALID_ARG;
+    if (!h->lpn_started) return fail(h, QJX_ERR_STATE, "qjx_lpn_start first");
+    CK(cudaSetDevice(h->cfg.device));
+    CK(launch_lpn(h->P, h->L, 2, 0.0, -1, h->stream));
+    h->stats.launches += 1;
+    CK(cudaStreamSynchronize(h->stream));
     return QJX_OK;
 }
 

@@ -219,7 +219,7 @@ __device__ int after_step(const Params &P, TrajState &s, int tr, const double2 *
 __device__ int finish_obs(const Params &P, TrajState &s)
 {
     s.di += 1;
-    if (s.pc >= P.target) {
+    if (s.pc >= P.target || (P.sub_target > 0 && s.di >= P.sub_target)) {
         s.phase = PH_DONE;
         return -1;
     }
@@ -946,7 +946,8 @@ __global__ void __launch_bounds__(1024) plan_kernel(const Params P)
 }
 
 // Bucket trajectories for step 0 of a call.  mode 0: start of a run of P.target periods;
-// mode 1: resume trajectories paused on a full record buffer.
+// mode 1: resume trajectories paused on a full record buffer; mode 2: continue a deep task from
+// where the previous call stopped (a sub-period boundary: branch, unit and period count kept).
 __global__ void schedule_kernel(const Params P, int mode)
 {
     const int tr = blockIdx.x * blockDim.x + threadIdx.x;
@@ -962,6 +963,10 @@ __global__ void schedule_kernel(const Params P, int mode)
         s.rk_sid = 0;
         s.paused = 0;
         s.phase = (P.target > 0 && runs(P, tr)) ? PH_STEP : PH_DONE;
+    } else if (mode == 2) {
+        s.di = 0;
+        s.paused = 0;
+        s.phase = (P.sub_target > 0 && runs(P, tr)) ? PH_STEP : PH_DONE;
     } else {
         if (!s.paused) return;
         s.paused = 0;

@@ -345,7 +345,8 @@ __device__ void store_chars(const Params &P, const LpnParams &L, int tr, const L
     for (int o = threadIdx.x; o < P.nr; o += blockDim.x) L.robs_lpn[(size_t)tr * P.nr + o] = c.robs[o];
 }
 
-// mode 0: start (after the bases' transient); mode 1: after one observation period at curr_time.
+// mode 0: start (after the bases' transient); mode 1: after one observation period at curr_time;
+// mode 2: the bases' characteristics only (LpnMultDeep sub-periods between Lyapunov updates).
 // adr_dump >= 0: the variations' |psi_i|^2 / |psi|^2 after the update go to that dump's adr slot.
 __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const LpnParams L, int mode,
                                                            double curr_time, int adr_dump)
@@ -380,6 +381,7 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(const Params P, const 
     const int full = CH_MEAN | CH_ENERGY | CH_ROBS_ALL;
     cta_chars(P, L, E, pb, full, -1, xh, y, sh, sh.bc, adr);  // calc_chars_lpn of the base
     store_chars(P, L, b, sh.bc);
+    if (mode == 2) return;
     bool moved = false;
     if (mode == 0) {
         // copy_trajectory_lpn + var_trajectory_lpn; calc_chars_lpn_start

@@ -69,9 +69,14 @@ void write_2d_inv(const std::string &fn, const std::vector<double> &v, int nrec,
 // / spec_div (alpha or W); the mean characteristics are <a^+ a> (JCS) or imbalances (MBL); each
 // system writes its own file set.  calc_T is the period of the Lyapunov time (calc_T: JCS
 // part_1 alpha + part_2 alpha, core.cpp:2833-2845).
+// LpnMultDeep (task_id 8, the dimer; nsub = deep_num_steps > 0): the same pairs advanced one
+// sub-period at a time (LpnMultDeepExperimentBehaviour::obser_process, experiment.cpp:302-350;
+// ex_period_obs_deep_mult_lpn, core.cpp:155-241): the Lyapunov step after every sub-period at
+// curr_time = dump_id / (2 nsub) T (lambda_per_periods 0) or at the last sub-period of each period
+// (lambda_per_periods 1; the bases' characteristics only in between), one dump per sub-period.
 void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, const qjx_config &cfg,
                   const std::vector<double> &H, int d, int num_robs, int robs_seed, int sys, int Nc, double spec_div,
-                  double calc_T)
+                  double calc_T, int nsub)
 {
     const bool mbl = sys == 3, jcs = sys == 1, integ = sys == 5, spec = mbl || jcs || integ;
     const double W = spec_div;
@@ -103,7 +108,15 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
         const double v = std::fabs(H[2 * ((size_t)st * d + st)]);
         if (v > lc.max_energy) lc.max_energy = v;
     }
-    const std::vector<int> dp = dump_periods(int(param(cp, "dump_type")), int(param(cp, "dump_num")), cp.num_obs_periods);
+    const int nss = 2 * nsub;  // sub-periods per period (num_ham_qj deep_num_steps)
+    std::vector<int> dp;
+    if (nsub > 0) {  // init_dump_periods_deep (newdel_exp.cpp:377-406)
+        dp.push_back(0);
+        for (int p = 0; p < cp.num_obs_periods; p++)
+            for (int k = 0; k < nss; k++) dp.push_back(p);
+    } else {
+        dp = dump_periods(int(param(cp, "dump_type")), int(param(cp, "dump_num")), cp.num_obs_periods);
+    }
     if (dp.empty()) die("Wrong dump_type");
     const int ndt = (int)dp.size();
 
@@ -194,9 +207,34 @@ void run_lpn_mult(qjx_engine *h, const RunParam &rp, const ConfigParam &cp, cons
     write_adr_single(0, false);
     if (dump_evo_avg == 1) write_adr_avg(0, n, false);
 
-    // obser_process: period by period (the Lyapunov update follows every period)
     std::vector<bool> zero_span(ndt, false);
-    for (int dump_id = 1; dump_id < ndt; dump_id++) {
+    if (nsub > 0) {  // LpnMultDeep obser_process: sub-period by sub-period
+        if (int(param(cp, "dump_phi_evo")) == 1) {  // dump_phi_evo(ad, false) (core.cpp:12591-12613)
+            std::vector<double> psi(2 * (size_t)n * d);
+            check(qjx_get_states(h, psi.data(), nullptr, nullptr, nullptr), h, "qjx_get_states");
+            for (int tr = 0; tr < n; tr++)
+                save_complex_data(path + "phi_evo_" + std::to_string(tr) + sfx, psi.data() + 2 * (size_t)tr * d, d, 16,
+                                  false);
+        }
+        for (int p = 0; p < cp.num_obs_periods; p++) {
+            if (rp.is_pp == 1) std::cout << "dump_id: " << p + 1 << std::endl;
+            for (int k = 0; k < nss; k++) {
+                const int dump_id = p * nss + k + 1;
+                check(qjx_run_sub_periods(h, 1, dump_id), h, "qjx_run_sub_periods");
+                if (lc.per_period == 0 || k == nss - 1) {
+                    check(qjx_lpn_period(h, double(dump_id) / double(nss) * calc_T, dump_id), h, "qjx_lpn_period");
+                    after_lpn(false);
+                } else {
+                    check(qjx_lpn_bases(h), h, "qjx_lpn_bases");
+                }
+                take_lpn();
+                write_adr_single(dump_id, true);
+            }
+            if (dump_evo_avg == 1) write_adr_avg((p + 1) * nss, half, true);
+        }
+    }
+    // obser_process: period by period (the Lyapunov update follows every period)
+    for (int dump_id = 1; dump_id < ndt && nsub == 0; dump_id++) {
         if (rp.is_pp == 1) std::cout << "dump_id: " << dump_id << std::endl;
         for (int period_id = dp[dump_id - 1]; period_id < dp[dump_id]; period_id++) {
             const bool at_dump = period_id + 1 == dp[dump_id];
@@ -397,10 +435,11 @@ int main(int argc, char **argv)
     if ((jcs || mbl || integ) && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
         die("Wrong task_id / prop_id for sys_id " + std::to_string(rp.sys_id) +
             " (this engine runs JCS, MBL and Integrable with the Std and LpnMult tasks and the QJ propagator)");
-    if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7)
+    if (rp.task_id != 1 && rp.task_id != 4 && rp.task_id != 7 && rp.task_id != 8)
         die("Wrong task_id: " + std::to_string(rp.task_id) +
             " (this engine runs the Std (1), StdDeep (4) and LpnMult (7) tasks)");
-    if (rp.task_id == 4 && rp.prop_id != 0) die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (StdDeep runs the QJ propagator)");
+    if ((rp.task_id == 4 || rp.task_id == 8) && rp.prop_id != 0)
+        die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (StdDeep and LpnMultDeep run the QJ propagator)");
     if (rp.prop_id != 0 && rp.prop_id != 1)
         die("Wrong prop_id: " + std::to_string(rp.prop_id) + " (this engine runs the QJ (0) and RK (1) propagators)");
 
@@ -472,7 +511,7 @@ int main(int argc, char **argv)
         const double ps_alpha = ps ? param(cp, "ps_prm_alpha") : 0.0;
         const double ps_p1 = ps ? param(cp, "ps_drv_part_1") : 0.0, ps_p2 = ps ? param(cp, "ps_drv_part_2") : 0.0;
         // StdDeep (task_id 4): the split tree of the sub-period T / (2 deep_num_steps)
-        const bool deep_task = rp.task_id == 4;
+        const bool deep_task = rp.task_id == 4 || rp.task_id == 8;  // StdDeep, LpnMultDeep
         const int nsub = deep_task ? int(param(cp, "deep_num_steps")) : 0;
         if (deep_task && nsub < 1) die("deep_num_steps must be positive");
         // JCS: the number operator (energy slot) and a = special (first random-observable slot)
@@ -634,9 +673,9 @@ int main(int argc, char **argv)
         check(qjx_set_states(h, psi.data()), h, "qjx_set_states");
         std::cout << "init_data" << std::endl;
 
-        if (rp.task_id == 7) {
+        if (rp.task_id == 7 || rp.task_id == 8) {
             run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, rp.sys_id, Nc, jcs ? jcs_alpha : mbl ? mbl_W : 1.0,
-                         jcs ? jcs_p1 * jcs_alpha + jcs_p2 * jcs_alpha : cfg.T);
+                         jcs ? jcs_p1 * jcs_alpha + jcs_p2 * jcs_alpha : cfg.T, nsub);
             qjx_destroy(h);
             return 0;
         }

@@ -257,6 +257,14 @@ class Engine:
         """calc_chars_lpn of the bases and lambda_lpn of the variations after one period."""
         self._chk(N.lib().qjx_lpn_period(self.h, float(curr_time), int(adr_dump)), "qjx_lpn_period")
 
+    def lpn_bases(self):
+        """calc_chars_lpn of the bases only (LpnMultDeep sub-periods without a Lyapunov step)."""
+        self._chk(N.lib().qjx_lpn_bases(self.h), "qjx_lpn_bases")
+
+    def run_sub_periods(self, n_sub, dump_base=0):
+        """Deep tasks: continue every trajectory for n_sub sub-periods, observables after each."""
+        self._chk(N.lib().qjx_run_sub_periods(self.h, int(n_sub), int(dump_base)), "qjx_run_sub_periods")
+
     def lpn_values(self):
         n = self.n
         out = {k: np.zeros(n) for k in ("lambda_now", "lambda", "delta_s", "mean_lpn", "energy_lpn")}

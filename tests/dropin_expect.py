@@ -122,7 +122,7 @@ def integrable_model(prm):
 
 def expected_outputs(cfg, prm, R=None):
     """All files the drop-in writes, as {relative file name: text}."""
-    if cfg.get("task_id", 1) == 7:
+    if cfg.get("task_id", 1) in (7, 8):
         return expected_lpn_outputs(cfg, prm, R)
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
@@ -396,6 +396,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
     """LpnMult (task_id 7): LpnMultExperimentBehaviour::trans_process / obser_process
     (experiment.cpp:138-286) with dump_std, dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127)
     and the adr files (dump.cpp:3-98)."""
+    nsub = int(prm["deep_num_steps"]) if cfg.get("task_id", 7) == 8 else 0  # LpnMultDeep
+    nss = 2 * nsub
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
     jcs = cfg.get("sys_id", 0) == 1  # JCS: a in observable slot 0, <a^+ a>, JCS file set
     integ = cfg.get("sys_id", 0) == 5  # Integrable: the special matrix in slot 0, spec only
@@ -448,9 +450,11 @@ def expected_lpn_outputs(cfg, prm, R=None):
         H, Hd, L, K0, K1 = O.dimer_operators(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"],
                                              prm["dimer_drv_ampl"], prm["diss_gamma"])
         T = TWO_PI / prm["dimer_drv_freq"]
-        U = np.stack([O.split_tree(K0, T, deep), O.split_tree(K1, T, deep)])
+        # LpnMultDeep (task_id 8): the split trees of the sub-period T / (2 deep_num_steps)
+        t_head = 0.5 * T / nsub if nsub else T
+        U = np.stack([O.split_tree(K0, t_head, deep), O.split_tree(K1, t_head, deep)])
         HE = H + prm["dimer_prm_E"] * Hd
-        ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, T, n, seed=seed, record=int(prm["jump"]),
+        ens = O.Ensemble(U, L, [1.0], HE, R if nr else None, t_head, n, seed=seed, record=int(prm["jump"]),
                          rec_cap=100000)
         calc_T = T
     ens.init(int(prm["start_type"]), int(prm["start_state"]))
@@ -458,6 +462,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
     period = [0]
 
     def advance(k, is_obs=1, tr1=None):
+        if nsub:  # deep: a period is 2 deep_num_steps units of each branch
+            return sum(ens.run_branch_units(b, nss, is_obs=is_obs, tr1=tr1) for _ in range(k) for b in range(2))
         if prop == 0:
             return ens.run_periods(k, is_obs=is_obs, tr1=tr1)
         Heff = O.dimer_heff(N, prm["dimer_prm_J"], prm["dimer_prm_U"], prm["dimer_prm_E"], prm["diss_gamma"])
@@ -475,7 +481,10 @@ def expected_lpn_outputs(cfg, prm, R=None):
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
                mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0, chars_sys=cfg.get("sys_id", 0))
-    dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
+    if nsub:  # init_dump_periods_deep (newdel_exp.cpp:377-406)
+        dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(nss)]
+    else:
+        dp = O.dump_periods(int(prm["dump_type"]), int(prm["dump_num"]), cfg.get("num_obs_periods", 10))
     ndt = len(dp)
     assert advance(cfg.get("num_tp_periods", 0), is_obs=0, tr1=half) == 0
     lp.start()
@@ -506,7 +515,33 @@ def expected_lpn_outputs(cfg, prm, R=None):
             emit("adr_%d" % tr + sfx, f_double_data(obs[0]["adr"][tr]), False)
     if evo_avg == 1 and adr_avg_on == 1:
         emit("adr_avg" + sfx, f_double_data(adr_avg(obs[0]["adr"], n)), False)
-    for dump_id in range(1, ndt):
+    if nsub and int(prm["dump_phi_evo"]) == 1:
+        for tr in range(n):
+            emit("phi_evo_%d" % tr + sfx, f_complex_data(ens.phi[tr]), False)
+    for p in range(cfg.get("num_obs_periods", 10) if nsub else 0):  # ex_period_obs_deep_mult_lpn
+        for b in range(2):
+            for k in range(nsub):
+                dump_id = p * nss + b * nsub + k + 1
+                assert ens.run_branch_units(b, 2) == 0
+                o = ens.observables(want_adr=True)
+                if lp.cfg.per_period == 0 or (b == 1 and k == nsub - 1):
+                    lp.period(float(dump_id) / float(nss) * calc_T)
+                    o["adr"][half:] = ens.observables(want_adr=True)["adr"][half:]
+                    last = lp.last()
+                    for v in range(half, n):
+                        if save_lambdas > 0 and last["renormed"][v]:
+                            for kk in recs:
+                                recs[kk][v].append(last[kk][v])
+                else:
+                    lp.bases()
+                obs.append(o)
+                lpn.append(lp.values())
+                if evo_sep == 1 and adr_sep == 1:
+                    for tr in range(n):
+                        emit("adr_%d" % tr + sfx, f_double_data(o["adr"][tr]), True)
+        if evo_avg == 1 and adr_avg_on == 1:
+            emit("adr_avg" + sfx, f_double_data(adr_avg(obs[-1]["adr"], half)), True)
+    for dump_id in range(1, ndt if not nsub else 1):
         o = {k: v.copy() for k, v in obs[-1].items()}
         for period_id in range(dp[dump_id - 1], dp[dump_id]):
             assert advance(1) == 0

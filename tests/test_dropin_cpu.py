@@ -88,6 +88,20 @@ def test_jcs_mbl_other_tasks_exit_with_error(tmp_path, sys_id, task_id, prop_id)
     assert r.returncode != 0 and "Error: Wrong task_id / prop_id for sys_id %d" % sys_id in r.stdout
 
 
+def test_lpn_mult_deep_checks(tmp_path):
+    """LpnMultDeep (task_id 8) appends suffix_lpn, runs the dimer with the QJ propagator only."""
+    cfg = dict(BASE_CONFIG, task_id=8)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, "deep_num_steps": 2}
+    r = check(tmp_path, cfg, prm)
+    assert r.returncode == 0, r.stdout
+    line = [x for x in r.stdout.splitlines() if x.startswith("fn_suffix = ")][0]
+    assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_setup(0_8_0)" in line
+    r = check(tmp_path, dict(cfg, prop_id=1), prm)
+    assert r.returncode != 0 and "Error: Wrong prop_id" in r.stdout
+    r = check(tmp_path, dict(cfg, sys_id=1), {**prm, **JCS_PARAMS})
+    assert r.returncode != 0 and "Error: Wrong task_id / prop_id for sys_id 1" in r.stdout
+
+
 SYS_PARAMS = {1: JCS_PARAMS, 2: PS_PARAMS, 3: MBL_PARAMS, 5: INTEGRABLE_PARAMS}
 
 

@@ -193,6 +193,21 @@ def test_integrable_lpn_mult_files_match(tmp_path, lpn_type):
     assert sum(int(x) for x in exp[k].split()) > 0
 
 
+@pytest.mark.parametrize("per_period", [0, 1])
+def test_lpn_mult_deep_files_match(tmp_path, per_period):
+    """LpnMultDeep (task_id 8, the dimer): base/variation pairs advanced sub-period by sub-period
+    (qjx_run_sub_periods), the Lyapunov step after every sub-period (lambda_per_periods 0) or at the
+    last one of each period with the bases' characteristics in between (1), one dump per sub-period
+    (experiment.cpp:302-350; core.cpp:155-241)."""
+    cfg = dict(BASE_CONFIG, task_id=8, num_trajectories=12, num_tp_periods=1, num_obs_periods=2)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, "deep_num_steps": 2, "lambda_per_periods": per_period, "jump": 1,
+           "dump_adr_sep": 1, "dump_adr_avg": 1, "dump_evo_avg": 1, "save_lambdas": 1, "lpn_delta_f_high": 1e-2,
+           "dump_phi_evo": 1}
+    exp = run_case(tmp_path, cfg, prm)
+    k = [k for k in exp if k.startswith("num_renorms")][0]
+    assert sum(int(x) for x in exp[k].split()) > 0
+
+
 def test_jcs_system_files_match(tmp_path):
     """The JCS system (sys_id 1): kick and free evolution of unequal duration, spec = <a> / alpha,
     mean = <a^+ a> (newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601; core.cpp:2739-3102)."""
