@@ -207,6 +207,28 @@ std::string ps_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string dimersync_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    auto f = [&](const char *key) {
+        std::stringstream v;
+        v << std::setprecision(precision) << std::fixed << param(cp, key);
+        return v.str();
+    };
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_N(" << int(param(cp, "dimersync_N")) << ")";
+    s << "_diss(" << int(param(cp, "diss_type")) << "_" << f("diss_gamma") << "_" << f("diss_phase") << ")";
+    s << "_drv1(" << f("dimersync_drv_ampl_1") << "_" << f("dimersync_drv_freq_1") << "_" << f("dimersync_drv_phase_1")
+      << ")";
+    s << "_drv2(" << f("dimersync_drv_ampl_2") << "_" << f("dimersync_drv_freq_2") << "_" << f("dimersync_drv_phase_2")
+      << ")";
+    s << "_T(" << int(param(cp, "dimersync_main_period")) << ")";
+    s << "_prm(" << f("dimersync_prm_E") << "_" << f("dimersync_prm_U") << "_" << f("dimersync_prm_J") << ")";
+    s << "_start(" << int(param(cp, "start_type")) << "_" << int(param(cp, "start_state")) << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

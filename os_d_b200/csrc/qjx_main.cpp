@@ -2,7 +2,9 @@
 // Std task (task_id 1) and the LpnMult task (task_id 7) with the QJ propagator (prop_id 0) or the
 // RK propagator (prop_id 1), and the StdDeep task (task_id 4, QJ propagator), for the dimer (sys_id 0);
 // the Std and LpnMult tasks with the QJ propagator for the JCS (sys_id 1), MBL (sys_id 3) and
-// Integrable (sys_id 5) systems, and the Std task with the QJ propagator for PS (sys_id 2).
+// Integrable (sys_id 5) systems, the Std task with the QJ propagator for PS (sys_id 2), and the
+// Std and LpnMult tasks with the QJ propagator for DimerSync (sys_id 6, whose QJ branches are the
+// dimer's with its first drive; the second drive enters the RK propagator only).
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -423,13 +425,17 @@ int main(int argc, char **argv)
     if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
     std::cout << params_echo(rp, cp);
 
-    if (rp.sys_id < 0 || rp.sys_id > 5 || rp.sys_id == 4)
+    if (rp.sys_id < 0 || rp.sys_id > 6 || rp.sys_id == 4)
         die("Wrong sys_id: " + std::to_string(rp.sys_id) +
-            " (this engine runs the dimer (0), JCS (1), PS (2), MBL (3) and Integrable (5) systems)");
+            " (this engine runs the dimer (0), JCS (1), PS (2), MBL (3), Integrable (5) and DimerSync (6) systems)");
     const bool jcs = rp.sys_id == 1;  // JCS, MBL, Integrable: Std and LpnMult with the QJ propagator
     const bool mbl = rp.sys_id == 3;
     const bool integ = rp.sys_id == 5;
     const bool ps = rp.sys_id == 2;  // PS: the Std task with the QJ propagator
+    const bool dsync = rp.sys_id == 6;
+    if (dsync && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
+        die("Wrong task_id / prop_id for sys_id 6 (this engine runs DimerSync with the Std and LpnMult tasks and the "
+            "QJ propagator)");
     if (ps && (rp.task_id != 1 || rp.prop_id != 0))
         die("Wrong task_id / prop_id for sys_id 2 (this engine runs PS with the Std task and the QJ propagator)");
     if ((jcs || mbl || integ) && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
@@ -448,6 +454,7 @@ int main(int argc, char **argv)
                        : mbl ? mbl_suffix(rp, cp, 4)
                        : integ ? integrable_suffix(rp, cp, 4)
                        : ps    ? ps_suffix(rp, cp, 4)
+                       : dsync ? dimersync_suffix(rp, cp, 4)
                                : dimer_suffix(rp, cp, 4);
     } catch (const std::exception &e) {
         die(e.what());
@@ -459,7 +466,7 @@ int main(int argc, char **argv)
 
     try {
         const bool dimer = !jcs && !mbl && !integ && !ps;
-        const int N = (mbl || integ || ps) ? 0 : int(param(cp, "N"));
+        const int N = (mbl || integ || ps) ? 0 : int(param(cp, dsync ? "dimersync_N" : "N"));
         // PS: 2^ps_num_spins spin states times ps_num_photons_states photon states
         const int ps_ns = ps ? int(param(cp, "ps_num_spins")) : 0, ps_np = ps ? int(param(cp, "ps_num_photons_states")) : 0;
         const int ps_dt = ps ? int(param(cp, "diss_type")) : 0;
@@ -480,9 +487,17 @@ int main(int argc, char **argv)
         // JCS and PS run each drive part as two halves of its tree (init_split_structure_jcs / _ps,
         // core.cpp:10086-10157, 10234-10305: counter 2): four engine branches [K_0, K_0, K_1, K_1]
         const int nbr = (ps || jcs) ? 4 : 2;
-        const double J = dimer ? param(cp, "dimer_prm_J") : 0.0, U = dimer ? param(cp, "dimer_prm_U") : 0.0;
-        const double E = dimer ? param(cp, "dimer_prm_E") : 0.0;
-        const double A = dimer ? param(cp, "dimer_drv_ampl") : 0.0, omega = dimer ? param(cp, "dimer_drv_freq") : 1.0;
+        // DimerSync (newdel.cpp:39-95, 500-563, 2390-2498): the dimer's operators under its own keys,
+        // drive 1 in the QJ branches, the period of drive dimersync_main_period
+        const int dsync_main = dsync ? int(param(cp, "dimersync_main_period")) : 0;
+        if (dsync && dsync_main != 1 && dsync_main != 2) die("Error: wrong dimersync_main_period");
+        const double J = dimer ? param(cp, dsync ? "dimersync_prm_J" : "dimer_prm_J") : 0.0;
+        const double U = dimer ? param(cp, dsync ? "dimersync_prm_U" : "dimer_prm_U") : 0.0;
+        const double E = dimer ? param(cp, dsync ? "dimersync_prm_E" : "dimer_prm_E") : 0.0;
+        const double A = dimer ? param(cp, dsync ? "dimersync_drv_ampl_1" : "dimer_drv_ampl") : 0.0;
+        const double omega = !dimer ? 1.0
+                             : dsync ? param(cp, dsync_main == 1 ? "dimersync_drv_freq_1" : "dimersync_drv_freq_2")
+                                     : param(cp, "dimer_drv_freq");
         const double mbl_W = mbl ? param(cp, "mbl_prm_W") : 1.0;
         const double g = param(cp, "diss_gamma");
         const double jcs_alpha = jcs ? param(cp, "jcs_prm_alpha") : 0.0;
@@ -674,7 +689,8 @@ int main(int argc, char **argv)
         std::cout << "init_data" << std::endl;
 
         if (rp.task_id == 7 || rp.task_id == 8) {
-            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, rp.sys_id, Nc, jcs ? jcs_alpha : mbl ? mbl_W : 1.0,
+            // DimerSync's Lyapunov characteristics are the dimer's (DimerSyncCoreBehaviour, core.cpp:1812-1997)
+            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, dsync ? 0 : rp.sys_id, Nc, jcs ? jcs_alpha : mbl ? mbl_W : 1.0,
                          jcs ? jcs_p1 * jcs_alpha + jcs_p2 * jcs_alpha : cfg.T, nsub);
             qjx_destroy(h);
             return 0;

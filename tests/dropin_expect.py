@@ -62,6 +62,18 @@ def suffix(cfg, prm):
     JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
     for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 6:  # DimerSyncOutputBehavior::suffix_param (outputter.cpp:45-93)
+        return ("_setup(%d_%d_%d)" % (6, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_N(%d)" % int(prm["dimersync_N"])
+                + "_diss(%d_%s_%s)" % (int(prm["diss_type"]), f4(prm["diss_gamma"]), f4(prm["diss_phase"]))
+                + "".join("_drv%d(%s_%s_%s)" % (i, f4(prm["dimersync_drv_ampl_%d" % i]),
+                                                f4(prm["dimersync_drv_freq_%d" % i]), f4(prm["dimersync_drv_phase_%d" % i]))
+                          for i in (1, 2))
+                + "_T(%d)" % int(prm["dimersync_main_period"])
+                + "_prm(%s_%s_%s)" % (f4(prm["dimersync_prm_E"]), f4(prm["dimersync_prm_U"]), f4(prm["dimersync_prm_J"]))
+                + "_start(%d_%d)" % (int(prm["start_type"]), int(prm["start_state"]))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 2:  # PSOutputBehavior::suffix_param (outputter.cpp:135-174)
         return ("_setup(%d_%d_%d)" % (2, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -120,10 +132,22 @@ def integrable_model(prm):
                                   float(prm["integrable_k"]))
 
 
+def dimersync_as_dimer(cfg, prm):
+    """DimerSync (sys_id 6) runs the dimer's QJ branches under its own keys (newdel.cpp:39-95,
+    500-563, 2390-2498): drive 1, the period of drive dimersync_main_period."""
+    if cfg.get("sys_id", 0) != 6:
+        return prm
+    main = int(prm["dimersync_main_period"])
+    return {**prm, "N": prm["dimersync_N"], "dimer_prm_J": prm["dimersync_prm_J"], "dimer_prm_U": prm["dimersync_prm_U"],
+            "dimer_prm_E": prm["dimersync_prm_E"], "dimer_drv_ampl": prm["dimersync_drv_ampl_1"],
+            "dimer_drv_freq": prm["dimersync_drv_freq_%d" % main]}
+
+
 def expected_outputs(cfg, prm, R=None):
     """All files the drop-in writes, as {relative file name: text}."""
     if cfg.get("task_id", 1) in (7, 8):
         return expected_lpn_outputs(cfg, prm, R)
+    sfx_prm, prm = prm, dimersync_as_dimer(cfg, prm)
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
     integ = cfg.get("sys_id", 0) == 5
@@ -141,7 +165,7 @@ def expected_outputs(cfg, prm, R=None):
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
     path = cfg.get("path", "")
-    sfx = suffix(cfg, prm)
+    sfx = suffix(cfg, sfx_prm)
     nr = int(prm["num_random_obs"])
     deep_task = cfg.get("task_id", 1) == 4
     nsub = int(prm.get("deep_num_steps", 0)) if deep_task else 0
@@ -396,6 +420,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
     """LpnMult (task_id 7): LpnMultExperimentBehaviour::trans_process / obser_process
     (experiment.cpp:138-286) with dump_std, dump_lpn, dump_std_evo, dump_lpn_evo (core.cpp:918-1127)
     and the adr files (dump.cpp:3-98)."""
+    sfx_prm, prm = prm, dimersync_as_dimer(cfg, prm)
     nsub = int(prm["deep_num_steps"]) if cfg.get("task_id", 7) == 8 else 0  # LpnMultDeep
     nss = 2 * nsub
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
@@ -416,7 +441,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
     deep = cfg.get("ex_deep", 16)
     seed = cfg.get("seed", 0)
     path = cfg.get("path", "")
-    sfx = suffix(cfg, prm)
+    sfx = suffix(cfg, sfx_prm)
     nr = int(prm["num_random_obs"])
     if jcs:
         alpha = W
@@ -480,7 +505,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
                eps_error=float(prm["lpn_eps_error"]), delta_s=float(prm["lpn_delta_s"]),
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
-               mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0, chars_sys=cfg.get("sys_id", 0))
+               mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0,
+               chars_sys=0 if cfg.get("sys_id", 0) == 6 else cfg.get("sys_id", 0))  # DimerSync: the dimer's
     if nsub:  # init_dump_periods_deep (newdel_exp.cpp:377-406)
         dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(nss)]
     else:
@@ -651,6 +677,12 @@ def expected_lpn_outputs(cfg, prm, R=None):
 
 
 JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_1": 0.5, "jcs_drv_part_2": 1.5}
+
+# a DimerSync system (two drives; the QJ branches carry drive 1, the period is drive 2's)
+DIMERSYNC_PARAMS = {"dimersync_N": 16, "dimersync_prm_E": 1.0, "dimersync_prm_U": 0.5, "dimersync_prm_J": 1.0,
+                    "dimersync_drv_ampl_1": 1.5, "dimersync_drv_freq_1": 1.0, "dimersync_drv_phase_1": 0.0,
+                    "dimersync_drv_ampl_2": 0.5, "dimersync_drv_freq_2": 2.0, "dimersync_drv_phase_2": 0.25,
+                    "dimersync_main_period": 2}
 
 # submit_ps.py's system (1 spin, alpha 5, parts 1 / 1 (x T), diss_w 0.05; 300 photon states there, 24 here)
 PS_PARAMS = {"ps_num_spins": 1, "ps_num_photons_states": 24, "ps_prm_alpha": 5.0, "ps_prm_d": 1.0, "ps_prm_g": 0.5,

@@ -5,8 +5,8 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS,
-                                 PS_PARAMS, config_text, params_text, suffix)
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS,
+                                 MBL_PARAMS, PS_PARAMS, config_text, params_text, suffix)
 
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
 
@@ -81,7 +81,8 @@ def test_mbl_suffix_matches_reference_rule(tmp_path, over):
     assert line[len("fn_suffix = "):] == suffix(cfg, prm) and "_Nc(8)_rnd(" in line
 
 
-@pytest.mark.parametrize("sys_id,task_id,prop_id", [(3, 4, 0), (1, 4, 0), (3, 7, 1), (1, 1, 1), (5, 4, 0), (2, 7, 0)])
+@pytest.mark.parametrize("sys_id,task_id,prop_id", [(3, 4, 0), (1, 4, 0), (3, 7, 1), (1, 1, 1), (5, 4, 0), (2, 7, 0),
+                                                     (6, 8, 0), (6, 1, 1)])
 def test_jcs_mbl_other_tasks_exit_with_error(tmp_path, sys_id, task_id, prop_id):
     prm = {**BASE_PARAMS, **LPN_PARAMS, **SYS_PARAMS[sys_id]}
     r = check(tmp_path, dict(BASE_CONFIG, sys_id=sys_id, task_id=task_id, prop_id=prop_id), prm)
@@ -102,10 +103,10 @@ def test_lpn_mult_deep_checks(tmp_path):
     assert r.returncode != 0 and "Error: Wrong task_id / prop_id for sys_id 1" in r.stdout
 
 
-SYS_PARAMS = {1: JCS_PARAMS, 2: PS_PARAMS, 3: MBL_PARAMS, 5: INTEGRABLE_PARAMS}
+SYS_PARAMS = {1: JCS_PARAMS, 2: PS_PARAMS, 3: MBL_PARAMS, 5: INTEGRABLE_PARAMS, 6: DIMERSYNC_PARAMS}
 
 
-@pytest.mark.parametrize("sys_id,task_id", [(1, 7), (3, 7), (5, 7), (5, 1), (2, 1)])
+@pytest.mark.parametrize("sys_id,task_id", [(1, 7), (3, 7), (5, 7), (5, 1), (2, 1), (6, 1), (6, 7)])
 def test_jcs_mbl_integrable_suffix(tmp_path, sys_id, task_id):
     """suffix_param (+ suffix_lpn for LpnMult) of JCS, MBL and Integrable (outputter.cpp:95-269,
     371-381); Integrable prints tau and k as integers."""

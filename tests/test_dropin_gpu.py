@@ -8,8 +8,8 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS,
-                                 PS_PARAMS, config_text, expected_outputs, params_text)
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS,
+                                 MBL_PARAMS, PS_PARAMS, config_text, expected_outputs, params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -27,6 +27,7 @@ def run_case(tmp_path, cfg, prm):
     d = math.comb(int(prm["mbl_Nc"]), int(prm["mbl_Nc"]) // 2) if cfg.get("sys_id", 0) == 3 else d
     d = 1 << int(prm["integrable_N"]) if cfg.get("sys_id", 0) == 5 else d
     d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"]) if cfg.get("sys_id", 0) == 2 else d
+    d = int(prm["dimersync_N"]) + 1 if cfg.get("sys_id", 0) == 6 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -206,6 +207,16 @@ def test_lpn_mult_deep_files_match(tmp_path, per_period):
     exp = run_case(tmp_path, cfg, prm)
     k = [k for k in exp if k.startswith("num_renorms")][0]
     assert sum(int(x) for x in exp[k].split()) > 0
+
+
+@pytest.mark.parametrize("task_id", [1, 7])
+def test_dimersync_files_match(tmp_path, task_id):
+    """DimerSync (sys_id 6): the dimer's QJ branches under the dimersync_* keys, drive 1 in the
+    branches and drive 2's period (newdel.cpp:39-95, 500-563, 2390-2498; core.cpp:9983-10030)."""
+    cfg = dict(BASE_CONFIG, sys_id=6, task_id=task_id, num_trajectories=12, num_tp_periods=1, num_obs_periods=4)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **DIMERSYNC_PARAMS, "dump_num": 4, "jump": 1, "dump_adr_sep": 1,
+           "lpn_delta_f_high": 1e-2}
+    run_case(tmp_path, cfg, prm)
 
 
 def test_jcs_system_files_match(tmp_path):
