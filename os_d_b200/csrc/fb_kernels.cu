@@ -118,10 +118,14 @@ struct FbClusterParams {
 __device__ __forceinline__ double row_sum_lanes(const int *rp, const int *col, const double *val, const double *arg,
                                                 int r)
 {
+    const int b = rp[r], e = rp[r + 1];
+    // A row with at most one nonzero (every row of the drive matrix Qs, so warps do not diverge
+    // here): lane 0 holds fma(v, a, 0) and the tree adds only +0.0 to it, which leaves every value
+    // but -0 unchanged and turns -0 into +0, i.e. the result is p0 + 0.0.
+    if (e - b <= 1) return e > b ? __dadd_rn(__fma_rn(val[b], arg[col[b]], 0.0), 0.0) : 0.0;
     double p[32];
 #pragma unroll
     for (int l = 0; l < 32; l++) p[l] = 0.0;
-    const int b = rp[r], e = rp[r + 1];
     for (int base = b; base < e; base += 32) {
 #pragma unroll
         for (int l = 0; l < 32; l++) {
