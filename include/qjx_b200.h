@@ -317,6 +317,14 @@ qjx_status qjx_build_ps(int ns, int nps, double alpha, double d_prm, double g_pr
  * (init_split_structure_integrable, core.cpp:10610-10660).  Any output pointer may be NULL. */
 qjx_status qjx_build_integrable(int N, int seed, int num_seeds, double tau, double k, double T, int deep, double *L,
                                 double *special, double *K, double *Utree);
+/* The Floquet two-spin system (sys_id 7; Floq2SpinsNewDelBehaviour, newdel.cpp:346-378, 1096-1182,
+ * 2077-2136, 3005-3101), QJ branch: d = 4, H = (Delta_1 sz (x) 1 + Delta_2 1 (x) sz)/2 + J sy (x) sy
+ * (also the spec observable), L [2] = sigma_- on each spin, K = -i (H - (i/2) gamma sum L^H L), jump
+ * rates 1; Utree [deep][4][4] = exp(K T 2^-(l+2)) for one branch that covers T / 2 per period
+ * (init_split_structure_floq2spins, core.cpp:10722-10766); the drive enters the RK propagator only.
+ * Any output pointer may be NULL. */
+qjx_status qjx_build_floq2spins(double D1, double D2, double J, double gamma, double T, int deep, double *H,
+                                double *L, double *K, double *Utree);
 /* The MBL imbalance of n probability rows adr [n][d] (get_imbalance_mbl, experiment.cpp:1753-1800). */
 qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double *out);
 /* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)

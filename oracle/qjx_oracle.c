@@ -498,6 +498,52 @@ int orc_ps_operators(int ns, int nps, double alpha, double dprm, double gprm, do
     return 0;
 }
 
+/* Floq2Spins (sys_id 7, newdel.cpp:346-378, 1096-1182, 2077-2136, 3005-3101): two spins, d = 4 (spin 0
+ * the more significant), H = (Delta_1 sz (x) 1 + Delta_2 1 (x) sz) / 2 + J sy (x) sy (real: diagonal
+ * (Delta_1 s1 + Delta_2 s2) / 2, anti-diagonal -J, J, J, -J), special = H, L = [sm (x) 1, 1 (x) sm]
+ * with sm = |1><0|, K = -i (H - (i/2) gamma sum L^H L); the drive enters the RK propagator only. */
+int orc_floq2spins_operators(double D1, double D2, double J, double gamma, double *H, double *L, double *K)
+{
+    const int d = 4;
+    const size_t dd = 16;
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 4 * dd * sizeof(double));
+    for (int x = 0; x < d; x++) {
+        const double s1 = (x & 2) ? -1.0 : 1.0, s2 = (x & 1) ? -1.0 : 1.0;
+        H[2 * (x * d + x)] = 0.5 * (D1 * s1 + D2 * s2);
+    }
+    H[2 * (0 * d + 3)] = -J;
+    H[2 * (1 * d + 2)] = J;
+    H[2 * (2 * d + 1)] = J;
+    H[2 * (3 * d + 0)] = -J;
+    for (int x = 0; x < d; x++) {
+        if (!(x & 2)) L[2 * ((x | 2) * d + x)] = 1.0;           /* sm on spin 0 */
+        if (!(x & 1)) L[2 * (dd + (x | 1) * d + x)] = 1.0;      /* sm on spin 1 */
+    }
+    double hp[32];
+    for (size_t e = 0; e < 2 * dd; e++) hp[e] = H[e];
+    for (int c = 0; c < 2; c++) {
+        const double *Lc = L + 2 * dd * c;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int k = 0; k < d; k++) {
+                    const double ar = Lc[2 * (k * d + i)], ai = Lc[2 * (k * d + i) + 1];
+                    const double br = Lc[2 * (k * d + j)], bi = Lc[2 * (k * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                hp[2 * (i * d + j)] += 0.5 * (gamma * si);
+                hp[2 * (i * d + j) + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        K[2 * e] = 0.0 + hp[2 * e + 1];
+        K[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    return 0;
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

@@ -75,6 +75,10 @@ int orc_ps_operators(int ns, int nps, double alpha, double dprm, double gprm, do
 int orc_integrable_operators(int N, int seed, int num_seeds, double tau, double kk, double *L, double *special,
                              double *K);
 
+/* Floq2Spins (sys_id 7, newdel.cpp:346-378, 1096-1182, 2077-2136, 3005-3101): d = 4; H (= special),
+ * L [2], K = hamiltonians_qj[0] (undriven). */
+int orc_floq2spins_operators(double D1, double D2, double J, double gamma, double *H, double *L, double *K);
+
 /* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
  * propagator (newdel.cpp:2354-2366), complex d x d. */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);

@@ -229,6 +229,21 @@ std::string dimersync_suffix(const RunParam &rp, const ConfigParam &cp, int prec
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string floq2spins_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    auto f = [&](const char *key) {
+        std::stringstream v;
+        v << std::setprecision(precision) << std::fixed << param(cp, key);
+        return v.str();
+    };
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_ampl(" << f("flq2sp_ampl") << ")_freq(" << f("flq2sp_freq") << ")_D1(" << f("flq2sp_Delta_1") << ")_D2("
+      << f("flq2sp_Delta_2") << ")_J(" << f("flq2sp_J") << ")_gamma(" << f("flq2sp_gamma") << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

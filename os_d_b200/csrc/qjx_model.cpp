@@ -760,3 +760,64 @@ extern "C" qjx_status qjx_build_ps(int ns, int nps, double alpha, double dprm, d
         }
     return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
 }
+
+// ------------------------------------------------------------------------------------ Floq2Spins
+// Floq2SpinsNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp:346-378, 1096-1182, 2077-2136,
+// 3005-3101): two spins (spin 0 the more significant bit), d = 4; the QJ branch is undriven.
+extern "C" qjx_status qjx_build_floq2spins(double D1, double D2, double J, double gamma, double T, int deep,
+                                           double *H, double *L, double *Kout, double *Utree)
+{
+    if (Utree && (deep < 1 || !(T > 0.0))) return QJX_ERR_INVALID_ARG;
+    const int d = 4;
+    const size_t dd = 16, e2 = 32;
+    cvec h(e2, 0.0), l(2 * e2, 0.0);
+    for (int x = 0; x < d; x++) {  // (Delta_1 sz (x) 1 + Delta_2 1 (x) sz) / 2
+        const double s1 = (x & 2) ? -1.0 : 1.0, s2 = (x & 1) ? -1.0 : 1.0;
+        h[2 * (x * d + x)] = 0.5 * (D1 * s1 + D2 * s2);
+    }
+    // J sy (x) sy: anti-diagonal -J, J, J, -J
+    h[2 * (0 * d + 3)] = -J;
+    h[2 * (1 * d + 2)] = J;
+    h[2 * (2 * d + 1)] = J;
+    h[2 * (3 * d + 0)] = -J;
+    for (int x = 0; x < d; x++) {  // sm (x) 1 and 1 (x) sm, sm = |1><0|
+        if (!(x & 2)) l[2 * ((x | 2) * d + x)] = 1.0;
+        if (!(x & 1)) l[2 * (dd + (x | 1) * d + x)] = 1.0;
+    }
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), 2 * e2 * sizeof(double));
+    if (!Kout && !Utree) return QJX_OK;
+    cvec hp(h), k(e2);
+    for (int c = 0; c < 2; c++) {
+        const double *lc = l.data() + e2 * c;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int q = 0; q < d; q++) {
+                    const double ar = lc[2 * (q * d + i)], ai = lc[2 * (q * d + i) + 1];
+                    const double br = lc[2 * (q * d + j)], bi = lc[2 * (q * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                hp[2 * (i * d + j)] += 0.5 * (gamma * si);
+                hp[2 * (i * d + j) + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        k[2 * e] = 0.0 + hp[2 * e + 1];
+        k[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    if (Kout) std::memcpy(Kout, k.data(), e2 * sizeof(double));
+    if (!Utree) return QJX_OK;
+    // init_split_structure_floq2spins (core.cpp:10722-10766): a head of duration T whose one branch
+    // runs the tree of T (so a period advances T / 2)
+    bool ok = true;
+    for (int lv = 0; lv < deep; lv++) {
+        double dt = T * 0.5;
+        for (int q = 0; q <= lv; q++) dt *= 0.5;
+        cvec scaled(e2);
+        for (size_t e = 0; e < e2; e++) scaled[e] = k[e] * dt;
+        ok = expm(d, scaled.data(), Utree + e2 * (size_t)lv) && ok;
+    }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

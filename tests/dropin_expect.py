@@ -62,6 +62,13 @@ def suffix(cfg, prm):
     JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
     for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 7:  # Floq2SpinsOutputBehavior::suffix_param (outputter.cpp:271-299)
+        return ("_setup(%d_%d_%d)" % (7, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "".join("_%s(%s)" % (k, f4(prm[key])) for k, key in (
+                    ("ampl", "flq2sp_ampl"), ("freq", "flq2sp_freq"), ("D1", "flq2sp_Delta_1"), ("D2", "flq2sp_Delta_2"),
+                    ("J", "flq2sp_J"), ("gamma", "flq2sp_gamma")))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 6:  # DimerSyncOutputBehavior::suffix_param (outputter.cpp:45-93)
         return ("_setup(%d_%d_%d)" % (6, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -125,6 +132,21 @@ def lpn_suffix(prm):
                                         np.log10(prm["lpn_delta_f_high"]), np.log10(prm["lpn_delta_f_low"]))
 
 
+def spec_system(cfg, prm, deep):
+    """Integrable (sys_id 5) or Floq2Spins (sys_id 7): L, special, H, period T, split trees U, K.
+    Integrable: H = 0, a head of duration integrable_T with two children of the same tree;
+    Floq2Spins: special = H, one undriven branch covering T / 2 per period (core.cpp:10722-10766)."""
+    if cfg.get("sys_id", 0) == 7:
+        H, L, K = O.floq2spins_operators(prm["flq2sp_Delta_1"], prm["flq2sp_Delta_2"], prm["flq2sp_J"],
+                                         prm["flq2sp_gamma"])
+        T = TWO_PI / prm["flq2sp_freq"]
+        return L, H, H, T, O.split_tree(K, T, deep)[None], K
+    L, S, K = integrable_model(prm)
+    T = prm["integrable_T"]
+    Ut = O.split_tree(K, T, deep)
+    return L, S, np.zeros_like(S), T, np.stack([Ut, Ut]), K
+
+
 def integrable_model(prm):
     """The Integrable operators (L [N], special, K) of a params dict."""
     return O.integrable_operators(int(prm["integrable_N"]), int(prm["integrable_seed"]),
@@ -150,7 +172,7 @@ def expected_outputs(cfg, prm, R=None):
     sfx_prm, prm = prm, dimersync_as_dimer(cfg, prm)
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
-    integ = cfg.get("sys_id", 0) == 5
+    integ = cfg.get("sys_id", 0) in (5, 7)  # Integrable, Floq2Spins
     ps = cfg.get("sys_id", 0) == 2
     N = 0 if (mbl or integ or ps) else int(prm["N"])
     d = N if jcs else N + 1
@@ -158,7 +180,7 @@ def expected_outputs(cfg, prm, R=None):
         Nc = int(prm["mbl_Nc"])
         d = len(O.mbl_basis(Nc))
     if integ:
-        d = 1 << int(prm["integrable_N"])
+        d = 4 if cfg.get("sys_id", 0) == 7 else 1 << int(prm["integrable_N"])
     if ps:
         d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"])
     n = cfg["num_trajectories"]
@@ -193,12 +215,9 @@ def expected_outputs(cfg, prm, R=None):
         T = alpha
         ens = O.Ensemble(U, L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
                          branch_len=[0.5 * heads[0], 0.5 * heads[0], 0.5 * heads[1], 0.5 * heads[1]])
-    elif integ:  # Integrable: H = 0, one head of duration integrable_T, two children; spec = <special>
-        Ls, S, K = integrable_model(prm)
-        T = prm["integrable_T"]
-        Ut = O.split_tree(K, T, deep)
-        U = np.stack([Ut, Ut])
-        H = np.zeros_like(S)
+    elif integ:  # Integrable / Floq2Spins: spec = <special>
+        Ls, S, H, T, U, K = spec_system(cfg, prm, deep)
+        Ut = U[0]
         Rs = np.concatenate([S[None], R]) if nr else S[None]
         ens = O.Ensemble(U, Ls, [1.0] * Ls.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
     elif mbl:  # MBL: one head of duration mbl_T, two children of the same tree; spec = <H> / W
@@ -425,7 +444,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
     nss = 2 * nsub
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
     jcs = cfg.get("sys_id", 0) == 1  # JCS: a in observable slot 0, <a^+ a>, JCS file set
-    integ = cfg.get("sys_id", 0) == 5  # Integrable: the special matrix in slot 0, spec only
+    integ = cfg.get("sys_id", 0) in (5, 7)  # Integrable, Floq2Spins: the special matrix in slot 0
     spec = mbl or jcs or integ
     N = 0 if (mbl or integ) else int(prm["N"])
     d = N if jcs else N + 1
@@ -435,7 +454,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
     if jcs:
         W = float(prm["jcs_prm_alpha"])  # the spec divisor
     if integ:
-        d, W = 1 << int(prm["integrable_N"]), 1.0
+        d, W = (4 if cfg.get("sys_id", 0) == 7 else 1 << int(prm["integrable_N"])), 1.0
     n = cfg["num_trajectories"]
     half = n // 2
     deep = cfg.get("ex_deep", 16)
@@ -455,13 +474,10 @@ def expected_lpn_outputs(cfg, prm, R=None):
         ens = O.Ensemble(U, L, [1.0], Nop, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000,
                          branch_len=[0.5 * heads[0], 0.5 * heads[0], 0.5 * heads[1], 0.5 * heads[1]])
     elif integ:
-        L, S, K = integrable_model(prm)
-        T = calc_T = prm["integrable_T"]
-        Ut = O.split_tree(K, T, deep)
-        H = np.zeros_like(S)
+        L, S, H, T, U, _ = spec_system(cfg, prm, deep)
+        calc_T = T
         Rs = np.concatenate([S[None], R]) if nr else S[None]
-        ens = O.Ensemble(np.stack([Ut, Ut]), L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]),
-                         rec_cap=100000)
+        ens = O.Ensemble(U, L, [1.0] * L.shape[0], H, Rs, T, n, seed=seed, record=int(prm["jump"]), rec_cap=100000)
     elif mbl:
         en, H, L, K = O.mbl_operators(Nc, W, prm["mbl_prm_U"], prm["mbl_prm_J"], int(prm["mbl_seed"]),
                                       int(prm["mbl_mns"]), int(prm["diss_type"]), prm["diss_phase"], prm["diss_gamma"])
@@ -506,7 +522,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
                mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0,
-               chars_sys=0 if cfg.get("sys_id", 0) == 6 else cfg.get("sys_id", 0))  # DimerSync: the dimer's
+               chars_sys={6: 0, 7: 5}.get(cfg.get("sys_id", 0), cfg.get("sys_id", 0)))  # DimerSync, Floq2Spins
     if nsub:  # init_dump_periods_deep (newdel_exp.cpp:377-406)
         dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(nss)]
     else:
@@ -677,6 +693,10 @@ def expected_lpn_outputs(cfg, prm, R=None):
 
 
 JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_1": 0.5, "jcs_drv_part_2": 1.5}
+
+# a Floquet two-spin system (its QJ branch is undriven: flq2sp_ampl enters the RK propagator only)
+FLOQ2_PARAMS = {"flq2sp_ampl": 1.0, "flq2sp_freq": 1.0, "flq2sp_Delta_1": 1.0, "flq2sp_Delta_2": 0.6, "flq2sp_J": 0.4,
+                "flq2sp_gamma": 0.3}
 
 # a DimerSync system (two drives; the QJ branches carry drive 1, the period is drive 2's)
 DIMERSYNC_PARAMS = {"dimersync_N": 16, "dimersync_prm_E": 1.0, "dimersync_prm_U": 0.5, "dimersync_prm_J": 1.0,

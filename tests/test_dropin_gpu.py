@@ -8,8 +8,8 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS,
-                                 MBL_PARAMS, PS_PARAMS, config_text, expected_outputs, params_text)
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS,
+                                 LPN_PARAMS, MBL_PARAMS, PS_PARAMS, config_text, expected_outputs, params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -28,6 +28,7 @@ def run_case(tmp_path, cfg, prm):
     d = 1 << int(prm["integrable_N"]) if cfg.get("sys_id", 0) == 5 else d
     d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"]) if cfg.get("sys_id", 0) == 2 else d
     d = int(prm["dimersync_N"]) + 1 if cfg.get("sys_id", 0) == 6 else d
+    d = 4 if cfg.get("sys_id", 0) == 7 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -215,6 +216,17 @@ def test_dimersync_files_match(tmp_path, task_id):
     branches and drive 2's period (newdel.cpp:39-95, 500-563, 2390-2498; core.cpp:9983-10030)."""
     cfg = dict(BASE_CONFIG, sys_id=6, task_id=task_id, num_trajectories=12, num_tp_periods=1, num_obs_periods=4)
     prm = {**BASE_PARAMS, **LPN_PARAMS, **DIMERSYNC_PARAMS, "dump_num": 4, "jump": 1, "dump_adr_sep": 1,
+           "lpn_delta_f_high": 1e-2}
+    run_case(tmp_path, cfg, prm)
+
+
+@pytest.mark.parametrize("task_id,is_debug", [(1, 1), (7, 0)])
+def test_floq2spins_files_match(tmp_path, task_id, is_debug):
+    """Floq2Spins (sys_id 7): two spins, sigma_- on each, the undriven QJ branch covering T / 2 per
+    period, spec = <H> (newdel.cpp:346-378, 1096-1182, 2077-2136, 3005-3101; core.cpp:6865-7830)."""
+    cfg = dict(BASE_CONFIG, sys_id=7, task_id=task_id, num_trajectories=16, num_tp_periods=1, num_obs_periods=4,
+               is_debug=is_debug)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **FLOQ2_PARAMS, "dump_num": 4, "jump": 2, "dump_adr_sep": 1,
            "lpn_delta_f_high": 1e-2}
     run_case(tmp_path, cfg, prm)
 
