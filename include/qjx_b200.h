@@ -325,6 +325,13 @@ qjx_status qjx_build_integrable(int N, int seed, int num_seeds, double tau, doub
  * Any output pointer may be NULL. */
 qjx_status qjx_build_floq2spins(double D1, double D2, double J, double gamma, double T, int deep, double *H,
                                 double *L, double *K, double *Utree);
+/* The Floquet many-spin system (sys_id 8; FloqManySpinsNewDelBehaviour, newdel.cpp:379-413, 1184-1332,
+ * 2138-2224, 3103-3199), QJ branch: n spins (1 <= n <= 10), d = 2^n, H = (Delta / 2) sum sz + J sy^(x)n
+ * (n >= 2; (Delta / 2) sz for n = 1), also the spec observable; L [n] = sigma_- on each spin; K = -i (H
+ * - (i/2) gamma sum L^H L), jump rates 1; Utree [deep][d][d] = exp(K T 2^-(l+2)) for one branch covering
+ * T / 2 per period (init_split_structure_floqnspins, core.cpp:10825-10871).  Any output may be NULL. */
+qjx_status qjx_build_floqnspins(int n, double Delta, double J, double gamma, double T, int deep, double *H, double *L,
+                                double *K, double *Utree);
 /* The MBL imbalance of n probability rows adr [n][d] (get_imbalance_mbl, experiment.cpp:1753-1800). */
 qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double *out);
 /* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)

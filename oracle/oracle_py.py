@@ -68,6 +68,7 @@ def lib():
         L.orc_mbl_imbalance.argtypes = [C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
         L.orc_ps_operators.argtypes = [C.c_int] * 2 + [C.c_double] * 4 + [C.c_int, C.c_double] + [c_double_p] * 6
         L.orc_floq2spins_operators.argtypes = [C.c_double] * 4 + [c_double_p] * 3
+        L.orc_floqnspins_operators.argtypes = [C.c_int] + [C.c_double] * 3 + [c_double_p] * 3
         L.orc_integrable_operators.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [c_double_p] * 3
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -165,6 +166,14 @@ def floq2spins_operators(D1, D2, J, gamma):
     """Floq2Spins (sys_id 7): H (= special), L [2], K = hamiltonians_qj[0] (d = 4)."""
     H, K, L = _cplx((4, 4)), _cplx((4, 4)), _cplx((2, 4, 4))
     assert lib().orc_floq2spins_operators(D1, D2, J, gamma, _dp(H), _dp(L), _dp(K)) == 0
+    return H, L, K
+
+
+def floqnspins_operators(n, Delta, J, gamma):
+    """FloqManySpins (sys_id 8): H (= special), L [n], K = hamiltonians_qj[0] (d = 2^n)."""
+    d = 1 << n
+    H, K, L = _cplx((d, d)), _cplx((d, d)), _cplx((n, d, d))
+    assert lib().orc_floqnspins_operators(n, Delta, J, gamma, _dp(H), _dp(L), _dp(K)) == 0
     return H, L, K
 
 

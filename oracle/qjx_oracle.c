@@ -544,6 +544,66 @@ int orc_floq2spins_operators(double D1, double D2, double J, double gamma, doubl
     return 0;
 }
 
+/* FloqManySpins (sys_id 8, newdel.cpp:379-413, 1184-1332, 2138-2224, 3103-3199): n spins, d = 2^n
+ * (spin 0 the most significant bit); H = (Delta / 2) sum_s sz_s + J sy^(x)n for n >= 2, (Delta / 2)
+ * sz for n = 1 (sy^(x)n couples x with x ^ (2^n - 1) by i^(n + 2 z(x)), z = zeros of x); special = H;
+ * L_s = sm on spin s; K = -i (H - (i/2) gamma sum L^H L); the drive enters the RK propagator only. */
+int orc_floqnspins_operators(int n, double Delta, double J, double gamma, double *H, double *L, double *K)
+{
+    if (n < 1 || n > 10) return 1;
+    const int d = 1 << n;
+    const size_t dd = (size_t)d * d;
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 2 * dd * (size_t)n * sizeof(double));
+    const double hd = 0.5 * Delta;
+    for (int x = 0; x < d; x++) {
+        double sz = 0.0;
+        int z = 0;
+        for (int sp = 0; sp < n; sp++) {
+            const int b = (x >> (n - 1 - sp)) & 1;
+            sz = sz + (b ? -1.0 : 1.0);
+            z += !b;
+        }
+        H[2 * ((size_t)x * d + x)] = (n == 1) ? hd * sz : sz * hd;
+        if (n >= 2) {
+            static const double ire[4] = {1.0, 0.0, -1.0, 0.0}, iim[4] = {0.0, 1.0, 0.0, -1.0};
+            const int k = (n + 2 * z) & 3;
+            const size_t e = (size_t)x * d + (x ^ (d - 1));
+            H[2 * e] = J * ire[k];
+            H[2 * e + 1] = J * iim[k];
+        }
+        for (int sp = 0; sp < n; sp++) {
+            const int bit = 1 << (n - 1 - sp);
+            if (!(x & bit)) L[2 * (dd * sp + (size_t)(x | bit) * d + x)] = 1.0;
+        }
+    }
+    double *hp = (double *)malloc(2 * dd * sizeof(double));
+    if (!hp) return 2;
+    memcpy(hp, H, 2 * dd * sizeof(double));
+    for (int c = 0; c < n; c++) {
+        const double *Lc = L + 2 * dd * (size_t)c;
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int k = 0; k < d; k++) {
+                    const double ar = Lc[2 * ((size_t)k * d + i)], ai = Lc[2 * ((size_t)k * d + i) + 1];
+                    const double br = Lc[2 * ((size_t)k * d + j)], bi = Lc[2 * ((size_t)k * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (gamma * si);
+                hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        K[2 * e] = 0.0 + hp[2 * e + 1];
+        K[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    free(hp);
+    return 0;
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

@@ -79,6 +79,10 @@ int orc_integrable_operators(int N, int seed, int num_seeds, double tau, double 
  * L [2], K = hamiltonians_qj[0] (undriven). */
 int orc_floq2spins_operators(double D1, double D2, double J, double gamma, double *H, double *L, double *K);
 
+/* FloqManySpins (sys_id 8, newdel.cpp:379-413, 1184-1332, 2138-2224, 3103-3199): d = 2^n; H (= special),
+ * L [n], K = hamiltonians_qj[0] (undriven). */
+int orc_floqnspins_operators(int n, double Delta, double J, double gamma, double *H, double *L, double *K);
+
 /* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
  * propagator (newdel.cpp:2354-2366), complex d x d. */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);

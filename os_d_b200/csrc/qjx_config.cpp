@@ -244,6 +244,21 @@ std::string floq2spins_suffix(const RunParam &rp, const ConfigParam &cp, int pre
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string floqnspins_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    auto f = [&](const char *key) {
+        std::stringstream v;
+        v << std::setprecision(precision) << std::fixed << param(cp, key);
+        return v.str();
+    };
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_n(" << int(param(cp, "flqnsp_n")) << ")_ampl(" << f("flqnsp_ampl") << ")_freq(" << f("flqnsp_freq")
+      << ")_D(" << f("flqnsp_Delta") << ")_J(" << f("flqnsp_J") << ")_gamma(" << f("flqnsp_gamma") << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

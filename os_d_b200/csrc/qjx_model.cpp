@@ -821,3 +821,79 @@ extern "C" qjx_status qjx_build_floq2spins(double D1, double D2, double J, doubl
     }
     return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
 }
+
+// -------------------------------------------------------------------------------- FloqManySpins
+// FloqManySpinsNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp:379-413, 1184-1332, 2138-2224,
+// 3103-3199): n spins (spin 0 the most significant bit), d = 2^n; the QJ branch is undriven.
+extern "C" qjx_status qjx_build_floqnspins(int n, double Delta, double J, double gamma, double T, int deep, double *H,
+                                           double *L, double *Kout, double *Utree)
+{
+    if (n < 1 || n > 10) return QJX_ERR_INVALID_ARG;
+    if (Utree && (deep < 1 || !(T > 0.0))) return QJX_ERR_INVALID_ARG;
+    const int d = 1 << n;
+    const size_t dd = (size_t)d * d, e2 = 2 * dd;
+    cvec h(e2, 0.0), l(e2 * n, 0.0);
+    const double hd = 0.5 * Delta;
+    // i^k for the sy^(x)n entries
+    const double ire[4] = {1.0, 0.0, -1.0, 0.0}, iim[4] = {0.0, 1.0, 0.0, -1.0};
+    for (int x = 0; x < d; x++) {
+        double sz = 0.0;  // sum of the spins' sz (exact integers)
+        int z = 0;
+        for (int sp = 0; sp < n; sp++) {
+            const int b = (x >> (n - 1 - sp)) & 1;
+            sz = sz + (b ? -1.0 : 1.0);
+            z += !b;
+        }
+        // n = 1: (Delta / 2) sz; n >= 2: (sum sz) (Delta / 2) + J sy^(x)n, whose only entry in row x
+        // is column x ^ (2^n - 1), value i^(n + 2 z) (a factor -i per 0 bit, i per 1 bit)
+        h[2 * ((size_t)x * d + x)] = (n == 1) ? hd * sz : sz * hd;
+        if (n >= 2) {
+            const int k = (n + 2 * z) & 3;
+            const size_t e = (size_t)x * d + (x ^ (d - 1));
+            h[2 * e] = J * ire[k];
+            h[2 * e + 1] = J * iim[k];
+        }
+        for (int sp = 0; sp < n; sp++) {  // sigma_- = |1><0| on spin sp
+            const int bit = 1 << (n - 1 - sp);
+            if (!(x & bit)) l[2 * (dd * sp + (size_t)(x | bit) * d + x)] = 1.0;
+        }
+    }
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), e2 * n * sizeof(double));
+    if (!Kout && !Utree) return QJX_OK;
+    cvec hp(h), k(e2);
+    for (int c = 0; c < n; c++) {
+        const double *lc = l.data() + e2 * c;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < d; i++)
+            for (int j = 0; j < d; j++) {
+                double sr = 0.0, si = 0.0;
+                for (int q = 0; q < d; q++) {
+                    const double ar = lc[2 * ((size_t)q * d + i)], ai = lc[2 * ((size_t)q * d + i) + 1];
+                    const double br = lc[2 * ((size_t)q * d + j)], bi = lc[2 * ((size_t)q * d + j) + 1];
+                    sr = sr + (ar * br + ai * bi);
+                    si = si + (ar * bi - ai * br);
+                }
+                const size_t idx = (size_t)i * d + j;
+                hp[2 * idx] += 0.5 * (gamma * si);
+                hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+            }
+    }
+    for (size_t e = 0; e < dd; e++) {
+        k[2 * e] = 0.0 + hp[2 * e + 1];
+        k[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    if (Kout) std::memcpy(Kout, k.data(), e2 * sizeof(double));
+    if (!Utree) return QJX_OK;
+    // init_split_structure_floqnspins (core.cpp:10825-10871): one branch covering T / 2 per period
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
+    for (int lv = 0; lv < deep; lv++) {
+        double dt = T * 0.5;
+        for (int q = 0; q <= lv; q++) dt *= 0.5;
+        cvec scaled(e2);
+        for (size_t e = 0; e < e2; e++) scaled[e] = k[e] * dt;
+        ok = expm(d, scaled.data(), Utree + e2 * (size_t)lv) && ok;
+    }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

@@ -62,6 +62,14 @@ def suffix(cfg, prm):
     JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
     for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 8:  # FloqManySpinsOutputBehavior::suffix_param (outputter.cpp:299-326)
+        return ("_setup(%d_%d_%d)" % (8, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_n(%d)" % int(prm["flqnsp_n"])
+                + "".join("_%s(%s)" % (k, f4(prm[key])) for k, key in (
+                    ("ampl", "flqnsp_ampl"), ("freq", "flqnsp_freq"), ("D", "flqnsp_Delta"), ("J", "flqnsp_J"),
+                    ("gamma", "flqnsp_gamma")))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 7:  # Floq2SpinsOutputBehavior::suffix_param (outputter.cpp:271-299)
         return ("_setup(%d_%d_%d)" % (7, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -136,10 +144,15 @@ def spec_system(cfg, prm, deep):
     """Integrable (sys_id 5) or Floq2Spins (sys_id 7): L, special, H, period T, split trees U, K.
     Integrable: H = 0, a head of duration integrable_T with two children of the same tree;
     Floq2Spins: special = H, one undriven branch covering T / 2 per period (core.cpp:10722-10766)."""
-    if cfg.get("sys_id", 0) == 7:
-        H, L, K = O.floq2spins_operators(prm["flq2sp_Delta_1"], prm["flq2sp_Delta_2"], prm["flq2sp_J"],
-                                         prm["flq2sp_gamma"])
-        T = TWO_PI / prm["flq2sp_freq"]
+    if cfg.get("sys_id", 0) in (7, 8):  # Floq2Spins, FloqManySpins
+        if cfg.get("sys_id", 0) == 7:
+            H, L, K = O.floq2spins_operators(prm["flq2sp_Delta_1"], prm["flq2sp_Delta_2"], prm["flq2sp_J"],
+                                             prm["flq2sp_gamma"])
+            T = TWO_PI / prm["flq2sp_freq"]
+        else:
+            H, L, K = O.floqnspins_operators(int(prm["flqnsp_n"]), prm["flqnsp_Delta"], prm["flqnsp_J"],
+                                             prm["flqnsp_gamma"])
+            T = TWO_PI / prm["flqnsp_freq"]
         return L, H, H, T, O.split_tree(K, T, deep)[None], K
     L, S, K = integrable_model(prm)
     T = prm["integrable_T"]
@@ -172,7 +185,7 @@ def expected_outputs(cfg, prm, R=None):
     sfx_prm, prm = prm, dimersync_as_dimer(cfg, prm)
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
-    integ = cfg.get("sys_id", 0) in (5, 7)  # Integrable, Floq2Spins
+    integ = cfg.get("sys_id", 0) in (5, 7, 8)  # Integrable, Floq2Spins, FloqManySpins
     ps = cfg.get("sys_id", 0) == 2
     N = 0 if (mbl or integ or ps) else int(prm["N"])
     d = N if jcs else N + 1
@@ -180,7 +193,7 @@ def expected_outputs(cfg, prm, R=None):
         Nc = int(prm["mbl_Nc"])
         d = len(O.mbl_basis(Nc))
     if integ:
-        d = 4 if cfg.get("sys_id", 0) == 7 else 1 << int(prm["integrable_N"])
+        d = {7: 4, 8: 1 << int(prm.get("flqnsp_n", 0))}.get(cfg.get("sys_id", 0), 1 << int(prm.get("integrable_N", 0)))
     if ps:
         d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"])
     n = cfg["num_trajectories"]
@@ -444,7 +457,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
     nss = 2 * nsub
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
     jcs = cfg.get("sys_id", 0) == 1  # JCS: a in observable slot 0, <a^+ a>, JCS file set
-    integ = cfg.get("sys_id", 0) in (5, 7)  # Integrable, Floq2Spins: the special matrix in slot 0
+    integ = cfg.get("sys_id", 0) in (5, 7, 8)  # Integrable, Floq*Spins: the special matrix in slot 0
     spec = mbl or jcs or integ
     N = 0 if (mbl or integ) else int(prm["N"])
     d = N if jcs else N + 1
@@ -454,7 +467,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
     if jcs:
         W = float(prm["jcs_prm_alpha"])  # the spec divisor
     if integ:
-        d, W = (4 if cfg.get("sys_id", 0) == 7 else 1 << int(prm["integrable_N"])), 1.0
+        d = {7: 4, 8: 1 << int(prm.get("flqnsp_n", 0))}.get(cfg.get("sys_id", 0), 1 << int(prm.get("integrable_N", 0)))
+        W = 1.0
     n = cfg["num_trajectories"]
     half = n // 2
     deep = cfg.get("ex_deep", 16)
@@ -522,7 +536,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
                mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0,
-               chars_sys={6: 0, 7: 5}.get(cfg.get("sys_id", 0), cfg.get("sys_id", 0)))  # DimerSync, Floq2Spins
+               chars_sys={6: 0, 7: 5, 8: 5}.get(cfg.get("sys_id", 0), cfg.get("sys_id", 0)))  # DimerSync, Floq*
     if nsub:  # init_dump_periods_deep (newdel_exp.cpp:377-406)
         dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(nss)]
     else:
@@ -697,6 +711,10 @@ JCS_PARAMS = {"N": 40, "jcs_prm_alpha": 5.0, "jcs_drv_ampl": 3.2, "jcs_drv_part_
 # a Floquet two-spin system (its QJ branch is undriven: flq2sp_ampl enters the RK propagator only)
 FLOQ2_PARAMS = {"flq2sp_ampl": 1.0, "flq2sp_freq": 1.0, "flq2sp_Delta_1": 1.0, "flq2sp_Delta_2": 0.6, "flq2sp_J": 0.4,
                 "flq2sp_gamma": 0.3}
+
+# a Floquet many-spin system (3 spins; sy (x) sy (x) sy is imaginary)
+FLOQN_PARAMS = {"flqnsp_n": 3, "flqnsp_ampl": 1.0, "flqnsp_freq": 1.0, "flqnsp_Delta": 1.0, "flqnsp_J": 0.4,
+                "flqnsp_gamma": 0.3}
 
 # a DimerSync system (two drives; the QJ branches carry drive 1, the period is drive 2's)
 DIMERSYNC_PARAMS = {"dimersync_N": 16, "dimersync_prm_E": 1.0, "dimersync_prm_U": 0.5, "dimersync_prm_J": 1.0,

@@ -8,8 +8,9 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, INTEGRABLE_PARAMS, JCS_PARAMS,
-                                 LPN_PARAMS, MBL_PARAMS, PS_PARAMS, config_text, expected_outputs, params_text)
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, FLOQN_PARAMS,
+                                 INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS, PS_PARAMS, config_text,
+                                 expected_outputs, params_text)
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(os.path.dirname(q.__file__), "qjx_b200")
@@ -29,6 +30,7 @@ def run_case(tmp_path, cfg, prm):
     d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"]) if cfg.get("sys_id", 0) == 2 else d
     d = int(prm["dimersync_N"]) + 1 if cfg.get("sys_id", 0) == 6 else d
     d = 4 if cfg.get("sys_id", 0) == 7 else d
+    d = 1 << int(prm["flqnsp_n"]) if cfg.get("sys_id", 0) == 8 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -227,6 +229,17 @@ def test_floq2spins_files_match(tmp_path, task_id, is_debug):
     cfg = dict(BASE_CONFIG, sys_id=7, task_id=task_id, num_trajectories=16, num_tp_periods=1, num_obs_periods=4,
                is_debug=is_debug)
     prm = {**BASE_PARAMS, **LPN_PARAMS, **FLOQ2_PARAMS, "dump_num": 4, "jump": 2, "dump_adr_sep": 1,
+           "lpn_delta_f_high": 1e-2}
+    run_case(tmp_path, cfg, prm)
+
+
+@pytest.mark.parametrize("task_id,is_debug", [(1, 1), (7, 0)])
+def test_floqnspins_files_match(tmp_path, task_id, is_debug):
+    """FloqManySpins (sys_id 8): 3 spins, H = (Delta/2) sum sz + J sy sy sy (imaginary), sigma_- on
+    each spin, the undriven QJ branch (newdel.cpp:379-413, 1184-1332, 2138-2224, 3103-3199)."""
+    cfg = dict(BASE_CONFIG, sys_id=8, task_id=task_id, num_trajectories=16, num_tp_periods=1, num_obs_periods=4,
+               is_debug=is_debug)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **FLOQN_PARAMS, "dump_num": 4, "jump": 2, "dump_adr_sep": 1,
            "lpn_delta_f_high": 1e-2}
     run_case(tmp_path, cfg, prm)
 
