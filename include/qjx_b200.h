@@ -332,6 +332,13 @@ qjx_status qjx_build_floq2spins(double D1, double D2, double J, double gamma, do
  * T / 2 per period (init_split_structure_floqnspins, core.cpp:10825-10871).  Any output may be NULL. */
 qjx_status qjx_build_floqnspins(int n, double Delta, double J, double gamma, double T, int deep, double *H, double *L,
                                 double *K, double *Utree);
+/* The Floquet spin-photon system (sys_id 9; FloqSpinPhNewDelBehaviour, newdel.cpp:414-449, 1334-1452,
+ * 2226-2284, 3201-3297), QJ branch: photons (x) spin (index 2 k + s), d = 2 (n_ph + 1), H = (Delta / 2)
+ * sz + (Omega / 2)(a^+ sm + a sp) (also the spec observable), L [1] = a (x) 1, K = -i (H - (i/2) gamma
+ * L^H L), jump rate 1; Utree [deep][d][d] for one branch covering T / 2 per period
+ * (init_split_structure_flq_sp_ph, core.cpp:10928-10974).  Any output pointer may be NULL. */
+qjx_status qjx_build_floqspph(int n_ph, double Delta, double Omega, double gamma, double T, int deep, double *H,
+                              double *L, double *K, double *Utree);
 /* The MBL imbalance of n probability rows adr [n][d] (get_imbalance_mbl, experiment.cpp:1753-1800). */
 qjx_status qjx_mbl_imbalance(int Nc, int n, const double *adr, double *out);
 /* qjx_build_dimer with the split tree of the deep tasks' sub-period T / (2 deep_num_steps)

@@ -69,6 +69,7 @@ def lib():
         L.orc_ps_operators.argtypes = [C.c_int] * 2 + [C.c_double] * 4 + [C.c_int, C.c_double] + [c_double_p] * 6
         L.orc_floq2spins_operators.argtypes = [C.c_double] * 4 + [c_double_p] * 3
         L.orc_floqnspins_operators.argtypes = [C.c_int] + [C.c_double] * 3 + [c_double_p] * 3
+        L.orc_floqspph_operators.argtypes = [C.c_int] + [C.c_double] * 3 + [c_double_p] * 3
         L.orc_integrable_operators.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [c_double_p] * 3
         L.orc_split_tree.argtypes = [C.c_int, c_double_p, C.c_double, C.c_int, c_double_p]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -174,6 +175,14 @@ def floqnspins_operators(n, Delta, J, gamma):
     d = 1 << n
     H, K, L = _cplx((d, d)), _cplx((d, d)), _cplx((n, d, d))
     assert lib().orc_floqnspins_operators(n, Delta, J, gamma, _dp(H), _dp(L), _dp(K)) == 0
+    return H, L, K
+
+
+def floqspph_operators(n_ph, Delta, Omega, gamma):
+    """FloqSpinPh (sys_id 9): H (= special), L [1], K = hamiltonians_qj[0] (d = 2 (n_ph + 1))."""
+    d = 2 * (n_ph + 1)
+    H, K, L = _cplx((d, d)), _cplx((d, d)), _cplx((1, d, d))
+    assert lib().orc_floqspph_operators(n_ph, Delta, Omega, gamma, _dp(H), _dp(L), _dp(K)) == 0
     return H, L, K
 
 

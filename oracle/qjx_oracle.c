@@ -604,6 +604,51 @@ int orc_floqnspins_operators(int n, double Delta, double J, double gamma, double
     return 0;
 }
 
+/* FloqSpinPh (sys_id 9, newdel.cpp:414-449, 1334-1452, 2226-2284, 3201-3297): photons (x) spin, index
+ * 2 k + s, d = 2 (n_ph + 1); H = (Delta / 2) 1 (x) sz + (Omega / 2)(a^+ (x) sm + a (x) sp), special = H,
+ * L = a (x) 1, K = -i (H - (i/2) gamma L^H L); the drive enters the RK propagator only. */
+int orc_floqspph_operators(int n_ph, double Delta, double Omega, double gamma, double *H, double *L, double *K)
+{
+    if (n_ph < 1) return 1;
+    const int d = 2 * (n_ph + 1);
+    const size_t dd = (size_t)d * d;
+    memset(H, 0, 2 * dd * sizeof(double));
+    memset(L, 0, 2 * dd * sizeof(double));
+    const double hd = 0.5 * Delta, ho = 0.5 * Omega;
+    for (int k = 0; k <= n_ph; k++) {
+        H[2 * ((size_t)(2 * k) * d + 2 * k)] = hd * 1.0;
+        H[2 * ((size_t)(2 * k + 1) * d + 2 * k + 1)] = hd * -1.0;
+    }
+    for (int k = 0; k < n_ph; k++) {
+        const double a = sqrt((double)(k + 1));
+        H[2 * ((size_t)(2 * (k + 1) + 1) * d + 2 * k)] = ho * a; /* a^+ (x) sm: (k, 0) -> (k + 1, 1) */
+        H[2 * ((size_t)(2 * k) * d + 2 * (k + 1) + 1)] = ho * a; /* a (x) sp: (k + 1, 1) -> (k, 0) */
+        for (int sp = 0; sp < 2; sp++) L[2 * ((size_t)(2 * k + sp) * d + 2 * (k + 1) + sp)] = a;
+    }
+    double *hp = (double *)malloc(2 * dd * sizeof(double));
+    if (!hp) return 2;
+    memcpy(hp, H, 2 * dd * sizeof(double));
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            double sr = 0.0, si = 0.0;
+            for (int k = 0; k < d; k++) {
+                const double ar = L[2 * ((size_t)k * d + i)], ai = L[2 * ((size_t)k * d + i) + 1];
+                const double br = L[2 * ((size_t)k * d + j)], bi = L[2 * ((size_t)k * d + j) + 1];
+                sr = sr + (ar * br + ai * bi);
+                si = si + (ar * bi - ai * br);
+            }
+            const size_t idx = (size_t)i * d + j;
+            hp[2 * idx] += 0.5 * (gamma * si);
+            hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+        }
+    for (size_t e = 0; e < dd; e++) {
+        K[2 * e] = 0.0 + hp[2 * e + 1];
+        K[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    free(hp);
+    return 0;
+}
+
 /* H_eff = H - (i/2) gamma L^H L (newdel.cpp:2327-2352), the RK propagator's non_drv_part */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff)
 {

@@ -83,6 +83,10 @@ int orc_floq2spins_operators(double D1, double D2, double J, double gamma, doubl
  * L [n], K = hamiltonians_qj[0] (undriven). */
 int orc_floqnspins_operators(int n, double Delta, double J, double gamma, double *H, double *L, double *K);
 
+/* FloqSpinPh (sys_id 9, newdel.cpp:414-449, 1334-1452, 2226-2284, 3201-3297): d = 2 (n_ph + 1); H (= special),
+ * L = a (x) 1, K = hamiltonians_qj[0] (undriven). */
+int orc_floqspph_operators(int n_ph, double Delta, double Omega, double gamma, double *H, double *L, double *K);
+
 /* H_eff = H - (i/2) gamma L^H L, gamma = g / N (newdel.cpp:2293-2352): the non_drv_part of the RK
  * propagator (newdel.cpp:2354-2366), complex d x d. */
 int orc_dimer_heff(int N, double J, double U, double E, double g, double *Heff);

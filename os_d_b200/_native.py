@@ -21,7 +21,7 @@ EXPORTS = [
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
     "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
-    "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_build_ps", "qjx_build_floq2spins", "qjx_build_floqnspins", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
+    "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_build_ps", "qjx_build_floq2spins", "qjx_build_floqnspins", "qjx_build_floqspph", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
     "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_bases", "qjx_run_sub_periods", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
@@ -123,6 +123,7 @@ def lib():
                                    + [c_double_p] * 6)
         L.qjx_build_floq2spins.argtypes = [C.c_double] * 5 + [C.c_int] + [c_double_p] * 4
         L.qjx_build_floqnspins.argtypes = [C.c_int] + [C.c_double] * 4 + [C.c_int] + [c_double_p] * 4
+        L.qjx_build_floqspph.argtypes = [C.c_int] + [C.c_double] * 4 + [C.c_int] + [c_double_p] * 4
         L.qjx_build_integrable.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int] + [c_double_p] * 4
         L.qjx_build_dimer_rk.argtypes = [C.c_int] + [C.c_double] * 4 + [c_double_p] * 2
         L.qjx_fb_build_dimer.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -238,6 +239,16 @@ def build_floqnspins(n, Delta, J, gamma, T, deep):
                  np.zeros((deep, d, d), np.complex128))
     check(lib().qjx_build_floqnspins(n, Delta, J, gamma, T, deep, dp(H), dp(Lm), None, dp(Ut)),
           what="qjx_build_floqnspins")
+    return H, Lm, Ut
+
+
+def build_floqspph(n_ph, Delta, Omega, gamma, T, deep):
+    """Floquet spin-photon system (sys_id 9), QJ branch: H (= special), L [1], split tree [deep][d][d]."""
+    d = 2 * (n_ph + 1)
+    H, Lm, Ut = (np.zeros((d, d), np.complex128), np.zeros((1, d, d), np.complex128),
+                 np.zeros((deep, d, d), np.complex128))
+    check(lib().qjx_build_floqspph(n_ph, Delta, Omega, gamma, T, deep, dp(H), dp(Lm), None, dp(Ut)),
+          what="qjx_build_floqspph")
     return H, Lm, Ut
 
 

@@ -259,6 +259,22 @@ std::string floqnspins_suffix(const RunParam &rp, const ConfigParam &cp, int pre
     return s.str() + lpn_suffix(rp, cp) + ".txt";
 }
 
+std::string floqspph_suffix(const RunParam &rp, const ConfigParam &cp, int precision)
+{
+    std::stringstream s;
+    auto f = [&](const char *key) {
+        std::stringstream v;
+        v << std::setprecision(precision) << std::fixed << param(cp, key);
+        return v.str();
+    };
+    s << "_setup(" << rp.sys_id << "_" << rp.task_id << "_" << rp.prop_id << ")";
+    s << "_rnd(" << cp.seed << "_" << cp.mns << ")";
+    s << "_nph(" << int(param(cp, "flq_sp_ph_n_ph")) << ")_ampl(" << f("flq_sp_ph_ampl") << ")_freq("
+      << f("flq_sp_ph_freq") << ")_D(" << f("flq_sp_ph_Delta") << ")_O(" << f("flq_sp_ph_Omega") << ")_gamma("
+      << f("flq_sp_ph_gamma") << ")";
+    return s.str() + lpn_suffix(rp, cp) + ".txt";
+}
+
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods)
 {
     std::vector<int> out;

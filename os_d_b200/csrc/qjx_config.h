@@ -59,6 +59,8 @@ std::string dimersync_suffix(const RunParam &rp, const ConfigParam &cp, int prec
 std::string floq2spins_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 // FloqManySpinsOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:299-326)
 std::string floqnspins_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
+// FloqSpinPhOutputBehavior::suffix_param (source/cpp/QJX/QJX/outputter.cpp:326-353)
+std::string floqspph_suffix(const RunParam &rp, const ConfigParam &cp, int precision = 4);
 
 // init_dump_periods (source/cpp/QJX/QJX/newdel_exp.cpp:408-455); empty on a bad dump_type.
 std::vector<int> dump_periods(int dump_type, int dump_num, int num_obs_periods);

@@ -5,7 +5,7 @@
 // Integrable (sys_id 5) systems, the Std task with the QJ propagator for PS (sys_id 2), and the
 // Std and LpnMult tasks with the QJ propagator for DimerSync (sys_id 6, whose QJ branches are the
 // dimer's with its first drive; the second drive enters the RK propagator only), and Floq2Spins
-// and FloqManySpins (sys_id 7, 8: Std and LpnMult with their undriven QJ branches).
+// FloqManySpins and FloqSpinPh (sys_id 7, 8, 9: Std and LpnMult with their undriven QJ branches).
 //
 // Flow of the generic main + Processor::process (source/cpp/QJX/QJX/main.cpp:3-192,
 // processor.cpp:50-76): read ./config.txt and ./params.txt, build the dimer model, run the
@@ -426,16 +426,16 @@ int main(int argc, char **argv)
     if (!read_params(cp, fn_params)) std::cout << "Unable to open file" << std::endl << "Init with default params" << std::endl;
     std::cout << params_echo(rp, cp);
 
-    if (rp.sys_id < 0 || rp.sys_id > 8 || rp.sys_id == 4)
+    if (rp.sys_id < 0 || rp.sys_id > 9 || rp.sys_id == 4)
         die("Wrong sys_id: " + std::to_string(rp.sys_id) +
             " (this engine runs the dimer (0), JCS (1), PS (2), MBL (3), Integrable (5), DimerSync (6), Floq2Spins "
-            "(7) and FloqManySpins (8) systems)");
+            "(7), FloqManySpins (8) and FloqSpinPh (9) systems)");
     const bool jcs = rp.sys_id == 1;  // JCS, MBL, Integrable: Std and LpnMult with the QJ propagator
     const bool mbl = rp.sys_id == 3;
     // Floq2Spins, FloqManySpins: their QJ branch and observables follow the Integrable pattern
     // (spec = <special>)
-    const bool floq2 = rp.sys_id == 7, floqn = rp.sys_id == 8;
-    const bool integ = rp.sys_id == 5 || floq2 || floqn;
+    const bool floq2 = rp.sys_id == 7, floqn = rp.sys_id == 8, floqp = rp.sys_id == 9;
+    const bool integ = rp.sys_id == 5 || floq2 || floqn || floqp;
     const bool ps = rp.sys_id == 2;  // PS: the Std task with the QJ propagator
     const bool dsync = rp.sys_id == 6;
     if (dsync && ((rp.task_id != 1 && rp.task_id != 7) || rp.prop_id != 0))
@@ -459,6 +459,7 @@ int main(int argc, char **argv)
                        : mbl ? mbl_suffix(rp, cp, 4)
                        : floq2 ? floq2spins_suffix(rp, cp, 4)
                        : floqn ? floqnspins_suffix(rp, cp, 4)
+                       : floqp ? floqspph_suffix(rp, cp, 4)
                        : integ ? integrable_suffix(rp, cp, 4)
                        : ps    ? ps_suffix(rp, cp, 4)
                        : dsync ? dimersync_suffix(rp, cp, 4)
@@ -484,22 +485,27 @@ int main(int argc, char **argv)
         if (rp.sys_id == 5 && (Ni < 3 || Ni > 10)) die("integrable_N must be in [3, 10]");
         const int nfl = floqn ? int(param(cp, "flqnsp_n")) : 0;
         if (floqn && (nfl < 1 || nfl > 10)) die("flqnsp_n must be in [1, 10]");
+        const int nph = floqp ? int(param(cp, "flq_sp_ph_n_ph")) : 0;
+        if (floqp && (nph < 1 || nph > 511)) die("flq_sp_ph_n_ph must be in [1, 511]");
         // MBL: C(Nc, Nc/2) basis words and Nc (diss_type 0) or Nc - 1 (diss_type 1) jump channels
         const int Nc = mbl ? int(param(cp, "mbl_Nc")) : 0, mbl_dt = mbl ? int(param(cp, "diss_type")) : 0;
         int d_mbl = 0, nd_mbl = 0;
         if (mbl && qjx_mbl_size(Nc, mbl_dt, &d_mbl, &nd_mbl) != QJX_OK)
             die("mbl_Nc must be even and in [2, 24], diss_type 0 or 1");
         // the dimer has N + 1 Fock states; the JCS oscillator is truncated at N states (newdel.cpp:110)
-        const int d = mbl ? d_mbl : floq2 ? 4 : floqn ? (1 << nfl) : integ ? (1 << Ni) : ps ? (1 << ps_ns) * ps_np
+        const int d = mbl ? d_mbl : floq2 ? 4 : floqn ? (1 << nfl) : floqp ? 2 * (nph + 1) : integ ? (1 << Ni)
+                    : ps ? (1 << ps_ns) * ps_np
                     : jcs ? N : N + 1;
         const int n = cp.num_trajectories, deep = cp.ex_deep;
-        const int num_diss = mbl ? nd_mbl : floq2 ? 2 : floqn ? nfl : integ ? Ni : ps ? (ps_dt == 0 ? 1 : 1 + ps_ns) : 1;
+        const int num_diss = mbl ? nd_mbl : floq2 ? 2 : floqn ? nfl : floqp ? 1 : integ ? Ni
+                             : ps ? (ps_dt == 0 ? 1 : 1 + ps_ns) : 1;
         // JCS and PS run each drive part as two halves of its tree (init_split_structure_jcs / _ps,
         // core.cpp:10086-10157, 10234-10305: counter 2): four engine branches [K_0, K_0, K_1, K_1]
         // Floq2Spins: one branch of T / 2 per period (init_split_structure_floq2spins)
-        const int nbr = (ps || jcs) ? 4 : (floq2 || floqn) ? 1 : 2;
+        const int nbr = (ps || jcs) ? 4 : (floq2 || floqn || floqp) ? 1 : 2;
         const double floq2_T = floq2   ? 2.0 * 3.1415926535897932384626433832795 / param(cp, "flq2sp_freq")
                                : floqn ? 2.0 * 3.1415926535897932384626433832795 / param(cp, "flqnsp_freq")
+                               : floqp ? 2.0 * 3.1415926535897932384626433832795 / param(cp, "flq_sp_ph_freq")
                                        : 0.0;
         // DimerSync (newdel.cpp:39-95, 500-563, 2390-2498): the dimer's operators under its own keys,
         // drive 1 in the QJ branches, the period of drive dimersync_main_period
@@ -581,6 +587,11 @@ int main(int argc, char **argv)
                                        param(cp, "flq2sp_gamma"), floq2_T, deep, H.data(), L.data(), K.data(),
                                        Ut.data()),
                   nullptr, "qjx_build_floq2spins");
+            Hd = H;
+        } else if (floqp) {  // as Floq2Spins, for a spin and a photon mode
+            check(qjx_build_floqspph(nph, param(cp, "flq_sp_ph_Delta"), param(cp, "flq_sp_ph_Omega"),
+                                     param(cp, "flq_sp_ph_gamma"), floq2_T, deep, H.data(), L.data(), K.data(), Ut.data()),
+                  nullptr, "qjx_build_floqspph");
             Hd = H;
         } else if (floqn) {  // as Floq2Spins, for n spins
             check(qjx_build_floqnspins(nfl, param(cp, "flqnsp_Delta"), param(cp, "flqnsp_J"), param(cp, "flqnsp_gamma"),
@@ -671,7 +682,7 @@ int main(int argc, char **argv)
         cfg.T = jcs     ? jcs_alpha
                 : ps    ? ps_alpha
                 : mbl   ? param(cp, "mbl_T")
-                : (floq2 || floqn) ? floq2_T
+                : (floq2 || floqn || floqp) ? floq2_T
                 : integ ? param(cp, "integrable_T")
                         : 2.0 * 3.1415926535897932384626433832795 / omega;
         // JCS: part b's head is jcs_drv_part_b * alpha, run as two halves (init_split_structure_jcs,
@@ -717,7 +728,7 @@ int main(int argc, char **argv)
         if (rp.task_id == 7 || rp.task_id == 8) {
             // DimerSync's Lyapunov characteristics are the dimer's (DimerSyncCoreBehaviour, core.cpp:1812-1997)
             // Floq2Spins's are the Integrable ones (spec only; core.cpp:7546-7690)
-            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, dsync ? 0 : (floq2 || floqn) ? 5 : rp.sys_id, Nc, jcs ? jcs_alpha : mbl ? mbl_W : 1.0,
+            run_lpn_mult(h, rp, cp, cfg, H, d, num_robs, robs_seed, dsync ? 0 : (floq2 || floqn || floqp) ? 5 : rp.sys_id, Nc, jcs ? jcs_alpha : mbl ? mbl_W : 1.0,
                          jcs ? jcs_p1 * jcs_alpha + jcs_p2 * jcs_alpha : cfg.T, nsub);
             qjx_destroy(h);
             return 0;

@@ -897,3 +897,62 @@ extern "C" qjx_status qjx_build_floqnspins(int n, double Delta, double J, double
     }
     return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
 }
+
+// ----------------------------------------------------------------------------------- FloqSpinPh
+// FloqSpinPhNewDelBehaviour (source/cpp/QJX/QJX/newdel.cpp:414-449, 1334-1452, 2226-2284, 3201-3297):
+// photons (x) spin, basis index 2 k + s, d = 2 (n_ph + 1); the QJ branch is undriven.
+extern "C" qjx_status qjx_build_floqspph(int n_ph, double Delta, double Omega, double gamma, double T, int deep,
+                                         double *H, double *L, double *Kout, double *Utree)
+{
+    if (n_ph < 1 || 2 * (n_ph + 1) > 4096) return QJX_ERR_INVALID_ARG;
+    if (Utree && (deep < 1 || !(T > 0.0))) return QJX_ERR_INVALID_ARG;
+    const int d = 2 * (n_ph + 1);
+    const size_t dd = (size_t)d * d, e2 = 2 * dd;
+    cvec h(e2, 0.0), l(e2, 0.0);
+    const double hd = 0.5 * Delta, ho = 0.5 * Omega;
+    for (int k = 0; k <= n_ph; k++) {  // (Delta / 2) 1 (x) sz
+        h[2 * ((size_t)(2 * k) * d + 2 * k)] = hd * 1.0;
+        h[2 * ((size_t)(2 * k + 1) * d + 2 * k + 1)] = hd * -1.0;
+    }
+    for (int k = 0; k < n_ph; k++) {
+        const double a = std::sqrt(double(k + 1));
+        h[2 * ((size_t)(2 * (k + 1) + 1) * d + 2 * k)] = ho * a;  // (Omega / 2) a^+ (x) sm
+        h[2 * ((size_t)(2 * k) * d + 2 * (k + 1) + 1)] = ho * a;  // (Omega / 2) a (x) sp
+        for (int sp = 0; sp < 2; sp++) l[2 * ((size_t)(2 * k + sp) * d + 2 * (k + 1) + sp)] = a;  // a (x) 1
+    }
+    if (H) std::memcpy(H, h.data(), e2 * sizeof(double));
+    if (L) std::memcpy(L, l.data(), e2 * sizeof(double));
+    if (!Kout && !Utree) return QJX_OK;
+    cvec hp(h), k(e2);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) {
+            double sr = 0.0, si = 0.0;
+            for (int q = 0; q < d; q++) {
+                const double ar = l[2 * ((size_t)q * d + i)], ai = l[2 * ((size_t)q * d + i) + 1];
+                const double br = l[2 * ((size_t)q * d + j)], bi = l[2 * ((size_t)q * d + j) + 1];
+                sr = sr + (ar * br + ai * bi);
+                si = si + (ar * bi - ai * br);
+            }
+            const size_t idx = (size_t)i * d + j;
+            hp[2 * idx] += 0.5 * (gamma * si);
+            hp[2 * idx + 1] -= 0.5 * (gamma * sr);
+        }
+    for (size_t e = 0; e < dd; e++) {
+        k[2 * e] = 0.0 + hp[2 * e + 1];
+        k[2 * e + 1] = 0.0 - hp[2 * e];
+    }
+    if (Kout) std::memcpy(Kout, k.data(), e2 * sizeof(double));
+    if (!Utree) return QJX_OK;
+    // init_split_structure_flq_sp_ph (core.cpp:10928-10974): one branch covering T / 2 per period
+    bool ok = true;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
+    for (int lv = 0; lv < deep; lv++) {
+        double dt = T * 0.5;
+        for (int q = 0; q <= lv; q++) dt *= 0.5;
+        cvec scaled(e2);
+        for (size_t e = 0; e < e2; e++) scaled[e] = k[e] * dt;
+        ok = expm(d, scaled.data(), Utree + e2 * (size_t)lv) && ok;
+    }
+    return ok ? QJX_OK : QJX_ERR_INVALID_ARG;
+}

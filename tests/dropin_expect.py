@@ -62,6 +62,14 @@ def suffix(cfg, prm):
     JCSOutputBehavior::suffix_param for sys_id 1 (outputter.cpp:95-133); MBLOutputBehavior::suffix_param
     for sys_id 3 (outputter.cpp:176-212)."""
     f4 = lambda x: format(float(x), "0.4f")  # noqa: E731
+    if cfg.get("sys_id", 0) == 9:  # FloqSpinPhOutputBehavior::suffix_param (outputter.cpp:326-353)
+        return ("_setup(%d_%d_%d)" % (9, cfg.get("task_id", 0), cfg.get("prop_id", 0))
+                + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
+                + "_nph(%d)" % int(prm["flq_sp_ph_n_ph"])
+                + "".join("_%s(%s)" % (k, f4(prm[key])) for k, key in (
+                    ("ampl", "flq_sp_ph_ampl"), ("freq", "flq_sp_ph_freq"), ("D", "flq_sp_ph_Delta"),
+                    ("O", "flq_sp_ph_Omega"), ("gamma", "flq_sp_ph_gamma")))
+                + (lpn_suffix(prm) if cfg.get("task_id", 0) in (7, 8) else "") + ".txt")
     if cfg.get("sys_id", 0) == 8:  # FloqManySpinsOutputBehavior::suffix_param (outputter.cpp:299-326)
         return ("_setup(%d_%d_%d)" % (8, cfg.get("task_id", 0), cfg.get("prop_id", 0))
                 + "_rnd(%d_%d)" % (cfg.get("seed", 0), cfg.get("mns", 1000000))
@@ -144,8 +152,12 @@ def spec_system(cfg, prm, deep):
     """Integrable (sys_id 5) or Floq2Spins (sys_id 7): L, special, H, period T, split trees U, K.
     Integrable: H = 0, a head of duration integrable_T with two children of the same tree;
     Floq2Spins: special = H, one undriven branch covering T / 2 per period (core.cpp:10722-10766)."""
-    if cfg.get("sys_id", 0) in (7, 8):  # Floq2Spins, FloqManySpins
-        if cfg.get("sys_id", 0) == 7:
+    if cfg.get("sys_id", 0) in (7, 8, 9):  # Floq2Spins, FloqManySpins, FloqSpinPh
+        if cfg.get("sys_id", 0) == 9:
+            H, L, K = O.floqspph_operators(int(prm["flq_sp_ph_n_ph"]), prm["flq_sp_ph_Delta"], prm["flq_sp_ph_Omega"],
+                                           prm["flq_sp_ph_gamma"])
+            T = TWO_PI / prm["flq_sp_ph_freq"]
+        elif cfg.get("sys_id", 0) == 7:
             H, L, K = O.floq2spins_operators(prm["flq2sp_Delta_1"], prm["flq2sp_Delta_2"], prm["flq2sp_J"],
                                              prm["flq2sp_gamma"])
             T = TWO_PI / prm["flq2sp_freq"]
@@ -185,7 +197,7 @@ def expected_outputs(cfg, prm, R=None):
     sfx_prm, prm = prm, dimersync_as_dimer(cfg, prm)
     jcs = cfg.get("sys_id", 0) == 1
     mbl = cfg.get("sys_id", 0) == 3
-    integ = cfg.get("sys_id", 0) in (5, 7, 8)  # Integrable, Floq2Spins, FloqManySpins
+    integ = cfg.get("sys_id", 0) in (5, 7, 8, 9)  # Integrable and the Floquet systems
     ps = cfg.get("sys_id", 0) == 2
     N = 0 if (mbl or integ or ps) else int(prm["N"])
     d = N if jcs else N + 1
@@ -193,7 +205,8 @@ def expected_outputs(cfg, prm, R=None):
         Nc = int(prm["mbl_Nc"])
         d = len(O.mbl_basis(Nc))
     if integ:
-        d = {7: 4, 8: 1 << int(prm.get("flqnsp_n", 0))}.get(cfg.get("sys_id", 0), 1 << int(prm.get("integrable_N", 0)))
+        d = {7: 4, 8: 1 << int(prm.get("flqnsp_n", 0)), 9: 2 * (int(prm.get("flq_sp_ph_n_ph", 0)) + 1)}.get(
+            cfg.get("sys_id", 0), 1 << int(prm.get("integrable_N", 0)))
     if ps:
         d = (1 << int(prm["ps_num_spins"])) * int(prm["ps_num_photons_states"])
     n = cfg["num_trajectories"]
@@ -457,7 +470,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
     nss = 2 * nsub
     mbl = cfg.get("sys_id", 0) == 3  # MBL: H in observable slot 0, imbalances, MBL file set
     jcs = cfg.get("sys_id", 0) == 1  # JCS: a in observable slot 0, <a^+ a>, JCS file set
-    integ = cfg.get("sys_id", 0) in (5, 7, 8)  # Integrable, Floq*Spins: the special matrix in slot 0
+    integ = cfg.get("sys_id", 0) in (5, 7, 8, 9)  # Integrable, Floquet: the special matrix in slot 0
     spec = mbl or jcs or integ
     N = 0 if (mbl or integ) else int(prm["N"])
     d = N if jcs else N + 1
@@ -467,7 +480,8 @@ def expected_lpn_outputs(cfg, prm, R=None):
     if jcs:
         W = float(prm["jcs_prm_alpha"])  # the spec divisor
     if integ:
-        d = {7: 4, 8: 1 << int(prm.get("flqnsp_n", 0))}.get(cfg.get("sys_id", 0), 1 << int(prm.get("integrable_N", 0)))
+        d = {7: 4, 8: 1 << int(prm.get("flqnsp_n", 0)), 9: 2 * (int(prm.get("flq_sp_ph_n_ph", 0)) + 1)}.get(
+            cfg.get("sys_id", 0), 1 << int(prm.get("integrable_N", 0)))
         W = 1.0
     n = cfg["num_trajectories"]
     half = n // 2
@@ -536,7 +550,7 @@ def expected_lpn_outputs(cfg, prm, R=None):
                delta_f_high=float(prm["lpn_delta_f_high"]), delta_f_low=float(prm["lpn_delta_f_low"]),
                per_period=int(prm["lambda_per_periods"]) != 0, max_energy=max_energy,
                mbl_Nc=Nc if mbl else 0, spec_div=W if spec else 1.0,
-               chars_sys={6: 0, 7: 5, 8: 5}.get(cfg.get("sys_id", 0), cfg.get("sys_id", 0)))  # DimerSync, Floq*
+               chars_sys={6: 0, 7: 5, 8: 5, 9: 5}.get(cfg.get("sys_id", 0), cfg.get("sys_id", 0)))  # DimerSync, Floq*
     if nsub:  # init_dump_periods_deep (newdel_exp.cpp:377-406)
         dp = [0] + [p for p in range(cfg.get("num_obs_periods", 10)) for _ in range(nss)]
     else:
@@ -715,6 +729,12 @@ FLOQ2_PARAMS = {"flq2sp_ampl": 1.0, "flq2sp_freq": 1.0, "flq2sp_Delta_1": 1.0, "
 # a Floquet many-spin system (3 spins; sy (x) sy (x) sy is imaginary)
 FLOQN_PARAMS = {"flqnsp_n": 3, "flqnsp_ampl": 1.0, "flqnsp_freq": 1.0, "flqnsp_Delta": 1.0, "flqnsp_J": 0.4,
                 "flqnsp_gamma": 0.3}
+
+# a Floquet spin-photon system (up to 8 photons, d = 18).  Its state |0 photons, spin 1> is dark (no loss,
+# isolated), where repeated matvecs let the norm drift an ulp above 1, which the reference rejects
+# ("norm more than 1", experiment.cpp:1247-1251): the test starts high in the photon ladder with weak loss
+FLOQP_PARAMS = {"flq_sp_ph_n_ph": 8, "flq_sp_ph_ampl": 1.0, "flq_sp_ph_freq": 1.0, "flq_sp_ph_Delta": 1.0,
+                "flq_sp_ph_Omega": 0.5, "flq_sp_ph_gamma": 0.02}
 
 # a DimerSync system (two drives; the QJ branches carry drive 1, the period is drive 2's)
 DIMERSYNC_PARAMS = {"dimersync_N": 16, "dimersync_prm_E": 1.0, "dimersync_prm_U": 0.5, "dimersync_prm_J": 1.0,

@@ -5,7 +5,7 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, FLOQN_PARAMS,
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, FLOQN_PARAMS, FLOQP_PARAMS,
                                  INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS, PS_PARAMS, config_text, params_text,
                                  suffix)
 
@@ -105,11 +105,11 @@ def test_lpn_mult_deep_checks(tmp_path):
 
 
 SYS_PARAMS = {1: JCS_PARAMS, 2: PS_PARAMS, 3: MBL_PARAMS, 5: INTEGRABLE_PARAMS, 6: DIMERSYNC_PARAMS, 7: FLOQ2_PARAMS,
-              8: FLOQN_PARAMS}
+              8: FLOQN_PARAMS, 9: FLOQP_PARAMS}
 
 
 @pytest.mark.parametrize("sys_id,task_id", [(1, 7), (3, 7), (5, 7), (5, 1), (2, 1), (6, 1), (6, 7), (7, 1), (7, 7),
-                                            (8, 1), (8, 7)])
+                                            (8, 1), (8, 7), (9, 1), (9, 7)])
 def test_jcs_mbl_integrable_suffix(tmp_path, sys_id, task_id):
     """suffix_param (+ suffix_lpn for LpnMult) of JCS, MBL and Integrable (outputter.cpp:95-269,
     371-381); Integrable prints tau and k as integers."""
@@ -121,7 +121,7 @@ def test_jcs_mbl_integrable_suffix(tmp_path, sys_id, task_id):
     assert line[len("fn_suffix = "):] == suffix(cfg, prm) and ("_lpn(" in line) == (task_id == 7)
 
 
-@pytest.mark.parametrize("key,val", [("sys_id", 4), ("sys_id", 9), ("task_id", 9), ("prop_id", 2)])
+@pytest.mark.parametrize("key,val", [("sys_id", 4), ("sys_id", 10), ("task_id", 9), ("prop_id", 2)])
 def test_unsupported_ids_exit_with_error(tmp_path, key, val):
     r = check(tmp_path, dict(BASE_CONFIG, **{key: val}), BASE_PARAMS)
     assert r.returncode != 0 and "Error: Wrong " + key in r.stdout

@@ -8,7 +8,7 @@ import subprocess
 import pytest
 
 import os_d_b200 as q
-from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, FLOQN_PARAMS,
+from tests.dropin_expect import (BASE_CONFIG, BASE_PARAMS, DIMERSYNC_PARAMS, FLOQ2_PARAMS, FLOQN_PARAMS, FLOQP_PARAMS,
                                  INTEGRABLE_PARAMS, JCS_PARAMS, LPN_PARAMS, MBL_PARAMS, PS_PARAMS, config_text,
                                  expected_outputs, params_text)
 
@@ -31,6 +31,7 @@ def run_case(tmp_path, cfg, prm):
     d = int(prm["dimersync_N"]) + 1 if cfg.get("sys_id", 0) == 6 else d
     d = 4 if cfg.get("sys_id", 0) == 7 else d
     d = 1 << int(prm["flqnsp_n"]) if cfg.get("sys_id", 0) == 8 else d
+    d = 2 * (int(prm["flq_sp_ph_n_ph"]) + 1) if cfg.get("sys_id", 0) == 9 else d
     R = q.random_observables(d, int(prm["num_random_obs"]), int(prm["random_obs_seed"]),
                              int(prm["random_obs_mns"]), int(prm["random_obs_type"]))
     exp = expected_outputs(cfg, prm, R)
@@ -241,6 +242,17 @@ def test_floqnspins_files_match(tmp_path, task_id, is_debug):
                is_debug=is_debug)
     prm = {**BASE_PARAMS, **LPN_PARAMS, **FLOQN_PARAMS, "dump_num": 4, "jump": 2, "dump_adr_sep": 1,
            "lpn_delta_f_high": 1e-2}
+    run_case(tmp_path, cfg, prm)
+
+
+@pytest.mark.parametrize("task_id,is_debug", [(1, 1), (7, 0)])
+def test_floqspph_files_match(tmp_path, task_id, is_debug):
+    """FloqSpinPh (sys_id 9): a spin and 9 photon states, photon loss a, the undriven QJ branch
+    (newdel.cpp:414-449, 1334-1452, 2226-2284, 3201-3297)."""
+    cfg = dict(BASE_CONFIG, sys_id=9, task_id=task_id, num_trajectories=16, num_tp_periods=1, num_obs_periods=4,
+               is_debug=is_debug)
+    prm = {**BASE_PARAMS, **LPN_PARAMS, **FLOQP_PARAMS, "dump_num": 4, "jump": 2, "dump_adr_sep": 1,
+           "lpn_delta_f_high": 1e-2, "start_state": 16}
     run_case(tmp_path, cfg, prm)
 
 
