@@ -3,9 +3,15 @@
 
 Workload: the driven dissipative Bose dimer at N = 200 (Hilbert dim 201), 10^4 trajectories
 per GPU, ex_deep 16, QJ propagator, complex FP64 end to end (the plain drop-in form), Philox
-thresholds seed 7, start state |N,0>.  One step = one dump interval of 10 periods for every
-trajectory with the observables taken at its end (1000 periods with 100 dumps is the full
-job).  Metric: trajectory-periods per second over all GPUs.
+thresholds seed 7, start state |N,0>.  Metric: trajectory-periods per second over all GPUs.
+
+Protocol (the same window in every arm): W untimed warm-up steps of P periods each carry the
+ensemble from |N,0> through its transient (periods 1 .. W P); the state at that point is
+checkpointed, and each of the K timed steps restores it and runs periods W P + 1 .. W P + P, with
+the observables at the end.  `value` is device time of those runs; `e2e` times the same window
+through the C ABI from pinned host memory (checkpoint load, run, observables and states read
+back); the CPU baseline and the reference arm run the CPU restatement over the same periods on a
+sample of the same trajectories (their Philox streams, hence their paths, are the GPU's).
 
   python bench.py --gpus N --steps K --warmup W            # this engine
   python bench.py --impl reference --steps K --warmup W    # CPU restatement of the reference
@@ -14,9 +20,9 @@ Multi-GPU: one process per GPU (torchrun); trajectories are sharded (rank r owns
 trajectories r*n .. r*n+n-1, so the ensemble is the one a single GPU would run), the
 ensemble sums of the observables are all-reduced over NCCL once per step.
 
-The same protocol then times the split-precision form (bf16x3 matvecs on the tcgen05 tensor
-cores, FP64 states and norms) on the same inputs; it is reported beside the plain form as
-"split_form" with its speed-up and its deviation from the plain form's ensemble <n1 - n2>.
+The same protocol then times the split-precision form (tcgen05 matvecs, FP64 states and norms)
+from the same checkpoint; it is reported beside the plain form as "split_form" with its speed-up
+and its deviation from the plain form against the horizon.
 """
 import argparse
 import json
@@ -73,18 +79,33 @@ def dist_env():
     return rank, world, local
 
 
-def model():
-    import os_d_b200 as q
+def model(impl="ours"):
+    """Operators of the workload: the library's builder, or for the reference arm the CPU
+    restatement's (bit-identical to each other; the reference arm loads no library of ours)."""
+    T = 2.0 * 3.1415926535897932384626433832795 / PRM["omega"]
+    if impl == "reference":
+        from oracle import oracle_py as O
 
-    H, Hd, L, Ut = q.build_dimer(N_BOSONS, PRM["J"], PRM["U"], PRM["E"], PRM["A"], PRM["g"], PRM["omega"], DEEP)
+        H, Hd, L, K0, K1 = O.dimer_operators(N_BOSONS, PRM["J"], PRM["U"], PRM["E"], PRM["A"], PRM["g"])
+        Ut = np.stack([O.split_tree(K0, T, DEEP), O.split_tree(K1, T, DEEP)])
+    else:
+        import os_d_b200 as q
+
+        H, Hd, L, Ut = q.build_dimer(N_BOSONS, PRM["J"], PRM["U"], PRM["E"], PRM["A"], PRM["g"], PRM["omega"], DEEP)
     d = N_BOSONS + 1
     HE = H + PRM["E"] * Hd
     rng = np.random.default_rng(1)  # one random observable X X^H / (tr/d)
     X = 0.5 * (rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d)))
     R = X @ X.conj().T
     R = (R / (np.trace(R).real / d))[None]
-    T = 2.0 * 3.1415926535897932384626433832795 / PRM["omega"]
     return dict(H=H, Hd=Hd, L=L, U=Ut, HE=HE, R=R, T=T, d=d)
+
+
+def bench_config(world, n, d, P, W):
+    return {"workload": WORKLOAD, "n_traj_per_gpu": n, "dim": d, "ex_deep": DEEP, "periods_per_step": P,
+            "window": f"periods {W * P + 1}..{W * P + P} (after a {W * P}-period transient from |N,0>)",
+            "seed": SEED, "start": "|N,0>", "parallelism": f"dp{world} (trajectories)",
+            "l2": "flushed between timed steps (256 MB write)"}
 
 
 def kernel_name(d):
@@ -101,49 +122,63 @@ def start_states(n, d):
 
 
 # ---------------------------------------------------------------- CPU restatement (baseline)
-def cpu_rate(M, n_traj, periods, threads, tr_base=0):
-    """Trajectory-periods/s of the CPU oracle (OpenMP over trajectories like the reference)."""
+CPU_STATE = ("phi", "eta", "t", "rng_pos", "jumps_counts", "n_rec", "error")
+
+
+def cpu_windows(M, n_traj, threads, warm_periods, P, windows):
+    """The CPU restatement (oracle/qjx_oracle.c, OpenMP over trajectories like the reference,
+    QJX/experiment.cpp:484) on trajectories 0 .. n_traj - 1 of the benchmark ensemble: an untimed
+    transient of warm_periods periods, then `windows` timed runs of the next P periods, each from
+    the state the transient left.  Returns [(traj*periods/s, seconds, matvecs per traj*period)]."""
     from oracle import oracle_py as O
 
     ens = O.Ensemble(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n_traj, seed=SEED, record=0)
     ens.init(0, 0)
-    t0 = time.perf_counter()
-    bad = ens.run_periods(periods, is_obs=1, n_threads=threads)
-    dt = time.perf_counter() - t0
-    if bad:
+    if warm_periods and ens.run_periods(warm_periods, is_obs=1, n_threads=threads):
         raise RuntimeError("oracle reported trajectory errors")
-    return n_traj * periods / dt, dt, float(ens.matvecs.sum()) / (n_traj * periods)
+    snap = {k: getattr(ens, k).copy() for k in CPU_STATE}
+    out = []
+    for _ in range(windows):
+        for k, v in snap.items():
+            getattr(ens, k)[...] = v
+        mv0 = int(ens.matvecs.sum())
+        t0 = time.perf_counter()
+        bad = ens.run_periods(P, is_obs=1, n_threads=threads)
+        dt = time.perf_counter() - t0
+        if bad:
+            raise RuntimeError("oracle reported trajectory errors")
+        out.append((n_traj * P / dt, dt, (int(ens.matvecs.sum()) - mv0) / (n_traj * P)))
+    return out
+
+
+CPU_TRAJ_PER_THREAD = 3
 
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    M = model()
+    M = model("reference")
     threads = os.cpu_count() or 1
-    sample = 2 * threads
-    for _ in range(args.warmup):
-        cpu_rate(M, sample, 1, threads)
-    rates = []
-    tot = 0.0
-    for _ in range(args.steps):
-        r, dt, mv = cpu_rate(M, sample, 1, threads)
-        rates.append(r)
-        tot += dt
-    value = float(np.mean(rates))
+    sample = CPU_TRAJ_PER_THREAD * threads
+    P = args.periods_per_step
+    res = cpu_windows(M, sample, threads, args.warmup * P, P, args.steps)
+    value = float(np.mean([r[0] for r in res]))
+    tot = sum(r[1] for r in res)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD.replace("10^4 trajectories per GPU x 10 periods per step",
-                                                f"{sample} trajectories x 1 period per step (bounded CPU sample)"),
-                   "n_traj": sample, "dim": M["d"], "ex_deep": DEEP, "seed": SEED},
+        "config": bench_config(args.gpus, args.n_traj, M["d"], P, args.warmup),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-                         "sample": f"{sample} trajectories x 1 period at dim 201 per step, OpenMP over trajectories"},
+                         "sample": (f"trajectories 0..{sample - 1} of the ensemble (their paths are the GPU's), "
+                                    f"the same {P}-period window after the same {args.warmup * P}-period transient, "
+                                    f"OpenMP over trajectories on {threads} host threads")},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": ("the reference (source/cpp/QJX) needs Intel MKL and Eigen, absent here; this arm times the "
-                 "C restatement of its algorithm (oracle/qjx_oracle.c) on the host cores"),
-        "matvecs_per_traj_period": mv,
+                 "C restatement of its algorithm (oracle/qjx_oracle.c) on the host cores, with operators from "
+                 "oracle/oracle_py.py (no library of this repository is loaded)"),
+        "matvecs_per_traj_period": float(np.mean([r[2] for r in res])),
     }
     print(json.dumps(line), flush=True)
 
@@ -494,6 +529,64 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---------------------------------------------------------------- split-precision form
+def split_form(args, q, new_engine, timed_windows, snap, value, ens_plain, x_plain, eng_plain, n, d, P, W, world):
+    """The split-precision form (precision 1) from the same checkpoint over the same windows, its
+    speed-up over the plain form, and its deviation from the plain form against the horizon: one
+    more window of both forms with the observables after every period."""
+    eng_s = new_engine(1)
+    ms_s, _, _, s0, s1, ens_split, x_split = timed_windows(eng_s, snap)
+    v_s = world * n * P * args.steps / (ms_s * 1e-3)
+    tiles = s1["mma_tiles"] - s0["mma_tiles"]
+    mds, ks = 16 * ((d + 15) // 16), (d + 15) // 16
+    exec_flops = tiles * ks * 12 * 2.0 * 128 * mds * 16
+    kern_s = (s1["step_kernel_ms"] - s0["step_kernel_ms"]) * 1e-3
+    peaks = {}
+    pk_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_file):
+        with open(pk_file) as f:
+            peaks = json.load(f)
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    # horizon: observables after each of the P periods of one more window, both forms
+    base = W + args.steps + 1
+    per_period = {}
+    for name, e in (("plain", eng_plain), ("split", eng_s)):
+        e.restore(snap)
+        e.run_periods(P, is_obs=1, dump_at=list(range(1, P + 1)), dump_base=base)
+        ob = e.observables(base, P)
+        per_period[name] = (N_BOSONS - 2.0 * ob["mean"], ob["energy"])
+        per_period[name + "_jumps"] = e.states()[3]
+    hor = []
+    for h in range(P):
+        xp, xs = per_period["plain"][0][h], per_period["split"][0][h]
+        ep, es = per_period["plain"][1][h], per_period["split"][1][h]
+        same = np.abs(xs - xp) < 1e-3  # an identical jump path leaves only the matvec rounding
+        hor.append({"periods": h + 1,
+                    "n1_minus_n2_abs_diff": float(abs(xs.mean() - xp.mean())),
+                    "n1_minus_n2_stderr": float(xp.std() / np.sqrt(xp.size)),
+                    "energy_abs_diff": float(abs(es.mean() - ep.mean())),
+                    "same_path_fraction": float(same.mean()),
+                    "max_abs_diff_on_same_paths": float(np.abs(xs - xp)[same].max()) if same.any() else None})
+    eng_s.close()
+    return {
+        "metric": METRIC, "value": v_s, "unit": METRIC, "ms_per_step": ms_s / args.steps,
+        "speedup_vs_plain": v_s / value,
+        "dtype": "bf16x3 matvec on tcgen05 (FP32 accumulate), FP64 states, norms, decisions and observables",
+        "n1_minus_n2_abs_diff_vs_plain_per_step": [abs(a[0] - b[0]) for a, b in zip(ens_split, ens_plain)],
+        "n1_minus_n2_stderr_per_step": [b[1] for b in ens_plain],
+        "same_jump_count_fraction_after_window": float(np.mean(per_period["split_jumps"] == per_period["plain_jumps"])),
+        "horizon": hor,
+        "roofline": {"bound": "tensor", "kernel": "qjx::split_step_kernel",
+                     "achieved": exec_flops / kern_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": exec_flops / kern_s / 1e12 / bf16_peak,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)" if peaks else "fallback 1590",
+                     "flops": "executed tcgen05 bf16 flops: 12 MMAs of 128 x MDs x 16 per k-step and tile",
+                     "algorithmic_tflops": 8.0 * d * d * (s1["matvecs"] - s0["matvecs"]) / kern_s / 1e12},
+        "matvecs_per_traj_period": (s1["matvecs"] - s0["matvecs"]) / (n * P * args.steps),
+        "gpu_launches": int(s1["launches"] - s0["launches"]),
+    }
+
+
 # ---------------------------------------------------------------- this engine
 def run_ours(args):
     import torch
@@ -524,47 +617,52 @@ def run_ours(args):
         return t.cpu().numpy()
 
     M = model()
-    n, d, P = args.n_traj, M["d"], args.periods_per_step
-    steps_total = args.warmup + args.steps
+    n, d, P, W = args.n_traj, M["d"], args.periods_per_step, args.warmup
+    steps_total = W + args.steps
     psi0 = start_states(n, d)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     def new_engine(precision):
         e = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, record=0, rec_cap=16,
-                     keep_adr=0, max_dumps=steps_total + 1, device=local, tr_base=rank * n, precision=precision)
+                     keep_adr=0, max_dumps=steps_total + P + 2, device=local, tr_base=rank * n, precision=precision)
         e.set_states(psi0)
         e.init_thresholds()
         e.reset_times()
         e.observe(0, is_start=True)
         return e
 
-    def timed_run(eng, clocks=None):
-        """W untimed + K timed steps of P periods; device time of the K steps (max over ranks),
-        stats before/after, and the ensemble <n1 - n2> with its standard error after every step."""
-        def one_step(slot):
-            eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=slot)
-            x = N_BOSONS - 2.0 * eng.observables(slot, 1)["mean"][0]
-            # ensemble sums reduced over ranks (the one exchange of the path)
-            s = allreduce([float(np.sum(x)), float(np.sum(x * x)), float(n)])
-            m = s[0] / s[2]
-            return m, float(np.sqrt(max(s[1] / s[2] - m * m, 0.0) / s[2]))
+    def n1n2(eng, slot):
+        return N_BOSONS - 2.0 * eng.observables(slot, 1)["mean"][0]
 
-        ens = [one_step(1 + w) for w in range(args.warmup)]
+    def ensemble(x):
+        """ensemble mean of <n1 - n2> and its standard error; the sums are reduced over ranks
+        (the one exchange of the path)"""
+        s = allreduce([float(np.sum(x)), float(np.sum(x * x)), float(x.size)])
+        m = s[0] / s[2]
+        return m, float(np.sqrt(max(s[1] / s[2] - m * m, 0.0) / s[2]))
+
+    def timed_windows(eng, snap, clocks=None):
+        """K timed runs of the window, each from the checkpoint `snap`; device time of each run
+        (CUDA events around the micro-step launches), max over ranks."""
         st0 = eng.stats()
         barrier()
         if clocks:
             clocks.start()
         t0 = time.perf_counter()
-        dev_ms = 0.0
+        dev_ms, ens, x_last = 0.0, [], None
         for k in range(args.steps):
+            eng.restore(snap)
             flush.zero_()  # L2 flush between timed steps
             torch.cuda.synchronize()
-            ens.append(one_step(1 + args.warmup + k))
+            slot = 1 + W + k
+            eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=slot)
             dev_ms += eng.stats()["last_call_ms"]
+            x_last = n1n2(eng, slot)
+            ens.append(ensemble(x_last))
         barrier()
         wall = time.perf_counter() - t0
         clk = clocks.stop() if clocks else None
-        return float(allreduce([dev_ms], "max")[0]), wall, clk, st0, eng.stats(), ens
+        return float(allreduce([dev_ms], "max")[0]), wall, clk, st0, eng.stats(), ens, x_last
 
     if args.production_sweep > 0:
         if rank == 0:
@@ -582,7 +680,12 @@ def run_ours(args):
         eng.run_periods(1, is_obs=1)
         eng.close()
         return
-    dev_ms_max, wall, clk, st0, st1, ens_plain = timed_run(eng, ClockSampler(local))
+    # transient: W untimed steps of P periods from |N,0>, then the window's start state
+    for w in range(W):
+        eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=1 + w)
+    snap = torch.empty(eng.checkpoint_size(), dtype=torch.uint8, pin_memory=True).numpy()
+    snap = eng.checkpoint(out=snap)
+    dev_ms_max, wall, clk, st0, st1, ens_plain, x_plain = timed_windows(eng, snap, ClockSampler(local))
     value = world * n * P * args.steps / (dev_ms_max * 1e-3)
     ms_per_step = dev_ms_max / args.steps
     ens_sum = ens_plain[-1]
@@ -612,67 +715,37 @@ def run_ours(args):
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": W, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_traj_per_gpu": n, "dim": d, "ex_deep": DEEP,
-                   "periods_per_step": P, "seed": SEED, "start": "|N,0>", "parallelism": f"dp{world} (trajectories)",
-                   "l2": "flushed between timed steps (256 MB write)"},
+        "config": bench_config(world, n, d, P, W),
         "wall_s": wall, "roofline": roofline, "clocks": clk,
         "gpu_launches": int(st1["launches"] - st0["launches"]),
         "ensemble_n1_minus_n2": ens_sum[0], "ensemble_n1_minus_n2_stderr": ens_sum[1],
+        "matvecs_per_traj_period": matvecs / (n * P * args.steps),
     }
 
-    # split-precision form on the same inputs and protocol
+    # split-precision form: same checkpoint, same windows
     if not args.no_split:
-        eng_s = new_engine(1)
-        ms_s, _, _, s0, s1, ens_split = timed_run(eng_s)
-        eng_s.close()
-        v_s = world * n * P * args.steps / (ms_s * 1e-3)
-        tiles = s1["mma_tiles"] - s0["mma_tiles"]
-        mds, ks = 16 * ((d + 15) // 16), (d + 15) // 16
-        exec_flops = tiles * ks * 12 * 2.0 * 128 * mds * 16
-        kern_s = (s1["step_kernel_ms"] - s0["step_kernel_ms"]) * 1e-3
-        peaks = {}
-        pk_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
-        if os.path.exists(pk_file):
-            with open(pk_file) as f:
-                peaks = json.load(f)
-        bf16_peak = peaks.get("bf16_tflops", 1590.0)
-        diffs = [abs(a[0] - b[0]) for a, b in zip(ens_split, ens_plain)]
-        line["split_form"] = {
-            "metric": METRIC, "value": v_s, "unit": METRIC, "ms_per_step": ms_s / args.steps,
-            "speedup_vs_plain": v_s / value, "dtype": "bf16x3 matvec (FP32 accumulate), FP64 state and norms",
-            "n1_minus_n2_abs_diff_vs_plain_per_step": diffs,
-            "n1_minus_n2_stderr_per_step": [b[1] for b in ens_plain],
-            "periods_per_step": P,
-            "roofline": {"bound": "tensor", "kernel": "qjx::split_step_kernel",
-                         "achieved": exec_flops / kern_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
-                         "frac": exec_flops / kern_s / 1e12 / bf16_peak,
-                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)" if peaks else "fallback 1590",
-                         "flops": "executed tcgen05 bf16 flops: 12 MMAs of 128 x MDs x 16 per k-step and tile",
-                         "algorithmic_tflops": 8.0 * d * d * (s1["matvecs"] - s0["matvecs"]) / kern_s / 1e12},
-            "gpu_launches": int(s1["launches"] - s0["launches"]),
-        }
+        line["split_form"] = split_form(args, q, new_engine, timed_windows, snap, value, ens_plain, x_plain,
+                                        eng, n, d, P, W, world)
 
     # e2e through the public C ABI with host buffers, copies inside the timed region
     if not args.no_e2e:
-        host_psi = torch.empty((n, d), dtype=torch.complex128, pin_memory=True).numpy()
-        host_psi[:] = psi0
         barrier()
         t0 = time.perf_counter()
         for k in range(args.steps):
-            eng.set_states(host_psi)
-            eng.init_thresholds()
-            eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=1 + args.warmup + k)
-            ob = eng.observables(1 + args.warmup + k, 1)
+            slot = 1 + W + k
+            eng.restore(snap)  # H2D: the window's start state from pinned host memory
+            eng.run_periods(P, is_obs=1, dump_at=[P], dump_base=slot)
+            ob = eng.observables(slot, 1)
             eng.states()
             allreduce([float(np.sum(N_BOSONS - 2.0 * ob["mean"][0])), float(n)])
         barrier()
         e2e_s = float(allreduce([time.perf_counter() - t0], "max")[0])
         line["e2e"] = {"value": world * n * P * args.steps / e2e_s, "unit": METRIC,
-                       "h2d_bytes_per_step": int(n * d * 16), "d2h_bytes_per_step": int(n * d * 16 + 5 * n * 8 + n * 16),
-                       "path": "qjx_set_states + qjx_init_thresholds + qjx_run_periods + qjx_get_observables + "
-                               "qjx_get_states per step"}
+                       "h2d_bytes_per_step": int(snap.nbytes), "d2h_bytes_per_step": int(n * d * 16 + 5 * n * 8 + n * 16),
+                       "path": "qjx_checkpoint_load (window start, pinned host buffer) + qjx_run_periods + "
+                               "qjx_get_observables + qjx_get_states per step, same window as value"}
     if rank == 0 and not args.no_fbasis:
         line["fbasis"] = fbasis_bench(args, local)
     if rank == 0 and world == 1 and not args.no_batch:  # single-GPU measurements
@@ -681,11 +754,13 @@ def run_ours(args):
         line["serving"] = serving_bench(args, local)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample = 128 * threads  # about 15 s of CPU work
-        rate, dt, mv = cpu_rate(M, sample, 1, threads)
+        sample = CPU_TRAJ_PER_THREAD * threads
+        rate, dt, mv = cpu_windows(M, sample, threads, W * P, P, 1)[0]
         line["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
-                                "sample": f"{sample} trajectories x 1 period at dim 201 ({dt:.1f} s), "
-                                          f"OpenMP over trajectories, oracle/qjx_oracle.c"}
+                                "sample": (f"trajectories 0..{sample - 1} x the same {P}-period window after the "
+                                           f"same {W * P}-period transient ({dt:.1f} s timed), OpenMP over "
+                                           f"trajectories, oracle/qjx_oracle.c"),
+                                "matvecs_per_traj_period": mv}
     eng.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

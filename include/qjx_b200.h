@@ -89,6 +89,11 @@ typedef struct {
                           and free evolution, init_split_structure_jcs, core.cpp:10086-10124) give
                           them here.  Level l of branch b steps 2 len_b / brep 2^-(l+2), brep = 1
                           or 2 deep_num_steps. */
+    double split_recheck; /* split form (precision 1): a norm test whose split-precision norm p lies
+                          within split_recheck * p of the threshold is not decided; that step's
+                          matvec is computed again in FP64 (the plain form's arithmetic) in the next
+                          micro-step and decides.  0 selects 1e-5 (about 5x the measured split error
+                          of the norm), a negative value turns the recheck off. */
 } qjx_config;
 
 typedef struct {
@@ -100,6 +105,7 @@ typedef struct {
     double step_kernel_ms;   /* device time of the micro-step kernel batches alone (CUDA events) */
     int64_t launches;        /* kernels launched by the engine */
     int64_t mma_tiles;       /* split form: 128-row tcgen05 tiles (12 MMAs of 128 x MDs x 16 per k-step) */
+    int64_t rechecks;        /* split form: norm tests taken again on an FP64 matvec */
 } qjx_stats;
 
 /* U: [num_branches][deep][d][d] split propagators exp(K_b dt_l), dt_l = T 2^-(l+2).
@@ -389,9 +395,11 @@ void qjx_fb_destroy(qjx_fb *h);
  * pressure in the middle of a run.  Same arithmetic as qjx_fb_create + qjx_fb_run (the same
  * kernels); every pointer is DEVICE memory owned by the caller: the CSR arrays of Gs and
  * Qs_drv (0-based), Ks [n], and x [n], advanced in place by n_periods periods of num_steps RK4
- * steps starting at period index period0.  The RK4 stage vectors live in a static device array
- * sized for n <= QJX_FB_NOALLOC_MAX_N (2 MiB, held by every GPU that loads the library until the
- * process exits); larger n is rejected with QJX_ERR_UNSUPPORTED.  Work is queued on `stream`
+ * steps starting at period index period0, four kernel launches per RK4 step.  The RK4 stage
+ * vectors (two stage arguments and k1..k3) live in a static device array sized for
+ * n <= QJX_FB_NOALLOC_MAX_N (2.5 MiB, held by every GPU that loads the library until the process
+ * exits); larger n is rejected with QJX_ERR_UNSUPPORTED.  The return status covers this call's own
+ * launches only; an earlier error of other code is neither reported nor cleared.  Work is queued on `stream`
  * (a cudaStream_t, NULL for the default stream) and the call returns without waiting.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
  * that device current; make that first call before any stream capture.  All calls on a device

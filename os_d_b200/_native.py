@@ -32,7 +32,7 @@ class QjxConfig(C.Structure):
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
                 ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("deep_num_steps", C.c_int),
-                ("precision", C.c_int), ("branch_len", c_double_p)]
+                ("precision", C.c_int), ("branch_len", c_double_p), ("split_recheck", C.c_double)]
 
 
 class QjxEnsemble(C.Structure):
@@ -51,7 +51,7 @@ class QjxLpnConfig(C.Structure):
 class QjxStats(C.Structure):
     _fields_ = [("micro_steps", C.c_int64), ("matvecs", C.c_int64), ("jumps", C.c_int64),
                 ("kernel_ms", C.c_double), ("last_call_ms", C.c_double), ("step_kernel_ms", C.c_double),
-                ("launches", C.c_int64), ("mma_tiles", C.c_int64)]
+                ("launches", C.c_int64), ("mma_tiles", C.c_int64), ("rechecks", C.c_int64)]
 
 
 _lib = None

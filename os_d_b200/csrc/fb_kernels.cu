@@ -2,10 +2,14 @@
 //
 // The reference integrates dx/dt = Gs x + E(t) Qs_drv x - Ks with classic RK4
 // (source/cpp/CQdiss_os_dimer/CQdiss/calcODE.cpp:75-118 calcVectValue_real, :249-389
-// calcODE_trans/std), two mkl_dcsrgemv per stage.  Here one kernel per RK stage computes
-// both CSR row products, the stage vector k = (Gs x + drv Qs x - Ks) h and the next stage
-// argument (or the RK4 update) in one pass; the steps of a period are captured once as a
-// CUDA graph and replayed.
+// calcODE_trans/std), two mkl_dcsrgemv per stage.  Two GPU paths:
+//   * rk4_cluster: one thread-block cluster holds the whole system in distributed shared memory
+//     and integrates a period per launch (systems that fit <= 16 CTAs);
+//   * rk_stage: one launch per RK stage (four per step) computes both CSR row products, the
+//     stage vector k = (Gs x + drv Qs x - Ks) h and the next stage argument, or in stage 4 the
+//     RK4 update of x.  The stage arguments are double-buffered (stage s reads one buffer and
+//     writes the other), as the reference keeps x, tmp and k1..k4 apart (calcODE.cpp:249-309):
+//     a row may read any other row's argument, and rows of one launch run in no fixed order.
 //
 // Canonical row sum (shared bit-for-bit with the CPU oracle): lane l of a warp accumulates
 // the row's nonzeros l, l+32, l+64, ... in CSR order with fma, then the 32 partial sums are
@@ -36,7 +40,9 @@ struct FbParams {
     double drv_ampl;  // -A (calcODE.cpp:91)
     double drv_freq, drv_phase;
     int drv_type;
-    double *x, *val, *k1, *k2, *k3;
+    double *x;
+    double *va, *vb;     // stage arguments: stage 1 writes va, 2 writes vb, 3 writes va
+    double *k1, *k2, *k3;
 };
 
 __device__ __forceinline__ double warp_row_sum(const int *rp, const int *ci, const double *v, const double *x, int row,
@@ -50,14 +56,16 @@ __device__ __forceinline__ double warp_row_sum(const int *rp, const int *ci, con
     return s;
 }
 
-// stage 1..4 of one RK4 step at time t (calcODE.cpp:278-302)
+// Stage 1..4 of one RK4 step at time t (calcODE.cpp:278-302), one warp per row.  Stage s reads
+// its argument (x, va, vb, va) and writes only a buffer no row of this launch reads (va, vb, va,
+// and in stage 4 the row's own x: x += (k1 + 2 k2 + 2 k3 + k4) / 6, calcODE.cpp:299-302).
 __global__ void rk_stage(const FbParams P, int stage, double t, double h)
 {
     const int warps = blockDim.x >> 5;
     const int row = blockIdx.x * warps + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= P.n) return;
-    const double *arg = (stage == 1) ? P.x : P.val;
+    const double *arg = (stage == 1) ? P.x : ((stage == 3) ? P.vb : P.va);
     const double tt = (stage == 1) ? t : ((stage == 4) ? __dadd_rn(t, h) : __dadd_rn(t, __ddiv_rn(h, 2.0)));
     const double t1 = warp_row_sum(P.gr, P.gc, P.gv, arg, row, lane);
     const double t2 = warp_row_sum(P.qr, P.qc, P.qv, arg, row, lane);
@@ -70,24 +78,40 @@ __global__ void rk_stage(const FbParams P, int stage, double t, double h)
     const double x = P.x[row];
     if (stage == 1) {
         P.k1[row] = k;
-        P.val[row] = __dadd_rn(x, __ddiv_rn(k, 2.0));
+        P.va[row] = __dadd_rn(x, __ddiv_rn(k, 2.0));
     } else if (stage == 2) {
         P.k2[row] = k;
-        P.val[row] = __dadd_rn(x, __ddiv_rn(k, 2.0));
+        P.vb[row] = __dadd_rn(x, __ddiv_rn(k, 2.0));
     } else if (stage == 3) {
         P.k3[row] = k;
-        P.val[row] = __dadd_rn(x, k);
+        P.va[row] = __dadd_rn(x, k);
+    } else {
+        const double sum =
+            __dadd_rn(__dadd_rn(__dadd_rn(P.k1[row], __dmul_rn(2.0, P.k2[row])), __dmul_rn(2.0, P.k3[row])), k);
+        P.x[row] = __dadd_rn(x, __ddiv_rn(sum, 6.0));
     }
-    // stage 4 is finished by rk_update once every row has read val
-    if (stage == 4) P.k3[row] = __dadd_rn(__dadd_rn(__dadd_rn(P.k1[row], __dmul_rn(2.0, P.k2[row])),
-                                                     __dmul_rn(2.0, P.k3[row])), k);
 }
 
-// x += (k1 + 2 k2 + 2 k3 + k4) / 6  (calcODE.cpp:299-302); the sum was left in k3.
-__global__ void rk_update(const FbParams P)
+// Queues the four stage launches of every RK4 step of n_periods periods from period0 on `st`;
+// returns the first launch error (cudaLaunchKernelEx reports the launch's own status).
+static cudaError_t queue_rk_stages(const FbParams &P, double T, int num_steps, int period0, int n_periods,
+                                   cudaStream_t st)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P.n) P.x[i] = __dadd_rn(P.x[i], __ddiv_rn(P.k3[i], 6.0));
+    const double step = T / double(num_steps);  // data.cpp:10
+    const int warps = 8;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((P.n + warps - 1) / warps);
+    lc.blockDim = dim3(warps * 32);
+    lc.stream = st;
+    for (int p = period0; p < period0 + n_periods; p++)
+        for (int s = 0; s < num_steps; s++) {
+            const double t = double(p) * T + double(s) * step;  // calcODE.cpp:280
+            for (int stage = 1; stage <= 4; stage++) {
+                const cudaError_t e = cudaLaunchKernelEx(&lc, rk_stage, P, stage, t, step);
+                if (e != cudaSuccess) return e;
+            }
+        }
+    return cudaSuccess;
 }
 
 // ---------------------------------------------------------------- cluster-resident RK4
@@ -278,11 +302,12 @@ extern "C" qjx_status qjx_fb_create(int n, const int *gs_rowptr, const int *gs_c
     double *gv = (double *)fb_alloc(h, sizeof(double) * gnz), *qv = (double *)fb_alloc(h, sizeof(double) * qnz);
     double *ks = (double *)fb_alloc(h, sizeof(double) * n);
     P.x = (double *)fb_alloc(h, sizeof(double) * n);
-    P.val = (double *)fb_alloc(h, sizeof(double) * n);
+    P.va = (double *)fb_alloc(h, sizeof(double) * n);
+    P.vb = (double *)fb_alloc(h, sizeof(double) * n);
     P.k1 = (double *)fb_alloc(h, sizeof(double) * n);
     P.k2 = (double *)fb_alloc(h, sizeof(double) * n);
     P.k3 = (double *)fb_alloc(h, sizeof(double) * n);
-    if (!gr || !gc || !qr || !qc || !gv || !qv || !ks || !P.x || !P.val || !P.k1 || !P.k2 || !P.k3) {
+    if (!gr || !gc || !qr || !qc || !gv || !qv || !ks || !P.x || !P.va || !P.vb || !P.k1 || !P.k2 || !P.k3) {
         qjx_fb_destroy(h);
         return QJX_ERR_OOM;
     }
@@ -398,8 +423,6 @@ extern "C" qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods)
     if (!h || period0 < 0 || n_periods < 0) return QJX_ERR_INVALID_ARG;
     if (cudaSetDevice(h->device) != cudaSuccess) return QJX_ERR_CUDA;
     const fb::FbParams &P = h->P;
-    const double step = h->T / double(h->num_steps);  // data.cpp:10
-    const int warps = 8, rblocks = (P.n + warps - 1) / warps, ublocks = (P.n + 255) / 256;
     cudaEventRecord(h->e0, h->stream);
     if (h->cluster) {  // one cluster launch per period
         cudaLaunchConfig_t lc = {};
@@ -420,18 +443,11 @@ extern "C" qjx_status qjx_fb_run(qjx_fb *h, int period0, int n_periods)
             C.n_periods = 1;
             if (cudaLaunchKernelEx(&lc, fb::rk4_cluster, C) != cudaSuccess) return QJX_ERR_CUDA;
         }
-    } else {
-        for (int p = period0; p < period0 + n_periods; p++) {
-            for (int s = 0; s < h->num_steps; s++) {
-                const double t = double(p) * h->T + double(s) * step;  // calcODE.cpp:280
-                for (int stage = 1; stage <= 4; stage++)
-                    fb::rk_stage<<<rblocks, warps * 32, 0, h->stream>>>(P, stage, t, step);
-                fb::rk_update<<<ublocks, 256, 0, h->stream>>>(P);
-            }
-        }
+    } else if (fb::queue_rk_stages(P, h->T, h->num_steps, period0, n_periods, h->stream) != cudaSuccess) {
+        return QJX_ERR_CUDA;
     }
     cudaEventRecord(h->e1, h->stream);
-    if (cudaEventSynchronize(h->e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return QJX_ERR_CUDA;
+    if (cudaEventSynchronize(h->e1) != cudaSuccess) return QJX_ERR_CUDA;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->e0, h->e1);
     h->last_ms = ms;
@@ -456,10 +472,10 @@ extern "C" qjx_status qjx_fb_get(qjx_fb *h, double *x, double *last_period_ms)
 }
 
 // ---------------------------------------------------------------- allocation-free variant
-// Stage vectors val, k1, k2, k3 of the allocation-free entry point, one static array shared by
+// Stage vectors va, vb, k1, k2, k3 of the allocation-free entry point, one static array shared by
 // all its calls on a device.  In host code this name is only a stand-in for the symbol; its
 // device address comes from cudaGetSymbolAddress.
-static __device__ __align__(256) double g_fb_noalloc_scratch[4 * QJX_FB_NOALLOC_MAX_N];
+static __device__ __align__(256) double g_fb_noalloc_scratch[5 * QJX_FB_NOALLOC_MAX_N];
 
 static double *fb_noalloc_scratch_ptr(int device)
 {
@@ -503,20 +519,16 @@ extern "C" qjx_status qjx_fb_rk4_noalloc(int n, const int *gs_rowptr, const int 
     P.drv_phase = drv_phase;
     P.drv_type = drv_type;
     P.x = x;
-    P.val = scratch;
-    P.k1 = scratch + QJX_FB_NOALLOC_MAX_N;
-    P.k2 = scratch + 2 * QJX_FB_NOALLOC_MAX_N;
-    P.k3 = scratch + 3 * QJX_FB_NOALLOC_MAX_N;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const double step = T / double(num_steps);
-    const int warps = 8, rblocks = (n + warps - 1) / warps, ublocks = (n + 255) / 256;
-    for (int p = period0; p < period0 + n_periods; p++)
-        for (int s = 0; s < num_steps; s++) {
-            const double t = double(p) * T + double(s) * step;
-            for (int stage = 1; stage <= 4; stage++) fb::rk_stage<<<rblocks, warps * 32, 0, st>>>(P, stage, t, step);
-            fb::rk_update<<<ublocks, 256, 0, st>>>(P);
-        }
-    return cudaGetLastError() == cudaSuccess ? QJX_OK : QJX_ERR_CUDA;
+    P.va = scratch;
+    P.vb = scratch + QJX_FB_NOALLOC_MAX_N;
+    P.k1 = scratch + 2 * QJX_FB_NOALLOC_MAX_N;
+    P.k2 = scratch + 3 * QJX_FB_NOALLOC_MAX_N;
+    P.k3 = scratch + 4 * QJX_FB_NOALLOC_MAX_N;
+    // only the status of this call's own launches is reported; an error left by other code
+    // stays where the caller can still read it
+    const cudaError_t e =
+        fb::queue_rk_stages(P, T, num_steps, period0, n_periods, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? QJX_OK : QJX_ERR_CUDA;
 }
 
 extern "C" void qjx_fb_destroy(qjx_fb *h)

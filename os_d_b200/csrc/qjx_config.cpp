@@ -13,18 +13,25 @@
 
 namespace qjxio {
 
+// Tokens of a config.txt line: the pieces of `str` between occurrences of `delim`, with empty
+// pieces dropped.  A run of delimiters, or one at either end, therefore yields no token, while
+// any other character (a tab, a trailing carriage return) stays inside its token.  This is the
+// tokenisation of the reference's reader (QJX/config.cpp:3-27, used at :109-114).
 std::vector<std::string> split(const std::string &str, const std::string &delim)
 {
-    std::vector<std::string> tokens;
-    size_t prev = 0, pos = 0;
-    do {
-        pos = str.find(delim, prev);
-        if (pos == std::string::npos) pos = str.length();
-        std::string token = str.substr(prev, pos - prev);
-        if (!token.empty()) tokens.push_back(token);
-        prev = pos + delim.length();
-    } while (pos < str.length() && prev < str.length());
-    return tokens;
+    std::vector<std::string> out;
+    if (delim.empty()) {
+        if (!str.empty()) out.push_back(str);
+        return out;
+    }
+    std::string::size_type start = 0;
+    for (;;) {
+        const std::string::size_type hit = str.find(delim, start);
+        const std::string::size_type stop = (hit == std::string::npos) ? str.size() : hit;
+        if (stop > start) out.emplace_back(str, start, stop - start);
+        if (hit == std::string::npos) return out;
+        start = hit + delim.size();
+    }
 }
 
 void set_param(RunParam &rp, ConfigParam &cp, const std::string &k, const std::string &v)

@@ -43,6 +43,18 @@ constexpr int kSlotArgs = 2, kSlotK1 = 3, kSlotND = 6, kRkSlots = 7;
 
 enum ErrCode : int { ERR_NONE = 0, ERR_NORM = 1, ERR_ZERO_W = 2, ERR_RNG = 3, ERR_TIMEOUT = 6 };
 
+// Where the input vector of a trajectory's next matvec is, as the epilogue leaves it (the split
+// form writes that vector's bf16 planes for the next micro-step): the epilogue's column itself,
+// the column divided by a scalar, the input of this micro-step again, or a state slot in global
+// memory.
+enum NextSrc : int { SRC_NONE = 0, SRC_COL = 1, SRC_SCALED = 2, SRC_SAME = 3, SRC_GLOBAL = 4 };
+constexpr int kRecheck = -2;  // column_epilogue: the trajectory goes to the FP64 recheck list
+struct EpiOut {
+    int mode;    // NextSrc
+    int slot;    // state slot of the next input (SRC_GLOBAL)
+    double div;  // SRC_SCALED: the next input is col / div
+};
+
 // Per-trajectory state (one 144-byte record per trajectory).
 struct __align__(16) TrajState {
     double t;          // times_all
@@ -65,7 +77,7 @@ struct __align__(16) TrajState {
     int rk_part;       // 0: H_eff arg, 1: H_drv arg
     int rk_ctx;        // 0: step checked for a crossing; 1: begin part of a located jump
     int ens;           // ensemble of the trajectory (batched engines; 0 otherwise)
-    int rk_pad;
+    int rechk;         // split form: this step's norm test waits for its FP64 recheck
 };
 static_assert(sizeof(TrajState) == 144, "TrajState layout");
 
@@ -116,6 +128,21 @@ struct Params {
     int MDs, KS;                  // rows padded to 16 (MMA N), k-steps of 16 complex components
     int sstages;                  // depth of the split kernel's operand ring
     const unsigned char *usplit;  // [G][KS][4 planes: Re hi, Re lo, Im hi, Im lo][MDs rows x 16 k] bf16
+    // bf16 planes of the input vector of every bucket position, two buffers (micro-step s reads
+    // buffer s & 1 and its epilogue fills buffer (s + 1) & 1): group g's region starts at byte
+    // g_soff[g] and holds, for each k-step and plane, scap positions x 32 bytes in the tcgen05
+    // K-major core-matrix order (8-position groups of 256 bytes, the two K-halves 128 bytes apart)
+    unsigned char *stage;
+    size_t stage_bytes;           // one buffer
+    long long scap;               // positions per (group, k-step, plane), a multiple of 8
+    const long long *g_soff;      // [G]
+    // near-threshold FP64 rechecks of the split form: band (relative to the norm; 0: off), the
+    // recheck lists of the micro-steps ([3] counts, [2][n] trajectories) and the k rows of the
+    // FP64 matrix slabs streamed through the operand ring
+    double recheck_tol;
+    int *rcnt;
+    int *rlist;
+    int rchk_kb;
     // RK propagator (prop 1): groups 0 and 1 are H_eff and H_drv; psi has kRkSlots slots
     int prop;                     // 0 QJ split tree, 1 RK
     int rk_ns, period0, drv_type;

@@ -33,6 +33,7 @@ cudaError_t launch_clear_records(const Params &P, cudaStream_t st);
 cudaError_t launch_fp64_peak(double *out, int blocks, int iters, cudaStream_t st);
 size_t split_smem_bytes(int MDs, int MD, int stages);
 size_t split_stage_bytes(int MDs);
+size_t split_static_smem();
 cudaError_t launch_lpn(const Params &P, const LpnParams &L, int mode, double curr_time, int adr_dump,
                        cudaStream_t st);
 }  // namespace qjx
@@ -64,7 +65,7 @@ struct qjx_engine {
     double *d_purity = nullptr;
     // host mirrors
     int *h_cnt = nullptr;   // pinned [G]
-    int *h_ctrl = nullptr;  // pinned [8]
+    int *h_ctrl = nullptr;  // pinned [16]: the control words [0, 8), the split form's recheck count [8]
     std::vector<std::vector<double>> jt, jn, je;
     std::vector<std::vector<int>> jtype;
     qjx_stats stats{};
@@ -395,11 +396,30 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
         P.KS = (d + 15) / 16;
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
-        // deepest operand ring (2..8 stages) that fits next to 8 KB of static shared memory
+        // deepest operand ring (2..8 stages) that fits next to the kernel's static shared memory
+        const size_t fixed = split_static_smem() + 1024;
         P.sstages = 0;
         for (int st = 8; st >= 2 && !P.sstages; st--)
-            if (split_smem_bytes(P.MDs, MD, st) + 8192 <= (size_t)optin) P.sstages = st;
+            if (split_smem_bytes(P.MDs, MD, st) + fixed <= (size_t)optin) P.sstages = st;
         if (!P.sstages) return bail(QJX_ERR_UNSUPPORTED);
+        // input-vector planes of every bucket position, two buffers
+        P.scap = 8 * (((long long)n + 7) / 8);
+        const size_t greg = (size_t)P.KS * 4 * (size_t)P.scap * 32;
+        std::vector<long long> soff(G);
+        for (int gg = 0; gg < G; gg++) soff[gg] = (long long)(gg * greg);
+        P.g_soff = upload(h, soff);
+        P.stage_bytes = (size_t)G * greg;
+        P.stage = (unsigned char *)dalloc(h, 2 * P.stage_bytes);
+        // near-threshold FP64 rechecks: lists, band, and the matrix slab height that fits the ring
+        // next to the input and product vectors
+        P.rcnt = (int *)dalloc(h, 3 * sizeof(int));
+        P.rlist = (int *)dalloc(h, (size_t)2 * n * sizeof(int));
+        if (!P.g_soff || !P.stage || !P.rcnt || !P.rlist) return bail(QJX_ERR_OOM);
+        P.recheck_tol = c.split_recheck == 0.0 ? 1e-5 : (c.split_recheck < 0.0 ? 0.0 : c.split_recheck);
+        const size_t ring = (size_t)P.sstages * split_stage_bytes(P.MDs);
+        const size_t vec = (size_t)(2 * MD + 2) * sizeof(double2);
+        P.rchk_kb = std::min<int>(32, (int)((ring - vec) / (2 * (size_t)MD * sizeof(double2)))) & ~1;
+        if (P.rchk_kb < 2) return bail(QJX_ERR_UNSUPPORTED);
         const size_t per_s = (size_t)P.KS * 4 * P.MDs * 16;
         std::vector<uint16_t> hs((size_t)G * per_s, 0);
         for (int b = 0; b < c.num_branches; b++)
@@ -435,7 +455,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     P.r_eta = (double *)dalloc(h, rc * sizeof(double));
     P.r_type = (int *)dalloc(h, rc * sizeof(int));
     P.ctrl = (int *)dalloc(h, 16 * sizeof(int));
-    P.work = (long long *)dalloc(h, 2 * sizeof(long long));
+    P.work = (long long *)dalloc(h, 4 * sizeof(long long));
     if (!P.psi || !P.st || !P.gn || !P.cnt || !P.lists || !P.o_norm || !P.o_mean || !P.o_disp || !P.o_m2 ||
         !P.o_energy || !P.o_robs || !P.o_adr || !P.mean_start || !P.r_time || !P.r_norm || !P.r_eta || !P.r_type ||
         !P.ctrl || !P.work)
@@ -629,8 +649,8 @@ static qjx_status run_until_idle(qjx_engine *h)
     FILE *bucket_log = nullptr;
     if (const char *fn = getenv("QJX_TRACE_BUCKETS")) bucket_log = fopen(fn, "a");
     int64_t steps = 0;
-    long long work0[2] = {0, 0};
-    cudaMemcpy(work0, P.work, 2 * sizeof(long long), cudaMemcpyDeviceToHost);
+    long long work0[3] = {0, 0, 0};
+    cudaMemcpy(work0, P.work, 3 * sizeof(long long), cudaMemcpyDeviceToHost);
     cudaEventRecord(h->ev0, h->stream);
     while (true) {
         cudaEventRecord(h->eb0, h->stream);
@@ -649,7 +669,8 @@ static qjx_status run_until_idle(qjx_engine *h)
         const bool all_counts = P.split || bucket_log;
         if (all_counts) cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
         else cudaMemcpyAsync(h->h_cnt, P.plan + P.G, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
-        cudaMemcpyAsync(h->h_ctrl, P.ctrl, sizeof(int) * 16, cudaMemcpyDeviceToHost, h->stream);
+        if (P.split) cudaMemcpyAsync(h->h_ctrl + 8, P.rcnt, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        cudaMemcpyAsync(h->h_ctrl, P.ctrl, sizeof(int) * 8, cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
             rs = cuda_fail(h, e, "micro-step batch");
@@ -663,6 +684,7 @@ static qjx_status run_until_idle(qjx_engine *h)
         long long active = all_counts ? 0 : h->h_cnt[0];
         if (all_counts)
             for (int g = 0; g < P.G; g++) active += h->h_cnt[g];
+        if (P.split) active += h->h_ctrl[8];  // trajectories waiting for an FP64 recheck
         if (bucket_log) {
             for (int g = 0; g < P.G; g++) fprintf(bucket_log, g ? " %d" : "%d", h->h_cnt[g]);
             fprintf(bucket_log, "\n");
@@ -673,6 +695,7 @@ static qjx_status run_until_idle(qjx_engine *h)
                 if (rs != QJX_OK) break;
                 cudaMemsetAsync(P.ctrl + 2, 0, sizeof(int), h->stream);
                 cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream);
+                if (P.rcnt) cudaMemsetAsync(P.rcnt, 0, 3 * sizeof(int), h->stream);
                 cudaError_t le = launch_schedule(P, 1, h->stream);
                 h->stats.launches += 2;
                 if (le != cudaSuccess) {
@@ -694,10 +717,11 @@ static qjx_status run_until_idle(qjx_engine *h)
     h->stats.last_call_ms = ms;
     h->stats.micro_steps += steps;
     h->stats.launches += steps;
-    long long work1[2] = {0, 0};
-    cudaMemcpy(work1, P.work, 2 * sizeof(long long), cudaMemcpyDeviceToHost);
+    long long work1[3] = {0, 0, 0};
+    cudaMemcpy(work1, P.work, 3 * sizeof(long long), cudaMemcpyDeviceToHost);
     h->stats.matvecs += work1[0] - work0[0];
     h->stats.mma_tiles += work1[1] - work0[1];
+    h->stats.rechecks += work1[2] - work0[2];
     cudaGraphExecDestroy(exec);
     return rs;
 }
@@ -894,6 +918,7 @@ extern "C" qjx_status qjx_run_periods(qjx_engine *h, int n_periods, int is_obs, 
     P.subdump = subdump;
     P.record = (is_obs == 1 && h->cfg.record > 0) ? 1 : 0;
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
+    if (P.rcnt) CK(cudaMemsetAsync(P.rcnt, 0, 3 * sizeof(int), h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
     P.period0 = h->period_base;
     if (P.prop == 1) CK(launch_rk_schedule(P, h->stream));
@@ -928,6 +953,7 @@ extern "C" qjx_status qjx_run_sub_periods(qjx_engine *h, int n_sub, int dump_bas
     P.subdump = 1;
     P.record = h->cfg.record > 0 ? 1 : 0;
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
+    if (P.rcnt) CK(cudaMemsetAsync(P.rcnt, 0, 3 * sizeof(int), h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
     P.period0 = h->period_base;
     cudaError_t e = launch_schedule(P, 2, h->stream);
@@ -951,6 +977,7 @@ extern "C" qjx_status qjx_observe(qjx_engine *h, int dump, int is_start)
     P.record = 0;
     P.subdump = 0;
     CK(cudaMemsetAsync(P.cnt, 0, sizeof(int) * 3 * P.G, h->stream));
+    if (P.rcnt) CK(cudaMemsetAsync(P.rcnt, 0, 3 * sizeof(int), h->stream));
     CK(cudaMemsetAsync(P.ctrl, 0, sizeof(int) * 16, h->stream));
     CK(launch_observe(P, dump, is_start, h->stream));
     h->stats.launches += 1;

@@ -8,7 +8,7 @@
 //   Re y[m][r] = sum_k Xr[m][k] Ur[r][k] - Xi[m][k] Ui[r][k]     m: trajectory (128 TMEM lanes)
 //   Im y[m][r] = sum_k Xr[m][k] Ui[r][k] + Xi[m][k] Ur[r][k]     r: output row (MMA N = MDs)
 //
-//   A = the tile's states (Xr, Xi) as bf16 planes, written by the CTA from the FP64 states,
+//   A = the tile's input vectors (Xr, Xi) as bf16 planes,
 //   B = Re M and Im M as bf16 planes prepared once by the host,
 //   D = two FP32 accumulators in tensor memory, Re in columns [0, MDs), Im in [MDs, 2 MDs);
 //       the minus sign is the instruction descriptor's negate-A bit.
@@ -18,6 +18,14 @@
 // product and the FP32 accumulation error (measured about 4e-6 of max|y| per matvec at
 // d = 201).  The accumulators are read back to FP64 and the FP64 epilogue of the plain form
 // runs unchanged (norm test, jump, renormalisation, observables).
+//
+// Both operands arrive by TMA bulk copies.  The A planes of a micro-step are written by the
+// previous micro-step's epilogue: once a trajectory's next bucket and its position in it are
+// known, its next input vector (the new state, the renormalised state, or the unchanged input
+// of a bisection step) is split into bf16 planes and stored at that position of the next
+// step's stage buffer, already in the core-matrix order; a tile of R trajectories of one bucket
+// is then one contiguous copy of R x 32 bytes per plane and k-step.  (After a host-side enqueue
+// the stage buffer is filled from the FP64 states by stage_lists_kernel.)
 //
 // Shared-memory operands use the K-major no-swizzle canonical layout: a core matrix is
 // 8 rows x 16 bytes (8 bf16 along K) stored contiguously; within one k-step (16 bf16 of K)
@@ -114,16 +122,164 @@ __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo
     lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
+// Byte offset, in a stage buffer, of the 16-byte chunk (k-step ks, plane p, K-half kh) of bucket
+// position pos of group g.
+__device__ __forceinline__ size_t stage_chunk(const Params &P, int g, int ks, int p, int kh, int pos)
+{
+    return (size_t)P.g_soff[g] + ((size_t)(ks * kAPlanes + p) * (size_t)P.scap + (size_t)(pos & ~7)) * 32 +
+           (size_t)kh * 128 + (size_t)(pos & 7) * 16;
+}
+
+// Writes the bf16 planes of a trajectory's next input vector at position pos of group g of the
+// stage buffer `dst` (warp-cooperative; a lane converts 8 consecutive components, one K-half of
+// one k-step, into its four 16-byte chunks).  Components from d on are zero.  The vector is
+// col, col / div, the planes at position pos0 of group g0 in `src_stage`, or gsrc.
+__device__ void stage_write(const Params &P, unsigned char *dst, int g, int pos, int mode, const double2 *col,
+                            double div, const double2 *gsrc, const unsigned char *src_stage, int g0, int pos0, int d,
+                            int lane)
+{
+    for (int pr = lane; pr < 2 * P.KS; pr += 32) {
+        const int ks = pr >> 1, kh = pr & 1;
+        uint4 c[kAPlanes];
+        if (mode == SRC_SAME) {
+#pragma unroll
+            for (int p = 0; p < kAPlanes; p++)
+                c[p] = *reinterpret_cast<const uint4 *>(src_stage + stage_chunk(P, g0, ks, p, kh, pos0));
+        } else {
+            double2 v[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int k = 16 * ks + 8 * kh + i;
+                double2 x = make_double2(0.0, 0.0);
+                if (k < d) {
+                    if (mode == SRC_GLOBAL) {
+                        x = gsrc[k];
+                    } else {
+                        x = col[k];
+                        if (mode == SRC_SCALED) x = make_double2(__ddiv_rn(x.x, div), __ddiv_rn(x.y, div));
+                    }
+                }
+                v[i] = x;
+            }
+            uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                split_pair(make_double2(v[2 * j].x, v[2 * j + 1].x), rh[j], rl[j]);
+                split_pair(make_double2(v[2 * j].y, v[2 * j + 1].y), ih[j], il[j]);
+            }
+            c[0] = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+            c[1] = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+            c[2] = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+            c[3] = make_uint4(il[0], il[1], il[2], il[3]);
+        }
+#pragma unroll
+        for (int p = 0; p < kAPlanes; p++) *reinterpret_cast<uint4 *>(dst + stage_chunk(P, g, ks, p, kh, pos)) = c[p];
+    }
+}
+
+// Planes of step 0 after a host-side enqueue (schedule, observe, resume): block (x, g) takes
+// positions of bucket g, one warp per position, from the trajectories' FP64 input slots.
+__global__ void stage_lists_kernel(const Params P)
+{
+    const int g = blockIdx.y, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int cnt = P.cnt[g];
+    for (int pos = blockIdx.x * nw + (threadIdx.x >> 5); pos < cnt; pos += gridDim.x * nw) {
+        const int tr = P.lists[P.g_loff[g] + pos];
+        const TrajState s = P.st[tr];
+        const int slot = src_slot(s.phase, s.cur, s.rk_stage);
+        stage_write(P, P.stage, g, pos, SRC_GLOBAL, nullptr, 1.0, slot_ptr(P, slot, tr), nullptr, 0, 0, dim_of(P, s),
+                    lane);
+    }
+}
+
+// FP64 recheck of one trajectory's step (split form): y = M x with the plain form's arithmetic
+// (per output the k-ascending fma chain of the contract, k up to the even kp), the matrix
+// streamed through the free operand ring in slabs of kb k rows by TMA bulk copies (two buffers,
+// mbarriers rbar[0..1]), then the epilogue decides with the FP64 norm and the trajectory is
+// appended to its next bucket with its next input's planes.  Whole CTA; returns false when a
+// bounded wait gave up.
+__device__ bool recheck_column(const Params &P, int tr, unsigned char *smem, TrajState *st_s, uint64_t *rbar,
+                               uint32_t &rphase, int *cnt_next, int *list_next, unsigned char *stage_next)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) load_state(st_s, &P.st[tr]);
+    __syncthreads();
+    const TrajState st = *st_s;
+    const int dg = P.e_d[st.ens], MDg = 8 * ((dg + 7) / 8), kp = (dg + 1) & ~1, kb = P.rchk_kb;
+    const int g = P.e_g0[st.ens] + st.b * P.deep + st.lvl;
+    const double2 *mat = P.mats + P.g_off[g];
+    double2 *slab = reinterpret_cast<double2 *>(smem);  // [2][kb][MDg]
+    double2 *xs = slab + 2 * (size_t)kb * MDg;           // [kp] input
+    double2 *ys = xs + kp;                               // [MDg] FP64 product
+    const double2 *x = slot_ptr(P, st.cur, tr);
+    for (int k = tid; k < kp; k += blockDim.x) xs[k] = (k < dg) ? x[k] : make_double2(0.0, 0.0);
+    const int nslab = (kp + kb - 1) / kb;
+    if (tid == 0) {
+        fence_proxy_async();
+        for (int q = 0; q < 2 && q < nslab; q++) {
+            const int kc = min(kb, kp - q * kb);
+            mbar_expect_tx(&rbar[q], (uint32_t)(kc * MDg * 16));
+            bulk_g2s(slab + (size_t)q * kb * MDg, mat + (size_t)q * kb * MDg, (uint32_t)(kc * MDg * 16), &rbar[q]);
+        }
+    }
+    __syncthreads();
+    bool ok = true;
+    double re = 0.0, im = 0.0;
+    for (int sl = 0; sl < nslab; sl++) {
+        const int q = sl & 1;
+        if (!mbar_wait_bounded(&rbar[q], (rphase >> q) & 1u, kSplitWait)) ok = false;
+        rphase ^= 1u << q;
+        const int k0 = sl * kb, kc = min(kb, kp - k0);
+        if (ok && tid < dg) {
+            const double2 *Mq = slab + (size_t)q * kb * MDg + tid;
+            for (int kk = 0; kk < kc; kk++) {
+                const double2 m = Mq[(size_t)kk * MDg], v = xs[k0 + kk];
+                re = __fma_rn(m.x, v.x, re);
+                re = __fma_rn(-m.y, v.y, re);
+                im = __fma_rn(m.x, v.y, im);
+                im = __fma_rn(m.y, v.x, im);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && ok && sl + 2 < nslab) {
+            const int kn = min(kb, kp - (sl + 2) * kb);
+            fence_proxy_async();
+            mbar_expect_tx(&rbar[q], (uint32_t)(kn * MDg * 16));
+            bulk_g2s(slab + (size_t)q * kb * MDg, mat + (size_t)(sl + 2) * kb * MDg, (uint32_t)(kn * MDg * 16), &rbar[q]);
+        }
+    }
+    if (!__syncthreads_and(ok ? 1 : 0)) return false;
+    if (tid < dg) ys[tid] = make_double2(re, im);
+    __syncthreads();
+    if (warp == 0) {
+        EpiOut eo{SRC_NONE, 0, 1.0};
+        const int g2 = column_epilogue(P, ys, tr, st, lane, &eo);
+        if (g2 >= 0) {
+            int pos = 0;
+            if (lane == 0) {
+                pos = atomicAdd(&cnt_next[g2], 1);
+                list_next[P.g_loff[g2] + pos] = tr;
+            }
+            pos = __shfl_sync(0xffffffffu, pos, 0);
+            // the unchanged input of a bisection step has no planes at a position of this step
+            const int mode = (eo.mode == SRC_SAME) ? SRC_GLOBAL : eo.mode;
+            stage_write(P, stage_next, g2, pos, mode, ys, eo.div, slot_ptr(P, eo.slot, tr), nullptr, 0, 0, dg, lane);
+        }
+    }
+    fence_proxy_async();  // generic writes to the ring before later bulk copies into it
+    __syncthreads();
+    return true;
+}
+
 // Dynamic shared memory: a ring of `stages` operand stages, each [A planes][B planes] of one
-// k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs+1)),
-// the per-warp epilogue scratch (16 x MD) and the tile's 128 trajectory records.
+// k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs + 1)).
 size_t split_stage_bytes(int MDs) { return (size_t)kAPlanes * (kABytes + (size_t)MDs * 32); }
 
 size_t split_smem_bytes(int MDs, int MD, int stages)
 {
     const size_t ring = (size_t)stages * split_stage_bytes(MDs);
     (void)MD;
-    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2) + (size_t)kTileM * sizeof(TrajState);
+    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2);
     return ring > epi ? ring : epi;
 }
 
@@ -135,34 +291,44 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const size_t stage_bytes = (size_t)kAPlanes * (kABytes + bbytes);
     const int S16 = MDs + 1;
     double2 *Bt = reinterpret_cast<double2 *>(smem);          // epilogue: [32][S16] FP64 columns
-    TrajState *s_st = reinterpret_cast<TrajState *>(Bt + 32 * S16);  // [128]
-    __shared__ __align__(8) uint64_t fullA[kMaxSStages], fullB[kMaxSStages], empty[kMaxSStages], accf;
+    __shared__ __align__(8) uint64_t full[kMaxSStages], empty[kMaxSStages], accf, rbar[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_tstart[kMaxGroups + 1];
     __shared__ int s_tr[kTileM];
-    __shared__ long long s_src[kTileM];
+    __shared__ __align__(16) TrajState s_st[kTileM];
     __shared__ int s_fail;
     __shared__ int s_rows;  // trajectories per tile in this micro-step
     __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
-    __shared__ int s_g2[kTileM];
+    __shared__ int s_g2[32], s_pos[32];
+    __shared__ EpiOut s_eo[32];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int G = P.G, n = P.n, d = P.d;
+    const int G = P.G;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
     const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
     int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
+    const unsigned char *stage_cur = P.stage + (size_t)(s & 1) * P.stage_bytes;
+    unsigned char *stage_next = P.stage + (size_t)((s + 1) & 1) * P.stage_bytes;
+    const int *rlist_cur = P.rlist + (size_t)(s & 1) * P.n;
+    int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
+    int *rcnt_next = P.rcnt + (s + 1) % 3;
+    const int Rtot = P.rcnt[s % 3];  // FP64 rechecks of this micro-step
 
     for (int i = tid; i < G; i += kThreads) cnt_cur[i] = P.cnt[(s % 3) * G + i];
-    if (blockIdx.x == 0)
+    if (blockIdx.x == 0) {
         for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
+        if (tid == 0) P.rcnt[(s + 2) % 3] = 0;
+    }
     __syncthreads();
     if (warp == 0) {
-        // rows per tile: the smallest multiple of 8 (<= 128) whose tiles fit one wave of CTAs, so
-        // the trajectories (and their epilogues) spread over all SMs; 128 when none does
+        // rows per tile: the smallest multiple of 8 (<= 128) whose tiles fit one wave of CTAs next
+        // to the FP64 rechecks, so the trajectories (and their epilogues) spread over all SMs; 128
+        // when none does
+        const int avail = max(1, (int)gridDim.x - Rtot);
         int tiles = 0;
         if (lane < 16)
             for (int g = 0; g < G; g++) tiles += (cnt_cur[g] + 8 * lane + 7) / (8 * lane + 8);
-        const unsigned fit = __ballot_sync(0xffffffffu, lane < 16 && tiles <= (int)gridDim.x);
+        const unsigned fit = __ballot_sync(0xffffffffu, lane < 16 && tiles <= avail);
         const int R = fit ? 8 * (__ffs(fit)) : kTileM;
         if (lane == 0) {
             s_rows = R;
@@ -173,11 +339,12 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             }
             s_tstart[G] = acc;
             for (int q = 0; q < S; q++) {
-                mbar_init(&fullA[q], kTileM);
-                mbar_init(&fullB[q], 1);
+                mbar_init(&full[q], 1);
                 mbar_init(&empty[q], 1);
             }
             mbar_init(&accf, 1);
+            mbar_init(&rbar[0], 1);
+            mbar_init(&rbar[1], 1);
             s_fail = 0;
             fence_proxy_async();
         }
@@ -195,13 +362,22 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const int T = s_tstart[G];
     const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
     const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
-    long long work = 0;
-    uint32_t ntile = 0;
+    long long work = 0, nrechk = 0;
+    uint32_t ntile = 0, rphase = 0;
     bool ok = true;
     long long tr_setup = 0, tr_mma = 0, tr_stage = 0, tr_epi = 0;
     const long long t_begin = clock64();
 
-    for (int t = blockIdx.x; t < T && ok; t += gridDim.x, ntile++) {
+    for (int t = blockIdx.x; t < T + Rtot && ok; t += gridDim.x) {
+        if (t >= T) {  // an FP64 recheck (the CTAs past the split tiles take these first)
+            if (!recheck_column(P, rlist_cur[t - T], smem, &s_st[0], rbar, rphase, cnt_next, list_next, stage_next)) {
+                ok = false;
+                break;
+            }
+            work += 1;
+            nrechk += 1;
+            continue;
+        }
         const long long t0 = clock64();
         int lo = 0, hi = G;
         while (hi - lo > 1) {
@@ -212,74 +388,34 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         const int g = lo;
         const int base = (t - s_tstart[g]) * s_rows;
         const int rows = min(s_rows, cnt_cur[g] - base);
-        if (tid < kTileM) {
-            if (tid < rows) {
-                const int tr = list_cur[P.g_loff[g] + base + tid];
-                const int slot = src_slot(P.st[tr].phase, P.st[tr].cur, P.st[tr].rk_stage);
-                s_tr[tid] = tr;
-                s_src[tid] = ((long long)slot * n + tr) * P.MD;
-            } else {
-                s_tr[tid] = -1;
-                s_src[tid] = -1;
-            }
-        }
-        __syncthreads();
-        const long long t1 = clock64();
+        const int rows8 = (rows + 7) & ~7;
         const uint32_t it0 = ntile * (uint32_t)KS;  // k-steps issued before this tile
+        const long long t1 = clock64();
 
-        const int agrp = (warp < 4) ? 0 : (warp >= 6 && warp < 10) ? 1 : (warp >= 10 && warp < 14) ? 2 : -1;
-        if (agrp >= 0) {
-            // A producers: group p (4 warps, thread m = row m) handles the k-steps ks = p (mod 3), so
-            // three independent load-convert chains run in parallel; each thread issues its loads
-            // before waiting for the stage to drain
-            const int m = tid - (agrp == 0 ? 0 : (agrp == 1 ? 192 : 320));
-            const double2 *src = (s_src[m] >= 0) ? P.psi + s_src[m] : nullptr;
-            const int off = (m & 7) * 16 + (m >> 3) * 256;
-            for (int ks = agrp; ks < KS && ok; ks += 3) {
-                const uint32_t it = it0 + ks, q = it % S;
-                unsigned char *As = smem + q * stage_bytes + off;
-                for (int hh = 0; hh < 2; hh++) {  // K-halves: components 16 ks + 8 hh .. + 7
-                    double2 v[8];
-#pragma unroll
-                    for (int i = 0; i < 8; i++) {
-                        const int k = 16 * ks + 8 * hh + i;
-                        v[i] = (src && k < d) ? src[k] : make_double2(0.0, 0.0);
-                    }
-                    if (hh == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
-                        ok = false;
-                    uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        split_pair(make_double2(v[2 * j].x, v[2 * j + 1].x), rh[j], rl[j]);
-                        split_pair(make_double2(v[2 * j].y, v[2 * j + 1].y), ih[j], il[j]);
-                    }
-                    *reinterpret_cast<uint4 *>(As + 128 * hh) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-                    *reinterpret_cast<uint4 *>(As + kABytes + 128 * hh) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-                    *reinterpret_cast<uint4 *>(As + 2 * kABytes + 128 * hh) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-                    *reinterpret_cast<uint4 *>(As + 3 * kABytes + 128 * hh) = make_uint4(il[0], il[1], il[2], il[3]);
-                }
-                fence_proxy_async();
-                mbar_arrive(&fullA[q]);
-            }
-        } else if (warp == 4) {
-            if (lane == 0) {  // B producer
+        if (warp == 4) {
+            if (lane == 0) {  // producer: per k-step the four A planes of the tile's rows and the B planes
                 const unsigned char *ug = P.usplit + (size_t)g * KS * kAPlanes * bbytes;
+                const uint32_t abytes = (uint32_t)rows8 * 32;
                 for (int ks = 0; ks < KS && ok; ks++) {
                     const uint32_t it = it0 + ks, q = it % S;
                     if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait)) {
                         ok = false;
                         break;
                     }
-                    mbar_expect_tx(&fullB[q], (uint32_t)(kAPlanes * bbytes));
-                    bulk_g2s(smem + q * stage_bytes + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes,
-                             (uint32_t)(kAPlanes * bbytes), &fullB[q]);
+                    unsigned char *dq = smem + q * stage_bytes;
+                    mbar_expect_tx(&full[q], kAPlanes * (abytes + (uint32_t)bbytes));
+#pragma unroll
+                    for (int p = 0; p < kAPlanes; p++)
+                        bulk_g2s(dq + p * kABytes, stage_cur + stage_chunk(P, g, ks, p, 0, base), abytes, &full[q]);
+                    bulk_g2s(dq + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes, (uint32_t)(kAPlanes * bbytes),
+                             &full[q]);
                 }
             }
         } else if (warp == 5) {
             if (lane == 0) {  // MMA issuer
                 for (int ks = 0; ks < KS && ok; ks++) {
                     const uint32_t it = it0 + ks, q = it % S, par = (it / S) & 1u;
-                    if (!mbar_wait_bounded(&fullA[q], par, kSplitWait) || !mbar_wait_bounded(&fullB[q], par, kSplitWait)) {
+                    if (!mbar_wait_bounded(&full[q], par, kSplitWait)) {
                         ok = false;
                         break;
                     }
@@ -310,6 +446,13 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                 }
                 umma_commit(&accf);
             }
+        } else if (warp < 4) {
+            // the tile's trajectories and their state records, loaded while the MMAs run
+            if (tid < rows) {
+                const int tr = list_cur[P.g_loff[g] + base + tid];
+                s_tr[tid] = tr;
+                load_state(&s_st[tid], &P.st[tr]);
+            }
         }
         if (!ok) atomicExch(&s_fail, 1);
         // accumulator complete (every thread waits on the commit); the ring is free afterwards
@@ -320,8 +463,6 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             ok = false;
             break;
         }
-        // the tile's state records, all loaded at once (one L2 round trip for the whole tile)
-        for (int m = tid; m < rows; m += kThreads) load_state(&s_st[m], &P.st[s_tr[m]]);
         const long long t2 = clock64();
         for (int c = 0; c < 4 && 32 * c < rows; c++) {
             const long long ts = clock64();
@@ -341,17 +482,45 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             tr_stage += clock64() - ts;
             for (int cc = warp; cc < 32; cc += kThreads / 32) {
                 const int m = 32 * c + cc;
-                if (m < rows) {
-                    const int g2 = column_epilogue(P, Bt + (size_t)cc * S16, s_tr[m], s_st[m], lane);
-                    if (lane == 0) s_g2[m] = g2;
+                int g2 = -1;
+                EpiOut eo{SRC_NONE, 0, 1.0};
+                if (m < rows) g2 = column_epilogue(P, Bt + (size_t)cc * S16, s_tr[m], s_st[m], lane, &eo);
+                if (lane == 0) {
+                    s_g2[cc] = g2;
+                    s_eo[cc] = eo;
+                }
+            }
+            __syncthreads();
+            if (warp == 0) {  // positions in the next buckets: one atomic per distinct bucket of the 32 columns
+                const int g2 = s_g2[lane];
+                const unsigned mm = __match_any_sync(0xffffffffu, g2);
+                const int leader = __ffs(mm) - 1;
+                int b0 = 0;
+                if (g2 != -1 && lane == leader) b0 = atomicAdd(g2 >= 0 ? &cnt_next[g2] : rcnt_next, __popc(mm));
+                b0 = __shfl_sync(0xffffffffu, b0, leader);
+                const int pos = b0 + __popc(mm & ((1u << lane) - 1u));
+                if (g2 >= 0) {
+                    s_pos[lane] = pos;
+                    list_next[P.g_loff[g2] + pos] = s_tr[32 * c + lane];
+                } else if (g2 == kRecheck) {
+                    rlist_next[pos] = s_tr[32 * c + lane];
+                }
+            }
+            __syncthreads();
+            for (int cc = warp; cc < 32; cc += kThreads / 32) {  // the next input vectors' planes
+                const int m = 32 * c + cc, g2 = s_g2[cc];
+                if (m < rows && g2 >= 0) {
+                    const EpiOut eo = s_eo[cc];
+                    const int tr = s_tr[m];
+                    stage_write(P, stage_next, g2, s_pos[cc], eo.mode, Bt + (size_t)cc * S16, eo.div,
+                                slot_ptr(P, eo.slot, tr), stage_cur, g, base + m, P.e_d[s_st[m].ens], lane);
                 }
             }
             fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
             __syncthreads();
         }
-        __syncthreads();
-        enqueue_batch(P, cnt_next, list_next, s_tr, s_g2, rows);
         work += rows;
+        ntile++;
         const long long t3 = clock64();
         tr_setup += t1 - t0;
         tr_mma += t2 - t1;
@@ -364,11 +533,16 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             umma_commit(&accf);
             mbar_wait_bounded(&accf, ntile & 1u, kSplitWait);
         }
-        if (warp == 4 && lane == 0)
+        if (warp == 4 && lane == 0) {
             for (int q = 0; q < S; q++) {
-                mbar_wait_bounded(&fullB[q], 0u, 1024);
-                mbar_wait_bounded(&fullB[q], 1u, 1024);
+                mbar_wait_bounded(&full[q], 0u, 1024);
+                mbar_wait_bounded(&full[q], 1u, 1024);
             }
+            for (int q = 0; q < 2; q++) {
+                mbar_wait_bounded(&rbar[q], 0u, 1024);
+                mbar_wait_bounded(&rbar[q], 1u, 1024);
+            }
+        }
         if (tid == 0) {
             atomicAdd(&P.ctrl[4], 1);
             report_error(P, -1, ERR_TIMEOUT);
@@ -383,6 +557,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     }
     if (tid == 0 && work) atomicAdd((unsigned long long *)P.work, (unsigned long long)work);
     if (tid == 0 && ntile) atomicAdd((unsigned long long *)(P.work + 1), (unsigned long long)ntile);
+    if (tid == 0 && nrechk) atomicAdd((unsigned long long *)(P.work + 2), (unsigned long long)nrechk);
     if (P.trace && tid == 0) {  // fields: total, setup, -, MMA phase, epilogue, tiles, TMEM staging, rows
         long long *tr = P.trace + (size_t)blockIdx.x * kTraceFields;
         tr[0] += clock64() - t_begin;

@@ -15,7 +15,8 @@ class Engine:
     """One ensemble of trajectories resident on a GPU."""
 
     def __init__(self, U, L, g, HE, R=None, T=2 * np.pi, n_traj=1, seed=0, record=0, rng_kind=0, rec_cap=1024,
-                 keep_adr=0, max_dumps=1, device=0, tr_base=0, precision=0, deep_num_steps=0, branch_len=None):
+                 keep_adr=0, max_dumps=1, device=0, tr_base=0, precision=0, deep_num_steps=0, branch_len=None,
+                 split_recheck=0.0):
         U = np.ascontiguousarray(U, np.complex128)
         nb, deep, d, _ = U.shape
         L = np.ascontiguousarray(L, np.complex128).reshape(-1, d, d)
@@ -28,6 +29,7 @@ class Engine:
         cfg.rng_kind, cfg.seed, cfg.rec_cap, cfg.keep_adr = rng_kind, seed, rec_cap, keep_adr
         cfg.max_dumps, cfg.device, cfg.tr_base = max_dumps, device, tr_base
         cfg.precision = precision  # 0 complex FP64, 1 split bf16x3 on tcgen05
+        cfg.split_recheck = split_recheck  # split form: FP64 recheck band (0: default 1e-5, < 0: off)
         cfg.deep_num_steps = deep_num_steps  # > 0: StdDeep task (U from build_dimer_deep)
         self._branch_len = None if branch_len is None else np.ascontiguousarray(branch_len, np.float64)
         cfg.branch_len = N.dp(self._branch_len)  # per-branch durations (None: T / 2 each)
@@ -287,16 +289,34 @@ class Engine:
         out["eps_iters"] = it
         return out
 
-    def checkpoint(self):
-        """The engine's complete trajectory state as bytes (qjx_checkpoint_save)."""
+    def checkpoint(self, out=None):
+        """The engine's complete trajectory state (qjx_checkpoint_save): bytes, or written into the
+        caller's uint8 numpy array `out` (e.g. pinned host memory) and returned as its used prefix."""
         size = C.c_size_t()
         self._chk(N.lib().qjx_checkpoint_size(self.h, C.byref(size)), "qjx_checkpoint_size")
+        if out is not None:
+            if out.dtype != np.uint8 or out.nbytes < size.value or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"checkpoint needs a contiguous uint8 buffer of {size.value} bytes")
+            self._chk(N.lib().qjx_checkpoint_save(self.h, out.ctypes.data_as(C.c_void_p), size.value),
+                      "qjx_checkpoint_save")
+            return out[: size.value]
         buf = C.create_string_buffer(size.value)
         self._chk(N.lib().qjx_checkpoint_save(self.h, buf, size.value), "qjx_checkpoint_save")
         return buf.raw
 
+    def checkpoint_size(self):
+        size = C.c_size_t()
+        self._chk(N.lib().qjx_checkpoint_size(self.h, C.byref(size)), "qjx_checkpoint_size")
+        return size.value
+
     def restore(self, blob):
-        """Continue from a checkpoint of an engine with the same configuration."""
+        """Continue from a checkpoint of an engine with the same configuration (bytes, or a uint8
+        numpy array such as a pinned host buffer)."""
+        if isinstance(blob, np.ndarray):
+            blob = np.ascontiguousarray(blob, np.uint8)
+            self._chk(N.lib().qjx_checkpoint_load(self.h, blob.ctypes.data_as(C.c_void_p), blob.nbytes),
+                      "qjx_checkpoint_load")
+            return
         buf = C.create_string_buffer(blob, len(blob))
         self._chk(N.lib().qjx_checkpoint_load(self.h, buf, len(blob)), "qjx_checkpoint_load")
 

@@ -138,3 +138,15 @@ def test_missing_files_use_defaults(tmp_path):
     r = subprocess.run([EXE, "--check"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
     assert "Unable to open file" in r.stdout and "Init with default params" in r.stdout
     assert r.returncode != 0  # default task_id 0 is not the Std task
+
+
+def test_config_tokenisation_edge_cases(tmp_path):
+    """Only the single space separates tokens, runs of spaces and spaces at either end make no
+    token, and a tab stays inside its token (so such a line has one token and is ignored)."""
+    extra = "seed\t5\n  mns   77  \n num_trajectories  7 \n  \nex_deep 12 \t\n"
+    r = check(tmp_path, BASE_CONFIG, BASE_PARAMS, extra)
+    assert r.returncode == 0, r.stdout
+    assert "mns = 77" in r.stdout and "num_trajectories = 7" in r.stdout
+    assert "seed = 5" not in r.stdout
+    # "ex_deep 12 \t" has the tokens "ex_deep", "12" and "\t": three tokens, ignored
+    assert "ex_deep = 12" not in r.stdout

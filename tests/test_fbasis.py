@@ -161,3 +161,40 @@ def test_gpu_cluster_rk4_matches_oracle_and_stage_kernels(N, monkeypatch):
     assert np.all(np.isfinite(x_c)) and np.array_equal(x_c, x_s)
     x_o = O.fb_rk4(Gc, Qc, Ks, x0, 1.5, drv_type=0, T=T2PI, num_steps=steps, n_periods=2)
     assert np.array_equal(x_c, x_o)
+
+
+def _fb_system(N):
+    """CSR Gs, Qs_drv and Ks of the dimer from the library's builder (the oracle's dense projection
+    would hold n^2 doubles at these sizes), as scipy matrices for the oracle's RK4."""
+    import scipy.sparse as sp
+
+    from os_d_b200 import _native as Nt
+
+    (gr, gc, gv), (qr, qc, qv), ks = Nt.fb_build_dimer(N, 1.0, 0.5, 1.0, 0.1)
+    n = (N + 1) ** 2 - 1
+    return sp.csr_matrix((gv, gc, gr), shape=(n, n)), sp.csr_matrix((qv, qc, qr), shape=(n, n)), ks
+
+
+@pytest.mark.gpu
+def test_gpu_stage_kernels_beyond_the_cluster_match_oracle_and_repeat(monkeypatch):
+    """N = 100 (n = 10,200) does not fit the cluster-resident path: the per-stage kernels, whose
+    rows read other rows' stage arguments, run over 8,400 blocks that cannot all be resident at
+    once.  60 RK4 steps across a sign change of the drive equal the oracle bit for bit, twice."""
+    import os_d_b200 as q
+
+    N = 100
+    Gc, Qc, Ks = _fb_system(N)
+    x0 = q.fbasis_pure_state(N, 0)
+    steps, T, period0 = 60, 0.24, 12  # t in [2.88, 3.12] and [3.12, 3.36]: sign(sin t) flips at pi
+    monkeypatch.setenv("QJX_FB_PATH", "stages")
+    runs = []
+    for _ in range(2):
+        fb = q.FBasis(Gc, Qc, Ks, x0, 1.5, drv_type=0, T=T, num_steps=steps)
+        assert fb.cluster_size() == 0
+        fb.run(period0, 2)
+        runs.append(fb.get()[0])
+        fb.close()
+    x_o = O.fb_rk4(Gc, Qc, Ks, x0, 1.5, drv_type=0, T=T, num_steps=steps, period0=period0, n_periods=2)
+    assert np.all(np.isfinite(x_o)) and np.abs(x_o - x0).max() > 1e-6
+    assert np.array_equal(runs[0], x_o)
+    assert np.array_equal(runs[1], x_o)

@@ -10,19 +10,41 @@ from tests.helpers import dimer_problem, start_states
 pytestmark = pytest.mark.gpu
 
 
-def run(P, n, periods, precision, seed=3):
+def run(P, n, periods, precision, seed=3, split_recheck=0.0, want_stats=False):
     import os_d_b200 as q
 
     eng = q.Engine(P["U"], P["L"], [1.0], P["HE"], None, P["T"], n, seed=seed, record=1, max_dumps=2, rec_cap=4096,
-                   keep_adr=1, precision=precision)
+                   keep_adr=1, precision=precision, split_recheck=split_recheck)
     eng.set_states(start_states(n, P["d"], 0, 0))
     eng.init_thresholds()
     eng.observe(0, is_start=True)
     eng.run_periods(periods, dump_at=[periods], dump_base=1)
     psi, t, eta, jc = eng.states()
     obs = eng.observables(1, 1)
+    st = eng.stats()
     eng.close()
-    return psi, jc, obs
+    return (psi, jc, obs, st) if want_stats else (psi, jc, obs)
+
+
+@pytest.mark.parametrize("N", [20, 200])
+def test_split_recheck_of_every_step_reproduces_fp64_bit_for_bit(N):
+    """With no dissipation every norm test passes, and a recheck band of 1 sends every step to the
+    FP64 recheck, whose product follows the plain form's arithmetic: the states after 2 periods
+    equal the plain form's bit for bit, and every matvec of the run was taken twice."""
+    P = dimer_problem(N, g=0.0)
+    psi_s, jc_s, _, st = run(P, 40, 2, 1, split_recheck=1.0, want_stats=True)
+    psi_d, jc_d, _ = run(P, 40, 2, 0)
+    assert jc_s.sum() == 0 and jc_d.sum() == 0
+    assert np.array_equal(psi_s, psi_d)
+    assert st["rechecks"] == 40 * 2 * 4  # 2 periods x 2 branches x 2 level-0 steps
+
+
+def test_split_without_recheck_runs_and_counts_none():
+    P = dimer_problem(20)
+    psi, jc, _, st = run(P, 64, 2, 1, split_recheck=-1.0, want_stats=True)
+    assert st["rechecks"] == 0 and jc.sum() > 0
+    nrm = np.linalg.norm(psi, axis=1)
+    assert np.all(np.isfinite(nrm)) and nrm.max() < 1 + 1e-4 and nrm.min() > 0
 
 
 def test_split_unitary_dynamics_matches_fp64():
