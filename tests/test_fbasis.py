@@ -198,3 +198,44 @@ def test_gpu_stage_kernels_beyond_the_cluster_match_oracle_and_repeat(monkeypatc
     assert np.all(np.isfinite(x_o)) and np.abs(x_o - x0).max() > 1e-6
     assert np.array_equal(runs[0], x_o)
     assert np.array_equal(runs[1], x_o)
+
+
+@pytest.mark.gpu
+def test_config3_qj_ensemble_within_3_sigma_of_fbasis_rho():
+    """Configuration 3: dimer N = 50 (d = 51; J 1, U 0.5, E 1, A 1.5, g 0.1), the QJ ensemble of 10^4
+    trajectories from |N,0> against the f-basis density matrix from the same state (Liouvillian from
+    the library's builder, RK4 with dt = 1e-3: 6284 steps per period), both on the GPU.  After 40
+    periods (the periodic steady state: the populations change by less than their statistical error
+    between the last two dumps) every one of the 51 populations lies within 3 standard errors of the
+    ensemble estimate, with no absolute slack."""
+    import math
+
+    import os_d_b200 as q
+
+    N, n, J, U, E, A, g = 50, 10000, 1.0, 0.5, 1.0, 1.5, 0.1
+    dumps = [10, 20, 30, 40]
+    Gc, Qc, Ks = _fb_system(N)
+    steps = math.ceil(T2PI / 1e-3)
+    fb = q.FBasis(Gc, Qc, Ks, q.fbasis_pure_state(N, 0), A, T=T2PI, num_steps=steps)
+    H, Hd, L, Ut = q.build_dimer(N, J, U, E, A, g, 1.0, 16)
+    eng = q.Engine(Ut, L, [1.0], H + E * Hd, None, T2PI, n, seed=7, max_dumps=len(dumps) + 1, keep_adr=1)
+    psi0 = np.zeros((n, N + 1), complex)
+    psi0[:, 0] = 1
+    eng.set_states(psi0)
+    eng.init_thresholds()
+    eng.run_periods(dumps[-1], dump_at=dumps, dump_base=1)
+    adr = eng.observables(1, len(dumps), want_adr=True)["adr"]
+    eng.close()
+    zmax, done = [], 0
+    for i, p in enumerate(dumps):
+        fb.run(done, p - done)
+        done = p
+        pops_f = np.real(np.diag(O.fb_rho(N, fb.get()[0])))
+        est, err = adr[i].mean(axis=0), adr[i].std(axis=0) / np.sqrt(n)
+        assert np.all(err > 0)
+        zmax.append(float(np.abs((est - pops_f) / err).max()))
+    fb.close()
+    print("max |z| per dump (periods %s): %s" % (dumps, zmax))
+    last = adr[-1].mean(axis=0) - adr[-2].mean(axis=0)
+    assert np.all(np.abs(last) < 3 * np.hypot(adr[-1].std(axis=0), adr[-2].std(axis=0)) / np.sqrt(n))
+    assert zmax[-1] <= 3.0
