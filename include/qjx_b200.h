@@ -55,6 +55,16 @@ typedef enum {
 
 typedef struct qjx_engine qjx_engine;
 
+/* Tile shapes of the micro-step kernels.  All zero: the engine's rule, or the choice the autotuner
+ * (qjx_autotune) cached for this dimension and precision.  Tiles never change results: every
+ * output keeps its own summation order whatever the tiling. */
+typedef struct {
+    int nc;      /* plain form: trajectory columns per sub-tile (32, 16 or 8) */
+    int kb;      /* plain form: k rows per propagator slab (even, 2..16) */
+    int stages;  /* split form: depth of the operand ring (2..8) */
+    int rows;    /* split form: fewest trajectories per tcgen05 tile (multiple of 8, 8..128) */
+} qjx_tiles;
+
 typedef struct {
     int d;             /* sys_size (N + 1 for the dimer) */
     int n_traj;        /* num_trajectories */
@@ -94,6 +104,7 @@ typedef struct {
                           matvec is computed again in FP64 (the plain form's arithmetic) in the next
                           micro-step and decides.  0 selects 1e-5 (about 5x the measured split error
                           of the norm), a negative value turns the recheck off. */
+    qjx_tiles tiles;   /* tile shapes (all 0: rule or autotuner cache) */
 } qjx_config;
 
 typedef struct {
@@ -197,6 +208,17 @@ qjx_status qjx_get_states(qjx_engine *h, double *psi, double *t, double *eta, in
 qjx_status qjx_jump_count(qjx_engine *h, int tr, int64_t *count);
 qjx_status qjx_get_jumps(qjx_engine *h, int tr, double *times, int *types, double *norms, double *etas);
 qjx_status qjx_get_stats(qjx_engine *h, qjx_stats *stats);
+
+/* The project's tile autotuner (no counterpart in the reference, which has no tiles): times the
+ * candidate tile shapes of cfg->precision (plain: sub-tile columns x slab rows; split: ring depth x
+ * fewest rows per tile) on scratch engines of cfg with the given operators (cfg->n_traj
+ * trajectories from |0>, one untimed period, then n_periods timed periods of device time) and
+ * returns the fastest in *best.  cand / us (capacity *n_cand; NULL to skip) receive every
+ * candidate and its device microseconds per trajectory-period; *n_cand the count.  The winner is
+ * stored under (precision, d) in the tile cache file: $QJX_TILE_CACHE, else
+ * $HOME/.cache/qjx_b200/tiles.txt; engines created later with all-zero cfg->tiles use it. */
+qjx_status qjx_autotune(const qjx_config *cfg, const double *U, const double *L, const double *g, const double *HE,
+                        int n_periods, qjx_tiles *best, qjx_tiles *cand, double *us, int *n_cand);
 /* Later qjx_run_periods calls advance trajectories [0, n_active) only (the others keep their
  * states); the Lyapunov task runs its transient on the bases alone (LpnMultExperimentBehaviour::
  * trans_process, experiment.cpp:147-155).  n_active = n_traj restores the default. */

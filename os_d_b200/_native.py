@@ -20,11 +20,15 @@ EXPORTS = [
     "qjx_create", "qjx_create_rk", "qjx_build_dimer_rk", "qjx_build_dimer_deep", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
-    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_build_dimer", "qjx_expm",
+    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_autotune", "qjx_build_dimer", "qjx_expm",
     "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_build_ps", "qjx_build_floq2spins", "qjx_build_floqnspins", "qjx_build_floqspph", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
     "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_bases", "qjx_run_sub_periods", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
 ]
+
+
+class QjxTiles(C.Structure):
+    _fields_ = [("nc", C.c_int), ("kb", C.c_int), ("stages", C.c_int), ("rows", C.c_int)]
 
 
 class QjxConfig(C.Structure):
@@ -32,7 +36,8 @@ class QjxConfig(C.Structure):
                 ("num_diss", C.c_int), ("num_robs", C.c_int), ("T", C.c_double), ("record", C.c_int),
                 ("rng_kind", C.c_int), ("seed", C.c_uint64), ("rec_cap", C.c_int), ("keep_adr", C.c_int),
                 ("max_dumps", C.c_int), ("device", C.c_int), ("tr_base", C.c_int64), ("deep_num_steps", C.c_int),
-                ("precision", C.c_int), ("branch_len", c_double_p), ("split_recheck", C.c_double)]
+                ("precision", C.c_int), ("branch_len", c_double_p), ("split_recheck", C.c_double),
+                ("tiles", QjxTiles)]
 
 
 class QjxEnsemble(C.Structure):
@@ -111,6 +116,8 @@ def lib():
         L.qjx_lpn_get_last.argtypes = [vp, c_int_p, c_double_p, c_double_p, c_double_p, c_int_p, c_double_p]
         L.qjx_get_trace.argtypes = [vp, c_i64_p, c_int_p, c_int_p]
         L.qjx_measure_fp64_peak.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_autotune.argtypes = ([C.POINTER(QjxConfig)] + [c_double_p] * 4 +
+                                   [C.c_int, C.POINTER(QjxTiles), C.POINTER(QjxTiles), c_double_p, c_int_p])
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
         L.qjx_build_dimer_deep.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int, C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]

@@ -21,6 +21,7 @@ constexpr int kStages = 2;             // slab pipeline depth
 constexpr int kMaxGroups = 256;        // distinct matrices in one engine
 constexpr int kMaxMD = 1024;           // d <= 1024 (plain form; the split form takes d <= 256)
 constexpr double kSplitNormSlack = 1e-4;  // split precision: tolerated norm excess over 1
+constexpr int kMaxSplitStages = 8;        // split precision: deepest operand ring
 // Thread layouts of a sub-tile (rows ty + TY i, columns tx + TX j, TY * TX = 256):
 //   TY = 32: MD = 32 * MT padded rows, TX = 8 column threads, up to 4 columns each
 //   TY = 16: MD = 16 * MT padded rows, TX = 16 column threads, up to 2 columns each
@@ -143,6 +144,7 @@ struct Params {
     int *rcnt;
     int *rlist;
     int rchk_kb;
+    int min_rows;                 // split form: fewest trajectories per tcgen05 tile (tile shape)
     // RK propagator (prop 1): groups 0 and 1 are H_eff and H_drv; psi has kRkSlots slots
     int prop;                     // 0 QJ split tree, 1 RK
     int rk_ns, period0, drv_type;

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
+#include <sys/stat.h>
 
 #include "../../include/qjx_b200.h"
 #include "qjx_device.cuh"
@@ -220,6 +221,65 @@ static T *upload(qjx_engine *h, const std::vector<T> &v)
     return p;
 }
 
+// ---------------------------------------------------------------- tile shapes
+// Whether the plain kernel can run sub-tiles of nc columns and slabs of kb k rows for padded rows
+// MD within `budget` bytes of dynamic shared memory (the constraints pick_step_tiles applies).
+static bool tiles_fit(int MD, size_t budget, int nc, int kb)
+{
+    if (nc != 8 && nc != 16 && nc != 32) return false;
+    if (kb < 2 || kb > kKB || (kb & 1)) return false;
+    const int RB = MD / 8, W1 = 16 / (nc / 8);
+    if ((RB + W1 - 1) / W1 > 8) return false;
+    return step_smem_bytes(MD, nc, kb) <= budget;
+}
+
+// The autotuner's cache: text lines "precision d nc kb stages rows us" (later lines win), in
+// $QJX_TILE_CACHE or $HOME/.cache/qjx_b200/tiles.txt.
+static std::string tile_cache_path()
+{
+    if (const char *p = getenv("QJX_TILE_CACHE")) return p;
+    if (const char *home = getenv("HOME")) return std::string(home) + "/.cache/qjx_b200/tiles.txt";
+    return std::string();
+}
+
+static bool tile_cache_get(int precision, int d, qjx_tiles *t)
+{
+    const std::string fn = tile_cache_path();
+    if (fn.empty()) return false;
+    FILE *f = fopen(fn.c_str(), "r");
+    if (!f) return false;
+    bool found = false;
+    char line[256];
+    while (fgets(line, sizeof line, f)) {
+        int pr = 0, dd = 0;
+        qjx_tiles x{};
+        double us = 0.0;
+        if (sscanf(line, "%d %d %d %d %d %d %lf", &pr, &dd, &x.nc, &x.kb, &x.stages, &x.rows, &us) == 7 &&
+            pr == precision && dd == d) {
+            *t = x;
+            found = true;
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+static void tile_cache_put(int precision, int d, const qjx_tiles &t, double us)
+{
+    const std::string fn = tile_cache_path();
+    if (fn.empty()) return;
+    const size_t slash = fn.rfind('/');
+    if (slash != std::string::npos && slash > 0) {  // create the directory chain
+        const std::string dir = fn.substr(0, slash);
+        for (size_t i = 1; i <= dir.size(); i++)
+            if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
+    }
+    FILE *f = fopen(fn.c_str(), "a");
+    if (!f) return;
+    fprintf(f, "%d %d %d %d %d %d %.6f\n", precision, d, t.nc, t.kb, t.stages, t.rows, us);
+    fclose(f);
+}
+
 // Engine over E ensembles (E = 1: an ordinary engine).  cfg supplies what the ensembles share:
 // deep, num_branches, num_diss, num_robs, record, rng_kind, rec_cap, keep_adr, max_dumps,
 // device, precision, deep_num_steps.
@@ -293,9 +353,20 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
         const size_t fixed = step_static_smem() + 1024;
         if ((size_t)optin <= fixed) return bail(QJX_ERR_UNSUPPORTED);
         size_t smem = 0;
+        const size_t budget = (size_t)optin - fixed;
         for (int e = 0; e < E; e++) {
             const int MDe = 8 * ((ens[e].d + 7) / 8);
-            if (!pick_step_tiles(MDe, (size_t)optin - fixed, &e_nc[e], &e_kb[e])) return bail(QJX_ERR_UNSUPPORTED);
+            qjx_tiles ct{};
+            if (c.tiles.nc > 0 || c.tiles.kb > 0) {  // explicit shapes must fit
+                if (!tiles_fit(MDe, budget, c.tiles.nc, c.tiles.kb)) return bail(QJX_ERR_UNSUPPORTED);
+                e_nc[e] = c.tiles.nc;
+                e_kb[e] = c.tiles.kb;
+            } else if (tile_cache_get(0, ens[e].d, &ct) && tiles_fit(MDe, budget, ct.nc, ct.kb)) {
+                e_nc[e] = ct.nc;  // the autotuner's choice for this dimension
+                e_kb[e] = ct.kb;
+            } else if (!pick_step_tiles(MDe, budget, &e_nc[e], &e_kb[e])) {
+                return bail(QJX_ERR_UNSUPPORTED);
+            }
             smem = std::max(smem, step_smem_bytes(MDe, e_nc[e], e_kb[e]));
         }
         P.step_smem = (int)smem;
@@ -398,10 +469,18 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
         // deepest operand ring (2..8 stages) that fits next to the kernel's static shared memory
         const size_t fixed = split_static_smem() + 1024;
-        P.sstages = 0;
-        for (int st = 8; st >= 2 && !P.sstages; st--)
-            if (split_smem_bytes(P.MDs, MD, st) + fixed <= (size_t)optin) P.sstages = st;
-        if (!P.sstages) return bail(QJX_ERR_UNSUPPORTED);
+        int smax = 0;
+        for (int st = kMaxSplitStages; st >= 2 && !smax; st--)
+            if (split_smem_bytes(P.MDs, MD, st) + fixed <= (size_t)optin) smax = st;
+        if (!smax) return bail(QJX_ERR_UNSUPPORTED);
+        qjx_tiles ct{};
+        const bool cached = !c.tiles.stages && !c.tiles.rows && tile_cache_get(1, d, &ct);
+        const int want_st = c.tiles.stages ? c.tiles.stages : (cached ? ct.stages : smax);
+        const int want_rows = c.tiles.rows ? c.tiles.rows : (cached ? ct.rows : 8);
+        if (want_st < 2 || want_st > smax || want_rows < 8 || want_rows > 128 || (want_rows & 7))
+            return bail(QJX_ERR_UNSUPPORTED);
+        P.sstages = want_st;
+        P.min_rows = want_rows;
         // input-vector planes of every bucket position, two buffers
         P.scap = 8 * (((long long)n + 7) / 8);
         const size_t greg = (size_t)P.KS * 4 * (size_t)P.scap * 32;
@@ -789,7 +868,13 @@ extern "C" qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble 
     CK(cudaStreamSynchronize(h->stream));
     const int MDe = 8 * ((d + 7) / 8), kpe = (d + 1) & ~1;
     int nc = 0, kb = 0;
-    if (!pick_step_tiles(MDe, (size_t)P.step_smem, &nc, &kb)) return fail(h, QJX_ERR_UNSUPPORTED, "no tiling");
+    qjx_tiles ct{};
+    if (tile_cache_get(0, d, &ct) && tiles_fit(MDe, (size_t)P.step_smem, ct.nc, ct.kb)) {
+        nc = ct.nc;  // the autotuner's choice for this dimension
+        kb = ct.kb;
+    } else if (!pick_step_tiles(MDe, (size_t)P.step_smem, &nc, &kb)) {
+        return fail(h, QJX_ERR_UNSUPPORTED, "no tiling");
+    }
     // operators into the slot's resident matrix region
     const int Ge = P.G / h->n_ens;
     const size_t per = (size_t)kpe * MDe * 2, dd2 = (size_t)2 * d * d;
@@ -1436,5 +1521,60 @@ extern "C" qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, dou
     if (cudaGetLastError() != cudaSuccess) return QJX_ERR_CUDA;
     if (ffma_tflops) *ffma_tflops = best;
     if (dmma_tflops) *dmma_tflops = best_mma;
+    return QJX_OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+extern "C" qjx_status qjx_autotune(const qjx_config *cfg, const double *U, const double *L, const double *g,
+                                   const double *HE, int n_periods, qjx_tiles *best, qjx_tiles *cand, double *us,
+                                   int *n_cand)
+{
+    if (!cfg || !U || !L || !g || !HE || !best || n_periods < 1 || ((cand || us) && !n_cand))
+        return QJX_ERR_INVALID_ARG;
+    const int d = cfg->d, n = cfg->n_traj;
+    if (d < 2 || n < 1) return QJX_ERR_INVALID_ARG;
+    std::vector<qjx_tiles> list;
+    if (cfg->precision == 1) {
+        for (int st : {2, 3, 4, 6, 8})
+            for (int rows : {8, 32, 64, 128}) list.push_back(qjx_tiles{0, 0, st, rows});
+    } else {
+        for (int nc : {32, 16, 8})
+            for (int kb : {16, 12, 8, 4}) list.push_back(qjx_tiles{nc, kb, 0, 0});
+    }
+    std::vector<double> psi((size_t)n * d * 2, 0.0);
+    for (int i = 0; i < n; i++) psi[(size_t)i * d * 2] = 1.0;  // |0>
+    const int cap = n_cand ? *n_cand : 0;
+    int filled = 0;
+    double best_us = 0.0;
+    for (const qjx_tiles &t : list) {
+        qjx_config c = *cfg;
+        c.tiles = t;
+        c.num_robs = 0;
+        c.record = 0;
+        c.max_dumps = 1;
+        qjx_engine *h = nullptr;
+        if (create_engine(&c, U, L, g, HE, nullptr, 2, &h) != QJX_OK) continue;  // the shape does not fit
+        double t_us = -1.0;
+        if (qjx_set_states(h, psi.data()) == QJX_OK && qjx_init_thresholds(h) == QJX_OK &&
+            qjx_run_periods(h, 1, 0, nullptr, 0, 0) == QJX_OK) {
+            const double ms0 = h->stats.step_kernel_ms;
+            if (qjx_run_periods(h, n_periods, 0, nullptr, 0, 0) == QJX_OK)
+                t_us = (h->stats.step_kernel_ms - ms0) * 1e3 / ((double)n * n_periods);
+        }
+        qjx_destroy(h);
+        if (t_us <= 0.0) continue;
+        if (filled < cap) {
+            if (cand) cand[filled] = t;
+            if (us) us[filled] = t_us;
+            filled++;
+        }
+        if (best_us == 0.0 || t_us < best_us) {
+            best_us = t_us;
+            *best = t;
+        }
+    }
+    if (n_cand) *n_cand = filled;
+    if (best_us == 0.0) return QJX_ERR_UNSUPPORTED;
+    tile_cache_put(cfg->precision, d, *best, best_us);
     return QJX_OK;
 }

@@ -47,7 +47,7 @@
 
 constexpr int kAPlanes = 4;                  // A and B planes: Re hi, Re lo, Im hi, Im lo
 constexpr int kTileM = 128;                  // MMA M = TMEM lanes (a tile holds up to 128 trajectories)
-constexpr int kMaxSStages = 8;               // operand ring depth (runtime: as deep as shared memory allows)
+constexpr int kMaxSStages = kMaxSplitStages;  // operand ring depth (runtime: the tile shape's, at most this)
 constexpr int kABytes = kTileM * 32;         // one plane of one k-step of A: 128 rows x 16 bf16
 constexpr int kTmemCols = 512;
 constexpr long long kSplitWait = 1ll << 20;  // bounded mbarrier polls (normal waits end within microseconds)
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         if (lane < 16)
             for (int g = 0; g < G; g++) tiles += (cnt_cur[g] + 8 * lane + 7) / (8 * lane + 8);
         const unsigned fit = __ballot_sync(0xffffffffu, lane < 16 && tiles <= avail);
-        const int R = fit ? 8 * (__ffs(fit)) : kTileM;
+        const int R = max(P.min_rows, fit ? 8 * (__ffs(fit)) : kTileM);
         if (lane == 0) {
             s_rows = R;
             int acc = 0;

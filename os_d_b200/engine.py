@@ -16,7 +16,7 @@ class Engine:
 
     def __init__(self, U, L, g, HE, R=None, T=2 * np.pi, n_traj=1, seed=0, record=0, rng_kind=0, rec_cap=1024,
                  keep_adr=0, max_dumps=1, device=0, tr_base=0, precision=0, deep_num_steps=0, branch_len=None,
-                 split_recheck=0.0):
+                 split_recheck=0.0, tiles=None):
         U = np.ascontiguousarray(U, np.complex128)
         nb, deep, d, _ = U.shape
         L = np.ascontiguousarray(L, np.complex128).reshape(-1, d, d)
@@ -30,6 +30,8 @@ class Engine:
         cfg.max_dumps, cfg.device, cfg.tr_base = max_dumps, device, tr_base
         cfg.precision = precision  # 0 complex FP64, 1 split bf16x3 on tcgen05
         cfg.split_recheck = split_recheck  # split form: FP64 recheck band (0: default 1e-5, < 0: off)
+        if tiles:  # explicit tile shapes (dict nc / kb / stages / rows); default: rule or autotuner cache
+            cfg.tiles = N.QjxTiles(**tiles)
         cfg.deep_num_steps = deep_num_steps  # > 0: StdDeep task (U from build_dimer_deep)
         self._branch_len = None if branch_len is None else np.ascontiguousarray(branch_len, np.float64)
         cfg.branch_len = N.dp(self._branch_len)  # per-branch durations (None: T / 2 each)
@@ -403,3 +405,29 @@ class FBasis:
             self.close()
         except Exception:
             pass
+
+
+def autotune(U, L, g, HE, T=2 * np.pi, n_traj=2048, precision=0, n_periods=2, seed=0, device=0):
+    """Times the candidate tile shapes of one dimension and precision (qjx_autotune) and caches the
+    fastest for later engines.  Returns (best, [(tiles, microseconds per trajectory-period)])."""
+    U = np.ascontiguousarray(U, np.complex128)
+    nb, deep, d, _ = U.shape
+    L = np.ascontiguousarray(L, np.complex128).reshape(-1, d, d)
+    g = np.ascontiguousarray(np.atleast_1d(g), np.float64)
+    HE = np.ascontiguousarray(HE, np.complex128)
+    cfg = N.QjxConfig()
+    cfg.d, cfg.n_traj, cfg.deep, cfg.num_branches = d, n_traj, deep, nb
+    cfg.num_diss, cfg.T, cfg.seed, cfg.device, cfg.precision = L.shape[0], T, seed, device, precision
+    cfg.rec_cap, cfg.max_dumps = 16, 1
+    best = N.QjxTiles()
+    cap = 32
+    cand = (N.QjxTiles * cap)()
+    us = np.zeros(cap)
+    nc = C.c_int(cap)
+    N.check(N.lib().qjx_autotune(C.byref(cfg), N.dp(U), N.dp(L), N.dp(g), N.dp(HE), n_periods, C.byref(best), cand,
+                                 N.dp(us), C.byref(nc)), what="qjx_autotune")
+
+    def as_dict(t):
+        return {k: getattr(t, k) for k, _ in N.QjxTiles._fields_}
+
+    return as_dict(best), [(as_dict(cand[i]), float(us[i])) for i in range(nc.value)]

@@ -71,3 +71,26 @@ def test_split_dissipative_ensemble_close_to_fp64(N, n, periods):
     # the ensemble mean of <n1 - n2> agrees within the split-form tolerance of this short run
     m_s, m_d = o_s["mean"][0].mean(), o_d["mean"][0].mean()
     assert abs(m_s - m_d) < 0.02 * N, (m_s, m_d)
+
+
+def test_autotuner_picks_and_caches_a_fitting_shape(tmp_path, monkeypatch):
+    """qjx_autotune times every fitting tile shape of the split and plain forms at d = 41 and
+    stores the fastest under (precision, d); a later engine with default tiles picks it from the
+    cache, and its results equal an engine with the rule's shapes (tiles never change results)."""
+    import os_d_b200 as q
+
+    monkeypatch.setenv("QJX_TILE_CACHE", str(tmp_path / "tiles.txt"))
+    P = dimer_problem(40)
+    for precision in (0, 1):
+        best, table = q.autotune(P["U"], P["L"], [1.0], P["HE"], T=P["T"], n_traj=512, precision=precision,
+                                 n_periods=1)
+        assert len(table) >= 4 and all(us > 0 for _, us in table)
+        assert min(table, key=lambda x: x[1])[0] == best
+    lines = (tmp_path / "tiles.txt").read_text().split("\n")
+    assert lines[0].startswith("0 41 ") and lines[1].startswith("1 41 ")
+    for precision in (0, 1):
+        psi_c, jc_c, _ = run(P, 256, 2, precision)  # default tiles: the cached choice
+        monkeypatch.setenv("QJX_TILE_CACHE", str(tmp_path / "none.txt"))
+        psi_r, jc_r, _ = run(P, 256, 2, precision)  # the rule
+        monkeypatch.setenv("QJX_TILE_CACHE", str(tmp_path / "tiles.txt"))
+        assert np.array_equal(psi_c, psi_r) and np.array_equal(jc_c, jc_r)
