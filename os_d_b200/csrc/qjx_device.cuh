@@ -135,8 +135,15 @@ struct Params {
     // K-major core-matrix order (8-position groups of 256 bytes, the two K-halves 128 bytes apart)
     unsigned char *stage;
     size_t stage_bytes;           // one buffer
-    long long scap;               // positions per (group, k-step, plane), a multiple of 8
     const long long *g_soff;      // [G]
+    // per ensemble: rows padded to 16 (MMA N), k-steps, stage positions per (group, k-step,
+    // plane) (its trajectories rounded up to 8); per group: byte offset of its B planes in usplit
+    const int *e_mds, *e_ks, *e_scap;
+    const long long *g_uoff;
+    // tile plan of the next micro-step: [0] rows per tile, [1 + g] first tile of group g,
+    // [1 + G] tiles in all; written by the last CTA of a micro-step (or split_plan_kernel)
+    int *splan;
+    int grid;                     // CTAs of the micro-step kernels
     // near-threshold FP64 rechecks of the split form: band (relative to the norm; 0: off), the
     // recheck lists of the micro-steps ([3] counts, [2][n] trajectories) and the k rows of the
     // FP64 matrix slabs streamed through the operand ring

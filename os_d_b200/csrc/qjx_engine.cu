@@ -306,7 +306,7 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     if (c.precision != 0 && c.precision != 1) return QJX_ERR_INVALID_ARG;
     // the split kernel's N = MDs <= 256 and its shared-memory bucket tables hold one ensemble of
     // at most kMaxGroups matrices
-    if (c.precision == 1 && (dmax > 256 || E > 1 || Ge > kMaxGroups)) return QJX_ERR_UNSUPPORTED;
+    if (c.precision == 1 && dmax > 256) return QJX_ERR_UNSUPPORTED;
     const int G = (int)Gl;
     const int n = (int)ntot;
 
@@ -458,12 +458,18 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     cudaMemset(P.plan, 0, (size_t)(2 * G + 2) * sizeof(int));
     cudaMemset(P.plan_sync, 0, sizeof(unsigned int));
 
+    P.grid = h->grid;
     if (c.precision == 1) {  // split precision: bf16 planes of every matrix in the tcgen05 order
-        const EnsDesc &x = ens[0];
-        const double *U = x.U, *L = x.L, *HE = x.HE, *R = x.R;
-        const size_t dd2 = (size_t)d * d * 2;
         P.split = 1;
-        P.MDs = 16 * ((d + 15) / 16);
+        std::vector<int> e_mds(E), e_ks(E), e_scap(E);
+        int mds_max = 16;
+        for (int e = 0; e < E; e++) {
+            e_mds[e] = 16 * ((ens[e].d + 15) / 16);
+            e_ks[e] = (ens[e].d + 15) / 16;
+            e_scap[e] = 8 * ((ens[e].n + 7) / 8);
+            mds_max = std::max(mds_max, e_mds[e]);
+        }
+        P.MDs = mds_max;
         P.KS = (d + 15) / 16;
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device);
@@ -481,35 +487,51 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
             return bail(QJX_ERR_UNSUPPORTED);
         P.sstages = want_st;
         P.min_rows = want_rows;
-        // input-vector planes of every bucket position, two buffers
-        P.scap = 8 * (((long long)n + 7) / 8);
-        const size_t greg = (size_t)P.KS * 4 * (size_t)P.scap * 32;
-        std::vector<long long> soff(G);
-        for (int gg = 0; gg < G; gg++) soff[gg] = (long long)(gg * greg);
+        // per group: its bf16 matrix planes (usplit) and the input-vector planes of every bucket
+        // position (two stage buffers), in its ensemble's own padded layout
+        std::vector<long long> soff(G), uoff(G);
+        size_t sbytes = 0, ubytes = 0;
+        for (int gg = 0; gg < G; gg++) {
+            const int e = g_ens[gg];
+            soff[gg] = (long long)sbytes;
+            uoff[gg] = (long long)ubytes;
+            sbytes += (size_t)e_ks[e] * 4 * (size_t)e_scap[e] * 32;
+            ubytes += (size_t)e_ks[e] * 4 * (size_t)e_mds[e] * 32;
+        }
+        P.e_mds = upload(h, e_mds);
+        P.e_ks = upload(h, e_ks);
+        P.e_scap = upload(h, e_scap);
         P.g_soff = upload(h, soff);
-        P.stage_bytes = (size_t)G * greg;
+        P.g_uoff = upload(h, uoff);
+        P.stage_bytes = sbytes;
         P.stage = (unsigned char *)dalloc(h, 2 * P.stage_bytes);
+        P.splan = (int *)dalloc(h, (size_t)(G + 2) * sizeof(int));
         // near-threshold FP64 rechecks: lists, band, and the matrix slab height that fits the ring
         // next to the input and product vectors
         P.rcnt = (int *)dalloc(h, 3 * sizeof(int));
         P.rlist = (int *)dalloc(h, (size_t)2 * n * sizeof(int));
-        if (!P.g_soff || !P.stage || !P.rcnt || !P.rlist) return bail(QJX_ERR_OOM);
+        if (!P.e_mds || !P.e_ks || !P.e_scap || !P.g_soff || !P.g_uoff || !P.stage || !P.splan || !P.rcnt || !P.rlist)
+            return bail(QJX_ERR_OOM);
         P.recheck_tol = c.split_recheck == 0.0 ? 1e-5 : (c.split_recheck < 0.0 ? 0.0 : c.split_recheck);
         const size_t ring = (size_t)P.sstages * split_stage_bytes(P.MDs);
         const size_t vec = (size_t)(2 * MD + 2) * sizeof(double2);
         P.rchk_kb = std::min<int>(32, (int)((ring - vec) / (2 * (size_t)MD * sizeof(double2)))) & ~1;
         if (P.rchk_kb < 2) return bail(QJX_ERR_UNSUPPORTED);
-        const size_t per_s = (size_t)P.KS * 4 * P.MDs * 16;
-        std::vector<uint16_t> hs((size_t)G * per_s, 0);
-        for (int b = 0; b < c.num_branches; b++)
-            for (int l = 0; l < c.deep; l++)
-                pack_split(U + dd2 * ((size_t)b * c.deep + l), d, P.MDs, P.KS, hs.data() + per_s * (b * c.deep + l));
-        for (int i = 0; i < c.num_diss; i++) pack_split(L + dd2 * i, d, P.MDs, P.KS, hs.data() + per_s * (P.gL0 + i));
-        pack_split(HE, d, P.MDs, P.KS, hs.data() + per_s * P.gHE);
-        for (int i = 0; i < c.num_robs; i++) pack_split(R + dd2 * i, d, P.MDs, P.KS, hs.data() + per_s * (P.gR0 + i));
-        unsigned char *us = (unsigned char *)dalloc(h, hs.size() * sizeof(uint16_t));
+        std::vector<uint16_t> hs(ubytes / 2, 0);
+        for (int e = 0; e < E; e++) {
+            const EnsDesc &x = ens[e];
+            const size_t dd2 = (size_t)x.d * x.d * 2;
+            auto dst = [&](int l) { return hs.data() + uoff[e * Ge + l] / 2; };
+            for (int b = 0; b < c.num_branches; b++)
+                for (int l = 0; l < c.deep; l++)
+                    pack_split(x.U + dd2 * ((size_t)b * c.deep + l), x.d, e_mds[e], e_ks[e], dst(b * c.deep + l));
+            for (int i = 0; i < c.num_diss; i++) pack_split(x.L + dd2 * i, x.d, e_mds[e], e_ks[e], dst(P.gL0 + i));
+            pack_split(x.HE, x.d, e_mds[e], e_ks[e], dst(P.gHE));
+            for (int i = 0; i < c.num_robs; i++) pack_split(x.R + dd2 * i, x.d, e_mds[e], e_ks[e], dst(P.gR0 + i));
+        }
+        unsigned char *us = (unsigned char *)dalloc(h, std::max<size_t>(ubytes, 16));
         if (!us) return bail(QJX_ERR_OOM);
-        cudaMemcpy(us, hs.data(), hs.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(us, hs.data(), ubytes, cudaMemcpyHostToDevice);
         P.usplit = us;
     }
     P.brep = c.deep_num_steps > 0 ? 2 * c.deep_num_steps : 1;
@@ -814,7 +836,6 @@ extern "C" qjx_status qjx_create(const qjx_config *cfg, const double *U, const d
 extern "C" qjx_status qjx_create_batch(const qjx_config *cfg, int n_ens, const qjx_ensemble *ens, qjx_engine **out)
 {
     if (!cfg || !out || n_ens < 1 || !ens) return QJX_ERR_INVALID_ARG;
-    if (cfg->precision != 0) return QJX_ERR_UNSUPPORTED;
     std::vector<EnsDesc> v(n_ens);
     for (int e = 0; e < n_ens; e++) {
         const qjx_ensemble &x = ens[e];

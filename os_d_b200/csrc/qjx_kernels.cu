@@ -1412,7 +1412,8 @@ cudaError_t launch_stage_lists(const Params &P, cudaStream_t st)
 {
     const int warps = 8;
     const int bx = std::max(1, std::min(64, (P.n + warps - 1) / warps));
-    stage_lists_kernel<<<dim3(bx, P.G), warps * 32, 0, st>>>(P);
+    stage_lists_kernel<<<dim3(bx, std::min(P.G, 65535)), warps * 32, 0, st>>>(P);
+    split_plan_kernel<<<1, 512, 0, st>>>(P, P.grid);
     return cudaGetLastError();
 }
 

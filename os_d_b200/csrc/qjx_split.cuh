@@ -126,8 +126,9 @@ __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo
 // position pos of group g.
 __device__ __forceinline__ size_t stage_chunk(const Params &P, int g, int ks, int p, int kh, int pos)
 {
-    return (size_t)P.g_soff[g] + ((size_t)(ks * kAPlanes + p) * (size_t)P.scap + (size_t)(pos & ~7)) * 32 +
-           (size_t)kh * 128 + (size_t)(pos & 7) * 16;
+    const size_t cap = (size_t)P.e_scap[P.g_ens[g]];
+    return (size_t)P.g_soff[g] + ((size_t)(ks * kAPlanes + p) * cap + (size_t)(pos & ~7)) * 32 + (size_t)kh * 128 +
+           (size_t)(pos & 7) * 16;
 }
 
 // Writes the bf16 planes of a trajectory's next input vector at position pos of group g of the
@@ -138,7 +139,8 @@ __device__ void stage_write(const Params &P, unsigned char *dst, int g, int pos,
                             double div, const double2 *gsrc, const unsigned char *src_stage, int g0, int pos0, int d,
                             int lane)
 {
-    for (int pr = lane; pr < 2 * P.KS; pr += 32) {
+    const int KS = P.e_ks[P.g_ens[g]];
+    for (int pr = lane; pr < 2 * KS; pr += 32) {
         const int ks = pr >> 1, kh = pr & 1;
         uint4 c[kAPlanes];
         if (mode == SRC_SAME) {
@@ -177,18 +179,21 @@ __device__ void stage_write(const Params &P, unsigned char *dst, int g, int pos,
     }
 }
 
-// Planes of step 0 after a host-side enqueue (schedule, observe, resume): block (x, g) takes
-// positions of bucket g, one warp per position, from the trajectories' FP64 input slots.
+// Planes of step 0 after a host-side enqueue (schedule, observe, resume): block (x, y) takes
+// positions of buckets y, y + gridDim.y, ..., one warp per position, from the trajectories' FP64
+// input slots.
 __global__ void stage_lists_kernel(const Params P)
 {
-    const int g = blockIdx.y, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int cnt = P.cnt[g];
-    for (int pos = blockIdx.x * nw + (threadIdx.x >> 5); pos < cnt; pos += gridDim.x * nw) {
-        const int tr = P.lists[P.g_loff[g] + pos];
-        const TrajState s = P.st[tr];
-        const int slot = src_slot(s.phase, s.cur, s.rk_stage);
-        stage_write(P, P.stage, g, pos, SRC_GLOBAL, nullptr, 1.0, slot_ptr(P, slot, tr), nullptr, 0, 0, dim_of(P, s),
-                    lane);
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int g = blockIdx.y; g < P.G; g += gridDim.y) {
+        const int cnt = P.cnt[g];
+        for (int pos = blockIdx.x * nw + (threadIdx.x >> 5); pos < cnt; pos += gridDim.x * nw) {
+            const int tr = P.lists[P.g_loff[g] + pos];
+            const TrajState s = P.st[tr];
+            const int slot = src_slot(s.phase, s.cur, s.rk_stage);
+            stage_write(P, P.stage, g, pos, SRC_GLOBAL, nullptr, 1.0, slot_ptr(P, slot, tr), nullptr, 0, 0,
+                        dim_of(P, s), lane);
+        }
     }
 }
 
@@ -271,39 +276,142 @@ __device__ bool recheck_column(const Params &P, int tr, unsigned char *smem, Tra
     return true;
 }
 
+// Tile plan of a micro-step from its bucket sizes cnt[G] and its rtot FP64 rechecks (block-wide,
+// blockDim.x a multiple of 32): rows per tile R, the smallest multiple of 8 (at least P.min_rows,
+// at most 128) whose tiles fit one wave of `grid` CTAs next to the rechecks, so that trajectories
+// and their epilogues spread over all SMs; then the first tile of every group.
+__device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
+{
+    __shared__ int w_t[32][17];
+    __shared__ int w_s[32];
+    __shared__ int s_R;
+    const int G = P.G, nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    int part[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) part[j] = 0;
+    for (int g = tid; g < G; g += nt) {
+        const int m = __ldcg(cnt + g);
+#pragma unroll
+        for (int j = 0; j < 16; j++) part[j] += (m + 8 * j + 7) / (8 * j + 8);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        int v = part[j];
+        for (int off = 16; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) w_t[warp][j] = v;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int avail = max(1, grid - rtot);
+        int R = kTileM;
+        for (int j = 0; j < 16; j++) {
+            int tiles = 0;
+            for (int w = 0; w < nw; w++) tiles += w_t[w][j];
+            if (tiles <= avail) {
+                R = 8 * (j + 1);
+                break;
+            }
+        }
+        s_R = max(P.min_rows, R);
+    }
+    __syncthreads();
+    const int R = s_R;
+    // exclusive scan of the tiles per group over the block: each thread a contiguous range
+    const int per = (G + nt - 1) / nt, g0 = min(G, tid * per), g1 = min(G, g0 + per);
+    int c = 0;
+    for (int g = g0; g < g1; g++) c += (__ldcg(cnt + g) + R - 1) / R;
+    int inc = c;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += y;
+    }
+    if (lane == 31) w_s[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < nw ? w_s[lane] : 0;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, off);
+            if (lane >= off) v += y;
+        }
+        if (lane < nw) w_s[lane] = v;
+    }
+    __syncthreads();
+    int acc = inc - c + (warp ? w_s[warp - 1] : 0);
+    for (int g = g0; g < g1; g++) {
+        P.splan[1 + g] = acc;
+        acc += (__ldcg(cnt + g) + R - 1) / R;
+    }
+    if (tid == nt - 1) {
+        P.splan[1 + G] = acc;
+        P.splan[0] = R;
+    }
+    __syncthreads();
+}
+
+// Plan of step 0 after a host-side enqueue (one block).
+__global__ void __launch_bounds__(512) split_plan_kernel(const Params P, int grid)
+{
+    split_plan(P, P.cnt, __ldcg(P.rcnt), grid);
+}
+
+// Group of tile t: the last g with splan[1 + g] <= t (warp-cooperative search over the global plan).
+__device__ __forceinline__ int split_tile_group(const Params &P, int t, int lane)
+{
+    int lo = 0, hi = P.G;  // answer in [lo, hi)
+    while (hi - lo > 1) {
+        const int step = (hi - lo + 31) / 32;
+        const int g = lo + lane * step;
+        const bool le = g < hi && __ldcg(P.splan + 1 + g) <= t;
+        const unsigned m = __ballot_sync(0xffffffffu, le);
+        const int last = 31 - __clz(m);  // lane 0 always qualifies (splan[1 + lo] <= t)
+        lo = lo + last * step;
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
+
 // Dynamic shared memory: a ring of `stages` operand stages, each [A planes][B planes] of one
 // k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs + 1)).
 size_t split_stage_bytes(int MDs) { return (size_t)kAPlanes * (kABytes + (size_t)MDs * 32); }
+
+// Epilogue shared memory (in the idle ring): the FP32 accumulators of `rows` trajectories, one row
+// of 2 MDs + 1 floats each (Re then Im), then one FP64 column of MDs + 1 per warp.
+__host__ __device__ inline size_t split_epi_f32_bytes(int MDs, int rows)
+{
+    return ((size_t)rows * (2 * MDs + 1) * 4 + 15) & ~(size_t)15;
+}
+__host__ __device__ inline size_t split_epi_bytes(int MDs, int rows)
+{
+    return split_epi_f32_bytes(MDs, rows) + (size_t)(kThreads / 32) * (MDs + 1) * sizeof(double2);
+}
 
 size_t split_smem_bytes(int MDs, int MD, int stages)
 {
     const size_t ring = (size_t)stages * split_stage_bytes(MDs);
     (void)MD;
-    const size_t epi = (size_t)32 * (MDs + 1) * sizeof(double2);
+    const size_t epi = split_epi_bytes(MDs, 32);
     return ring > epi ? ring : epi;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P, int s)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int MDs = P.MDs, KS = P.KS, S = P.sstages;
-    const int bbytes = MDs * 32;                               // one plane of one k-step of B
-    const size_t stage_bytes = (size_t)kAPlanes * (kABytes + bbytes);
-    const int S16 = MDs + 1;
-    double2 *Bt = reinterpret_cast<double2 *>(smem);          // epilogue: [32][S16] FP64 columns
+    const int S = P.sstages;
+    const size_t stage_bytes = (size_t)kAPlanes * (kABytes + (size_t)P.MDs * 32);  // ring stride (largest MDs)
     __shared__ __align__(8) uint64_t full[kMaxSStages], empty[kMaxSStages], accf, rbar[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_tstart[kMaxGroups + 1];
     __shared__ int s_tr[kTileM];
     __shared__ __align__(16) TrajState s_st[kTileM];
-    __shared__ int s_fail;
-    __shared__ int s_rows;  // trajectories per tile in this micro-step
-    __shared__ int cnt_cur[kMaxGroups];  // bucket sizes of this step, read once in parallel
-    __shared__ int s_g2[32], s_pos[32];
-    __shared__ EpiOut s_eo[32];
+    __shared__ int s_fail, s_last;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // epilogue rows staged per pass: 64 when their FP32 accumulators and the warps' FP64 columns
+    // fit the dynamic shared memory, else 32
+    const size_t dyn = max((size_t)S * stage_bytes, split_epi_bytes(P.MDs, 32));
+    const int RP = split_epi_bytes(P.MDs, 64) <= dyn ? 64 : 32;
+    double2 *wcol = reinterpret_cast<double2 *>(smem + split_epi_f32_bytes(P.MDs, RP)) + (size_t)warp * (P.MDs + 1);
     const int G = P.G;
+    const int *cnt_cur = P.cnt + (s % 3) * G;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
     const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
     int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
@@ -313,31 +421,14 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
     int *rcnt_next = P.rcnt + (s + 1) % 3;
     const int Rtot = P.rcnt[s % 3];  // FP64 rechecks of this micro-step
+    const int R = P.splan[0], T = P.splan[1 + G];  // this step's plan (rows per tile, tiles)
 
-    for (int i = tid; i < G; i += kThreads) cnt_cur[i] = P.cnt[(s % 3) * G + i];
     if (blockIdx.x == 0) {
         for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
         if (tid == 0) P.rcnt[(s + 2) % 3] = 0;
     }
-    __syncthreads();
     if (warp == 0) {
-        // rows per tile: the smallest multiple of 8 (<= 128) whose tiles fit one wave of CTAs next
-        // to the FP64 rechecks, so the trajectories (and their epilogues) spread over all SMs; 128
-        // when none does
-        const int avail = max(1, (int)gridDim.x - Rtot);
-        int tiles = 0;
-        if (lane < 16)
-            for (int g = 0; g < G; g++) tiles += (cnt_cur[g] + 8 * lane + 7) / (8 * lane + 8);
-        const unsigned fit = __ballot_sync(0xffffffffu, lane < 16 && tiles <= avail);
-        const int R = max(P.min_rows, fit ? 8 * (__ffs(fit)) : kTileM);
         if (lane == 0) {
-            s_rows = R;
-            int acc = 0;
-            for (int g = 0; g < G; g++) {
-                s_tstart[g] = acc;
-                acc += (cnt_cur[g] + R - 1) / R;
-            }
-            s_tstart[G] = acc;
             for (int q = 0; q < S; q++) {
                 mbar_init(&full[q], 1);
                 mbar_init(&empty[q], 1);
@@ -359,11 +450,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const int T = s_tstart[G];
-    const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
-    const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
     long long work = 0, nrechk = 0;
-    uint32_t ntile = 0, rphase = 0;
+    uint32_t ntile = 0, kit = 0, rphase = 0;  // tiles done, k-steps issued (ring position)
     bool ok = true;
     long long tr_setup = 0, tr_mma = 0, tr_stage = 0, tr_epi = 0;
     const long long t_begin = clock64();
@@ -379,22 +467,20 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             continue;
         }
         const long long t0 = clock64();
-        int lo = 0, hi = G;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_tstart[mid] <= t) lo = mid;
-            else hi = mid;
-        }
-        const int g = lo;
-        const int base = (t - s_tstart[g]) * s_rows;
-        const int rows = min(s_rows, cnt_cur[g] - base);
+        const int g = split_tile_group(P, t, lane);  // every warp finds it (warp-uniform)
+        const int e = P.g_ens[g];
+        const int MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
+        const int base = (t - __ldcg(P.splan + 1 + g)) * R;
+        const int rows = min(R, __ldcg(cnt_cur + g) - base);
         const int rows8 = (rows + 7) & ~7;
-        const uint32_t it0 = ntile * (uint32_t)KS;  // k-steps issued before this tile
+        const uint32_t it0 = kit;  // k-steps issued before this tile
+        const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
+        const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
         const long long t1 = clock64();
 
         if (warp == 4) {
             if (lane == 0) {  // producer: per k-step the four A planes of the tile's rows and the B planes
-                const unsigned char *ug = P.usplit + (size_t)g * KS * kAPlanes * bbytes;
+                const unsigned char *ug = P.usplit + P.g_uoff[g];
                 const uint32_t abytes = (uint32_t)rows8 * 32;
                 for (int ks = 0; ks < KS && ok; ks++) {
                     const uint32_t it = it0 + ks, q = it % S;
@@ -454,6 +540,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                 load_state(&s_st[tid], &P.st[tr]);
             }
         }
+        kit += (uint32_t)KS;
         if (!ok) atomicExch(&s_fail, 1);
         // accumulator complete (every thread waits on the commit); the ring is free afterwards
         if (!mbar_wait_bounded(&accf, ntile & 1u, kSplitWait)) atomicExch(&s_fail, 1);
@@ -464,57 +551,52 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             break;
         }
         const long long t2 = clock64();
-        for (int c = 0; c < 4 && 32 * c < rows; c++) {
+        float *sacc = reinterpret_cast<float *>(smem);  // [RP][2 MDs + 1] FP32 accumulators
+        const int SR = 2 * MDs + 1;
+        for (int p0 = 0; p0 < rows; p0 += RP) {  // passes of RP trajectories
             const long long ts = clock64();
-            if ((warp & 3) == c) {  // TMEM lanes 32c..32c+31 belong to warps c, c+4, c+8, c+12
-                const uint32_t lanes = tmem + ((uint32_t)(32 * c) << 16);
+            const int q = warp & 3;  // TMEM lanes 32q..32q+31 belong to warps q, q+4, q+8, q+12
+            if (32 * q >= p0 && 32 * q < p0 + RP && 32 * q < rows) {
+                const uint32_t lanes = tmem + ((uint32_t)(32 * q) << 16);
+                float *dst = sacc + (size_t)(32 * q - p0 + lane) * SR;
                 for (int r0 = 8 * (warp >> 2); r0 < MDs; r0 += 32) {  // 8 output rows at a time
                     float vr[8], vi[8];
                     tmem_ld8(lanes + (uint32_t)r0, vr);
                     tmem_ld8(lanes + (uint32_t)(MDs + r0), vi);
-                    double2 *dst = Bt + (size_t)lane * S16 + r0;
 #pragma unroll
-                    for (int i = 0; i < 8; i++) dst[i] = make_double2((double)vr[i], (double)vi[i]);
+                    for (int i = 0; i < 8; i++) {
+                        dst[r0 + i] = vr[i];
+                        dst[MDs + r0 + i] = vi[i];
+                    }
                 }
             }
             tc_fence_before();
             __syncthreads();
             tr_stage += clock64() - ts;
-            for (int cc = warp; cc < 32; cc += kThreads / 32) {
-                const int m = 32 * c + cc;
-                int g2 = -1;
+            // every warp runs its trajectories through the epilogue, takes their positions in the
+            // next buckets (one atomic each) and writes their next input vectors' planes
+            const int pn = min(RP, rows - p0);
+            for (int cc = warp; cc < pn; cc += kThreads / 32) {
+                const int m = p0 + cc;
+                const float *row = sacc + (size_t)cc * SR;
+                for (int k = lane; k < MDs; k += 32) wcol[k] = make_double2((double)row[k], (double)row[MDs + k]);
+                __syncwarp();
                 EpiOut eo{SRC_NONE, 0, 1.0};
-                if (m < rows) g2 = column_epilogue(P, Bt + (size_t)cc * S16, s_tr[m], s_st[m], lane, &eo);
-                if (lane == 0) {
-                    s_g2[cc] = g2;
-                    s_eo[cc] = eo;
+                const int tr = s_tr[m];
+                const int g2 = column_epilogue(P, wcol, tr, s_st[m], lane, &eo);
+                if (g2 >= 0 || g2 == kRecheck) {
+                    int pos = 0;
+                    if (lane == 0) pos = atomicAdd(g2 >= 0 ? &cnt_next[g2] : rcnt_next, 1);
+                    pos = __shfl_sync(0xffffffffu, pos, 0);
+                    if (g2 >= 0) {
+                        if (lane == 0) list_next[P.g_loff[g2] + pos] = tr;
+                        stage_write(P, stage_next, g2, pos, eo.mode, wcol, eo.div, slot_ptr(P, eo.slot, tr), stage_cur,
+                                    g, base + m, P.e_d[s_st[m].ens], lane);
+                    } else if (lane == 0) {
+                        rlist_next[pos] = tr;
+                    }
                 }
-            }
-            __syncthreads();
-            if (warp == 0) {  // positions in the next buckets: one atomic per distinct bucket of the 32 columns
-                const int g2 = s_g2[lane];
-                const unsigned mm = __match_any_sync(0xffffffffu, g2);
-                const int leader = __ffs(mm) - 1;
-                int b0 = 0;
-                if (g2 != -1 && lane == leader) b0 = atomicAdd(g2 >= 0 ? &cnt_next[g2] : rcnt_next, __popc(mm));
-                b0 = __shfl_sync(0xffffffffu, b0, leader);
-                const int pos = b0 + __popc(mm & ((1u << lane) - 1u));
-                if (g2 >= 0) {
-                    s_pos[lane] = pos;
-                    list_next[P.g_loff[g2] + pos] = s_tr[32 * c + lane];
-                } else if (g2 == kRecheck) {
-                    rlist_next[pos] = s_tr[32 * c + lane];
-                }
-            }
-            __syncthreads();
-            for (int cc = warp; cc < 32; cc += kThreads / 32) {  // the next input vectors' planes
-                const int m = 32 * c + cc, g2 = s_g2[cc];
-                if (m < rows && g2 >= 0) {
-                    const EpiOut eo = s_eo[cc];
-                    const int tr = s_tr[m];
-                    stage_write(P, stage_next, g2, s_pos[cc], eo.mode, Bt + (size_t)cc * S16, eo.div,
-                                slot_ptr(P, eo.slot, tr), stage_cur, g, base + m, P.e_d[s_st[m].ens], lane);
-                }
+                __syncwarp();
             }
             fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
             __syncthreads();
@@ -567,5 +649,17 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         tr[5] += ntile;
         tr[6] += tr_stage;
         tr[7] += work;
+    }
+    // the last CTA to finish plans the next micro-step from the buckets all CTAs filled
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(P.plan_sync, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        split_plan(P, cnt_next, __ldcg(rcnt_next), gridDim.x);
+        if (tid == 0) *P.plan_sync = 0u;
     }
 }

@@ -74,7 +74,7 @@ class Engine:
 
     @classmethod
     def batch(cls, ensembles, deep=16, num_branches=2, record=0, rng_kind=0, rec_cap=1024, keep_adr=0, max_dumps=1,
-              device=0, deep_num_steps=0):
+              device=0, deep_num_steps=0, precision=0, split_recheck=0.0):
         """Batched engine over ensembles of uneven dimension: each item is a dict with U
         ([nb][deep][d][d]), L, g, HE, optional R, n_traj, T, seed, tr_base.  Trajectories are numbered
         ensemble after ensemble (`ranges` gives each ensemble's slice); state rows have the largest d."""
@@ -97,7 +97,8 @@ class Engine:
         cfg = N.QjxConfig()
         cfg.deep, cfg.num_branches, cfg.num_diss, cfg.num_robs = deep, num_branches, keep[1].shape[0], nr
         cfg.record, cfg.rng_kind, cfg.rec_cap, cfg.keep_adr = record, rng_kind, rec_cap, keep_adr
-        cfg.max_dumps, cfg.device, cfg.deep_num_steps, cfg.precision = max_dumps, device, deep_num_steps, 0
+        cfg.max_dumps, cfg.device, cfg.deep_num_steps, cfg.precision = max_dumps, device, deep_num_steps, precision
+        cfg.split_recheck = split_recheck
         h = C.c_void_p()
         N.check(N.lib().qjx_create_batch(C.byref(cfg), len(ensembles), arr, C.byref(h)), what="qjx_create_batch")
         self.h = h
