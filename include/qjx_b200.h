@@ -168,6 +168,10 @@ qjx_status qjx_create_slots(const qjx_config *cfg, int n_slots, int d_cap, int n
 qjx_status qjx_slot_load(qjx_engine *h, int slot, const qjx_ensemble *e, const double *psi);
 /* Stop advancing and observing a slot; its states stay readable until it is loaded again. */
 qjx_status qjx_slot_release(qjx_engine *h, int slot);
+/* Free and total device memory of `device` in bytes (cudaMemGetInfo), for admission by footprint. */
+qjx_status qjx_mem_info(int device, size_t *free_bytes, size_t *total_bytes);
+/* Device bytes an engine holds (all its allocations). */
+qjx_status qjx_engine_bytes(qjx_engine *h, size_t *bytes);
 void qjx_destroy(qjx_engine *h);
 const char *qjx_last_error(const qjx_engine *h);
 const char *qjx_status_string(qjx_status s);
@@ -303,6 +307,14 @@ qjx_status qjx_measure_fp64_peak(int device, double *ffma_tflops, double *dmma_t
  * T = 2 pi / omega.  Any output may be NULL. */
 qjx_status qjx_build_dimer(int N, double J, double U, double E, double A, double g, double omega, int deep,
                            double *H, double *Hd, double *L, double *K, double *Utree);
+/* A split tree built on the GPU (for serving; no counterpart in the reference, which exponentiates
+ * every level on the host, QJX/qj_proc.cpp:55,98): for nb generators K_b (complex [d][d] row-major,
+ * e.g. qjx_build_dimer's K), Utree [nb][deep][d][d] = exp(K_b head_b 2^-(l+2)).  The finest level is a
+ * degree-14 Taylor series of K dt / 2^s with 1-norm at most 1/4, squared s times; every coarser level
+ * is the square of the next finer (the tree's dt halves per level).  FP64 complex GEMMs on `device`
+ * on a private stream (stream-ordered allocations, no device-wide synchronisation); agrees with the
+ * host build to about 1e-12. */
+qjx_status qjx_expm_tree(int d, int nb, const double *K, const double *head, int deep, int device, double *Utree);
 /* The JCS system (sys_id 1; newdel.cpp:96-130, 564-649, 1546-1580, 2499-2601; split structure
  * core.cpp:10086-10157): d = N, H = 0.5/alpha^3 a^+a^+aa, H_drv = a^+ - a, L = a, the number
  * operator Nop = a^+ a and the observable `special` A_op = a; K_0 = -i H_eff + E0 H_drv (the kick),

@@ -23,7 +23,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler",
 CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-fPIC", "-std=c++17",
             "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include"]
 
-CU_SOURCES = ["qjx_kernels.cu", "qjx_engine.cu", "fb_kernels.cu", "qjx_lpn.cu"]
+CU_SOURCES = ["qjx_kernels.cu", "qjx_engine.cu", "fb_kernels.cu", "qjx_lpn.cu", "qjx_tree.cu"]
 CXX_SOURCES = ["qjx_model.cpp", "qjx_config.cpp", "fb_model.cpp"]
 EXE_SOURCES = ["qjx_main.cpp"]
 HEADERS = ["qjx_device.cuh", "qjx_split.cuh", "qjx_config.h"]

@@ -57,6 +57,7 @@ struct qjx_engine {
     std::string err;
     // device allocations
     std::vector<void *> allocs;
+    size_t dev_bytes = 0;  // bytes of allocs
     double *d_inj_u = nullptr;
     long long *d_inj_off = nullptr;
     int *d_dump_at = nullptr;
@@ -92,6 +93,7 @@ static void *dalloc(qjx_engine *h, size_t bytes)
     if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
     cudaMemset(p, 0, bytes ? bytes : 16);
     h->allocs.push_back(p);
+    h->dev_bytes += bytes ? bytes : 16;
     return p;
 }
 
@@ -1597,5 +1599,19 @@ extern "C" qjx_status qjx_autotune(const qjx_config *cfg, const double *U, const
     if (n_cand) *n_cand = filled;
     if (best_us == 0.0) return QJX_ERR_UNSUPPORTED;
     tile_cache_put(cfg->precision, d, *best, best_us);
+    return QJX_OK;
+}
+
+extern "C" qjx_status qjx_mem_info(int device, size_t *free_bytes, size_t *total_bytes)
+{
+    if (!free_bytes || !total_bytes) return QJX_ERR_INVALID_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return QJX_ERR_CUDA;
+    return cudaMemGetInfo(free_bytes, total_bytes) == cudaSuccess ? QJX_OK : QJX_ERR_CUDA;
+}
+
+extern "C" qjx_status qjx_engine_bytes(qjx_engine *h, size_t *bytes)
+{
+    if (!h || !bytes) return QJX_ERR_INVALID_ARG;
+    *bytes = h->dev_bytes;
     return QJX_OK;
 }
