@@ -310,6 +310,26 @@ def batched_bench(args, local):
     kern_s = (m1["step_kernel_ms"] - m0["step_kernel_ms"]) * 1e-3
     peak_ffma, peak_dmma = q.measure_fp64_peak(local)
     peak = max(peak_ffma, peak_dmma)
+    # the split form batched: the ensembles of d <= 256 (the tcgen05 N limit), both precisions
+    small = [x for x in ens if x["U"].shape[-1] <= 256]
+    sub = {}
+    for prec in (0, 1):
+        E = prepare(q.Engine.batch(small, deep=DEEP, device=local, precision=prec), BATCH_TRAJ * len(small),
+                    max(x["U"].shape[-1] for x in small))
+        for _ in range(args.warmup):
+            E.run_periods(1, is_obs=1)
+        ms_p = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            E.run_periods(1, is_obs=1)
+            ms_p += E.stats()["last_call_ms"]
+        sub[prec] = (BATCH_TRAJ * len(small) * args.steps / (ms_p * 1e-3), E.stats().get("rechecks", 0))
+        E.close()
+    split_batch = {"ensembles": len(small), "dims": [min(x["U"].shape[-1] for x in small),
+                                                      max(x["U"].shape[-1] for x in small)],
+                   "plain_value": sub[0][0], "split_value": sub[1][0], "split_speedup": sub[1][0] / sub[0][0],
+                   "split_rechecks": sub[1][1]}
     return {
         "workload": (f"{len(ens)} of configuration 4's 256 dimer ensembles (N ~ U[50,400], E0 ~ U[0,2], g log-uniform "
                      f"[0.01,1], seed {BATCH_SEED}; dims {min(dims)}-{max(dims)}), {BATCH_TRAJ} trajectories each, "
@@ -325,6 +345,7 @@ def batched_bench(args, local):
                               "same ensembles run alone, whose trajectories are bit-identical)"},
         "gpu_launches": int(m1["launches"] - m0["launches"]),
         "host_build_s": t_build,
+        "split_precision_batch": split_batch,
     }
 
 
@@ -432,10 +453,13 @@ def production_sweep(args, local):
 
 # ---------------------------------------------------------------- serving loop (configuration 5, sampled)
 def serving_bench(args, local):
-    """Continuous batching (os_d_b200.serve): Poisson arrivals at 50/s over a short window, each
-    request a dimer ensemble with N log-uniform in [31, 255], E0 ~ U[0, 2], g log-uniform in
-    [0.01, 1], seed 23; latency from arrival to result on the wall clock; the same requests then
-    solved one after another by single-ensemble engines (serial plain FP64)."""
+    """Continuous batching (os_d_b200.serve): Poisson arrivals at 50/s over a short window with
+    configuration 5's size range (N log-uniform in [31, 1023]; E0 ~ U[0, 2], g log-uniform in
+    [0.01, 1], seed 23) but trajectories U[10, 1000] and 1-3 periods (its full sizes, up to 10^4
+    trajectories x 500 periods at d = 1024, are hours of device time per request); size-class pools
+    admitted against the device's free memory, operators built on the GPU; latency from arrival to
+    result on the wall clock; the same requests then solved one after another by single-ensemble
+    engines (serial plain FP64)."""
     import os_d_b200 as q
     from os_d_b200.serve import Server, dimer_ensemble
 
@@ -445,22 +469,22 @@ def serving_bench(args, local):
         t += rng.exponential(1.0 / 50.0)
         if t > args.serve_window:
             break
-        N = int(round(10 ** rng.uniform(np.log10(31), np.log10(255))))
-        arrivals.append((t, dict(N=N, n_traj=int(rng.integers(100, 501)), periods=int(rng.integers(5, 21)),
+        N = int(round(10 ** rng.uniform(np.log10(31), np.log10(1023))))
+        arrivals.append((t, dict(N=N, n_traj=int(rng.integers(10, 1001)), periods=int(rng.integers(1, 4)),
                                  E0=float(rng.uniform(0, 2)), g=float(10 ** rng.uniform(-2, 0)), seed=23,
                                  tr_base=1000 * len(arrivals))))
-    srv = Server(n_slots=64, d_cap=256, n_cap=500, deep=DEEP, hbm_budget=40 << 30, device=local)
+    srv = Server(deep=DEEP, device=local)
     t0 = time.perf_counter()
     res = srv.run(arrivals)
     wall = time.perf_counter() - t0
-    dev_ms = srv.device_ms
+    dev_ms, pools, peak = srv.device_ms, srv.pools_created, srv.peak_bytes
     srv.close()
     lat = np.array([r["t_done"] - r["t_submit"] for r in res])
     work = float(sum(r["n_traj"] * r["periods"] for r in res))
     # serial plain FP64 solves of the same requests (device time of each alone)
     ser_ms = 0.0
     for _, r in arrivals:
-        e = dimer_ensemble(r, DEEP)
+        e = dimer_ensemble(r, DEEP, local)
         d, n = e["U"].shape[-1], e["n_traj"]
         A = q.Engine(e["U"], e["L"], e["g"], e["HE"], None, e["T"], n, seed=e["seed"], tr_base=e["tr_base"],
                      max_dumps=1, device=local)
@@ -472,14 +496,15 @@ def serving_bench(args, local):
         ser_ms += A.stats()["kernel_ms"]
         A.close()
     return {
-        "workload": (f"{len(arrivals)} requests, Poisson 50/s over {args.serve_window:g} s; dimer N log-uniform [31,255], "
-                     f"trajectories U[100,500], periods U[5,20], E0 ~ U[0,2], g log-uniform [0.01,1], seed 23; "
-                     f"64 resident slots (d <= 256, 500 trajectories), one period per tick"),
+        "workload": (f"{len(arrivals)} requests, Poisson 50/s over {args.serve_window:g} s; dimer N log-uniform "
+                     f"[31,1023] (d up to 1024), trajectories U[10,1000], periods U[1,3], E0 ~ U[0,2], g log-uniform "
+                     f"[0.01,1], seed 23; size-class pools of 8 slots admitted against free device memory"),
         "metric": METRIC, "value": work / wall, "device_value": work / (dev_ms * 1e-3),
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
         "serial_single_ensemble_engines": {"value": work / (ser_ms * 1e-3), "device_s": ser_ms * 1e-3},
-        "speedup_vs_serial_device": ser_ms / dev_ms, "ticks": srv.ticks, "wall_s": wall,
+        "speedup_vs_serial_device": ser_ms / dev_ms, "pools_created": pools, "peak_pool_bytes": peak,
+        "wall_s": wall, "max_d": int(max(r["N"] for _, r in arrivals)) + 1,
     }
 
 
@@ -618,6 +643,17 @@ def run_ours(args):
 
     M = model()
     n, d, P, W = args.n_traj, M["d"], args.periods_per_step, args.warmup
+    tuned = None
+    if not args.profile and args.production_sweep == 0:
+        # the project's autotuner picks the tile shapes of this dimension in both precisions (cached
+        # for the engines below in a file of this run)
+        os.environ.setdefault("QJX_TILE_CACHE", os.path.join(tempfile.mkdtemp(), "tiles.txt"))
+        tuned = {}
+        for prec in (0, 1):
+            best, table = q.autotune(M["U"], M["L"], [1.0], M["HE"], T=M["T"], n_traj=2048, precision=prec,
+                                     n_periods=1, device=local)
+            tuned["split" if prec else "plain"] = {"best": best, "candidates_us_per_traj_period":
+                                                   [[t, round(us, 4)] for t, us in table]}
     steps_total = W + args.steps
     psi0 = start_states(n, d)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -723,6 +759,8 @@ def run_ours(args):
         "ensemble_n1_minus_n2": ens_sum[0], "ensemble_n1_minus_n2_stderr": ens_sum[1],
         "matvecs_per_traj_period": matvecs / (n * P * args.steps),
     }
+    if tuned:
+        line["autotune"] = tuned
 
     # split-precision form: same checkpoint, same windows
     if not args.no_split:

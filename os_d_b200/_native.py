@@ -20,7 +20,7 @@ EXPORTS = [
     "qjx_create", "qjx_create_rk", "qjx_build_dimer_rk", "qjx_build_dimer_deep", "qjx_destroy", "qjx_last_error", "qjx_status_string", "qjx_set_states", "qjx_set_uniforms",
     "qjx_init_thresholds", "qjx_run_periods", "qjx_reset_times", "qjx_observe", "qjx_get_observables",
     "qjx_get_mean_start", "qjx_purity", "qjx_get_states", "qjx_jump_count", "qjx_get_jumps", "qjx_get_stats",
-    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_autotune", "qjx_build_dimer", "qjx_expm",
+    "qjx_set_trace", "qjx_get_trace", "qjx_measure_fp64_peak", "qjx_autotune", "qjx_expm_tree", "qjx_mem_info", "qjx_engine_bytes", "qjx_build_dimer", "qjx_expm",
     "qjx_random_observables", "qjx_build_jcs", "qjx_mbl_size", "qjx_build_mbl", "qjx_mbl_imbalance", "qjx_build_integrable", "qjx_build_ps", "qjx_build_floq2spins", "qjx_build_floqnspins", "qjx_build_floqspph", "qjx_create_batch", "qjx_create_slots", "qjx_slot_load", "qjx_slot_release",
     "qjx_set_active", "qjx_set_bases_only", "qjx_checkpoint_size", "qjx_checkpoint_save", "qjx_checkpoint_load", "qjx_lpn_start", "qjx_lpn_period", "qjx_lpn_bases", "qjx_run_sub_periods", "qjx_lpn_get",
     "qjx_lpn_get_last", "qjx_fb_rk4_noalloc", "qjx_fb_build_dimer", "qjx_fb_create", "qjx_fb_run", "qjx_fb_info", "qjx_fb_get", "qjx_fb_destroy",
@@ -121,6 +121,9 @@ def lib():
         L.qjx_build_dimer.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int] + [c_double_p] * 5
         L.qjx_build_dimer_deep.argtypes = [C.c_int] + [C.c_double] * 6 + [C.c_int, C.c_int] + [c_double_p] * 5
         L.qjx_expm.argtypes = [C.c_int, c_double_p, c_double_p]
+        L.qjx_expm_tree.argtypes = [C.c_int, C.c_int, c_double_p, c_double_p, C.c_int, C.c_int, c_double_p]
+        L.qjx_mem_info.argtypes = [C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+        L.qjx_engine_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
         L.qjx_build_jcs.argtypes = [C.c_int] + [C.c_double] * 4 + [C.c_int] + [c_double_p] * 7
         L.qjx_mbl_size.argtypes = [C.c_int, C.c_int, c_int_p, c_int_p]
         L.qjx_build_mbl.argtypes = ([C.c_int] + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_double] * 3 + [C.c_int]
@@ -322,6 +325,28 @@ def fb_build_dimer(N, J, U, E, g):
     check(L.qjx_fb_build_dimer(N, J, U, E, g, C.byref(gn), C.byref(qn), ip(gr), ip(gc), dp(gv), ip(qr), ip(qc),
                                dp(qv), dp(ks)), what="qjx_fb_build_dimer")
     return (gr, gc, gv), (qr, qc, qv), ks
+
+
+def build_dimer_gpu(N, J, U, E, A, g, omega, deep, device=0):
+    """The dimer's H, Hd, L on the host and its split tree on the GPU (qjx_expm_tree): the outputs
+    of build_dimer, the tree within about 1e-12 of the host's level-by-level exponentials."""
+    d = N + 1
+    H, Hd, L = (np.zeros((d, d), np.complex128) for _ in range(3))
+    K = np.zeros((2, d, d), np.complex128)
+    check(lib().qjx_build_dimer(N, J, U, E, A, g, omega, deep, dp(H), dp(Hd), dp(L), dp(K), None),
+          what="qjx_build_dimer")
+    T = 2.0 * 3.1415926535897932384626433832795 / omega
+    Ut = np.zeros((2, deep, d, d), np.complex128)
+    head = np.array([T, T])
+    check(lib().qjx_expm_tree(d, 2, dp(K), dp(head), deep, device, dp(Ut)), what="qjx_expm_tree")
+    return H, Hd, L, Ut
+
+
+def mem_info(device=0):
+    """(free, total) device bytes (cudaMemGetInfo)."""
+    f, t = C.c_size_t(), C.c_size_t()
+    check(lib().qjx_mem_info(device, C.byref(f), C.byref(t)), what="qjx_mem_info")
+    return f.value, t.value
 
 
 def expm(A):

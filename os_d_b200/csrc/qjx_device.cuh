@@ -44,17 +44,7 @@ constexpr int kSlotArgs = 2, kSlotK1 = 3, kSlotND = 6, kRkSlots = 7;
 
 enum ErrCode : int { ERR_NONE = 0, ERR_NORM = 1, ERR_ZERO_W = 2, ERR_RNG = 3, ERR_TIMEOUT = 6 };
 
-// Where the input vector of a trajectory's next matvec is, as the epilogue leaves it (the split
-// form writes that vector's bf16 planes for the next micro-step): the epilogue's column itself,
-// the column divided by a scalar, the input of this micro-step again, or a state slot in global
-// memory.
-enum NextSrc : int { SRC_NONE = 0, SRC_COL = 1, SRC_SCALED = 2, SRC_SAME = 3, SRC_GLOBAL = 4 };
 constexpr int kRecheck = -2;  // column_epilogue: the trajectory goes to the FP64 recheck list
-struct EpiOut {
-    int mode;    // NextSrc
-    int slot;    // state slot of the next input (SRC_GLOBAL)
-    double div;  // SRC_SCALED: the next input is col / div
-};
 
 // Per-trajectory state (one 144-byte record per trajectory).
 struct __align__(16) TrajState {
@@ -129,16 +119,9 @@ struct Params {
     int MDs, KS;                  // rows padded to 16 (MMA N), k-steps of 16 complex components
     int sstages;                  // depth of the split kernel's operand ring
     const unsigned char *usplit;  // [G][KS][4 planes: Re hi, Re lo, Im hi, Im lo][MDs rows x 16 k] bf16
-    // bf16 planes of the input vector of every bucket position, two buffers (micro-step s reads
-    // buffer s & 1 and its epilogue fills buffer (s + 1) & 1): group g's region starts at byte
-    // g_soff[g] and holds, for each k-step and plane, scap positions x 32 bytes in the tcgen05
-    // K-major core-matrix order (8-position groups of 256 bytes, the two K-halves 128 bytes apart)
-    unsigned char *stage;
-    size_t stage_bytes;           // one buffer
-    const long long *g_soff;      // [G]
-    // per ensemble: rows padded to 16 (MMA N), k-steps, stage positions per (group, k-step,
-    // plane) (its trajectories rounded up to 8); per group: byte offset of its B planes in usplit
-    const int *e_mds, *e_ks, *e_scap;
+    // per ensemble: rows padded to 16 (MMA N) and k-steps; per group: byte offset of its B planes
+    // in usplit
+    const int *e_mds, *e_ks;
     const long long *g_uoff;
     // tile plan of the next micro-step: [0] rows per tile, [1 + g] first tile of group g,
     // [1 + G] tiles in all; written by the last CTA of a micro-step (or split_plan_kernel)

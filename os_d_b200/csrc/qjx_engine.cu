@@ -463,12 +463,11 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     P.grid = h->grid;
     if (c.precision == 1) {  // split precision: bf16 planes of every matrix in the tcgen05 order
         P.split = 1;
-        std::vector<int> e_mds(E), e_ks(E), e_scap(E);
+        std::vector<int> e_mds(E), e_ks(E);
         int mds_max = 16;
         for (int e = 0; e < E; e++) {
             e_mds[e] = 16 * ((ens[e].d + 15) / 16);
             e_ks[e] = (ens[e].d + 15) / 16;
-            e_scap[e] = 8 * ((ens[e].n + 7) / 8);
             mds_max = std::max(mds_max, e_mds[e]);
         }
         P.MDs = mds_max;
@@ -489,30 +488,23 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
             return bail(QJX_ERR_UNSUPPORTED);
         P.sstages = want_st;
         P.min_rows = want_rows;
-        // per group: its bf16 matrix planes (usplit) and the input-vector planes of every bucket
-        // position (two stage buffers), in its ensemble's own padded layout
-        std::vector<long long> soff(G), uoff(G);
-        size_t sbytes = 0, ubytes = 0;
+        // per group: its bf16 matrix planes (usplit) in its ensemble's own padded layout
+        std::vector<long long> uoff(G);
+        size_t ubytes = 0;
         for (int gg = 0; gg < G; gg++) {
             const int e = g_ens[gg];
-            soff[gg] = (long long)sbytes;
             uoff[gg] = (long long)ubytes;
-            sbytes += (size_t)e_ks[e] * 4 * (size_t)e_scap[e] * 32;
             ubytes += (size_t)e_ks[e] * 4 * (size_t)e_mds[e] * 32;
         }
         P.e_mds = upload(h, e_mds);
         P.e_ks = upload(h, e_ks);
-        P.e_scap = upload(h, e_scap);
-        P.g_soff = upload(h, soff);
         P.g_uoff = upload(h, uoff);
-        P.stage_bytes = sbytes;
-        P.stage = (unsigned char *)dalloc(h, 2 * P.stage_bytes);
         P.splan = (int *)dalloc(h, (size_t)(G + 2) * sizeof(int));
         // near-threshold FP64 rechecks: lists, band, and the matrix slab height that fits the ring
         // next to the input and product vectors
         P.rcnt = (int *)dalloc(h, 3 * sizeof(int));
         P.rlist = (int *)dalloc(h, (size_t)2 * n * sizeof(int));
-        if (!P.e_mds || !P.e_ks || !P.e_scap || !P.g_soff || !P.g_uoff || !P.stage || !P.splan || !P.rcnt || !P.rlist)
+        if (!P.e_mds || !P.e_ks || !P.g_uoff || !P.splan || !P.rcnt || !P.rlist)
             return bail(QJX_ERR_OOM);
         P.recheck_tol = c.split_recheck == 0.0 ? 1e-5 : (c.split_recheck < 0.0 ? 0.0 : c.split_recheck);
         const size_t ring = (size_t)P.sstages * split_stage_bytes(P.MDs);

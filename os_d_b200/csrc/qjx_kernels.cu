@@ -288,16 +288,13 @@ __device__ int apply_jump(const Params &P, TrajState &s, int tr, double2 *col, i
 // Warp-cooperative epilogue of one trajectory column: `col` holds M_g * psi in shared memory,
 // `s_in` the trajectory's state record (loaded by the caller).  Returns the bucket of the
 // trajectory's next micro-step, or -1 (done, paused or failed); the caller appends it.
-__device__ int column_epilogue(const Params &P, double2 *col, int tr, const TrajState &s_in, int lane,
-                                EpiOut *eo = nullptr)
+__device__ int column_epilogue(const Params &P, double2 *col, int tr, const TrajState &s_in, int lane)
 {
     const int d = dim_of(P, s_in);
     TrajState s = s_in;
     int g2 = -1;
     int err = 0;
     bool paused = false;
-    int nsrc = SRC_GLOBAL;  // where the next matvec's input is (read by the split form)
-    double ndiv = 1.0;
 
     switch (s.phase) {
     case PH_STEP: {
@@ -324,11 +321,9 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
             s.cur ^= 1;
             s.t = __dadd_rn(s.t, dt);
             g2 = after_step(P, s, tr, col, lane);
-            nsrc = (s.phase == PH_STEP) ? SRC_COL : SRC_GLOBAL;
         } else if (s.lvl < P.deep - 1) {  // crossed on a coarse level: bisect from psi (qj_proc.cpp:328-331)
             s.lvl += 1;
             g2 = s.b * P.deep + s.lvl;
-            nsrc = SRC_SAME;
         } else {  // crossed on the finest level: jump (qj_proc.cpp:294-315)
             if (P.record) {
                 if (s.nrec >= P.rec_cap) {  // record buffer full: hold here, host drains and resumes
@@ -359,8 +354,6 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
             s.phase = PH_REC_W;
             s.sub = 0;
             g2 = P.gL0;
-            nsrc = SRC_SCALED;
-            ndiv = sq;
         }
     } break;
 
@@ -372,7 +365,6 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
         if (s.sub + 1 < P.nd) {
             s.sub += 1;
             g2 = P.gL0 + s.sub;
-            nsrc = SRC_SAME;
             break;
         }
         __syncwarp();
@@ -398,19 +390,16 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
         if (err) break;
         if (P.nd == 1) {
             g2 = apply_jump(P, s, tr, col, lane, index, w, &err);
-            nsrc = (s.phase == PH_STEP && P.prop == 0) ? SRC_COL : SRC_GLOBAL;
         } else {
             s.phase = PH_REC_A;
             s.sub = index;
             g2 = P.gL0 + index;
-            nsrc = SRC_SAME;
         }
     } break;
 
     case PH_REC_A: {
         const double w = P.gn[(size_t)tr * P.nd + s.sub];
         g2 = apply_jump(P, s, tr, col, lane, s.sub, w, &err);
-        nsrc = (s.phase == PH_STEP && P.prop == 0) ? SRC_COL : SRC_GLOBAL;
     } break;
 
     case PH_RK: {  // one right-hand side of rk_int_dimer (core.cpp:11592-11619), col = M arg
@@ -519,7 +508,6 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
             s.phase = PH_OBS_R;
             s.sub = 0;
             g2 = P.gR0;
-            nsrc = SRC_SAME;
         } else {
             g2 = finish_obs(P, s);
         }
@@ -541,7 +529,6 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
         if (s.sub + 1 < P.nr) {
             s.sub += 1;
             g2 = P.gR0 + s.sub;
-            nsrc = SRC_SAME;
         } else {
             g2 = finish_obs(P, s);
         }
@@ -565,11 +552,6 @@ __device__ int column_epilogue(const Params &P, double2 *col, int tr, const Traj
         P.st[tr] = s;
     }
     __syncwarp();
-    if (eo) {
-        eo->mode = (g2 >= 0) ? nsrc : SRC_NONE;
-        eo->div = ndiv;
-        eo->slot = src_slot(s.phase, s.cur, s.rk_stage);
-    }
     if (to_recheck) return kRecheck;
     return g2 >= 0 ? P.e_g0[s.ens] + g2 : -1;  // local group -> the ensemble's bucket
 }
@@ -1264,13 +1246,12 @@ bool pick_step_tiles(int MD, size_t budget, int *nc, int *kb)
     return false;
 }
 
-// The first micro-step after a host-side enqueue needs its plan (plain form) or the bf16 planes
-// of its input vectors (split form).
-cudaError_t launch_stage_lists(const Params &P, cudaStream_t st);
+// The first micro-step after a host-side enqueue needs its plan (both forms).
+cudaError_t launch_split_plan(const Params &P, cudaStream_t st);
 
 static cudaError_t launch_plan(const Params &P, cudaStream_t st)
 {
-    if (P.split) return launch_stage_lists(P, st);
+    if (P.split) return launch_split_plan(P, st);
     plan_kernel<<<1, 1024, 0, st>>>(P);
     return cudaGetLastError();
 }
@@ -1408,11 +1389,8 @@ cudaError_t launch_clear_records(const Params &P, cudaStream_t st)
 // ---------------------------------------------------------------- split-precision form
 #include "qjx_split.cuh"
 
-cudaError_t launch_stage_lists(const Params &P, cudaStream_t st)
+cudaError_t launch_split_plan(const Params &P, cudaStream_t st)
 {
-    const int warps = 8;
-    const int bx = std::max(1, std::min(64, (P.n + warps - 1) / warps));
-    stage_lists_kernel<<<dim3(bx, std::min(P.G, 65535)), warps * 32, 0, st>>>(P);
     split_plan_kernel<<<1, 512, 0, st>>>(P, P.grid);
     return cudaGetLastError();
 }

@@ -8,7 +8,7 @@
 //   Re y[m][r] = sum_k Xr[m][k] Ur[r][k] - Xi[m][k] Ui[r][k]     m: trajectory (128 TMEM lanes)
 //   Im y[m][r] = sum_k Xr[m][k] Ui[r][k] + Xi[m][k] Ur[r][k]     r: output row (MMA N = MDs)
 //
-//   A = the tile's input vectors (Xr, Xi) as bf16 planes,
+//   A = the tile's states (Xr, Xi) as bf16 planes, written by the CTA from the FP64 states,
 //   B = Re M and Im M as bf16 planes prepared once by the host,
 //   D = two FP32 accumulators in tensor memory, Re in columns [0, MDs), Im in [MDs, 2 MDs);
 //       the minus sign is the instruction descriptor's negate-A bit.
@@ -17,15 +17,9 @@
 // hi*hi + hi*lo + lo*hi in FP32 ("bf16x3"), which leaves about 2^-16 of relative error per
 // product and the FP32 accumulation error (measured about 4e-6 of max|y| per matvec at
 // d = 201).  The accumulators are read back to FP64 and the FP64 epilogue of the plain form
-// runs unchanged (norm test, jump, renormalisation, observables).
-//
-// Both operands arrive by TMA bulk copies.  The A planes of a micro-step are written by the
-// previous micro-step's epilogue: once a trajectory's next bucket and its position in it are
-// known, its next input vector (the new state, the renormalised state, or the unchanged input
-// of a bisection step) is split into bf16 planes and stored at that position of the next
-// step's stage buffer, already in the core-matrix order; a tile of R trajectories of one bucket
-// is then one contiguous copy of R x 32 bytes per plane and k-step.  (After a host-side enqueue
-// the stage buffer is filled from the FP64 states by stage_lists_kernel.)
+// runs unchanged (norm test, jump, renormalisation, observables), except that a norm within the
+// split error of the threshold is not decided: that trajectory's step is computed again as an
+// FP64 matvec (the plain form's arithmetic) by a CTA the split tiles leave free, which decides.
 //
 // Shared-memory operands use the K-major no-swizzle canonical layout: a core matrix is
 // 8 rows x 16 bytes (8 bf16 along K) stored contiguously; within one k-step (16 bf16 of K)
@@ -33,17 +27,19 @@
 // 8-row groups 256 bytes apart (stride byte offset).  The host writes B in exactly this
 // order, so one k-step of all four B planes is one contiguous TMA bulk copy.
 //
-// Per tile (one matrix, up to 128 trajectories) a ring of S stages (as many as shared memory
-// holds, 5 at d = 201), one k-step of A and B planes each:
+// Per tile (one matrix, up to 128 trajectories of one bucket) a ring of S stages, one k-step of
+// A and B planes each:
 //   warps 0-3, 6-9, 10-13   three producer groups, one thread per trajectory row; group p
 //               converts the k-steps ks = p (mod 3): FP64 state -> bf16 planes of A (generic
 //               stores, then fence.proxy.async and an arrive on fullA)
 //   warp 4      one thread issues the bulk copy of the B planes (complete_tx on fullB)
 //   warp 5      one thread issues the 12 tcgen05.mma of a k-step and commits them to empty[stage]
-// then the accumulators (commit to accf) are read by the warps whose TMEM lane quarter holds
-// each group of 32 trajectories, staged as FP64 columns in the (now idle) ring, and run
-// through column_epilogue.  Rows per tile are chosen per micro-step so that the tiles fit
-// one wave of CTAs.
+//   warps 14-15 load the tile's trajectory records meanwhile
+// then the FP32 accumulators of up to 64 trajectories at a time are staged in the idle ring by
+// the warps that own their TMEM lane quarters, and every warp runs its trajectories through the
+// epilogue and appends them to their next buckets.  A batched engine's ensembles each have their
+// own padded rows and k-steps; the tile plan of the next micro-step (rows per tile, first tile of
+// every bucket) is made by the last CTA to finish one.
 
 constexpr int kAPlanes = 4;                  // A and B planes: Re hi, Re lo, Im hi, Im lo
 constexpr int kTileM = 128;                  // MMA M = TMEM lanes (a tile holds up to 128 trajectories)
@@ -122,89 +118,13 @@ __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo
     lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-// Byte offset, in a stage buffer, of the 16-byte chunk (k-step ks, plane p, K-half kh) of bucket
-// position pos of group g.
-__device__ __forceinline__ size_t stage_chunk(const Params &P, int g, int ks, int p, int kh, int pos)
-{
-    const size_t cap = (size_t)P.e_scap[P.g_ens[g]];
-    return (size_t)P.g_soff[g] + ((size_t)(ks * kAPlanes + p) * cap + (size_t)(pos & ~7)) * 32 + (size_t)kh * 128 +
-           (size_t)(pos & 7) * 16;
-}
-
-// Writes the bf16 planes of a trajectory's next input vector at position pos of group g of the
-// stage buffer `dst` (warp-cooperative; a lane converts 8 consecutive components, one K-half of
-// one k-step, into its four 16-byte chunks).  Components from d on are zero.  The vector is
-// col, col / div, the planes at position pos0 of group g0 in `src_stage`, or gsrc.
-__device__ void stage_write(const Params &P, unsigned char *dst, int g, int pos, int mode, const double2 *col,
-                            double div, const double2 *gsrc, const unsigned char *src_stage, int g0, int pos0, int d,
-                            int lane)
-{
-    const int KS = P.e_ks[P.g_ens[g]];
-    for (int pr = lane; pr < 2 * KS; pr += 32) {
-        const int ks = pr >> 1, kh = pr & 1;
-        uint4 c[kAPlanes];
-        if (mode == SRC_SAME) {
-#pragma unroll
-            for (int p = 0; p < kAPlanes; p++)
-                c[p] = *reinterpret_cast<const uint4 *>(src_stage + stage_chunk(P, g0, ks, p, kh, pos0));
-        } else {
-            double2 v[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int k = 16 * ks + 8 * kh + i;
-                double2 x = make_double2(0.0, 0.0);
-                if (k < d) {
-                    if (mode == SRC_GLOBAL) {
-                        x = gsrc[k];
-                    } else {
-                        x = col[k];
-                        if (mode == SRC_SCALED) x = make_double2(__ddiv_rn(x.x, div), __ddiv_rn(x.y, div));
-                    }
-                }
-                v[i] = x;
-            }
-            uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                split_pair(make_double2(v[2 * j].x, v[2 * j + 1].x), rh[j], rl[j]);
-                split_pair(make_double2(v[2 * j].y, v[2 * j + 1].y), ih[j], il[j]);
-            }
-            c[0] = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-            c[1] = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-            c[2] = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-            c[3] = make_uint4(il[0], il[1], il[2], il[3]);
-        }
-#pragma unroll
-        for (int p = 0; p < kAPlanes; p++) *reinterpret_cast<uint4 *>(dst + stage_chunk(P, g, ks, p, kh, pos)) = c[p];
-    }
-}
-
-// Planes of step 0 after a host-side enqueue (schedule, observe, resume): block (x, y) takes
-// positions of buckets y, y + gridDim.y, ..., one warp per position, from the trajectories' FP64
-// input slots.
-__global__ void stage_lists_kernel(const Params P)
-{
-    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int g = blockIdx.y; g < P.G; g += gridDim.y) {
-        const int cnt = P.cnt[g];
-        for (int pos = blockIdx.x * nw + (threadIdx.x >> 5); pos < cnt; pos += gridDim.x * nw) {
-            const int tr = P.lists[P.g_loff[g] + pos];
-            const TrajState s = P.st[tr];
-            const int slot = src_slot(s.phase, s.cur, s.rk_stage);
-            stage_write(P, P.stage, g, pos, SRC_GLOBAL, nullptr, 1.0, slot_ptr(P, slot, tr), nullptr, 0, 0,
-                        dim_of(P, s), lane);
-        }
-    }
-}
-
-// FP64 recheck of one trajectory's step (split form): y = M x with the plain form's arithmetic
-// (per output the k-ascending fma chain of the contract, k up to the even kp), the matrix
-// streamed through the free operand ring in slabs of kb k rows by TMA bulk copies (two buffers,
-// mbarriers rbar[0..1]), then the epilogue decides with the FP64 norm and the trajectory is
-// appended to its next bucket with its next input's planes.  Whole CTA; returns false when a
-// bounded wait gave up.
+// FP64 recheck of one trajectory's step: y = M x with the plain form's arithmetic (per output the
+// k-ascending fma chain of the contract, k up to the even kp), the matrix streamed through the free
+// operand ring in slabs of kb k rows by TMA bulk copies (two buffers, mbarriers rbar[0..1]), then
+// the epilogue decides with the FP64 norm and the trajectory joins its next bucket.  Whole CTA;
+// returns false when a bounded wait gave up.
 __device__ bool recheck_column(const Params &P, int tr, unsigned char *smem, TrajState *st_s, uint64_t *rbar,
-                               uint32_t &rphase, int *cnt_next, int *list_next, unsigned char *stage_next)
+                               uint32_t &rphase, int *cnt_next, int *list_next)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) load_state(st_s, &P.st[tr]);
@@ -257,18 +177,10 @@ __device__ bool recheck_column(const Params &P, int tr, unsigned char *smem, Tra
     if (tid < dg) ys[tid] = make_double2(re, im);
     __syncthreads();
     if (warp == 0) {
-        EpiOut eo{SRC_NONE, 0, 1.0};
-        const int g2 = column_epilogue(P, ys, tr, st, lane, &eo);
-        if (g2 >= 0) {
-            int pos = 0;
-            if (lane == 0) {
-                pos = atomicAdd(&cnt_next[g2], 1);
-                list_next[P.g_loff[g2] + pos] = tr;
-            }
-            pos = __shfl_sync(0xffffffffu, pos, 0);
-            // the unchanged input of a bisection step has no planes at a position of this step
-            const int mode = (eo.mode == SRC_SAME) ? SRC_GLOBAL : eo.mode;
-            stage_write(P, stage_next, g2, pos, mode, ys, eo.div, slot_ptr(P, eo.slot, tr), nullptr, 0, 0, dg, lane);
+        const int g2 = column_epilogue(P, ys, tr, st, lane);
+        if (g2 >= 0 && lane == 0) {
+            const int pos = atomicAdd(&cnt_next[g2], 1);
+            list_next[P.g_loff[g2] + pos] = tr;
         }
     }
     fence_proxy_async();  // generic writes to the ring before later bulk copies into it
@@ -371,11 +283,10 @@ __device__ __forceinline__ int split_tile_group(const Params &P, int t, int lane
 }
 
 // Dynamic shared memory: a ring of `stages` operand stages, each [A planes][B planes] of one
-// k-step; after the MMAs of a tile the ring holds the FP64 epilogue columns (32 x (MDs + 1)).
+// k-step; after the MMAs of a tile the ring holds the epilogue's FP32 accumulators of up to 64
+// trajectories (one row of 2 MDs + 1 floats each: Re then Im) and one FP64 column per warp.
 size_t split_stage_bytes(int MDs) { return (size_t)kAPlanes * (kABytes + (size_t)MDs * 32); }
 
-// Epilogue shared memory (in the idle ring): the FP32 accumulators of `rows` trajectories, one row
-// of 2 MDs + 1 floats each (Re then Im), then one FP64 column of MDs + 1 per warp.
 __host__ __device__ inline size_t split_epi_f32_bytes(int MDs, int rows)
 {
     return ((size_t)rows * (2 * MDs + 1) * 4 + 15) & ~(size_t)15;
@@ -398,11 +309,13 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     extern __shared__ __align__(128) unsigned char smem[];
     const int S = P.sstages;
     const size_t stage_bytes = (size_t)kAPlanes * (kABytes + (size_t)P.MDs * 32);  // ring stride (largest MDs)
-    __shared__ __align__(8) uint64_t full[kMaxSStages], empty[kMaxSStages], accf, rbar[2];
+    __shared__ __align__(8) uint64_t fullA[kMaxSStages], fullB[kMaxSStages], empty[kMaxSStages], accf, rbar[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_tr[kTileM];
+    __shared__ long long s_src[kTileM];
     __shared__ __align__(16) TrajState s_st[kTileM];
     __shared__ int s_fail, s_last;
+    __shared__ int w_g2[kThreads / 32][kTileM / (kThreads / 32)];  // per warp: its trajectories' next buckets
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // epilogue rows staged per pass: 64 when their FP32 accumulators and the warps' FP64 columns
@@ -410,13 +323,11 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const size_t dyn = max((size_t)S * stage_bytes, split_epi_bytes(P.MDs, 32));
     const int RP = split_epi_bytes(P.MDs, 64) <= dyn ? 64 : 32;
     double2 *wcol = reinterpret_cast<double2 *>(smem + split_epi_f32_bytes(P.MDs, RP)) + (size_t)warp * (P.MDs + 1);
-    const int G = P.G;
+    const int G = P.G, n = P.n;
     const int *cnt_cur = P.cnt + (s % 3) * G;
     int *cnt_next = P.cnt + ((s + 1) % 3) * G;
     const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
     int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
-    const unsigned char *stage_cur = P.stage + (size_t)(s & 1) * P.stage_bytes;
-    unsigned char *stage_next = P.stage + (size_t)((s + 1) & 1) * P.stage_bytes;
     const int *rlist_cur = P.rlist + (size_t)(s & 1) * P.n;
     int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
     int *rcnt_next = P.rcnt + (s + 1) % 3;
@@ -430,7 +341,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     if (warp == 0) {
         if (lane == 0) {
             for (int q = 0; q < S; q++) {
-                mbar_init(&full[q], 1);
+                mbar_init(&fullA[q], kTileM);
+                mbar_init(&fullB[q], 1);
                 mbar_init(&empty[q], 1);
             }
             mbar_init(&accf, 1);
@@ -458,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
 
     for (int t = blockIdx.x; t < T + Rtot && ok; t += gridDim.x) {
         if (t >= T) {  // an FP64 recheck (the CTAs past the split tiles take these first)
-            if (!recheck_column(P, rlist_cur[t - T], smem, &s_st[0], rbar, rphase, cnt_next, list_next, stage_next)) {
+            if (!recheck_column(P, rlist_cur[t - T], smem, &s_st[0], rbar, rphase, cnt_next, list_next)) {
                 ok = false;
                 break;
             }
@@ -469,39 +381,80 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         const long long t0 = clock64();
         const int g = split_tile_group(P, t, lane);  // every warp finds it (warp-uniform)
         const int e = P.g_ens[g];
-        const int MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
+        const int d = P.e_d[e], MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
         const int base = (t - __ldcg(P.splan + 1 + g)) * R;
         const int rows = min(R, __ldcg(cnt_cur + g) - base);
-        const int rows8 = (rows + 7) & ~7;
+        if (tid < kTileM) {
+            if (tid < rows) {
+                const int tr = list_cur[P.g_loff[g] + base + tid];
+                const TrajState *sp = &P.st[tr];
+                const int slot = src_slot(sp->phase, sp->cur, sp->rk_stage);
+                s_tr[tid] = tr;
+                s_src[tid] = ((long long)slot * n + tr) * P.MD;
+            } else {
+                s_tr[tid] = -1;
+                s_src[tid] = -1;
+            }
+        }
+        __syncthreads();
+        const long long t1 = clock64();
         const uint32_t it0 = kit;  // k-steps issued before this tile
         const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
         const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
-        const long long t1 = clock64();
 
-        if (warp == 4) {
-            if (lane == 0) {  // producer: per k-step the four A planes of the tile's rows and the B planes
+        const int agrp = (warp < 4) ? 0 : (warp >= 6 && warp < 10) ? 1 : (warp >= 10 && warp < 14) ? 2 : -1;
+        if (agrp >= 0) {
+            // A producers: group p (4 warps, thread m = row m) handles the k-steps ks = p (mod 3), so
+            // three independent load-convert chains run in parallel; each thread issues its loads
+            // before waiting for the stage to drain
+            const int m = tid - (agrp == 0 ? 0 : (agrp == 1 ? 192 : 320));
+            const double2 *src = (s_src[m] >= 0) ? P.psi + s_src[m] : nullptr;
+            const int off = (m & 7) * 16 + (m >> 3) * 256;
+            for (int ks = agrp; ks < KS && ok; ks += 3) {
+                const uint32_t it = it0 + ks, q = it % S;
+                unsigned char *As = smem + q * stage_bytes + off;
+                for (int hh = 0; hh < 2; hh++) {  // K-halves: components 16 ks + 8 hh .. + 7
+                    double2 v[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const int k = 16 * ks + 8 * hh + i;
+                        v[i] = (src && k < d) ? src[k] : make_double2(0.0, 0.0);
+                    }
+                    if (hh == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
+                        ok = false;
+                    uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        split_pair(make_double2(v[2 * j].x, v[2 * j + 1].x), rh[j], rl[j]);
+                        split_pair(make_double2(v[2 * j].y, v[2 * j + 1].y), ih[j], il[j]);
+                    }
+                    *reinterpret_cast<uint4 *>(As + 128 * hh) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                    *reinterpret_cast<uint4 *>(As + kABytes + 128 * hh) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                    *reinterpret_cast<uint4 *>(As + 2 * kABytes + 128 * hh) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                    *reinterpret_cast<uint4 *>(As + 3 * kABytes + 128 * hh) = make_uint4(il[0], il[1], il[2], il[3]);
+                }
+                fence_proxy_async();
+                mbar_arrive(&fullA[q]);
+            }
+        } else if (warp == 4) {
+            if (lane == 0) {  // B producer
                 const unsigned char *ug = P.usplit + P.g_uoff[g];
-                const uint32_t abytes = (uint32_t)rows8 * 32;
                 for (int ks = 0; ks < KS && ok; ks++) {
                     const uint32_t it = it0 + ks, q = it % S;
                     if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait)) {
                         ok = false;
                         break;
                     }
-                    unsigned char *dq = smem + q * stage_bytes;
-                    mbar_expect_tx(&full[q], kAPlanes * (abytes + (uint32_t)bbytes));
-#pragma unroll
-                    for (int p = 0; p < kAPlanes; p++)
-                        bulk_g2s(dq + p * kABytes, stage_cur + stage_chunk(P, g, ks, p, 0, base), abytes, &full[q]);
-                    bulk_g2s(dq + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes, (uint32_t)(kAPlanes * bbytes),
-                             &full[q]);
+                    mbar_expect_tx(&fullB[q], (uint32_t)(kAPlanes * bbytes));
+                    bulk_g2s(smem + q * stage_bytes + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes,
+                             (uint32_t)(kAPlanes * bbytes), &fullB[q]);
                 }
             }
         } else if (warp == 5) {
             if (lane == 0) {  // MMA issuer
                 for (int ks = 0; ks < KS && ok; ks++) {
                     const uint32_t it = it0 + ks, q = it % S, par = (it / S) & 1u;
-                    if (!mbar_wait_bounded(&full[q], par, kSplitWait)) {
+                    if (!mbar_wait_bounded(&fullA[q], par, kSplitWait) || !mbar_wait_bounded(&fullB[q], par, kSplitWait)) {
                         ok = false;
                         break;
                     }
@@ -532,13 +485,9 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                 }
                 umma_commit(&accf);
             }
-        } else if (warp < 4) {
-            // the tile's trajectories and their state records, loaded while the MMAs run
-            if (tid < rows) {
-                const int tr = list_cur[P.g_loff[g] + base + tid];
-                s_tr[tid] = tr;
-                load_state(&s_st[tid], &P.st[tr]);
-            }
+        } else {
+            // warps 14-15: the tile's state records, loaded while the MMAs run
+            for (int m = tid - 448; m < rows; m += 64) load_state(&s_st[m], &P.st[s_tr[m]]);
         }
         kit += (uint32_t)KS;
         if (!ok) atomicExch(&s_fail, 1);
@@ -573,30 +522,28 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             tc_fence_before();
             __syncthreads();
             tr_stage += clock64() - ts;
-            // every warp runs its trajectories through the epilogue, takes their positions in the
-            // next buckets (one atomic each) and writes their next input vectors' planes
+            // every warp runs its trajectories (columns warp, warp + 16, ...) through the epilogue,
+            // then appends them to their next buckets with one atomic each, all in flight together
             const int pn = min(RP, rows - p0);
-            for (int cc = warp; cc < pn; cc += kThreads / 32) {
+            int nm = 0;
+            for (int cc = warp; cc < pn; cc += kThreads / 32, nm++) {
                 const int m = p0 + cc;
                 const float *row = sacc + (size_t)cc * SR;
                 for (int k = lane; k < MDs; k += 32) wcol[k] = make_double2((double)row[k], (double)row[MDs + k]);
                 __syncwarp();
-                EpiOut eo{SRC_NONE, 0, 1.0};
-                const int tr = s_tr[m];
-                const int g2 = column_epilogue(P, wcol, tr, s_st[m], lane, &eo);
-                if (g2 >= 0 || g2 == kRecheck) {
-                    int pos = 0;
-                    if (lane == 0) pos = atomicAdd(g2 >= 0 ? &cnt_next[g2] : rcnt_next, 1);
-                    pos = __shfl_sync(0xffffffffu, pos, 0);
-                    if (g2 >= 0) {
-                        if (lane == 0) list_next[P.g_loff[g2] + pos] = tr;
-                        stage_write(P, stage_next, g2, pos, eo.mode, wcol, eo.div, slot_ptr(P, eo.slot, tr), stage_cur,
-                                    g, base + m, P.e_d[s_st[m].ens], lane);
-                    } else if (lane == 0) {
-                        rlist_next[pos] = tr;
-                    }
-                }
+                const int g2 = column_epilogue(P, wcol, s_tr[m], s_st[m], lane);
+                if (lane == 0) w_g2[warp][nm] = g2;
                 __syncwarp();
+            }
+            if (lane < nm) {
+                const int g2 = w_g2[warp][lane];
+                const int tr = s_tr[p0 + warp + (kThreads / 32) * lane];
+                if (g2 >= 0) {
+                    const int pos = atomicAdd(&cnt_next[g2], 1);
+                    list_next[P.g_loff[g2] + pos] = tr;
+                } else if (g2 == kRecheck) {
+                    rlist_next[atomicAdd(rcnt_next, 1)] = tr;
+                }
             }
             fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
             __syncthreads();
@@ -617,8 +564,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         }
         if (warp == 4 && lane == 0) {
             for (int q = 0; q < S; q++) {
-                mbar_wait_bounded(&full[q], 0u, 1024);
-                mbar_wait_bounded(&full[q], 1u, 1024);
+                mbar_wait_bounded(&fullB[q], 0u, 1024);
+                mbar_wait_bounded(&fullB[q], 1u, 1024);
             }
             for (int q = 0; q < 2; q++) {
                 mbar_wait_bounded(&rbar[q], 0u, 1024);

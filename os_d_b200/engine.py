@@ -336,6 +336,12 @@ class Engine:
                   "qjx_get_trace")
         return out
 
+    def device_bytes(self):
+        """Device memory this engine holds (qjx_engine_bytes)."""
+        b = C.c_size_t()
+        self._chk(N.lib().qjx_engine_bytes(self.h, C.byref(b)), "qjx_engine_bytes")
+        return b.value
+
     def stats(self):
         s = N.QjxStats()
         self._chk(N.lib().qjx_get_stats(self.h, C.byref(s)), "qjx_get_stats")

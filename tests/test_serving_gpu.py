@@ -60,6 +60,9 @@ def test_slots_join_and_leave_a_running_batch():
 
 
 def test_server_results_equal_solo_runs():
+    """Requests of several size classes, one of them d = 521 (a pool of class 1024), arrive while
+    others run; the server creates pools within the device's free memory, and every result equals
+    the same request solved alone with the same (GPU-built) operators, bit for bit."""
     import os_d_b200 as q
     from os_d_b200.serve import Server, dimer_ensemble
 
@@ -70,13 +73,45 @@ def test_server_results_equal_solo_runs():
         r = dict(N=int(rng.integers(8, 60)), n_traj=int(rng.integers(5, 40)), periods=int(rng.integers(1, 5)),
                  E0=float(rng.uniform(0, 2)), g=float(10 ** rng.uniform(-2, 0)), seed=100 + i, tr_base=1000 * i)
         arrivals.append((0.02 * i, r))
-    srv = Server(n_slots=4, d_cap=64, n_cap=40, deep=deep, hbm_budget=None)
+    arrivals.append((0.05, dict(N=520, n_traj=6, periods=1, E0=1.0, g=0.05, seed=77, tr_base=0)))
+    srv = Server(deep=deep, slots_per_pool=2, reserve_bytes=1 << 30)
     res = srv.run(arrivals)
+    created = srv.pools_created
     srv.close()
-    assert len(res) == 10
+    assert len(res) == 11 and created >= 3
     for r in res:
         ens = dimer_ensemble(r, deep)
         (psi_a, _, _, _), obs_a, _ = alone(q, ens, int(r["periods"]), deep)
         assert np.array_equal(r["result"]["psi"], psi_a)
         assert np.array_equal(r["result"]["mean"], obs_a["mean"][0])
         assert r["t_done"] >= r["t_admit"] >= r["t_submit"]
+
+
+@pytest.mark.parametrize("d_cap,n_cap", [(64, 256), (256, 1024), (1024, 256)])
+def test_pool_footprint_estimate_matches_engine(d_cap, n_cap):
+    """The admission estimate of a pool's device memory is within 10 % of what the engine allocates."""
+    import os_d_b200 as q
+    from os_d_b200.serve import pool_footprint
+
+    eng = q.Engine.slots(4, d_cap, n_cap, deep=16, max_dumps=1, rec_cap=16)
+    actual = eng.device_bytes()
+    eng.close()
+    est = pool_footprint(4, d_cap, n_cap, 16)
+    assert abs(est - actual) <= 0.1 * actual, (est, actual)
+
+
+@pytest.mark.parametrize("N", [20, 200, 700])
+def test_gpu_split_tree_matches_host_build(N):
+    """qjx_expm_tree (Taylor at the finest level, then one squaring per level, on the GPU) against
+    the host's level-by-level Pade exponentials of qjx_build_dimer: every level within 1e-11 of its
+    largest entry (the serving loop builds its operators this way)."""
+    import os_d_b200 as q
+
+    deep = 16 if N <= 200 else 12
+    H, Hd, L, Ug = q.build_dimer_gpu(N, 1.0, 0.5, 1.0, 1.5, 0.1, 1.0, deep)
+    H2, Hd2, L2, Uh = q.build_dimer(N, 1.0, 0.5, 1.0, 1.5, 0.1, 1.0, deep)
+    assert np.array_equal(H, H2) and np.array_equal(L, L2)
+    for b in range(2):
+        for lv in range(deep):
+            err = np.abs(Ug[b, lv] - Uh[b, lv]).max() / np.abs(Uh[b, lv]).max()
+            assert err < 1e-11, (b, lv, err)
