@@ -67,8 +67,11 @@ def parse():
     ap.add_argument("--batch-ensembles", type=int, default=32,
                     help="ensembles of configuration 4 in the batched measurement (of 256)")
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
-    ap.add_argument("--profile-target", default="plain", choices=["plain", "split", "fbasis", "lpn"],
-                    help="what --profile runs: one period of the plain or split form, or one f-basis period")
+    ap.add_argument("--profile-target", default="plain",
+                    choices=["plain", "split", "fbasis", "fbstages", "lpn", "purity", "rk", "batched"],
+                    help="what --profile runs: one period of the plain or split form, one f-basis period "
+                         "(cluster kernel, or the per-stage kernels), the Lyapunov pair case, ensemble purity, "
+                         "the RK propagator or the batched engine")
     return ap.parse_args()
 
 
@@ -375,6 +378,57 @@ def lpn_profile_case(local):
     print(json.dumps({"pairs": n // 2, "renormalisations": int(v["num_renorms"].sum()),
                       "bisection_steps_last": int(eng.lpn_last()["eps_iters"][n // 2:].sum())}), flush=True)
     eng.close()
+
+
+def profile_case(target, local):
+    """Short runs of the kernels outside the headline step, for ncu captures:
+    purity  -- dimer dim 201, 10^4 trajectories after one period: normalize, rho and purity kernels
+               (three ensemble-purity evaluations with the density matrix);
+    rk      -- the RK propagator (prop_id 1) on dim 101 (N = 100, g = 0.4, where 2000 RK4 steps per
+               period are stable), 2000 trajectories, one period;
+    batched -- the first 8 of configuration 4's ensembles (1000 trajectories each) in one batched
+               engine, one period."""
+    import os_d_b200 as q
+
+    if target == "purity":
+        M = model()
+        n, d = 10000, M["d"]
+        eng = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, max_dumps=1, device=local)
+        eng.set_states(start_states(n, d))
+        eng.init_thresholds()
+        eng.run_periods(1, is_obs=0)
+        for _ in range(3):
+            p, _ = eng.purity(want_rho=True)
+        print(json.dumps({"purity": p}), flush=True)
+        eng.close()
+    elif target == "rk":
+        N_ = 100
+        H, Hd, L, _ = q.build_dimer(N_, PRM["J"], PRM["U"], PRM["E"], PRM["A"], 0.4, PRM["omega"], 1)
+        n, d = 2000, N_ + 1
+        Lm = np.asarray(L).reshape(d, d)
+        Heff = H - 0.5j * (0.4 / N_) * (Lm.conj().T @ Lm)  # the dimer's rate g / N on L^+ L
+        eng = q.Engine.rk(Heff, Hd, L, [1.0], H + PRM["E"] * Hd, None, 2.0 * np.pi / PRM["omega"], n, E0=PRM["E"],
+                          A=PRM["A"], rk_ns=2000, seed=SEED, max_dumps=1, device=local)
+        eng.set_states(start_states(n, d))
+        eng.init_thresholds()
+        eng.run_periods(1, is_obs=1)
+        print(json.dumps({"rk_micro_steps": eng.stats()["micro_steps"]}), flush=True)
+        eng.close()
+    elif target == "batched":
+        ens = []
+        for i, (N_, E0, g) in enumerate(batch_draw(8)):
+            H, Hd, L, Ut = q.build_dimer(N_, PRM["J"], PRM["U"], E0, PRM["A"], g, PRM["omega"], DEEP)
+            ens.append(dict(U=Ut, L=L, g=[1.0], HE=H + E0 * Hd, n_traj=BATCH_TRAJ, T=2.0 * np.pi / PRM["omega"],
+                            seed=BATCH_SEED, tr_base=i * BATCH_TRAJ))
+        rows = max(x["U"].shape[-1] for x in ens)
+        B = q.Engine.batch(ens, deep=DEEP, device=local)
+        psi = np.zeros((BATCH_TRAJ * len(ens), rows), np.complex128)
+        psi[:, 0] = 1.0
+        B.set_states(psi)
+        B.init_thresholds()
+        B.run_periods(1, is_obs=1)
+        print(json.dumps({"batched_micro_steps": B.stats()["micro_steps"]}), flush=True)
+        B.close()
 
 
 # ---------------------------------------------------------------- production Lyapunov sweep (sampled)
@@ -707,9 +761,14 @@ def run_ours(args):
     if args.profile and args.profile_target == "lpn":
         lpn_profile_case(local)
         return
-    if args.profile and args.profile_target == "fbasis":
+    if args.profile and args.profile_target in ("fbasis", "fbstages"):
+        if args.profile_target == "fbstages":
+            os.environ["QJX_FB_PATH"] = "stages"
         args.warmup, args.steps, args.no_cpu_baseline = 0, 1, True
-        fbasis_bench(args, local)
+        print(json.dumps({"fbasis": fbasis_bench(args, local)["kernel"]}), flush=True)
+        return
+    if args.profile and args.profile_target in ("purity", "rk", "batched"):
+        profile_case(args.profile_target, local)
         return
     eng = new_engine(1 if args.profile and args.profile_target == "split" else 0)
     if args.profile:

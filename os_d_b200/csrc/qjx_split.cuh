@@ -108,6 +108,14 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
 // hi/lo planes of one (re, im) pair packed as two bf16 (re in the low half: lower address):
 // hi = bf16(f), lo = bf16(f - hi) with f the FP32 rounding of the FP64 value (f - hi is exact in
 // FP32; the FP32 rounding, 2^-24, is far below the 2^-17 the two planes resolve).
+// Two consecutive complex components (32 bytes, 32-byte aligned) in one 256-bit load.
+__device__ __forceinline__ void ld_pair(const double2 *p, double2 &a, double2 &b)
+{
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+                 : "l"(p));
+}
+
 __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo)
 {
     const float fr = __double2float_rn(v.x), fi = __double2float_rn(v.y);
@@ -404,34 +412,50 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
 
         const int agrp = (warp < 4) ? 0 : (warp >= 6 && warp < 10) ? 1 : (warp >= 10 && warp < 14) ? 2 : -1;
         if (agrp >= 0) {
-            // A producers: group p (4 warps, thread m = row m) handles the k-steps ks = p (mod 3), so
-            // three independent load-convert chains run in parallel; each thread issues its loads
-            // before waiting for the stage to drain
-            const int m = tid - (agrp == 0 ? 0 : (agrp == 1 ? 192 : 320));
-            const double2 *src = (s_src[m] >= 0) ? P.psi + s_src[m] : nullptr;
-            const int off = (m & 7) * 16 + (m >> 3) * 256;
+            // A producers: group p (4 warps) handles the k-steps ks = p (mod 3), so three
+            // independent load-convert chains run in parallel.  One warp-wide load covers 8 rows x
+            // one K-half (components 16 ks + 8 hh .. + 7, 128 contiguous bytes of each row): lane l
+            // takes row 8 rb + l / 4 and the component pair 2 (l % 4), 2 (l % 4) + 1, so every
+            // 32-byte sector is read whole by one lane, and a round's four plane stores are 128
+            // contiguous bytes each.  Round u of a warp is the (row block, half) pair 4 u + warp;
+            // all rounds of a k-step are loaded before the stage is waited for.  Rows past the
+            // tile's last trajectory are neither loaded nor stored: row i of an accumulator depends
+            // on row i of A only, and the epilogue reads live rows only.
+            const int gw = warp - (agrp == 0 ? 0 : (agrp == 1 ? 6 : 10));
+            const int r8 = lane >> 2, jq = lane & 3;
+            const int npairs = 2 * ((rows + 7) >> 3);
             for (int ks = agrp; ks < KS && ok; ks += 3) {
                 const uint32_t it = it0 + ks, q = it % S;
-                unsigned char *As = smem + q * stage_bytes + off;
-                for (int hh = 0; hh < 2; hh++) {  // K-halves: components 16 ks + 8 hh .. + 7
-                    double2 v[8];
+                unsigned char *As = smem + q * stage_bytes + 4 * lane;
+                for (int u0 = 0; u0 < 8; u0 += 4) {
+                    if (u0 > 0 && 4 * u0 + gw >= npairs) break;  // warp-uniform
+                    double2 v[4][2];
 #pragma unroll
-                    for (int i = 0; i < 8; i++) {
-                        const int k = 16 * ks + 8 * hh + i;
-                        v[i] = (src && k < d) ? src[k] : make_double2(0.0, 0.0);
+                    for (int u = 0; u < 4; u++) {
+                        const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
+                        const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
+                        const long long so = (pi < npairs && m < rows) ? s_src[m] : -1;
+                        v[u][0] = v[u][1] = make_double2(0.0, 0.0);
+                        if (so >= 0 && k < d) {
+                            ld_pair(P.psi + so + k, v[u][0], v[u][1]);  // k + 1 < MD: inside the row
+                            if (k + 1 >= d) v[u][1] = make_double2(0.0, 0.0);
+                        }
                     }
-                    if (hh == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
+                    if (u0 == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
                         ok = false;
-                    uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        split_pair(make_double2(v[2 * j].x, v[2 * j + 1].x), rh[j], rl[j]);
-                        split_pair(make_double2(v[2 * j].y, v[2 * j + 1].y), ih[j], il[j]);
+                    for (int u = 0; u < 4; u++) {
+                        const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
+                        if (pi >= npairs || m >= rows) continue;
+                        uint32_t rh, rl, ih, il;
+                        split_pair(make_double2(v[u][0].x, v[u][1].x), rh, rl);
+                        split_pair(make_double2(v[u][0].y, v[u][1].y), ih, il);
+                        unsigned char *dst = As + 256 * (pi >> 1) + 128 * (pi & 1);
+                        *reinterpret_cast<uint32_t *>(dst) = rh;
+                        *reinterpret_cast<uint32_t *>(dst + kABytes) = rl;
+                        *reinterpret_cast<uint32_t *>(dst + 2 * kABytes) = ih;
+                        *reinterpret_cast<uint32_t *>(dst + 3 * kABytes) = il;
                     }
-                    *reinterpret_cast<uint4 *>(As + 128 * hh) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-                    *reinterpret_cast<uint4 *>(As + kABytes + 128 * hh) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-                    *reinterpret_cast<uint4 *>(As + 2 * kABytes + 128 * hh) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-                    *reinterpret_cast<uint4 *>(As + 3 * kABytes + 128 * hh) = make_uint4(il[0], il[1], il[2], il[3]);
                 }
                 fence_proxy_async();
                 mbar_arrive(&fullA[q]);
