@@ -647,6 +647,27 @@ def split_form(args, q, new_engine, timed_windows, snap, value, ens_plain, x_pla
                     "same_path_fraction": float(same.mean()),
                     "max_abs_diff_on_same_paths": float(np.abs(xs - xp)[same].max()) if same.any() else None})
     eng_s.close()
+    # speed against accuracy: the recheck band is the knob (off, the default 1e-5, wider; a band
+    # of 1 rechecks every norm test, which makes the split form bit-identical to the plain one)
+    HC = 2
+    eng_plain.restore(snap)
+    eng_plain.run_periods(HC, is_obs=1, dump_at=list(range(1, HC + 1)), dump_base=base)
+    ms_plain_hc = eng_plain.stats()["last_call_ms"]
+    xp_hc = N_BOSONS - 2.0 * eng_plain.observables(base, HC)["mean"]
+    curve = []
+    for band in (-1.0, 1e-5, 1e-4, 1e-3, 1e-2, 1.0):
+        e = new_engine(1, split_recheck=band)
+        e.restore(snap)
+        r0 = e.stats()["rechecks"]
+        e.run_periods(HC, is_obs=1, dump_at=list(range(1, HC + 1)), dump_base=base)
+        ms_b = e.stats()["last_call_ms"]
+        xs_hc = N_BOSONS - 2.0 * e.observables(base, HC)["mean"]
+        curve.append({"split_recheck": band if band > 0 else "off",
+                      "speedup_vs_plain": ms_plain_hc / ms_b,
+                      "rechecks_per_traj_period": (e.stats()["rechecks"] - r0) / (n * HC),
+                      "same_path_fraction": [float(np.mean(np.abs(xs_hc[h] - xp_hc[h]) < 1e-3)) for h in range(HC)],
+                      "n1_minus_n2_abs_diff": [float(abs(xs_hc[h].mean() - xp_hc[h].mean())) for h in range(HC)]})
+        e.close()
     return {
         "metric": METRIC, "value": v_s, "unit": METRIC, "ms_per_step": ms_s / args.steps,
         "speedup_vs_plain": v_s / value,
@@ -655,6 +676,7 @@ def split_form(args, q, new_engine, timed_windows, snap, value, ens_plain, x_pla
         "n1_minus_n2_stderr_per_step": [b[1] for b in ens_plain],
         "same_jump_count_fraction_after_window": float(np.mean(per_period["split_jumps"] == per_period["plain_jumps"])),
         "horizon": hor,
+        "recheck_curve": {"periods": HC, "window_start": "the timed window's checkpoint", "points": curve},
         "roofline": {"bound": "tensor", "kernel": "qjx::split_step_kernel",
                      "achieved": exec_flops / kern_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
                      "frac": exec_flops / kern_s / 1e12 / bf16_peak,
@@ -712,9 +734,10 @@ def run_ours(args):
     psi0 = start_states(n, d)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
-    def new_engine(precision):
+    def new_engine(precision, split_recheck=0.0):
         e = q.Engine(M["U"], M["L"], [1.0], M["HE"], M["R"], M["T"], n, seed=SEED, record=0, rec_cap=16,
-                     keep_adr=0, max_dumps=steps_total + P + 2, device=local, tr_base=rank * n, precision=precision)
+                     keep_adr=0, max_dumps=steps_total + P + 2, device=local, tr_base=rank * n, precision=precision,
+                     split_recheck=split_recheck)
         e.set_states(psi0)
         e.init_thresholds()
         e.reset_times()
