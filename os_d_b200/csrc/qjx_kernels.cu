@@ -667,6 +667,7 @@ __device__ __forceinline__ bool tile_dmma(const double2 *mat, double2 *Bt, doubl
                 bulk_g2s(Us + q * KB * MD, mat + (size_t)sn * KB * MD, (uint32_t)(kn * MD * 16), &bar[q]);
             }
         }
+        __syncwarp();  // lanes 1-31 wait here, not spinning on the next slab beside the issuing lane
     }
     __syncthreads();
     // stage: thread (g, t) of row block rb holds rows 8 rb + g, columns 8 cb + 2t, 8 cb + 2t + 1
@@ -892,6 +893,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(const Params P, int s
                 bulk_g2s(Us + q * KB * MD, mat + (size_t)q * KB * MD, (uint32_t)(kcq * MD * 16), &bar[q]);
             }
         }
+        __syncwarp();  // warp 0's other lanes wait for the copies to be issued instead of spinning on them
         const long long t1 = clock64();
         bool ok;
         if (ncb == 1)

@@ -29,9 +29,9 @@
 //
 // Per tile (one matrix, up to 128 trajectories of one bucket) a ring of S stages, one k-step of
 // A and B planes each:
-//   warps 0-3, 6-9, 10-13   three producer groups, one thread per trajectory row; group p
-//               converts the k-steps ks = p (mod 3): FP64 state -> bf16 planes of A (generic
-//               stores, then fence.proxy.async and an arrive on fullA)
+//   warps 0-3, 6-9, 10-13   three producer groups; group p converts the k-steps ks = p (mod 3):
+//               FP64 state -> bf16 planes of A (a warp-wide 256-bit load covers 8 rows x 128 bytes;
+//               generic stores, then fence.proxy.async and an arrive on fullA)
 //   warp 4      one thread issues the bulk copy of the B planes (complete_tx on fullB)
 //   warp 5      one thread issues the 12 tcgen05.mma of a k-step and commits them to empty[stage]
 //   warps 14-15 load the tile's trajectory records meanwhile
@@ -105,17 +105,19 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
     v[7] = __uint_as_float(r7);
 }
 
-// hi/lo planes of one (re, im) pair packed as two bf16 (re in the low half: lower address):
-// hi = bf16(f), lo = bf16(f - hi) with f the FP32 rounding of the FP64 value (f - hi is exact in
-// FP32; the FP32 rounding, 2^-24, is far below the 2^-17 the two planes resolve).
-// Two consecutive complex components (32 bytes, 32-byte aligned) in one 256-bit load.
+// Two consecutive complex components (32 bytes, 32-byte aligned) in one 256-bit load, cached in L2
+// only: the state rows stream through once, and in L1 they would evict the small per-ensemble
+// tables that every trajectory's epilogue reads.
 __device__ __forceinline__ void ld_pair(const double2 *p, double2 &a, double2 &b)
 {
-    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+    asm volatile("ld.global.cg.v4.f64 {%0, %1, %2, %3}, [%4];"
                  : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
                  : "l"(p));
 }
 
+// hi/lo planes of one (re, im) pair packed as two bf16 (re in the low half: lower address):
+// hi = bf16(f), lo = bf16(f - hi) with f the FP32 rounding of the FP64 value (f - hi is exact in
+// FP32; the FP32 rounding, 2^-24, is far below the 2^-17 the two planes resolve).
 __device__ __forceinline__ void split_pair(double2 v, uint32_t &hi, uint32_t &lo)
 {
     const float fr = __double2float_rn(v.x), fi = __double2float_rn(v.y);
@@ -434,12 +436,12 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                     for (int u = 0; u < 4; u++) {
                         const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
                         const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
-                        const long long so = (pi < npairs && m < rows) ? s_src[m] : -1;
-                        v[u][0] = v[u][1] = make_double2(0.0, 0.0);
-                        if (so >= 0 && k < d) {
-                            ld_pair(P.psi + so + k, v[u][0], v[u][1]);  // k + 1 < MD: inside the row
-                            if (k + 1 >= d) v[u][1] = make_double2(0.0, 0.0);
-                        }
+                        // every lane of a live round loads (a lane without data reads component 0
+                        // of row 0) and nothing touches v before the stage wait, so the four loads
+                        // are in flight together: a select or a write on a load's destination
+                        // registers would wait for that load.  k + 1 < MD: inside the row.
+                        const long long so = (m < rows && k < d) ? s_src[m] + k : 0;
+                        if (pi < npairs) ld_pair(P.psi + so, v[u][0], v[u][1]);
                     }
                     if (u0 == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
                         ok = false;
@@ -447,9 +449,13 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                     for (int u = 0; u < 4; u++) {
                         const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
                         if (pi >= npairs || m >= rows) continue;
+                        // components from d on are row padding (or were not loaded): zeros
+                        const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
+                        const double2 z = make_double2(0.0, 0.0);
+                        const double2 a = (k < d) ? v[u][0] : z, b = (k + 1 < d) ? v[u][1] : z;
                         uint32_t rh, rl, ih, il;
-                        split_pair(make_double2(v[u][0].x, v[u][1].x), rh, rl);
-                        split_pair(make_double2(v[u][0].y, v[u][1].y), ih, il);
+                        split_pair(make_double2(a.x, b.x), rh, rl);
+                        split_pair(make_double2(a.y, b.y), ih, il);
                         unsigned char *dst = As + 256 * (pi >> 1) + 128 * (pi & 1);
                         *reinterpret_cast<uint32_t *>(dst) = rh;
                         *reinterpret_cast<uint32_t *>(dst + kABytes) = rl;
@@ -513,6 +519,9 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             // warps 14-15: the tile's state records, loaded while the MMAs run
             for (int m = tid - 448; m < rows; m += 64) load_state(&s_st[m], &P.st[s_tr[m]]);
         }
+        // lanes 1-31 of the B-producer and MMA warps park here until their lane 0 is done: spinning on
+        // the accumulator barrier instead would take the warp's issue slots from the lane issuing
+        __syncwarp();
         kit += (uint32_t)KS;
         if (!ok) atomicExch(&s_fail, 1);
         // accumulator complete (every thread waits on the commit); the ring is free afterwards
