@@ -173,6 +173,8 @@ struct Params {
     // prefix; written by the last CTA of a micro-step (or plan_kernel after a host call)
     int *plan;
     unsigned int *plan_sync;          // [1] CTAs finished in the current micro-step
+    unsigned int *gen;                // [1] split form: plans made (the grid barrier of a multi-step launch)
+    int *sdone;                       // [1] split form: micro-steps the last launch ran
 };
 
 // Dimension, split-level steps and jump rates of a trajectory's ensemble.

@@ -18,6 +18,7 @@
 
 namespace qjx {
 cudaError_t launch_step(const Params &P, int s, int grid, cudaStream_t st);
+cudaError_t launch_split_steps(const Params &P, int s0, int nsteps, int grid, cudaStream_t st);
 int pick_layout(int d, int *rows_per_block);
 cudaError_t launch_dmma_peak(double *out, int blocks, int iters, cudaStream_t st);
 size_t step_smem_bytes(int MD, int nc, int kb);
@@ -504,8 +505,12 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
         // next to the input and product vectors
         P.rcnt = (int *)dalloc(h, 3 * sizeof(int));
         P.rlist = (int *)dalloc(h, (size_t)2 * n * sizeof(int));
-        if (!P.e_mds || !P.e_ks || !P.g_uoff || !P.splan || !P.rcnt || !P.rlist)
+        P.gen = (unsigned int *)dalloc(h, sizeof(unsigned int));
+        P.sdone = (int *)dalloc(h, sizeof(int));
+        if (!P.e_mds || !P.e_ks || !P.g_uoff || !P.splan || !P.rcnt || !P.rlist || !P.gen || !P.sdone)
             return bail(QJX_ERR_OOM);
+        cudaMemset(P.gen, 0, sizeof(unsigned int));
+        cudaMemset(P.sdone, 0, sizeof(int));
         P.recheck_tol = c.split_recheck == 0.0 ? 1e-5 : (c.split_recheck < 0.0 ? 0.0 : c.split_recheck);
         const size_t ring = (size_t)P.sstages * split_stage_bytes(P.MDs);
         const size_t vec = (size_t)(2 * MD + 2) * sizeof(double2);
@@ -722,21 +727,27 @@ static qjx_status drain_records(qjx_engine *h)
 static qjx_status run_until_idle(qjx_engine *h)
 {
     Params &P = h->P;
+    // plain form: CUDA graphs of 6 micro-steps; split form: one cooperative launch runs up to
+    // 6 x batch micro-steps with grid barriers between them (the buffers rotate with period 6)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    for (int s = 0; s < 6; s++) {
-        cudaError_t e = launch_step(P, s, h->grid, h->stream);
-        if (e != cudaSuccess) {
-            cudaStreamEndCapture(h->stream, &graph);
-            if (graph) cudaGraphDestroy(graph);
-            return cuda_fail(h, e, "launch_step");
+    if (!P.split) {
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < 6; s++) {
+            cudaError_t e = launch_step(P, s, h->grid, h->stream);
+            if (e != cudaSuccess) {
+                cudaStreamEndCapture(h->stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                return cuda_fail(h, e, "launch_step");
+            }
         }
+        CK(cudaStreamEndCapture(h->stream, &graph));
+        cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return cuda_fail(h, ie, "cudaGraphInstantiate");
     }
-    CK(cudaStreamEndCapture(h->stream, &graph));
-    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ie != cudaSuccess) return cuda_fail(h, ie, "cudaGraphInstantiate");
+    int s0 = 0;  // split form: index of the next micro-step
+    int64_t nlaunch = 0;
 
     qjx_status rs = QJX_OK;
     int batch = 1;
@@ -749,27 +760,48 @@ static qjx_status run_until_idle(qjx_engine *h)
     cudaEventRecord(h->ev0, h->stream);
     while (true) {
         cudaEventRecord(h->eb0, h->stream);
-        for (int b = 0; b < batch; b++) {
-            cudaError_t e = cudaGraphLaunch(exec, h->stream);
+        if (P.split) {
+            cudaError_t e = launch_split_steps(P, s0, 6 * batch, h->grid, h->stream);
             if (e != cudaSuccess) {
-                rs = cuda_fail(h, e, "cudaGraphLaunch");
+                rs = cuda_fail(h, e, "launch_split_steps");
                 break;
             }
+            nlaunch += 1;
+        } else {
+            for (int b = 0; b < batch; b++) {
+                cudaError_t e = cudaGraphLaunch(exec, h->stream);
+                if (e != cudaSuccess) {
+                    rs = cuda_fail(h, e, "cudaGraphLaunch");
+                    break;
+                }
+            }
+            if (rs != QJX_OK) break;
+            steps += 6 * batch;
+            nlaunch += 6 * batch;
         }
-        if (rs != QJX_OK) break;
-        steps += 6 * batch;
         cudaEventRecord(h->eb1, h->stream);
-        // the next micro-step's bucket sizes (split form, bucket log) or the plain kernel's plan
-        // total, which the last micro-step computed
-        const bool all_counts = P.split || bucket_log;
-        if (all_counts) cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
-        else cudaMemcpyAsync(h->h_cnt, P.plan + P.G, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
-        if (P.split) cudaMemcpyAsync(h->h_ctrl + 8, P.rcnt, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        // plain form: the next micro-step's plan total (or all bucket sizes for the bucket log),
+        // which the last micro-step computed; split form: the micro-steps run, the recheck counts
+        // and the next step's tiles
+        const bool all_counts = !P.split && bucket_log;
+        if (P.split) {
+            cudaMemcpyAsync(h->h_ctrl + 8, P.rcnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+            cudaMemcpyAsync(h->h_ctrl + 11, P.sdone, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+            cudaMemcpyAsync(h->h_ctrl + 12, P.splan + 1 + P.G, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        } else if (all_counts) {
+            cudaMemcpyAsync(h->h_cnt, P.cnt, sizeof(int) * P.G, cudaMemcpyDeviceToHost, h->stream);
+        } else {
+            cudaMemcpyAsync(h->h_cnt, P.plan + P.G, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        }
         cudaMemcpyAsync(h->h_ctrl, P.ctrl, sizeof(int) * 8, cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
             rs = cuda_fail(h, e, "micro-step batch");
             break;
+        }
+        if (P.split) {
+            steps += h->h_ctrl[11];
+            s0 = (s0 + h->h_ctrl[11]) % 6;
         }
         float bms = 0.f;
         cudaEventElapsedTime(&bms, h->eb0, h->eb1);
@@ -779,8 +811,9 @@ static qjx_status run_until_idle(qjx_engine *h)
         long long active = all_counts ? 0 : h->h_cnt[0];
         if (all_counts)
             for (int g = 0; g < P.G; g++) active += h->h_cnt[g];
-        if (P.split) active += h->h_ctrl[8];  // trajectories waiting for an FP64 recheck
-        if (bucket_log) {
+        // split form: tiles of the next step and trajectories waiting for an FP64 recheck
+        if (P.split) active = (long long)h->h_ctrl[12] + h->h_ctrl[8 + s0 % 3];
+        if (bucket_log && all_counts) {
             for (int g = 0; g < P.G; g++) fprintf(bucket_log, g ? " %d" : "%d", h->h_cnt[g]);
             fprintf(bucket_log, "\n");
         }
@@ -797,6 +830,7 @@ static qjx_status run_until_idle(qjx_engine *h)
                     rs = cuda_fail(h, le, "launch_schedule");
                     break;
                 }
+                s0 = 0;  // the schedule wrote step 0's buckets
                 continue;
             }
             break;
@@ -811,13 +845,13 @@ static qjx_status run_until_idle(qjx_engine *h)
     h->stats.kernel_ms += ms;
     h->stats.last_call_ms = ms;
     h->stats.micro_steps += steps;
-    h->stats.launches += steps;
+    h->stats.launches += nlaunch;
     long long work1[3] = {0, 0, 0};
     cudaMemcpy(work1, P.work, 3 * sizeof(long long), cudaMemcpyDeviceToHost);
     h->stats.matvecs += work1[0] - work0[0];
     h->stats.mma_tiles += work1[1] - work0[1];
     h->stats.rechecks += work1[2] - work0[2];
-    cudaGraphExecDestroy(exec);
+    if (exec) cudaGraphExecDestroy(exec);
     return rs;
 }
 

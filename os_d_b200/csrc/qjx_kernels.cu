@@ -1405,17 +1405,37 @@ size_t split_static_smem()
     return a.sharedSizeBytes;
 }
 
-cudaError_t launch_split_step(const Params &P, int s, int grid, cudaStream_t st)
+static cudaError_t split_smem_attr(size_t smem)
 {
-    const size_t smem = split_smem_bytes(P.MDs, P.MD, P.sstages);
     static int attr_bytes = 0;
     if (attr_bytes < (int)smem) {
         cudaError_t e = cudaFuncSetAttribute(split_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_bytes = (int)smem;
     }
-    split_step_kernel<<<grid, kThreads, smem, st>>>(P, s);
+    return cudaSuccess;
+}
+
+cudaError_t launch_split_step(const Params &P, int s, int grid, cudaStream_t st)
+{
+    const size_t smem = split_smem_bytes(P.MDs, P.MD, P.sstages);
+    cudaError_t e = split_smem_attr(smem);
+    if (e != cudaSuccess) return e;
+    split_step_kernel<<<grid, kThreads, smem, st>>>(P, s, 1);
     return cudaGetLastError();
+}
+
+// Micro-steps s0 .. s0 + nsteps - 1 in one launch (fewer when the work runs out first; the
+// count is left in P.sdone): a cooperative launch, so that every CTA is resident for the grid
+// barriers between the steps.
+cudaError_t launch_split_steps(const Params &P, int s0, int nsteps, int grid, cudaStream_t st)
+{
+    const size_t smem = split_smem_bytes(P.MDs, P.MD, P.sstages);
+    cudaError_t e = split_smem_attr(smem);
+    if (e != cudaSuccess) return e;
+    Params Pc = P;
+    void *args[] = {&Pc, &s0, &nsteps};
+    return cudaLaunchCooperativeKernel((const void *)split_step_kernel, dim3(grid), dim3(kThreads), args, smem, st);
 }
 
 }  // namespace qjx

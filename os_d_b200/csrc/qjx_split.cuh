@@ -39,7 +39,10 @@
 // the warps that own their TMEM lane quarters, and every warp runs its trajectories through the
 // epilogue and appends them to their next buckets.  A batched engine's ensembles each have their
 // own padded rows and k-steps; the tile plan of the next micro-step (rows per tile, first tile of
-// every bucket) is made by the last CTA to finish one.
+// every bucket) is made by the last CTA to finish one.  One cooperative launch runs a batch of
+// micro-steps: between two of them every CTA waits at a grid barrier (an arrival counter, and a
+// generation number the planning CTA releases), and the operand ring, mbarriers and tensor
+// memory stay set up across them.
 
 constexpr int kAPlanes = 4;                  // A and B planes: Re hi, Re lo, Im hi, Im lo
 constexpr int kTileM = 128;                  // MMA M = TMEM lanes (a tile holds up to 128 trajectories)
@@ -47,6 +50,18 @@ constexpr int kMaxSStages = kMaxSplitStages;  // operand ring depth (runtime: th
 constexpr int kABytes = kTileM * 32;         // one plane of one k-step of A: 128 rows x 16 bf16
 constexpr int kTmemCols = 512;
 constexpr long long kSplitWait = 1ll << 20;  // bounded mbarrier polls (normal waits end within microseconds)
+constexpr long long kGridWait = 1ll << 24;   // bounded polls of the grid barrier (a micro-step is ~50 us)
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 __device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t saddr)
 {
@@ -314,7 +329,7 @@ size_t split_smem_bytes(int MDs, int MD, int stages)
     return ring > epi ? ring : epi;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P, int s)
+__global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P, int s0, int nsteps)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int S = P.sstages;
@@ -325,6 +340,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     __shared__ long long s_src[kTileM];
     __shared__ __align__(16) TrajState s_st[kTileM];
     __shared__ int s_fail, s_last;
+    __shared__ unsigned int s_gen;
     __shared__ int w_g2[kThreads / 32][kTileM / (kThreads / 32)];  // per warp: its trajectories' next buckets
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -334,20 +350,6 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     const int RP = split_epi_bytes(P.MDs, 64) <= dyn ? 64 : 32;
     double2 *wcol = reinterpret_cast<double2 *>(smem + split_epi_f32_bytes(P.MDs, RP)) + (size_t)warp * (P.MDs + 1);
     const int G = P.G, n = P.n;
-    const int *cnt_cur = P.cnt + (s % 3) * G;
-    int *cnt_next = P.cnt + ((s + 1) % 3) * G;
-    const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
-    int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
-    const int *rlist_cur = P.rlist + (size_t)(s & 1) * P.n;
-    int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
-    int *rcnt_next = P.rcnt + (s + 1) % 3;
-    const int Rtot = P.rcnt[s % 3];  // FP64 rechecks of this micro-step
-    const int R = P.splan[0], T = P.splan[1 + G];  // this step's plan (rows per tile, tiles)
-
-    if (blockIdx.x == 0) {
-        for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
-        if (tid == 0) P.rcnt[(s + 2) % 3] = 0;
-    }
     if (warp == 0) {
         if (lane == 0) {
             for (int q = 0; q < S; q++) {
@@ -377,6 +379,26 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     bool ok = true;
     long long tr_setup = 0, tr_mma = 0, tr_stage = 0, tr_epi = 0;
     const long long t_begin = clock64();
+    int steps_done = 0;
+
+    // micro-steps s0 .. s0 + nsteps - 1 (one, when launched per step); between two steps of one
+    // launch every CTA waits at a grid barrier whose last arrival plans the next step
+    for (int si = 0; si < nsteps; si++) {
+    const int s = s0 + si;
+    const int *cnt_cur = P.cnt + (s % 3) * G;
+    int *cnt_next = P.cnt + ((s + 1) % 3) * G;
+    const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
+    int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
+    const int *rlist_cur = P.rlist + (size_t)(s & 1) * P.n;
+    int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
+    int *rcnt_next = P.rcnt + (s + 1) % 3;
+    const int Rtot = __ldcg(P.rcnt + s % 3);  // FP64 rechecks of this micro-step
+    const int R = __ldcg(P.splan), T = __ldcg(P.splan + 1 + G);  // this step's plan (rows per tile, tiles)
+    if (T + Rtot == 0) break;  // nothing left in this call (every CTA reads the same plan)
+    if (blockIdx.x == 0) {
+        for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
+        if (tid == 0) P.rcnt[(s + 2) % 3] = 0;
+    }
 
     for (int t = blockIdx.x; t < T + Rtot && ok; t += gridDim.x) {
         if (t >= T) {  // an FP64 recheck (the CTAs past the split tiles take these first)
@@ -589,6 +611,39 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         tr_epi += t3 - t2;
     }
 
+    steps_done++;
+    if (!ok && tid == 0) atomicAdd(&P.ctrl[4], 1);  // every CTA stops after the barrier below
+    // the last CTA to finish plans the next micro-step from the buckets all CTAs filled; with a
+    // next step in this launch the others wait for that plan (bounded), then read it
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        s_gen = ld_acquire_u32(P.gen);
+        s_last = atomicAdd(P.plan_sync, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    const bool more = si + 1 < nsteps;
+    if (s_last) {
+        __threadfence();
+        split_plan(P, cnt_next, __ldcg(rcnt_next), gridDim.x);
+        if (tid == 0) {
+            *P.plan_sync = 0u;
+            __threadfence();
+            st_release_u32(P.gen, s_gen + 1u);
+        }
+    } else if (more && tid == 0) {
+        long long i = 0;
+        while (ld_acquire_u32(P.gen) == s_gen && i < kGridWait) i++;
+        if (i == kGridWait) {
+            atomicAdd(&P.ctrl[4], 1);
+            report_error(P, -1, ERR_TIMEOUT);
+        }
+    }
+    __syncthreads();
+    __threadfence();
+    if (!more || !ok || __ldcg(P.ctrl + 4) != 0) break;
+    }  // micro-steps
+
     if (!ok) {
         // give the copies and MMAs still in flight time to land before the memory goes away
         if (warp == 5 && lane == 0) {
@@ -605,10 +660,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                 mbar_wait_bounded(&rbar[q], 1u, 1024);
             }
         }
-        if (tid == 0) {
-            atomicAdd(&P.ctrl[4], 1);
-            report_error(P, -1, ERR_TIMEOUT);
-        }
+        if (tid == 0) report_error(P, -1, ERR_TIMEOUT);
     }
     tc_fence_before();
     __syncthreads();
@@ -630,16 +682,5 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         tr[6] += tr_stage;
         tr[7] += work;
     }
-    // the last CTA to finish plans the next micro-step from the buckets all CTAs filled
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        s_last = atomicAdd(P.plan_sync, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        split_plan(P, cnt_next, __ldcg(rcnt_next), gridDim.x);
-        if (tid == 0) *P.plan_sync = 0u;
-    }
+    if (blockIdx.x == 0 && tid == 0) *P.sdone = steps_done;
 }
