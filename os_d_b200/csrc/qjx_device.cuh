@@ -174,7 +174,7 @@ struct Params {
     int *plan;
     unsigned int *plan_sync;          // [1] CTAs finished in the current micro-step
     unsigned int *gen;                // [1] split form: plans made (the grid barrier of a multi-step launch)
-    int *sdone;                       // [1] split form: micro-steps the last launch ran
+    int *sdone;                       // [1] split form: micro-steps run since the host last cleared it
 };
 
 // Dimension, split-level steps and jump rates of a trajectory's ensemble.

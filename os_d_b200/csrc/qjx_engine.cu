@@ -68,7 +68,9 @@ struct qjx_engine {
     double *d_purity = nullptr;
     // host mirrors
     int *h_cnt = nullptr;   // pinned [G]
-    int *h_ctrl = nullptr;  // pinned [16]: the control words [0, 8), the split form's recheck count [8]
+    int *h_ctrl = nullptr;  // pinned [16]: the control words [0, 8); split form: recheck counts [8, 11),
+                            // micro-steps run [11], tiles of the next step [12]
+    bool split_coop = true;  // split form: batches of micro-steps as one cooperative launch
     std::vector<std::vector<double>> jt, jn, je;
     std::vector<std::vector<int>> jtype;
     qjx_stats stats{};
@@ -338,6 +340,9 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
     h->grid = sms > 0 ? sms : 148;
+    // QJX_SPLIT_COOP=0: run the split form's micro-steps as one launch each (the path taken when a
+    // cooperative launch cannot make every CTA resident)
+    if (const char *v = getenv("QJX_SPLIT_COOP")) h->split_coop = v[0] != '0';
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(QJX_ERR_CUDA);
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
@@ -761,12 +766,24 @@ static qjx_status run_until_idle(qjx_engine *h)
     while (true) {
         cudaEventRecord(h->eb0, h->stream);
         if (P.split) {
-            cudaError_t e = launch_split_steps(P, s0, 6 * batch, h->grid, h->stream);
+            cudaMemsetAsync(P.sdone, 0, sizeof(int), h->stream);
+            cudaError_t e = h->split_coop ? launch_split_steps(P, s0, 6 * batch, h->grid, h->stream)
+                                          : cudaErrorCooperativeLaunchTooLarge;
+            if (e == cudaErrorCooperativeLaunchTooLarge) {
+                // not every CTA can be resident (another context holds SMs): the same micro-steps
+                // as one launch each (an empty step returns at once)
+                cudaGetLastError();
+                h->split_coop = false;
+                e = cudaSuccess;
+                for (int k = 0; k < 6 * batch && e == cudaSuccess; k++) e = launch_step(P, s0 + k, h->grid, h->stream);
+                nlaunch += 6 * batch;
+            } else {
+                nlaunch += 1;
+            }
             if (e != cudaSuccess) {
                 rs = cuda_fail(h, e, "launch_split_steps");
                 break;
             }
-            nlaunch += 1;
         } else {
             for (int b = 0; b < batch; b++) {
                 cudaError_t e = cudaGraphLaunch(exec, h->stream);

@@ -682,5 +682,5 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         tr[6] += tr_stage;
         tr[7] += work;
     }
-    if (blockIdx.x == 0 && tid == 0) *P.sdone = steps_done;
+    if (blockIdx.x == 0 && tid == 0 && steps_done) atomicAdd(P.sdone, steps_done);
 }

@@ -97,3 +97,20 @@ def test_autotuner_picks_and_caches_a_fitting_shape(tmp_path, monkeypatch):
         psi_r, jc_r, _ = run(P, 256, 2, precision)  # the rule
         monkeypatch.setenv("QJX_TILE_CACHE", str(tmp_path / "tiles.txt"))
         assert np.array_equal(psi_c, psi_r) and np.array_equal(jc_c, jc_r)
+
+
+def test_split_per_step_launches_equal_the_multi_step_launch(monkeypatch):
+    """The split form runs a batch of micro-steps as one cooperative launch with grid barriers
+    between them; when that launch cannot make every CTA resident it falls back to one launch per
+    micro-step (forced here with QJX_SPLIT_COOP=0). Both give the same trajectories, jump records
+    and observables, bit for bit, with jumps and FP64 rechecks in the run."""
+    P = dimer_problem(40, g=0.3)
+    a = run(P, 300, 3, 1, want_stats=True)
+    monkeypatch.setenv("QJX_SPLIT_COOP", "0")
+    b = run(P, 300, 3, 1, want_stats=True)
+    assert a[1].sum() > 0 and a[3]["rechecks"] > 0
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for k in ("norm", "mean", "energy"):
+        assert np.array_equal(a[2][k], b[2][k]), k
+    assert a[3]["micro_steps"] == b[3]["micro_steps"]
+    assert b[3]["launches"] > a[3]["launches"]
