@@ -217,6 +217,16 @@ __device__ bool recheck_column(const Params &P, int tr, unsigned char *smem, Tra
 // blockDim.x a multiple of 32): rows per tile R, the smallest multiple of 8 (at least P.min_rows,
 // at most 128) whose tiles fit one wave of `grid` CTAs next to the rechecks, so that trajectories
 // and their epilogues spread over all SMs; then the first tile of every group.
+// Rows per tile of a bucket when the plan's rows per tile is R: the jump-operator and observable
+// buckets take about 5/8 of R (their epilogues renormalise, draw and reduce: a tile of them took
+// 1.3x as long as a matrix bucket's tile of as many rows, and a micro-step waits for its slowest
+// tile), the (branch, level) buckets R.
+__device__ __forceinline__ bool heavy_group(const Params &P, int g)
+{
+    return g - P.e_g0[P.g_ens[g]] >= P.nb * P.deep;
+}
+__device__ __forceinline__ int group_rows(int R, bool heavy) { return heavy ? max(8, (R * 5 / 8) & ~7) : R; }
+
 __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
 {
     __shared__ int w_t[32][17];
@@ -228,8 +238,12 @@ __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
     for (int j = 0; j < 16; j++) part[j] = 0;
     for (int g = tid; g < G; g += nt) {
         const int m = __ldcg(cnt + g);
+        const bool hv = heavy_group(P, g);
 #pragma unroll
-        for (int j = 0; j < 16; j++) part[j] += (m + 8 * j + 7) / (8 * j + 8);
+        for (int j = 0; j < 16; j++) {
+            const int r = group_rows(8 * j + 8, hv);
+            part[j] += (m + r - 1) / r;
+        }
     }
 #pragma unroll
     for (int j = 0; j < 16; j++) {
@@ -256,7 +270,10 @@ __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
     // exclusive scan of the tiles per group over the block: each thread a contiguous range
     const int per = (G + nt - 1) / nt, g0 = min(G, tid * per), g1 = min(G, g0 + per);
     int c = 0;
-    for (int g = g0; g < g1; g++) c += (__ldcg(cnt + g) + R - 1) / R;
+    for (int g = g0; g < g1; g++) {
+        const int r = group_rows(R, heavy_group(P, g));
+        c += (__ldcg(cnt + g) + r - 1) / r;
+    }
     int inc = c;
     for (int off = 1; off < 32; off <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, inc, off);
@@ -276,7 +293,8 @@ __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
     int acc = inc - c + (warp ? w_s[warp - 1] : 0);
     for (int g = g0; g < g1; g++) {
         P.splan[1 + g] = acc;
-        acc += (__ldcg(cnt + g) + R - 1) / R;
+        const int r = group_rows(R, heavy_group(P, g));
+        acc += (__ldcg(cnt + g) + r - 1) / r;
     }
     if (tid == nt - 1) {
         P.splan[1 + G] = acc;
@@ -414,8 +432,9 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         const int g = split_tile_group(P, t, lane);  // every warp finds it (warp-uniform)
         const int e = P.g_ens[g];
         const int d = P.e_d[e], MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
-        const int base = (t - __ldcg(P.splan + 1 + g)) * R;
-        const int rows = min(R, __ldcg(cnt_cur + g) - base);
+        const int Rg = group_rows(R, g - P.e_g0[e] >= P.nb * P.deep);
+        const int base = (t - __ldcg(P.splan + 1 + g)) * Rg;
+        const int rows = min(Rg, __ldcg(cnt_cur + g) - base);
         if (tid < kTileM) {
             if (tid < rows) {
                 const int tr = list_cur[P.g_loff[g] + base + tid];
