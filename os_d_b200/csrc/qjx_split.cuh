@@ -98,26 +98,28 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 8 consecutive FP32 accumulator columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
+// 8 consecutive FP32 accumulator columns of this thread's TMEM lane at each of two addresses (the
+// Re and Im accumulators), both loads in flight before the one wait.
+__device__ __forceinline__ void tmem_ld8x2(uint32_t ta, uint32_t tb, float *va, float *vb)
 {
-    uint32_t r0, r1, r2, r3, r4, r5, r6, r7;
+    uint32_t a[8], b[8];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4), "=r"(r5), "=r"(r6), "=r"(r7)
-                 : "r"(taddr));
+                 : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7])
+                 : "r"(ta));
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3]), "=r"(b[4]), "=r"(b[5]), "=r"(b[6]), "=r"(b[7])
+                 : "r"(tb));
     // the registers are valid after wait::ld; tying them to the wait keeps every use behind it
     asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3), "+r"(r4), "+r"(r5), "+r"(r6), "+r"(r7)
+                 : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7]),
+                   "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7])
                  :
                  : "memory");
-    v[0] = __uint_as_float(r0);
-    v[1] = __uint_as_float(r1);
-    v[2] = __uint_as_float(r2);
-    v[3] = __uint_as_float(r3);
-    v[4] = __uint_as_float(r4);
-    v[5] = __uint_as_float(r5);
-    v[6] = __uint_as_float(r6);
-    v[7] = __uint_as_float(r7);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        va[i] = __uint_as_float(a[i]);
+        vb[i] = __uint_as_float(b[i]);
+    }
 }
 
 // Two consecutive complex components (32 bytes, 32-byte aligned) in one 256-bit load, cached in L2
@@ -584,8 +586,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
                 float *dst = sacc + (size_t)(32 * q - p0 + lane) * SR;
                 for (int r0 = 8 * (warp >> 2); r0 < MDs; r0 += 32) {  // 8 output rows at a time
                     float vr[8], vi[8];
-                    tmem_ld8(lanes + (uint32_t)r0, vr);
-                    tmem_ld8(lanes + (uint32_t)(MDs + r0), vi);
+                    tmem_ld8x2(lanes + (uint32_t)r0, lanes + (uint32_t)(MDs + r0), vr, vi);
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
                         dst[r0 + i] = vr[i];
