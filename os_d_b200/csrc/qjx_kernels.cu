@@ -697,30 +697,33 @@ __device__ __forceinline__ int subtile_cols(int m, int NC)
     return min(m, NC);
 }
 
-__device__ __forceinline__ int subtile_cost(int m, int NC, int u_epi, int u_mma)
+__device__ __forceinline__ int subtile_cost(int m, int NC, int u_sub, int u_blk, int u_col4)
 {
     int c = 0;
     while (m > 0) {
         const int s = subtile_cols(m, NC);
         const int cb = (s + 7) / 8;
-        c += u_epi + u_mma * ((cb == 3) ? 4 : cb);
+        c += u_sub + u_blk * ((cb == 3) ? 4 : cb) + (s * u_col4) / 4;
         m -= s;
     }
     return c;
 }
 
-// Estimated cost of group g's bucket of m columns, in units of ~5k cycles at d = 201: per
-// sub-tile 2 (gather, epilogue; 3 more for the jump-operator and observable buckets, whose
-// epilogues renormalise, draw and reduce), per active 8-column block 6 (MMA loop), scaled to
-// the group's dimension (epilogue ~ d, MMA ~ row blocks x k rows).
+// Estimated cost of group g's bucket of m columns, in units of 0.25 us at d = 201, fitted to the
+// busy time of every CTA in 512 full micro-steps of the headline ensemble against the work it
+// got (least squares, 1.9 us rms): 7.8 us per sub-tile (gather, slab pipeline fill, epilogue
+// passes), 15.0 us per active 8-column block (MMA loop), 0.06 us per column and 0.15 us more per
+// column of the jump-operator and observable buckets (their epilogues renormalise, draw and
+// reduce); scaled to the group's dimension (epilogue ~ d, MMA ~ row blocks x k rows).
 __device__ __forceinline__ int group_cost(const Params &P, int g, int m)
 {
     if (m == 0) return 0;
     const int e = P.g_ens[g], d = P.e_d[e];
     const bool heavy = g - P.e_g0[e] >= P.gL0;
-    const int u_epi = max(1, ((heavy ? 5 : 2) * d + 100) / 201);
-    const int u_mma = max(1, (((d + 7) >> 3) * ((d + 1) & ~1) + 437) / 875);
-    return subtile_cost(m, P.e_nc[e], u_epi, u_mma);
+    const int u_sub = max(1, (31 * d + 100) / 201);
+    const int u_blk = max(1, (((d + 7) >> 3) * ((d + 1) & ~1) * 60 + 2626) / 5252);
+    const int u_col4 = max(1, ((heavy ? 7 : 2) * d + 200) / 402);
+    return subtile_cost(m, P.e_nc[e], u_sub, u_blk, u_col4);
 }
 
 // Plan of a micro-step from its bucket sizes cnt[G]: bucket starts plan[0..G] and cost prefix
