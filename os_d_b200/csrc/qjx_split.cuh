@@ -404,264 +404,264 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
     // micro-steps s0 .. s0 + nsteps - 1 (one, when launched per step); between two steps of one
     // launch every CTA waits at a grid barrier whose last arrival plans the next step
     for (int si = 0; si < nsteps; si++) {
-    const int s = s0 + si;
-    const int *cnt_cur = P.cnt + (s % 3) * G;
-    int *cnt_next = P.cnt + ((s + 1) % 3) * G;
-    const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
-    int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
-    const int *rlist_cur = P.rlist + (size_t)(s & 1) * P.n;
-    int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
-    int *rcnt_next = P.rcnt + (s + 1) % 3;
-    const int Rtot = __ldcg(P.rcnt + s % 3);  // FP64 rechecks of this micro-step
-    const int R = __ldcg(P.splan), T = __ldcg(P.splan + 1 + G);  // this step's plan (rows per tile, tiles)
-    if (T + Rtot == 0) break;  // nothing left in this call (every CTA reads the same plan)
-    if (blockIdx.x == 0) {
-        for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
-        if (tid == 0) P.rcnt[(s + 2) % 3] = 0;
-    }
+        const int s = s0 + si;
+        const int *cnt_cur = P.cnt + (s % 3) * G;
+        int *cnt_next = P.cnt + ((s + 1) % 3) * G;
+        const int *list_cur = P.lists + (size_t)(s & 1) * P.ltot;
+        int *list_next = P.lists + (size_t)((s + 1) & 1) * P.ltot;
+        const int *rlist_cur = P.rlist + (size_t)(s & 1) * P.n;
+        int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
+        int *rcnt_next = P.rcnt + (s + 1) % 3;
+        const int Rtot = __ldcg(P.rcnt + s % 3);  // FP64 rechecks of this micro-step
+        const int R = __ldcg(P.splan), T = __ldcg(P.splan + 1 + G);  // this step's plan (rows per tile, tiles)
+        if (T + Rtot == 0) break;  // nothing left in this call (every CTA reads the same plan)
+        if (blockIdx.x == 0) {
+            for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
+            if (tid == 0) P.rcnt[(s + 2) % 3] = 0;
+        }
 
-    for (int t = blockIdx.x; t < T + Rtot && ok; t += gridDim.x) {
-        if (t >= T) {  // an FP64 recheck (the CTAs past the split tiles take these first)
-            if (!recheck_column(P, rlist_cur[t - T], smem, &s_st[0], rbar, rphase, cnt_next, list_next)) {
+        for (int t = blockIdx.x; t < T + Rtot && ok; t += gridDim.x) {
+            if (t >= T) {  // an FP64 recheck (the CTAs past the split tiles take these first)
+                if (!recheck_column(P, rlist_cur[t - T], smem, &s_st[0], rbar, rphase, cnt_next, list_next)) {
+                    ok = false;
+                    break;
+                }
+                work += 1;
+                nrechk += 1;
+                continue;
+            }
+            const long long t0 = clock64();
+            const int g = split_tile_group(P, t, lane);  // every warp finds it (warp-uniform)
+            const int e = P.g_ens[g];
+            const int d = P.e_d[e], MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
+            const int Rg = group_rows(R, g - P.e_g0[e] >= P.nb * P.deep);
+            const int base = (t - __ldcg(P.splan + 1 + g)) * Rg;
+            const int rows = min(Rg, __ldcg(cnt_cur + g) - base);
+            if (tid < kTileM) {
+                if (tid < rows) {
+                    const int tr = list_cur[P.g_loff[g] + base + tid];
+                    const TrajState *sp = &P.st[tr];
+                    const int slot = src_slot(sp->phase, sp->cur, sp->rk_stage);
+                    s_tr[tid] = tr;
+                    s_src[tid] = ((long long)slot * n + tr) * P.MD;
+                } else {
+                    s_tr[tid] = -1;
+                    s_src[tid] = -1;
+                }
+            }
+            __syncthreads();
+            const long long t1 = clock64();
+            const uint32_t it0 = kit;  // k-steps issued before this tile
+            const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
+            const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
+
+            const int agrp = (warp < 4) ? 0 : (warp >= 6 && warp < 10) ? 1 : (warp >= 10 && warp < 14) ? 2 : -1;
+            if (agrp >= 0) {
+                // A producers: group p (4 warps) handles the k-steps ks = p (mod 3), so three
+                // independent load-convert chains run in parallel.  One warp-wide load covers 8 rows x
+                // one K-half (components 16 ks + 8 hh .. + 7, 128 contiguous bytes of each row): lane l
+                // takes row 8 rb + l / 4 and the component pair 2 (l % 4), 2 (l % 4) + 1, so every
+                // 32-byte sector is read whole by one lane, and a round's four plane stores are 128
+                // contiguous bytes each.  Round u of a warp is the (row block, half) pair 4 u + warp;
+                // all rounds of a k-step are loaded before the stage is waited for.  Rows past the
+                // tile's last trajectory are neither loaded nor stored: row i of an accumulator depends
+                // on row i of A only, and the epilogue reads live rows only.
+                const int gw = warp - (agrp == 0 ? 0 : (agrp == 1 ? 6 : 10));
+                const int r8 = lane >> 2, jq = lane & 3;
+                const int npairs = 2 * ((rows + 7) >> 3);
+                for (int ks = agrp; ks < KS && ok; ks += 3) {
+                    const uint32_t it = it0 + ks, q = it % S;
+                    unsigned char *As = smem + q * stage_bytes + 4 * lane;
+                    for (int u0 = 0; u0 < 8; u0 += 4) {
+                        if (u0 > 0 && 4 * u0 + gw >= npairs) break;  // warp-uniform
+                        double2 v[4][2];
+    #pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
+                            const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
+                            // every lane of a live round loads (a lane without data reads component 0
+                            // of row 0) and nothing touches v before the stage wait, so the four loads
+                            // are in flight together: a select or a write on a load's destination
+                            // registers would wait for that load.  k + 1 < MD: inside the row.
+                            const long long so = (m < rows && k < d) ? s_src[m] + k : 0;
+                            if (pi < npairs) ld_pair(P.psi + so, v[u][0], v[u][1]);
+                        }
+                        if (u0 == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
+                            ok = false;
+    #pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
+                            if (pi >= npairs || m >= rows) continue;
+                            // components from d on are row padding (or were not loaded): zeros
+                            const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
+                            const double2 z = make_double2(0.0, 0.0);
+                            const double2 a = (k < d) ? v[u][0] : z, b = (k + 1 < d) ? v[u][1] : z;
+                            uint32_t rh, rl, ih, il;
+                            split_pair(make_double2(a.x, b.x), rh, rl);
+                            split_pair(make_double2(a.y, b.y), ih, il);
+                            unsigned char *dst = As + 256 * (pi >> 1) + 128 * (pi & 1);
+                            *reinterpret_cast<uint32_t *>(dst) = rh;
+                            *reinterpret_cast<uint32_t *>(dst + kABytes) = rl;
+                            *reinterpret_cast<uint32_t *>(dst + 2 * kABytes) = ih;
+                            *reinterpret_cast<uint32_t *>(dst + 3 * kABytes) = il;
+                        }
+                    }
+                    fence_proxy_async();
+                    mbar_arrive(&fullA[q]);
+                }
+            } else if (warp == 4) {
+                if (lane == 0) {  // B producer
+                    const unsigned char *ug = P.usplit + P.g_uoff[g];
+                    for (int ks = 0; ks < KS && ok; ks++) {
+                        const uint32_t it = it0 + ks, q = it % S;
+                        if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait)) {
+                            ok = false;
+                            break;
+                        }
+                        mbar_expect_tx(&fullB[q], (uint32_t)(kAPlanes * bbytes));
+                        bulk_g2s(smem + q * stage_bytes + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes,
+                                 (uint32_t)(kAPlanes * bbytes), &fullB[q]);
+                    }
+                }
+            } else if (warp == 5) {
+                if (lane == 0) {  // MMA issuer
+                    for (int ks = 0; ks < KS && ok; ks++) {
+                        const uint32_t it = it0 + ks, q = it % S, par = (it / S) & 1u;
+                        if (!mbar_wait_bounded(&fullA[q], par, kSplitWait) || !mbar_wait_bounded(&fullB[q], par, kSplitWait)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t a = smem_u32(smem + q * stage_bytes);
+                        const uint64_t xrh = umma_desc_kmajor(a), xrl = umma_desc_kmajor(a + kABytes);
+                        const uint64_t xih = umma_desc_kmajor(a + 2 * kABytes), xil = umma_desc_kmajor(a + 3 * kABytes);
+                        const uint32_t b = a + kAPlanes * kABytes;
+                        const uint64_t urh = umma_desc_kmajor(b), url = umma_desc_kmajor(b + bbytes);
+                        const uint64_t uih = umma_desc_kmajor(b + 2 * bbytes), uil = umma_desc_kmajor(b + 3 * bbytes);
+                        const uint32_t acc = ks > 0 ? 1u : 0u;
+                        const uint32_t dre = tmem, dim = tmem + (uint32_t)MDs;
+                        // Re y += Xr Ur - Xi Ui
+                        umma_bf16(dre, xrh, urh, idesc, acc);
+                        umma_bf16(dre, xrh, url, idesc, 1u);
+                        umma_bf16(dre, xrl, urh, idesc, 1u);
+                        umma_bf16(dre, xih, uih, idesc_neg, 1u);
+                        umma_bf16(dre, xih, uil, idesc_neg, 1u);
+                        umma_bf16(dre, xil, uih, idesc_neg, 1u);
+                        // Im y += Xr Ui + Xi Ur
+                        umma_bf16(dim, xrh, uih, idesc, acc);
+                        umma_bf16(dim, xrh, uil, idesc, 1u);
+                        umma_bf16(dim, xrl, uih, idesc, 1u);
+                        umma_bf16(dim, xih, urh, idesc, 1u);
+                        umma_bf16(dim, xih, url, idesc, 1u);
+                        umma_bf16(dim, xil, urh, idesc, 1u);
+                        umma_commit(&empty[q]);  // frees the stage once these MMAs have read it
+                    }
+                    umma_commit(&accf);
+                }
+            } else {
+                // warps 14-15: the tile's state records, loaded while the MMAs run
+                for (int m = tid - 448; m < rows; m += 64) load_state(&s_st[m], &P.st[s_tr[m]]);
+            }
+            // lanes 1-31 of the B-producer and MMA warps park here until their lane 0 is done: spinning on
+            // the accumulator barrier instead would take the warp's issue slots from the lane issuing
+            __syncwarp();
+            kit += (uint32_t)KS;
+            if (!ok) atomicExch(&s_fail, 1);
+            // accumulator complete (every thread waits on the commit); the ring is free afterwards
+            if (!mbar_wait_bounded(&accf, ntile & 1u, kSplitWait)) atomicExch(&s_fail, 1);
+            tc_fence_after();
+            __syncthreads();
+            if (s_fail) {
                 ok = false;
                 break;
             }
-            work += 1;
-            nrechk += 1;
-            continue;
-        }
-        const long long t0 = clock64();
-        const int g = split_tile_group(P, t, lane);  // every warp finds it (warp-uniform)
-        const int e = P.g_ens[g];
-        const int d = P.e_d[e], MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
-        const int Rg = group_rows(R, g - P.e_g0[e] >= P.nb * P.deep);
-        const int base = (t - __ldcg(P.splan + 1 + g)) * Rg;
-        const int rows = min(Rg, __ldcg(cnt_cur + g) - base);
-        if (tid < kTileM) {
-            if (tid < rows) {
-                const int tr = list_cur[P.g_loff[g] + base + tid];
-                const TrajState *sp = &P.st[tr];
-                const int slot = src_slot(sp->phase, sp->cur, sp->rk_stage);
-                s_tr[tid] = tr;
-                s_src[tid] = ((long long)slot * n + tr) * P.MD;
-            } else {
-                s_tr[tid] = -1;
-                s_src[tid] = -1;
+            const long long t2 = clock64();
+            float *sacc = reinterpret_cast<float *>(smem);  // [RP][2 MDs + 1] FP32 accumulators
+            const int SR = 2 * MDs + 1;
+            for (int p0 = 0; p0 < rows; p0 += RP) {  // passes of RP trajectories
+                const long long ts = clock64();
+                const int q = warp & 3;  // TMEM lanes 32q..32q+31 belong to warps q, q+4, q+8, q+12
+                if (32 * q >= p0 && 32 * q < p0 + RP && 32 * q < rows) {
+                    const uint32_t lanes = tmem + ((uint32_t)(32 * q) << 16);
+                    float *dst = sacc + (size_t)(32 * q - p0 + lane) * SR;
+                    for (int r0 = 8 * (warp >> 2); r0 < MDs; r0 += 32) {  // 8 output rows at a time
+                        float vr[8], vi[8];
+                        tmem_ld8x2(lanes + (uint32_t)r0, lanes + (uint32_t)(MDs + r0), vr, vi);
+    #pragma unroll
+                        for (int i = 0; i < 8; i++) {
+                            dst[r0 + i] = vr[i];
+                            dst[MDs + r0 + i] = vi[i];
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncthreads();
+                tr_stage += clock64() - ts;
+                // every warp runs its trajectories (columns warp, warp + 16, ...) through the epilogue,
+                // then appends them to their next buckets with one atomic each, all in flight together
+                const int pn = min(RP, rows - p0);
+                int nm = 0;
+                for (int cc = warp; cc < pn; cc += kThreads / 32, nm++) {
+                    const int m = p0 + cc;
+                    const float *row = sacc + (size_t)cc * SR;
+                    for (int k = lane; k < MDs; k += 32) wcol[k] = make_double2((double)row[k], (double)row[MDs + k]);
+                    __syncwarp();
+                    const int g2 = column_epilogue(P, wcol, s_tr[m], s_st[m], lane);
+                    if (lane == 0) w_g2[warp][nm] = g2;
+                    __syncwarp();
+                }
+                if (lane < nm) {
+                    const int g2 = w_g2[warp][lane];
+                    const int tr = s_tr[p0 + warp + (kThreads / 32) * lane];
+                    if (g2 >= 0) {
+                        const int pos = atomicAdd(&cnt_next[g2], 1);
+                        list_next[P.g_loff[g2] + pos] = tr;
+                    } else if (g2 == kRecheck) {
+                        rlist_next[atomicAdd(rcnt_next, 1)] = tr;
+                    }
+                }
+                fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
+                __syncthreads();
             }
+            work += rows;
+            ntile++;
+            const long long t3 = clock64();
+            tr_setup += t1 - t0;
+            tr_mma += t2 - t1;
+            tr_epi += t3 - t2;
         }
-        __syncthreads();
-        const long long t1 = clock64();
-        const uint32_t it0 = kit;  // k-steps issued before this tile
-        const uint32_t idesc = umma_idesc_bf16(kTileM, MDs);
-        const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
 
-        const int agrp = (warp < 4) ? 0 : (warp >= 6 && warp < 10) ? 1 : (warp >= 10 && warp < 14) ? 2 : -1;
-        if (agrp >= 0) {
-            // A producers: group p (4 warps) handles the k-steps ks = p (mod 3), so three
-            // independent load-convert chains run in parallel.  One warp-wide load covers 8 rows x
-            // one K-half (components 16 ks + 8 hh .. + 7, 128 contiguous bytes of each row): lane l
-            // takes row 8 rb + l / 4 and the component pair 2 (l % 4), 2 (l % 4) + 1, so every
-            // 32-byte sector is read whole by one lane, and a round's four plane stores are 128
-            // contiguous bytes each.  Round u of a warp is the (row block, half) pair 4 u + warp;
-            // all rounds of a k-step are loaded before the stage is waited for.  Rows past the
-            // tile's last trajectory are neither loaded nor stored: row i of an accumulator depends
-            // on row i of A only, and the epilogue reads live rows only.
-            const int gw = warp - (agrp == 0 ? 0 : (agrp == 1 ? 6 : 10));
-            const int r8 = lane >> 2, jq = lane & 3;
-            const int npairs = 2 * ((rows + 7) >> 3);
-            for (int ks = agrp; ks < KS && ok; ks += 3) {
-                const uint32_t it = it0 + ks, q = it % S;
-                unsigned char *As = smem + q * stage_bytes + 4 * lane;
-                for (int u0 = 0; u0 < 8; u0 += 4) {
-                    if (u0 > 0 && 4 * u0 + gw >= npairs) break;  // warp-uniform
-                    double2 v[4][2];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
-                        const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
-                        // every lane of a live round loads (a lane without data reads component 0
-                        // of row 0) and nothing touches v before the stage wait, so the four loads
-                        // are in flight together: a select or a write on a load's destination
-                        // registers would wait for that load.  k + 1 < MD: inside the row.
-                        const long long so = (m < rows && k < d) ? s_src[m] + k : 0;
-                        if (pi < npairs) ld_pair(P.psi + so, v[u][0], v[u][1]);
-                    }
-                    if (u0 == 0 && it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait))
-                        ok = false;
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const int pi = 4 * (u0 + u) + gw, m = 8 * (pi >> 1) + r8;
-                        if (pi >= npairs || m >= rows) continue;
-                        // components from d on are row padding (or were not loaded): zeros
-                        const int k = 16 * ks + 8 * (pi & 1) + 2 * jq;
-                        const double2 z = make_double2(0.0, 0.0);
-                        const double2 a = (k < d) ? v[u][0] : z, b = (k + 1 < d) ? v[u][1] : z;
-                        uint32_t rh, rl, ih, il;
-                        split_pair(make_double2(a.x, b.x), rh, rl);
-                        split_pair(make_double2(a.y, b.y), ih, il);
-                        unsigned char *dst = As + 256 * (pi >> 1) + 128 * (pi & 1);
-                        *reinterpret_cast<uint32_t *>(dst) = rh;
-                        *reinterpret_cast<uint32_t *>(dst + kABytes) = rl;
-                        *reinterpret_cast<uint32_t *>(dst + 2 * kABytes) = ih;
-                        *reinterpret_cast<uint32_t *>(dst + 3 * kABytes) = il;
-                    }
-                }
-                fence_proxy_async();
-                mbar_arrive(&fullA[q]);
-            }
-        } else if (warp == 4) {
-            if (lane == 0) {  // B producer
-                const unsigned char *ug = P.usplit + P.g_uoff[g];
-                for (int ks = 0; ks < KS && ok; ks++) {
-                    const uint32_t it = it0 + ks, q = it % S;
-                    if (it >= (uint32_t)S && !mbar_wait_bounded(&empty[q], ((it / S) - 1) & 1u, kSplitWait)) {
-                        ok = false;
-                        break;
-                    }
-                    mbar_expect_tx(&fullB[q], (uint32_t)(kAPlanes * bbytes));
-                    bulk_g2s(smem + q * stage_bytes + kAPlanes * kABytes, ug + (size_t)ks * kAPlanes * bbytes,
-                             (uint32_t)(kAPlanes * bbytes), &fullB[q]);
-                }
-            }
-        } else if (warp == 5) {
-            if (lane == 0) {  // MMA issuer
-                for (int ks = 0; ks < KS && ok; ks++) {
-                    const uint32_t it = it0 + ks, q = it % S, par = (it / S) & 1u;
-                    if (!mbar_wait_bounded(&fullA[q], par, kSplitWait) || !mbar_wait_bounded(&fullB[q], par, kSplitWait)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t a = smem_u32(smem + q * stage_bytes);
-                    const uint64_t xrh = umma_desc_kmajor(a), xrl = umma_desc_kmajor(a + kABytes);
-                    const uint64_t xih = umma_desc_kmajor(a + 2 * kABytes), xil = umma_desc_kmajor(a + 3 * kABytes);
-                    const uint32_t b = a + kAPlanes * kABytes;
-                    const uint64_t urh = umma_desc_kmajor(b), url = umma_desc_kmajor(b + bbytes);
-                    const uint64_t uih = umma_desc_kmajor(b + 2 * bbytes), uil = umma_desc_kmajor(b + 3 * bbytes);
-                    const uint32_t acc = ks > 0 ? 1u : 0u;
-                    const uint32_t dre = tmem, dim = tmem + (uint32_t)MDs;
-                    // Re y += Xr Ur - Xi Ui
-                    umma_bf16(dre, xrh, urh, idesc, acc);
-                    umma_bf16(dre, xrh, url, idesc, 1u);
-                    umma_bf16(dre, xrl, urh, idesc, 1u);
-                    umma_bf16(dre, xih, uih, idesc_neg, 1u);
-                    umma_bf16(dre, xih, uil, idesc_neg, 1u);
-                    umma_bf16(dre, xil, uih, idesc_neg, 1u);
-                    // Im y += Xr Ui + Xi Ur
-                    umma_bf16(dim, xrh, uih, idesc, acc);
-                    umma_bf16(dim, xrh, uil, idesc, 1u);
-                    umma_bf16(dim, xrl, uih, idesc, 1u);
-                    umma_bf16(dim, xih, urh, idesc, 1u);
-                    umma_bf16(dim, xih, url, idesc, 1u);
-                    umma_bf16(dim, xil, urh, idesc, 1u);
-                    umma_commit(&empty[q]);  // frees the stage once these MMAs have read it
-                }
-                umma_commit(&accf);
-            }
-        } else {
-            // warps 14-15: the tile's state records, loaded while the MMAs run
-            for (int m = tid - 448; m < rows; m += 64) load_state(&s_st[m], &P.st[s_tr[m]]);
-        }
-        // lanes 1-31 of the B-producer and MMA warps park here until their lane 0 is done: spinning on
-        // the accumulator barrier instead would take the warp's issue slots from the lane issuing
-        __syncwarp();
-        kit += (uint32_t)KS;
-        if (!ok) atomicExch(&s_fail, 1);
-        // accumulator complete (every thread waits on the commit); the ring is free afterwards
-        if (!mbar_wait_bounded(&accf, ntile & 1u, kSplitWait)) atomicExch(&s_fail, 1);
-        tc_fence_after();
+        steps_done++;
+        if (!ok && tid == 0) atomicAdd(&P.ctrl[4], 1);  // every CTA stops after the barrier below
+        // the last CTA to finish plans the next micro-step from the buckets all CTAs filled; with a
+        // next step in this launch the others wait for that plan (bounded), then read it
         __syncthreads();
-        if (s_fail) {
-            ok = false;
-            break;
-        }
-        const long long t2 = clock64();
-        float *sacc = reinterpret_cast<float *>(smem);  // [RP][2 MDs + 1] FP32 accumulators
-        const int SR = 2 * MDs + 1;
-        for (int p0 = 0; p0 < rows; p0 += RP) {  // passes of RP trajectories
-            const long long ts = clock64();
-            const int q = warp & 3;  // TMEM lanes 32q..32q+31 belong to warps q, q+4, q+8, q+12
-            if (32 * q >= p0 && 32 * q < p0 + RP && 32 * q < rows) {
-                const uint32_t lanes = tmem + ((uint32_t)(32 * q) << 16);
-                float *dst = sacc + (size_t)(32 * q - p0 + lane) * SR;
-                for (int r0 = 8 * (warp >> 2); r0 < MDs; r0 += 32) {  // 8 output rows at a time
-                    float vr[8], vi[8];
-                    tmem_ld8x2(lanes + (uint32_t)r0, lanes + (uint32_t)(MDs + r0), vr, vi);
-#pragma unroll
-                    for (int i = 0; i < 8; i++) {
-                        dst[r0 + i] = vr[i];
-                        dst[MDs + r0 + i] = vi[i];
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncthreads();
-            tr_stage += clock64() - ts;
-            // every warp runs its trajectories (columns warp, warp + 16, ...) through the epilogue,
-            // then appends them to their next buckets with one atomic each, all in flight together
-            const int pn = min(RP, rows - p0);
-            int nm = 0;
-            for (int cc = warp; cc < pn; cc += kThreads / 32, nm++) {
-                const int m = p0 + cc;
-                const float *row = sacc + (size_t)cc * SR;
-                for (int k = lane; k < MDs; k += 32) wcol[k] = make_double2((double)row[k], (double)row[MDs + k]);
-                __syncwarp();
-                const int g2 = column_epilogue(P, wcol, s_tr[m], s_st[m], lane);
-                if (lane == 0) w_g2[warp][nm] = g2;
-                __syncwarp();
-            }
-            if (lane < nm) {
-                const int g2 = w_g2[warp][lane];
-                const int tr = s_tr[p0 + warp + (kThreads / 32) * lane];
-                if (g2 >= 0) {
-                    const int pos = atomicAdd(&cnt_next[g2], 1);
-                    list_next[P.g_loff[g2] + pos] = tr;
-                } else if (g2 == kRecheck) {
-                    rlist_next[atomicAdd(rcnt_next, 1)] = tr;
-                }
-            }
-            fence_proxy_async();  // generic writes to the ring before the next tile's bulk copies
-            __syncthreads();
-        }
-        work += rows;
-        ntile++;
-        const long long t3 = clock64();
-        tr_setup += t1 - t0;
-        tr_mma += t2 - t1;
-        tr_epi += t3 - t2;
-    }
-
-    steps_done++;
-    if (!ok && tid == 0) atomicAdd(&P.ctrl[4], 1);  // every CTA stops after the barrier below
-    // the last CTA to finish plans the next micro-step from the buckets all CTAs filled; with a
-    // next step in this launch the others wait for that plan (bounded), then read it
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        s_gen = ld_acquire_u32(P.gen);
-        s_last = atomicAdd(P.plan_sync, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    const bool more = si + 1 < nsteps;
-    if (s_last) {
-        __threadfence();
-        split_plan(P, cnt_next, __ldcg(rcnt_next), gridDim.x);
         if (tid == 0) {
-            *P.plan_sync = 0u;
             __threadfence();
-            st_release_u32(P.gen, s_gen + 1u);
+            s_gen = ld_acquire_u32(P.gen);
+            s_last = atomicAdd(P.plan_sync, 1u) == gridDim.x - 1;
         }
-    } else if (more && tid == 0) {
-        long long i = 0;
-        while (ld_acquire_u32(P.gen) == s_gen && i < kGridWait) i++;
-        if (i == kGridWait) {
-            atomicAdd(&P.ctrl[4], 1);
-            report_error(P, -1, ERR_TIMEOUT);
+        __syncthreads();
+        const bool more = si + 1 < nsteps;
+        if (s_last) {
+            __threadfence();
+            split_plan(P, cnt_next, __ldcg(rcnt_next), gridDim.x);
+            if (tid == 0) {
+                *P.plan_sync = 0u;
+                __threadfence();
+                st_release_u32(P.gen, s_gen + 1u);
+            }
+        } else if (more && tid == 0) {
+            long long i = 0;
+            while (ld_acquire_u32(P.gen) == s_gen && i < kGridWait) i++;
+            if (i == kGridWait) {
+                atomicAdd(&P.ctrl[4], 1);
+                report_error(P, -1, ERR_TIMEOUT);
+            }
         }
-    }
-    __syncthreads();
-    __threadfence();
-    if (!more || !ok || __ldcg(P.ctrl + 4) != 0) break;
+        __syncthreads();
+        __threadfence();
+        if (!more || !ok || __ldcg(P.ctrl + 4) != 0) break;
     }  // micro-steps
 
     if (!ok) {
