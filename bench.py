@@ -867,10 +867,18 @@ def run_ours(args):
     if tuned:
         line["autotune"] = tuned
 
+    # the split form and the other configurations' measurements: an error in one is reported in
+    # its object and does not take the headline line with it
+    def stage(fn, *a):
+        try:
+            return fn(*a)
+        except Exception as ex:  # noqa: BLE001 -- recorded in the JSON line
+            return {"error": f"{type(ex).__name__}: {ex}"}
+
     # split-precision form: same checkpoint, same windows
     if not args.no_split:
-        line["split_form"] = split_form(args, q, new_engine, timed_windows, snap, value, ens_plain, x_plain,
-                                        eng, n, d, P, W, world)
+        line["split_form"] = stage(split_form, args, q, new_engine, timed_windows, snap, value, ens_plain, x_plain,
+                                   eng, n, d, P, W, world)
 
     # e2e through the public C ABI with host buffers, copies inside the timed region
     if not args.no_e2e:
@@ -890,11 +898,11 @@ def run_ours(args):
                        "path": "qjx_checkpoint_load (window start, pinned host buffer) + qjx_run_periods + "
                                "qjx_get_observables + qjx_get_states per step, same window as value"}
     if rank == 0 and not args.no_fbasis:
-        line["fbasis"] = fbasis_bench(args, local)
+        line["fbasis"] = stage(fbasis_bench, args, local)
     if rank == 0 and world == 1 and not args.no_batch:  # single-GPU measurements
-        line["batched"] = batched_bench(args, local)
+        line["batched"] = stage(batched_bench, args, local)
     if rank == 0 and world == 1 and not args.no_serve:
-        line["serving"] = serving_bench(args, local)
+        line["serving"] = stage(serving_bench, args, local)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = CPU_TRAJ_PER_THREAD * threads

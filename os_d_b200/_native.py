@@ -165,8 +165,9 @@ def ip(a):
 def check(status, handle=None, what=""):
     if status != 0:
         msg = lib().qjx_status_string(status).decode()
-        if handle:
-            msg += ": " + lib().qjx_last_error(handle).decode()
+        detail = lib().qjx_last_error(handle).decode() if handle else lib().qjx_last_error(None).decode()
+        if detail:
+            msg += ": " + detail
         raise QjxError(f"{what} failed ({status}): {msg}")
 
 

@@ -134,7 +134,10 @@ extern "C" const char *qjx_status_string(qjx_status s)
     return "unknown";
 }
 
-extern "C" const char *qjx_last_error(const qjx_engine *h) { return h ? h->err.c_str() : "null handle"; }
+// The reason the calling thread's last engine creation failed (its handle no longer exists).
+static thread_local std::string g_create_err;
+
+extern "C" const char *qjx_last_error(const qjx_engine *h) { return h ? h->err.c_str() : g_create_err.c_str(); }
 
 // Transposes row-major complex d x d matrices into the device layout mats[g][k][row]
 // (rows padded to MD and k to an even count with zeros), so one K-slab is one contiguous
@@ -336,14 +339,20 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
         qjx_destroy(h);
         return s;
     };
-    if (cudaSetDevice(c.device) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    auto bail_cuda = [&](cudaError_t e, const char *where) {
+        g_create_err = std::string(where) + ": " + cudaGetErrorString(e);
+        return bail(QJX_ERR_CUDA);
+    };
+    g_create_err.clear();
+    if (cudaError_t e = cudaSetDevice(c.device); e != cudaSuccess) return bail_cuda(e, "cudaSetDevice");
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
     h->grid = sms > 0 ? sms : 148;
     // QJX_SPLIT_COOP=0: run the split form's micro-steps as one launch each (the path taken when a
     // cooperative launch cannot make every CTA resident)
     if (const char *v = getenv("QJX_SPLIT_COOP")) h->split_coop = v[0] != '0';
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    if (cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking); e != cudaSuccess)
+        return bail_cuda(e, "cudaStreamCreateWithFlags");
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     cudaEventCreate(&h->eb0);
@@ -572,9 +581,11 @@ static qjx_status create_engine(const qjx_config *cfg, const std::vector<EnsDesc
     h->jn.assign(n, {});
     h->je.assign(n, {});
     h->jtype.assign(n, {});
-    if (cudaDeviceSynchronize() != cudaSuccess) return bail(QJX_ERR_CUDA);
-    if (launch_init_state(P, h->stream) != cudaSuccess) return bail(QJX_ERR_CUDA);
-    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(QJX_ERR_CUDA);
+    // the setup's memsets and copies ran on the legacy default stream; the engine's stream does not
+    // wait for it (and a device-wide sync would wait for every other engine in the process)
+    if (cudaError_t e = cudaStreamSynchronize(0); e != cudaSuccess) return bail_cuda(e, "engine setup");
+    if (cudaError_t e = launch_init_state(P, h->stream); e != cudaSuccess) return bail_cuda(e, "init_state launch");
+    if (cudaError_t e = cudaStreamSynchronize(h->stream); e != cudaSuccess) return bail_cuda(e, "init_state");
     *out = h;
     return QJX_OK;
 }

@@ -257,19 +257,24 @@ class Server:
         self.queue = waiting
 
     def run(self, arrivals):
-        """Serve (arrival_time_s, request) pairs in arrival order on the wall clock until all are done."""
+        """Serve (arrival_time_s, request) pairs in arrival order on the wall clock until all are done.
+        On an error the pools are closed (their threads joined) before it propagates."""
         arrivals = sorted(arrivals, key=lambda x: x[0])
         k = 0
-        while k < len(arrivals) or self.busy():
-            while k < len(arrivals) and arrivals[k][0] <= self.now():
-                self.submit(arrivals[k][1])
-                k += 1
-            self._admit()
-            with self.cv:
-                err = next((p.error for p in self.pools if p.error is not None), None)
-                if err is not None:
-                    raise err
-                self.cv.wait(0.005)
+        try:
+            while k < len(arrivals) or self.busy():
+                while k < len(arrivals) and arrivals[k][0] <= self.now():
+                    self.submit(arrivals[k][1])
+                    k += 1
+                self._admit()
+                with self.cv:
+                    err = next((p.error for p in self.pools if p.error is not None), None)
+                    if err is not None:
+                        raise err
+                    self.cv.wait(0.005)
+        except BaseException:
+            self.close()
+            raise
         return list(self.results)
 
     def close(self):
