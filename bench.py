@@ -65,7 +65,7 @@ def parse():
                     help="only time this many points of the N=500 LpnMult production sweep (separate JSON line)")
     ap.add_argument("--serve-window", type=float, default=1.0, help="seconds of Poisson arrivals at 50/s")
     ap.add_argument("--batch-ensembles", type=int, default=32,
-                    help="ensembles of configuration 4 in the batched measurement (of 256)")
+                    help="ensembles of the 256-ensemble uneven sweep in the batched measurement")
     ap.add_argument("--profile", action="store_true", help="short run for ncu captures (no JSON line)")
     ap.add_argument("--profile-target", default="plain",
                     choices=["plain", "split", "fbasis", "fbstages", "lpn", "purity", "rk", "batched"],
@@ -186,7 +186,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# ---------------------------------------------------------------- f-basis Lindblad RK4 (configuration 3)
+# ---------------------------------------------------------------- f-basis Lindblad RK4 (dimer N = 50, dt = 1e-3)
 FB_N, FB_DT, FB_A = 50, 1e-3, 1.5
 
 
@@ -244,12 +244,12 @@ def fbasis_bench(args, local):
     return out
 
 
-# ---------------------------------------------------------------- batched uneven ensembles (configuration 4)
+# ---------------------------------------------------------------- batched uneven ensembles (256 dimers, N ~ U[50, 400])
 BATCH_SEED, BATCH_TRAJ = 11, 1000
 
 
 def batch_draw(count):
-    """Configuration 4's ensembles: N ~ U[50, 400], E0 ~ U[0, 2], g log-uniform in [0.01, 1], seed 11
+    """The uneven sweep's ensembles: N ~ U[50, 400], E0 ~ U[0, 2], g log-uniform in [0.01, 1], seed 11
     (the first `count` of the 256 draws)."""
     rng = np.random.default_rng(BATCH_SEED)
     Ns = rng.integers(50, 401, size=256)
@@ -334,7 +334,7 @@ def batched_bench(args, local):
                    "plain_value": sub[0][0], "split_value": sub[1][0], "split_speedup": sub[1][0] / sub[0][0],
                    "split_rechecks": sub[1][1]}
     return {
-        "workload": (f"{len(ens)} of configuration 4's 256 dimer ensembles (N ~ U[50,400], E0 ~ U[0,2], g log-uniform "
+        "workload": (f"{len(ens)} of the 256 uneven dimer ensembles (N ~ U[50,400], E0 ~ U[0,2], g log-uniform "
                      f"[0.01,1], seed {BATCH_SEED}; dims {min(dims)}-{max(dims)}), {BATCH_TRAJ} trajectories each, "
                      f"ex_deep {DEEP}, complex FP64, one period per step"),
         "metric": METRIC, "value": n_tot * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
@@ -386,7 +386,7 @@ def profile_case(target, local):
                (three ensemble-purity evaluations with the density matrix);
     rk      -- the RK propagator (prop_id 1) on dim 101 (N = 100, g = 0.4, where 2000 RK4 steps per
                period are stable), 2000 trajectories, one period;
-    batched -- the first 8 of configuration 4's ensembles (1000 trajectories each) in one batched
+    batched -- the first 8 of the 256 uneven ensembles (1000 trajectories each) in one batched
                engine, one period."""
     import os_d_b200 as q
 
@@ -505,10 +505,10 @@ def production_sweep(args, local):
     return out
 
 
-# ---------------------------------------------------------------- serving loop (configuration 5, sampled)
+# ---------------------------------------------------------------- serving loop (requests up to N = 1023, sampled)
 def serving_bench(args, local):
     """Continuous batching (os_d_b200.serve): Poisson arrivals at 50/s over a short window with
-    configuration 5's size range (N log-uniform in [31, 1023]; E0 ~ U[0, 2], g log-uniform in
+    the serving workload's size range (N log-uniform in [31, 1023]; E0 ~ U[0, 2], g log-uniform in
     [0.01, 1], seed 23) but trajectories U[10, 1000] and 1-3 periods (its full sizes, up to 10^4
     trajectories x 500 periods at d = 1024, are hours of device time per request); size-class pools
     admitted against the device's free memory, operators built on the GPU; latency from arrival to
@@ -551,9 +551,9 @@ def serving_bench(args, local):
         ser_ms += A.stats()["kernel_ms"]
         per_req.append((d, n * int(r["periods"]), A.stats()["kernel_ms"]))
         A.close()
-    # what one GPU sustains at configuration 5's full request sizes: the device time per
+    # what one GPU sustains at the serving workload's full request sizes: the device time per
     # trajectory-period of a request alone, fitted as a + b d^2 over the sample, averaged over
-    # config 5's distribution (N log-uniform [31, 1023], trajectories U[100, 10^4], periods
+    # the full request distribution (N log-uniform [31, 1023], trajectories U[100, 10^4], periods
     # U[50, 500]), and divided by the serving loop's measured gain over serial solves
     dd = np.array([x[0] for x in per_req], float)
     tp = np.array([x[1] for x in per_req], float)
@@ -576,12 +576,12 @@ def serving_bench(args, local):
         "serial_single_ensemble_engines": {"value": work / (ser_ms * 1e-3), "device_s": ser_ms * 1e-3},
         "speedup_vs_serial_device": ser_ms / dev_ms, "pools_created": pools, "peak_pool_bytes": peak,
         "wall_s": wall, "max_d": int(max(r["N"] for _, r in arrivals)) + 1,
-        "config5_sustained": {
+        "full_size_sustained": {
             "requests_per_s": sustain, "mean_request_device_s": float(req_ms.mean()) * 1e-3 / gain,
             "model": "device ms of a request alone = trajectory-periods x (a + b d^2), fitted over this sample "
-                     f"(a = {coef[0]:.3g}, b = {coef[1]:.3g}); averaged over configuration 5's sizes (N log-uniform "
+                     f"(a = {coef[0]:.3g}, b = {coef[1]:.3g}); averaged over the full request sizes (N log-uniform "
                      "[31,1023], trajectories U[100,10^4], periods U[50,500]) and divided by the serving loop's "
-                     "measured gain over serial solves; configuration 5's 50 requests/s exceeds it by the ratio"},
+                     "measured gain over serial solves; an arrival rate of 50 requests/s exceeds it by the ratio"},
     }
 
 

@@ -201,9 +201,9 @@ def test_gpu_stage_kernels_beyond_the_cluster_match_oracle_and_repeat(monkeypatc
 
 
 @pytest.mark.gpu
-def test_config3_qj_ensemble_within_3_sigma_of_fbasis_rho():
-    """Configuration 3: dimer N = 50 (d = 51; J 1, U 0.5, E 1, A 1.5, g 0.1), the QJ ensemble of 10^4
-    trajectories from |N,0> against the f-basis density matrix from the same state (Liouvillian from
+def test_qj_ensemble_at_d51_within_3_sigma_of_fbasis_rho():
+    """The f-basis steady-state check: dimer N = 50 (d = 51; J 1, U 0.5, E 1, A 1.5, g 0.1), the QJ
+    ensemble of 10^4 trajectories from |N,0> against the f-basis density matrix from the same state (Liouvillian from
     the library's builder, RK4 with dt = 1e-3: 6284 steps per period), both on the GPU.  After 40
     periods (the periodic steady state: the populations change by less than their statistical error
     between the last two dumps) every one of the 51 populations lies within 3 standard errors of the
