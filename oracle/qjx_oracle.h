@@ -1,7 +1,7 @@
 /*
  * qjx_oracle.h -- CPU restatement of the QJX quantum-jump path (TEST INFRASTRUCTURE).
  *
- * This library is the checker for the CUDA engine in os_d_b200.  Only tests/,
+ * This library is the oracle the CUDA engine in os_d_b200 is tested against.  Only tests/,
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.  The product
  * never links or calls it.
  *
