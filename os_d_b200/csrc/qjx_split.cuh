@@ -219,10 +219,11 @@ __device__ bool recheck_column(const Params &P, int tr, unsigned char *smem, Tra
 // blockDim.x a multiple of 32): rows per tile R, the smallest multiple of 8 (at least P.min_rows,
 // at most 128) whose tiles fit one wave of `grid` CTAs next to the rechecks, so that trajectories
 // and their epilogues spread over all SMs; then the first tile of every group.
-// Rows per tile of a bucket when the plan's rows per tile is R: the jump-operator and observable
-// buckets take about 5/8 of R (their epilogues renormalise, draw and reduce: a tile of them took
-// 1.3x as long as a matrix bucket's tile of as many rows, and a micro-step waits for its slowest
-// tile), the (branch, level) buckets R.
+// Rows per tile of a bucket when the plan's rows per tile is R: when the tiles fit one wave, the
+// jump-operator and observable buckets take about 5/8 of R (their epilogues renormalise, draw and
+// reduce: a tile of them took 1.3x as long as a matrix bucket's tile of as many rows, and a
+// micro-step waits for its slowest tile); the (branch, level) buckets, and every bucket when the
+// tiles take several waves (a batch of many ensembles: more tiles would only add MMA work), R.
 __device__ __forceinline__ bool heavy_group(const Params &P, int g)
 {
     return g - P.e_g0[P.g_ens[g]] >= P.nb * P.deep;
@@ -233,7 +234,7 @@ __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
 {
     __shared__ int w_t[32][17];
     __shared__ int w_s[32];
-    __shared__ int s_R;
+    __shared__ int s_R, s_hv;
     const int G = P.G, nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     int part[16];
 #pragma unroll
@@ -256,24 +257,27 @@ __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
     __syncthreads();
     if (tid == 0) {
         const int avail = max(1, grid - rtot);
-        int R = kTileM;
+        int R = kTileM, hv = 0;
         for (int j = 0; j < 16; j++) {
             int tiles = 0;
             for (int w = 0; w < nw; w++) tiles += w_t[w][j];
             if (tiles <= avail) {
                 R = 8 * (j + 1);
+                hv = 1;
                 break;
             }
         }
         s_R = max(P.min_rows, R);
+        s_hv = hv;
     }
     __syncthreads();
     const int R = s_R;
+    const bool hv = s_hv != 0;
     // exclusive scan of the tiles per group over the block: each thread a contiguous range
     const int per = (G + nt - 1) / nt, g0 = min(G, tid * per), g1 = min(G, g0 + per);
     int c = 0;
     for (int g = g0; g < g1; g++) {
-        const int r = group_rows(R, heavy_group(P, g));
+        const int r = group_rows(R, hv && heavy_group(P, g));
         c += (__ldcg(cnt + g) + r - 1) / r;
     }
     int inc = c;
@@ -295,12 +299,12 @@ __device__ void split_plan(const Params &P, const int *cnt, int rtot, int grid)
     int acc = inc - c + (warp ? w_s[warp - 1] : 0);
     for (int g = g0; g < g1; g++) {
         P.splan[1 + g] = acc;
-        const int r = group_rows(R, heavy_group(P, g));
+        const int r = group_rows(R, hv && heavy_group(P, g));
         acc += (__ldcg(cnt + g) + r - 1) / r;
     }
     if (tid == nt - 1) {
         P.splan[1 + G] = acc;
-        P.splan[0] = R;
+        P.splan[0] = R | (hv ? 0x10000 : 0);  // rows per tile; the bit: heavy buckets take fewer
     }
     __syncthreads();
 }
@@ -413,7 +417,9 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
         int *rlist_next = P.rlist + (size_t)((s + 1) & 1) * P.n;
         int *rcnt_next = P.rcnt + (s + 1) % 3;
         const int Rtot = __ldcg(P.rcnt + s % 3);  // FP64 rechecks of this micro-step
-        const int R = __ldcg(P.splan), T = __ldcg(P.splan + 1 + G);  // this step's plan (rows per tile, tiles)
+        const int Rw = __ldcg(P.splan), T = __ldcg(P.splan + 1 + G);  // this step's plan (rows per tile, tiles)
+        const int R = Rw & 0xFFFF;
+        const bool heavy_fewer = (Rw >> 16) != 0;
         if (T + Rtot == 0) break;  // nothing left in this call (every CTA reads the same plan)
         if (blockIdx.x == 0) {
             for (int i = tid; i < G; i += kThreads) P.cnt[((s + 2) % 3) * G + i] = 0;
@@ -434,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_step_kernel(const Params P,
             const int g = split_tile_group(P, t, lane);  // every warp finds it (warp-uniform)
             const int e = P.g_ens[g];
             const int d = P.e_d[e], MDs = P.e_mds[e], KS = P.e_ks[e], bbytes = MDs * 32;
-            const int Rg = group_rows(R, g - P.e_g0[e] >= P.nb * P.deep);
+            const int Rg = group_rows(R, heavy_fewer && g - P.e_g0[e] >= P.nb * P.deep);
             const int base = (t - __ldcg(P.splan + 1 + g)) * Rg;
             const int rows = min(Rg, __ldcg(cnt_cur + g) - base);
             if (tid < kTileM) {
