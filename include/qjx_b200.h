@@ -93,7 +93,10 @@ typedef struct {
                           cores as bf16 hi/lo planes with FP32 accumulation (products hi*hi + hi*lo +
                           lo*hi), states, norms, thresholds, jump times and renormalisation stay
                           FP64.  Needs d <= 256.  QJX has no such mode
-                          (its zgemv is FP64). */
+                          (its zgemv is FP64).  A split engine runs a batch of micro-steps as one
+                          cooperative launch (one CTA per SM); when another context holds SMs it
+                          runs them one launch each, with the same results ($QJX_SPLIT_COOP=0
+                          selects that from the start). */
     const double *branch_len; /* [num_branches] durations of the branches of a period (NULL: T / 2
                           each, the dimer's half periods); systems with unequal parts (the JCS kick
                           and free evolution, init_split_structure_jcs, core.cpp:10086-10124) give
@@ -150,8 +153,9 @@ typedef struct {
  * the same persistent micro-step launches (every (ensemble, matrix) pair is a bucket of the
  * grouped GEMM; a sub-tile multiplies only its ensemble's d x d block).  cfg supplies what the
  * ensembles share: deep, num_branches, num_diss, num_robs, record, rng_kind, rec_cap, keep_adr,
- * max_dumps, device, deep_num_steps; cfg's d, n_traj, T, seed and tr_base are ignored and
- * precision must be 0.  Trajectories are numbered ensemble after ensemble; states and
+ * max_dumps, device, deep_num_steps, precision (1 needs every ensemble's d <= 256; each then has
+ * its own bf16 planes, k-steps and padded rows); cfg's d, n_traj, T, seed and tr_base are
+ * ignored.  Trajectories are numbered ensemble after ensemble; states and
  * observables use the largest dimension as row length (qjx_set_states: rows zero-padded past
  * each ensemble's d).  Every trajectory is bit-identical to its run in an engine of its own.
  * The Lyapunov entry points, qjx_purity and the RK propagator take single-ensemble engines. */
